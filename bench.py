@@ -1,0 +1,374 @@
+"""Benchmark of the spin-dynamics step (spin-steps/s) on B200.
+
+Workload (one replica per GPU, weak scaling): 256x256x8 simple-cubic film,
+periodic in x/y and open in z (zero-padded FFT in z); nearest-neighbour
+exchange J=1; anisotropy K=0.05 along z; dipole g=0.02; applied field 0.1
+along x; thermal noise T=0.5; alpha=0.05, dt=0.005; spins +z with a seeded
+5-degree random tilt; LLG.Quaternion.  One step = resetFields, the five
+operators, sumFields, llg:apply -- the plain fused FFT path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Timing: each timed step is bracketed by CUDA events on the launching stream
+and followed by an L2 flush (a 1 GiB write, excluded from the step time);
+the value is total spin-steps over the max over ranks of the summed step
+times.  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 256, 256, 8
+J, K_ANI, G_DIP, BX = 1.0, 0.05, 0.02, 0.1
+TEMP, ALPHA, DT = 0.5, 0.05, 0.005
+WORKLOAD = "film 256x256x8, periodic x/y, open z (z padded to 16), J=1, K=0.05 z, g=0.02, B=0.1 x, T=0.5, alpha=0.05, dt=0.005, LLG.Quaternion"
+METRIC = "spin-steps/s"
+UNIT = "spin-steps/s"
+FLUSH_BYTES = 1 << 30
+
+
+def tilted_spins(n, seed, deg=5.0):
+    r = np.random.default_rng(seed)
+    phi = r.uniform(0, 2 * np.pi, n)
+    th = np.deg2rad(deg)
+    return np.stack([np.sin(th) * np.cos(phi), np.sin(th) * np.sin(phi), np.full(n, np.cos(th))])
+
+
+def nn_paths(nx, ny, nz, pbc=(1, 1, 0)):
+    """Pathways of the canonical setup loop ex:add({i,j,k},{i+-1,...},J)."""
+    idx = np.arange(nx * ny * nz).reshape(nz, ny, nx)
+    frm, to = [], []
+    for ax, n in ((2, nx), (1, ny), (0, nz)):
+        for sgn in (1, -1):
+            src = idx
+            dst = np.roll(idx, -sgn, axis=ax)
+            if not pbc[2 - ax]:
+                sl = [slice(None)] * 3
+                sl[ax] = slice(0, n - 1) if sgn == 1 else slice(1, n)
+                src, dst = src[tuple(sl)], dst[tuple(sl)]
+            frm.append(src.ravel())
+            to.append(dst.ravel())
+    f = np.concatenate(frm).astype(np.int32)
+    t = np.concatenate(to).astype(np.int32)
+    return f, t, np.full(len(f), J)
+
+
+def build_system(M, seed):
+    n = NX * NY * NZ
+    ss = M.SpinSystem(NX, NY, NZ)
+    ss.setSpinArrays(*tilted_spins(n, seed))
+    ss.setAlpha(ALPHA)
+    ss.setTimeStep(DT)
+    ex = M.Exchange(ss)
+    ex.addPaths(*nn_paths(NX, NY, NZ))
+    ani = M.Anisotropy(ss)
+    ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, K_ANI))
+    th = M.Thermal(ss, M.Random.Philox(1000 + seed))
+    th.setTemperature(TEMP)
+    z = M.AppliedField(ss)
+    z.set(BX, 0, 0)
+    dip = M.Dipole(ss)
+    dip.setStrength(G_DIP)
+    llg = M.LLG.new("Quaternion")
+    return ss, [ex, ani, th, z, dip], llg
+
+
+# ----------------------------------------------------------------- algorithmic bytes
+def algorithmic_bytes():
+    """Per-launch algorithmic bytes of each kernel, split from the per
+    spin-step figure B = 36 + 24 + (K/N)(24 + 48*2) with K = (Px/2+1)*Py*Pz:
+    fused stencil/LLG 36 B/site; forward x pass 12 B/site + 24 B/k;
+    (y,z) pass with the tensor multiply 24+24+24 B/k; inverse x pass 24 B/k
+    + 12 B/site."""
+    n = NX * NY * NZ
+    Px, Py, Pz = NX, NY, 16
+    Kk = (Px // 2 + 1) * Py * Pz
+    return {
+        "k_fused_step": 36 * n,
+        "k_conv_fx": 12 * n + 24 * Kk,
+        "k_conv_yz": 72 * Kk,
+        "k_conv_ix": 24 * Kk + 12 * n,
+    }, (36 + 24) * n + Kk * (24 + 48 * 2), n, Kk
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- CPU baseline (oracle)
+def _cpu_worker(args):
+    seed, steps = args
+    import oracle as O
+    n = NX * NY * NZ
+    ss = O.SpinSystem(NX, NY, NZ)
+    ss.set_spins(*tilted_spins(n, seed))
+    ss.alpha, ss.dt = ALPHA, DT
+    f, t, j = nn_paths(NX, NY, NZ)
+    sites = np.arange(n, dtype=np.int32)
+    ani = (sites, np.tile([0, 0, 1.0], (n, 1)), np.full(n, K_ANI))
+    lr = O.LongRange(NX, NY, NZ, O.dipole_tensor(NX, NY, NZ))
+    rng = O.MT(1000 + seed)
+    O.run_steps(ss, 1, paths=(f, t, j), ani=ani, T=TEMP, rng=rng, B=(BX, 0, 0), lr=lr, g=G_DIP,
+                llg="Quaternion")
+    t0 = time.perf_counter()
+    O.run_steps(ss, steps, paths=(f, t, j), ani=ani, T=TEMP, rng=rng, B=(BX, 0, 0), lr=lr, g=G_DIP,
+                llg="Quaternion")
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(procs=1, target_s=15.0):
+    """The FP64 CPU restatement of the reference's modules on the host cores:
+    `procs` independent replicas in parallel (one process each)."""
+    import multiprocessing as mp
+    import oracle as O  # noqa: F401  (builds liboracle.so if needed)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        t1 = pool.map(_cpu_worker, [(0, 1)])[0]
+    steps = int(max(2, min(200, target_s / max(t1, 1e-6))))
+    with ctx.Pool(procs) as pool:
+        times = pool.map(_cpu_worker, [(r, steps) for r in range(procs)])
+    n = NX * NY * NZ
+    val = procs * n * steps / max(times)
+    return {"value": val, "unit": UNIT, "cores": procs, "kind": "port",
+            "sample": f"{steps} steps of the full {NX}x{NY}x{NZ} workload per process, {procs} process(es), "
+                      f"FP64 C restatement (gcc -O2), Mersenne-Twister thermal noise, own FFT in place of FFTW"}
+
+
+# ----------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        procs = os.cpu_count() or 1
+        cb = cpu_baseline(procs=procs, target_s=20.0)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "replicas": procs, "parallelism": f"replicas{procs}"},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    import maglua_b200 as M
+    M.init(local)
+    ss, ops, llg = build_system(M, seed=rank)
+    stream = torch.cuda.ExternalStream(ss.stream())
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    n = NX * NY * NZ
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (plans, tensor setup, graphs)
+    M.run(ss, ops, llg, args.warmup)
+    ss.synchronize()
+
+    # timed region: per-step events, L2 flush between steps
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    with M.profile() as prof:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            evs[k][0].record(stream)
+            M.run(ss, ops, llg, 1)
+            evs[k][1].record(stream)
+        ss.synchronize()
+    barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms * 1e-3)
+
+    # steady state without flushes: graph-captured run (L2-resident state)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    M.run(ss, ops, llg, args.steps)
+    e1.record(stream)
+    ss.synchronize()
+    ss_ms = e0.elapsed_time(e1)
+
+    # end to end through the C ABI with host buffers
+    hx, hy, hz = (torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(3))
+    hm = torch.ones(n, dtype=torch.float32).pin_memory().numpy()
+    s0 = tilted_spins(n, rank)
+    hx[:], hy[:], hz[:] = s0
+    barrier()
+    t0 = time.perf_counter()
+    ss.uploadF32(hx, hy, hz, hm)
+    for k in range(args.steps):
+        M.run(ss, ops, llg, 1)
+        ss.netMoment()
+    ss.downloadF32(hx, hy, hz)
+    ss.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = world * n * args.steps / e2e_s
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    per_launch, bytes_step, _, Kk = algorithmic_bytes()
+    peak, peak_kind = measured_peak()
+    traffic = ncu_traffic()
+    kern = {k: v for k, v in prof.kernels.items() if k in per_launch}
+    dom = max(kern, key=lambda k: kern[k][0]) if kern else None
+    roof = None
+    kernels_out = {}
+    for k, (ms, nl) in kern.items():
+        avg = ms / nl
+        ach = per_launch[k] / (avg * 1e-3) / 1e9
+        kernels_out[k] = {"avg_us": avg * 1e3, "launches": nl, "share": ms / sum(v[0] for v in kern.values()),
+                          "algorithmic_bytes": per_launch[k], "achieved_gbs": ach}
+    if dom:
+        ms, nl = kern[dom]
+        avg = ms / nl
+        ach = per_launch[dom] / (avg * 1e-3) / 1e9
+        tr = traffic.get(dom)
+        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_kind": peak_kind + " (burst copy)",
+                "traffic": tr, "algorithmic_bytes_per_launch": per_launch[dom]}
+    step_bytes_gbs = bytes_step / (total_ms / args.steps * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu and world == 1:
+        cpu = cpu_baseline(procs=1, target_s=15.0)
+    launches = sum(v[1] for v in kern.values()) + sum(v[1] for k, v in prof.kernels.items() if k not in per_launch)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sites_per_gpu": n, "parallelism": f"replicas{world}",
+                   "l2": "flushed between steps (1 GiB write, excluded by per-step CUDA events)",
+                   "llg": "Quaternion", "path": "plain fused FFT path"},
+        "clocks": clk,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": (16 * n) / args.steps,
+                "d2h_bytes_per_step": 48 + (12 * n) / args.steps,
+                "how": "C-ABI calls from host: pinned FP32 upload, per step mlb_run(1) + netMoment read, final download"},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "kernels": kernels_out,
+        "step_roofline": {"bytes_per_spin_step": bytes_step / n, "achieved_gbs": step_bytes_gbs,
+                          "frac": step_bytes_gbs / peak, "K_points": Kk},
+        "steady_state_l2_resident": {"value": n * args.steps / (ss_ms * 1e-3), "ms_per_step": ss_ms / args.steps,
+                                     "how": "mlb_run graph over the same steps, no flush"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

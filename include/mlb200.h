@@ -1,0 +1,216 @@
+/*
+ * mlb200.h -- C ABI of the B200-native MagLua spin-dynamics step.
+ *
+ * Plain C types only (ints, doubles, pointers, sizes); every function returns
+ * MLB_OK (0) or a negative MLB_E* code and never throws, exits or traps.  The
+ * message of the last failure on the calling thread is mlb_last_error().
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the MagLua project root; M/ = src/modules/).  In MagLua those are Lua
+ * methods of C++ classes registered by luaT_register<T>
+ * (M/common/luabaseobject/luabaseobject.h:643-700); a Lua 5.1 glue module
+ * maps each method onto one call below.
+ *
+ * State lives on the GPU in FP32 (SoA x, y, z, ms; one stream per system);
+ * host-facing values are FP64 like the reference.  Reductions are FP64.
+ */
+#ifndef MLB200_H
+#define MLB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLB_OK 0
+#define MLB_EINVAL -1     /* bad argument (luaL_error "invalid ..." in the reference) */
+#define MLB_ENOMEM -2     /* device allocation failed */
+#define MLB_ECUDA -3      /* CUDA runtime error */
+#define MLB_ESTATE -4     /* operation not possible in this state ("Missing RNG", ...) */
+#define MLB_ENOTFOUND -5  /* unknown slot name ("Unknown field type") */
+#define MLB_ERANGE -6     /* site or size outside the system */
+#define MLB_EUNSUP -7     /* size/configuration this build does not support */
+
+typedef struct mlb_system mlb_system;
+typedef struct mlb_op mlb_op;
+typedef struct mlb_llg mlb_llg;
+
+/* ---------------------------------------------------------------- library */
+const char* mlb_last_error(void);
+int mlb_version(void);
+/* Select the CUDA device (the cuda core's lib_main / "-gpu N" option,
+ * M/cuda/core_cuda/maglua.cpp:50-93). */
+int mlb_init(int device);
+/* Per-kernel timing (no reference counterpart; the reference has only the
+ * wall-clock Timer, M/common/timer/mtimer.cpp:219-350).  Between begin and
+ * end every kernel launched outside a graph capture is bracketed by CUDA
+ * events on its stream; end synchronises and returns per kernel name
+ * (48-byte slots in names) the summed milliseconds and launch counts. */
+int mlb_profile_begin(void);
+int mlb_profile_end(int cap, char* names, double* ms, int* launches, int* count);
+/* The counter-based generator behind Thermal (no reference counterpart: the
+ * reference uses Mersenne Twister on the host, Random.HybridTaus on the GPU,
+ * M/cuda/random_cuda/hybridtaus.cu:32-88).  Host-callable; for checks. */
+int mlb_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* ---------------------------------------------------------------- SpinSystem
+ * M/cpu/core/spinsystem.h:33-140; methods spinsystem.cpp:3233-3318 and
+ * spinsystem_luafuncs.lua. */
+int mlb_system_create(int nx, int ny, int nz, mlb_system** out);      /* SpinSystem.new(nx,ny,nz) */
+int mlb_system_destroy(mlb_system* s);                                 /* __gc */
+int mlb_system_dims(const mlb_system* s, int out[3]);                  /* nx(), ny(), nz() */
+/* Launch on this stream from now on (NULL = the system's own stream). */
+int mlb_system_set_stream(mlb_system* s, void* cuda_stream);
+int mlb_system_get_stream(const mlb_system* s, void** cuda_stream);
+int mlb_system_synchronize(mlb_system* s);
+/* setSpin(i,j,k, sx,sy,sz[, m]) for one site (l_setspin :1312-1361); idx is
+ * the 0-based x + nx*(y + ny*z). */
+int mlb_system_set_spin(mlb_system* s, int idx, double sx, double sy, double sz);
+int mlb_system_get_spin(mlb_system* s, int idx, double out4[4]);       /* spin(i,j,k) */
+/* Whole arrays (setSpinArrayX/Y/Z/M, spinArrayX/Y/Z/M :2164-2305).  With
+ * ms == NULL every ms becomes |s| (SpinSystem::set). */
+int mlb_system_set_spins(mlb_system* s, const double* x, const double* y, const double* z,
+                         const double* ms);
+int mlb_system_get_spins(mlb_system* s, double* x, double* y, double* z, double* ms);
+/* FP32 host buffers (pinned memory recommended) for bulk I/O. */
+int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const float* z,
+                          const float* ms);
+int mlb_system_download_f32(mlb_system* s, float* x, float* y, float* z);
+/* Scalars: setAlpha/alpha, setGamma/gamma, setTimeStep/timeStep, setTime/time. */
+#define MLB_ALPHA 0
+#define MLB_GAMMA 1
+#define MLB_DT 2
+#define MLB_TIME 3
+int mlb_system_set_param(mlb_system* s, int which, double v);
+int mlb_system_get_param(const mlb_system* s, int which, double* v);
+/* setSiteAlphaArray / setSiteGammaArray (NULL clears: setAlpha resets). */
+int mlb_system_set_site_alpha(mlb_system* s, const double* a);
+int mlb_system_set_site_gamma(mlb_system* s, const double* g);
+/* resetFields (zeroFields :968-980), sumFields (:853-871). */
+int mlb_system_reset_fields(mlb_system* s);
+int mlb_system_sum_fields(mlb_system* s);
+/* sumFields(dest, {{w, name}, ...}) (spinsystem_luafuncs.lua:298-360). */
+int mlb_system_sum_fields_custom(mlb_system* s, const char* dest, int n, const char* const* src,
+                                 const double* w);
+/* fieldArrayX/Y/Z(name) (:1656-1690); any of hx/hy/hz may be NULL. */
+int mlb_system_get_field(mlb_system* s, const char* slot, double* hx, double* hy, double* hz);
+/* setFieldArrayX/Y/Z (:1692-1728); NULL components are left unchanged. */
+int mlb_system_set_field(mlb_system* s, const char* slot, const double* hx, const double* hy,
+                         const double* hz);
+int mlb_system_slot_used(mlb_system* s, const char* slot, int* used);  /* _slotUsed */
+int mlb_system_set_slot_used(mlb_system* s, const char* slot, int used);
+int mlb_system_ensure_slot(mlb_system* s, const char* slot);          /* _ensureSlotExists */
+/* netMoment(m): 8 numbers as the Lua method (spinsystem_luafuncs.lua:17-54). */
+int mlb_system_netmoment(mlb_system* s, double m, double out8[8]);
+/* sum_i s_i . h_slot,i in FP64 (the fieldArray:dot(spinArray) energy pattern). */
+int mlb_system_field_dot(mlb_system* s, const char* slot, double* out);
+/* copyTo / copySpinsTo (:1846-1898): spins, ms, scalars (and fields when
+ * with_fields). */
+int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields);
+
+/* ---------------------------------------------------------------- operators
+ * SpinOperation base, M/cpu/core/spinoperation.h:28-72. */
+#define MLB_OP_EXCHANGE 1       /* M/cpu/exchange */
+#define MLB_OP_ANISOTROPY 2     /* M/cpu/anisotropy (generic) */
+#define MLB_OP_UNIAXIAL 3       /* Anisotropy.Uniaxial */
+#define MLB_OP_CUBIC 4          /* Anisotropy.Cubic */
+#define MLB_OP_THERMAL 5        /* M/cpu/thermal */
+#define MLB_OP_APPLIEDFIELD 6   /* M/cpu/appliedfield */
+#define MLB_OP_DIPOLE 7         /* M/cpu/dipole */
+#define MLB_OP_LONGRANGE 8      /* M/cpu/longrange (user tensor) */
+#define MLB_OP_LONGRANGE3D 9    /* M/cpu/longrange3d */
+int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out);     /* X.new(nx,ny,nz) */
+int mlb_op_destroy(mlb_op* op);
+int mlb_op_kind(const mlb_op* op, int* kind);
+int mlb_op_set_scale(mlb_op* op, double global_scale);                 /* setScale */
+int mlb_op_get_scale(const mlb_op* op, double* global_scale);
+int mlb_op_set_slot_name(mlb_op* op, const char* name);                /* setSlotName */
+int mlb_op_get_slot_name(const mlb_op* op, char* buf, size_t len);     /* slotName */
+/* Reproduce the reference's arithmetic quirks (default on): Uniaxial sz*nx
+ * (..._uniaxial.cpp:287), Cubic n3s3 (..._cubic.cpp:372-374), LongRange
+ * interlayer z-sign (spinoperationlongrange.cpp:377-384). */
+int mlb_op_set_quirks(mlb_op* op, int on);
+/* op:apply(ss) and op:apply({ss1, ss2, ...}) (spinoperation.cpp:423-446). */
+int mlb_op_apply(mlb_op* op, mlb_system* s);
+int mlb_op_apply_many(mlb_op* op, mlb_system* const* s, int n);
+
+/* Exchange: ex:add(from, to, J) after pbc wrapping (l_addpath :368-420),
+ * normalizeMoments (:283-292, exchange_luafuncs.lua:10-17). */
+int mlb_exchange_add_path(mlb_op* op, int from, int to, double J);
+int mlb_exchange_add_paths(mlb_op* op, const int* from, const int* to, const double* J, int n);
+int mlb_exchange_set_normalize(mlb_op* op, int on);
+int mlb_exchange_num_paths(const mlb_op* op, int* n);
+/* Anisotropy: ani:add(site, axis, K) (axis normalised, spinoperationanisotropy.cpp:367-410). */
+int mlb_anisotropy_add(mlb_op* op, int site, const double axis[3], double K);
+/* Anisotropy.Uniaxial: add(site, axis, K1, K2) (..._uniaxial.cpp:158-179). */
+int mlb_uniaxial_add(mlb_op* op, int site, const double axis[3], double K1, double K2);
+/* Anisotropy.Cubic: add(site, a1, a2, K1, K2, K3) (..._cubic.cpp:180-236);
+ * MLB_EINVAL for zero-length or colinear axes. */
+int mlb_cubic_add(mlb_op* op, int site, const double a1[3], const double a2[3], const double K[3]);
+/* Bulk forms of the three add calls (one call per site in the reference's
+ * setup loops; n sites, axes 3 per site, K 1 (generic), K1/K2 (uniaxial),
+ * a1/a2 3 per site and K 3 per site (cubic)). */
+int mlb_anisotropy_add_many(mlb_op* op, int n, const int* sites, const double* axes, const double* K);
+int mlb_uniaxial_add_many(mlb_op* op, int n, const int* sites, const double* axes, const double* K1,
+                          const double* K2);
+int mlb_cubic_add_many(mlb_op* op, int n, const int* sites, const double* a1, const double* a2, const double* K);
+/* Thermal (spinoperationthermal.cpp:135-387): temperature, per-site scale,
+ * counter-based Philox stream (seed), or injected normals for the next apply
+ * (three arrays of nxyz standard normals, as drawn by the reference RNG). */
+int mlb_thermal_set_temperature(mlb_op* op, double T);
+int mlb_thermal_get_temperature(const mlb_op* op, double* T);
+int mlb_thermal_scale_site(mlb_op* op, int idx, double v);
+int mlb_thermal_set_seed(mlb_op* op, uint64_t seed);        /* keeps the counter */
+int mlb_thermal_set_counter(mlb_op* op, uint64_t counter);
+int mlb_thermal_inject(mlb_op* op, const double* nx, const double* ny, const double* nz);
+/* AppliedField set/get (appliedfield_luafuncs.lua), plus a per-step linear
+ * sweep used by mlb_run (B += dB each step). */
+int mlb_appliedfield_set(mlb_op* op, double bx, double by, double bz);
+int mlb_appliedfield_get(const mlb_op* op, double out3[3]);
+int mlb_appliedfield_set_sweep(mlb_op* op, double dbx, double dby, double dbz);
+/* LongRange / Dipole (spinoperationlongrange.cpp:460-875): strength,
+ * truncation gmax {r, x, y, z}, unit cell, tensor elements. */
+int mlb_longrange_set_strength(mlb_op* op, double g);
+int mlb_longrange_get_strength(const mlb_op* op, double* g);
+int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4]);
+int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9]);
+/* B200 extension: open (zero-padded) boundaries per axis for Dipole; the
+ * reference Dipole is periodic in x and y and open in z. */
+int mlb_longrange_set_open(mlb_op* op, int open_x, int open_y, int open_z);
+/* setMatrix/getMatrix(AB, {ox,oy,oz}) with AB in XX,XY,XZ,YY,YZ,ZZ = 0..5 */
+int mlb_longrange_set_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double v);
+int mlb_longrange_get_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double* v);
+/* The six tensor arrays, each nx*ny*(2nz-1), layout i + nx*(j + ny*(k+nz-1)). */
+int mlb_longrange_get_tensor(mlb_op* op, double* const t6[6]);
+/* LongRange3D (spinoperationlongrange3d.cpp:312-424, setMatrix): component
+ * ab = 3*a + b in XX..ZZ order, array nx*ny*nz. */
+int mlb_longrange3d_set_tensor(mlb_op* op, int ab, const double* t);
+
+/* ---------------------------------------------------------------- LLG
+ * M/cpu/llg/llg.cpp:91-171, llgcartesian.cpp:90-278, llgquat.cpp:126-378. */
+#define MLB_LLG_CARTESIAN 0
+#define MLB_LLG_QUATERNION 1
+int mlb_llg_create(int kind, mlb_llg** out);                            /* LLG.new("Cartesian") */
+int mlb_llg_destroy(mlb_llg* l);
+/* thermalOnlyFirstTerm (default 1), disableRenormalization (0),
+ * unphysical precession / damping scales (1, 1). */
+int mlb_llg_set_flags(mlb_llg* l, int thermal_only_first_term, int disable_renormalization,
+                      double precess_scale, double damp_scale);
+/* llg:apply(from[, scale], dmdt, to[, advance]) */
+int mlb_llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb_system* to,
+                  int advance);
+
+/* ---------------------------------------------------------------- fused run
+ * B200 extension: nsteps repetitions of the canonical script step
+ * (doc/manual/BasicMicromagneticSimulation.lua:84-94):
+ *   ss:resetFields(); for op in ops: op:apply(ss); ss:sumFields(); llg:apply(ss)
+ * with the per-step work captured in a CUDA graph.  The end state equals
+ * issuing those calls one by one. */
+int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,961 @@
+"""maglua_b200 -- B200-native MagLua spin-dynamics step.
+
+Python mirror of MagLua's Lua classes over the C ABI in include/mlb200.h
+(libmlb200.so, sm_100a).  Class and method names follow the reference's Lua
+API so scripts translate line by line:
+
+    ss  = SpinSystem.new(32, 32, 1)
+    ex  = Exchange.new(ss)
+    ani = Anisotropy.new(ss)
+    llg = LLG.new("Quaternion")
+    ...
+    ss.resetFields(); ex.apply(ss); ani.apply(ss); ss.sumFields(); llg.apply(ss)
+
+Sites are 1-based {x, y, z} tuples as in Lua.  Everything runs on the GPU;
+there is no CPU path: importing without the built library, or using it
+without a CUDA device, raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmlb200.so")
+
+MLB_OK = 0
+_ERRNAMES = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ESTATE", -5: "ENOTFOUND", -6: "ERANGE",
+             -7: "EUNSUP"}
+
+
+class MagLuaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+_I = C.POINTER(C.c_int)
+
+_SIGS = {
+    "mlb_last_error": ([], C.c_char_p),
+    "mlb_version": ([], C.c_int),
+    "mlb_init": ([C.c_int], C.c_int),
+    "mlb_profile_begin": ([], C.c_int),
+    "mlb_profile_end": ([C.c_int, C.c_char_p, _D, _I, _I], C.c_int),
+    "mlb_philox4x32_10": ([C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], C.c_int),
+    "mlb_system_create": ([C.c_int, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_system_destroy": ([_P], C.c_int),
+    "mlb_system_dims": ([_P, _I], C.c_int),
+    "mlb_system_set_stream": ([_P, _P], C.c_int),
+    "mlb_system_get_stream": ([_P, C.POINTER(_P)], C.c_int),
+    "mlb_system_synchronize": ([_P], C.c_int),
+    "mlb_system_set_spin": ([_P, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
+    "mlb_system_get_spin": ([_P, C.c_int, _D], C.c_int),
+    "mlb_system_set_spins": ([_P, _D, _D, _D, _D], C.c_int),
+    "mlb_system_get_spins": ([_P, _D, _D, _D, _D], C.c_int),
+    "mlb_system_upload_f32": ([_P, _P, _P, _P, _P], C.c_int),
+    "mlb_system_download_f32": ([_P, _P, _P, _P], C.c_int),
+    "mlb_system_set_param": ([_P, C.c_int, C.c_double], C.c_int),
+    "mlb_system_get_param": ([_P, C.c_int, _D], C.c_int),
+    "mlb_system_set_site_alpha": ([_P, _D], C.c_int),
+    "mlb_system_set_site_gamma": ([_P, _D], C.c_int),
+    "mlb_system_reset_fields": ([_P], C.c_int),
+    "mlb_system_sum_fields": ([_P], C.c_int),
+    "mlb_system_sum_fields_custom": ([_P, C.c_char_p, C.c_int, C.POINTER(C.c_char_p), _D], C.c_int),
+    "mlb_system_get_field": ([_P, C.c_char_p, _D, _D, _D], C.c_int),
+    "mlb_system_set_field": ([_P, C.c_char_p, _D, _D, _D], C.c_int),
+    "mlb_system_slot_used": ([_P, C.c_char_p, _I], C.c_int),
+    "mlb_system_set_slot_used": ([_P, C.c_char_p, C.c_int], C.c_int),
+    "mlb_system_ensure_slot": ([_P, C.c_char_p], C.c_int),
+    "mlb_system_netmoment": ([_P, C.c_double, _D], C.c_int),
+    "mlb_system_field_dot": ([_P, C.c_char_p, _D], C.c_int),
+    "mlb_system_copy": ([_P, _P, C.c_int], C.c_int),
+    "mlb_op_create": ([C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_op_destroy": ([_P], C.c_int),
+    "mlb_op_kind": ([_P, _I], C.c_int),
+    "mlb_op_set_scale": ([_P, C.c_double], C.c_int),
+    "mlb_op_get_scale": ([_P, _D], C.c_int),
+    "mlb_op_set_slot_name": ([_P, C.c_char_p], C.c_int),
+    "mlb_op_get_slot_name": ([_P, C.c_char_p, C.c_size_t], C.c_int),
+    "mlb_op_set_quirks": ([_P, C.c_int], C.c_int),
+    "mlb_op_apply": ([_P, _P], C.c_int),
+    "mlb_op_apply_many": ([_P, C.POINTER(_P), C.c_int], C.c_int),
+    "mlb_exchange_add_path": ([_P, C.c_int, C.c_int, C.c_double], C.c_int),
+    "mlb_exchange_add_paths": ([_P, _I, _I, _D, C.c_int], C.c_int),
+    "mlb_exchange_set_normalize": ([_P, C.c_int], C.c_int),
+    "mlb_exchange_num_paths": ([_P, _I], C.c_int),
+    "mlb_anisotropy_add": ([_P, C.c_int, _D, C.c_double], C.c_int),
+    "mlb_uniaxial_add": ([_P, C.c_int, _D, C.c_double, C.c_double], C.c_int),
+    "mlb_cubic_add": ([_P, C.c_int, _D, _D, _D], C.c_int),
+    "mlb_anisotropy_add_many": ([_P, C.c_int, _I, _D, _D], C.c_int),
+    "mlb_uniaxial_add_many": ([_P, C.c_int, _I, _D, _D, _D], C.c_int),
+    "mlb_cubic_add_many": ([_P, C.c_int, _I, _D, _D, _D], C.c_int),
+    "mlb_thermal_set_temperature": ([_P, C.c_double], C.c_int),
+    "mlb_thermal_get_temperature": ([_P, _D], C.c_int),
+    "mlb_thermal_scale_site": ([_P, C.c_int, C.c_double], C.c_int),
+    "mlb_thermal_set_seed": ([_P, C.c_uint64], C.c_int),
+    "mlb_thermal_set_counter": ([_P, C.c_uint64], C.c_int),
+    "mlb_thermal_inject": ([_P, _D, _D, _D], C.c_int),
+    "mlb_appliedfield_set": ([_P, C.c_double, C.c_double, C.c_double], C.c_int),
+    "mlb_appliedfield_get": ([_P, _D], C.c_int),
+    "mlb_appliedfield_set_sweep": ([_P, C.c_double, C.c_double, C.c_double], C.c_int),
+    "mlb_longrange_set_strength": ([_P, C.c_double], C.c_int),
+    "mlb_longrange_get_strength": ([_P, _D], C.c_int),
+    "mlb_longrange_set_truncation": ([_P, _I], C.c_int),
+    "mlb_longrange_set_unit_cell": ([_P, _D], C.c_int),
+    "mlb_longrange_set_open": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "mlb_longrange_set_matrix": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double], C.c_int),
+    "mlb_longrange_get_matrix": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, _D], C.c_int),
+    "mlb_longrange_get_tensor": ([_P, _D * 6], C.c_int),
+    "mlb_longrange3d_set_tensor": ([_P, C.c_int, _D], C.c_int),
+    "mlb_llg_create": ([C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_llg_destroy": ([_P], C.c_int),
+    "mlb_llg_set_flags": ([_P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
+    "mlb_llg_apply": ([_P, _P, C.c_double, _P, _P, C.c_int], C.c_int),
+    "mlb_run": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int], C.c_int),
+}
+EXPORTED = tuple(_SIGS)
+
+
+class _Lib:
+    """libmlb200.so, loaded on first use.  A missing library raises: there
+    is no fallback implementation."""
+
+    def __init__(self):
+        self._cdll = None
+
+    def load(self):
+        if self._cdll is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(f"{LIB_PATH} is missing: build it with "
+                                  "`python -m maglua_b200.build` (nvcc, sm_100a)")
+            lib = C.CDLL(LIB_PATH)
+            for name, (args, res) in _SIGS.items():
+                f = getattr(lib, name)
+                f.argtypes = args
+                f.restype = res
+            self._cdll = lib
+        return self._cdll
+
+    def __getattr__(self, name):
+        return getattr(self.load(), name)
+
+
+_lib = _Lib()
+
+
+def philox4x32_10(ctr, key):
+    """Host evaluation of the Thermal noise generator (for checks)."""
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    _lib.mlb_philox4x32_10(c, k, o)
+    return tuple(o)
+
+
+def _ck(rc):
+    if rc != MLB_OK:
+        raise MagLuaError(rc, _lib.mlb_last_error().decode())
+
+
+_initialised = [False]
+
+
+def init(device=None):
+    """Select the CUDA device (MagLua's -gpu N).  Called on first use."""
+    if device is None:
+        device = int(os.environ.get("LOCAL_RANK", "0"))
+    _ck(_lib.mlb_init(device))
+    _initialised[0] = True
+
+
+def _ensure_init():
+    if not _initialised[0]:
+        init()
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _site3(site):
+    s = list(site) if hasattr(site, "__len__") else [site]
+    while len(s) < 3:
+        s.append(1)
+    return int(s[0]), int(s[1]), int(s[2])
+
+
+# ====================================================================== SpinSystem
+class SpinSystem:
+    """SpinSystem (M/cpu/core/spinsystem.h:33-140) with its state on the GPU."""
+
+    ALPHA, GAMMA, DT, TIME = 0, 1, 2, 3
+
+    def __init__(self, nx, ny=1, nz=1):
+        _ensure_init()
+        if isinstance(nx, SpinSystem):
+            nx, ny, nz = nx.nx(), nx.ny(), nx.nz()
+        elif hasattr(nx, "__len__"):
+            nx, ny, nz = _site3(nx)
+        h = _P()
+        _ck(_lib.mlb_system_create(int(nx), int(ny), int(nz), C.byref(h)))
+        self._h = h
+        self._dims = (int(nx), int(ny), int(nz))
+
+    new = classmethod(lambda cls, *a: cls(*a))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_system_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    # geometry
+    def nx(self):
+        return self._dims[0]
+
+    def ny(self):
+        return self._dims[1]
+
+    def nz(self):
+        return self._dims[2]
+
+    def nxyz(self):
+        return self._dims[0] * self._dims[1] * self._dims[2]
+
+    def _idx(self, site):
+        x, y, z = _site3(site)
+        nx, ny, nz = self._dims
+        # SpinSystem::getidx wraps periodically (spinsystem.cpp:1125-1142)
+        x, y, z = (x - 1) % nx, (y - 1) % ny, (z - 1) % nz
+        return x + nx * (y + ny * z)
+
+    # streams
+    def setStream(self, stream):
+        _ck(_lib.mlb_system_set_stream(self._h, C.c_void_p(stream or 0)))
+
+    def stream(self):
+        out = _P()
+        _ck(_lib.mlb_system_get_stream(self._h, C.byref(out)))
+        return out.value or 0
+
+    def synchronize(self):
+        _ck(_lib.mlb_system_synchronize(self._h))
+
+    # spins
+    def setSpin(self, site, spin, m=None):
+        """l_setspin (spinsystem.cpp:1312-1361): optional length m."""
+        sx, sy, sz = (list(spin) + [0, 0, 0])[:3]
+        if m is not None:
+            ln = abs(m)
+            rr = sx * sx + sy * sy + sz * sz
+            if rr > 0:
+                rr = ln / np.sqrt(rr)
+                sx, sy, sz = sx * rr, sy * rr, sz * rr
+            else:
+                sx, sy, sz = 0.0, 0.0, ln
+        _ck(_lib.mlb_system_set_spin(self._h, self._idx(site), sx, sy, sz))
+
+    def spin(self, site):
+        out = np.zeros(4)
+        _ck(_lib.mlb_system_get_spin(self._h, self._idx(site), _dp(out)))
+        return tuple(out)
+
+    def setSpinArrays(self, x, y, z, ms=None):
+        n = self.nxyz()
+        x, y, z = _f64(x, n), _f64(y, n), _f64(z, n)
+        m = None if ms is None else _f64(ms, n)
+        _ck(_lib.mlb_system_set_spins(self._h, _dp(x), _dp(y), _dp(z), _dp(m)))
+
+    def spinArrays(self):
+        n = self.nxyz()
+        x, y, z, m = (np.zeros(n) for _ in range(4))
+        _ck(_lib.mlb_system_get_spins(self._h, _dp(x), _dp(y), _dp(z), _dp(m)))
+        return x, y, z, m
+
+    def spinArrayX(self):
+        return self.spinArrays()[0]
+
+    def spinArrayY(self):
+        return self.spinArrays()[1]
+
+    def spinArrayZ(self):
+        return self.spinArrays()[2]
+
+    def spinArrayM(self):
+        return self.spinArrays()[3]
+
+    def uploadF32(self, x, y, z, ms=None):
+        """Bulk FP32 upload from host buffers (pinned memory recommended)."""
+        _ck(_lib.mlb_system_upload_f32(self._h, x.ctypes.data, y.ctypes.data, z.ctypes.data,
+                                       ms.ctypes.data if ms is not None else None))
+
+    def downloadF32(self, x, y, z):
+        _ck(_lib.mlb_system_download_f32(self._h, x.ctypes.data, y.ctypes.data, z.ctypes.data))
+
+    # scalars
+    def _set(self, which, v):
+        _ck(_lib.mlb_system_set_param(self._h, which, float(v)))
+
+    def _get(self, which):
+        v = C.c_double()
+        _ck(_lib.mlb_system_get_param(self._h, which, C.byref(v)))
+        return v.value
+
+    def setAlpha(self, a):
+        self._set(0, a)
+
+    def alpha(self):
+        return self._get(0)
+
+    def setGamma(self, g):
+        self._set(1, g)
+
+    def gamma(self):
+        return self._get(1)
+
+    def setTimeStep(self, dt):
+        self._set(2, dt)
+
+    def timeStep(self):
+        return self._get(2)
+
+    def setTime(self, t):
+        self._set(3, t)
+
+    def time(self):
+        return self._get(3)
+
+    def setSiteAlphaArray(self, a):
+        _ck(_lib.mlb_system_set_site_alpha(self._h, _dp(None if a is None else _f64(a, self.nxyz()))))
+
+    def setSiteGammaArray(self, g):
+        _ck(_lib.mlb_system_set_site_gamma(self._h, _dp(None if g is None else _f64(g, self.nxyz()))))
+
+    # fields
+    def resetFields(self):
+        _ck(_lib.mlb_system_reset_fields(self._h))
+
+    zeroFields = resetFields
+
+    def sumFields(self, dest=None, srcs=None):
+        """sumFields() / sumFields({names}) / sumFields(dest, {{w, name}, ...})."""
+        if dest is None and srcs is None:
+            _ck(_lib.mlb_system_sum_fields(self._h))
+            return
+        if isinstance(dest, (list, tuple)) and srcs is None:
+            dest, srcs = "Total", dest
+        names, w = [], []
+        for s in srcs:
+            if isinstance(s, (list, tuple)):
+                w.append(float(s[0]))
+                names.append(_slotname(s[1]))
+            else:
+                w.append(1.0)
+                names.append(_slotname(s))
+        arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
+        ww = _f64(w)
+        _ck(_lib.mlb_system_sum_fields_custom(self._h, _slotname(dest).encode(), len(names), arr, _dp(ww)))
+
+    def fieldArrays(self, name):
+        n = self.nxyz()
+        hx, hy, hz = np.zeros(n), np.zeros(n), np.zeros(n)
+        _ck(_lib.mlb_system_get_field(self._h, _slotname(name).encode(), _dp(hx), _dp(hy), _dp(hz)))
+        return hx, hy, hz
+
+    def fieldArrayX(self, name):
+        return self.fieldArrays(name)[0]
+
+    def fieldArrayY(self, name):
+        return self.fieldArrays(name)[1]
+
+    def fieldArrayZ(self, name):
+        return self.fieldArrays(name)[2]
+
+    def field(self, name, site=None):
+        if site is None and not isinstance(name, str):
+            name, site = "Total", name
+        hx, hy, hz = self.fieldArrays(name)
+        i = self._idx(site)
+        v = (hx[i], hy[i], hz[i])
+        return v + (float(np.sqrt(sum(a * a for a in v))),)
+
+    def setFieldArrays(self, name, hx=None, hy=None, hz=None):
+        n = self.nxyz()
+        a = [None if v is None else _f64(v, n) for v in (hx, hy, hz)]
+        _ck(_lib.mlb_system_set_field(self._h, _slotname(name).encode(), *[_dp(v) for v in a]))
+
+    def setFieldArrayX(self, name, v):
+        self.setFieldArrays(name, hx=v)
+
+    def setFieldArrayY(self, name, v):
+        self.setFieldArrays(name, hy=v)
+
+    def setFieldArrayZ(self, name, v):
+        self.setFieldArrays(name, hz=v)
+
+    def slotUsed(self, name):
+        u = C.c_int()
+        _ck(_lib.mlb_system_slot_used(self._h, _slotname(name).encode(), C.byref(u)))
+        return bool(u.value)
+
+    def setSlotUsed(self, name, b=True):
+        _ck(_lib.mlb_system_set_slot_used(self._h, _slotname(name).encode(), int(bool(b))))
+
+    def ensureSlotExists(self, name):
+        _ck(_lib.mlb_system_ensure_slot(self._h, _slotname(name).encode()))
+
+    # reductions
+    def netMoment(self, m=1.0):
+        out = np.zeros(8)
+        _ck(_lib.mlb_system_netmoment(self._h, float(m), _dp(out)))
+        return tuple(out)
+
+    def fieldDot(self, name):
+        out = C.c_double()
+        _ck(_lib.mlb_system_field_dot(self._h, _slotname(name).encode(), C.byref(out)))
+        return out.value
+
+    # copies
+    def copyTo(self, dst):
+        _ck(_lib.mlb_system_copy(dst._h, self._h, 1))
+
+    def copySpinsTo(self, dst):
+        _ck(_lib.mlb_system_copy(dst._h, self._h, 0))
+
+    def copy(self):
+        c = SpinSystem(*self._dims)
+        self.copyTo(c)
+        return c
+
+
+def _slotname(x):
+    if isinstance(x, str):
+        return x
+    if hasattr(x, "slotName"):
+        return x.slotName()
+    raise TypeError("expected a slot name or an operator")
+
+
+# ====================================================================== operators
+class SpinOperation:
+    KIND = 0
+
+    def __init__(self, *args):
+        _ensure_init()
+        if args and isinstance(args[0], SpinSystem):
+            dims = args[0]._dims
+            rest = args[1:]
+        elif args and hasattr(args[0], "__len__"):
+            dims = _site3(args[0])
+            rest = args[1:]
+        else:
+            nums = [a for a in args if isinstance(a, (int, np.integer))][:3]
+            dims = _site3(nums or [1])
+            rest = args[len(nums):]
+        self._dims = tuple(int(d) for d in dims)
+        h = _P()
+        _ck(_lib.mlb_op_create(self.KIND, *self._dims, C.byref(h)))
+        self._h = h
+        self._init_extra(rest)
+
+    def _init_extra(self, rest):
+        pass
+
+    @classmethod
+    def new(cls, *a):
+        return cls(*a)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_op_destroy(h)
+            self._h = None
+
+    def nx(self):
+        return self._dims[0]
+
+    def ny(self):
+        return self._dims[1]
+
+    def nz(self):
+        return self._dims[2]
+
+    def _idx(self, site):
+        x, y, z = _site3(site)
+        return (x - 1) + self._dims[0] * ((y - 1) + self._dims[1] * (z - 1))
+
+    def member(self, site):
+        x, y, z = _site3(site)
+        return 1 <= x <= self._dims[0] and 1 <= y <= self._dims[1] and 1 <= z <= self._dims[2]
+
+    def apply(self, ss):
+        if isinstance(ss, (list, tuple)):
+            arr = (_P * len(ss))(*[s._h for s in ss])
+            _ck(_lib.mlb_op_apply_many(self._h, arr, len(ss)))
+        else:
+            _ck(_lib.mlb_op_apply(self._h, ss._h))
+
+    def setScale(self, s):
+        _ck(_lib.mlb_op_set_scale(self._h, float(s)))
+
+    def scale(self):
+        v = C.c_double()
+        _ck(_lib.mlb_op_get_scale(self._h, C.byref(v)))
+        return v.value
+
+    def setSlotName(self, name):
+        _ck(_lib.mlb_op_set_slot_name(self._h, name.encode()))
+
+    def slotName(self):
+        buf = C.create_string_buffer(256)
+        _ck(_lib.mlb_op_get_slot_name(self._h, buf, 256))
+        return buf.value.decode()
+
+    def setQuirks(self, on=True):
+        """Reproduce (True, default) or fix the reference's arithmetic quirks."""
+        _ck(_lib.mlb_op_set_quirks(self._h, int(bool(on))))
+
+
+class Exchange(SpinOperation):
+    """Exchange (M/cpu/exchange): pathways from -> to with strength J."""
+    KIND = 1
+    defaultMomentNormalization = None
+
+    def _init_extra(self, rest):
+        self._pbc = [1, 1, 1]
+        if Exchange.defaultMomentNormalization is not None:
+            self.normalizeMoments(bool(Exchange.defaultMomentNormalization))
+
+    def setPeriodicXYZ(self, px=True, py=True, pz=True):
+        self._pbc = [int(bool(px)), int(bool(py)), int(bool(pz))]
+
+    def periodicXYZ(self):
+        return tuple(bool(p) for p in self._pbc)
+
+    def add(self, a, b, J=1.0):
+        """l_addpath (spinoperationexchange.cpp:368-420): wrap by pbc, drop outside."""
+        a, b = list(_site3(a)), list(_site3(b))
+        for i in range(3):
+            a[i] -= 1
+            b[i] -= 1
+            n = self._dims[i]
+            if self._pbc[i]:
+                a[i] %= n
+                b[i] %= n
+            if not (0 <= a[i] < n and 0 <= b[i] < n):
+                return
+        nx, ny = self._dims[0], self._dims[1]
+        s1 = a[0] + nx * (a[1] + ny * a[2])
+        s2 = b[0] + nx * (b[1] + ny * b[2])
+        _ck(_lib.mlb_exchange_add_path(self._h, s1, s2, float(J)))
+
+    addPath = add
+
+    def addPaths(self, frm, to, J):
+        """Bulk add of 0-based site indices (already wrapped)."""
+        f, t, j = _i32(frm), _i32(to), _f64(J)
+        _ck(_lib.mlb_exchange_add_paths(self._h, f.ctypes.data_as(_I), t.ctypes.data_as(_I), _dp(j), len(f)))
+
+    def normalizeMoments(self, b=None):
+        if isinstance(b, bool):
+            _ck(_lib.mlb_exchange_set_normalize(self._h, int(b)))
+            self._norm = b
+        return getattr(self, "_norm", True)
+
+    def numberOfPaths(self):
+        n = C.c_int()
+        _ck(_lib.mlb_exchange_num_paths(self._h, C.byref(n)))
+        return n.value
+
+
+class Anisotropy(SpinOperation):
+    """Anisotropy (M/cpu/anisotropy/spinoperationanisotropy.cpp)."""
+    KIND = 2
+
+    def add(self, site, axis, K):
+        if not self.member(site):
+            raise MagLuaError(-1, f"site {site} is not part of operator {self._dims}")
+        _ck(_lib.mlb_anisotropy_add(self._h, self._idx(site), _dp(_f64(axis, 3)), float(K)))
+
+    def addMany(self, sites, axes, K):
+        s, a, k = _i32(sites), _f64(axes).reshape(-1), _f64(K)
+        _ck(_lib.mlb_anisotropy_add_many(self._h, len(s), s.ctypes.data_as(_I), _dp(a), _dp(k)))
+
+
+class AnisotropyUniaxial(SpinOperation):
+    KIND = 3
+
+    def add(self, site, axis, K1, K2=0.0):
+        if not self.member(site):
+            raise MagLuaError(-1, f"site {site} is not part of operator {self._dims}")
+        _ck(_lib.mlb_uniaxial_add(self._h, self._idx(site), _dp(_f64(axis, 3)), float(K1), float(K2)))
+
+    def addMany(self, sites, axes, K1, K2):
+        s, a = _i32(sites), _f64(axes).reshape(-1)
+        k1, k2 = _f64(K1), _f64(K2)
+        _ck(_lib.mlb_uniaxial_add_many(self._h, len(s), s.ctypes.data_as(_I), _dp(a), _dp(k1), _dp(k2)))
+
+
+class AnisotropyCubic(SpinOperation):
+    KIND = 4
+
+    def add(self, site, a1, a2, K1, K2=0.0, K3=0.0):
+        if not self.member(site):
+            raise MagLuaError(-1, f"site {site} is not part of operator {self._dims}")
+        K = _f64([K1, K2, K3])
+        _ck(_lib.mlb_cubic_add(self._h, self._idx(site), _dp(_f64(a1, 3)), _dp(_f64(a2, 3)), _dp(K)))
+
+    def addMany(self, sites, a1, a2, K):
+        s = _i32(sites)
+        A1, A2, KK = _f64(a1).reshape(-1), _f64(a2).reshape(-1), _f64(K).reshape(-1)
+        _ck(_lib.mlb_cubic_add_many(self._h, len(s), s.ctypes.data_as(_I), _dp(A1), _dp(A2), _dp(KK)))
+
+
+Anisotropy.Uniaxial = AnisotropyUniaxial
+Anisotropy.Cubic = AnisotropyCubic
+
+
+class Random:
+    """Random.* stand-ins.  Philox is the device generator the Thermal
+    operator uses: a seed plus a counter, one draw of three normals per site
+    and apply."""
+
+    class Philox:
+        def __init__(self, seed=0):
+            self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+
+        @classmethod
+        def new(cls, seed=0):
+            return cls(seed)
+
+        def setSeed(self, seed):
+            self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+
+
+class Thermal(SpinOperation):
+    """Thermal (M/cpu/thermal): Langevin field with counter-based noise."""
+    KIND = 5
+
+    def _init_extra(self, rest):
+        self._rng = None
+        for r in rest:
+            if isinstance(r, Random.Philox):
+                self._use_rng(r)
+
+    def _use_rng(self, rng):
+        self._rng = rng
+        _ck(_lib.mlb_thermal_set_seed(self._h, rng.seed))
+
+    def setTemperature(self, T):
+        if T is None:
+            raise MagLuaError(-1, "set temp cannot be nil")
+        _ck(_lib.mlb_thermal_set_temperature(self._h, float(T)))
+
+    set = setTemperature
+
+    def temperature(self):
+        v = C.c_double()
+        _ck(_lib.mlb_thermal_get_temperature(self._h, C.byref(v)))
+        return v.value
+
+    get = temperature
+
+    def scaleSite(self, site, v):
+        x, y, z = _site3(site)
+        if self.member((x, y, z)):
+            _ck(_lib.mlb_thermal_scale_site(self._h, self._idx(site), float(v)))
+
+    def setSeed(self, seed):
+        _ck(_lib.mlb_thermal_set_seed(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF))
+        _ck(_lib.mlb_thermal_set_counter(self._h, 0))
+
+    def setCounter(self, c):
+        _ck(_lib.mlb_thermal_set_counter(self._h, int(c)))
+
+    def inject(self, nx, ny, nz):
+        """Use these normals (one per site and component) on the next apply."""
+        n = self._dims[0] * self._dims[1] * self._dims[2]
+        a = [_f64(v, n) for v in (nx, ny, nz)]
+        _ck(_lib.mlb_thermal_inject(self._h, *[_dp(v) for v in a]))
+
+    def apply(self, ss, rng=None):
+        """Thermal:apply(ss[, rng]).  As in the reference (l_apply,
+        spinoperationthermal.cpp:205-217) a given RNG is applied first and
+        the operator's own RNG second, so the stored RNG decides the field;
+        without a stored RNG that second apply fails with "Missing RNG"."""
+        if rng is not None:
+            _ck(_lib.mlb_thermal_set_seed(self._h, rng.seed))
+            SpinOperation.apply(self, ss)
+            if self._rng is None:
+                raise MagLuaError(-4, "Missing RNG")
+            _ck(_lib.mlb_thermal_set_seed(self._h, self._rng.seed))
+        SpinOperation.apply(self, ss)
+
+
+class AppliedField(SpinOperation):
+    """AppliedField (M/cpu/appliedfield): uniform field in slot "Zeeman"."""
+    KIND = 6
+
+    def set(self, x=0.0, y=0.0, z=0.0):
+        if isinstance(x, (list, tuple)):
+            v = list(x) + [0, 0, 0]
+            x, y, z = v[0], v[1], v[2]
+        _ck(_lib.mlb_appliedfield_set(self._h, float(x or 0), float(y or 0), float(z or 0)))
+
+    def get(self):
+        out = np.zeros(3)
+        _ck(_lib.mlb_appliedfield_get(self._h, _dp(out)))
+        return tuple(out)
+
+    def add(self, x=0.0, y=0.0, z=0.0):
+        if isinstance(x, (list, tuple)):
+            v = list(x) + [0, 0, 0]
+            x, y, z = v[0], v[1], v[2]
+        b = self.get()
+        self.set(b[0] + x, b[1] + y, b[2] + z)
+
+    def toTable(self):
+        return list(self.get())
+
+    def x(self):
+        return self.get()[0]
+
+    def y(self):
+        return self.get()[1]
+
+    def z(self):
+        return self.get()[2]
+
+    def setX(self, v):
+        b = self.get()
+        self.set(v, b[1], b[2])
+
+    def setY(self, v):
+        b = self.get()
+        self.set(b[0], v, b[2])
+
+    def setZ(self, v):
+        b = self.get()
+        self.set(b[0], b[1], v)
+
+    def setSweep(self, dx=0.0, dy=0.0, dz=0.0):
+        """Per-step field increment used by run()."""
+        _ck(_lib.mlb_appliedfield_set_sweep(self._h, float(dx), float(dy), float(dz)))
+
+
+_AB6 = {"XX": 0, "XY": 1, "XZ": 2, "YY": 3, "YZ": 4, "ZZ": 5}
+_AB9 = {"XX": 0, "XY": 1, "XZ": 2, "YX": 3, "YY": 4, "YZ": 5, "ZX": 6, "ZY": 7, "ZZ": 8}
+
+
+class LongRange(SpinOperation):
+    """LongRange (M/cpu/longrange): user tensor, 2D FFT in-plane + layer sum."""
+    KIND = 8
+
+    def setStrength(self, g):
+        _ck(_lib.mlb_longrange_set_strength(self._h, float(g)))
+
+    def strength(self):
+        v = C.c_double()
+        _ck(_lib.mlb_longrange_get_strength(self._h, C.byref(v)))
+        return v.value
+
+    def setTruncation(self, r, x=None, y=None, z=None):
+        if x is None:
+            g = [int(r)] * 4
+        else:
+            xs = [max(1, int(v)) for v in (x, y, z)]
+            g = [max(xs)] + xs
+        arr = (C.c_int * 4)(*g)
+        _ck(_lib.mlb_longrange_set_truncation(self._h, arr))
+
+    def setUnitCell(self, A, B, C_):
+        abc = _f64(list(A) + list(B) + list(C_), 9)
+        _ck(_lib.mlb_longrange_set_unit_cell(self._h, _dp(abc)))
+
+    def setMatrix(self, ab, offset, value):
+        ox, oy, oz = (list(offset) + [0, 0, 0])[:3]
+        _ck(_lib.mlb_longrange_set_matrix(self._h, _AB6[ab.upper()], int(ox), int(oy), int(oz), float(value)))
+
+    def getMatrix(self, ab, offset):
+        ox, oy, oz = (list(offset) + [0, 0, 0])[:3]
+        v = C.c_double()
+        _ck(_lib.mlb_longrange_get_matrix(self._h, _AB6[ab.upper()], int(ox), int(oy), int(oz), C.byref(v)))
+        return v.value
+
+    def tensorArrays(self):
+        """XX, XY, XZ, YY, YZ, ZZ shaped (2nz-1, ny, nx)."""
+        nx, ny, nz = self._dims
+        arrs = [np.zeros(nx * ny * (2 * nz - 1)) for _ in range(6)]
+        ptrs = (_D * 6)(*[_dp(a) for a in arrs])
+        _ck(_lib.mlb_longrange_get_tensor(self._h, ptrs))
+        return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
+
+
+class Dipole(LongRange):
+    """Dipole (M/cpu/dipole): periodic-in-plane lattice-sum tensor."""
+    KIND = 7
+
+    def setOpen(self, ox=True, oy=True, oz=True):
+        """Open (zero-padded) boundaries in x and y instead of periodic images."""
+        _ck(_lib.mlb_longrange_set_open(self._h, int(bool(ox)), int(bool(oy)), int(bool(oz))))
+
+
+class LongRange3D(SpinOperation):
+    """LongRange3D (M/cpu/longrange3d): 9-component cyclic 3D convolution."""
+    KIND = 9
+
+    def setStrength(self, g):
+        _ck(_lib.mlb_longrange_set_strength(self._h, float(g)))
+
+    def strength(self):
+        v = C.c_double()
+        _ck(_lib.mlb_longrange_get_strength(self._h, C.byref(v)))
+        return v.value
+
+    def setTensorArray(self, ab, arr):
+        n = self._dims[0] * self._dims[1] * self._dims[2]
+        a = _f64(arr, n)
+        _ck(_lib.mlb_longrange3d_set_tensor(self._h, _AB9[ab.upper()], _dp(a)))
+
+
+# ====================================================================== LLG
+class _LLGBase:
+    KIND = 0
+    thermalOnlyFirstTerm = None
+
+    def __init__(self):
+        _ensure_init()
+        h = _P()
+        _ck(_lib.mlb_llg_create(self.KIND, C.byref(h)))
+        self._h = h
+        self._flags = [1, 0, 1.0, 1.0]
+        if LLG.thermalOnlyFirstTerm is not None:
+            self.setThermalOnlyFirstTerm(bool(LLG.thermalOnlyFirstTerm))
+
+    @classmethod
+    def new(cls):
+        return cls()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_llg_destroy(h)
+            self._h = None
+
+    def _push(self):
+        f = self._flags
+        _ck(_lib.mlb_llg_set_flags(self._h, int(f[0]), int(f[1]), float(f[2]), float(f[3])))
+
+    def setThermalOnlyFirstTerm(self, b):
+        self._flags[0] = int(bool(b))
+        self._push()
+
+    def thermalOnlyFirstTerm(self):
+        return bool(self._flags[0])
+
+    def setDisableRenormalization(self, b):
+        self._flags[1] = int(bool(b))
+        self._push()
+
+    def disableRenormalization(self):
+        return bool(self._flags[1])
+
+    def setUnphysicalPrecessionScale(self, v):
+        self._flags[2] = float(v)
+        self._push()
+
+    def setUnphysicalDampingScale(self, v):
+        self._flags[3] = float(v)
+        self._push()
+
+    def apply(self, *args):
+        """apply(A[, x], B, C[, advance]) as l_apply (llg.cpp:91-171)."""
+        args = list(args)
+        advance = True
+        if args and isinstance(args[-1], bool):
+            advance = args.pop()
+        frm = args[0]
+        scale = 1.0
+        rest = args[1:]
+        if rest and isinstance(rest[0], (int, float)) and not isinstance(rest[0], bool):
+            scale = float(rest[0])
+            rest = rest[1:]
+        dmdt = rest[0] if len(rest) > 0 and rest[0] is not None else frm
+        to = rest[1] if len(rest) > 1 and rest[1] is not None else frm
+        if isinstance(frm, (list, tuple)):
+            d = dmdt if isinstance(dmdt, (list, tuple)) else [dmdt] * len(frm)
+            t = to if isinstance(to, (list, tuple)) else [to] * len(frm)
+            if not (len(frm) == len(d) == len(t)):
+                raise MagLuaError(-1, "Size mismatch in number of SpinSystems given in each table")
+            for a, b, c in zip(frm, d, t):
+                _ck(_lib.mlb_llg_apply(self._h, a._h, scale, b._h, c._h, int(advance)))
+            return
+        _ck(_lib.mlb_llg_apply(self._h, frm._h, scale, dmdt._h, to._h, int(advance)))
+
+
+class LLGCartesian(_LLGBase):
+    KIND = 0
+
+
+class LLGQuaternion(_LLGBase):
+    KIND = 1
+
+
+class LLG:
+    """LLG.new("Cartesian"|"Quaternion") (llg_wrapper.lua)."""
+    Cartesian = LLGCartesian
+    Quaternion = LLGQuaternion
+    thermalOnlyFirstTerm = None
+
+    @staticmethod
+    def new(kind):
+        if kind not in ("Cartesian", "Quaternion"):
+            raise MagLuaError(-1, f"Failed to find LLG implementation of type `{kind}'")
+        return getattr(LLG, kind)()
+
+
+class profile:
+    """with profile() as prof: ... -> prof.kernels = {name: (total_ms, launches)}"""
+
+    def __enter__(self):
+        _ck(_lib.mlb_profile_begin())
+        self.kernels = {}
+        return self
+
+    def __exit__(self, *exc):
+        cap = 64
+        names = C.create_string_buffer(48 * cap)
+        ms = np.zeros(cap)
+        nl = np.zeros(cap, dtype=np.int32)
+        cnt = C.c_int()
+        _ck(_lib.mlb_profile_end(cap, names, _dp(ms), nl.ctypes.data_as(_I), C.byref(cnt)))
+        raw = names.raw
+        for k in range(cnt.value):
+            nm = raw[48 * k:48 * (k + 1)].split(b"\0", 1)[0].decode()
+            self.kernels[nm] = (float(ms[k]), int(nl[k]))
+        return False
+
+
+def run(ss, ops, llg, nsteps):
+    """nsteps of: ss.resetFields(); op.apply(ss) for op in ops; ss.sumFields();
+    llg.apply(ss) -- fused and captured in a CUDA graph."""
+    arr = (_P * len(ops))(*[o._h for o in ops])
+    _ck(_lib.mlb_run(ss._h, arr, len(ops), llg._h, int(nsteps)))

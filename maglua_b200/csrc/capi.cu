@@ -1,0 +1,2066 @@
+// capi.cu -- host layer behind include/mlb200.h.
+//
+// Object model (mirrors MagLua's SpinSystem / SpinOperation / LLG classes):
+//   * mlb_system: FP32 SoA spins in two generations (ping-pong buffers), ms,
+//     per-site alpha/gamma, named field slots ("Total" is slot 0).
+//   * Field slots are evaluated lazily.  A slot is ZERO, DATA (device arrays
+//     hold its value), LAZY (a base -- zero or its arrays -- plus operator terms
+//     recorded at apply time against a spin generation) or SUM ("Total" after
+//     sumFields, defined by the slots it sums).  Reading a slot, or anything
+//     that would invalidate a record, materialises it with k_eval_terms.  When
+//     llg:apply(ss) meets a lazily defined "Total", the whole step runs as one
+//     fused kernel (field terms + LLG) that writes the other spin buffer.
+//   * Dipole / LongRange / LongRange3D run eagerly (FFT convolution pipeline)
+//     into DATA slots that the fused kernel reads.
+#include "../../include/mlb200.h"
+#include "device.cuh"
+#include "kparams.h"
+#include "launch.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <strings.h>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Err {
+    int code;
+    std::string msg;
+};
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            throw Err{e_ == cudaErrorMemoryAllocation ? MLB_ENOMEM : MLB_ECUDA,                \
+                      std::string(#x) + ": " + cudaGetErrorString(e_)};                        \
+    } while (0)
+
+[[noreturn]] void fail(int code, const std::string& m) { throw Err{code, m}; }
+
+template <class F>
+int guard(F&& f)
+{
+    try {
+        f();
+        return MLB_OK;
+    } catch (Err& e) {
+        g_err = e.msg;
+        return e.code;
+    } catch (std::bad_alloc&) {
+        g_err = "host allocation failed";
+        return MLB_ENOMEM;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return MLB_EINVAL;
+    } catch (...) {
+        g_err = "unknown error";
+        return MLB_EINVAL;
+    }
+}
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t k)
+    {
+        if (k == n && p) return;
+        release();
+        if (k == 0) return;
+        CK(cudaMalloc(&p, k * sizeof(T)));
+        n = k;
+    }
+};
+
+bool name_eq(const std::string& a, const char* b) { return strcasecmp(a.c_str(), b) == 0; }
+
+// ------------------------------------------------------------------ FFT plans
+std::vector<int> factorize(int n)
+{
+    std::vector<int> r;
+    while (n % 8 == 0 && n != 16 && n / 8 != 2) { r.push_back(8); n /= 8; }
+    while (n % 4 == 0) { r.push_back(4); n /= 4; }
+    while (n % 2 == 0) { r.push_back(2); n /= 2; }
+    for (int p = 3; p <= 7; p += 2)
+        while (n % p == 0) { r.push_back(p); n /= p; }
+    for (int p = 11; n > 1; p += 2)
+        while (n % p == 0) { r.push_back(p); n /= p; }
+    return r;
+}
+
+FftLen make_len(int n, int tw_off)
+{
+    FftLen L;
+    memset(&L, 0, sizeof(L));
+    L.n = n;
+    std::vector<int> r = factorize(n);
+    if ((int)r.size() > MLB_FFT_MAX_STAGES) fail(MLB_EUNSUP, "FFT length has too many factors");
+    for (int p : r)
+        if (p > 32) fail(MLB_EUNSUP, "FFT length " + std::to_string(n) + " has a prime factor above 32");
+    L.nst = (int)r.size();
+    for (size_t i = 0; i < r.size(); i++) L.radix[i] = r[i];
+    L.tw_off = tw_off;
+    return L;
+}
+
+// smallest m' >= m of the form 2^a or 3*2^a
+int nice_len(int m)
+{
+    if (m <= 1) return 1;
+    int best = 1;
+    while (best < m) best *= 2;
+    int t = 3;
+    while (t < m) t *= 2;
+    return std::min(best, t);
+}
+
+template <class C>
+void append_twiddles(std::vector<C>& pool, int n)
+{
+    for (int k = 0; k < n; k++) {
+        const double a = 2.0 * M_PI * (double)k / (double)n;
+        C c;
+        c.x = (decltype(c.x))std::cos(a);
+        c.y = (decltype(c.y))(-std::sin(a));
+        pool.push_back(c);
+    }
+}
+
+// Convolution plan of one operator for one lattice size.
+struct ConvPlan {
+    ConvK k;
+    FftLen L[3];
+    DBuf<float2> tw;
+    DBuf<float2> spec;
+    DBuf<float> ten6;
+    DBuf<float2> ten9;
+    double max_imag = 0; // largest |Im| of the FP64 tensor transform (6-component)
+};
+
+} // namespace
+
+// ====================================================================== objects
+struct Term {
+    mlb_op* op;
+    int weight;
+    uint64_t counter;
+    float B[3];
+    double T;
+    double gs;
+    double dt_sys;
+};
+
+enum { ST_ZERO = 0, ST_DATA = 1, ST_LAZY = 2, ST_SUM = 3 };
+
+struct Slot {
+    std::string name;
+    float* h[3] = {nullptr, nullptr, nullptr};
+    bool used = false;
+    int state = ST_ZERO;
+    bool base_data = false;
+    std::vector<Term> terms;
+    long long gen = 0;
+    std::vector<int> sum_list;
+};
+
+struct mlb_system {
+    int nx, ny, nz, n;
+    float* sp[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int cur = 0;
+    long long gen = 0;
+    float* ms = nullptr;
+    std::vector<float> ms_host;
+    bool ms_dirty = true;
+    bool ms_uniform = true;
+    float ms_u = 0.f;
+    float* sa = nullptr;
+    float* sg = nullptr;
+    double alpha = 1.0, gamma = 1.0, dt = 1.0, time = 0.0;
+    std::vector<Slot> slots;
+    cudaStream_t own = nullptr;
+    cudaStream_t st = nullptr;
+    uint64_t* dctr = nullptr;
+    double* red = nullptr;
+    double* redout = nullptr;
+    int red_nb = 1;
+    bool capturing = false;
+    bool last_fused = false;
+};
+
+struct mlb_op {
+    int kind;
+    int nx, ny, nz;
+    double gs = 1.0;
+    std::string slot;
+    bool quirks = true;
+    // exchange
+    std::vector<int> ef, et;
+    std::vector<double> eJ;
+    bool normalize = true;
+    bool ex_dirty = true;
+    ExchangeK exk{};
+    DBuf<int> eptr, ecol;
+    DBuf<float> eval;
+    // anisotropies: per op site + parameters
+    std::vector<int> asite;
+    std::vector<double> apar; // generic: axis3,K ; uni: axis3,K1,K2 ; cubic: axes9,K3
+    bool a_dirty = true;
+    AniK anik{};
+    UniK unik{};
+    CubK cubk{};
+    DBuf<int> aptr;
+    DBuf<float> aaxes, aK;
+    double gs_compiled = -1;
+    // thermal
+    double T = 0.0;
+    std::vector<double> tscale;
+    DBuf<float> dscale;
+    bool tscale_dirty = false;
+    uint64_t seed = 0;
+    uint64_t counter = 0;
+    bool inject_pending = false;
+    DBuf<float> inj[3];
+    // applied field
+    double B[3] = {0, 0, 0};
+    double dB[3] = {0, 0, 0};
+    // longrange
+    double g = 1.0;
+    int gmax[4] = {1000, 1000, 1000, 1000};
+    double ABC[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    int open[3] = {0, 0, 1};
+    std::vector<double> t6[6];
+    bool t6_valid = false;
+    std::vector<double> t9[9];
+    bool plan_dirty = true;
+    std::unique_ptr<ConvPlan> plan;
+};
+
+struct mlb_llg {
+    int kind;
+    int tof = 1;
+    int disable_renorm = 0;
+    double precess = 1.0, damp = 1.0;
+};
+
+namespace {
+
+std::set<mlb_system*> g_systems;
+
+// ------------------------------------------------------------------ system helpers
+int slot_find(const mlb_system* s, const char* name)
+{
+    for (size_t i = 0; i < s->slots.size(); i++)
+        if (name_eq(s->slots[i].name, name)) return (int)i;
+    return -1;
+}
+
+int slot_register(mlb_system* s, const char* name)
+{
+    int i = slot_find(s, name);
+    if (i >= 0) return i;
+    Slot sl;
+    sl.name = name;
+    s->slots.push_back(sl);
+    return (int)s->slots.size() - 1;
+}
+
+void slot_alloc(mlb_system* s, Slot& sl)
+{
+    if (sl.h[0]) return;
+    for (int c = 0; c < 3; c++) CK(cudaMalloc(&sl.h[c], sizeof(float) * std::max(1, s->n)));
+}
+
+void refresh_ms(mlb_system* s)
+{
+    if (!s->ms_dirty) return;
+    s->ms_uniform = true;
+    s->ms_u = s->n ? s->ms_host[0] : 0.f;
+    for (int i = 1; i < s->n; i++)
+        if (s->ms_host[i] != s->ms_u) { s->ms_uniform = false; break; }
+    s->ms_dirty = false;
+}
+
+SysK sysk(mlb_system* s, int buf)
+{
+    refresh_ms(s);
+    SysK k;
+    k.nx = s->nx; k.ny = s->ny; k.nz = s->nz; k.n = s->n;
+    k.x = s->sp[buf][0]; k.y = s->sp[buf][1]; k.z = s->sp[buf][2];
+    k.ms = s->ms; k.ms_u = s->ms_u; k.ms_uniform = s->ms_uniform ? 1 : 0;
+    k.site_alpha = s->sa; k.site_gamma = s->sg;
+    k.alpha = (float)s->alpha; k.gamma = (float)s->gamma;
+    return k;
+}
+
+int buffer_for_gen(mlb_system* s, long long gen)
+{
+    if (gen == s->gen) return s->cur;
+    if (gen == s->gen - 1) return 1 - s->cur;
+    fail(MLB_ESTATE, "internal: lazy field refers to an overwritten spin generation");
+}
+
+// ------------------------------------------------------------------ operator compile
+void check_site(const mlb_op* op, int idx)
+{
+    if (idx < 0 || idx >= op->nx * op->ny * op->nz)
+        fail(MLB_ERANGE, "site index " + std::to_string(idx) + " outside the operator");
+}
+
+// Exchange pathways -> six-direction stencil when the pathway multiset is
+// exactly a nearest-neighbour lattice with one J per direction, else CSR by
+// target site keeping insertion order.
+void compile_exchange(mlb_op* op)
+{
+    if (!op->ex_dirty) return;
+    const int nx = op->nx, ny = op->ny, nz = op->nz, n = nx * ny * nz;
+    const size_t np = op->ef.size();
+    ExchangeK k{};
+    k.normalize = op->normalize ? 1 : 0;
+    bool stencil = np > 0;
+    double Jd[6];
+    bool seen[6] = {false, false, false, false, false, false};
+    int pbc[3] = {0, 0, 0};
+    const int dims[3] = {nx, ny, nz};
+    for (size_t p = 0; p < np && stencil; p++) {
+        const int f = op->ef[p], t = op->et[p];
+        const int fc[3] = {f % nx, (f / nx) % ny, f / (nx * ny)};
+        const int tc[3] = {t % nx, (t / nx) % ny, t / (nx * ny)};
+        int dir = -1, wrap = 0;
+        for (int a = 0; a < 3; a++) {
+            const int d = fc[a] - tc[a];
+            if (d == 0) continue;
+            if (dir >= 0) { stencil = false; break; }
+            if (d == 1) dir = 2 * a;
+            else if (d == -1) dir = 2 * a + 1;
+            else if (dims[a] > 2 && d == -(dims[a] - 1)) { dir = 2 * a; wrap = 1; }
+            else if (dims[a] > 2 && d == dims[a] - 1) { dir = 2 * a + 1; wrap = 1; }
+            else { stencil = false; break; }
+            if (wrap) pbc[a] = 1;
+        }
+        if (!stencil) break;
+        if (dir < 0) { stencil = false; break; }
+        if (!seen[dir]) { seen[dir] = true; Jd[dir] = op->eJ[p]; }
+        else if (Jd[dir] != op->eJ[p]) stencil = false;
+    }
+    if (stencil) {
+        // the candidate must reproduce the pathway multiset exactly
+        std::map<std::pair<int, int>, double> actual, expect;
+        for (size_t p = 0; p < np; p++) actual[{op->et[p], op->ef[p]}] += op->eJ[p];
+        for (int t = 0; t < n && stencil; t++) {
+            const int tc[3] = {t % nx, (t / nx) % ny, t / (nx * ny)};
+            for (int d = 0; d < 6; d++) {
+                if (!seen[d]) continue;
+                const int a = d >> 1, sg = (d & 1) ? -1 : 1;
+                int c[3] = {tc[0], tc[1], tc[2]};
+                c[a] += sg;
+                if (c[a] < 0 || c[a] >= dims[a]) {
+                    if (!pbc[a]) continue;
+                    c[a] = (c[a] + dims[a]) % dims[a];
+                }
+                const int f = c[0] + nx * (c[1] + ny * c[2]);
+                expect[{t, f}] += Jd[d];
+            }
+        }
+        if (actual.size() != expect.size()) stencil = false;
+        else {
+            for (auto& kv : actual) {
+                auto it = expect.find(kv.first);
+                if (it == expect.end() || std::fabs(it->second - kv.second) > 1e-12 * std::fabs(kv.second)) {
+                    stencil = false;
+                    break;
+                }
+            }
+        }
+    }
+    if (stencil) {
+        k.mode = EX_STENCIL;
+        for (int d = 0; d < 6; d++) k.J[d] = seen[d] ? (float)Jd[d] : 0.f;
+        for (int a = 0; a < 3; a++) k.pbc[a] = pbc[a];
+        op->eptr.release(); op->ecol.release(); op->eval.release();
+    } else if (np > 0) {
+        k.mode = EX_CSR;
+        std::vector<int> cnt(n + 1, 0);
+        for (size_t p = 0; p < np; p++) cnt[op->et[p] + 1]++;
+        for (int i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        std::vector<int> col(np);
+        std::vector<float> val(np);
+        std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+        for (size_t p = 0; p < np; p++) {
+            const int q = pos[op->et[p]]++;
+            col[q] = op->ef[p];
+            val[q] = (float)op->eJ[p];
+        }
+        op->eptr.alloc(n + 1); op->ecol.alloc(np); op->eval.alloc(np);
+        CK(cudaMemcpy(op->eptr.p, cnt.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->ecol.p, col.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->eval.p, val.data(), sizeof(float) * np, cudaMemcpyHostToDevice));
+        k.ptr = op->eptr.p; k.col = op->ecol.p; k.val = op->eval.p;
+    } else {
+        k.mode = EX_NONE;
+    }
+    op->exk = k;
+    op->ex_dirty = false;
+}
+
+// Per-site operator lists (generic / uniaxial / cubic anisotropy) -> uniform
+// constants when every site has exactly one op with identical parameters,
+// else CSR by site (list order kept).  global_scale is folded into K.
+void compile_aniso(mlb_op* op)
+{
+    if (!op->a_dirty && op->gs_compiled == op->gs) return;
+    const int n = op->nx * op->ny * op->nz;
+    const int npar = op->kind == MLB_OP_ANISOTROPY ? 4 : (op->kind == MLB_OP_UNIAXIAL ? 5 : 12);
+    const int nax = op->kind == MLB_OP_CUBIC ? 9 : 3;
+    const int nk = npar - nax;
+    const size_t no = op->asite.size();
+    bool uniform = (int)no == n && n > 0;
+    if (uniform) {
+        std::vector<char> hit(n, 0);
+        for (size_t j = 0; j < no && uniform; j++) {
+            if (hit[op->asite[j]]) uniform = false;
+            hit[op->asite[j]] = 1;
+            for (int q = 0; q < npar && uniform; q++)
+                if (op->apar[j * npar + q] != op->apar[q]) uniform = false;
+        }
+    }
+    const int mode = no == 0 ? ANI_NONE : (uniform ? ANI_UNIFORM : ANI_CSR);
+    const double gs = op->gs;
+    if (mode == ANI_CSR) {
+        std::vector<int> cnt(n + 1, 0);
+        for (size_t j = 0; j < no; j++) cnt[op->asite[j] + 1]++;
+        for (int i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+        std::vector<float> ax(no * nax), kk(no * nk);
+        std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+        for (size_t j = 0; j < no; j++) {
+            const int q = pos[op->asite[j]]++;
+            for (int a = 0; a < nax; a++) ax[q * nax + a] = (float)op->apar[j * npar + a];
+            for (int a = 0; a < nk; a++) kk[q * nk + a] = (float)(op->apar[j * npar + nax + a] * gs);
+        }
+        op->aptr.alloc(n + 1); op->aaxes.alloc(ax.size()); op->aK.alloc(kk.size());
+        CK(cudaMemcpy(op->aptr.p, cnt.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->aaxes.p, ax.data(), sizeof(float) * ax.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->aK.p, kk.data(), sizeof(float) * kk.size(), cudaMemcpyHostToDevice));
+    }
+    if (op->kind == MLB_OP_ANISOTROPY) {
+        AniK k{};
+        k.mode = mode;
+        if (mode == ANI_UNIFORM) {
+            for (int a = 0; a < 3; a++) k.axis[a] = (float)op->apar[a];
+            k.K = (float)(op->apar[3] * gs);
+        } else if (mode == ANI_CSR) { k.ptr = op->aptr.p; k.axes = op->aaxes.p; k.Ks = op->aK.p; }
+        op->anik = k;
+    } else if (op->kind == MLB_OP_UNIAXIAL) {
+        UniK k{};
+        k.mode = mode;
+        k.quirk = op->quirks ? 1 : 0;
+        if (mode == ANI_UNIFORM) {
+            for (int a = 0; a < 3; a++) k.axis[a] = (float)op->apar[a];
+            k.K1 = (float)(op->apar[3] * gs); k.K2 = (float)(op->apar[4] * gs);
+        } else if (mode == ANI_CSR) { k.ptr = op->aptr.p; k.axes = op->aaxes.p; k.K12 = op->aK.p; }
+        op->unik = k;
+    } else {
+        CubK k{};
+        k.mode = mode;
+        k.quirk = op->quirks ? 1 : 0;
+        if (mode == ANI_UNIFORM) {
+            for (int a = 0; a < 9; a++) k.axes[a] = (float)op->apar[a];
+            for (int a = 0; a < 3; a++) k.K[a] = (float)(op->apar[9 + a] * gs);
+        } else if (mode == ANI_CSR) { k.ptr = op->aptr.p; k.axs = op->aaxes.p; k.Ks = op->aK.p; }
+        op->cubk = k;
+    }
+    op->a_dirty = false;
+    op->gs_compiled = gs;
+}
+
+void compile_thermal_scale(mlb_op* op)
+{
+    if (!op->tscale_dirty) return;
+    const int n = op->nx * op->ny * op->nz;
+    std::vector<float> f(n);
+    for (int i = 0; i < n; i++) f[i] = (float)op->tscale[i];
+    op->dscale.alloc(n);
+    CK(cudaMemcpy(op->dscale.p, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    op->tscale_dirty = false;
+}
+
+// ------------------------------------------------------------------ convolution plans
+bool is_conv(int kind) { return kind == MLB_OP_DIPOLE || kind == MLB_OP_LONGRANGE || kind == MLB_OP_LONGRANGE3D; }
+
+void plan_sizes(mlb_op* op, ConvPlan& P)
+{
+    ConvK& k = P.k;
+    k.nx = op->nx; k.ny = op->ny; k.nz = op->nz;
+    if (op->kind == MLB_OP_LONGRANGE3D) {
+        k.Px = op->nx; k.Py = op->ny; k.Pz = op->nz;
+        k.general = 1;
+    } else {
+        const bool ox = op->kind == MLB_OP_DIPOLE && op->open[0];
+        const bool oy = op->kind == MLB_OP_DIPOLE && op->open[1];
+        k.Px = ox ? nice_len(2 * op->nx - 1) : op->nx;
+        k.Py = oy ? nice_len(2 * op->ny - 1) : op->ny;
+        k.Pz = op->nz == 1 ? 1 : nice_len(2 * op->nz - 1);
+        k.general = 0;
+    }
+    k.Kx = k.Px / 2 + 1;
+    int ty = 16;
+    while (ty > 1 && (size_t)2 * ty * k.Px * sizeof(float2) > 96 * 1024) ty /= 2;
+    k.ty = ty;
+    if ((size_t)6 * k.Py * k.Pz * sizeof(float2) > 227 * 1024)
+        fail(MLB_EUNSUP, "padded (y,z) plane " + std::to_string(k.Py) + "x" + std::to_string(k.Pz) +
+                             " exceeds the shared-memory plane of this build");
+    if ((size_t)2 * k.Px * sizeof(float2) > 96 * 1024) fail(MLB_EUNSUP, "x length too large");
+}
+
+void ensure_t6_layout(mlb_op* op)
+{
+    const size_t ne = (size_t)op->nx * op->ny * (2 * op->nz - 1);
+    for (int q = 0; q < 6; q++)
+        if (op->t6[q].size() != ne) op->t6[q].assign(ne, 0.0);
+}
+
+// Build or rebuild the tensor spectrum of op (FP64 on the GPU).
+void build_plan(mlb_op* op, cudaStream_t st)
+{
+    if (!op->plan_dirty && op->plan) return;
+    std::unique_ptr<ConvPlan> P(new ConvPlan());
+    plan_sizes(op, *P);
+    ConvK& k = P->k;
+    const int Px = k.Px, Py = k.Py, Pz = k.Pz;
+    // twiddle tables: float (per-step FFTs) and double (tensor FFT)
+    std::vector<float2> twf;
+    std::vector<double2> twd;
+    const int lens[3] = {Px, Py, Pz};
+    for (int a = 0; a < 3; a++) {
+        P->L[a] = make_len(lens[a], (int)twf.size());
+        append_twiddles(twf, lens[a]);
+        append_twiddles(twd, lens[a]);
+    }
+    P->tw.alloc(twf.size());
+    CK(cudaMemcpy(P->tw.p, twf.data(), sizeof(float2) * twf.size(), cudaMemcpyHostToDevice));
+    DBuf<double2> twdd;
+    twdd.alloc(twd.size());
+    CK(cudaMemcpy(twdd.p, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice));
+
+    const int ncomp = k.general ? 9 : 6;
+    const size_t plane = (size_t)Px * Py * Pz;
+    DBuf<double2> W;
+    W.alloc(plane * ncomp);
+    CK(cudaMemsetAsync(W.p, 0, sizeof(double2) * plane * ncomp, st));
+    const size_t ne = (size_t)op->nx * op->ny * (2 * op->nz - 1);
+    if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
+        if (op->open[0] || op->open[1]) {
+            if (!(op->open[0] && op->open[1])) fail(MLB_EUNSUP, "mixed periodic/open in-plane Dipole");
+            CK(mlb::launch_tensor_open(op->nx, op->ny, op->nz, op->ABC, Px, Py, Pz, W.p, st));
+        } else {
+            const int zsign = op->quirks ? -1 : 1;
+            CK(mlb::launch_tensor_lattice(op->nx, op->ny, op->nz, op->gmax, op->ABC, Px, Py, Pz, zsign, W.p, st));
+            // keep the reference-layout tensor on the host (getMatrix / tensor arrays)
+            DBuf<double> raw;
+            raw.alloc(ne * 6);
+            CK(mlb::launch_tensor_extract_ref(op->nx, op->ny, op->nz, Px, Py, Pz, zsign, W.p, raw.p, st));
+            std::vector<double> h(ne * 6);
+            CK(cudaMemcpyAsync(h.data(), raw.p, sizeof(double) * ne * 6, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int q = 0; q < 6; q++) op->t6[q].assign(h.begin() + q * ne, h.begin() + (q + 1) * ne);
+            op->t6_valid = true;
+        }
+    } else if (k.general) {
+        std::vector<double2> h(plane * 9);
+        for (int q = 0; q < 9; q++) {
+            if (op->t9[q].size() != plane) continue;
+            for (size_t i = 0; i < plane; i++) h[q * plane + i] = make_double2(op->t9[q][i], 0.0);
+        }
+        CK(cudaMemcpy(W.p, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice));
+    } else {
+        // host tensor (user-set LongRange, or an edited Dipole tensor), z offset
+        // k = source - target at padded index (zsign*k mod Pz)
+        ensure_t6_layout(op);
+        const int zsign = op->quirks ? -1 : 1;
+        std::vector<double2> h(plane * 6, make_double2(0, 0));
+        for (int q = 0; q < 6; q++)
+            for (int kk = -(op->nz - 1); kk < op->nz; kk++) {
+                int zi = (zsign * kk) % Pz;
+                if (zi < 0) zi += Pz;
+                for (int j = 0; j < op->ny; j++)
+                    for (int i = 0; i < op->nx; i++) {
+                        const size_t src = (size_t)i + op->nx * ((size_t)j + op->ny * (size_t)(kk + op->nz - 1));
+                        h[q * plane + ((size_t)zi * Py + j) * Px + i] = make_double2(op->t6[q][src], 0.0);
+                    }
+            }
+        CK(cudaMemcpy(W.p, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice));
+    }
+    CK(mlb::launch_fft3d_d(W.p, ncomp, Px, Py, Pz, P->L, twdd.p, -1, st));
+    if (k.general) {
+        P->ten9.alloc((size_t)k.Kx * Py * Pz * 9);
+        CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, st));
+    } else {
+        P->ten6.alloc((size_t)k.Kx * Py * Pz * 6);
+        DBuf<double> mi;
+        mi.alloc(1);
+        CK(cudaMemsetAsync(mi.p, 0, sizeof(double), st));
+        CK(mlb::launch_tensor_pack6(W.p, Px, Py, Pz, k.Kx, P->ten6.p, mi.p, st));
+        CK(cudaMemcpyAsync(&P->max_imag, mi.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    P->spec.alloc((size_t)k.Kx * 3 * op->nz * op->ny);
+    CK(cudaStreamSynchronize(st));
+    op->plan = std::move(P);
+    op->plan_dirty = false;
+}
+
+// ------------------------------------------------------------------ lazy evaluation
+struct TermsBuild {
+    TermsK T;
+    bool ok = true;
+    double dt_sys;
+    std::vector<int> conflict_slots;
+};
+
+void terms_init(TermsK& T)
+{
+    memset(&T, 0, sizeof(T));
+    T.ex_gs = 1.f;
+}
+
+// Add one recorded term to T; false when T already holds a different op
+// of the same kind (the fused kernel evaluates one of each).
+bool terms_add(TermsK& T, const Term& t, bool th_sub, mlb_system* s, bool capture)
+{
+    mlb_op* op = t.op;
+    switch (op->kind) {
+    case MLB_OP_EXCHANGE:
+        if (T.ex.mode != EX_NONE) return false;
+        T.ex = op->exk;
+        T.ex_gs = (float)(op->gs * t.weight);
+        return true;
+    case MLB_OP_ANISOTROPY:
+        if (T.ani.mode != ANI_NONE) return false;
+        T.ani = op->anik;
+        return true;
+    case MLB_OP_UNIAXIAL:
+        if (T.uni.mode != ANI_NONE) return false;
+        T.uni = op->unik;
+        return true;
+    case MLB_OP_CUBIC:
+        if (T.cub.mode != ANI_NONE) return false;
+        T.cub = op->cubk;
+        return true;
+    case MLB_OP_THERMAL:
+        if (T.th.mode != TH_NONE || !th_sub) return false;
+        T.th.mode = TH_PHILOX;
+        T.th.T = (float)(t.T * t.gs);
+        T.th.scale = op->tscale.empty() ? nullptr : op->dscale.p;
+        T.th.seed = op->seed;
+        T.th.counter = t.counter;
+        T.th.dctr = capture ? s->dctr : nullptr;
+        return true;
+    case MLB_OP_APPLIEDFIELD:
+        if (T.zee.on) return false;
+        T.zee.on = 1;
+        for (int a = 0; a < 3; a++) {
+            T.zee.B[a] = t.B[a];
+            T.zee.dB[a] = (float)(op->dB[a] * op->gs);
+        }
+        T.zee.dctr = capture ? s->dctr : nullptr;
+        return true;
+    }
+    return false;
+}
+
+bool add_addend(TermsK& T, float* const h[3], float w, bool thermal)
+{
+    if (T.nadd >= MLB_MAX_ADDENDS) return false;
+    for (int c = 0; c < 3; c++) T.add[T.nadd][c] = h[c];
+    T.addw[T.nadd] = w;
+    T.add_is_thermal[T.nadd] = thermal ? 1 : 0;
+    T.nadd++;
+    return true;
+}
+
+void materialize(mlb_system* s, int si);
+
+// Materialise every SUM slot that lists si (before si changes).
+void before_mutate(mlb_system* s, int si)
+{
+    for (size_t j = 0; j < s->slots.size(); j++) {
+        Slot& x = s->slots[j];
+        if ((int)j != si && x.state == ST_SUM &&
+            std::find(x.sum_list.begin(), x.sum_list.end(), si) != x.sum_list.end())
+            materialize(s, (int)j);
+    }
+}
+
+void eval_into(mlb_system* s, int buf, const TermsK& T, double dt_sys, Slot& out, int acc)
+{
+    slot_alloc(s, out);
+    CK(mlb::launch_eval(sysk(s, buf), T, (float)dt_sys, out.h, acc, s->st));
+}
+
+// Evaluate a LAZY slot into its arrays (state becomes DATA).
+void materialize_lazy(mlb_system* s, int si)
+{
+    Slot& sl = s->slots[si];
+    const int buf = buffer_for_gen(s, sl.gen);
+    const bool th_sub = name_eq(sl.name, "Thermal");
+    // terms one kind at a time so any combination is handled
+    slot_alloc(s, sl);
+    if (!sl.base_data) {
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(sl.h[c], 0, sizeof(float) * s->n, s->st));
+    }
+    for (const Term& t : sl.terms) {
+        TermsK T;
+        terms_init(T);
+        if (!terms_add(T, t, true, s, false)) fail(MLB_ESTATE, "internal: term not representable");
+        (void)th_sub;
+        eval_into(s, buf, T, t.dt_sys, sl, 1);
+    }
+    sl.terms.clear();
+    sl.state = ST_DATA;
+    sl.base_data = false;
+}
+
+// Build the terms of a SUM definition over slots in list (weights 1).
+// Slots that cannot join (different generation, conflicting kinds, too many
+// addends) are materialised first; each retry turns one more slot into DATA.
+void build_sum_terms(mlb_system* s, const std::vector<int>& list, TermsK& T, long long& gen, double& dt_sys,
+                     bool capture, int thermal_slot)
+{
+    for (int iter = 0; iter <= (int)s->slots.size() + 1; iter++) {
+        terms_init(T);
+        gen = s->gen;
+        dt_sys = s->dt;
+        for (int j : list)
+            if (s->slots[j].state == ST_LAZY) { gen = s->slots[j].gen; break; }
+        bool restart = false;
+        for (int j : list) {
+            Slot& x = s->slots[j];
+            const bool is_th = j == thermal_slot;
+            if (x.state == ST_SUM) {
+                if (capture) fail(MLB_ESTATE, "step is not fusable");
+                materialize(s, j);
+            }
+            if (x.state == ST_LAZY) {
+                bool ok = x.gen == gen;
+                TermsK T2 = T;
+                double dts = dt_sys;
+                if (ok && x.base_data) ok = add_addend(T2, x.h, 1.f, is_th);
+                for (const Term& t : x.terms) {
+                    if (!ok) break;
+                    const bool th_here = t.op->kind == MLB_OP_THERMAL;
+                    if (th_here != is_th) { ok = false; break; }
+                    ok = terms_add(T2, t, is_th, s, capture);
+                    if (ok && th_here) dts = t.dt_sys;
+                }
+                if (!ok) {
+                    if (capture) fail(MLB_ESTATE, "step is not fusable");
+                    materialize(s, j);
+                    restart = true;
+                    break;
+                }
+                T = T2;
+                dt_sys = dts;
+            } else if (x.state == ST_DATA) {
+                if (!add_addend(T, x.h, 1.f, is_th)) fail(MLB_EUNSUP, "too many materialised field slots in one sum");
+            }
+        }
+        if (!restart) return;
+    }
+    fail(MLB_ESTATE, "internal: field sum did not settle");
+}
+
+void materialize(mlb_system* s, int si)
+{
+    Slot& sl = s->slots[si];
+    switch (sl.state) {
+    case ST_DATA:
+        return;
+    case ST_ZERO:
+        slot_alloc(s, sl);
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(sl.h[c], 0, sizeof(float) * s->n, s->st));
+        sl.state = ST_DATA;
+        return;
+    case ST_LAZY:
+        materialize_lazy(s, si);
+        return;
+    case ST_SUM: {
+        std::vector<int> list = sl.sum_list;
+        TermsK T;
+        long long gen;
+        double dt_sys;
+        build_sum_terms(s, list, T, gen, dt_sys, false, slot_find(s, "Thermal"));
+        Slot& out = s->slots[si];
+        eval_into(s, buffer_for_gen(s, gen), T, dt_sys, out, 0);
+        out.state = ST_DATA;
+        out.sum_list.clear();
+        return;
+    }
+    }
+}
+
+void materialize_all(mlb_system* s)
+{
+    for (size_t j = 0; j < s->slots.size(); j++)
+        if (s->slots[j].state == ST_SUM) materialize(s, (int)j);
+    for (size_t j = 0; j < s->slots.size(); j++)
+        if (s->slots[j].state == ST_LAZY) materialize(s, (int)j);
+}
+
+// Materialise lazy records that depend on generation gen (before its buffer
+// is overwritten).
+void materialize_gen(mlb_system* s, long long gen)
+{
+    for (size_t j = 0; j < s->slots.size(); j++) {
+        Slot& x = s->slots[j];
+        if (x.state == ST_SUM) {
+            bool dep = false;
+            for (int k : x.sum_list)
+                if (s->slots[k].state == ST_LAZY && s->slots[k].gen == gen) dep = true;
+            if (dep) materialize(s, (int)j);
+        }
+    }
+    for (size_t j = 0; j < s->slots.size(); j++)
+        if (s->slots[j].state == ST_LAZY && s->slots[j].gen == gen) materialize(s, (int)j);
+}
+
+// Every lazy record of every system that references op (before op changes).
+void materialize_users(mlb_op* op)
+{
+    for (mlb_system* s : g_systems) {
+        bool any = false;
+        for (Slot& x : s->slots)
+            for (Term& t : x.terms)
+                if (t.op == op) any = true;
+        if (any) materialize_all(s);
+    }
+}
+
+// ------------------------------------------------------------------ apply
+void check_dims(const mlb_op* op, const mlb_system* s)
+{
+    if (op->nx != s->nx || op->ny != s->ny || op->nz != s->nz)
+        fail(MLB_EINVAL, "operator and SpinSystem sizes differ");
+}
+
+void op_apply(mlb_op* op, mlb_system* s)
+{
+    check_dims(op, s);
+    const int si = slot_register(s, op->slot.c_str());
+    before_mutate(s, si);
+    Slot& sl = s->slots[si];
+    Term t{};
+    t.op = op;
+    t.weight = 1;
+    t.gs = op->gs;
+    t.dt_sys = s->dt;
+    switch (op->kind) {
+    case MLB_OP_EXCHANGE: {
+        compile_exchange(op);
+        sl.used = true;
+        if (op->exk.mode == EX_NONE) {
+            if (sl.state == ST_ZERO) { sl.state = ST_ZERO; }
+            return;
+        }
+        if (sl.state == ST_LAZY && sl.gen != s->gen) materialize(s, si);
+        if (sl.state == ST_SUM) materialize(s, si);
+        if (sl.state == ST_ZERO) {
+            sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
+        } else if (sl.state == ST_DATA) {
+            sl.state = ST_LAZY; sl.base_data = true; sl.terms.assign(1, t); sl.gen = s->gen;
+        } else {
+            bool merged = false;
+            for (Term& x : sl.terms)
+                if (x.op == op && x.gs == t.gs) { x.weight++; merged = true; }
+            if (!merged) sl.terms.push_back(t);
+        }
+        return;
+    }
+    case MLB_OP_ANISOTROPY:
+    case MLB_OP_UNIAXIAL:
+    case MLB_OP_CUBIC:
+        compile_aniso(op);
+        sl.used = true;
+        sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
+        if (op->asite.empty()) { sl.state = ST_ZERO; sl.terms.clear(); }
+        return;
+    case MLB_OP_THERMAL: {
+        compile_thermal_scale(op);
+        sl.used = true;
+        t.T = op->T;
+        if (op->inject_pending) {
+            // injected normals: evaluate now (parity mode)
+            TermsK T;
+            terms_init(T);
+            T.th.mode = TH_INJECT;
+            T.th.T = (float)(op->T * op->gs);
+            T.th.scale = op->tscale.empty() ? nullptr : op->dscale.p;
+            T.th.nx = op->inj[0].p; T.th.ny = op->inj[1].p; T.th.nz = op->inj[2].p;
+            sl.terms.clear();
+            sl.base_data = false;
+            eval_into(s, s->cur, T, s->dt, sl, 0);
+            sl.state = ST_DATA;
+            op->inject_pending = false;
+            return;
+        }
+        t.counter = op->counter++;
+        sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
+        return;
+    }
+    case MLB_OP_APPLIEDFIELD:
+        sl.used = true;
+        for (int a = 0; a < 3; a++) t.B[a] = (float)(op->B[a] * op->gs);
+        sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
+        return;
+    case MLB_OP_DIPOLE:
+    case MLB_OP_LONGRANGE:
+    case MLB_OP_LONGRANGE3D: {
+        if (s->capturing && op->plan_dirty) fail(MLB_ESTATE, "tensor changed during capture");
+        build_plan(op, s->st);
+        sl.used = true;
+        sl.terms.clear();
+        sl.base_data = false;
+        slot_alloc(s, sl);
+        ConvPlan& P = *op->plan;
+        P.k.g = (float)(op->g * op->gs / ((double)P.k.Px * P.k.Py * P.k.Pz));
+        const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+        CK(mlb::launch_conv(P.k, P.L[0], P.L[1], P.L[2], P.tw.p, sp, P.spec.p, P.ten6.p, P.ten9.p, sl.h, s->st));
+        sl.state = ST_DATA;
+        return;
+    }
+    }
+    fail(MLB_EINVAL, "unknown operator kind");
+}
+
+// ------------------------------------------------------------------ llg
+LlgK llgk(const mlb_llg* l, double dt)
+{
+    LlgK k;
+    k.type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
+    k.thermal_only_first_term = l->tof;
+    k.renorm = l->disable_renorm ? 0 : 1;
+    k.precess = (float)l->precess;
+    k.damp = (float)l->damp;
+    k.dt = (float)dt;
+    k.dt_zero = dt == 0.0 ? 1 : 0;
+    return k;
+}
+
+// Fused in-place step when Total is lazily defined; returns false when the
+// caller must take the general path.
+bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
+{
+    Slot& tot = s->slots[0];
+    const int th = slot_find(s, "Thermal");
+    std::vector<int> list;
+    if (tot.state == ST_SUM) list = tot.sum_list;
+    else if (tot.state == ST_DATA) list.push_back(0);
+    else if (tot.state == ST_LAZY) return false;
+    // records of the previous generation are about to be overwritten
+    materialize_gen(s, s->gen - 1);
+    TermsK T;
+    long long gen;
+    double dt_sys;
+    // Thermal slot: its field must be subtracted even when not summed
+    bool th_in = th >= 0 && std::find(list.begin(), list.end(), th) != list.end();
+    if (th >= 0 && !th_in && s->slots[th].state != ST_ZERO) {
+        materialize(s, th);
+    }
+    build_sum_terms(s, list, T, gen, dt_sys, s->capturing, th);
+    if (gen != s->gen) {
+        if (s->capturing) fail(MLB_ESTATE, "step is not fusable");
+        return false;
+    }
+    if (th >= 0 && !th_in && s->slots[th].state == ST_DATA) {
+        if (!add_addend(T, s->slots[th].h, 0.f, true)) return false;
+    }
+    FusedK P;
+    P.sys = sysk(s, s->cur);
+    P.terms = T;
+    P.llg = llgk(l, dt);
+    const int nb = 1 - s->cur;
+    P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
+    CK(mlb::launch_fused(P, (float)dt_sys, s->st));
+    if (s->capturing) CK(mlb::launch_advance(s->dctr, s->st));
+    s->cur = nb;
+    s->gen++;
+    return true;
+}
+
+void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb_system* to, int advance)
+{
+    if (from->nx != dmdt->nx || from->nx != to->nx || from->ny != dmdt->ny || from->ny != to->ny ||
+        from->nz != dmdt->nz || from->nz != to->nz)
+        fail(MLB_EINVAL, "SpinSystems of different sizes");
+    const double dt = scale * dmdt->dt;
+    const bool cart = l->kind != MLB_LLG_QUATERNION;
+    bool done = false;
+    if (from == dmdt && dmdt == to) done = llg_fused(l, from, dt);
+    from->last_fused = done;
+    if (!done) {
+        if (from->capturing) fail(MLB_ESTATE, "step is not fusable");
+        materialize(dmdt, 0);
+        const int th = slot_find(dmdt, "Thermal");
+        if (th >= 0) materialize(dmdt, th);
+        // the destination's spins change in place: settle its lazy fields
+        materialize_all(to);
+        if (to != dmdt) { materialize(dmdt, 0); if (th >= 0) materialize(dmdt, th); }
+        if (from != to && !(cart && dt == 0.0)) {
+            CK(cudaMemcpyAsync(to->ms, from->ms, sizeof(float) * from->n, cudaMemcpyDeviceToDevice, to->st));
+            to->ms_host = from->ms_host;
+            to->ms_dirty = true;
+        }
+        if (from->st != to->st || dmdt->st != to->st) {
+            CK(cudaStreamSynchronize(from->st));
+            CK(cudaStreamSynchronize(dmdt->st));
+        }
+        const float* m[3] = {dmdt->sp[dmdt->cur][0], dmdt->sp[dmdt->cur][1], dmdt->sp[dmdt->cur][2]};
+        const float* H[3] = {dmdt->slots[0].h[0], dmdt->slots[0].h[1], dmdt->slots[0].h[2]};
+        const float* Ht[3] = {nullptr, nullptr, nullptr};
+        if (th >= 0) for (int c = 0; c < 3; c++) Ht[c] = dmdt->slots[th].h[c];
+        float* out[3] = {to->sp[to->cur][0], to->sp[to->cur][1], to->sp[to->cur][2]};
+        CK(mlb::launch_llg(sysk(from, from->cur), m, H, Ht, dmdt->sa, dmdt->sg, (float)dmdt->alpha,
+                           (float)dmdt->gamma, llgk(l, dt), out, to->st));
+    }
+    if (cart) {
+        if (dt != 0.0 && advance) to->time = from->time + dt;
+    } else if (advance) {
+        to->time = from->time + dt;
+    }
+}
+
+void sum_fields(mlb_system* s)
+{
+    Slot& tot = s->slots[0];
+    std::vector<int> list;
+    for (size_t j = 1; j < s->slots.size(); j++)
+        if (s->slots[j].used) list.push_back((int)j);
+    tot.terms.clear();
+    tot.base_data = false;
+    tot.sum_list = list;
+    tot.state = list.empty() ? ST_ZERO : ST_SUM;
+}
+
+void reset_fields(mlb_system* s)
+{
+    for (Slot& x : s->slots) {
+        x.used = false;
+        x.state = ST_ZERO;
+        x.terms.clear();
+        x.sum_list.clear();
+        x.base_data = false;
+    }
+}
+
+void spins_changing(mlb_system* s)
+{
+    // lazy records read the current buffer, which is about to change
+    materialize_all(s);
+}
+
+mlb_system* make_system(int nx, int ny, int nz)
+{
+    if (nx < 1 || ny < 1 || nz < 1) fail(MLB_EINVAL, "dimensions must be positive");
+    const long long n = (long long)nx * ny * nz;
+    if (n > (1LL << 31) - 1) fail(MLB_EUNSUP, "more than 2^31-1 sites");
+    std::unique_ptr<mlb_system> s(new mlb_system());
+    s->nx = nx; s->ny = ny; s->nz = nz; s->n = (int)n;
+    CK(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking));
+    s->st = s->own;
+    for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 3; c++) {
+            CK(cudaMalloc(&s->sp[b][c], sizeof(float) * n));
+            CK(cudaMemset(s->sp[b][c], 0, sizeof(float) * n));
+        }
+    CK(cudaMalloc(&s->ms, sizeof(float) * n));
+    CK(cudaMemset(s->ms, 0, sizeof(float) * n));
+    s->ms_host.assign(n, 0.f);
+    s->ms_dirty = true;
+    CK(cudaMalloc(&s->dctr, sizeof(uint64_t)));
+    CK(cudaMemset(s->dctr, 0, sizeof(uint64_t)));
+    s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
+    CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
+    CK(cudaMalloc(&s->redout, sizeof(double) * 8));
+    slot_register(s.get(), "Total");
+    mlb_system* r = s.release();
+    g_systems.insert(r);
+    return r;
+}
+
+void free_system(mlb_system* s)
+{
+    if (!s) return;
+    g_systems.erase(s);
+    cudaStreamSynchronize(s->st);
+    for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 3; c++) cudaFree(s->sp[b][c]);
+    cudaFree(s->ms);
+    cudaFree(s->sa);
+    cudaFree(s->sg);
+    cudaFree(s->dctr);
+    cudaFree(s->red);
+    cudaFree(s->redout);
+    for (Slot& x : s->slots)
+        for (int c = 0; c < 3; c++) cudaFree(x.h[c]);
+    if (s->own) cudaStreamDestroy(s->own);
+    delete s;
+}
+
+void upload_site_array(mlb_system* s, float** dst, const double* a)
+{
+    spins_changing(s);
+    if (!a) {
+        if (*dst) { CK(cudaStreamSynchronize(s->st)); cudaFree(*dst); }
+        *dst = nullptr;
+        return;
+    }
+    std::vector<float> f(s->n);
+    for (int i = 0; i < s->n; i++) f[i] = (float)a[i];
+    if (!*dst) CK(cudaMalloc(dst, sizeof(float) * s->n));
+    CK(cudaMemcpyAsync(*dst, f.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+}
+
+void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
+{
+    reset_fields(s);
+    for (int i = 0; i < nops; i++) op_apply(ops[i], s);
+    sum_fields(s);
+    llg_apply(l, s, 1.0, s, s, 1);
+}
+
+} // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* mlb_last_error(void) { return g_err.c_str(); }
+
+int mlb_profile_begin(void)
+{
+    return guard([&] { mlb::prof_begin(); });
+}
+
+int mlb_profile_end(int cap, char* names, double* ms, int* launches, int* count)
+{
+    return guard([&] { *count = mlb::prof_end(cap, names, ms, launches); });
+}
+
+int mlb_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    const Philox4 r = philox4x32_10(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1]);
+    for (int i = 0; i < 4; i++) out[i] = r.v[i];
+    return MLB_OK;
+}
+int mlb_version(void) { return 1; }
+
+int mlb_init(int device)
+{
+    return guard([&] {
+        CK(cudaSetDevice(device));
+        CK(cudaFree(0));
+        CK(mlb::conv_configure());
+    });
+}
+
+int mlb_system_create(int nx, int ny, int nz, mlb_system** out)
+{
+    return guard([&] {
+        if (!out) fail(MLB_EINVAL, "null output");
+        *out = make_system(nx, ny, nz);
+    });
+}
+
+int mlb_system_destroy(mlb_system* s)
+{
+    return guard([&] { free_system(s); });
+}
+
+int mlb_system_dims(const mlb_system* s, int out[3])
+{
+    return guard([&] {
+        out[0] = s->nx; out[1] = s->ny; out[2] = s->nz;
+    });
+}
+
+int mlb_system_set_stream(mlb_system* s, void* stream)
+{
+    return guard([&] {
+        CK(cudaStreamSynchronize(s->st));
+        s->st = stream ? (cudaStream_t)stream : s->own;
+    });
+}
+
+int mlb_system_get_stream(const mlb_system* s, void** stream)
+{
+    return guard([&] { *stream = (void*)s->st; });
+}
+
+int mlb_system_synchronize(mlb_system* s)
+{
+    return guard([&] { CK(cudaStreamSynchronize(s->st)); });
+}
+
+int mlb_system_set_spin(mlb_system* s, int idx, double sx, double sy, double sz)
+{
+    return guard([&] {
+        if (idx < 0 || idx >= s->n) fail(MLB_ERANGE, "site outside the SpinSystem");
+        spins_changing(s);
+        const float v[3] = {(float)sx, (float)sy, (float)sz};
+        for (int c = 0; c < 3; c++)
+            CK(cudaMemcpyAsync(s->sp[s->cur][c] + idx, &v[c], sizeof(float), cudaMemcpyHostToDevice, s->st));
+        s->ms_host[idx] = (float)std::sqrt(sx * sx + sy * sy + sz * sz);
+        CK(cudaMemcpyAsync(s->ms + idx, &s->ms_host[idx], sizeof(float), cudaMemcpyHostToDevice, s->st));
+        s->ms_dirty = true;
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int mlb_system_get_spin(mlb_system* s, int idx, double out4[4])
+{
+    return guard([&] {
+        if (idx < 0 || idx >= s->n) fail(MLB_ERANGE, "site outside the SpinSystem");
+        float v[3];
+        for (int c = 0; c < 3; c++)
+            CK(cudaMemcpyAsync(&v[c], s->sp[s->cur][c] + idx, sizeof(float), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        out4[0] = v[0]; out4[1] = v[1]; out4[2] = v[2]; out4[3] = s->ms_host[idx];
+    });
+}
+
+int mlb_system_set_spins(mlb_system* s, const double* x, const double* y, const double* z, const double* ms)
+{
+    return guard([&] {
+        if (!x || !y || !z) fail(MLB_EINVAL, "null spin array");
+        spins_changing(s);
+        std::vector<float> f[3];
+        const double* src[3] = {x, y, z};
+        for (int c = 0; c < 3; c++) {
+            f[c].resize(s->n);
+            for (int i = 0; i < s->n; i++) f[c][i] = (float)src[c][i];
+            CK(cudaMemcpyAsync(s->sp[s->cur][c], f[c].data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+        }
+        for (int i = 0; i < s->n; i++)
+            s->ms_host[i] = ms ? (float)ms[i] : (float)std::sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+        CK(cudaMemcpyAsync(s->ms, s->ms_host.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+        s->ms_dirty = true;
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int mlb_system_get_spins(mlb_system* s, double* x, double* y, double* z, double* ms)
+{
+    return guard([&] {
+        std::vector<float> f(s->n);
+        double* dst[3] = {x, y, z};
+        for (int c = 0; c < 3; c++) {
+            if (!dst[c]) continue;
+            CK(cudaMemcpyAsync(f.data(), s->sp[s->cur][c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            for (int i = 0; i < s->n; i++) dst[c][i] = f[i];
+        }
+        if (ms)
+            for (int i = 0; i < s->n; i++) ms[i] = s->ms_host[i];
+    });
+}
+
+int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const float* z, const float* ms)
+{
+    return guard([&] {
+        spins_changing(s);
+        const float* src[3] = {x, y, z};
+        for (int c = 0; c < 3; c++)
+            CK(cudaMemcpyAsync(s->sp[s->cur][c], src[c], sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+        if (ms) {
+            CK(cudaMemcpyAsync(s->ms, ms, sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+            if (memcmp(s->ms_host.data(), ms, sizeof(float) * s->n) != 0) {
+                memcpy(s->ms_host.data(), ms, sizeof(float) * s->n);
+                s->ms_dirty = true;
+            }
+        }
+    });
+}
+
+int mlb_system_download_f32(mlb_system* s, float* x, float* y, float* z)
+{
+    return guard([&] {
+        float* dst[3] = {x, y, z};
+        for (int c = 0; c < 3; c++)
+            if (dst[c]) CK(cudaMemcpyAsync(dst[c], s->sp[s->cur][c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
+    });
+}
+
+int mlb_system_set_param(mlb_system* s, int which, double v)
+{
+    return guard([&] {
+        switch (which) {
+        case MLB_ALPHA:
+            // setAlpha drops per-site values (SpinSystem::setAlpha :1003-1008)
+            if (s->sa) { spins_changing(s); CK(cudaStreamSynchronize(s->st)); cudaFree(s->sa); s->sa = nullptr; }
+            s->alpha = v;
+            break;
+        case MLB_GAMMA:
+            if (s->sg) { spins_changing(s); CK(cudaStreamSynchronize(s->st)); cudaFree(s->sg); s->sg = nullptr; }
+            s->gamma = v;
+            break;
+        case MLB_DT: s->dt = v; break;
+        case MLB_TIME: s->time = v; break;
+        default: fail(MLB_EINVAL, "unknown parameter");
+        }
+    });
+}
+
+int mlb_system_get_param(const mlb_system* s, int which, double* v)
+{
+    return guard([&] {
+        switch (which) {
+        case MLB_ALPHA: *v = s->alpha; break;
+        case MLB_GAMMA: *v = s->gamma; break;
+        case MLB_DT: *v = s->dt; break;
+        case MLB_TIME: *v = s->time; break;
+        default: fail(MLB_EINVAL, "unknown parameter");
+        }
+    });
+}
+
+int mlb_system_set_site_alpha(mlb_system* s, const double* a)
+{
+    return guard([&] { upload_site_array(s, &s->sa, a); });
+}
+
+int mlb_system_set_site_gamma(mlb_system* s, const double* g)
+{
+    return guard([&] { upload_site_array(s, &s->sg, g); });
+}
+
+int mlb_system_reset_fields(mlb_system* s)
+{
+    return guard([&] { reset_fields(s); });
+}
+
+int mlb_system_sum_fields(mlb_system* s)
+{
+    return guard([&] {
+        before_mutate(s, 0);
+        sum_fields(s);
+    });
+}
+
+int mlb_system_sum_fields_custom(mlb_system* s, const char* dest, int n, const char* const* src, const double* w)
+{
+    return guard([&] {
+        const int d = slot_register(s, dest);
+        before_mutate(s, d);
+        // materialise the sources and the destination, then a weighted sum
+        std::vector<int> idx;
+        std::vector<float> ww;
+        for (int k = 0; k < n; k++) {
+            const int j = slot_find(s, src[k]);
+            if (j < 0 || !s->slots[j].used) continue;
+            materialize(s, j);
+            idx.push_back(j);
+            ww.push_back((float)(w ? w[k] : 1.0));
+        }
+        Slot& out = s->slots[d];
+        out.terms.clear();
+        out.sum_list.clear();
+        slot_alloc(s, out);
+        // accumulate in batches of addends
+        int acc = 0;
+        size_t k = 0;
+        do {
+            TermsK T;
+            terms_init(T);
+            for (; k < idx.size() && T.nadd < MLB_MAX_ADDENDS; k++) {
+                const int j = idx[k];
+                if (j == d) {
+                    // the destination is also a source: copy it aside first
+                    fail(MLB_EUNSUP, "destination listed among the sources");
+                }
+                add_addend(T, s->slots[j].h, ww[k], false);
+            }
+            eval_into(s, s->cur, T, s->dt, out, acc);
+            acc = 1;
+        } while (k < idx.size());
+        out.state = ST_DATA;
+    });
+}
+
+int mlb_system_get_field(mlb_system* s, const char* slot, double* hx, double* hy, double* hz)
+{
+    return guard([&] {
+        const int j = slot_find(s, slot);
+        if (j < 0) fail(MLB_ENOTFOUND, std::string("Unknown field type `") + slot + "'");
+        materialize(s, j);
+        std::vector<float> f(s->n);
+        double* dst[3] = {hx, hy, hz};
+        for (int c = 0; c < 3; c++) {
+            if (!dst[c]) continue;
+            CK(cudaMemcpyAsync(f.data(), s->slots[j].h[c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            for (int i = 0; i < s->n; i++) dst[c][i] = f[i];
+        }
+    });
+}
+
+int mlb_system_set_field(mlb_system* s, const char* slot, const double* hx, const double* hy, const double* hz)
+{
+    return guard([&] {
+        const int j = slot_register(s, slot);
+        before_mutate(s, j);
+        materialize(s, j);
+        std::vector<float> f(s->n);
+        const double* src[3] = {hx, hy, hz};
+        for (int c = 0; c < 3; c++) {
+            if (!src[c]) continue;
+            for (int i = 0; i < s->n; i++) f[i] = (float)src[c][i];
+            CK(cudaMemcpyAsync(s->slots[j].h[c], f.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+            CK(cudaStreamSynchronize(s->st));
+        }
+    });
+}
+
+int mlb_system_slot_used(mlb_system* s, const char* slot, int* used)
+{
+    return guard([&] {
+        const int j = slot_find(s, slot);
+        if (j < 0) fail(MLB_ENOTFOUND, std::string("Unknown field type `") + slot + "'");
+        *used = s->slots[j].used ? 1 : 0;
+    });
+}
+
+int mlb_system_set_slot_used(mlb_system* s, const char* slot, int used)
+{
+    return guard([&] {
+        const int j = slot_find(s, slot);
+        if (j < 0) fail(MLB_ENOTFOUND, std::string("Unknown field type`") + slot + "'");
+        s->slots[j].used = used != 0;
+    });
+}
+
+int mlb_system_ensure_slot(mlb_system* s, const char* slot)
+{
+    return guard([&] { slot_register(s, slot); });
+}
+
+int mlb_system_netmoment(mlb_system* s, double m, double out8[8])
+{
+    return guard([&] {
+        CK(mlb::launch_netmoment(s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2], s->n, m, s->red, s->red_nb,
+                                 s->redout, s->st));
+        double r[6];
+        CK(cudaMemcpyAsync(r, s->redout, sizeof(r), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        out8[0] = r[0]; out8[1] = r[1]; out8[2] = r[2];
+        out8[3] = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        out8[4] = r[3]; out8[5] = r[4]; out8[6] = r[5];
+        out8[7] = std::sqrt(r[3] * r[3] + r[4] * r[4] + r[5] * r[5]);
+    });
+}
+
+int mlb_system_field_dot(mlb_system* s, const char* slot, double* out)
+{
+    return guard([&] {
+        const int j = slot_find(s, slot);
+        if (j < 0) fail(MLB_ENOTFOUND, std::string("Unknown field type `") + slot + "'");
+        materialize(s, j);
+        const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+        const float* h[3] = {s->slots[j].h[0], s->slots[j].h[1], s->slots[j].h[2]};
+        CK(mlb::launch_dot(sp, h, s->n, s->red, s->red_nb, s->redout, s->st));
+        CK(cudaMemcpyAsync(out, s->redout, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    });
+}
+
+int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
+{
+    return guard([&] {
+        if (dst->nx != src->nx || dst->ny != src->ny || dst->nz != src->nz) fail(MLB_EINVAL, "size mismatch");
+        if (dst == src) return;
+        spins_changing(dst);
+        CK(cudaStreamSynchronize(src->st));
+        for (int c = 0; c < 3; c++)
+            CK(cudaMemcpyAsync(dst->sp[dst->cur][c], src->sp[src->cur][c], sizeof(float) * src->n,
+                               cudaMemcpyDeviceToDevice, dst->st));
+        CK(cudaMemcpyAsync(dst->ms, src->ms, sizeof(float) * src->n, cudaMemcpyDeviceToDevice, dst->st));
+        dst->ms_host = src->ms_host;
+        dst->ms_dirty = true;
+        dst->alpha = src->alpha; dst->gamma = src->gamma; dst->dt = src->dt; dst->time = src->time;
+        CK(cudaStreamSynchronize(dst->st));
+        upload_site_array(dst, &dst->sa, nullptr);
+        upload_site_array(dst, &dst->sg, nullptr);
+        if (src->sa) {
+            CK(cudaMalloc(&dst->sa, sizeof(float) * src->n));
+            CK(cudaMemcpy(dst->sa, src->sa, sizeof(float) * src->n, cudaMemcpyDeviceToDevice));
+        }
+        if (src->sg) {
+            CK(cudaMalloc(&dst->sg, sizeof(float) * src->n));
+            CK(cudaMemcpy(dst->sg, src->sg, sizeof(float) * src->n, cudaMemcpyDeviceToDevice));
+        }
+        if (with_fields) {
+            materialize_all(src);
+            reset_fields(dst);
+            for (Slot& x : src->slots) {
+                const int j = slot_register(dst, x.name.c_str());
+                Slot& y = dst->slots[j];
+                y.used = x.used;
+                if (x.state == ST_DATA) {
+                    slot_alloc(dst, y);
+                    for (int c = 0; c < 3; c++)
+                        CK(cudaMemcpy(y.h[c], x.h[c], sizeof(float) * src->n, cudaMemcpyDeviceToDevice));
+                    y.state = ST_DATA;
+                }
+            }
+        }
+        CK(cudaDeviceSynchronize());
+    });
+}
+
+// ---------------------------------------------------------------- operators
+int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out)
+{
+    return guard([&] {
+        if (nx < 1 || ny < 1 || nz < 1) fail(MLB_EINVAL, "dimensions must be positive");
+        std::unique_ptr<mlb_op> op(new mlb_op());
+        op->kind = kind;
+        op->nx = nx; op->ny = ny; op->nz = nz;
+        switch (kind) {
+        case MLB_OP_EXCHANGE: op->slot = "Exchange"; break;
+        case MLB_OP_ANISOTROPY: op->slot = "Anisotropy"; break;
+        case MLB_OP_UNIAXIAL: op->slot = "UniaxialAnisotropy"; break;
+        case MLB_OP_CUBIC: op->slot = "CubicAnisotropy"; break;
+        case MLB_OP_THERMAL: op->slot = "Thermal"; break;
+        case MLB_OP_APPLIEDFIELD: op->slot = "Zeeman"; break;
+        case MLB_OP_DIPOLE: op->slot = "Dipole"; break;
+        case MLB_OP_LONGRANGE: op->slot = "LongRange"; break;
+        case MLB_OP_LONGRANGE3D: op->slot = "LongRange3D"; break;
+        default: fail(MLB_EINVAL, "unknown operator kind");
+        }
+        *out = op.release();
+    });
+}
+
+int mlb_op_destroy(mlb_op* op)
+{
+    return guard([&] {
+        if (!op) return;
+        materialize_users(op);
+        cudaDeviceSynchronize();
+        delete op;
+    });
+}
+
+int mlb_op_kind(const mlb_op* op, int* kind) { return guard([&] { *kind = op->kind; }); }
+
+int mlb_op_set_scale(mlb_op* op, double gs)
+{
+    return guard([&] {
+        materialize_users(op);
+        op->gs = gs;
+    });
+}
+
+int mlb_op_get_scale(const mlb_op* op, double* gs) { return guard([&] { *gs = op->gs; }); }
+
+int mlb_op_set_slot_name(mlb_op* op, const char* name)
+{
+    return guard([&] {
+        if (!name || !*name) fail(MLB_EINVAL, "empty slot name");
+        op->slot = name;
+    });
+}
+
+int mlb_op_get_slot_name(const mlb_op* op, char* buf, size_t len)
+{
+    return guard([&] {
+        if (!buf || len == 0) fail(MLB_EINVAL, "null buffer");
+        snprintf(buf, len, "%s", op->slot.c_str());
+    });
+}
+
+int mlb_op_set_quirks(mlb_op* op, int on)
+{
+    return guard([&] {
+        materialize_users(op);
+        op->quirks = on != 0;
+        op->a_dirty = true;
+        op->plan_dirty = true;
+    });
+}
+
+int mlb_op_apply(mlb_op* op, mlb_system* s)
+{
+    return guard([&] { op_apply(op, s); });
+}
+
+int mlb_op_apply_many(mlb_op* op, mlb_system* const* s, int n)
+{
+    return guard([&] {
+        for (int i = 0; i < n; i++) op_apply(op, s[i]);
+    });
+}
+
+int mlb_exchange_add_path(mlb_op* op, int from, int to, double J)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_EXCHANGE) fail(MLB_EINVAL, "not an Exchange operator");
+        check_site(op, from);
+        check_site(op, to);
+        if (J == 0) return; // addPath ignores zero strengths (:330)
+        materialize_users(op);
+        op->ef.push_back(from); op->et.push_back(to); op->eJ.push_back(J);
+        op->ex_dirty = true;
+    });
+}
+
+int mlb_exchange_add_paths(mlb_op* op, const int* from, const int* to, const double* J, int n)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_EXCHANGE) fail(MLB_EINVAL, "not an Exchange operator");
+        for (int p = 0; p < n; p++) { check_site(op, from[p]); check_site(op, to[p]); }
+        materialize_users(op);
+        for (int p = 0; p < n; p++) {
+            if (J[p] == 0) continue;
+            op->ef.push_back(from[p]); op->et.push_back(to[p]); op->eJ.push_back(J[p]);
+        }
+        op->ex_dirty = true;
+    });
+}
+
+int mlb_exchange_set_normalize(mlb_op* op, int on)
+{
+    return guard([&] {
+        materialize_users(op);
+        op->normalize = on != 0;
+        op->ex_dirty = true;
+    });
+}
+
+int mlb_exchange_num_paths(const mlb_op* op, int* n) { return guard([&] { *n = (int)op->ef.size(); }); }
+
+int mlb_anisotropy_add(mlb_op* op, int site, const double axis[3], double K)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_ANISOTROPY) fail(MLB_EINVAL, "not an Anisotropy operator");
+        check_site(op, site);
+        const double len = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+        if (!(len > 0)) return; // l_add: zero axis is not added
+        materialize_users(op);
+        op->asite.push_back(site);
+        for (int a = 0; a < 3; a++) op->apar.push_back(axis[a] / len);
+        op->apar.push_back(K);
+        op->a_dirty = true;
+    });
+}
+
+int mlb_uniaxial_add(mlb_op* op, int site, const double axis[3], double K1, double K2)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_UNIAXIAL) fail(MLB_EINVAL, "not an Anisotropy.Uniaxial operator");
+        check_site(op, site);
+        materialize_users(op);
+        // addAnisotropy scales by 1/dot(a,a) (..._uniaxial.cpp:172-174)
+        const double len = axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2];
+        op->asite.push_back(site);
+        for (int a = 0; a < 3; a++) op->apar.push_back(len > 0 ? axis[a] * (1.0 / len) : axis[a]);
+        op->apar.push_back(K1);
+        op->apar.push_back(K2);
+        op->a_dirty = true;
+    });
+}
+
+int mlb_cubic_add(mlb_op* op, int site, const double a1[3], const double a2[3], const double K[3])
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_CUBIC) fail(MLB_EINVAL, "not an Anisotropy.Cubic operator");
+        check_site(op, site);
+        // axis construction of AnisotropyCubic::addAnisotropy (..._cubic.cpp:180-236)
+        double u[3] = {a1[0], a1[1], a1[2]}, v[3] = {a2[0], a2[1], a2[2]};
+        auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+        auto cross = [](const double* a, const double* b, double* c) {
+            c[0] = a[1] * b[2] - a[2] * b[1];
+            c[1] = a[2] * b[0] - a[0] * b[2];
+            c[2] = a[0] * b[1] - a[1] * b[0];
+        };
+        if (dot(u, u) == 0 || dot(v, v) == 0) fail(MLB_EINVAL, "Failed to add anisotropy, are your vectors colinear or empty?");
+        double s1 = 1.0 / std::sqrt(dot(u, u));
+        for (int a = 0; a < 3; a++) u[a] *= s1;
+        double s2 = 1.0 / std::sqrt(dot(v, v));
+        for (int a = 0; a < 3; a++) v[a] *= s2;
+        if (std::fabs(dot(u, v)) == 1) fail(MLB_EINVAL, "Failed to add anisotropy, are your vectors colinear or empty?");
+        if (dot(u, v) != 0) {
+            const double d = dot(u, v);
+            double p[3] = {u[0] * d, u[1] * d, u[2] * d};
+            for (int a = 0; a < 3; a++) v[a] = v[a] + -1 * p[a];
+        }
+        double ax[9];
+        memcpy(ax, u, sizeof(u));
+        memcpy(ax + 3, v, sizeof(v));
+        cross(ax, ax + 3, ax + 6);
+        for (int i = 0; i < 3; i++) {
+            const double len = dot(ax + 3 * i, ax + 3 * i);
+            if (len > 0) { const double sc = 1.0 / len; for (int a = 0; a < 3; a++) ax[3 * i + a] *= sc; }
+        }
+        materialize_users(op);
+        op->asite.push_back(site);
+        for (int a = 0; a < 9; a++) op->apar.push_back(ax[a]);
+        for (int a = 0; a < 3; a++) op->apar.push_back(K[a]);
+        op->a_dirty = true;
+    });
+}
+
+int mlb_anisotropy_add_many(mlb_op* op, int n, const int* sites, const double* axes, const double* K)
+{
+    for (int j = 0; j < n; j++) {
+        const int rc = mlb_anisotropy_add(op, sites[j], axes + 3 * j, K[j]);
+        if (rc != MLB_OK) return rc;
+    }
+    return MLB_OK;
+}
+
+int mlb_uniaxial_add_many(mlb_op* op, int n, const int* sites, const double* axes, const double* K1,
+                          const double* K2)
+{
+    for (int j = 0; j < n; j++) {
+        const int rc = mlb_uniaxial_add(op, sites[j], axes + 3 * j, K1[j], K2[j]);
+        if (rc != MLB_OK) return rc;
+    }
+    return MLB_OK;
+}
+
+int mlb_cubic_add_many(mlb_op* op, int n, const int* sites, const double* a1, const double* a2, const double* K)
+{
+    for (int j = 0; j < n; j++) {
+        const int rc = mlb_cubic_add(op, sites[j], a1 + 3 * j, a2 + 3 * j, K + 3 * j);
+        if (rc != MLB_OK) return rc;
+    }
+    return MLB_OK;
+}
+
+int mlb_thermal_set_temperature(mlb_op* op, double T)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
+        op->T = T;
+    });
+}
+
+int mlb_thermal_get_temperature(const mlb_op* op, double* T) { return guard([&] { *T = op->T; }); }
+
+int mlb_thermal_scale_site(mlb_op* op, int idx, double v)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
+        const int n = op->nx * op->ny * op->nz;
+        if (idx < 0 || idx >= n) return; // scaleSite ignores non-members
+        materialize_users(op);
+        if (op->tscale.empty()) op->tscale.assign(n, 1.0);
+        op->tscale[idx] = v;
+        op->tscale_dirty = true;
+    });
+}
+
+int mlb_thermal_set_seed(mlb_op* op, uint64_t seed)
+{
+    return guard([&] {
+        materialize_users(op);
+        op->seed = seed;
+    });
+}
+
+int mlb_thermal_set_counter(mlb_op* op, uint64_t counter)
+{
+    return guard([&] { op->counter = counter; });
+}
+
+int mlb_thermal_inject(mlb_op* op, const double* nx, const double* ny, const double* nz)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
+        const int n = op->nx * op->ny * op->nz;
+        const double* src[3] = {nx, ny, nz};
+        std::vector<float> f(n);
+        for (int c = 0; c < 3; c++) {
+            op->inj[c].alloc(n);
+            for (int i = 0; i < n; i++) f[i] = (float)src[c][i];
+            CK(cudaMemcpy(op->inj[c].p, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+        }
+        op->inject_pending = true;
+    });
+}
+
+int mlb_appliedfield_set(mlb_op* op, double bx, double by, double bz)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_APPLIEDFIELD) fail(MLB_EINVAL, "not an AppliedField operator");
+        op->B[0] = bx; op->B[1] = by; op->B[2] = bz;
+    });
+}
+
+int mlb_appliedfield_get(const mlb_op* op, double out3[3])
+{
+    return guard([&] { for (int a = 0; a < 3; a++) out3[a] = op->B[a]; });
+}
+
+int mlb_appliedfield_set_sweep(mlb_op* op, double dbx, double dby, double dbz)
+{
+    return guard([&] { op->dB[0] = dbx; op->dB[1] = dby; op->dB[2] = dbz; });
+}
+
+int mlb_longrange_set_strength(mlb_op* op, double g)
+{
+    return guard([&] {
+        if (!is_conv(op->kind)) fail(MLB_EINVAL, "not a LongRange operator");
+        op->g = g;
+    });
+}
+
+int mlb_longrange_get_strength(const mlb_op* op, double* g) { return guard([&] { *g = op->g; }); }
+
+int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4])
+{
+    return guard([&] {
+        for (int i = 0; i < 4; i++) op->gmax[i] = gmax[i];
+        if (op->gmax[0] < 0) fail(MLB_EUNSUP, "infinite truncation (extrapolated lattice sum) is not built");
+        op->t6_valid = false;
+        op->plan_dirty = true;
+    });
+}
+
+int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9])
+{
+    return guard([&] {
+        for (int i = 0; i < 9; i++) op->ABC[i] = ABC[i];
+        op->t6_valid = false;
+        op->plan_dirty = true;
+    });
+}
+
+int mlb_longrange_set_open(mlb_op* op, int ox, int oy, int oz)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_DIPOLE) fail(MLB_EINVAL, "open boundaries apply to Dipole");
+        if (!oz && op->nz > 1) fail(MLB_EUNSUP, "the Dipole layer sum is open in z");
+        op->open[0] = ox != 0; op->open[1] = oy != 0; op->open[2] = 1;
+        op->t6_valid = false;
+        op->plan_dirty = true;
+    });
+}
+
+static void offset_index(const mlb_op* op, int ox, int oy, int oz, long long* off)
+{
+    // getsetPattern (spinoperationlongrange.cpp:154-178): wrap in-plane, z in [-nz, nz)
+    ox = (ox + 10 * op->nx) % op->nx;
+    oy = (oy + 10 * op->ny) % op->ny;
+    if (oz < -op->nz || oz >= op->nz) { *off = -1; return; }
+    // the reference's offsetOK accepts z = -nz (:144-151), one layer below the
+    // stored range; treat it as outside
+    if (oz <= -op->nz) { *off = -1; return; }
+    *off = ox + (long long)op->nx * (oy + (long long)op->ny * (oz + op->nz - 1));
+}
+
+int mlb_longrange_set_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double v)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE) fail(MLB_EINVAL, "not a LongRange operator");
+        if (ab < 0 || ab > 5) fail(MLB_EINVAL, "1st argument must be matrix name: XX, XY, XZ, YY, YZ or ZZ");
+        if (op->kind == MLB_OP_DIPOLE && (op->open[0] || op->open[1])) fail(MLB_EUNSUP, "open-boundary tensor");
+        if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
+            cudaStream_t st;
+            CK(cudaStreamCreate(&st));
+            build_plan(op, st);
+            cudaStreamDestroy(st);
+        }
+        ensure_t6_layout(op);
+        long long off;
+        offset_index(op, ox, oy, oz, &off);
+        if (off < 0) return;
+        materialize_users(op);
+        op->t6[ab][off] = v;
+        op->t6_valid = true;
+        op->plan_dirty = true;
+    });
+}
+
+int mlb_longrange_get_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double* v)
+{
+    return guard([&] {
+        if (ab < 0 || ab > 5) fail(MLB_EINVAL, "1st argument must be matrix name: XX, XY, XZ, YY, YZ or ZZ");
+        if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
+            cudaStream_t st;
+            CK(cudaStreamCreate(&st));
+            build_plan(op, st);
+            cudaStreamDestroy(st);
+        }
+        ensure_t6_layout(op);
+        long long off;
+        offset_index(op, ox, oy, oz, &off);
+        *v = off < 0 ? 0.0 : op->t6[ab][off];
+    });
+}
+
+int mlb_longrange_get_tensor(mlb_op* op, double* const t6[6])
+{
+    return guard([&] {
+        if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
+            if (op->open[0] || op->open[1]) fail(MLB_EUNSUP, "open-boundary tensor has no reference layout");
+            cudaStream_t st;
+            CK(cudaStreamCreate(&st));
+            build_plan(op, st);
+            cudaStreamDestroy(st);
+        }
+        ensure_t6_layout(op);
+        for (int q = 0; q < 6; q++)
+            if (t6[q]) memcpy(t6[q], op->t6[q].data(), sizeof(double) * op->t6[q].size());
+    });
+}
+
+int mlb_longrange3d_set_tensor(mlb_op* op, int ab, const double* t)
+{
+    return guard([&] {
+        if (op->kind != MLB_OP_LONGRANGE3D) fail(MLB_EINVAL, "not a LongRange3D operator");
+        if (ab < 0 || ab > 8) fail(MLB_EINVAL, "tensor component must be 0..8");
+        materialize_users(op);
+        const size_t n = (size_t)op->nx * op->ny * op->nz;
+        op->t9[ab].assign(t, t + n);
+        op->plan_dirty = true;
+    });
+}
+
+// ---------------------------------------------------------------- LLG
+int mlb_llg_create(int kind, mlb_llg** out)
+{
+    return guard([&] {
+        if (kind != MLB_LLG_CARTESIAN && kind != MLB_LLG_QUATERNION) fail(MLB_EINVAL, "unknown LLG type");
+        mlb_llg* l = new mlb_llg();
+        l->kind = kind;
+        *out = l;
+    });
+}
+
+int mlb_llg_destroy(mlb_llg* l)
+{
+    return guard([&] { delete l; });
+}
+
+int mlb_llg_set_flags(mlb_llg* l, int tof, int disable_renorm, double precess, double damp)
+{
+    return guard([&] {
+        l->tof = tof != 0;
+        l->disable_renorm = disable_renorm != 0;
+        l->precess = precess;
+        l->damp = damp;
+    });
+}
+
+int mlb_llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb_system* to, int advance)
+{
+    return guard([&] {
+        if (!from) fail(MLB_EINVAL, "apply requires 1, 2 or 3 SpinSystems");
+        if (!dmdt) dmdt = from;
+        if (!to) to = from;
+        llg_apply(l, from, scale, dmdt, to, advance);
+    });
+}
+
+// ---------------------------------------------------------------- fused run
+int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps)
+{
+    return guard([&] {
+        if (nsteps <= 0) return;
+        for (int i = 0; i < nops; i++) check_dims(ops[i], s);
+        // step 1 (host path) sets up plans, slot arrays and fusability
+        do_step(s, ops, nops, l);
+        for (int i = 0; i < nops; i++)
+            if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
+                for (int a = 0; a < 3; a++) ops[i]->B[a] += ops[i]->dB[a];
+        int left = nsteps - 1;
+        bool graphable = s->last_fused && left >= 3;
+        for (int i = 0; i < nops; i++)
+            if (ops[i]->kind == MLB_OP_THERMAL && ops[i]->inject_pending) graphable = false;
+        if (graphable) {
+            const int pairs = (left - 1) / 2;
+            if (pairs > 0) {
+                // capture two steps (buffer A->B, B->A); the Thermal counter and
+                // the field sweep read the device step counter
+                const int cur0 = s->cur;
+                const long long gen0 = s->gen;
+                const double time0 = s->time;
+                std::vector<uint64_t> ctr0(nops);
+                for (int i = 0; i < nops; i++) ctr0[i] = ops[i]->counter;
+                CK(cudaMemsetAsync(s->dctr, 0, sizeof(uint64_t), s->st));
+                CK(cudaStreamSynchronize(s->st));
+                cudaGraph_t graph = nullptr;
+                cudaGraphExec_t exec = nullptr;
+                bool captured = false;
+                if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                    s->capturing = true;
+                    bool ok = true;
+                    try {
+                        do_step(s, ops, nops, l);
+                        for (int i = 0; i < nops; i++)
+                            if (ops[i]->kind == MLB_OP_THERMAL) ops[i]->counter = ctr0[i];
+                        do_step(s, ops, nops, l);
+                    } catch (Err&) {
+                        ok = false;
+                    }
+                    s->capturing = false;
+                    cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+                    if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess)
+                        captured = true;
+                    cudaGetLastError();
+                }
+                // host state as it was before the capture
+                s->cur = cur0;
+                s->gen = gen0;
+                s->time = time0;
+                for (int i = 0; i < nops; i++)
+                    if (ops[i]->kind == MLB_OP_THERMAL) ops[i]->counter = ctr0[i];
+                reset_fields(s);
+                if (captured) {
+                    for (int p = 0; p < pairs; p++) CK(cudaGraphLaunch(exec, s->st));
+                    // bookkeeping of the 2*pairs graph steps
+                    s->gen = gen0 + 2LL * pairs;
+                    for (int k = 0; k < 2 * pairs; k++) s->time = s->time + s->dt;
+                    for (int i = 0; i < nops; i++) {
+                        if (ops[i]->kind == MLB_OP_THERMAL) ops[i]->counter = ctr0[i] + 2ULL * pairs;
+                        if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
+                            for (int a = 0; a < 3; a++) ops[i]->B[a] += 2.0 * pairs * ops[i]->dB[a];
+                    }
+                    left -= 2 * pairs;
+                }
+                if (exec) cudaGraphExecDestroy(exec);
+                if (graph) cudaGraphDestroy(graph);
+            }
+        }
+        for (int k = 0; k < left; k++) {
+            do_step(s, ops, nops, l);
+            for (int i = 0; i < nops; i++)
+                if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
+                    for (int a = 0; a < 3; a++) ops[i]->B[a] += ops[i]->dB[a];
+        }
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,954 @@
+// kernels.cu -- sm_100a kernels of the spin-dynamics step.
+//
+//   k_fused_step     one pass: Exchange + Anisotropy (generic/uniaxial/cubic)
+//                    + Thermal (Philox or injected normals) + Zeeman + materialised
+//                    slot arrays (the dipole field) -> LLG (Cartesian or Quaternion)
+//                    -> renormalised spins written to the other spin buffer.
+//   k_eval_terms     the same field evaluation written to a slot (materialise).
+//   k_llg            stand-alone LLG over slot arrays (general from/dmdt/to).
+//   k_conv_fx/yz/ix  dipole convolution: R2C along x; per-kx 2D FFT over (y,z)
+//                    with the per-k tensor multiply fused; C2R along x.
+//   k_tensor_*       FP64 interaction-tensor setup and its FP64 FFT.
+//   k_netmoment_*    FP64 reductions.
+//
+// Reference semantics are cited per device function (paths relative to the
+// reference project, M/ = src/modules/).
+#include "device.cuh"
+#include "kparams.h"
+#include "launch.h"
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+
+// ------------------------------------------------------------ helpers
+__device__ __forceinline__ float ms_at(const SysK& s, int i) { return s.ms_uniform ? s.ms_u : __ldg(s.ms + i); }
+__device__ __forceinline__ float alpha_at(const SysK& s, int i) { return s.site_alpha ? __ldg(s.site_alpha + i) : s.alpha; }
+__device__ __forceinline__ float gamma_at(const SysK& s, int i) { return s.site_gamma ? __ldg(s.site_gamma + i) : s.gamma; }
+__device__ __forceinline__ float3 f3(float a, float b, float c) { return make_float3(a, b, c); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 scl3(float a, float3 b) { return f3(a * b.x, a * b.y, a * b.z); }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b)
+{
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 spin_at(const SysK& s, int i)
+{
+    return f3(__ldg(s.x + i), __ldg(s.y + i), __ldg(s.z + i));
+}
+
+// ------------------------------------------------------------ field terms
+// Exchange: h_t += J s_f / (m_f m_t) (normalised) or J s_f / m_f, only for
+// m_f != 0 (M/cpu/exchange/spinoperationexchange.cpp:134-213).
+__device__ __forceinline__ float3 ex_term(const ExchangeK& e, const SysK& s, int i, float mt)
+{
+    float3 h = f3(0.f, 0.f, 0.f);
+    if (e.mode == EX_STENCIL) {
+        const int ix = i % s.nx;
+        const int iy = (i / s.nx) % s.ny;
+        const int iz = i / (s.nx * s.ny);
+        const int nxy = s.nx * s.ny;
+#pragma unroll
+        for (int d = 0; d < 6; d++) {
+            const float J = e.J[d];
+            if (J == 0.f) continue;
+            const int ax = d >> 1;
+            const int sg = (d & 1) ? -1 : 1;
+            int c = ax == 0 ? ix : (ax == 1 ? iy : iz);
+            const int n = ax == 0 ? s.nx : (ax == 1 ? s.ny : s.nz);
+            c += sg;
+            if (c < 0 || c >= n) {
+                if (!e.pbc[ax]) continue;
+                c = c < 0 ? c + n : c - n;
+            }
+            const int f = ax == 0 ? (i - ix + c) : (ax == 1 ? (i + (c - iy) * s.nx) : (i + (c - iz) * nxy));
+            const float mf = ms_at(s, f);
+            if (mf != 0.f) {
+                const float3 sf = spin_at(s, f);
+                const float den = e.normalize ? mf * mt : mf;
+                h = add3(h, f3(sf.x * J / den, sf.y * J / den, sf.z * J / den));
+            }
+        }
+    } else if (e.mode == EX_CSR) {
+        const int p0 = __ldg(e.ptr + i), p1 = __ldg(e.ptr + i + 1);
+        for (int p = p0; p < p1; p++) {
+            const int f = __ldg(e.col + p);
+            const float J = __ldg(e.val + p);
+            const float mf = ms_at(s, f);
+            if (mf != 0.f) {
+                const float3 sf = spin_at(s, f);
+                const float den = e.normalize ? mf * mt : mf;
+                h = add3(h, f3(sf.x * J / den, sf.y * J / den, sf.z * J / den));
+            }
+        }
+    }
+    return h;
+}
+
+// Anisotropy: H = 2K (s.n)/ms^2 n for ms > 0
+// (M/cpu/anisotropy/spinoperationanisotropy.cpp:247-283).
+__device__ __forceinline__ float3 ani_one(float3 sp, float ms, const float* n, float K)
+{
+    const float sda = sp.x * n[0] + sp.y * n[1] + sp.z * n[2];
+    const float v = 2.0f * K * sda / (ms * ms);
+    return f3(n[0] * v, n[1] * v, n[2] * v);
+}
+__device__ __forceinline__ float3 ani_term(const AniK& a, float3 sp, float ms, int i)
+{
+    float3 h = f3(0.f, 0.f, 0.f);
+    if (!(ms > 0.f)) return h;
+    if (a.mode == ANI_UNIFORM) return ani_one(sp, ms, a.axis, a.K);
+    if (a.mode == ANI_CSR) {
+        const int p0 = __ldg(a.ptr + i), p1 = __ldg(a.ptr + i + 1);
+        for (int p = p0; p < p1; p++) {
+            const float n[3] = {__ldg(a.axes + 3 * p), __ldg(a.axes + 3 * p + 1), __ldg(a.axes + 3 * p + 2)};
+            h = add3(h, ani_one(sp, ms, n, __ldg(a.Ks + p)));
+        }
+    }
+    return h;
+}
+
+// Uniaxial: [2K1 u + 4K2 u^3] n with u = s.n of the unit spin; quirk keeps
+// the reference's sz*nx (..._uniaxial.cpp:250-298, :287).
+__device__ __forceinline__ float3 uni_one(float3 u3, const float* n, float K1, float K2, int quirk)
+{
+    const float u = u3.x * n[0] + u3.y * n[1] + u3.z * (quirk ? n[0] : n[2]);
+    const float mag = 2.0f * K1 * u + 4.0f * K2 * (u * u * u);
+    return f3(n[0] * mag, n[1] * mag, n[2] * mag);
+}
+__device__ __forceinline__ float3 uni_term(const UniK& a, float3 sp, float ms, int i)
+{
+    float3 h = f3(0.f, 0.f, 0.f);
+    if (!(ms > 0.f) || a.mode == ANI_NONE) return h;
+    const float3 u = f3(sp.x / ms, sp.y / ms, sp.z / ms);
+    if (a.mode == ANI_UNIFORM) return uni_one(u, a.axis, a.K1, a.K2, a.quirk);
+    const int p0 = __ldg(a.ptr + i), p1 = __ldg(a.ptr + i + 1);
+    for (int p = p0; p < p1; p++) {
+        const float n[3] = {__ldg(a.axes + 3 * p), __ldg(a.axes + 3 * p + 1), __ldg(a.axes + 3 * p + 2)};
+        h = add3(h, uni_one(u, n, __ldg(a.K12 + 2 * p), __ldg(a.K12 + 2 * p + 1), a.quirk));
+    }
+    return h;
+}
+
+// Cubic (..._cubic.cpp:308-390); quirk keeps (n2s2 + n3s3) in the first K1 term.
+__device__ __forceinline__ float3 cub_one(float3 s, const float* n, const float* K, int quirk)
+{
+    const float n1s = n[0] * s.x + n[1] * s.y + n[2] * s.z;
+    const float n2s = n[3] * s.x + n[4] * s.y + n[5] * s.z;
+    const float n3s = n[6] * s.x + n[7] * s.y + n[8] * s.z;
+    const float n1s2 = n1s * n1s, n2s2 = n2s * n2s, n3s2 = n3s * n3s;
+    const float n1s3 = n1s2 * n1s, n2s3 = n2s2 * n2s, n3s3 = n3s2 * n3s;
+    const float n1s4 = n1s2 * n1s2, n2s4 = n2s2 * n2s2, n3s4 = n3s2 * n3s2;
+    const float q = quirk ? n3s3 : n3s2;
+    const float a1 = 2.0f * K[0] * n1s * (n2s2 + q), a2 = 2.0f * K[0] * n2s * (n1s2 + n3s2), a3 = 2.0f * K[0] * n3s * (n1s2 + n2s2);
+    const float p = n1s * n2s * n3s;
+    const float b1 = 2.0f * K[1] * p * n2s * n3s, b2 = 2.0f * K[1] * p * n1s * n3s, b3 = 2.0f * K[1] * p * n1s * n2s;
+    const float c1 = 4.0f * K[2] * n1s3 * (n2s4 + n3s4), c2 = 4.0f * K[2] * n2s3 * (n1s4 + n3s4), c3 = 4.0f * K[2] * n3s3 * (n1s4 + n2s4);
+    float3 h;
+    h.x = (n[0] * a1 + n[3] * a2 + n[6] * a3) + (n[0] * b1 + n[3] * b2 + n[6] * b3) + (n[0] * c1 + n[3] * c2 + n[6] * c3);
+    h.y = (n[1] * a1 + n[4] * a2 + n[7] * a3) + (n[1] * b1 + n[4] * b2 + n[7] * b3) + (n[1] * c1 + n[4] * c2 + n[7] * c3);
+    h.z = (n[2] * a1 + n[5] * a2 + n[8] * a3) + (n[2] * b1 + n[5] * b2 + n[8] * b3) + (n[2] * c1 + n[5] * c2 + n[8] * c3);
+    return h;
+}
+__device__ __forceinline__ float3 cub_term(const CubK& a, float3 sp, float ms, int i)
+{
+    float3 h = f3(0.f, 0.f, 0.f);
+    if (!(ms > 0.f) || a.mode == ANI_NONE) return h;
+    const float3 u = f3(sp.x / ms, sp.y / ms, sp.z / ms);
+    if (a.mode == ANI_UNIFORM) return cub_one(u, a.axes, a.K, a.quirk);
+    const int p0 = __ldg(a.ptr + i), p1 = __ldg(a.ptr + i + 1);
+    for (int p = p0; p < p1; p++) {
+        float n[9], K[3];
+#pragma unroll
+        for (int q = 0; q < 9; q++) n[q] = __ldg(a.axs + 9 * p + q);
+#pragma unroll
+        for (int q = 0; q < 3; q++) K[q] = __ldg(a.Ks + 3 * p + q);
+        h = add3(h, cub_one(u, n, K, a.quirk));
+    }
+    return h;
+}
+
+// Thermal: sigma = sqrt(2 alpha T scale / (ms dt gamma)) times N(0,1) per
+// component, zero where ms == 0, T == 0 or gamma <= 0
+// (M/cpu/thermal/spinoperationthermal.cpp:135-191).
+__device__ __forceinline__ float3 th_term(const ThermalK& t, const SysK& s, float dt_sys, int i, float ms)
+{
+    float3 h = f3(0.f, 0.f, 0.f);
+    if (t.mode == TH_NONE || ms == 0.f || t.T == 0.f) return h;
+    const float a = alpha_at(s, i), g = gamma_at(s, i);
+    if (!(g > 0.f)) return h;
+    const float sc = t.scale ? __ldg(t.scale + i) : 1.0f;
+    const float sd = sqrtf((2.0f * a * t.T * sc) / (ms * dt_sys * g));
+    float3 n;
+    if (t.mode == TH_PHILOX) {
+        const uint64_t ctr = t.counter + (t.dctr ? *t.dctr : 0ull);
+        n = philox_normal3(t.seed, ctr, (uint32_t)i, 0x6d6c6232u);
+    } else {
+        n = f3(__ldg(t.nx + i), __ldg(t.ny + i), __ldg(t.nz + i));
+    }
+    return f3(sd * n.x, sd * n.y, sd * n.z);
+}
+
+struct Fields { float3 H; float3 Hth; };
+
+// Every term of TermsK at site i.  H is the would-be "Total" slot, Hth the
+// "Thermal" slot that LLG subtracts (llgcartesian.cpp:160-172).
+__device__ __forceinline__ Fields eval_terms(const TermsK& T, const SysK& s, float dt_sys, int i)
+{
+    const float ms = ms_at(s, i);
+    const float3 sp = spin_at(s, i);
+    float3 H = f3(0.f, 0.f, 0.f);
+    float3 Hth = f3(0.f, 0.f, 0.f);
+    if (T.ex.mode != EX_NONE) H = add3(H, scl3(T.ex_gs, ex_term(T.ex, s, i, ms)));
+    if (T.ani.mode != ANI_NONE) H = add3(H, ani_term(T.ani, sp, ms, i));
+    if (T.uni.mode != ANI_NONE) H = add3(H, uni_term(T.uni, sp, ms, i));
+    if (T.cub.mode != ANI_NONE) H = add3(H, cub_term(T.cub, sp, ms, i));
+    if (T.th.mode != TH_NONE) { Hth = th_term(T.th, s, dt_sys, i, ms); H = add3(H, Hth); }
+    if (T.zee.on) {
+        float3 B = f3(T.zee.B[0], T.zee.B[1], T.zee.B[2]);
+        if (T.zee.dctr) {
+            const float k = (float)(*T.zee.dctr);
+            B = f3(B.x + k * T.zee.dB[0], B.y + k * T.zee.dB[1], B.z + k * T.zee.dB[2]);
+        }
+        H = add3(H, B);
+    }
+    for (int a = 0; a < T.nadd; a++) {
+        const float3 v = f3(__ldg(T.add[a][0] + i), __ldg(T.add[a][1] + i), __ldg(T.add[a][2] + i));
+        const float w = T.addw[a];
+        H = add3(H, f3(w * v.x, w * v.y, w * v.z));
+        if (T.add_is_thermal[a]) Hth = add3(Hth, v);
+    }
+    Fields f;
+    f.H = H;
+    f.Hth = Hth;
+    return f;
+}
+
+// ------------------------------------------------------------ LLG
+// Cartesian Euler step (M/cpu/llg/llgcartesian.cpp:90-278) or quaternion
+// rotation (M/cpu/llg/llgquat.cpp:126-378) for one site with ms > 0.
+// S: from-spin, M: dmdt-spin, H: Total, Hth: Thermal.
+__device__ __forceinline__ float3 llg_site(const LlgK& L, float3 S, float3 M, float3 H, float3 Hth,
+                                           float ms, float a, float g)
+{
+    if (L.type == LLG_CART) {
+        if (L.dt_zero) return S;
+        const float gaa = g / (1.0f + a * a);
+        float3 MH, MMH;
+        if (L.thermal_only_first_term) {
+            const float3 h = sub3(H, Hth);
+            const float3 Mh = cross3(M, h);
+            MMH = cross3(M, Mh);
+            MH = cross3(M, H);
+            const float3 dM = sub3(scl3(L.precess * -gaa, MH), scl3(L.damp * (a / ms) * gaa, MMH));
+            return add3(S, scl3(L.dt, dM));
+        }
+        MH = cross3(M, H);
+        MMH = cross3(M, MH);
+        const float3 dM = sub3(scl3(-gaa, MH), scl3((a / ms) * gaa, MMH));
+        return add3(S, scl3(L.dt, dM));
+    }
+    // quaternion
+    const float inv = 1.0f / ms;
+    float3 Hp;
+    if (L.thermal_only_first_term) {
+        const float3 h = sub3(H, Hth);
+        const float3 Sh = cross3(M, h);
+        Hp = add3(scl3(L.precess, H), scl3(L.damp * a * inv, Sh));
+    } else {
+        const float3 SH = cross3(S, H);
+        Hp = add3(H, scl3(a * inv, SH));
+    }
+    const float HLen = sqrtf(Hp.x * Hp.x + Hp.y * Hp.y + Hp.z * Hp.z);
+    if (!(HLen > 0.f)) return S;
+    const float iHLen = 1.0f / HLen;
+    const float ra = 1.0f * g * HLen / (1.0f + a * a);
+    float sint, cost;
+    sincosf(0.5f * ra * L.dt, &sint, &cost);
+    // qRot = (cost, sint * Hp/|Hp|); qRes = qRot * (0,S) * conj(qRot)
+    const float qw = cost, qx = sint * Hp.x * iHLen, qy = sint * Hp.y * iHLen, qz = sint * Hp.z * iHLen;
+    // t = qRot * (0, S)
+    const float tw = -qx * S.x - qy * S.y - qz * S.z;
+    const float tx = qw * S.x + qy * S.z - qz * S.y;
+    const float ty = qw * S.y + qz * S.x - qx * S.z;
+    const float tz = qw * S.z + qx * S.y - qy * S.x;
+    // r = t * conj(qRot), conj = (qw, -qx, -qy, -qz)
+    const float cx = -qx, cy = -qy, cz = -qz;
+    float3 r;
+    r.x = tw * cx + qw * tx + ty * cz - tz * cy;
+    r.y = tw * cy + qw * ty + tz * cx - tx * cz;
+    r.z = tw * cz + qw * tz + tx * cy - ty * cx;
+    return r;
+}
+
+__device__ __forceinline__ float3 renorm(float3 v, float ms)
+{
+    const float mm = v.x * v.x + v.y * v.y + v.z * v.z;
+    if (mm != 0.f) {
+        const float inv = ms / sqrtf(mm);
+        return f3(v.x * inv, v.y * inv, v.z * inv);
+    }
+    return v;
+}
+
+// ------------------------------------------------------------ kernels
+__global__ void __launch_bounds__(256) k_fused_step(FusedK P, float dt_sys)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.sys.n) return;
+    const float ms = ms_at(P.sys, i);
+    const float3 S = spin_at(P.sys, i);
+    float3 out = S;
+    if (ms > 0.f) {
+        const Fields F = eval_terms(P.terms, P.sys, dt_sys, i);
+        out = llg_site(P.llg, S, S, F.H, F.Hth, ms, alpha_at(P.sys, i), gamma_at(P.sys, i));
+    }
+    if (P.llg.renorm) out = renorm(out, ms);
+    P.ox[i] = out.x;
+    P.oy[i] = out.y;
+    P.oz[i] = out.z;
+}
+
+// out = (accumulate ? out : 0) + terms
+__global__ void __launch_bounds__(256) k_eval_terms(SysK s, TermsK T, float dt_sys, float* hx, float* hy,
+                                                    float* hz, int accumulate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    const Fields F = eval_terms(T, s, dt_sys, i);
+    if (accumulate) { hx[i] += F.H.x; hy[i] += F.H.y; hz[i] += F.H.z; }
+    else { hx[i] = F.H.x; hy[i] = F.H.y; hz[i] = F.H.z; }
+}
+
+// Stand-alone LLG: from (spins+ms), dmdt spins M, Total H, optional Thermal.
+// Sites with ms <= 0 keep the destination's current value.
+__global__ void __launch_bounds__(256) k_llg(SysK from, const float* mx, const float* my, const float* mz,
+                                             const float* hx, const float* hy, const float* hz,
+                                             const float* tx, const float* ty, const float* tz,
+                                             const float* dsa, const float* dsg, float da, float dg,
+                                             LlgK L, float* ox, float* oy, float* oz)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= from.n) return;
+    const float ms = ms_at(from, i);
+    float3 out = f3(ox[i], oy[i], oz[i]);
+    if (L.type == LLG_CART && L.dt_zero) {
+        out = spin_at(from, i);
+    } else if (ms > 0.f) {
+        const float3 S = spin_at(from, i);
+        const float3 M = f3(mx[i], my[i], mz[i]);
+        const float3 H = f3(hx[i], hy[i], hz[i]);
+        const float3 Ht = tx ? f3(tx[i], ty[i], tz[i]) : f3(0.f, 0.f, 0.f);
+        const float a = dsa ? dsa[i] : da, g = dsg ? dsg[i] : dg;
+        out = llg_site(L, S, M, H, Ht, ms, a, g);
+    }
+    if (L.renorm) out = renorm(out, ms);
+    ox[i] = out.x; oy[i] = out.y; oz[i] = out.z;
+}
+
+__global__ void k_advance_counter(uint64_t* c) { *c += 1ull; }
+
+// FP64 partial sums for netMoment: per block (sum v*m, sum (v*m)^2) x 3.
+__global__ void __launch_bounds__(256) k_netmoment_partial(const float* x, const float* y, const float* z,
+                                                           int n, double m, double* part)
+{
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a = (double)x[i] * m, b = (double)y[i] * m, c = (double)z[i] * m;
+        acc[0] += a; acc[1] += b; acc[2] += c;
+        acc[3] += a * a; acc[4] += b * b; acc[5] += c * c;
+    }
+    __shared__ double sh[6][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[q][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) v += sh[threadIdx.x][k];
+        part[blockIdx.x * 6 + threadIdx.x] = v;
+    }
+}
+
+// out[q] = sum_b part[b*nq + q], fixed order (deterministic).
+__global__ void k_partial_final(const double* part, int nb, int nq, double* out)
+{
+    const int q = threadIdx.x;
+    if (q < nq) {
+        double v = 0;
+        for (int b = 0; b < nb; b++) v += part[b * nq + q];
+        out[q] = v;
+    }
+}
+
+// FP64 sum of s . h over sites (energy-style dot product).
+__global__ void __launch_bounds__(256) k_dot_partial(const float* x, const float* y, const float* z,
+                                                     const float* hx, const float* hy, const float* hz,
+                                                     int n, double* part)
+{
+    double acc = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc += (double)x[i] * hx[i] + (double)y[i] * hy[i] + (double)z[i] * hz[i];
+    __shared__ double sh[8];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) v += sh[k];
+        part[blockIdx.x] = v;
+    }
+}
+
+// ------------------------------------------------------------ dipole convolution
+// Forward x pass: rows (y0..y0+ty) of layer z, three components, zero-padded
+// to Px, complex FFT, first Kx bins written to SPEC[kx][c][z][y].
+__global__ void __launch_bounds__(256) k_conv_fx(ConvK c, FftLen Lx, const float2* tw, const float* sx,
+                                                 const float* sy, const float* sz, float2* spec)
+{
+    extern __shared__ float2 smf[];
+    const int y0 = blockIdx.x * c.ty, zz = blockIdx.y;
+    const int rows = min(c.ty, c.ny - y0);
+    float2* A = smf;
+    float2* B = smf + c.ty * c.Px;
+    LineGeo g;
+    g.nlines = rows; g.lpg = 1 << 30; g.gstride = 0; g.ls = c.Px; g.es = 1; g.line_fast = 0;
+    for (int comp = 0; comp < 3; comp++) {
+        const float* src = comp == 0 ? sx : (comp == 1 ? sy : sz);
+        for (int t = threadIdx.x; t < rows * c.Px; t += blockDim.x) {
+            const int r = t / c.Px, x = t % c.Px;
+            const float v = x < c.nx ? __ldg(src + ((size_t)zz * c.ny + y0 + r) * c.nx + x) : 0.f;
+            A[r * c.Px + x] = make_float2(v, 0.f);
+        }
+        __syncthreads();
+        const float2* R = c.Px > 1 ? cta_fft<float2>(A, B, g, Lx, tw, -1) : A;
+        for (int t = threadIdx.x; t < c.Kx * rows; t += blockDim.x) {
+            const int kx = t / rows, r = t % rows;
+            spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + y0 + r] = R[r * c.Px + kx];
+        }
+        __syncthreads();
+    }
+}
+
+// Per-kx (y,z) plane: forward FFT in y then z (zero padded), tensor
+// multiply, inverse z then y, write back the data rows.
+__global__ void __launch_bounds__(512) k_conv_yz(ConvK c, FftLen Ly, FftLen Lz, const float2* tw,
+                                                 float2* spec, const float* ten6, const float2* ten9)
+{
+    extern __shared__ float2 smf[];
+    const int kx = blockIdx.x;
+    const int PP = c.Py * c.Pz;
+    float2* A = smf;
+    float2* B = smf + 3 * PP;
+    for (int t = threadIdx.x; t < 6 * PP; t += blockDim.x) smf[t] = make_float2(0.f, 0.f);
+    __syncthreads();
+    float2* sp = spec + (size_t)kx * 3 * c.nz * c.ny;
+    const int NZY = c.nz * c.ny;
+    for (int t = threadIdx.x; t < 3 * NZY; t += blockDim.x) {
+        const int comp = t / NZY, rem = t % NZY, z = rem / c.ny, y = rem % c.ny;
+        A[comp * PP + z * c.Py + y] = sp[t];
+    }
+    __syncthreads();
+    LineGeo gy; gy.nlines = 3 * c.nz; gy.lpg = c.nz; gy.gstride = PP; gy.ls = c.Py; gy.es = 1; gy.line_fast = 0;
+    LineGeo gz; gz.nlines = 3 * c.Py; gz.lpg = c.Py; gz.gstride = PP; gz.ls = 1; gz.es = c.Py; gz.line_fast = 1;
+    float2* cur = A;
+    float2* oth = B;
+    if (c.Py > 1) { cur = cta_fft<float2>(cur, oth, gy, Ly, tw, -1); oth = cur == A ? B : A; }
+    if (c.Pz > 1) { cur = cta_fft<float2>(cur, oth, gz, Lz, tw, -1); oth = cur == A ? B : A; }
+    const float gg = c.g;
+    if (!c.general) {
+        const float* T = ten6 + (size_t)kx * PP * 6;
+        for (int t = threadIdx.x; t < PP; t += blockDim.x) {
+            const float t0 = __ldg(T + 6 * t), t1 = __ldg(T + 6 * t + 1), t2 = __ldg(T + 6 * t + 2);
+            const float t3 = __ldg(T + 6 * t + 3), t4 = __ldg(T + 6 * t + 4), t5 = __ldg(T + 6 * t + 5);
+            const float2 s0 = cur[t], s1 = cur[PP + t], s2 = cur[2 * PP + t];
+            cur[t] = make_float2(gg * (t0 * s0.x + t1 * s1.x + t2 * s2.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2.y));
+            cur[PP + t] = make_float2(gg * (t1 * s0.x + t3 * s1.x + t4 * s2.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2.y));
+            cur[2 * PP + t] = make_float2(gg * (t2 * s0.x + t4 * s1.x + t5 * s2.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2.y));
+        }
+    } else {
+        const float2* T = ten9 + (size_t)kx * PP * 9;
+        for (int t = threadIdx.x; t < PP; t += blockDim.x) {
+            const float2 s[3] = {cur[t], cur[PP + t], cur[2 * PP + t]};
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int b = 0; b < 3; b++) acc = cadd(acc, cmul(T[9 * t + 3 * a + b], s[b]));
+                cur[a * PP + t] = make_float2(gg * acc.x, gg * acc.y);
+            }
+        }
+    }
+    __syncthreads();
+    if (c.Pz > 1) { cur = cta_fft<float2>(cur, oth, gz, Lz, tw, +1); oth = cur == A ? B : A; }
+    if (c.Py > 1) { cur = cta_fft<float2>(cur, oth, gy, Ly, tw, +1); oth = cur == A ? B : A; }
+    for (int t = threadIdx.x; t < 3 * NZY; t += blockDim.x) {
+        const int comp = t / NZY, rem = t % NZY, z = rem / c.ny, y = rem % c.ny;
+        sp[t] = cur[comp * PP + z * c.Py + y];
+    }
+}
+
+// Inverse x pass: Hermitian completion, complex inverse FFT, real part of
+// the first nx points written to the field slot.
+__global__ void __launch_bounds__(256) k_conv_ix(ConvK c, FftLen Lx, const float2* tw, const float2* spec,
+                                                 float* hx, float* hy, float* hz)
+{
+    extern __shared__ float2 smf[];
+    const int y0 = blockIdx.x * c.ty, zz = blockIdx.y;
+    const int rows = min(c.ty, c.ny - y0);
+    float2* A = smf;
+    float2* B = smf + c.ty * c.Px;
+    LineGeo g;
+    g.nlines = rows; g.lpg = 1 << 30; g.gstride = 0; g.ls = c.Px; g.es = 1; g.line_fast = 0;
+    const int nh = c.Px - c.Kx;
+    for (int comp = 0; comp < 3; comp++) {
+        float* dst = comp == 0 ? hx : (comp == 1 ? hy : hz);
+        for (int t = threadIdx.x; t < c.Kx * rows; t += blockDim.x) {
+            const int kx = t / rows, r = t % rows;
+            A[r * c.Px + kx] = spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + y0 + r];
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < rows * nh; t += blockDim.x) {
+            const int r = t / nh, k = c.Kx + t % nh;
+            A[r * c.Px + k] = cconj(A[r * c.Px + c.Px - k]);
+        }
+        __syncthreads();
+        const float2* R = c.Px > 1 ? cta_fft<float2>(A, B, g, Lx, tw, +1) : A;
+        for (int t = threadIdx.x; t < rows * c.nx; t += blockDim.x) {
+            const int r = t / c.nx, x = t % c.nx;
+            dst[((size_t)zz * c.ny + y0 + r) * c.nx + x] = R[r * c.Px + x].x;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ FP64 tensor setup
+// Closed-form element, dipolesupport.cpp:32-70 (written without fused
+// multiply-adds so the sums match a plain C evaluation bit for bit).
+__device__ __forceinline__ void gamma_dip_d(double rx, double ry, double rz, double* g6)
+{
+    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+    const double r = __dsqrt_rn(r2);
+    if (r < 1E-40) { for (int q = 0; q < 6; q++) g6[q] = 0; return; }
+    const double ir = __ddiv_rn(1.0, r);
+    const double ir3 = __dmul_rn(__dmul_rn(ir, ir), ir);
+    const double ir5 = __dmul_rn(__dmul_rn(ir3, ir), ir);
+    g6[0] = -__dsub_rn(ir3, __dmul_rn(__dmul_rn(__dmul_rn(3.0, rx), rx), ir5));
+    g6[1] = -(-__dmul_rn(__dmul_rn(__dmul_rn(3.0, rx), ry), ir5));
+    g6[2] = -(-__dmul_rn(__dmul_rn(__dmul_rn(3.0, rx), rz), ir5));
+    g6[3] = -__dsub_rn(ir3, __dmul_rn(__dmul_rn(__dmul_rn(3.0, ry), ry), ir5));
+    g6[4] = -(-__dmul_rn(__dmul_rn(__dmul_rn(3.0, ry), rz), ir5));
+    g6[5] = -__dsub_rn(ir3, __dmul_rn(__dmul_rn(__dmul_rn(3.0, rz), rz), ir5));
+}
+
+__device__ __forceinline__ long long fdiv_floor(long long a, long long b)
+{
+    long long q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) q--;
+    return q;
+}
+
+// Periodic-in-plane lattice sum for element (i, j, k), getWAB/getWAB_range
+// (dipolesupport.cpp:71-240) with the image ranges narrowed to the ones that
+// pass the box tests (same terms, same order).  The z offset is written at
+// padded index (zsign*k mod Pz): zsign = -1 reproduces the reference's
+// source-minus-target layer convention (spinoperationlongrange.cpp:377-384),
+// +1 gives the physical target-minus-source one.
+__global__ void k_tensor_lattice(int nx, int ny, int nz, int G, int lim0, int limx, int limy,
+                                 double A0, double A1, double A2, double B0, double B1, double B2,
+                                 double C0, double C1, double C2, int Px, int Py, int Pz, int zsign,
+                                 double2* W)
+{
+    const long long ne = (long long)nx * ny * (2 * nz - 1);
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const int i = (int)(e % nx);
+    const int j = (int)((e / nx) % ny);
+    const int k = (int)(e / ((long long)nx * ny)) - (nz - 1);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const long long R = lim0;
+    if (llabs((long long)k) <= R) {
+        long long xlo = -(G - 1), xhi = G - 1, ylo = -(G - 1), yhi = G - 1;
+        long long a = -fdiv_floor((long long)limx + i, nx), b = fdiv_floor((long long)limx - i, nx);
+        if (a > xlo) xlo = a;
+        if (b < xhi) xhi = b;
+        a = -fdiv_floor((long long)limy + j, ny);
+        b = fdiv_floor((long long)limy - j, ny);
+        if (a > ylo) ylo = a;
+        if (b < yhi) yhi = b;
+        const double RR = __dmul_rn((double)R, (double)R);
+        for (long long X = xlo; X <= xhi; X++) {
+            const long long xx = X * nx + i;
+            for (long long Y = ylo; Y <= yhi; Y++) {
+                const long long yy = Y * ny + j;
+                const long long zz = k;
+                const double d2 = __dadd_rn(__dadd_rn(__dmul_rn((double)xx, (double)xx), __dmul_rn((double)yy, (double)yy)),
+                                            __dmul_rn((double)zz, (double)zz));
+                if (d2 <= RR) {
+                    const double fx = (double)xx, fy = (double)yy, fz = (double)zz;
+                    const double rx = __dadd_rn(__dadd_rn(__dmul_rn(fx, A0), __dmul_rn(fy, B0)), __dmul_rn(fz, C0));
+                    const double ry = __dadd_rn(__dadd_rn(__dmul_rn(fx, A1), __dmul_rn(fy, B1)), __dmul_rn(fz, C1));
+                    const double rz = __dadd_rn(__dadd_rn(__dmul_rn(fx, A2), __dmul_rn(fy, B2)), __dmul_rn(fz, C2));
+                    double g6[6];
+                    gamma_dip_d(rx, ry, rz, g6);
+#pragma unroll
+                    for (int q = 0; q < 6; q++) acc[q] = __dadd_rn(acc[q], g6[q]);
+                }
+            }
+        }
+    }
+    int zi = (zsign * k) % Pz;
+    if (zi < 0) zi += Pz;
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)zi * Py + j) * Px + i;
+    for (int q = 0; q < 6; q++) W[q * plane + off] = make_double2(acc[q], 0.0);
+}
+
+// Also stores the raw (unpadded) reference tensor for inspection:
+// out[q][k+nz-1][j][i] like the reference's XX..ZZ arrays.
+__global__ void k_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, int Pz, int zsign,
+                                     const double2* W, double* out)
+{
+    const long long ne = (long long)nx * ny * (2 * nz - 1);
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const int i = (int)(e % nx);
+    const int j = (int)((e / nx) % ny);
+    const int k = (int)(e / ((long long)nx * ny)) - (nz - 1);
+    int zi = (zsign * k) % Pz;
+    if (zi < 0) zi += Pz;
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)zi * Py + j) * Px + i;
+    for (int q = 0; q < 6; q++) out[q * ne + e] = W[q * plane + off].x;
+}
+
+// Open boundaries: Gamma(d) for |dx|<nx, |dy|<ny, |dz|<nz, no images,
+// placed at (d mod P).
+__global__ void k_tensor_open(int nx, int ny, int nz, double A0, double A1, double A2, double B0,
+                              double B1, double B2, double C0, double C1, double C2, int Px, int Py,
+                              int Pz, double2* W)
+{
+    const long long ex = 2 * nx - 1, ey = 2 * ny - 1, ez = 2 * nz - 1;
+    const long long ne = ex * ey * ez;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const int dx = (int)(e % ex) - (nx - 1);
+    const int dy = (int)((e / ex) % ey) - (ny - 1);
+    const int dz = (int)(e / (ex * ey)) - (nz - 1);
+    const double fx = dx, fy = dy, fz = dz;
+    const double rx = __dadd_rn(__dadd_rn(__dmul_rn(fx, A0), __dmul_rn(fy, B0)), __dmul_rn(fz, C0));
+    const double ry = __dadd_rn(__dadd_rn(__dmul_rn(fx, A1), __dmul_rn(fy, B1)), __dmul_rn(fz, C1));
+    const double rz = __dadd_rn(__dadd_rn(__dmul_rn(fx, A2), __dmul_rn(fy, B2)), __dmul_rn(fz, C2));
+    double g6[6];
+    gamma_dip_d(rx, ry, rz, g6);
+    const int xi = (dx % Px + Px) % Px, yi = (dy % Py + Py) % Py, zi = (dz % Pz + Pz) % Pz;
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)zi * Py + yi) * Px + xi;
+    for (int q = 0; q < 6; q++) W[q * plane + off] = make_double2(g6[q], 0.0);
+}
+
+// One FFT line per CTA of a complex FP64 (or FP32) volume; the line along
+// axis ax of component q.  Used for the one-off tensor transforms.
+template <typename C>
+__global__ void k_fft_lines(C* data, int Px, int Py, int Pz, int ax, FftLen L, const C* tw, int sign)
+{
+    extern __shared__ unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw);
+    C* B = A + L.n;
+    const long long line = blockIdx.x;
+    const int q = blockIdx.y;
+    long long base;
+    int es;
+    if (ax == 0) { base = line * Px; es = 1; }
+    else if (ax == 1) { const long long zz = line / Px, xx = line % Px; base = zz * Px * Py + xx; es = Px; }
+    else { base = line; es = Px * Py; }
+    C* d = data + (size_t)q * Px * Py * Pz + base;
+    for (int t = threadIdx.x; t < L.n; t += blockDim.x) A[t] = d[(size_t)t * es];
+    __syncthreads();
+    LineGeo g;
+    g.nlines = 1; g.lpg = 1; g.gstride = 0; g.ls = 0; g.es = 1; g.line_fast = 0;
+    const C* R = L.n > 1 ? cta_fft<C>(A, B, g, L, tw, sign) : A;
+    for (int t = threadIdx.x; t < L.n; t += blockDim.x) d[(size_t)t * es] = R[t];
+}
+
+// Real symmetric tensor: TEN6[kx][kz][ky][q] = Re W_q(kx,ky,kz) (float).
+__global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, float* ten6,
+                               double* maxim)
+{
+    const long long total = (long long)Kx * Py * Pz;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int kx = (int)(e / ((long long)Py * Pz));
+    const int rem = (int)(e % ((long long)Py * Pz));
+    const int kz = rem / Py, ky = rem % Py;
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)kz * Py + ky) * Px + kx;
+    double mi = 0;
+    for (int q = 0; q < 6; q++) {
+        const double2 v = W[q * plane + off];
+        ten6[(size_t)e * 6 + q] = (float)v.x;
+        mi = fmax(mi, fabs(v.y));
+    }
+    if (maxim) {
+        unsigned long long* p = reinterpret_cast<unsigned long long*>(maxim);
+        atomicMax(p, (unsigned long long)__double_as_longlong(mi));
+    }
+}
+
+// General 9-component complex tensor: TEN9[kx][kz][ky][q].
+__global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, float2* ten9)
+{
+    const long long total = (long long)Kx * Py * Pz;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int kx = (int)(e / ((long long)Py * Pz));
+    const int rem = (int)(e % ((long long)Py * Pz));
+    const int kz = rem / Py, ky = rem % Py;
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)kz * Py + ky) * Px + kx;
+    for (int q = 0; q < 9; q++) {
+        const double2 v = W[q * plane + off];
+        ten9[(size_t)e * 9 + q] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+// ------------------------------------------------------------ launchers
+#include <map>
+#include <string>
+#include <vector>
+
+namespace mlb {
+
+// Opt-in per-kernel timing: each launcher brackets its kernels with CUDA
+// events on the launching stream while profiling is on (never inside a
+// graph capture).  prof_collect() sums elapsed times per kernel name.
+namespace {
+struct ProfRec {
+    const char* name;
+    cudaEvent_t a, b;
+};
+bool g_prof = false;
+std::vector<ProfRec> g_recs;
+std::vector<cudaEvent_t> g_pool;
+cudaEvent_t ev_get()
+{
+    if (!g_pool.empty()) {
+        cudaEvent_t e = g_pool.back();
+        g_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+struct Prof {
+    bool on = false;
+    const char* name;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    Prof(const char* n, cudaStream_t s) : name(n), st(s)
+    {
+        if (!g_prof) return;
+        cudaStreamCaptureStatus cs;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+        on = true;
+        a = ev_get();
+        cudaEventRecord(a, st);
+    }
+    ~Prof()
+    {
+        if (!on) return;
+        cudaEvent_t b = ev_get();
+        cudaEventRecord(b, st);
+        g_recs.push_back({name, a, b});
+    }
+};
+} // namespace
+
+void prof_begin()
+{
+    g_prof = true;
+    g_recs.clear();
+}
+
+int prof_end(int cap, char* names, double* ms, int* launches)
+{
+    std::map<std::string, std::pair<double, int>> agg;
+    std::vector<std::string> order;
+    for (ProfRec& r : g_recs) {
+        cudaEventSynchronize(r.b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        if (!agg.count(r.name)) order.push_back(r.name);
+        agg[r.name].first += t;
+        agg[r.name].second += 1;
+        g_pool.push_back(r.a);
+        g_pool.push_back(r.b);
+    }
+    g_recs.clear();
+    g_prof = false;
+    int k = 0;
+    for (const std::string& nm : order) {
+        if (k >= cap) break;
+        snprintf(names + 48 * k, 48, "%s", nm.c_str());
+        ms[k] = agg[nm].first;
+        launches[k] = agg[nm].second;
+        k++;
+    }
+    return k;
+}
+
+static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+cudaError_t launch_fused(const FusedK& P, float dt_sys, cudaStream_t st)
+{
+    if (P.sys.n == 0) return cudaSuccess;
+    Prof pf("k_fused_step", st);
+    k_fused_step<<<blocks_for(P.sys.n, 256), 256, 0, st>>>(P, dt_sys);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval(const SysK& s, const TermsK& T, float dt_sys, float* h[3], int acc, cudaStream_t st)
+{
+    if (s.n == 0) return cudaSuccess;
+    Prof pf("k_eval_terms", st);
+    k_eval_terms<<<blocks_for(s.n, 256), 256, 0, st>>>(s, T, dt_sys, h[0], h[1], h[2], acc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_llg(const SysK& from, const float* m[3], const float* H[3], const float* Ht[3],
+                       const float* dsa, const float* dsg, float da, float dg, const LlgK& L,
+                       float* out[3], cudaStream_t st)
+{
+    if (from.n == 0) return cudaSuccess;
+    Prof pf("k_llg", st);
+    k_llg<<<blocks_for(from.n, 256), 256, 0, st>>>(from, m[0], m[1], m[2], H[0], H[1], H[2], Ht[0], Ht[1],
+                                                   Ht[2], dsa, dsg, da, dg, L, out[0], out[1], out[2]);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance(uint64_t* c, cudaStream_t st)
+{
+    k_advance_counter<<<1, 1, 0, st>>>(c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_netmoment(const float* x, const float* y, const float* z, int n, double m,
+                             double* part, int nb, double* out, cudaStream_t st)
+{
+    k_netmoment_partial<<<nb, 256, 0, st>>>(x, y, z, n, m, part);
+    k_partial_final<<<1, 32, 0, st>>>(part, nb, 6, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dot(const float* s[3], const float* h[3], int n, double* part, int nb, double* out,
+                       cudaStream_t st)
+{
+    k_dot_partial<<<nb, 256, 0, st>>>(s[0], s[1], s[2], h[0], h[1], h[2], n, part);
+    k_partial_final<<<1, 32, 0, st>>>(part, nb, 1, out);
+    return cudaGetLastError();
+}
+
+size_t conv_x_smem(const ConvK& c) { return (size_t)2 * c.ty * c.Px * sizeof(float2); }
+size_t conv_yz_smem(const ConvK& c) { return (size_t)6 * c.Py * c.Pz * sizeof(float2); }
+
+cudaError_t conv_configure()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_conv_yz, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_fx, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_conv_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_fft_lines<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return e;
+}
+
+cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz,
+                        const float2* tw, const float* s[3], float2* spec, const float* ten6,
+                        const float2* ten9, float* h[3], cudaStream_t st)
+{
+    dim3 gx(blocks_for(c.ny, c.ty), c.nz);
+    {
+        Prof pf("k_conv_fx", st);
+        k_conv_fx<<<gx, 256, conv_x_smem(c), st>>>(c, Lx, tw, s[0], s[1], s[2], spec);
+    }
+    {
+        Prof pf("k_conv_yz", st);
+        k_conv_yz<<<c.Kx, 512, conv_yz_smem(c), st>>>(c, Ly, Lz, tw, spec, ten6, ten9);
+    }
+    {
+        Prof pf("k_conv_ix", st);
+        k_conv_ix<<<gx, 256, conv_x_smem(c), st>>>(c, Lx, tw, spec, h[0], h[1], h[2]);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_lattice(int nx, int ny, int nz, const int gmax[4], const double ABC[9], int Px,
+                                  int Py, int Pz, int zsign, double2* W, cudaStream_t st)
+{
+    const long long ne = (long long)nx * ny * (2 * nz - 1);
+    const int lim0 = gmax[0];
+    const int limx = gmax[2] < gmax[0] ? gmax[2] : gmax[0];
+    const int limy = gmax[3] < gmax[0] ? gmax[3] : gmax[0];
+    k_tensor_lattice<<<blocks_for(ne, 128), 128, 0, st>>>(nx, ny, nz, gmax[0], lim0, limx, limy, ABC[0], ABC[1],
+                                                          ABC[2], ABC[3], ABC[4], ABC[5], ABC[6], ABC[7], ABC[8],
+                                                          Px, Py, Pz, zsign, W);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, int Pz, int zsign,
+                                      const double2* W, double* out, cudaStream_t st)
+{
+    const long long ne = (long long)nx * ny * (2 * nz - 1);
+    k_tensor_extract_ref<<<blocks_for(ne, 256), 256, 0, st>>>(nx, ny, nz, Px, Py, Pz, zsign, W, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int Px, int Py, int Pz,
+                               double2* W, cudaStream_t st)
+{
+    const long long ne = (long long)(2 * nx - 1) * (2 * ny - 1) * (2 * nz - 1);
+    k_tensor_open<<<blocks_for(ne, 256), 256, 0, st>>>(nx, ny, nz, ABC[0], ABC[1], ABC[2], ABC[3], ABC[4],
+                                                       ABC[5], ABC[6], ABC[7], ABC[8], Px, Py, Pz, W);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const FftLen L[3],
+                           const double2* tw, int sign, cudaStream_t st)
+{
+    const int P[3] = {Px, Py, Pz};
+    for (int ax = 0; ax < 3; ax++) {
+        if (P[ax] == 1) continue;
+        const long long nlines = (long long)Px * Py * Pz / P[ax];
+        dim3 g((unsigned)nlines, ncomp);
+        const size_t sm = (size_t)2 * P[ax] * sizeof(double2);
+        k_fft_lines<double2><<<g, 128, sm, st>>>(W, Px, Py, Pz, ax, L[ax], tw, sign);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, float* ten6, double* maxim,
+                                cudaStream_t st)
+{
+    const long long total = (long long)Kx * Py * Pz;
+    k_tensor_pack6<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten6, maxim);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, float2* ten9, cudaStream_t st)
+{
+    const long long total = (long long)Kx * Py * Pz;
+    k_tensor_pack9<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten9);
+    return cudaGetLastError();
+}
+
+} // namespace mlb

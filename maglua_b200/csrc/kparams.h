@@ -1,0 +1,113 @@
+// kparams.h -- plain-old-data launch parameters shared by the host layer
+// (capi.cu) and the kernels (kernels.cu).  Device pointers only; FP32 state,
+// FP64 where noted.
+#pragma once
+#include <stdint.h>
+
+#define MLB_MAX_ADDENDS 6
+
+// Exchange in one of two forms (see exchange compile in capi.cu):
+//   STENCIL: six lattice directions, J per direction, per-axis periodicity;
+//   CSR:     pathways grouped by target site (insertion order kept).
+enum { EX_NONE = 0, EX_STENCIL = 1, EX_CSR = 2 };
+// Anisotropy: uniform (same axis/constants on every site, one op per site)
+// or a per-site op list in CSR form.
+enum { ANI_NONE = 0, ANI_UNIFORM = 1, ANI_CSR = 2 };
+enum { TH_NONE = 0, TH_PHILOX = 1, TH_INJECT = 2 };
+enum { LLG_CART = 0, LLG_QUAT = 1 };
+
+struct ExchangeK {
+    int mode;
+    int normalize;
+    float J[6];            // (+x,-x,+y,-y,+z,-z): source offset from target, times global_scale
+    int pbc[3];
+    const int* ptr;        // CSR (n+1)
+    const int* col;        // source sites
+    const float* val;      // J * global_scale
+};
+
+// Generic Anisotropy (H = 2K (s.n)/ms^2 n)
+struct AniK {
+    int mode;
+    float axis[3]; float K;        // uniform (K already times global_scale)
+    const int* ptr; const float* axes; const float* Ks;   // CSR: axes 3/op, K 1/op
+};
+// Uniaxial (H = [2K1 u + 4K2 u^3] n, u from unit spin)
+struct UniK {
+    int mode; int quirk;
+    float axis[3]; float K1, K2;
+    const int* ptr; const float* axes; const float* K12;  // axes 3/op, K 2/op
+};
+// Cubic
+struct CubK {
+    int mode; int quirk;
+    float axes[9]; float K[3];
+    const int* ptr; const float* axs; const float* Ks;    // axes 9/op, K 3/op
+};
+struct ThermalK {
+    int mode;
+    float T;                  // temperature * global_scale
+    const float* scale;       // per-site scale or null
+    uint64_t seed;
+    uint64_t counter;         // host part of the Philox counter
+    const uint64_t* dctr;     // device step counter added to it (null = 0)
+    const float* nx; const float* ny; const float* nz;   // injected normals
+};
+struct ZeemanK {
+    int on;
+    float B[3];               // times global_scale
+    float dB[3];              // per-step sweep increment (uses *dctr)
+    const uint64_t* dctr;
+};
+
+struct SysK {
+    int nx, ny, nz, n;
+    const float* x; const float* y; const float* z;   // spins read
+    const float* ms; float ms_u; int ms_uniform;
+    const float* site_alpha; const float* site_gamma;
+    float alpha, gamma;
+};
+
+// Which terms a kernel evaluates, in slot order for the sum.
+struct TermsK {
+    ExchangeK ex; float ex_gs;   // (unused)
+    AniK ani;
+    UniK uni;
+    CubK cub;
+    ThermalK th;
+    ZeemanK zee;
+    int nadd;
+    const float* add[MLB_MAX_ADDENDS][3];   // materialised slot arrays added to Total
+    float addw[MLB_MAX_ADDENDS];
+    int add_is_thermal[MLB_MAX_ADDENDS];    // this addend is the Thermal slot
+};
+
+struct LlgK {
+    int type;
+    int thermal_only_first_term;
+    int renorm;
+    float precess, damp;
+    float dt;                 // scale * dmdt->dt
+    int dt_zero;
+};
+
+// One fused step: read spins (sys), evaluate terms, LLG, write spins (out).
+struct FusedK {
+    SysK sys;
+    TermsK terms;
+    LlgK llg;
+    float* ox; float* oy; float* oz;
+};
+
+// ------------------------------------------------------------- dipole
+// Convolution plan: padded grid P, data grid n, R2C along x (Kx = Px/2+1).
+// Spectrum layout SPEC[kx][c][z][y] (y fastest, data rows only).
+struct ConvK {
+    int nx, ny, nz;
+    int Px, Py, Pz;
+    int Kx;
+    int ty;                  // rows per CTA in the x passes
+    int general;             // 0: 6 real tensor entries per k, 1: 9 complex
+    float g;                 // strength * global_scale / (Px*Py*Pz)
+    int fx, fy, fz;          // FftLen indices
+};

@@ -1,0 +1,38 @@
+// launch.h -- host-callable launchers for the kernels in kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "device.cuh"
+#include "kparams.h"
+
+namespace mlb {
+void prof_begin();
+int prof_end(int cap, char* names, double* ms, int* launches);
+cudaError_t launch_fused(const FusedK& P, float dt_sys, cudaStream_t st);
+cudaError_t launch_eval(const SysK& s, const TermsK& T, float dt_sys, float* h[3], int acc, cudaStream_t st);
+cudaError_t launch_llg(const SysK& from, const float* m[3], const float* H[3], const float* Ht[3],
+                       const float* dsa, const float* dsg, float da, float dg, const LlgK& L,
+                       float* out[3], cudaStream_t st);
+cudaError_t launch_advance(uint64_t* c, cudaStream_t st);
+cudaError_t launch_netmoment(const float* x, const float* y, const float* z, int n, double m,
+                             double* part, int nb, double* out, cudaStream_t st);
+cudaError_t launch_dot(const float* s[3], const float* h[3], int n, double* part, int nb, double* out,
+                       cudaStream_t st);
+size_t conv_x_smem(const ConvK& c);
+size_t conv_yz_smem(const ConvK& c);
+cudaError_t conv_configure();
+cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz,
+                        const float2* tw, const float* s[3], float2* spec, const float* ten6,
+                        const float2* ten9, float* h[3], cudaStream_t st);
+cudaError_t launch_tensor_lattice(int nx, int ny, int nz, const int gmax[4], const double ABC[9], int Px,
+                                  int Py, int Pz, int zsign, double2* W, cudaStream_t st);
+cudaError_t launch_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, int Pz, int zsign,
+                                      const double2* W, double* out, cudaStream_t st);
+cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int Px, int Py, int Pz,
+                               double2* W, cudaStream_t st);
+cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const FftLen L[3],
+                           const double2* tw, int sign, cudaStream_t st);
+cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, float* ten6, double* maxim,
+                                cudaStream_t st);
+cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, float2* ten9, cudaStream_t st);
+} // namespace mlb

@@ -1,0 +1,447 @@
+"""ctypes wrapper around the FP64 oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker the CUDA path is compared against.
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
+this package; the product (maglua_b200) never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+
+MAX_SLOTS = 32
+SLOT_NAME = 32
+
+
+def build():
+    """Compile oracle.c into liboracle.so (gcc -O2, as the reference's CFLAGS)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+
+
+def _load():
+    src = os.path.join(_HERE, "oracle.c")
+    if (not os.path.exists(_LIB)) or os.path.getmtime(_LIB) < os.path.getmtime(src):
+        build()
+    return C.CDLL(_LIB)
+
+
+class _SS(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("n", C.c_int),
+        ("x", C.POINTER(C.c_double)), ("y", C.POINTER(C.c_double)),
+        ("z", C.POINTER(C.c_double)), ("ms", C.POINTER(C.c_double)),
+        ("alpha", C.c_double), ("gamma", C.c_double), ("dt", C.c_double), ("time", C.c_double),
+        ("site_alpha", C.POINTER(C.c_double)), ("site_gamma", C.POINTER(C.c_double)),
+        ("nslots", C.c_int),
+        ("names", (C.c_char * SLOT_NAME) * MAX_SLOTS),
+        ("hx", C.POINTER(C.c_double) * MAX_SLOTS),
+        ("hy", C.POINTER(C.c_double) * MAX_SLOTS),
+        ("hz", C.POINTER(C.c_double) * MAX_SLOTS),
+        ("used", C.c_int * MAX_SLOTS),
+    ]
+
+
+class _MT(C.Structure):
+    _fields_ = [("state", C.c_ulonglong * 624), ("pnext", C.c_int), ("left", C.c_int)]
+
+
+class _LLG(C.Structure):
+    _fields_ = [("thermal_only_first_term", C.c_int), ("disable_renormalization", C.c_int),
+                ("precess_scale", C.c_double), ("damp_scale", C.c_double)]
+
+
+class _StepCfg(C.Structure):
+    _fields_ = [
+        ("npath", C.c_int), ("from_", C.POINTER(C.c_int)), ("to", C.POINTER(C.c_int)),
+        ("J", C.POINTER(C.c_double)), ("ex_normalize", C.c_int),
+        ("nani", C.c_int), ("ani_site", C.POINTER(C.c_int)), ("ani_axis", C.POINTER(C.c_double)),
+        ("ani_K", C.POINTER(C.c_double)),
+        ("ncub", C.c_int), ("cub_site", C.POINTER(C.c_int)), ("cub_axes", C.POINTER(C.c_double)),
+        ("cub_K", C.POINTER(C.c_double)), ("cub_quirk", C.c_int),
+        ("T", C.c_double), ("rng", C.POINTER(_MT)),
+        ("zeeman", C.c_int), ("B", C.c_double * 3),
+        ("dipole", C.c_int), ("lr", C.c_void_p), ("g", C.c_double),
+        ("llg_type", C.c_int), ("llg", _LLG),
+    ]
+
+
+lib = _load()
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_PSS = C.POINTER(_SS)
+
+lib.orc_ss_new.restype = _PSS
+lib.orc_ss_new.argtypes = [C.c_int, C.c_int, C.c_int]
+lib.orc_ss_free.argtypes = [_PSS]
+lib.orc_ss_copy.argtypes = [_PSS, _PSS]
+lib.orc_ss_slot.argtypes = [_PSS, C.c_char_p]
+lib.orc_ss_find_slot.argtypes = [_PSS, C.c_char_p]
+lib.orc_ss_field.restype = _D
+lib.orc_ss_field.argtypes = [_PSS, C.c_char_p, C.c_int]
+lib.orc_ss_set_spin.argtypes = [_PSS, C.c_int, C.c_double, C.c_double, C.c_double]
+lib.orc_ss_set_site_alpha.argtypes = [_PSS, _D]
+lib.orc_ss_set_site_gamma.argtypes = [_PSS, _D]
+lib.orc_ss_reset_fields.argtypes = [_PSS]
+lib.orc_ss_sum_fields.argtypes = [_PSS]
+lib.orc_ss_sum_fields_weighted.argtypes = [_PSS, C.c_char_p, C.c_int, C.POINTER(C.c_char_p), _D]
+lib.orc_ss_netmoment.argtypes = [_PSS, C.c_double, _D]
+lib.orc_mt_seed.argtypes = [C.POINTER(_MT), C.c_ulonglong]
+lib.orc_mt_seed_array.argtypes = [C.POINTER(_MT), C.POINTER(C.c_ulonglong), C.c_int]
+lib.orc_mt_randint.restype = C.c_ulonglong
+lib.orc_mt_randint.argtypes = [C.POINTER(_MT)]
+lib.orc_mt_rand.restype = C.c_double
+lib.orc_mt_rand.argtypes = [C.POINTER(_MT)]
+lib.orc_mt_randnorm.restype = C.c_double
+lib.orc_mt_randnorm.argtypes = [C.POINTER(_MT), C.c_double, C.c_double]
+lib.orc_exchange_apply.argtypes = [_PSS, _I, _I, _D, C.c_int, C.c_int, C.c_double]
+lib.orc_anisotropy_apply.argtypes = [_PSS, _I, _D, _D, C.c_int, C.c_double]
+lib.orc_anisotropy_uniaxial_apply.argtypes = [_PSS, _I, _D, _D, _D, C.c_int, C.c_double, C.c_int]
+lib.orc_anisotropy_cubic_apply.argtypes = [_PSS, _I, _D, _D, C.c_int, C.c_double, C.c_int]
+lib.orc_cubic_axes.argtypes = [_D, _D, _D]
+lib.orc_uniaxial_axis.argtypes = [_D, _D]
+lib.orc_thermal_apply.argtypes = [_PSS, C.c_double, _D, C.c_double, C.POINTER(_MT)]
+lib.orc_thermal_apply_noise.argtypes = [_PSS, C.c_double, _D, C.c_double, _D, _D, _D]
+lib.orc_thermal_draw.argtypes = [_PSS, C.c_double, C.POINTER(_MT), _D, _D, _D]
+lib.orc_zeeman_apply.argtypes = [_PSS, _D, C.c_double]
+lib.orc_dipole_tensor.argtypes = [C.c_int, C.c_int, C.c_int, _I, _D, _D, _D, _D, _D, _D, _D]
+lib.orc_longrange_apply.argtypes = [_PSS, C.c_char_p, _D * 6, C.c_double, C.c_double]
+lib.orc_lr_new.restype = C.c_void_p
+lib.orc_lr_new.argtypes = [C.c_int, C.c_int, C.c_int, _D * 6]
+lib.orc_lr_apply.argtypes = [C.c_void_p, _PSS, C.c_char_p, C.c_double, C.c_double]
+lib.orc_lr_free.argtypes = [C.c_void_p]
+lib.orc_longrange3d_apply.argtypes = [_PSS, _D * 9, C.c_double, C.c_double]
+lib.orc_dipole_direct.argtypes = [_PSS, _D, C.c_double, C.c_int, C.c_int, C.c_int, _D, _D, _D]
+lib.orc_llg_default.argtypes = [C.POINTER(_LLG)]
+lib.orc_llg_cart_apply.argtypes = [C.POINTER(_LLG), _PSS, C.c_double, _PSS, _PSS, C.c_int]
+lib.orc_llg_quat_apply.argtypes = [C.POINTER(_LLG), _PSS, C.c_double, _PSS, _PSS, C.c_int]
+lib.orc_fft1d.argtypes = [_D, C.c_int, C.c_int, C.c_int]
+lib.orc_fft2d_layers.argtypes = [_D, C.c_int, C.c_int, C.c_int, C.c_int]
+lib.orc_fft3d.argtypes = [_D, C.c_int, C.c_int, C.c_int, C.c_int]
+lib.orc_run_steps.argtypes = [_PSS, C.POINTER(_StepCfg), C.c_int]
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_I)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class MT:
+    """Random.MersenneTwister restatement."""
+
+    def __init__(self, seed=None, key=None):
+        self.s = _MT()
+        if key is not None:
+            k = (C.c_ulonglong * len(key))(*key)
+            lib.orc_mt_seed_array(C.byref(self.s), k, len(key))
+        else:
+            lib.orc_mt_seed(C.byref(self.s), seed)
+
+    def randint(self):
+        return lib.orc_mt_randint(C.byref(self.s))
+
+    def rand(self):
+        return lib.orc_mt_rand(C.byref(self.s))
+
+    def normal(self):
+        return lib.orc_mt_randnorm(C.byref(self.s), 0.0, 1.0)
+
+    def ptr(self):
+        return C.pointer(self.s)
+
+
+class LLG:
+    def __init__(self, kind="Cartesian", **kw):
+        self.kind = kind
+        self.s = _LLG()
+        lib.orc_llg_default(C.byref(self.s))
+        for k, v in kw.items():
+            setattr(self.s, k, v)
+
+    def apply(self, frm, scale=1.0, dmdt=None, to=None, advance=True):
+        dmdt = dmdt or frm
+        to = to or frm
+        f = lib.orc_llg_cart_apply if self.kind == "Cartesian" else lib.orc_llg_quat_apply
+        f(C.byref(self.s), frm.p, scale, dmdt.p, to.p, int(bool(advance)))
+
+
+class SpinSystem:
+    """FP64 SpinSystem with numpy views of its arrays."""
+
+    def __init__(self, nx, ny=1, nz=1):
+        self.p = lib.orc_ss_new(nx, ny, nz)
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.n = nx * ny * nz
+        s = self.p.contents
+        self.x = np.ctypeslib.as_array(s.x, shape=(self.n,))
+        self.y = np.ctypeslib.as_array(s.y, shape=(self.n,))
+        self.z = np.ctypeslib.as_array(s.z, shape=(self.n,))
+        self.ms = np.ctypeslib.as_array(s.ms, shape=(self.n,))
+
+    def __del__(self):
+        try:
+            lib.orc_ss_free(self.p)
+        except Exception:
+            pass
+
+    def __getattr__(self, k):
+        if k in ("alpha", "gamma", "dt", "time"):
+            return getattr(self.p.contents, k)
+        raise AttributeError(k)
+
+    def __setattr__(self, k, v):
+        if k in ("alpha", "gamma", "dt", "time"):
+            setattr(self.p.contents, k, float(v))
+        else:
+            object.__setattr__(self, k, v)
+
+    def set_spins(self, x, y, z):
+        """SpinSystem::set(i, sx, sy, sz) for every site (ms = |s|)."""
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        self.x[:] = x
+        self.y[:] = y
+        self.z[:] = z
+        self.ms[:] = np.sqrt(x * x + y * y + z * z)
+
+    def spins(self):
+        return np.stack([self.x.copy(), self.y.copy(), self.z.copy()])
+
+    def field(self, name):
+        ptrs = [lib.orc_ss_field(self.p, name.encode(), c) for c in range(3)]
+        return np.stack([np.ctypeslib.as_array(q, shape=(self.n,)).copy() for q in ptrs])
+
+    def field_views(self, name):
+        ptrs = [lib.orc_ss_field(self.p, name.encode(), c) for c in range(3)]
+        return [np.ctypeslib.as_array(q, shape=(self.n,)) for q in ptrs]
+
+    def slot_used(self, name):
+        s = lib.orc_ss_find_slot(self.p, name.encode())
+        return s >= 0 and bool(self.p.contents.used[s])
+
+    def set_slot_used(self, name, used=True):
+        s = lib.orc_ss_slot(self.p, name.encode())
+        self.p.contents.used[s] = int(bool(used))
+
+    def set_site_alpha(self, a):
+        self._sa = None if a is None else _f64(a)
+        lib.orc_ss_set_site_alpha(self.p, None if a is None else _dp(self._sa))
+
+    def set_site_gamma(self, g):
+        self._sg = None if g is None else _f64(g)
+        lib.orc_ss_set_site_gamma(self.p, None if g is None else _dp(self._sg))
+
+    def reset_fields(self):
+        lib.orc_ss_reset_fields(self.p)
+
+    def sum_fields(self):
+        lib.orc_ss_sum_fields(self.p)
+
+    def sum_fields_weighted(self, dest, names, weights):
+        arr = (C.c_char_p * len(names))(*[n.encode() for n in names])
+        w = _f64(weights)
+        lib.orc_ss_sum_fields_weighted(self.p, dest.encode(), len(names), arr, _dp(w))
+
+    def netmoment(self, m=1.0):
+        out = np.zeros(8)
+        lib.orc_ss_netmoment(self.p, m, _dp(out))
+        return out
+
+    def copy_from(self, other):
+        lib.orc_ss_copy(self.p, other.p)
+
+
+# ---------------------------------------------------------------- operators
+def exchange_apply(ss, frm, to, J, normalize=True, gscale=1.0):
+    f, t, j = _i32(frm), _i32(to), _f64(J)
+    lib.orc_exchange_apply(ss.p, _ip(f), _ip(t), _dp(j), len(f), int(normalize), gscale)
+
+
+def anisotropy_apply(ss, site, axis, K, gscale=1.0):
+    s, a, k = _i32(site), _f64(axis).reshape(-1), _f64(K)
+    lib.orc_anisotropy_apply(ss.p, _ip(s), _dp(a), _dp(k), len(s), gscale)
+
+
+def anisotropy_uniaxial_apply(ss, site, axis, K1, K2, gscale=1.0, quirk=True):
+    s, a, k1, k2 = _i32(site), _f64(axis).reshape(-1), _f64(K1), _f64(K2)
+    lib.orc_anisotropy_uniaxial_apply(ss.p, _ip(s), _dp(a), _dp(k1), _dp(k2), len(s), gscale, int(quirk))
+
+
+def anisotropy_cubic_apply(ss, site, axes, K, gscale=1.0, quirk=True):
+    s, a, k = _i32(site), _f64(axes).reshape(-1), _f64(K).reshape(-1)
+    lib.orc_anisotropy_cubic_apply(ss.p, _ip(s), _dp(a), _dp(k), len(s), gscale, int(quirk))
+
+
+def cubic_axes(a1, a2):
+    a, b, out = _f64(a1), _f64(a2), np.zeros(9)
+    rc = lib.orc_cubic_axes(_dp(a), _dp(b), _dp(out))
+    return rc, out
+
+
+def uniaxial_axis(a):
+    a, out = _f64(a), np.zeros(3)
+    lib.orc_uniaxial_axis(_dp(a), _dp(out))
+    return out
+
+
+def thermal_apply(ss, T, rng, scale=None, gscale=1.0):
+    sc = None if scale is None else _f64(scale)
+    return lib.orc_thermal_apply(ss.p, T, None if sc is None else _dp(sc), gscale, rng.ptr())
+
+
+def thermal_draw(ss, T, rng):
+    nx, ny, nz = np.zeros(ss.n), np.zeros(ss.n), np.zeros(ss.n)
+    lib.orc_thermal_draw(ss.p, T, rng.ptr(), _dp(nx), _dp(ny), _dp(nz))
+    return nx, ny, nz
+
+
+def thermal_apply_noise(ss, T, noise, scale=None, gscale=1.0):
+    nx, ny, nz = (_f64(a) for a in noise)
+    sc = None if scale is None else _f64(scale)
+    lib.orc_thermal_apply_noise(ss.p, T, None if sc is None else _dp(sc), gscale,
+                                _dp(nx), _dp(ny), _dp(nz))
+
+
+def zeeman_apply(ss, B, gscale=1.0):
+    b = _f64(B)
+    lib.orc_zeeman_apply(ss.p, _dp(b), gscale)
+
+
+def dipole_tensor(nx, ny, nz, gmax=(1000, 1000, 1000, 1000), ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
+    """Six arrays of shape (2nz-1, ny, nx): XX, XY, XZ, YY, YZ, ZZ."""
+    g = _i32(gmax)
+    abc = _f64(ABC)
+    n = nx * ny * (2 * nz - 1)
+    arrs = [np.zeros(n) for _ in range(6)]
+    lib.orc_dipole_tensor(nx, ny, nz, _ip(g), _dp(abc), *[_dp(a) for a in arrs])
+    return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
+
+
+class LongRange:
+    """LongRange/Dipole with cached tensor transforms."""
+
+    def __init__(self, nx, ny, nz, T6):
+        self.T6 = [_f64(t).reshape(-1) for t in T6]
+        arr = (_D * 6)(*[_dp(t) for t in self.T6])
+        self.c = lib.orc_lr_new(nx, ny, nz, arr)
+
+    def apply(self, ss, g, slot="Dipole", gscale=1.0):
+        lib.orc_lr_apply(self.c, ss.p, slot.encode(), g, gscale)
+
+    def __del__(self):
+        try:
+            lib.orc_lr_free(self.c)
+        except Exception:
+            pass
+
+
+def longrange3d_apply(ss, T9, g, gscale=1.0):
+    T9 = [_f64(t).reshape(-1) for t in T9]
+    arr = (_D * 9)(*[_dp(t) for t in T9])
+    lib.orc_longrange3d_apply(ss.p, arr, g, gscale)
+
+
+def dipole_direct(ss, g, periodic=(0, 0, 0), ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
+    abc = _f64(ABC)
+    hx, hy, hz = np.zeros(ss.n), np.zeros(ss.n), np.zeros(ss.n)
+    lib.orc_dipole_direct(ss.p, _dp(abc), g, *[int(p) for p in periodic], _dp(hx), _dp(hy), _dp(hz))
+    return np.stack([hx, hy, hz])
+
+
+def fft1d(data, sign):
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128)).copy()
+    lib.orc_fft1d(d.view(np.float64).ctypes.data_as(_D), len(d), 1, sign)
+    return d
+
+
+def fft3d(data, sign):
+    """data shaped (nz, ny, nx) complex."""
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128)).copy()
+    nz, ny, nx = d.shape
+    lib.orc_fft3d(d.view(np.float64).ctypes.data_as(_D), nx, ny, nz, sign)
+    return d
+
+
+def fft2d_layers(data, sign):
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128)).copy()
+    nz, ny, nx = d.shape
+    lib.orc_fft2d_layers(d.view(np.float64).ctypes.data_as(_D), nx, ny, nz, sign)
+    return d
+
+
+def run_steps(ss, nsteps, *, paths=None, ex_normalize=True, ani=None, cubic=None,
+              cubic_quirk=True, T=0.0, rng=None, B=None, lr=None, g=0.0,
+              llg="Cartesian", llg_kw=None):
+    """Canonical step loop in C (used for CPU timing)."""
+    c = _StepCfg()
+    keep = []
+    if paths is not None:
+        f, t, j = _i32(paths[0]), _i32(paths[1]), _f64(paths[2])
+        keep += [f, t, j]
+        c.npath, c.from_, c.to, c.J = len(f), _ip(f), _ip(t), _dp(j)
+        c.ex_normalize = int(ex_normalize)
+    if ani is not None:
+        s, a, k = _i32(ani[0]), _f64(ani[1]).reshape(-1), _f64(ani[2])
+        keep += [s, a, k]
+        c.nani, c.ani_site, c.ani_axis, c.ani_K = len(s), _ip(s), _dp(a), _dp(k)
+    if cubic is not None:
+        s, a, k = _i32(cubic[0]), _f64(cubic[1]).reshape(-1), _f64(cubic[2]).reshape(-1)
+        keep += [s, a, k]
+        c.ncub, c.cub_site, c.cub_axes, c.cub_K = len(s), _ip(s), _dp(a), _dp(k)
+        c.cub_quirk = int(cubic_quirk)
+    if T and rng is not None:
+        c.T = T
+        c.rng = rng.ptr()
+    if B is not None:
+        c.zeeman = 1
+        for i in range(3):
+            c.B[i] = B[i]
+    if lr is not None:
+        c.dipole = 1
+        c.lr = lr.c
+        c.g = g
+    c.llg_type = 0 if llg == "Cartesian" else 1
+    lib.orc_llg_default(C.byref(c.llg))
+    for k, v in (llg_kw or {}).items():
+        setattr(c.llg, k, v)
+    lib.orc_run_steps(ss.p, C.byref(c), nsteps)
+
+
+def nn_paths(nx, ny, nz, J=1.0, pbc=(1, 1, 1), dirs=6):
+    """Pathways the canonical Lua setup loop adds with ex:add({i,j,k},{i±1,..},J):
+    from = neighbour, to = site, periodic wrap per pbc, open edges dropped
+    (spinoperationexchange.cpp:368-420)."""
+    frm, to, Js = [], [], []
+    offs = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)][:dirs]
+    dims = (nx, ny, nz)
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                for o in offs:
+                    a = [i, j, k]
+                    b = [i + o[0], j + o[1], k + o[2]]
+                    ok = True
+                    for d in range(3):
+                        if pbc[d]:
+                            a[d] %= dims[d]
+                            b[d] %= dims[d]
+                        if not (0 <= b[d] < dims[d]):
+                            ok = False
+                    if ok:
+                        frm.append(a[0] + nx * (a[1] + ny * a[2]))
+                        to.append(b[0] + nx * (b[1] + ny * b[2]))
+                        Js.append(J)
+    return np.array(frm, np.int32), np.array(to, np.int32), np.array(Js)

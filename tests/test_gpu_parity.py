@@ -1,0 +1,478 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle on
+the same seeded inputs.
+
+Tolerances (FP32 state on the device, FP64 oracle):
+  * per-term fields: relative error ||h_gpu - h_oracle|| / ||h_oracle|| <= 1e-5;
+  * T = 0 trajectories: max |dm| <= 1e-4 after 1000 steps;
+  * injected thermal noise: the same bound as the fields.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import Pair, random_spins, rel_err, tilted_spins
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-5
+TRAJ_TOL = 1e-4
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.json")
+
+
+@pytest.fixture(scope="module")
+def M():
+    import maglua_b200 as M
+    M.init(0)
+    return M
+
+
+def _fields_compare(p, names):
+    p.o.reset_fields()
+    for f in p.oapply:
+        f(p.o)
+    p.o.sum_fields()
+    p.g.resetFields()
+    for op in p.ops:
+        op.apply(p.g)
+    p.g.sumFields()
+    errs = {}
+    for name in names:
+        errs[name] = rel_err(np.stack(p.g.fieldArrays(name)), p.o.field(name))
+    return errs
+
+
+# ---------------------------------------------------------------- per-term fields
+@pytest.mark.parametrize("dims,pbc", [((8, 7, 5), (1, 1, 1)), ((6, 5, 4), (1, 0, 0)), ((16, 16, 1), (1, 1, 1)),
+                                      ((2, 3, 4), (1, 1, 1)), ((1, 1, 1), (1, 1, 1))])
+def test_exchange_field(M, dims, pbc):
+    n = int(np.prod(dims))
+    p = Pair(*dims, random_spins(n, 1, lengths=True))
+    p.exchange(J=1.0, pbc=pbc)
+    e = _fields_compare(p, ["Exchange", "Total"])
+    assert e["Exchange"] <= FIELD_TOL and e["Total"] <= FIELD_TOL, e
+
+
+def test_exchange_irregular_pathways_and_normalisation(M):
+    nx, ny, nz = 7, 6, 3
+    n = nx * ny * nz
+    r = np.random.default_rng(3)
+    f = r.integers(0, n, 5 * n).astype(np.int32)
+    t = r.integers(0, n, 5 * n).astype(np.int32)
+    j = r.normal(size=5 * n)
+    for norm in (True, False):
+        p = Pair(nx, ny, nz, random_spins(n, 2, lengths=True))
+        p.exchange(paths=(f, t, j), normalize=norm)
+        e = _fields_compare(p, ["Exchange"])
+        assert e["Exchange"] <= FIELD_TOL, (norm, e)
+
+
+def test_exchange_accumulates_without_reset(M):
+    nx, ny, nz = 5, 4, 3
+    n = nx * ny * nz
+    p = Pair(nx, ny, nz, random_spins(n, 4))
+    p.exchange()
+    # two applies without resetFields add twice (spinoperationexchange.cpp:134-213)
+    p.o.reset_fields()
+    p.g.resetFields()
+    for _ in range(2):
+        p.oapply[0](p.o)
+        p.ops[0].apply(p.g)
+    assert rel_err(np.stack(p.g.fieldArrays("Exchange")), p.o.field("Exchange")) <= FIELD_TOL
+
+
+@pytest.mark.parametrize("axis", [(0, 0, 1), (1, 1, 0), (0.3, -0.2, 0.9)])
+def test_anisotropy_field(M, axis):
+    dims = (9, 5, 3)
+    n = int(np.prod(dims))
+    p = Pair(*dims, random_spins(n, 5, lengths=True))
+    p.anisotropy(axis=axis, K=0.37)
+    e = _fields_compare(p, ["Anisotropy"])
+    assert e["Anisotropy"] <= FIELD_TOL, e
+
+
+def test_anisotropy_per_site_lists(M):
+    dims = (6, 6, 2)
+    n = int(np.prod(dims))
+    r = np.random.default_rng(8)
+    s = random_spins(n, 6, lengths=True)
+    p = Pair(*dims, s)
+    ani = p.M.Anisotropy(*dims)
+    sites = np.concatenate([np.arange(n), r.integers(0, n, n // 2)]).astype(np.int32)
+    axes = r.normal(size=(len(sites), 3))
+    axes /= np.linalg.norm(axes, axis=1)[:, None]
+    K = r.normal(size=len(sites))
+    ani.addMany(sites, axes, K)
+    p.ops.append(ani)
+    p.oapply.append(lambda ss: O.anisotropy_apply(ss, sites, axes, K))
+    e = _fields_compare(p, ["Anisotropy"])
+    assert e["Anisotropy"] <= FIELD_TOL
+
+
+@pytest.mark.parametrize("quirk", [True, False])
+def test_uniaxial_field(M, quirk):
+    dims = (5, 4, 3)
+    n = int(np.prod(dims))
+    s = random_spins(n, 7, lengths=True)
+    p = Pair(*dims, s)
+    uni = p.M.AnisotropyUniaxial(*dims)
+    uni.setQuirks(quirk)
+    sites = np.arange(n, dtype=np.int32)
+    ax = np.tile([0.6, 0.0, 0.8], (n, 1))
+    K1, K2 = np.full(n, 0.3), np.full(n, 0.05)
+    uni.addMany(sites, ax, K1, K2)
+    AX = np.tile(O.uniaxial_axis([0.6, 0.0, 0.8]), (n, 1))
+    p.ops.append(uni)
+    p.oapply.append(lambda ss: O.anisotropy_uniaxial_apply(ss, sites, AX, K1, K2, quirk=quirk))
+    e = _fields_compare(p, ["UniaxialAnisotropy"])
+    assert e["UniaxialAnisotropy"] <= FIELD_TOL, e
+
+
+@pytest.mark.parametrize("quirk", [True, False])
+def test_cubic_field(M, quirk):
+    dims = (5, 4, 3)
+    n = int(np.prod(dims))
+    p = Pair(*dims, random_spins(n, 9, lengths=True))
+    p.cubic(K=(0.05, 0.02, 0.01), quirk=quirk)
+    e = _fields_compare(p, ["CubicAnisotropy"])
+    assert e["CubicAnisotropy"] <= FIELD_TOL, e
+
+
+def test_zeeman_and_sum(M):
+    dims = (4, 4, 4)
+    n = 64
+    p = Pair(*dims, random_spins(n, 10))
+    p.exchange()
+    p.anisotropy()
+    p.zeeman((0.1, -0.2, 0.3))
+    e = _fields_compare(p, ["Zeeman", "Total"])
+    assert e["Zeeman"] <= 1e-7 and e["Total"] <= FIELD_TOL, e
+
+
+def test_thermal_injected_normals_match_mersenne_stream(M):
+    dims = (6, 5, 2)
+    n = 60
+    s = random_spins(n, 11, lengths=True)
+    p = Pair(*dims, s, alpha=0.2, dt=0.005)
+    th = p.M.Thermal(*dims)
+    th.setTemperature(0.5)
+    rng = O.MT(1234)
+    noise = O.thermal_draw(p.o, 0.5, rng)
+    th.inject(*noise)
+    O.thermal_apply(p.o, 0.5, O.MT(1234))
+    th.apply(p.g)
+    assert rel_err(np.stack(p.g.fieldArrays("Thermal")), p.o.field("Thermal")) <= FIELD_TOL
+
+
+def test_thermal_philox_statistics(M):
+    nx, ny, nz = 64, 64, 8
+    n = nx * ny * nz
+    ss = M.SpinSystem(nx, ny, nz)
+    s = random_spins(n, 12)
+    ss.setSpinArrays(*s)
+    ss.setAlpha(0.1)
+    ss.setTimeStep(0.01)
+    th = M.Thermal(ss, M.Random.Philox(77))
+    th.setTemperature(0.3)
+    th.apply(ss)
+    h = np.stack(ss.fieldArrays("Thermal"))
+    sig = np.sqrt(2 * 0.1 * 0.3 / (0.01 * 1.0))
+    z = h / sig
+    assert abs(z.mean()) < 5e-3
+    assert abs(z.std() - 1.0) < 5e-3
+    # components independent
+    c = np.corrcoef(z)
+    assert np.abs(c - np.eye(3)).max() < 5e-3
+    # a second apply draws new noise; the same counter reproduces it
+    th.apply(ss)
+    h2 = np.stack(ss.fieldArrays("Thermal"))
+    assert np.abs(np.corrcoef(h.ravel(), h2.ravel())[0, 1]) < 5e-3
+    th.setCounter(0)
+    th.apply(ss)
+    np.testing.assert_array_equal(np.stack(ss.fieldArrays("Thermal")), h)
+
+
+# ---------------------------------------------------------------- dipole
+@pytest.mark.parametrize("dims", [(32, 32, 1), (8, 8, 3), (12, 10, 4), (6, 5, 2), (1, 1, 1), (5, 1, 3)])
+def test_dipole_reference_mode(M, dims):
+    n = int(np.prod(dims))
+    p = Pair(*dims, random_spins(n, 13, lengths=True))
+    dip = p.dipole(g=0.7)
+    e = _fields_compare(p, ["Dipole"])
+    assert e["Dipole"] <= FIELD_TOL, e
+    # the FP64 GPU lattice sum equals the oracle's tensor
+    T_gpu = dip.tensorArrays()
+    T_cpu = O.dipole_tensor(*dims)
+    for a, b in zip(T_gpu, T_cpu):
+        np.testing.assert_allclose(a, b, rtol=1e-13, atol=1e-15)
+
+
+def test_dipole_physical_z_sign(M):
+    dims = (6, 6, 3)
+    n = 108
+    s = random_spins(n, 14)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    dip = M.Dipole(ss)
+    dip.setQuirks(False)
+    dip.setStrength(1.0)
+    dip.apply(ss)
+    h = np.stack(ss.fieldArrays("Dipole"))
+    # physical convention: the same lattice sum with z offset target - source,
+    # i.e. the reference tensor with its layer axis reversed
+    T6 = [t[::-1].copy() for t in O.dipole_tensor(*dims)]
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    O.LongRange(*dims, T6).apply(o, 1.0)
+    assert rel_err(h, o.field("Dipole")) <= FIELD_TOL
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 4), (7, 5, 3), (16, 16, 1)])
+def test_dipole_open_boundaries_direct_sum(M, dims):
+    n = int(np.prod(dims))
+    p = Pair(*dims, random_spins(n, 15, lengths=True))
+    p.dipole(g=0.5, open_xy=True)
+    e = _fields_compare(p, ["Dipole"])
+    assert e["Dipole"] <= FIELD_TOL, e
+
+
+def test_longrange_user_tensor(M):
+    dims = (6, 4, 2)
+    nx, ny, nz = dims
+    n = 48
+    r = np.random.default_rng(16)
+    T6 = [r.normal(size=(2 * nz - 1, ny, nx)) for _ in range(6)]
+    s = random_spins(n, 17)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    lr = M.LongRange(ss)
+    names = ["XX", "XY", "XZ", "YY", "YZ", "ZZ"]
+    for q, nm in enumerate(names):
+        for k in range(2 * nz - 1):
+            for j in range(ny):
+                for i in range(nx):
+                    lr.setMatrix(nm, (i, j, k - (nz - 1)), T6[q][k, j, i])
+    lr.setStrength(0.4)
+    lr.apply(ss)
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    O.LongRange(*dims, T6).apply(o, 0.4, slot="LongRange")
+    assert rel_err(np.stack(ss.fieldArrays("LongRange")), o.field("LongRange")) <= FIELD_TOL
+
+
+def test_longrange3d_general_tensor(M):
+    dims = (6, 5, 4)
+    nx, ny, nz = dims
+    n = 120
+    r = np.random.default_rng(18)
+    T9 = [r.normal(size=(nz, ny, nx)) for _ in range(9)]
+    s = random_spins(n, 19)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    lr = M.LongRange3D(ss)
+    for q, nm in enumerate(["XX", "XY", "XZ", "YX", "YY", "YZ", "ZX", "ZY", "ZZ"]):
+        lr.setTensorArray(nm, T9[q])
+    lr.setStrength(0.8)
+    lr.apply(ss)
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    O.longrange3d_apply(o, T9, 0.8)
+    assert rel_err(np.stack(ss.fieldArrays("LongRange3D")), o.field("LongRange3D")) <= FIELD_TOL
+
+
+# ---------------------------------------------------------------- LLG
+@pytest.mark.parametrize("kind", ["Cartesian", "Quaternion"])
+@pytest.mark.parametrize("tof", [True, False])
+def test_llg_single_step_general_form(M, kind, tof):
+    n = 200
+    s = random_spins(n, 20, lengths=True)
+    H = random_spins(n, 21) * 0.7
+    Th = random_spins(n, 22) * 0.2
+    o = O.SpinSystem(n, 1, 1)
+    o.set_spins(*s)
+    o.alpha, o.dt = 0.3, 0.02
+    hv = o.field_views("Total")
+    tv = o.field_views("Thermal")
+    for c in range(3):
+        hv[c][:] = H[c]
+        tv[c][:] = Th[c]
+    O.LLG(kind, thermal_only_first_term=int(tof), precess_scale=0.9, damp_scale=1.1).apply(o, 1.5)
+    g = M.SpinSystem(n, 1, 1)
+    g.setSpinArrays(*s)
+    g.setAlpha(0.3)
+    g.setTimeStep(0.02)
+    g.setFieldArrays("Total", *H)
+    g.setFieldArrays("Thermal", *Th)
+    l = M.LLG.new(kind)
+    l.setThermalOnlyFirstTerm(tof)
+    l.setUnphysicalPrecessionScale(0.9)
+    l.setUnphysicalDampingScale(1.1)
+    l.apply(g, 1.5, g, g)
+    x, y, z, _ = g.spinArrays()
+    assert np.abs(np.stack([x, y, z]) - o.spins()).max() <= 2e-6
+    assert g.time() == pytest.approx(o.time)
+
+
+def test_llg_from_dmdt_to_distinct_systems(M):
+    n = 64
+    a, b = random_spins(n, 23), random_spins(n, 24)
+    H = random_spins(n, 25)
+    oa, ob, oc = O.SpinSystem(n, 1, 1), O.SpinSystem(n, 1, 1), O.SpinSystem(n, 1, 1)
+    oa.set_spins(*a)
+    ob.set_spins(*b)
+    oc.set_spins(*a)
+    ob.dt = 0.05
+    hv = ob.field_views("Total")
+    for c in range(3):
+        hv[c][:] = H[c]
+    O.LLG("Cartesian").apply(oa, 0.5, ob, oc, advance=True)
+    ga, gb, gc = M.SpinSystem(n, 1, 1), M.SpinSystem(n, 1, 1), M.SpinSystem(n, 1, 1)
+    ga.setSpinArrays(*a)
+    gb.setSpinArrays(*b)
+    gc.setSpinArrays(*a)
+    gb.setTimeStep(0.05)
+    gb.setFieldArrays("Total", *H)
+    M.LLG.new("Cartesian").apply(ga, 0.5, gb, gc, True)
+    x, y, z, _ = gc.spinArrays()
+    assert np.abs(np.stack([x, y, z]) - oc.spins()).max() <= 2e-6
+    assert gc.time() == pytest.approx(oc.time)
+
+
+def _golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def _c1_gpu(M, kind):
+    from golden.make_golden import c1_spins, NX, NY, NZ, J, K, G, ALPHA, DT
+    n = NX * NY * NZ
+    p = Pair(NX, NY, NZ, c1_spins(), alpha=ALPHA, dt=DT)
+    p.exchange(J=J, paths=O.nn_paths(NX, NY, NZ, J=J, dirs=4))
+    p.anisotropy(axis=(0, 0, 1), K=K)
+    p.dipole(g=G)
+    return p, M.LLG.new(kind)
+
+
+def test_c1_fields_against_golden(M):
+    gold = _golden()
+    p, _ = _c1_gpu(M, "Cartesian")
+    p.g.resetFields()
+    for op in p.ops:
+        op.apply(p.g)
+    p.g.sumFields()
+    for name in ("Exchange", "Anisotropy", "Dipole", "Total"):
+        assert rel_err(np.stack(p.g.fieldArrays(name)), gold["c1_field_" + name]) <= FIELD_TOL, name
+
+
+@pytest.mark.parametrize("kind", ["Cartesian", "Quaternion"])
+def test_c1_trajectory_1000_steps_step_by_step(M, kind):
+    gold = np.array(_golden()[f"c1_{kind}_1000"])
+    p, l = _c1_gpu(M, kind)
+    for _ in range(1000):
+        p.step_gpu(l)
+    x, y, z, _ = p.g.spinArrays()
+    err = np.abs(np.stack([x, y, z]) - gold).max()
+    assert err <= TRAJ_TOL, err
+    assert p.g.time() == pytest.approx(10.0, rel=1e-12)
+
+
+@pytest.mark.parametrize("kind", ["Cartesian", "Quaternion"])
+def test_c1_trajectory_1000_steps_fused_run(M, kind):
+    gold = np.array(_golden()[f"c1_{kind}_1000"])
+    p, l = _c1_gpu(M, kind)
+    M.run(p.g, p.ops, l, 1000)
+    x, y, z, _ = p.g.spinArrays()
+    err = np.abs(np.stack([x, y, z]) - gold).max()
+    assert err <= TRAJ_TOL, err
+
+
+def test_run_equals_individual_calls_bitwise(M):
+    dims = (16, 12, 3)
+    n = int(np.prod(dims))
+    s = tilted_spins(n, 26)
+    res = []
+    for mode in ("calls", "run"):
+        ss = M.SpinSystem(*dims)
+        ss.setSpinArrays(*s)
+        ss.setAlpha(0.05)
+        ss.setTimeStep(0.005)
+        ex = M.Exchange(ss)
+        ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 0)))
+        ani = M.Anisotropy(ss)
+        ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.05))
+        th = M.Thermal(ss, M.Random.Philox(5))
+        th.setTemperature(0.5)
+        z = M.AppliedField(ss)
+        z.set(0.1, 0, 0)
+        dip = M.Dipole(ss)
+        dip.setStrength(0.02)
+        l = M.LLG.new("Quaternion")
+        ops = [ex, ani, th, z, dip]
+        if mode == "calls":
+            for _ in range(9):
+                ss.resetFields()
+                for op in ops:
+                    op.apply(ss)
+                ss.sumFields()
+                l.apply(ss)
+        else:
+            M.run(ss, ops, l, 9)
+        res.append(np.stack(ss.spinArrays()[:3]))
+        res.append(np.stack(ss.fieldArrays("Total")))
+    np.testing.assert_array_equal(res[0], res[2])
+    np.testing.assert_array_equal(res[1], res[3])
+
+
+def test_fused_step_equals_materialised_step(M):
+    # reading a slot before llg:apply forces the unfused path
+    dims = (10, 9, 2)
+    n = 180
+    s = random_spins(n, 27)
+    out = []
+    for read in (False, True):
+        ss = M.SpinSystem(*dims)
+        ss.setSpinArrays(*s)
+        ss.setAlpha(0.1)
+        ss.setTimeStep(0.01)
+        ex = M.Exchange(ss)
+        ex.addPaths(*O.nn_paths(*dims))
+        ani = M.Anisotropy(ss)
+        ani.addMany(np.arange(n), np.tile([1.0, 0, 0], (n, 1)), np.full(n, 0.2))
+        l = M.LLG.new("Cartesian")
+        ss.resetFields()
+        ex.apply(ss)
+        ani.apply(ss)
+        ss.sumFields()
+        if read:
+            ss.fieldArrays("Total")
+        l.apply(ss)
+        out.append(np.stack(ss.spinArrays()[:3]))
+    np.testing.assert_allclose(out[0], out[1], atol=1e-6)
+
+
+def test_netmoment_fp64(M):
+    n = 4096
+    s = random_spins(n, 28, lengths=True)
+    ss = M.SpinSystem(64, 64, 1)
+    ss.setSpinArrays(*s)
+    o = O.SpinSystem(64, 64, 1)
+    o.set_spins(*s.astype(np.float32).astype(np.float64))
+    np.testing.assert_allclose(ss.netMoment(2.0), o.netmoment(2.0), rtol=1e-12)
+
+
+def test_slot_api_semantics(M):
+    ss = M.SpinSystem(4, 4, 1)
+    ss.setSpinArrays(*random_spins(16, 29))
+    ex = M.Exchange(ss)
+    ex.addPaths(*O.nn_paths(4, 4, 1, dirs=4))
+    ex.apply(ss)
+    assert ss.slotUsed("Exchange")
+    ss.resetFields()
+    assert not ss.slotUsed("exchange")  # case-insensitive names
+    np.testing.assert_array_equal(np.stack(ss.fieldArrays("Exchange")), 0)
+    with pytest.raises(M.MagLuaError):
+        ss.fieldArrays("NoSuchSlot")
+    with pytest.raises(M.MagLuaError):
+        M.SpinSystem(0, 1, 1)
