@@ -23,7 +23,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <map>
 #include <memory>
 #include <new>
 #include <set>
@@ -254,6 +253,7 @@ struct mlb_op {
     int open[3] = {0, 0, 1};
     std::vector<double> t6[6];
     bool t6_valid = false;
+    bool t6_edited = false;
     std::vector<double> t9[9];
     bool plan_dirty = true;
     std::unique_ptr<ConvPlan> plan;
@@ -367,33 +367,31 @@ void compile_exchange(mlb_op* op)
         else if (Jd[dir] != op->eJ[p]) stencil = false;
     }
     if (stencil) {
-        // the candidate must reproduce the pathway multiset exactly
-        std::map<std::pair<int, int>, double> actual, expect;
-        for (size_t p = 0; p < np; p++) actual[{op->et[p], op->ef[p]}] += op->eJ[p];
-        for (int t = 0; t < n && stencil; t++) {
+        // The candidate must reproduce the pathway multiset exactly: every
+        // (target, direction) at most once, and per direction as many paths
+        // as targets that have that neighbour.
+        std::vector<unsigned char> hit((size_t)n * 6, 0);
+        long long cnt[6] = {0, 0, 0, 0, 0, 0};
+        for (size_t p = 0; p < np && stencil; p++) {
+            const int f = op->ef[p], t = op->et[p];
+            const int fc[3] = {f % nx, (f / nx) % ny, f / (nx * ny)};
             const int tc[3] = {t % nx, (t / nx) % ny, t / (nx * ny)};
-            for (int d = 0; d < 6; d++) {
-                if (!seen[d]) continue;
-                const int a = d >> 1, sg = (d & 1) ? -1 : 1;
-                int c[3] = {tc[0], tc[1], tc[2]};
-                c[a] += sg;
-                if (c[a] < 0 || c[a] >= dims[a]) {
-                    if (!pbc[a]) continue;
-                    c[a] = (c[a] + dims[a]) % dims[a];
-                }
-                const int f = c[0] + nx * (c[1] + ny * c[2]);
-                expect[{t, f}] += Jd[d];
+            int dir = -1;
+            for (int a = 0; a < 3; a++) {
+                const int d = fc[a] - tc[a];
+                if (d == 0) continue;
+                dir = (d == 1 || (dims[a] > 2 && d == -(dims[a] - 1))) ? 2 * a : 2 * a + 1;
             }
+            unsigned char& h = hit[(size_t)t * 6 + dir];
+            if (h) stencil = false;
+            h = 1;
+            cnt[dir]++;
         }
-        if (actual.size() != expect.size()) stencil = false;
-        else {
-            for (auto& kv : actual) {
-                auto it = expect.find(kv.first);
-                if (it == expect.end() || std::fabs(it->second - kv.second) > 1e-12 * std::fabs(kv.second)) {
-                    stencil = false;
-                    break;
-                }
-            }
+        for (int d = 0; d < 6 && stencil; d++) {
+            if (!seen[d]) continue;
+            const int a = d >> 1;
+            const long long want = pbc[a] ? (long long)n : (long long)n - n / dims[a];
+            if (cnt[d] != want) stencil = false;
         }
     }
     if (stencil) {
@@ -518,12 +516,14 @@ void plan_sizes(mlb_op* op, ConvPlan& P)
         k.Px = op->nx; k.Py = op->ny; k.Pz = op->nz;
         k.general = 1;
     } else {
+        // a user tensor need not be inversion symmetric, so its transform is
+        // complex: multiply with the general 3x3 complex form
+        k.general = (op->kind == MLB_OP_LONGRANGE || op->t6_edited) ? 1 : 0;
         const bool ox = op->kind == MLB_OP_DIPOLE && op->open[0];
         const bool oy = op->kind == MLB_OP_DIPOLE && op->open[1];
         k.Px = ox ? nice_len(2 * op->nx - 1) : op->nx;
         k.Py = oy ? nice_len(2 * op->ny - 1) : op->ny;
         k.Pz = op->nz == 1 ? 1 : nice_len(2 * op->nz - 1);
-        k.general = 0;
     }
     k.Kx = k.Px / 2 + 1;
     int ty = 16;
@@ -588,7 +588,7 @@ void build_plan(mlb_op* op, cudaStream_t st)
             for (int q = 0; q < 6; q++) op->t6[q].assign(h.begin() + q * ne, h.begin() + (q + 1) * ne);
             op->t6_valid = true;
         }
-    } else if (k.general) {
+    } else if (op->kind == MLB_OP_LONGRANGE3D) {
         std::vector<double2> h(plane * 9);
         for (int q = 0; q < 9; q++) {
             if (op->t9[q].size() != plane) continue;
@@ -600,15 +600,18 @@ void build_plan(mlb_op* op, cudaStream_t st)
         // k = source - target at padded index (zsign*k mod Pz)
         ensure_t6_layout(op);
         const int zsign = op->quirks ? -1 : 1;
-        std::vector<double2> h(plane * 6, make_double2(0, 0));
-        for (int q = 0; q < 6; q++)
+        // six planes (symmetric real path) or nine (general path, XY=YX ...)
+        static const int map9[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        std::vector<double2> h(plane * ncomp, make_double2(0, 0));
+        for (int q = 0; q < ncomp; q++)
             for (int kk = -(op->nz - 1); kk < op->nz; kk++) {
                 int zi = (zsign * kk) % Pz;
                 if (zi < 0) zi += Pz;
                 for (int j = 0; j < op->ny; j++)
                     for (int i = 0; i < op->nx; i++) {
                         const size_t src = (size_t)i + op->nx * ((size_t)j + op->ny * (size_t)(kk + op->nz - 1));
-                        h[q * plane + ((size_t)zi * Py + j) * Px + i] = make_double2(op->t6[q][src], 0.0);
+                        const int qq = ncomp == 9 ? map9[q] : q;
+                        h[q * plane + ((size_t)zi * Py + j) * Px + i] = make_double2(op->t6[qq][src], 0.0);
                     }
             }
         CK(cudaMemcpy(W.p, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice));
@@ -1844,6 +1847,7 @@ int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4])
         for (int i = 0; i < 4; i++) op->gmax[i] = gmax[i];
         if (op->gmax[0] < 0) fail(MLB_EUNSUP, "infinite truncation (extrapolated lattice sum) is not built");
         op->t6_valid = false;
+        op->t6_edited = false;
         op->plan_dirty = true;
     });
 }
@@ -1853,6 +1857,7 @@ int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9])
     return guard([&] {
         for (int i = 0; i < 9; i++) op->ABC[i] = ABC[i];
         op->t6_valid = false;
+        op->t6_edited = false;
         op->plan_dirty = true;
     });
 }
@@ -1899,6 +1904,7 @@ int mlb_longrange_set_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double 
         materialize_users(op);
         op->t6[ab][off] = v;
         op->t6_valid = true;
+        op->t6_edited = true;
         op->plan_dirty = true;
     });
 }
