@@ -11,8 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmlb200.so")
-SOURCES = ["kernels.cu", "capi.cu"]
-HEADERS = ["device.cuh", "kparams.h", "launch.h"]
+SOURCES = ["kernels.cu", "conv_fast.cu", "capi.cu"]
+HEADERS = ["device.cuh", "fftreg.cuh", "kparams.h", "launch.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

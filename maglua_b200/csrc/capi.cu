@@ -126,15 +126,14 @@ FftLen make_len(int n, int tw_off)
     return L;
 }
 
-// smallest m' >= m of the form 2^a or 3*2^a
+// padded length for an open axis: the smallest power of two >= m (the
+// register-FFT fast path covers powers of two)
 int nice_len(int m)
 {
     if (m <= 1) return 1;
     int best = 1;
     while (best < m) best *= 2;
-    int t = 3;
-    while (t < m) t *= 2;
-    return std::min(best, t);
+    return best;
 }
 
 template <class C>
@@ -948,7 +947,10 @@ void op_apply(mlb_op* op, mlb_system* s)
         ConvPlan& P = *op->plan;
         P.k.g = (float)(op->g * op->gs / ((double)P.k.Px * P.k.Py * P.k.Pz));
         const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
-        CK(mlb::launch_conv(P.k, P.L[0], P.L[1], P.L[2], P.tw.p, sp, P.spec.p, P.ten6.p, P.ten9.p, sl.h, s->st));
+        if (mlb::conv_fast_ok(P.k))
+            CK(mlb::launch_conv_fast(P.k, P.L, P.tw.p, sp, P.spec.p, P.ten6.p, sl.h, s->st));
+        else
+            CK(mlb::launch_conv(P.k, P.L[0], P.L[1], P.L[2], P.tw.p, sp, P.spec.p, P.ten6.p, P.ten9.p, sl.h, s->st));
         sl.state = ST_DATA;
         return;
     }
@@ -968,6 +970,57 @@ LlgK llgk(const mlb_llg* l, double dt)
     k.dt = (float)dt;
     k.dt_zero = dt == 0.0 ? 1 : 0;
     return k;
+}
+
+// Constants of k_fused_fast when every parameter is uniform across sites;
+// false sends the step to the general fused kernel.
+bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, double dt_sys, FastK& F)
+{
+    refresh_ms(s);
+    if (!s->ms_uniform || !(s->ms_u > 0.f) || s->sa || s->sg) return false;
+    if (T.ex.mode == EX_CSR || T.ani.mode == ANI_CSR || T.uni.mode != ANI_NONE || T.cub.mode != ANI_NONE) return false;
+    if (T.th.mode == TH_INJECT || (T.th.mode == TH_PHILOX && T.th.scale)) return false;
+    if (T.nadd > 1 || (T.nadd == 1 && T.add_is_thermal[0])) return false;
+    const double ms = s->ms_u, a = s->alpha, g = s->gamma;
+    memset(&F, 0, sizeof(F));
+    F.nx = s->nx; F.ny = s->ny; F.nz = s->nz;
+    F.ex = T.ex.mode == EX_STENCIL;
+    if (F.ex) {
+        const double den = T.ex.normalize ? ms * ms : ms;
+        for (int d = 0; d < 6; d++) F.J[d] = (float)((double)T.ex.J[d] * T.ex_gs / den);
+        for (int c = 0; c < 3; c++) F.pbc[c] = T.ex.pbc[c];
+    }
+    F.ani = T.ani.mode == ANI_UNIFORM;
+    if (F.ani) {
+        for (int c = 0; c < 3; c++) F.axis[c] = T.ani.axis[c];
+        F.ani_c = (float)(2.0 * (double)T.ani.K / (ms * ms));
+    }
+    F.th = T.th.mode == TH_PHILOX && T.th.T != 0.f && g > 0;
+    if (F.th) {
+        F.sigma = (float)std::sqrt((2.0 * a * (double)T.th.T) / (ms * dt_sys * g));
+        F.seed = T.th.seed; F.counter = T.th.counter; F.dctr = T.th.dctr;
+    }
+    if (T.zee.on) {
+        for (int c = 0; c < 3; c++) { F.B[c] = T.zee.B[c]; F.dB[c] = T.zee.dB[c]; }
+        F.zdctr = T.zee.dctr;
+    }
+    F.addw = T.nadd == 1 ? T.addw[0] : 0.f;
+    F.llg_type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
+    F.tof = l->tof;
+    F.renorm = l->disable_renorm ? 0 : 1;
+    F.dt_zero = dt == 0.0;
+    F.dt = (float)dt;
+    F.precess = (float)l->precess;
+    F.ms = (float)ms;
+    const double gaa = g / (1.0 + a * a);
+    if (F.llg_type == LLG_CART) {
+        F.c_prec = (float)(l->tof ? l->precess * -gaa : -gaa);
+        F.c_damp = (float)(l->tof ? l->damp * (a / ms) * gaa : (a / ms) * gaa);
+    } else {
+        F.c_damp = (float)(l->tof ? l->damp * a / ms : a / ms);
+        F.c_rot = (float)(0.5 * g * dt / (1.0 + a * a));
+    }
+    return true;
 }
 
 // Fused in-place step when Total is lazily defined; returns false when the
@@ -998,13 +1051,22 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
     if (th >= 0 && !th_in && s->slots[th].state == ST_DATA) {
         if (!add_addend(T, s->slots[th].h, 0.f, true)) return false;
     }
-    FusedK P;
-    P.sys = sysk(s, s->cur);
-    P.terms = T;
-    P.llg = llgk(l, dt);
     const int nb = 1 - s->cur;
-    P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
-    CK(mlb::launch_fused(P, (float)dt_sys, s->st));
+    FastK F;
+    if (fast_fused(s, T, l, dt, dt_sys, F)) {
+        const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+        const float* ad[3] = {nullptr, nullptr, nullptr};
+        if (T.nadd == 1) for (int c = 0; c < 3; c++) ad[c] = T.add[0][c];
+        float* out[3] = {s->sp[nb][0], s->sp[nb][1], s->sp[nb][2]};
+        CK(mlb::launch_fused_fast(F, sp, ad, out, s->st));
+    } else {
+        FusedK P;
+        P.sys = sysk(s, s->cur);
+        P.terms = T;
+        P.llg = llgk(l, dt);
+        P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
+        CK(mlb::launch_fused(P, (float)dt_sys, s->st));
+    }
     if (s->capturing) CK(mlb::launch_advance(s->dctr, s->st));
     s->cur = nb;
     s->gen++;
@@ -1184,6 +1246,7 @@ int mlb_init(int device)
         CK(cudaSetDevice(device));
         CK(cudaFree(0));
         CK(mlb::conv_configure());
+        CK(mlb::fftreg_init());
     });
 }
 

@@ -725,9 +725,9 @@ __global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx,
 
 namespace mlb {
 
-// Opt-in per-kernel timing: each launcher brackets its kernels with CUDA
+// Opt-in per-kernel timing: launchers bracket their kernels with CUDA
 // events on the launching stream while profiling is on (never inside a
-// graph capture).  prof_collect() sums elapsed times per kernel name.
+// graph capture); prof_end() sums elapsed times per kernel name.
 namespace {
 struct ProfRec {
     const char* name;
@@ -736,7 +736,17 @@ struct ProfRec {
 bool g_prof = false;
 std::vector<ProfRec> g_recs;
 std::vector<cudaEvent_t> g_pool;
-cudaEvent_t ev_get()
+} // namespace
+
+bool prof_active(cudaStream_t st)
+{
+    if (!g_prof) return false;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+    return true;
+}
+
+cudaEvent_t prof_event()
 {
     if (!g_pool.empty()) {
         cudaEvent_t e = g_pool.back();
@@ -747,29 +757,8 @@ cudaEvent_t ev_get()
     cudaEventCreate(&e);
     return e;
 }
-struct Prof {
-    bool on = false;
-    const char* name;
-    cudaStream_t st;
-    cudaEvent_t a = nullptr;
-    Prof(const char* n, cudaStream_t s) : name(n), st(s)
-    {
-        if (!g_prof) return;
-        cudaStreamCaptureStatus cs;
-        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
-        on = true;
-        a = ev_get();
-        cudaEventRecord(a, st);
-    }
-    ~Prof()
-    {
-        if (!on) return;
-        cudaEvent_t b = ev_get();
-        cudaEventRecord(b, st);
-        g_recs.push_back({name, a, b});
-    }
-};
-} // namespace
+
+void prof_push(const char* name, cudaEvent_t a, cudaEvent_t b) { g_recs.push_back({name, a, b}); }
 
 void prof_begin()
 {

@@ -111,3 +111,25 @@ struct ConvK {
     float g;                 // strength * global_scale / (Px*Py*Pz)
     int fx, fy, fz;          // FftLen indices
 };
+
+// Fused step for uniform-parameter systems (k_fused_fast): every constant
+// folded on the host.
+struct FastK {
+    int nx, ny, nz;
+    int ex;                   // six-direction stencil present
+    float J[6];               // J * scale / ms^2 (normalised) or / ms
+    int pbc[3];
+    int ani;
+    float axis[3];
+    float ani_c;              // 2 K scale / ms^2
+    int th;
+    float sigma;              // sqrt(2 alpha T scale / (ms dt gamma))
+    uint64_t seed, counter;
+    const uint64_t* dctr;
+    float B[3];               // Zeeman (+ dB * *zdctr)
+    float dB[3];
+    const uint64_t* zdctr;
+    float addw;
+    int llg_type, tof, renorm, dt_zero;
+    float dt, precess, c_prec, c_damp, c_rot, ms;
+};

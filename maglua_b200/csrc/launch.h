@@ -6,6 +6,32 @@
 #include "kparams.h"
 
 namespace mlb {
+bool prof_active(cudaStream_t st);
+cudaEvent_t prof_event();
+void prof_push(const char* name, cudaEvent_t a, cudaEvent_t b);
+// Scope timer used around kernel launches (active only while profiling).
+struct Prof {
+    bool on;
+    const char* name;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    Prof(const char* n, cudaStream_t s) : on(prof_active(s)), name(n), st(s)
+    {
+        if (on) { a = prof_event(); cudaEventRecord(a, st); }
+    }
+    ~Prof()
+    {
+        if (!on) return;
+        cudaEvent_t b = prof_event();
+        cudaEventRecord(b, st);
+        prof_push(name, a, b);
+    }
+};
+cudaError_t fftreg_init();
+bool conv_fast_ok(const ConvK& c);
+cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
+                             const float* ten6, float* h[3], cudaStream_t st);
+cudaError_t launch_fused_fast(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st);
 void prof_begin();
 int prof_end(int cap, char* names, double* ms, int* launches);
 cudaError_t launch_fused(const FusedK& P, float dt_sys, cudaStream_t st);

@@ -198,7 +198,8 @@ def test_thermal_philox_statistics(M):
 
 
 # ---------------------------------------------------------------- dipole
-@pytest.mark.parametrize("dims", [(32, 32, 1), (8, 8, 3), (12, 10, 4), (6, 5, 2), (1, 1, 1), (5, 1, 3)])
+@pytest.mark.parametrize("dims", [(32, 32, 1), (8, 8, 3), (12, 10, 4), (6, 5, 2), (1, 1, 1), (5, 1, 3),
+                                  (32, 16, 4), (64, 64, 2), (16, 64, 8)])
 def test_dipole_reference_mode(M, dims):
     n = int(np.prod(dims))
     p = Pair(*dims, random_spins(n, 13, lengths=True))
@@ -232,7 +233,7 @@ def test_dipole_physical_z_sign(M):
     assert rel_err(h, o.field("Dipole")) <= FIELD_TOL
 
 
-@pytest.mark.parametrize("dims", [(8, 8, 4), (7, 5, 3), (16, 16, 1)])
+@pytest.mark.parametrize("dims", [(8, 8, 4), (7, 5, 3), (16, 16, 1), (16, 5, 3), (31, 9, 2), (20, 33, 5)])
 def test_dipole_open_boundaries_direct_sum(M, dims):
     n = int(np.prod(dims))
     p = Pair(*dims, random_spins(n, 15, lengths=True))
