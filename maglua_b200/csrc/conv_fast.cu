@@ -20,6 +20,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 namespace mlb {
 
 cudaError_t fftreg_init()
@@ -55,6 +57,9 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
     using X = XCfg<PX>;
     constexpr int T = X::T, E = X::E;
     extern __shared__ float2 sm[];
+    float2* twl = sm + X::LINES * X::EX;
+    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
+    __syncthreads();
     const int comp = blockIdx.z, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
     const float* src = comp == 0 ? sx : (comp == 1 ? sy : sz);
@@ -75,7 +80,7 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
             }
             v[j] = make_float2(a, b);
         }
-        fr::line_fft<PX, -1>(v, ex, t, mask, tw);
+        fr::line_fft<PX, -1>(v, ex, t, mask, twl);
         // stage Z in natural order
 #pragma unroll
         for (int r = 0; r < E; r++) ex[fr::out_index<PX>(t, r)] = v[r];
@@ -105,6 +110,8 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
     extern __shared__ float2 sm[];
     float2* S = sm;                              // [ROWS][KX] spectra
     float2* EXB = sm + X::ROWS * KX;             // per-line buffers
+    float2* twl = EXB + X::LINES * X::EX;        // twiddles
+    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
     const int comp = blockIdx.z, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
     const int rows_here = min(X::ROWS, c.ny - row0);
@@ -132,7 +139,7 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
             else { a = cconj(A[PX - k]); b = cconj(B[PX - k]); }
             v[j] = make_float2(a.x - b.y, a.y + b.x); // A + iB
         }
-        fr::line_fft<PX, +1>(v, ex, t, mask, tw);
+        fr::line_fft<PX, +1>(v, ex, t, mask, twl);
 #pragma unroll
         for (int r = 0; r < E; r++) ex[fr::out_index<PX>(t, r)] = v[r];
     }
@@ -150,29 +157,49 @@ template <int PY>
 struct YCfg {
     static constexpr int T = Split<PY>::T;
     static constexpr int E = Split<PY>::E;
-    static constexpr int LINES = 256 / T;              // lines in flight
     static constexpr int EX = E * (T + 1);
 };
 
+// threads of k_yz_fast: 768 (80 registers each), 512 for PY = 512 whose
+// 32-element lanes need more registers
+template <int PY>
+struct YZT {
+    static constexpr int N = PY >= 512 ? 512 : 768;
+};
+
 template <int PY, int PZ>
-__global__ void __launch_bounds__(256) k_yz_fast(ConvK c, const float2* __restrict__ twy, float2* __restrict__ spec,
-                                                 const float* __restrict__ ten6)
+__global__ void __launch_bounds__(YZT<PY>::N, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
+                                                           float2* __restrict__ spec, const float* __restrict__ ten6)
 {
     using Y = YCfg<PY>;
+    constexpr int YZ_THREADS = YZT<PY>::N;
     constexpr int T = Y::T, E = Y::E;
     extern __shared__ float2 sm[];
     const int kx = blockIdx.x;
     const int nz = c.nz, ny = c.ny;
-    float2* P = sm;                          // [3][nz][PY]
-    float2* EXB = sm + 3 * nz * PY;          // [LINES][EX]
+    const int nlines = 3 * nz;
+    const int LIN = min(nlines, YZ_THREADS / T);                 // y lines in flight
+    const int R2 = max(3 * PZ * PY, LIN * Y::EX);
+    float2* P = sm;                          // [3][nz][PY] data rows
+    float2* Q = P + 3 * nz * PY;             // [3][PZ][PY] z spectra (z phase)
+    float2* EXB = Q;                         // [LIN][EX] line buffers (y phases)
+    float2* twl = Q + R2;                    // [PY]
+    const float* Tk = ten6 + (size_t)kx * PZ * PY * 6;
+    if (threadIdx.x == 0) {
+        // pull this kx's tensor chunk into L2 while the y transforms run
+        const unsigned bytes = (unsigned)(PZ * PY * 6 * sizeof(float));
+        if ((((uintptr_t)Tk) & 15) == 0 && (bytes & 15) == 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tk), "r"(bytes) : "memory");
+    }
+    for (int k = threadIdx.x; k < PY; k += blockDim.x) twl[k] = twy[k];
+    __syncthreads();
     float2* sp = spec + (size_t)kx * 3 * nz * ny;
     const int g = threadIdx.x / T, t = threadIdx.x % T;
     const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x & 31) / T * T));
-    const int nlines = 3 * nz;
     // forward y FFT of every data line (c, z)
-    for (int l0 = 0; l0 < nlines; l0 += Y::LINES) {
+    for (int l0 = 0; l0 < nlines; l0 += LIN) {
         const int l = l0 + g;
-        if (g < Y::LINES && l < nlines) {
+        if (g < LIN && l < nlines) {
             const float2* in = sp + (size_t)l * ny;
             float2 v[E];
 #pragma unroll
@@ -180,53 +207,55 @@ __global__ void __launch_bounds__(256) k_yz_fast(ConvK c, const float2* __restri
                 const int y = t + T * j;
                 v[j] = y < ny ? in[y] : make_float2(0.f, 0.f);
             }
-            fr::line_fft<PY, -1>(v, EXB + g * Y::EX, t, mask, twy);
+            fr::line_fft<PY, -1>(v, EXB + g * Y::EX, t, mask, twl);
             float2* out = P + (size_t)l * PY;
 #pragma unroll
             for (int r = 0; r < E; r++) out[fr::out_index<PY>(t, r)] = v[r];
         }
     }
     __syncthreads();
-    // z FFT, tensor multiply, inverse z FFT: one ky per thread
+    // forward z FFT: one (component, ky) column per thread
+    for (int w = threadIdx.x; w < 3 * PY; w += blockDim.x) {
+        const int a = w / PY, ky = w % PY;
+        float2 s[PZ];
+#pragma unroll
+        for (int z = 0; z < PZ; z++) s[z] = z < nz ? P[((size_t)a * nz + z) * PY + ky] : make_float2(0.f, 0.f);
+        fr::RegFFT<PZ, -1, float2>::run(s);
+#pragma unroll
+        for (int z = 0; z < PZ; z++) Q[((size_t)a * PZ + z) * PY + ky] = s[z];
+    }
+    __syncthreads();
+    // tensor multiply (row a of the symmetric tensor) and inverse z FFT
     const float gg = c.g;
-    for (int ky = threadIdx.x; ky < PY; ky += blockDim.x) {
-        float2 s[3][PZ];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-#pragma unroll
-            for (int z = 0; z < PZ; z++) s[a][z] = z < nz ? P[((size_t)a * nz + z) * PY + ky] : make_float2(0.f, 0.f);
-            fr::RegFFT<PZ, -1, float2>::run(s[a]);
-        }
-        const float* Tk = ten6 + ((size_t)kx * PZ * PY + ky) * 6;
+    for (int w = threadIdx.x; w < 3 * PY; w += blockDim.x) {
+        const int a = w / PY, ky = w % PY;
+        // row a of [[0,1,2],[1,3,4],[2,4,5]]
+        const int i0 = a == 0 ? 0 : (a == 1 ? 1 : 2);
+        const int i1 = a == 0 ? 1 : (a == 1 ? 3 : 4);
+        const int i2 = a == 0 ? 2 : (a == 1 ? 4 : 5);
+        float2 h[PZ];
 #pragma unroll
         for (int kz = 0; kz < PZ; kz++) {
-            const float2* Tp = reinterpret_cast<const float2*>(Tk + (size_t)kz * PY * 6);
-            const float2 q01 = __ldg(Tp), q23 = __ldg(Tp + 1), q45 = __ldg(Tp + 2);
-            const float t0 = q01.x * gg, t1 = q01.y * gg, t2 = q23.x * gg;
-            const float t3 = q23.y * gg, t4 = q45.x * gg, t5 = q45.y * gg;
-            const float2 a = s[0][kz], b = s[1][kz], d = s[2][kz];
-            s[0][kz] = make_float2(t0 * a.x + t1 * b.x + t2 * d.x, t0 * a.y + t1 * b.y + t2 * d.y);
-            s[1][kz] = make_float2(t1 * a.x + t3 * b.x + t4 * d.x, t1 * a.y + t3 * b.y + t4 * d.y);
-            s[2][kz] = make_float2(t2 * a.x + t4 * b.x + t5 * d.x, t2 * a.y + t4 * b.y + t5 * d.y);
+            const float* Tp = Tk + ((size_t)kz * PY + ky) * 6;
+            const float q0 = __ldg(Tp + i0) * gg, q1 = __ldg(Tp + i1) * gg, q2 = __ldg(Tp + i2) * gg;
+            const float2 s0 = Q[(0 * PZ + kz) * PY + ky], s1 = Q[(1 * PZ + kz) * PY + ky], s2 = Q[(2 * PZ + kz) * PY + ky];
+            h[kz] = make_float2(q0 * s0.x + q1 * s1.x + q2 * s2.x, q0 * s0.y + q1 * s1.y + q2 * s2.y);
         }
+        fr::RegFFT<PZ, +1, float2>::run(h);
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-            fr::RegFFT<PZ, +1, float2>::run(s[a]);
-#pragma unroll
-            for (int z = 0; z < PZ; z++)
-                if (z < nz) P[((size_t)a * nz + z) * PY + ky] = s[a][z];
-        }
+        for (int z = 0; z < PZ; z++)
+            if (z < nz) P[((size_t)a * nz + z) * PY + ky] = h[z];
     }
     __syncthreads();
     // inverse y FFT, store the data rows
-    for (int l0 = 0; l0 < nlines; l0 += Y::LINES) {
+    for (int l0 = 0; l0 < nlines; l0 += LIN) {
         const int l = l0 + g;
-        if (g < Y::LINES && l < nlines) {
+        if (g < LIN && l < nlines) {
             const float2* in = P + (size_t)l * PY;
             float2 v[E];
 #pragma unroll
             for (int j = 0; j < E; j++) v[j] = in[t + T * j];
-            fr::line_fft<PY, +1>(v, EXB + g * Y::EX, t, mask, twy);
+            fr::line_fft<PY, +1>(v, EXB + g * Y::EX, t, mask, twl);
             float2* out = sp + (size_t)l * ny;
 #pragma unroll
             for (int r = 0; r < E; r++) {
@@ -319,9 +348,10 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
             const float shx = Sy * Hz - Sz * Hy, shy = Sz * Hx - Sx * Hz, shz = Sx * Hy - Sy * Hx;
             Hpx = Hx + F.c_damp * shx; Hpy = Hy + F.c_damp * shy; Hpz = Hz + F.c_damp * shz;
         }
-        const float HL = sqrtf(Hpx * Hpx + Hpy * Hpy + Hpz * Hpz);
-        if (HL > 0.f) {
-            const float iHL = 1.0f / HL;
+        const float HL2 = Hpx * Hpx + Hpy * Hpy + Hpz * Hpz;
+        if (HL2 > 0.f) {
+            const float iHL = rsqrtf(HL2);
+            const float HL = HL2 * iHL;
             float sn, cs;
             sincosf(F.c_rot * HL, &sn, &cs);
             const float qw = cs, qx = sn * Hpx * iHL, qy = sn * Hpy * iHL, qz = sn * Hpz * iHL;
@@ -337,7 +367,7 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
     if (F.renorm) {
         const float mm = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
         if (mm != 0.f) {
-            const float inv = F.ms / sqrtf(mm);
+            const float inv = F.ms * rsqrtf(mm);
             nx_ *= inv; ny_ *= inv; nz_ *= inv;
         }
     }
@@ -349,12 +379,21 @@ namespace mlb {
 
 static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
+// shared memory of k_yz_fast: data rows, z spectra, line buffers, twiddles
+static size_t yz_fast_smem(int PY, int PZ, int nz)
+{
+    const int T = PY <= 4 ? 1 : (PY <= 32 ? (PY <= 8 ? 2 : 4) : (PY <= 128 ? 8 : 16));
+    const int E = PY / T;
+    const int threads = PY >= 512 ? 512 : 768;
+    const int lines = std::min(3 * nz, threads / T);
+    const size_t r2 = std::max((size_t)3 * PZ * PY, (size_t)lines * E * (T + 1));
+    return ((size_t)3 * nz * PY + r2 + PY) * sizeof(float2);
+}
+
 bool conv_fast_ok(const ConvK& c)
 {
     if (c.general || !pow2_in(c.Px, 16, 512) || !pow2_in(c.Py, 16, 512) || !pow2_in(c.Pz, 1, 16)) return false;
-    int T = c.Py <= 4 ? 1 : (c.Py <= 32 ? (c.Py <= 8 ? 2 : 4) : (c.Py <= 128 ? 8 : 16));
-    const size_t yz = ((size_t)3 * c.nz * c.Py + (size_t)(256 / T) * (c.Py / T) * (T + 1)) * sizeof(float2);
-    return yz <= 200 * 1024;
+    return yz_fast_smem(c.Py, c.Pz, c.nz) <= 227 * 1024;
 }
 
 template <int PX>
@@ -364,12 +403,12 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
     using X = XCfg<PX>;
     dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3);
     if (fwd) {
-        const size_t smem = (size_t)X::LINES * X::EX * sizeof(float2);
+        const size_t smem = ((size_t)X::LINES * X::EX + PX) * sizeof(float2);
         static bool cfg = false;
         if (!cfg) { cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
         k_fx_fast<PX><<<grid, 256, smem, st>>>(c, tw, s[0], s[1], s[2], spec);
     } else {
-        const size_t smem = ((size_t)X::ROWS * X::KX + (size_t)X::LINES * X::EX) * sizeof(float2);
+        const size_t smem = ((size_t)X::ROWS * X::KX + (size_t)X::LINES * X::EX + PX) * sizeof(float2);
         static bool cfg = false;
         if (!cfg) { cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
         k_ix_fast<PX><<<grid, 256, smem, st>>>(c, tw, spec, h[0], h[1], h[2]);
@@ -394,11 +433,10 @@ static cudaError_t launch_x_any(const ConvK& c, const float2* tw, const float* s
 template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
-    using Y = YCfg<PY>;
-    const size_t smem = ((size_t)3 * c.nz * PY + (size_t)Y::LINES * Y::EX) * sizeof(float2);
+    const size_t smem = yz_fast_smem(PY, PZ, c.nz);
     static bool cfg = false;
-    if (!cfg) { cudaFuncSetAttribute(k_yz_fast<PY, PZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
-    k_yz_fast<PY, PZ><<<c.Kx, 256, smem, st>>>(c, twy, spec, ten6);
+    if (!cfg) { cudaFuncSetAttribute(k_yz_fast<PY, PZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); cfg = true; }
+    k_yz_fast<PY, PZ><<<c.Kx, YZT<PY>::N, smem, st>>>(c, twy, spec, ten6);
     return cudaGetLastError();
 }
 
