@@ -39,13 +39,14 @@ cudaError_t fftreg_init()
 using fr::Split;
 
 // ------------------------------------------------------------------ x passes
+// A CTA of 256 threads transforms L = 256/TPL complex lines; line l packs
+// rows (row0 + 2l, row0 + 2l + 1) of one component of one layer as real and
+// imaginary parts.
 template <int PX>
 struct XCfg {
-    static constexpr int T = Split<PX>::T;
-    static constexpr int E = Split<PX>::E;
-    static constexpr int LINES = 256 / (T > 0 ? T : 1) > 32 ? 32 : 256 / T; // lines per CTA
-    static constexpr int ROWS = 2 * LINES;
-    static constexpr int EX = E * (T + 1) > PX ? E * (T + 1) : PX;         // per-line buffer
+    static constexpr int TPL = fr::Tpl<PX>::V;
+    static constexpr int L = 256 / TPL;
+    static constexpr int ROWS = 2 * L;
     static constexpr int KX = PX / 2 + 1;
 };
 
@@ -55,43 +56,33 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
                                                  float2* __restrict__ spec)
 {
     using X = XCfg<PX>;
-    constexpr int T = X::T, E = X::E;
     extern __shared__ float2 sm[];
-    float2* twl = sm + X::LINES * X::EX;
-    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
-    __syncthreads();
+    float2* A = sm;                 // [L][PX]
+    float2* B = A + X::L * PX;      // [L][PX]
+    float2* twl = B + X::L * PX;    // [PX]
     const int comp = blockIdx.z, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
-    const float* src = comp == 0 ? sx : (comp == 1 ? sy : sz);
-    const int g = threadIdx.x / T, t = threadIdx.x % T;
-    const bool active = g < X::LINES;
-    float2* ex = sm + g * X::EX;
-    const int ya = row0 + 2 * g, yb = ya + 1;
-    const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x & 31) / T * T));
-    if (active) {
-        float2 v[E];
-#pragma unroll
-        for (int j = 0; j < E; j++) {
-            const int x = t + T * j;
-            float a = 0.f, b = 0.f;
-            if (x < c.nx) {
-                if (ya < c.ny) a = __ldg(src + ((size_t)zz * c.ny + ya) * c.nx + x);
-                if (yb < c.ny) b = __ldg(src + ((size_t)zz * c.ny + yb) * c.nx + x);
-            }
-            v[j] = make_float2(a, b);
+    const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + (size_t)zz * c.ny * c.nx;
+    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
+    for (int idx = threadIdx.x; idx < X::L * PX; idx += blockDim.x) {
+        const int l = idx / PX, x = idx % PX;
+        const int ya = row0 + 2 * l, yb = ya + 1;
+        float a = 0.f, b = 0.f;
+        if (x < c.nx) {
+            if (ya < c.ny) a = __ldg(src + (size_t)ya * c.nx + x);
+            if (yb < c.ny) b = __ldg(src + (size_t)yb * c.nx + x);
         }
-        fr::line_fft<PX, -1>(v, ex, t, mask, twl);
-        // stage Z in natural order
-#pragma unroll
-        for (int r = 0; r < E; r++) ex[fr::out_index<PX>(t, r)] = v[r];
+        A[idx] = make_float2(a, b);
     }
     __syncthreads();
+    const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
+    const float2* R = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
     // split the two real rows and store SPEC[kx][comp][zz][row]
     const int rows_here = min(X::ROWS, c.ny - row0);
     for (int idx = threadIdx.x; idx < X::KX * X::ROWS; idx += blockDim.x) {
         const int kx = idx / X::ROWS, row = idx % X::ROWS;
         if (row >= rows_here) continue;
-        const float2* Z = sm + (row >> 1) * X::EX;
+        const float2* Z = R + (row >> 1) * PX;
         const float2 zk = Z[kx], zn = Z[(PX - kx) & (PX - 1)];
         float2 o;
         if ((row & 1) == 0) o = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
@@ -106,84 +97,68 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
                                                  float* __restrict__ hz)
 {
     using X = XCfg<PX>;
-    constexpr int T = X::T, E = X::E, KX = X::KX;
+    constexpr int KX = X::KX;
     extern __shared__ float2 sm[];
-    float2* S = sm;                              // [ROWS][KX] spectra
-    float2* EXB = sm + X::ROWS * KX;             // per-line buffers
-    float2* twl = EXB + X::LINES * X::EX;        // twiddles
-    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
+    float2* A = sm;                 // [L][PX] lines (first the [ROWS][KX] spectra)
+    float2* B = A + X::L * PX;      // [L][PX]
+    float2* twl = B + X::L * PX;    // [PX]
     const int comp = blockIdx.z, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
     const int rows_here = min(X::ROWS, c.ny - row0);
-    float* dst = comp == 0 ? hx : (comp == 1 ? hy : hz);
+    float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + (size_t)zz * c.ny * c.nx;
+    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
+    // spectra of the ROWS rows into B as [row][kx]
     for (int idx = threadIdx.x; idx < KX * X::ROWS; idx += blockDim.x) {
         const int kx = idx / X::ROWS, row = idx % X::ROWS;
         float2 v = make_float2(0.f, 0.f);
         if (row < rows_here) v = spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + row0 + row];
-        S[row * KX + kx] = v;
+        B[row * KX + kx] = v;
     }
     __syncthreads();
-    const int g = threadIdx.x / T, t = threadIdx.x % T;
-    const bool active = g < X::LINES;
-    float2* ex = EXB + g * X::EX;
-    const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x & 31) / T * T));
-    if (active) {
-        const float2* A = S + (2 * g) * KX;
-        const float2* B = S + (2 * g + 1) * KX;
-        float2 v[E];
-#pragma unroll
-        for (int j = 0; j < E; j++) {
-            const int k = t + T * j;
-            float2 a, b;
-            if (k < KX) { a = A[k]; b = B[k]; }
-            else { a = cconj(A[PX - k]); b = cconj(B[PX - k]); }
-            v[j] = make_float2(a.x - b.y, a.y + b.x); // A + iB
-        }
-        fr::line_fft<PX, +1>(v, ex, t, mask, twl);
-#pragma unroll
-        for (int r = 0; r < E; r++) ex[fr::out_index<PX>(t, r)] = v[r];
+    // line l: Z[k] = A_row(2l)[k] + i A_row(2l+1)[k] with Hermitian completion
+    for (int idx = threadIdx.x; idx < X::L * PX; idx += blockDim.x) {
+        const int l = idx / PX, k = idx % PX;
+        const float2* Sa = B + (2 * l) * KX;
+        const float2* Sb = B + (2 * l + 1) * KX;
+        float2 a, b;
+        if (k < KX) { a = Sa[k]; b = Sb[k]; }
+        else { a = cconj(Sa[PX - k]); b = cconj(Sb[PX - k]); }
+        A[idx] = make_float2(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
+    const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
+    const float2* R = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
     for (int idx = threadIdx.x; idx < X::ROWS * c.nx; idx += blockDim.x) {
         const int row = idx / c.nx, x = idx % c.nx;
         if (row >= rows_here) continue;
-        const float2 z = EXB[(row >> 1) * X::EX + x];
-        dst[((size_t)zz * c.ny + row0 + row) * c.nx + x] = (row & 1) ? z.y : z.x;
+        const float2 z = R[(row >> 1) * PX + x];
+        dst[(size_t)(row0 + row) * c.nx + x] = (row & 1) ? z.y : z.x;
     }
 }
 
 // ------------------------------------------------------------------ (y,z) pass
-template <int PY>
-struct YCfg {
-    static constexpr int T = Split<PY>::T;
-    static constexpr int E = Split<PY>::E;
-    static constexpr int EX = E * (T + 1);
-};
-
-// threads of k_yz_fast: 768 (80 registers each), 512 for PY = 512 whose
-// 32-element lanes need more registers
+// One CTA per kx.  y transforms of the 3*nz data lines by TPL threads each
+// (in rounds), z transforms + tensor multiply with one thread per
+// (component, ky) column, inverse y transforms.
 template <int PY>
 struct YZT {
-    static constexpr int N = PY >= 512 ? 512 : 768;
+    static constexpr int N = 768;
 };
 
 template <int PY, int PZ>
-__global__ void __launch_bounds__(YZT<PY>::N, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
-                                                           float2* __restrict__ spec, const float* __restrict__ ten6)
+__global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
+                                                    float2* __restrict__ spec, const float* __restrict__ ten6)
 {
-    using Y = YCfg<PY>;
-    constexpr int YZ_THREADS = YZT<PY>::N;
-    constexpr int T = Y::T, E = Y::E;
+    constexpr int TPL = fr::Tpl<PY>::V;
+    constexpr int LPR = 768 / TPL;   // lines per round
     extern __shared__ float2 sm[];
     const int kx = blockIdx.x;
     const int nz = c.nz, ny = c.ny;
     const int nlines = 3 * nz;
-    const int LIN = min(nlines, YZ_THREADS / T);                 // y lines in flight
-    const int R2 = max(3 * PZ * PY, LIN * Y::EX);
-    float2* P = sm;                          // [3][nz][PY] data rows
-    float2* Q = P + 3 * nz * PY;             // [3][PZ][PY] z spectra (z phase)
-    float2* EXB = Q;                         // [LIN][EX] line buffers (y phases)
-    float2* twl = Q + R2;                    // [PY]
+    float2* P = sm;                          // [3][nz][PY]
+    float2* Pb = P + (size_t)nlines * PY;    // scratch [3][nz][PY]
+    float2* Q = Pb + (size_t)nlines * PY;    // [3][PZ][PY]
+    float2* twl = Q + (size_t)3 * PZ * PY;   // [PY]
     const float* Tk = ten6 + (size_t)kx * PZ * PY * 6;
     if (threadIdx.x == 0) {
         // pull this kx's tensor chunk into L2 while the y transforms run
@@ -192,44 +167,33 @@ __global__ void __launch_bounds__(YZT<PY>::N, 1) k_yz_fast(ConvK c, const float2
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tk), "r"(bytes) : "memory");
     }
     for (int k = threadIdx.x; k < PY; k += blockDim.x) twl[k] = twy[k];
-    __syncthreads();
-    float2* sp = spec + (size_t)kx * 3 * nz * ny;
-    const int g = threadIdx.x / T, t = threadIdx.x % T;
-    const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << ((threadIdx.x & 31) / T * T));
-    // forward y FFT of every data line (c, z)
-    for (int l0 = 0; l0 < nlines; l0 += LIN) {
-        const int l = l0 + g;
-        if (g < LIN && l < nlines) {
-            const float2* in = sp + (size_t)l * ny;
-            float2 v[E];
-#pragma unroll
-            for (int j = 0; j < E; j++) {
-                const int y = t + T * j;
-                v[j] = y < ny ? in[y] : make_float2(0.f, 0.f);
-            }
-            fr::line_fft<PY, -1>(v, EXB + g * Y::EX, t, mask, twl);
-            float2* out = P + (size_t)l * PY;
-#pragma unroll
-            for (int r = 0; r < E; r++) out[fr::out_index<PY>(t, r)] = v[r];
-        }
+    float2* sp = spec + (size_t)kx * nlines * ny;
+    for (int idx = threadIdx.x; idx < nlines * PY; idx += blockDim.x) {
+        const int l = idx / PY, y = idx % PY;
+        P[idx] = y < ny ? sp[(size_t)l * ny + y] : make_float2(0.f, 0.f);
     }
     __syncthreads();
+    const int lr = threadIdx.x / TPL, tl = threadIdx.x % TPL;
+    float2* Y = P;
+    for (int l0 = 0; l0 < nlines; l0 += LPR) {
+        const int l = l0 + lr;
+        Y = fr::sm_fft<PY, -1, TPL>(P, Pb, l < nlines ? l : 0, tl, twl, l < nlines);
+    }
     // forward z FFT: one (component, ky) column per thread
     for (int w = threadIdx.x; w < 3 * PY; w += blockDim.x) {
         const int a = w / PY, ky = w % PY;
         float2 s[PZ];
 #pragma unroll
-        for (int z = 0; z < PZ; z++) s[z] = z < nz ? P[((size_t)a * nz + z) * PY + ky] : make_float2(0.f, 0.f);
+        for (int z = 0; z < PZ; z++) s[z] = z < nz ? Y[((size_t)a * nz + z) * PY + ky] : make_float2(0.f, 0.f);
         fr::RegFFT<PZ, -1, float2>::run(s);
 #pragma unroll
         for (int z = 0; z < PZ; z++) Q[((size_t)a * PZ + z) * PY + ky] = s[z];
     }
     __syncthreads();
-    // tensor multiply (row a of the symmetric tensor) and inverse z FFT
+    // tensor multiply (row a of the symmetric tensor) and inverse z FFT into P
     const float gg = c.g;
     for (int w = threadIdx.x; w < 3 * PY; w += blockDim.x) {
         const int a = w / PY, ky = w % PY;
-        // row a of [[0,1,2],[1,3,4],[2,4,5]]
         const int i0 = a == 0 ? 0 : (a == 1 ? 1 : 2);
         const int i1 = a == 0 ? 1 : (a == 1 ? 3 : 4);
         const int i2 = a == 0 ? 2 : (a == 1 ? 4 : 5);
@@ -247,22 +211,14 @@ __global__ void __launch_bounds__(YZT<PY>::N, 1) k_yz_fast(ConvK c, const float2
             if (z < nz) P[((size_t)a * nz + z) * PY + ky] = h[z];
     }
     __syncthreads();
-    // inverse y FFT, store the data rows
-    for (int l0 = 0; l0 < nlines; l0 += LIN) {
-        const int l = l0 + g;
-        if (g < LIN && l < nlines) {
-            const float2* in = P + (size_t)l * PY;
-            float2 v[E];
-#pragma unroll
-            for (int j = 0; j < E; j++) v[j] = in[t + T * j];
-            fr::line_fft<PY, +1>(v, EXB + g * Y::EX, t, mask, twl);
-            float2* out = sp + (size_t)l * ny;
-#pragma unroll
-            for (int r = 0; r < E; r++) {
-                const int y = fr::out_index<PY>(t, r);
-                if (y < ny) out[y] = v[r];
-            }
-        }
+    // inverse y FFT
+    for (int l0 = 0; l0 < nlines; l0 += LPR) {
+        const int l = l0 + lr;
+        Y = fr::sm_fft<PY, +1, TPL>(P, Pb, l < nlines ? l : 0, tl, twl, l < nlines);
+    }
+    for (int idx = threadIdx.x; idx < nlines * ny; idx += blockDim.x) {
+        const int l = idx / ny, y = idx % ny;
+        sp[idx] = Y[(size_t)l * PY + y];
     }
 }
 
@@ -352,8 +308,17 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
         if (HL2 > 0.f) {
             const float iHL = rsqrtf(HL2);
             const float HL = HL2 * iHL;
+            // half rotation angle; small angles by their Taylor series
+            // (|th| <= 0.1: truncation below 1e-10), else sincosf
+            const float th = F.c_rot * HL;
             float sn, cs;
-            sincosf(F.c_rot * HL, &sn, &cs);
+            if (fabsf(th) <= 0.1f) {
+                const float t2 = th * th;
+                sn = th * (1.0f - t2 * (1.0f / 6.0f) * (1.0f - t2 * (1.0f / 20.0f) * (1.0f - t2 * (1.0f / 42.0f))));
+                cs = 1.0f - t2 * 0.5f * (1.0f - t2 * (1.0f / 12.0f) * (1.0f - t2 * (1.0f / 30.0f) * (1.0f - t2 * (1.0f / 56.0f))));
+            } else {
+                sincosf(th, &sn, &cs);
+            }
             const float qw = cs, qx = sn * Hpx * iHL, qy = sn * Hpy * iHL, qz = sn * Hpz * iHL;
             const float tw = -qx * Sx - qy * Sy - qz * Sz;
             const float tx = qw * Sx + qy * Sz - qz * Sy;
@@ -379,15 +344,10 @@ namespace mlb {
 
 static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
-// shared memory of k_yz_fast: data rows, z spectra, line buffers, twiddles
+// shared memory of k_yz_fast: data rows and scratch, z spectra, twiddles
 static size_t yz_fast_smem(int PY, int PZ, int nz)
 {
-    const int T = PY <= 4 ? 1 : (PY <= 32 ? (PY <= 8 ? 2 : 4) : (PY <= 128 ? 8 : 16));
-    const int E = PY / T;
-    const int threads = PY >= 512 ? 512 : 768;
-    const int lines = std::min(3 * nz, threads / T);
-    const size_t r2 = std::max((size_t)3 * PZ * PY, (size_t)lines * E * (T + 1));
-    return ((size_t)3 * nz * PY + r2 + PY) * sizeof(float2);
+    return ((size_t)2 * 3 * nz * PY + (size_t)3 * PZ * PY + PY) * sizeof(float2);
 }
 
 bool conv_fast_ok(const ConvK& c)
@@ -402,13 +362,12 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
 {
     using X = XCfg<PX>;
     dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3);
+    const size_t smem = ((size_t)2 * X::L * PX + PX) * sizeof(float2);
     if (fwd) {
-        const size_t smem = ((size_t)X::LINES * X::EX + PX) * sizeof(float2);
         static bool cfg = false;
         if (!cfg) { cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
         k_fx_fast<PX><<<grid, 256, smem, st>>>(c, tw, s[0], s[1], s[2], spec);
     } else {
-        const size_t smem = ((size_t)X::ROWS * X::KX + (size_t)X::LINES * X::EX + PX) * sizeof(float2);
         static bool cfg = false;
         if (!cfg) { cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
         k_ix_fast<PX><<<grid, 256, smem, st>>>(c, tw, spec, h[0], h[1], h[2]);
