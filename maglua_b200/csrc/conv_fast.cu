@@ -41,13 +41,20 @@ using fr::Split;
 // ------------------------------------------------------------------ x passes
 // A CTA of 256 threads transforms L = 256/TPL complex lines; line l packs
 // rows (row0 + 2l, row0 + 2l + 1) of one component of one layer as real and
-// imaginary parts.
+// imaginary parts.  Global loads are gathered into registers in unrolled
+// batches before they are written to shared memory, so each thread has all
+// its loads in flight at once.
 template <int PX>
 struct XCfg {
+    static constexpr int NT = 256;
     static constexpr int TPL = fr::Tpl<PX>::V;
-    static constexpr int L = 256 / TPL;
+    static constexpr int L = NT / TPL;
     static constexpr int ROWS = 2 * L;
     static constexpr int KX = PX / 2 + 1;
+    static constexpr int LINE = L * PX;                        // line buffer
+    static constexpr int SPEC = ROWS * KX;                     // [ROWS][KX] staging
+    static constexpr int BUF = LINE > SPEC ? LINE : SPEC;      // each of A, B
+    static constexpr int SMEM = (PX + 2 * BUF) * 8;            // bytes
 };
 
 template <int PX>
@@ -56,32 +63,45 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
                                                  float2* __restrict__ spec)
 {
     using X = XCfg<PX>;
+    constexpr int NT = X::NT;
     extern __shared__ float2 sm[];
-    float2* A = sm;                 // [L][PX]
-    float2* B = A + X::L * PX;      // [L][PX]
-    float2* twl = B + X::L * PX;    // [PX]
+    float2* twl = sm;               // [PX]
+    float2* A = twl + PX;           // [L][PX]
+    float2* B = A + X::BUF;         // [L][PX]
     const int comp = blockIdx.z, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
     const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + (size_t)zz * c.ny * c.nx;
-    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
-    for (int idx = threadIdx.x; idx < X::L * PX; idx += blockDim.x) {
+    for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
+    constexpr int IT = (X::LINE + NT - 1) / NT;
+    float2 v[IT];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int idx = threadIdx.x + it * NT;
         const int l = idx / PX, x = idx % PX;
         const int ya = row0 + 2 * l, yb = ya + 1;
         float a = 0.f, b = 0.f;
-        if (x < c.nx) {
+        if (idx < X::LINE && x < c.nx) {
             if (ya < c.ny) a = __ldg(src + (size_t)ya * c.nx + x);
             if (yb < c.ny) b = __ldg(src + (size_t)yb * c.nx + x);
         }
-        A[idx] = make_float2(a, b);
+        v[it] = make_float2(a, b);
+    }
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int idx = threadIdx.x + it * NT;
+        if (idx < X::LINE) A[idx] = v[it];
     }
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
     const float2* R = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
     // split the two real rows and store SPEC[kx][comp][zz][row]
     const int rows_here = min(X::ROWS, c.ny - row0);
-    for (int idx = threadIdx.x; idx < X::KX * X::ROWS; idx += blockDim.x) {
+    constexpr int IS = (X::SPEC + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < IS; it++) {
+        const int idx = threadIdx.x + it * NT;
         const int kx = idx / X::ROWS, row = idx % X::ROWS;
-        if (row >= rows_here) continue;
+        if (idx >= X::SPEC || row >= rows_here) continue;
         const float2* Z = R + (row >> 1) * PX;
         const float2 zk = Z[kx], zn = Z[(PX - kx) & (PX - 1)];
         float2 o;
@@ -97,26 +117,41 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
                                                  float* __restrict__ hz)
 {
     using X = XCfg<PX>;
-    constexpr int KX = X::KX;
+    constexpr int KX = X::KX, NT = X::NT;
     extern __shared__ float2 sm[];
-    float2* A = sm;                 // [L][PX] lines (first the [ROWS][KX] spectra)
-    float2* B = A + X::L * PX;      // [L][PX]
-    float2* twl = B + X::L * PX;    // [PX]
+    float2* twl = sm;               // [PX]
+    float2* A = twl + PX;           // [L][PX] lines
+    float2* B = A + X::BUF;         // [ROWS][KX] spectra, then scratch
     const int comp = blockIdx.z, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
     const int rows_here = min(X::ROWS, c.ny - row0);
     float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + (size_t)zz * c.ny * c.nx;
-    for (int k = threadIdx.x; k < PX; k += blockDim.x) twl[k] = tw[k];
-    // spectra of the ROWS rows into B as [row][kx]
-    for (int idx = threadIdx.x; idx < KX * X::ROWS; idx += blockDim.x) {
-        const int kx = idx / X::ROWS, row = idx % X::ROWS;
-        float2 v = make_float2(0.f, 0.f);
-        if (row < rows_here) v = spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + row0 + row];
-        B[row * KX + kx] = v;
+    for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
+    constexpr int IS = (X::SPEC + NT - 1) / NT;
+    {
+        float2 v[IS];
+#pragma unroll
+        for (int it = 0; it < IS; it++) {
+            const int idx = threadIdx.x + it * NT;
+            const int kx = idx / X::ROWS, row = idx % X::ROWS;
+            v[it] = make_float2(0.f, 0.f);
+            if (idx < X::SPEC && row < rows_here)
+                v[it] = spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + row0 + row];
+        }
+#pragma unroll
+        for (int it = 0; it < IS; it++) {
+            const int idx = threadIdx.x + it * NT;
+            const int kx = idx / X::ROWS, row = idx % X::ROWS;
+            if (idx < X::SPEC) B[row * KX + kx] = v[it];
+        }
     }
     __syncthreads();
-    // line l: Z[k] = A_row(2l)[k] + i A_row(2l+1)[k] with Hermitian completion
-    for (int idx = threadIdx.x; idx < X::L * PX; idx += blockDim.x) {
+    // line l: Z[k] = S_row(2l)[k] + i S_row(2l+1)[k] with Hermitian completion
+    constexpr int IL = (X::LINE + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < IL; it++) {
+        const int idx = threadIdx.x + it * NT;
+        if (idx >= X::LINE) continue;
         const int l = idx / PX, k = idx % PX;
         const float2* Sa = B + (2 * l) * KX;
         const float2* Sb = B + (2 * l + 1) * KX;
@@ -128,9 +163,12 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
     const float2* R = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
-    for (int idx = threadIdx.x; idx < X::ROWS * c.nx; idx += blockDim.x) {
-        const int row = idx / c.nx, x = idx % c.nx;
-        if (row >= rows_here) continue;
+    constexpr int IO = (X::ROWS * PX + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < IO; it++) {
+        const int idx = threadIdx.x + it * NT;
+        const int row = idx / PX, x = idx % PX;
+        if (idx >= X::ROWS * PX || row >= rows_here || x >= c.nx) continue;
         const float2 z = R[(row >> 1) * PX + x];
         dst[(size_t)(row0 + row) * c.nx + x] = (row & 1) ? z.y : z.x;
     }
@@ -168,9 +206,21 @@ __global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __res
     }
     for (int k = threadIdx.x; k < PY; k += blockDim.x) twl[k] = twy[k];
     float2* sp = spec + (size_t)kx * nlines * ny;
-    for (int idx = threadIdx.x; idx < nlines * PY; idx += blockDim.x) {
-        const int l = idx / PY, y = idx % PY;
-        P[idx] = y < ny ? sp[(size_t)l * ny + y] : make_float2(0.f, 0.f);
+    {
+        // at most 3*PZ*PY elements (nz <= PZ): unrolled gather, then store
+        constexpr int IG = (3 * PZ * PY + 767) / 768;
+        float2 v[IG];
+#pragma unroll
+        for (int it = 0; it < IG; it++) {
+            const int idx = threadIdx.x + it * 768;
+            const int l = idx / PY, y = idx % PY;
+            v[it] = (l < nlines && y < ny) ? sp[(size_t)l * ny + y] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int it = 0; it < IG; it++) {
+            const int idx = threadIdx.x + it * 768;
+            if (idx < nlines * PY) P[idx] = v[it];
+        }
     }
     __syncthreads();
     const int lr = threadIdx.x / TPL, tl = threadIdx.x % TPL;
@@ -216,9 +266,14 @@ __global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __res
         const int l = l0 + lr;
         Y = fr::sm_fft<PY, +1, TPL>(P, Pb, l < nlines ? l : 0, tl, twl, l < nlines);
     }
-    for (int idx = threadIdx.x; idx < nlines * ny; idx += blockDim.x) {
-        const int l = idx / ny, y = idx % ny;
-        sp[idx] = Y[(size_t)l * PY + y];
+    {
+        constexpr int IG = (3 * PZ * PY + 767) / 768;
+#pragma unroll
+        for (int it = 0; it < IG; it++) {
+            const int idx = threadIdx.x + it * 768;
+            const int l = idx / PY, y = idx % PY;
+            if (l < nlines && y < ny) sp[(size_t)l * ny + y] = Y[idx];
+        }
     }
 }
 
@@ -362,7 +417,7 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
 {
     using X = XCfg<PX>;
     dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3);
-    const size_t smem = ((size_t)2 * X::L * PX + PX) * sizeof(float2);
+    const size_t smem = X::SMEM;
     if (fwd) {
         static bool cfg = false;
         if (!cfg) { cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
