@@ -202,6 +202,21 @@ int mlb_llg_set_flags(mlb_llg* l, int thermal_only_first_term, int disable_renor
 int mlb_llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb_system* to,
                   int advance);
 
+/* ---------------------------------------------------------------- plans
+ * B200 extension (the reference steps from Lua, one operator call at a time):
+ * a plan captures the canonical step of a system (resetFields; each op's
+ * apply; sumFields; llg:apply) as CUDA graphs so that one host call
+ * enqueues a whole step.  The Thermal counter and the applied field (with
+ * its sweep) advance on the device; any other parameter change makes the
+ * next launch capture again.  With timing set, every kernel of the step is
+ * bracketed by graph event nodes and mlb_plan_kernel_times returns the
+ * milliseconds of the last launched step per kernel (48-byte name slots). */
+typedef struct mlb_plan mlb_plan;
+int mlb_plan_create(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int timing, mlb_plan** out);
+int mlb_plan_launch(mlb_plan* p, int nsteps);
+int mlb_plan_kernel_times(mlb_plan* p, int cap, char* names, double* ms, int* count);
+int mlb_plan_destroy(mlb_plan* p);
+
 /* ---------------------------------------------------------------- fused run
  * B200 extension: nsteps repetitions of the canonical script step
  * (doc/manual/BasicMicromagneticSimulation.lua:84-94):

@@ -116,6 +116,10 @@ _SIGS = {
     "mlb_llg_set_flags": ([_P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
     "mlb_llg_apply": ([_P, _P, C.c_double, _P, _P, C.c_int], C.c_int),
     "mlb_run": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int], C.c_int),
+    "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_plan_launch": ([_P, C.c_int], C.c_int),
+    "mlb_plan_kernel_times": ([_P, C.c_int, C.c_char_p, _D, _I], C.c_int),
+    "mlb_plan_destroy": ([_P], C.c_int),
 }
 EXPORTED = tuple(_SIGS)
 
@@ -952,6 +956,44 @@ class profile:
             nm = raw[48 * k:48 * (k + 1)].split(b"\0", 1)[0].decode()
             self.kernels[nm] = (float(ms[k]), int(nl[k]))
         return False
+
+
+class Plan:
+    """The canonical step of ss (resetFields; op.apply for op in ops;
+    sumFields; llg.apply) captured as CUDA graphs; launch(n) runs n steps with
+    one graph launch each.  timing=True adds event nodes around every kernel
+    (kernelTimes() -> {name: ms} of the last launched step)."""
+
+    def __init__(self, ss, ops, llg, timing=False):
+        self._keep = (ss, list(ops), llg)
+        arr = (_P * len(ops))(*[o._h for o in ops])
+        h = _P()
+        _ck(_lib.mlb_plan_create(ss._h, arr, len(ops), llg._h, int(bool(timing)), C.byref(h)))
+        self._h = h
+
+    def launch(self, nsteps=1):
+        _ck(_lib.mlb_plan_launch(self._h, int(nsteps)))
+
+    def kernelTimes(self):
+        cap = 32
+        names = C.create_string_buffer(48 * cap)
+        ms = np.zeros(cap)
+        cnt = C.c_int()
+        _ck(_lib.mlb_plan_kernel_times(self._h, cap, names, _dp(ms), C.byref(cnt)))
+        out = {}
+        raw = names.raw
+        for k in range(cnt.value):
+            nm = raw[48 * k:48 * (k + 1)].split(b"\0", 1)[0].decode()
+            out[nm] = out.get(nm, 0.0) + float(ms[k])
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_plan_destroy(h)
+            self._h = None
+
+    close = __del__
 
 
 def run(ss, ops, llg, nsteps):

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -201,11 +202,12 @@ struct mlb_system {
     std::vector<Slot> slots;
     cudaStream_t own = nullptr;
     cudaStream_t st = nullptr;
-    uint64_t* dctr = nullptr;
+    DevStep* dstep = nullptr;       // device step block (captured steps)
     double* red = nullptr;
     double* redout = nullptr;
     int red_nb = 1;
     bool capturing = false;
+    bool dry = false;               // replay host bookkeeping without launching
     bool last_fused = false;
 };
 
@@ -265,9 +267,25 @@ struct mlb_llg {
     double precess = 1.0, damp = 1.0;
 };
 
+// A captured step (two graphs, one per spin-buffer parity).
+struct mlb_plan {
+    mlb_system* s = nullptr;
+    std::vector<mlb_op*> ops;
+    mlb_llg* l = nullptr;
+    bool timing = false;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    std::vector<mlb::ProfCaptured> ev[2];
+    std::vector<mlb::ProfCaptured>* last = nullptr;
+    unsigned long long version = 0;
+};
+
 namespace {
 
 std::set<mlb_system*> g_systems;
+// bumped by every parameter setter; a plan captured under an older value
+// is captured again before its next launch
+unsigned long long g_version = 1;
+using mlb::ProfCaptured;
 
 // ------------------------------------------------------------------ system helpers
 int slot_find(const mlb_system* s, const char* name)
@@ -676,17 +694,15 @@ bool terms_add(TermsK& T, const Term& t, bool th_sub, mlb_system* s, bool captur
         T.th.T = (float)(t.T * t.gs);
         T.th.scale = op->tscale.empty() ? nullptr : op->dscale.p;
         T.th.seed = op->seed;
-        T.th.counter = t.counter;
-        T.th.dctr = capture ? s->dctr : nullptr;
+        // captured steps read the counter from the device step block
+        T.th.counter = capture ? 0 : t.counter;
+        T.th.dctr = capture ? &s->dstep->th_counter : nullptr;
         return true;
     case MLB_OP_APPLIEDFIELD:
         if (T.zee.on) return false;
         T.zee.on = 1;
-        for (int a = 0; a < 3; a++) {
-            T.zee.B[a] = t.B[a];
-            T.zee.dB[a] = (float)(op->dB[a] * op->gs);
-        }
-        T.zee.dctr = capture ? s->dctr : nullptr;
+        for (int a = 0; a < 3; a++) T.zee.B[a] = t.B[a];
+        T.zee.Bdev = capture ? s->dstep->B : nullptr;
         return true;
     }
     return false;
@@ -946,6 +962,8 @@ void op_apply(mlb_op* op, mlb_system* s)
         slot_alloc(s, sl);
         ConvPlan& P = *op->plan;
         P.k.g = (float)(op->g * op->gs / ((double)P.k.Px * P.k.Py * P.k.Pz));
+        sl.state = ST_DATA;
+        if (s->dry) return;
         const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
         if (mlb::conv_fast_ok(P.k))
             CK(mlb::launch_conv_fast(P.k, P.L, P.tw.p, sp, P.spec.p, P.ten6.p, sl.h, s->st));
@@ -1001,8 +1019,8 @@ bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, dou
         F.seed = T.th.seed; F.counter = T.th.counter; F.dctr = T.th.dctr;
     }
     if (T.zee.on) {
-        for (int c = 0; c < 3; c++) { F.B[c] = T.zee.B[c]; F.dB[c] = T.zee.dB[c]; }
-        F.zdctr = T.zee.dctr;
+        for (int c = 0; c < 3; c++) F.B[c] = T.zee.B[c];
+        F.Bdev = T.zee.Bdev;
     }
     F.addw = T.nadd == 1 ? T.addw[0] : 0.f;
     F.llg_type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
@@ -1053,7 +1071,9 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
     }
     const int nb = 1 - s->cur;
     FastK F;
-    if (fast_fused(s, T, l, dt, dt_sys, F)) {
+    if (s->dry) {
+        // bookkeeping only: the kernels of this step ran in a captured graph
+    } else if (fast_fused(s, T, l, dt, dt_sys, F)) {
         const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
         const float* ad[3] = {nullptr, nullptr, nullptr};
         if (T.nadd == 1) for (int c = 0; c < 3; c++) ad[c] = T.add[0][c];
@@ -1067,7 +1087,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
         CK(mlb::launch_fused(P, (float)dt_sys, s->st));
     }
-    if (s->capturing) CK(mlb::launch_advance(s->dctr, s->st));
+    if (s->capturing) CK(mlb::launch_advance_step(s->dstep, s->st));
     s->cur = nb;
     s->gen++;
     return true;
@@ -1162,8 +1182,8 @@ mlb_system* make_system(int nx, int ny, int nz)
     CK(cudaMemset(s->ms, 0, sizeof(float) * n));
     s->ms_host.assign(n, 0.f);
     s->ms_dirty = true;
-    CK(cudaMalloc(&s->dctr, sizeof(uint64_t)));
-    CK(cudaMemset(s->dctr, 0, sizeof(uint64_t)));
+    CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
+    CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
     s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
     CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
     CK(cudaMalloc(&s->redout, sizeof(double) * 8));
@@ -1183,7 +1203,7 @@ void free_system(mlb_system* s)
     cudaFree(s->ms);
     cudaFree(s->sa);
     cudaFree(s->sg);
-    cudaFree(s->dctr);
+    cudaFree(s->dstep);
     cudaFree(s->red);
     cudaFree(s->redout);
     for (Slot& x : s->slots)
@@ -1213,6 +1233,161 @@ void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
     for (int i = 0; i < nops; i++) op_apply(ops[i], s);
     sum_fields(s);
     llg_apply(l, s, 1.0, s, s, 1);
+}
+
+void advance_sweep(mlb_op* const* ops, int nops)
+{
+    for (int i = 0; i < nops; i++)
+        if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
+            for (int a = 0; a < 3; a++) ops[i]->B[a] += ops[i]->dB[a];
+}
+
+struct HostState {
+    int cur;
+    long long gen;
+    double time;
+    std::vector<Slot> slots;
+    std::vector<uint64_t> ctr;
+    std::vector<std::array<double, 3>> B;
+    bool last_fused;
+};
+
+HostState save_state(mlb_system* s, const std::vector<mlb_op*>& ops)
+{
+    HostState h;
+    h.cur = s->cur; h.gen = s->gen; h.time = s->time; h.slots = s->slots; h.last_fused = s->last_fused;
+    for (mlb_op* o : ops) {
+        h.ctr.push_back(o->counter);
+        h.B.push_back({o->B[0], o->B[1], o->B[2]});
+    }
+    return h;
+}
+
+void load_state(mlb_system* s, const std::vector<mlb_op*>& ops, const HostState& h)
+{
+    s->cur = h.cur; s->gen = h.gen; s->time = h.time; s->slots = h.slots; s->last_fused = h.last_fused;
+    for (size_t i = 0; i < ops.size(); i++) {
+        ops[i]->counter = h.ctr[i];
+        for (int a = 0; a < 3; a++) ops[i]->B[a] = h.B[i][a];
+    }
+}
+
+void plan_release(mlb_plan* p)
+{
+    for (int q = 0; q < 2; q++) {
+        if (p->exec[q]) cudaGraphExecDestroy(p->exec[q]);
+        p->exec[q] = nullptr;
+        for (ProfCaptured& r : p->ev[q]) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        p->ev[q].clear();
+    }
+    p->last = nullptr;
+}
+
+// Capture one step for each spin-buffer parity.  A dry pass first runs the
+// host logic (compiling operators, building tensor spectra, allocating
+// slots) so that the captured pass only enqueues kernels.
+void plan_capture(mlb_plan* p)
+{
+    mlb_system* s = p->s;
+    const int nops = (int)p->ops.size();
+    for (mlb_op* o : p->ops) {
+        check_dims(o, s);
+        if (o->kind == MLB_OP_THERMAL && o->inject_pending) fail(MLB_ESTATE, "injected noise cannot be replayed");
+    }
+    int nth = 0, nz = 0;
+    for (mlb_op* o : p->ops) { nth += o->kind == MLB_OP_THERMAL; nz += o->kind == MLB_OP_APPLIEDFIELD; }
+    if (nth > 1 || nz > 1) fail(MLB_ESTATE, "a captured step holds at most one Thermal and one AppliedField");
+    plan_release(p);
+    const HostState h0 = save_state(s, p->ops);
+    try {
+        s->dry = true;
+        do_step(s, p->ops.data(), nops, p->l);
+        s->dry = false;
+        if (!s->last_fused) fail(MLB_ESTATE, "step is not fusable");
+        load_state(s, p->ops, h0);
+        CK(cudaStreamSynchronize(s->st));
+        for (int q = 0; q < 2; q++) {
+            s->cur = q;
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+            s->capturing = true;
+            if (p->timing) mlb::prof_set_capture_sink(&p->ev[q]);
+            bool ok = true;
+            std::string why;
+            try {
+                do_step(s, p->ops.data(), nops, p->l);
+            } catch (Err& e) {
+                ok = false;
+                why = e.msg;
+            }
+            mlb::prof_set_capture_sink(nullptr);
+            s->capturing = false;
+            cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+            if (!ok || e != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                fail(MLB_ESTATE, "step capture failed: " + (ok ? std::string(cudaGetErrorString(e)) : why));
+            }
+            e = cudaGraphInstantiate(&p->exec[q], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) fail(MLB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            load_state(s, p->ops, h0);
+        }
+    } catch (...) {
+        s->dry = false;
+        s->capturing = false;
+        mlb::prof_set_capture_sink(nullptr);
+        load_state(s, p->ops, h0);
+        throw;
+    }
+    p->version = g_version;
+}
+
+void advance_host(mlb_plan* p)
+{
+    mlb_system* s = p->s;
+    const double dt = s->dt;
+    for (mlb_op* o : p->ops)
+        if (o->kind == MLB_OP_THERMAL) o->counter++;
+    s->cur = 1 - s->cur;
+    s->gen++;
+    const bool cart = p->l->kind != MLB_LLG_QUATERNION;
+    if (!cart || dt != 0.0) s->time = s->time + dt;
+}
+
+// nsteps captured steps; the host state and lazy field records end as after
+// nsteps canonical script steps.
+void plan_launch(mlb_plan* p, int nsteps)
+{
+    if (nsteps <= 0) return;
+    mlb_system* s = p->s;
+    if (p->version != g_version) plan_capture(p);
+    DevStep h;
+    memset(&h, 0, sizeof(h));
+    for (mlb_op* o : p->ops) {
+        if (o->kind == MLB_OP_THERMAL) h.th_counter = o->counter;
+        if (o->kind == MLB_OP_APPLIEDFIELD)
+            for (int a = 0; a < 3; a++) { h.B[a] = (float)(o->B[a] * o->gs); h.dB[a] = (float)(o->dB[a] * o->gs); }
+    }
+    CK(cudaMemcpyAsync(s->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
+    for (int k = 0; k < nsteps; k++) {
+        CK(cudaGraphLaunch(p->exec[s->cur], s->st));
+        p->last = &p->ev[s->cur];
+        if (k < nsteps - 1) {
+            advance_host(p);
+            advance_sweep(p->ops.data(), (int)p->ops.size());
+        }
+    }
+    // the last step once more without launching: lazy field records
+    s->dry = true;
+    try {
+        do_step(s, p->ops.data(), (int)p->ops.size(), p->l);
+    } catch (...) {
+        s->dry = false;
+        throw;
+    }
+    s->dry = false;
+    advance_sweep(p->ops.data(), (int)p->ops.size());
 }
 
 } // namespace
@@ -1247,6 +1422,7 @@ int mlb_init(int device)
         CK(cudaFree(0));
         CK(mlb::conv_configure());
         CK(mlb::fftreg_init());
+        CK(mlb::conv_fast_configure());
     });
 }
 
@@ -1260,7 +1436,8 @@ int mlb_system_create(int nx, int ny, int nz, mlb_system** out)
 
 int mlb_system_destroy(mlb_system* s)
 {
-    return guard([&] { free_system(s); });
+    return guard([&] {
+        g_version++; free_system(s); });
 }
 
 int mlb_system_dims(const mlb_system* s, int out[3])
@@ -1273,6 +1450,7 @@ int mlb_system_dims(const mlb_system* s, int out[3])
 int mlb_system_set_stream(mlb_system* s, void* stream)
 {
     return guard([&] {
+        g_version++;
         CK(cudaStreamSynchronize(s->st));
         s->st = stream ? (cudaStream_t)stream : s->own;
     });
@@ -1291,6 +1469,7 @@ int mlb_system_synchronize(mlb_system* s)
 int mlb_system_set_spin(mlb_system* s, int idx, double sx, double sy, double sz)
 {
     return guard([&] {
+        g_version++;
         if (idx < 0 || idx >= s->n) fail(MLB_ERANGE, "site outside the SpinSystem");
         spins_changing(s);
         const float v[3] = {(float)sx, (float)sy, (float)sz};
@@ -1318,6 +1497,7 @@ int mlb_system_get_spin(mlb_system* s, int idx, double out4[4])
 int mlb_system_set_spins(mlb_system* s, const double* x, const double* y, const double* z, const double* ms)
 {
     return guard([&] {
+        g_version++;
         if (!x || !y || !z) fail(MLB_EINVAL, "null spin array");
         spins_changing(s);
         std::vector<float> f[3];
@@ -1354,6 +1534,7 @@ int mlb_system_get_spins(mlb_system* s, double* x, double* y, double* z, double*
 int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const float* z, const float* ms)
 {
     return guard([&] {
+        g_version++;
         spins_changing(s);
         const float* src[3] = {x, y, z};
         for (int c = 0; c < 3; c++)
@@ -1380,6 +1561,7 @@ int mlb_system_download_f32(mlb_system* s, float* x, float* y, float* z)
 int mlb_system_set_param(mlb_system* s, int which, double v)
 {
     return guard([&] {
+        g_version++;
         switch (which) {
         case MLB_ALPHA:
             // setAlpha drops per-site values (SpinSystem::setAlpha :1003-1008)
@@ -1412,12 +1594,14 @@ int mlb_system_get_param(const mlb_system* s, int which, double* v)
 
 int mlb_system_set_site_alpha(mlb_system* s, const double* a)
 {
-    return guard([&] { upload_site_array(s, &s->sa, a); });
+    return guard([&] {
+        g_version++; upload_site_array(s, &s->sa, a); });
 }
 
 int mlb_system_set_site_gamma(mlb_system* s, const double* g)
 {
-    return guard([&] { upload_site_array(s, &s->sg, g); });
+    return guard([&] {
+        g_version++; upload_site_array(s, &s->sg, g); });
 }
 
 int mlb_system_reset_fields(mlb_system* s)
@@ -1493,6 +1677,7 @@ int mlb_system_get_field(mlb_system* s, const char* slot, double* hx, double* hy
 int mlb_system_set_field(mlb_system* s, const char* slot, const double* hx, const double* hy, const double* hz)
 {
     return guard([&] {
+        g_version++;
         const int j = slot_register(s, slot);
         before_mutate(s, j);
         materialize(s, j);
@@ -1562,6 +1747,7 @@ int mlb_system_field_dot(mlb_system* s, const char* slot, double* out)
 int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
 {
     return guard([&] {
+        g_version++;
         if (dst->nx != src->nx || dst->ny != src->ny || dst->nz != src->nz) fail(MLB_EINVAL, "size mismatch");
         if (dst == src) return;
         spins_changing(dst);
@@ -1630,6 +1816,7 @@ int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out)
 int mlb_op_destroy(mlb_op* op)
 {
     return guard([&] {
+        g_version++;
         if (!op) return;
         materialize_users(op);
         cudaDeviceSynchronize();
@@ -1642,6 +1829,7 @@ int mlb_op_kind(const mlb_op* op, int* kind) { return guard([&] { *kind = op->ki
 int mlb_op_set_scale(mlb_op* op, double gs)
 {
     return guard([&] {
+        g_version++;
         materialize_users(op);
         op->gs = gs;
     });
@@ -1652,6 +1840,7 @@ int mlb_op_get_scale(const mlb_op* op, double* gs) { return guard([&] { *gs = op
 int mlb_op_set_slot_name(mlb_op* op, const char* name)
 {
     return guard([&] {
+        g_version++;
         if (!name || !*name) fail(MLB_EINVAL, "empty slot name");
         op->slot = name;
     });
@@ -1668,6 +1857,7 @@ int mlb_op_get_slot_name(const mlb_op* op, char* buf, size_t len)
 int mlb_op_set_quirks(mlb_op* op, int on)
 {
     return guard([&] {
+        g_version++;
         materialize_users(op);
         op->quirks = on != 0;
         op->a_dirty = true;
@@ -1690,6 +1880,7 @@ int mlb_op_apply_many(mlb_op* op, mlb_system* const* s, int n)
 int mlb_exchange_add_path(mlb_op* op, int from, int to, double J)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_EXCHANGE) fail(MLB_EINVAL, "not an Exchange operator");
         check_site(op, from);
         check_site(op, to);
@@ -1703,6 +1894,7 @@ int mlb_exchange_add_path(mlb_op* op, int from, int to, double J)
 int mlb_exchange_add_paths(mlb_op* op, const int* from, const int* to, const double* J, int n)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_EXCHANGE) fail(MLB_EINVAL, "not an Exchange operator");
         for (int p = 0; p < n; p++) { check_site(op, from[p]); check_site(op, to[p]); }
         materialize_users(op);
@@ -1717,6 +1909,7 @@ int mlb_exchange_add_paths(mlb_op* op, const int* from, const int* to, const dou
 int mlb_exchange_set_normalize(mlb_op* op, int on)
 {
     return guard([&] {
+        g_version++;
         materialize_users(op);
         op->normalize = on != 0;
         op->ex_dirty = true;
@@ -1728,6 +1921,7 @@ int mlb_exchange_num_paths(const mlb_op* op, int* n) { return guard([&] { *n = (
 int mlb_anisotropy_add(mlb_op* op, int site, const double axis[3], double K)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_ANISOTROPY) fail(MLB_EINVAL, "not an Anisotropy operator");
         check_site(op, site);
         const double len = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
@@ -1743,6 +1937,7 @@ int mlb_anisotropy_add(mlb_op* op, int site, const double axis[3], double K)
 int mlb_uniaxial_add(mlb_op* op, int site, const double axis[3], double K1, double K2)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_UNIAXIAL) fail(MLB_EINVAL, "not an Anisotropy.Uniaxial operator");
         check_site(op, site);
         materialize_users(op);
@@ -1759,6 +1954,7 @@ int mlb_uniaxial_add(mlb_op* op, int site, const double axis[3], double K1, doub
 int mlb_cubic_add(mlb_op* op, int site, const double a1[3], const double a2[3], const double K[3])
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_CUBIC) fail(MLB_EINVAL, "not an Anisotropy.Cubic operator");
         check_site(op, site);
         // axis construction of AnisotropyCubic::addAnisotropy (..._cubic.cpp:180-236)
@@ -1827,6 +2023,7 @@ int mlb_cubic_add_many(mlb_op* op, int n, const int* sites, const double* a1, co
 int mlb_thermal_set_temperature(mlb_op* op, double T)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
         op->T = T;
     });
@@ -1837,6 +2034,7 @@ int mlb_thermal_get_temperature(const mlb_op* op, double* T) { return guard([&] 
 int mlb_thermal_scale_site(mlb_op* op, int idx, double v)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
         const int n = op->nx * op->ny * op->nz;
         if (idx < 0 || idx >= n) return; // scaleSite ignores non-members
@@ -1850,6 +2048,7 @@ int mlb_thermal_scale_site(mlb_op* op, int idx, double v)
 int mlb_thermal_set_seed(mlb_op* op, uint64_t seed)
 {
     return guard([&] {
+        g_version++;
         materialize_users(op);
         op->seed = seed;
     });
@@ -1863,6 +2062,7 @@ int mlb_thermal_set_counter(mlb_op* op, uint64_t counter)
 int mlb_thermal_inject(mlb_op* op, const double* nx, const double* ny, const double* nz)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
         const int n = op->nx * op->ny * op->nz;
         const double* src[3] = {nx, ny, nz};
@@ -1891,12 +2091,14 @@ int mlb_appliedfield_get(const mlb_op* op, double out3[3])
 
 int mlb_appliedfield_set_sweep(mlb_op* op, double dbx, double dby, double dbz)
 {
-    return guard([&] { op->dB[0] = dbx; op->dB[1] = dby; op->dB[2] = dbz; });
+    return guard([&] {
+        g_version++; op->dB[0] = dbx; op->dB[1] = dby; op->dB[2] = dbz; });
 }
 
 int mlb_longrange_set_strength(mlb_op* op, double g)
 {
     return guard([&] {
+        g_version++;
         if (!is_conv(op->kind)) fail(MLB_EINVAL, "not a LongRange operator");
         op->g = g;
     });
@@ -1907,6 +2109,7 @@ int mlb_longrange_get_strength(const mlb_op* op, double* g) { return guard([&] {
 int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4])
 {
     return guard([&] {
+        g_version++;
         for (int i = 0; i < 4; i++) op->gmax[i] = gmax[i];
         if (op->gmax[0] < 0) fail(MLB_EUNSUP, "infinite truncation (extrapolated lattice sum) is not built");
         op->t6_valid = false;
@@ -1918,6 +2121,7 @@ int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4])
 int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9])
 {
     return guard([&] {
+        g_version++;
         for (int i = 0; i < 9; i++) op->ABC[i] = ABC[i];
         op->t6_valid = false;
         op->t6_edited = false;
@@ -1928,6 +2132,7 @@ int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9])
 int mlb_longrange_set_open(mlb_op* op, int ox, int oy, int oz)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_DIPOLE) fail(MLB_EINVAL, "open boundaries apply to Dipole");
         if (!oz && op->nz > 1) fail(MLB_EUNSUP, "the Dipole layer sum is open in z");
         op->open[0] = ox != 0; op->open[1] = oy != 0; op->open[2] = 1;
@@ -1951,6 +2156,7 @@ static void offset_index(const mlb_op* op, int ox, int oy, int oz, long long* of
 int mlb_longrange_set_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double v)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE) fail(MLB_EINVAL, "not a LongRange operator");
         if (ab < 0 || ab > 5) fail(MLB_EINVAL, "1st argument must be matrix name: XX, XY, XZ, YY, YZ or ZZ");
         if (op->kind == MLB_OP_DIPOLE && (op->open[0] || op->open[1])) fail(MLB_EUNSUP, "open-boundary tensor");
@@ -2008,6 +2214,7 @@ int mlb_longrange_get_tensor(mlb_op* op, double* const t6[6])
 int mlb_longrange3d_set_tensor(mlb_op* op, int ab, const double* t)
 {
     return guard([&] {
+        g_version++;
         if (op->kind != MLB_OP_LONGRANGE3D) fail(MLB_EINVAL, "not a LongRange3D operator");
         if (ab < 0 || ab > 8) fail(MLB_EINVAL, "tensor component must be 0..8");
         materialize_users(op);
@@ -2030,12 +2237,14 @@ int mlb_llg_create(int kind, mlb_llg** out)
 
 int mlb_llg_destroy(mlb_llg* l)
 {
-    return guard([&] { delete l; });
+    return guard([&] {
+        g_version++; delete l; });
 }
 
 int mlb_llg_set_flags(mlb_llg* l, int tof, int disable_renorm, double precess, double damp)
 {
     return guard([&] {
+        g_version++;
         l->tof = tof != 0;
         l->disable_renorm = disable_renorm != 0;
         l->precess = precess;
@@ -2053,81 +2262,79 @@ int mlb_llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, 
     });
 }
 
+// ---------------------------------------------------------------- plans
+int mlb_plan_create(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int timing, mlb_plan** out)
+{
+    return guard([&] {
+        std::unique_ptr<mlb_plan> p(new mlb_plan());
+        p->s = s;
+        p->ops.assign(ops, ops + nops);
+        p->l = l;
+        p->timing = timing != 0;
+        plan_capture(p.get());
+        *out = p.release();
+    });
+}
+
+int mlb_plan_launch(mlb_plan* p, int nsteps)
+{
+    return guard([&] { plan_launch(p, nsteps); });
+}
+
+int mlb_plan_kernel_times(mlb_plan* p, int cap, char* names, double* ms, int* count)
+{
+    return guard([&] {
+        CK(cudaStreamSynchronize(p->s->st));
+        int k = 0;
+        if (p->last)
+            for (ProfCaptured& r : *p->last) {
+                if (k >= cap) break;
+                float t = 0.f;
+                CK(cudaEventElapsedTime(&t, r.a, r.b));
+                snprintf(names + 48 * k, 48, "%s", r.name);
+                ms[k] = t;
+                k++;
+            }
+        *count = k;
+    });
+}
+
+int mlb_plan_destroy(mlb_plan* p)
+{
+    return guard([&] {
+        if (!p) return;
+        plan_release(p);
+        delete p;
+    });
+}
+
 // ---------------------------------------------------------------- fused run
 int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps)
 {
     return guard([&] {
         if (nsteps <= 0) return;
         for (int i = 0; i < nops; i++) check_dims(ops[i], s);
-        // step 1 (host path) sets up plans, slot arrays and fusability
-        do_step(s, ops, nops, l);
-        for (int i = 0; i < nops; i++)
-            if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
-                for (int a = 0; a < 3; a++) ops[i]->B[a] += ops[i]->dB[a];
-        int left = nsteps - 1;
-        bool graphable = s->last_fused && left >= 3;
-        for (int i = 0; i < nops; i++)
-            if (ops[i]->kind == MLB_OP_THERMAL && ops[i]->inject_pending) graphable = false;
-        if (graphable) {
-            const int pairs = (left - 1) / 2;
-            if (pairs > 0) {
-                // capture two steps (buffer A->B, B->A); the Thermal counter and
-                // the field sweep read the device step counter
-                const int cur0 = s->cur;
-                const long long gen0 = s->gen;
-                const double time0 = s->time;
-                std::vector<uint64_t> ctr0(nops);
-                for (int i = 0; i < nops; i++) ctr0[i] = ops[i]->counter;
-                CK(cudaMemsetAsync(s->dctr, 0, sizeof(uint64_t), s->st));
-                CK(cudaStreamSynchronize(s->st));
-                cudaGraph_t graph = nullptr;
-                cudaGraphExec_t exec = nullptr;
-                bool captured = false;
-                if (cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-                    s->capturing = true;
-                    bool ok = true;
-                    try {
-                        do_step(s, ops, nops, l);
-                        for (int i = 0; i < nops; i++)
-                            if (ops[i]->kind == MLB_OP_THERMAL) ops[i]->counter = ctr0[i];
-                        do_step(s, ops, nops, l);
-                    } catch (Err&) {
-                        ok = false;
-                    }
-                    s->capturing = false;
-                    cudaError_t e = cudaStreamEndCapture(s->st, &graph);
-                    if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess)
-                        captured = true;
-                    cudaGetLastError();
-                }
-                // host state as it was before the capture
-                s->cur = cur0;
-                s->gen = gen0;
-                s->time = time0;
-                for (int i = 0; i < nops; i++)
-                    if (ops[i]->kind == MLB_OP_THERMAL) ops[i]->counter = ctr0[i];
-                reset_fields(s);
-                if (captured) {
-                    for (int p = 0; p < pairs; p++) CK(cudaGraphLaunch(exec, s->st));
-                    // bookkeeping of the 2*pairs graph steps
-                    s->gen = gen0 + 2LL * pairs;
-                    for (int k = 0; k < 2 * pairs; k++) s->time = s->time + s->dt;
-                    for (int i = 0; i < nops; i++) {
-                        if (ops[i]->kind == MLB_OP_THERMAL) ops[i]->counter = ctr0[i] + 2ULL * pairs;
-                        if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
-                            for (int a = 0; a < 3; a++) ops[i]->B[a] += 2.0 * pairs * ops[i]->dB[a];
-                    }
-                    left -= 2 * pairs;
-                }
-                if (exec) cudaGraphExecDestroy(exec);
-                if (graph) cudaGraphDestroy(graph);
+        if (nsteps >= 3) {
+            mlb_plan p;
+            p.s = s;
+            p.ops.assign(ops, ops + nops);
+            p.l = l;
+            bool ok = true;
+            try {
+                plan_capture(&p);
+            } catch (Err&) {
+                ok = false;
             }
+            if (ok) {
+                plan_launch(&p, nsteps);
+                plan_release(&p);
+                return;
+            }
+            plan_release(&p);
         }
-        for (int k = 0; k < left; k++) {
+        for (int k = 0; k < nsteps; k++) {
             do_step(s, ops, nops, l);
-            for (int i = 0; i < nops; i++)
-                if (ops[i]->kind == MLB_OP_APPLIEDFIELD)
-                    for (int a = 0; a < 3; a++) ops[i]->B[a] += ops[i]->dB[a];
+            advance_sweep(ops, nops);
         }
     });
 }

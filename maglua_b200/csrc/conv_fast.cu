@@ -295,11 +295,9 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
     const int nxy = F.nx * F.ny;
     const int i = x + F.nx * y + nxy * z;
     const float Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
-    float Hx = F.B[0], Hy = F.B[1], Hz = F.B[2];
-    if (F.zdctr) {
-        const float kk = (float)(*F.zdctr);
-        Hx += kk * F.dB[0]; Hy += kk * F.dB[1]; Hz += kk * F.dB[2];
-    }
+    float Hx, Hy, Hz;
+    if (F.Bdev) { Hx = F.Bdev[0]; Hy = F.Bdev[1]; Hz = F.Bdev[2]; }
+    else { Hx = F.B[0]; Hy = F.B[1]; Hz = F.B[2]; }
     if (EXS) {
         float ex = 0.f, ey = 0.f, ez = 0.f;
 #define MLB_NB(cond, wrapcond, off, woff, J)                                                       \
@@ -419,12 +417,8 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
     dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3);
     const size_t smem = X::SMEM;
     if (fwd) {
-        static bool cfg = false;
-        if (!cfg) { cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
         k_fx_fast<PX><<<grid, 256, smem, st>>>(c, tw, s[0], s[1], s[2], spec);
     } else {
-        static bool cfg = false;
-        if (!cfg) { cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); cfg = true; }
         k_ix_fast<PX><<<grid, 256, smem, st>>>(c, tw, spec, h[0], h[1], h[2]);
     }
     return cudaGetLastError();
@@ -448,8 +442,6 @@ template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
     const size_t smem = yz_fast_smem(PY, PZ, c.nz);
-    static bool cfg = false;
-    if (!cfg) { cudaFuncSetAttribute(k_yz_fast<PY, PZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024); cfg = true; }
     k_yz_fast<PY, PZ><<<c.Kx, YZT<PY>::N, smem, st>>>(c, twy, spec, ten6);
     return cudaGetLastError();
 }
@@ -478,6 +470,39 @@ static cudaError_t launch_yz_any(const ConvK& c, const float2* twy, float2* spec
     case 512: return launch_yz_py<512>(c, twy, spec, ten6, st);
     }
     return cudaErrorInvalidValue;
+}
+
+// Shared-memory limits of every instantiation, set once before any launch
+// (a first launch may happen while a graph is being captured).
+template <int PX>
+static cudaError_t cfg_x()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+template <int PY>
+static cudaError_t cfg_yz()
+{
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 1>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 2>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 4>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 8>, a, 227 * 1024)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_yz_fast<PY, 16>, a, 227 * 1024);
+}
+
+cudaError_t conv_fast_configure()
+{
+    cudaError_t e;
+    if ((e = cfg_x<16>()) || (e = cfg_x<32>()) || (e = cfg_x<64>()) || (e = cfg_x<128>()) || (e = cfg_x<256>()) ||
+        (e = cfg_x<512>()))
+        return e;
+    if ((e = cfg_yz<16>()) || (e = cfg_yz<32>()) || (e = cfg_yz<64>()) || (e = cfg_yz<128>()) || (e = cfg_yz<256>()) ||
+        (e = cfg_yz<512>()))
+        return e;
+    return cudaSuccess;
 }
 
 cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,

@@ -207,11 +207,8 @@ __device__ __forceinline__ Fields eval_terms(const TermsK& T, const SysK& s, flo
     if (T.cub.mode != ANI_NONE) H = add3(H, cub_term(T.cub, sp, ms, i));
     if (T.th.mode != TH_NONE) { Hth = th_term(T.th, s, dt_sys, i, ms); H = add3(H, Hth); }
     if (T.zee.on) {
-        float3 B = f3(T.zee.B[0], T.zee.B[1], T.zee.B[2]);
-        if (T.zee.dctr) {
-            const float k = (float)(*T.zee.dctr);
-            B = f3(B.x + k * T.zee.dB[0], B.y + k * T.zee.dB[1], B.z + k * T.zee.dB[2]);
-        }
+        const float3 B = T.zee.Bdev ? f3(T.zee.Bdev[0], T.zee.Bdev[1], T.zee.Bdev[2])
+                                    : f3(T.zee.B[0], T.zee.B[1], T.zee.B[2]);
         H = add3(H, B);
     }
     for (int a = 0; a < T.nadd; a++) {
@@ -348,7 +345,12 @@ __global__ void __launch_bounds__(256) k_llg(SysK from, const float* mx, const f
     ox[i] = out.x; oy[i] = out.y; oz[i] = out.z;
 }
 
-__global__ void k_advance_counter(uint64_t* c) { *c += 1ull; }
+// One step of the device step block: next Thermal counter, swept field.
+__global__ void k_advance_step(DevStep* d)
+{
+    d->th_counter += 1ull;
+    for (int a = 0; a < 3; a++) d->B[a] += d->dB[a];
+}
 
 // FP64 partial sums for netMoment: per block (sum v*m, sum (v*m)^2) x 3.
 __global__ void __launch_bounds__(256) k_netmoment_partial(const float* x, const float* y, const float* z,
@@ -736,14 +738,22 @@ struct ProfRec {
 bool g_prof = false;
 std::vector<ProfRec> g_recs;
 std::vector<cudaEvent_t> g_pool;
+std::vector<ProfCaptured>* g_sink = nullptr;
 } // namespace
 
-bool prof_active(cudaStream_t st)
+void prof_set_capture_sink(std::vector<ProfCaptured>* sink) { g_sink = sink; }
+
+int prof_active(cudaStream_t st)
 {
-    if (!g_prof) return false;
     cudaStreamCaptureStatus cs;
-    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
-    return true;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return 0;
+    if (cs != cudaStreamCaptureStatusNone) return g_sink ? 2 : 0;
+    return g_prof ? 1 : 0;
+}
+
+void prof_push_captured(const char* name, cudaEvent_t a, cudaEvent_t b)
+{
+    if (g_sink) g_sink->push_back({name, a, b});
 }
 
 cudaEvent_t prof_event()
@@ -822,9 +832,9 @@ cudaError_t launch_llg(const SysK& from, const float* m[3], const float* H[3], c
     return cudaGetLastError();
 }
 
-cudaError_t launch_advance(uint64_t* c, cudaStream_t st)
+cudaError_t launch_advance_step(DevStep* d, cudaStream_t st)
 {
-    k_advance_counter<<<1, 1, 0, st>>>(c);
+    k_advance_step<<<1, 1, 0, st>>>(d);
     return cudaGetLastError();
 }
 

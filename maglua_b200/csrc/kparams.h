@@ -56,8 +56,15 @@ struct ThermalK {
 struct ZeemanK {
     int on;
     float B[3];               // times global_scale
-    float dB[3];              // per-step sweep increment (uses *dctr)
-    const uint64_t* dctr;
+    const float* Bdev;        // captured steps: B read from the device step block
+};
+
+// Parameters a captured step reads on the device and advances once per step
+// (k_advance_step): the Thermal counter and the applied field with its sweep.
+struct DevStep {
+    uint64_t th_counter;
+    float B[3];
+    float dB[3];
 };
 
 struct SysK {
@@ -126,9 +133,8 @@ struct FastK {
     float sigma;              // sqrt(2 alpha T scale / (ms dt gamma))
     uint64_t seed, counter;
     const uint64_t* dctr;
-    float B[3];               // Zeeman (+ dB * *zdctr)
-    float dB[3];
-    const uint64_t* zdctr;
+    float B[3];               // Zeeman (Bdev when read from the device step block)
+    const float* Bdev;
     float addw;
     int llg_type, tof, renorm, dt_zero;
     float dt, precess, c_prec, c_damp, c_rot, ms;

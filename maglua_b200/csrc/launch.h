@@ -5,29 +5,41 @@
 #include "device.cuh"
 #include "kparams.h"
 
+#include <vector>
+
 namespace mlb {
-bool prof_active(cudaStream_t st);
+// Kernel timing: 1 = eager profiling (mlb_profile_begin/end), 2 = event
+// nodes inside a graph being captured for a plan with timing, 0 = off.
+struct ProfCaptured {
+    const char* name;
+    cudaEvent_t a, b;
+};
+int prof_active(cudaStream_t st);
 cudaEvent_t prof_event();
 void prof_push(const char* name, cudaEvent_t a, cudaEvent_t b);
-// Scope timer used around kernel launches (active only while profiling).
+void prof_push_captured(const char* name, cudaEvent_t a, cudaEvent_t b);
+void prof_set_capture_sink(std::vector<ProfCaptured>* sink);
+// Scope timer used around kernel launches.
 struct Prof {
-    bool on;
+    int mode;
     const char* name;
     cudaStream_t st;
     cudaEvent_t a = nullptr;
-    Prof(const char* n, cudaStream_t s) : on(prof_active(s)), name(n), st(s)
+    Prof(const char* n, cudaStream_t s) : mode(prof_active(s)), name(n), st(s)
     {
-        if (on) { a = prof_event(); cudaEventRecord(a, st); }
+        if (mode == 1) { a = prof_event(); cudaEventRecord(a, st); }
+        else if (mode == 2) { cudaEventCreate(&a); cudaEventRecord(a, st); }
     }
     ~Prof()
     {
-        if (!on) return;
-        cudaEvent_t b = prof_event();
-        cudaEventRecord(b, st);
-        prof_push(name, a, b);
+        if (mode == 0) return;
+        cudaEvent_t b;
+        if (mode == 1) { b = prof_event(); cudaEventRecord(b, st); prof_push(name, a, b); }
+        else { cudaEventCreate(&b); cudaEventRecord(b, st); prof_push_captured(name, a, b); }
     }
 };
 cudaError_t fftreg_init();
+cudaError_t conv_fast_configure();
 bool conv_fast_ok(const ConvK& c);
 cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                              const float* ten6, float* h[3], cudaStream_t st);
@@ -39,7 +51,7 @@ cudaError_t launch_eval(const SysK& s, const TermsK& T, float dt_sys, float* h[3
 cudaError_t launch_llg(const SysK& from, const float* m[3], const float* H[3], const float* Ht[3],
                        const float* dsa, const float* dsg, float da, float dg, const LlgK& L,
                        float* out[3], cudaStream_t st);
-cudaError_t launch_advance(uint64_t* c, cudaStream_t st);
+cudaError_t launch_advance_step(DevStep* d, cudaStream_t st);
 cudaError_t launch_netmoment(const float* x, const float* y, const float* z, int n, double m,
                              double* part, int nb, double* out, cudaStream_t st);
 cudaError_t launch_dot(const float* s[3], const float* h[3], int n, double* part, int nb, double* out,

@@ -518,3 +518,49 @@ def test_slot_api_semantics(M):
         ss.fieldArrays("NoSuchSlot")
     with pytest.raises(M.MagLuaError):
         M.SpinSystem(0, 1, 1)
+
+
+def test_plan_matches_calls_and_recaptures(M):
+    dims = (32, 16, 4)
+    n = int(np.prod(dims))
+    s = tilted_spins(n, 40)
+    res = []
+    for mode in ("calls", "plan"):
+        ss = M.SpinSystem(*dims)
+        ss.setSpinArrays(*s)
+        ss.setAlpha(0.05)
+        ss.setTimeStep(0.005)
+        ex = M.Exchange(ss)
+        ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 0)))
+        ani = M.Anisotropy(ss)
+        ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.05))
+        th = M.Thermal(ss, M.Random.Philox(9))
+        th.setTemperature(0.3)
+        z = M.AppliedField(ss)
+        z.set(0.0, 0.1, 0)
+        dip = M.Dipole(ss)
+        dip.setStrength(0.03)
+        l = M.LLG.new("Cartesian")
+        ops = [ex, ani, th, z, dip]
+        if mode == "calls":
+            for k in range(9):
+                if k == 5:
+                    th.setTemperature(0.6)
+                ss.resetFields()
+                for op in ops:
+                    op.apply(ss)
+                ss.sumFields()
+                l.apply(ss)
+        else:
+            plan = M.Plan(ss, ops, l, timing=True)
+            plan.launch(5)
+            th.setTemperature(0.6)      # changes the captured constants: recapture
+            plan.launch(4)
+            kt = plan.kernelTimes()
+            assert "k_fused_step" in kt and all(v > 0 for v in kt.values())
+        res.append(np.stack(ss.spinArrays()[:3]))
+        res.append(np.stack(ss.fieldArrays("Total")))
+        res.append(ss.time())
+    np.testing.assert_array_equal(res[0], res[3])
+    np.testing.assert_array_equal(res[1], res[4])
+    assert res[2] == res[5]
