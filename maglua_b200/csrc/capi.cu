@@ -1263,9 +1263,24 @@ HostState save_state(mlb_system* s, const std::vector<mlb_op*>& ops)
     return h;
 }
 
+// Restore the bookkeeping saved by save_state.  Slot registrations and
+// their device arrays made in between are kept (new slots return to ZERO).
 void load_state(mlb_system* s, const std::vector<mlb_op*>& ops, const HostState& h)
 {
-    s->cur = h.cur; s->gen = h.gen; s->time = h.time; s->slots = h.slots; s->last_fused = h.last_fused;
+    s->cur = h.cur; s->gen = h.gen; s->time = h.time; s->last_fused = h.last_fused;
+    for (size_t i = 0; i < s->slots.size(); i++) {
+        Slot& x = s->slots[i];
+        float* keep[3] = {x.h[0], x.h[1], x.h[2]};
+        if (i < h.slots.size()) {
+            const bool had = h.slots[i].h[0] != nullptr;
+            x = h.slots[i];
+            // an array allocated since then stays; a DATA state needs the
+            // array it had
+            if (!had) for (int c = 0; c < 3; c++) x.h[c] = keep[c];
+        } else {
+            x.used = false; x.state = ST_ZERO; x.terms.clear(); x.sum_list.clear(); x.base_data = false;
+        }
+    }
     for (size_t i = 0; i < ops.size(); i++) {
         ops[i]->counter = h.ctr[i];
         for (int a = 0; a < 3; a++) ops[i]->B[a] = h.B[i][a];

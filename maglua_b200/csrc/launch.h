@@ -28,14 +28,14 @@ struct Prof {
     Prof(const char* n, cudaStream_t s) : mode(prof_active(s)), name(n), st(s)
     {
         if (mode == 1) { a = prof_event(); cudaEventRecord(a, st); }
-        else if (mode == 2) { cudaEventCreate(&a); cudaEventRecord(a, st); }
+        else if (mode == 2) { cudaEventCreate(&a); cudaEventRecordWithFlags(a, st, cudaEventRecordExternal); }
     }
     ~Prof()
     {
         if (mode == 0) return;
         cudaEvent_t b;
         if (mode == 1) { b = prof_event(); cudaEventRecord(b, st); prof_push(name, a, b); }
-        else { cudaEventCreate(&b); cudaEventRecord(b, st); prof_push_captured(name, a, b); }
+        else { cudaEventCreate(&b); cudaEventRecordWithFlags(b, st, cudaEventRecordExternal); prof_push_captured(name, a, b); }
     }
 };
 cudaError_t fftreg_init();
