@@ -220,7 +220,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ncu-steps", type=int, default=0,
+                    help="profiling driver: run this many eager steps of the workload and exit (for ncu)")
     args = ap.parse_args()
+    if args.ncu_steps:
+        import maglua_b200 as M
+        M.init(int(os.environ.get("LOCAL_RANK", "0")))
+        ss, ops, llg = build_system(M, 0)
+        for _ in range(args.ncu_steps):
+            M.run(ss, ops, llg, 1)
+        ss.synchronize()
+        return
     args.warmup = max(3, args.warmup)
 
     rank = int(os.environ.get("RANK", "0"))
