@@ -217,6 +217,42 @@ int mlb_plan_launch(mlb_plan* p, int nsteps);
 int mlb_plan_kernel_times(mlb_plan* p, int cap, char* names, double* ms, int* count);
 int mlb_plan_destroy(mlb_plan* p);
 
+/* ---------------------------------------------------------------- ensembles
+ * B200 extension for the reference's batched form op:apply({ss1, ss2, ...})
+ * (SpinOperation::apply(SpinSystem**, n), spinoperation.cpp:288-300; the
+ * CUDA build's *_N kernels need equal sizes): nrep independent replicas of
+ * uneven sizes packed by size class, one launch per phase for all of them,
+ * the step captured in CUDA graphs.  All replicas share the operator set of
+ * mlb_ensemble_cfg: nearest-neighbour Exchange (normalised moments), uniform
+ * Anisotropy, Thermal (Philox), AppliedField with a per-step sweep, Dipole
+ * (open or periodic in-plane images), LLG.  Replica spins must share one
+ * length.  dims holds nx, ny, nz per replica. */
+typedef struct mlb_ensemble mlb_ensemble;
+typedef struct mlb_ensemble_cfg {
+    double alpha, gamma, dt;
+    double J;                 /* exchange with the six neighbours */
+    int pbc[3];               /* periodic x, y, z */
+    double K;                 /* anisotropy strength along axis */
+    double axis[3];
+    double T;                 /* temperature */
+    uint64_t seed;            /* Philox seed */
+    double B[3];              /* applied field at the first step */
+    double dB[3];             /* added after every step */
+    double g;                 /* dipole strength (0: off) */
+    int open_xy;              /* 1: zero-padded open in-plane boundaries */
+    int llg;                  /* MLB_LLG_CARTESIAN or MLB_LLG_QUATERNION */
+} mlb_ensemble_cfg;
+int mlb_ensemble_create(int nrep, const int* dims, mlb_ensemble** out);
+int mlb_ensemble_destroy(mlb_ensemble* e);
+int mlb_ensemble_configure(mlb_ensemble* e, const mlb_ensemble_cfg* cfg);
+int mlb_ensemble_set_spins(mlb_ensemble* e, int rep, const double* x, const double* y, const double* z);
+int mlb_ensemble_get_spins(mlb_ensemble* e, int rep, double* x, double* y, double* z);
+int mlb_ensemble_run(mlb_ensemble* e, int nsteps);
+/* netMoment of every replica (8 numbers each, as mlb_system_netmoment with m = 1). */
+int mlb_ensemble_netmoment(mlb_ensemble* e, double* out8);
+int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, double* time);
+int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
+
 /* ---------------------------------------------------------------- fused run
  * B200 extension: nsteps repetitions of the canonical script step
  * (doc/manual/BasicMicromagneticSimulation.lua:84-94):

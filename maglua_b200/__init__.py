@@ -120,6 +120,15 @@ _SIGS = {
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
     "mlb_plan_kernel_times": ([_P, C.c_int, C.c_char_p, _D, _I], C.c_int),
     "mlb_plan_destroy": ([_P], C.c_int),
+    "mlb_ensemble_create": ([C.c_int, _I, C.POINTER(_P)], C.c_int),
+    "mlb_ensemble_destroy": ([_P], C.c_int),
+    "mlb_ensemble_configure": ([_P, _P], C.c_int),
+    "mlb_ensemble_set_spins": ([_P, C.c_int, _D, _D, _D], C.c_int),
+    "mlb_ensemble_get_spins": ([_P, C.c_int, _D, _D, _D], C.c_int),
+    "mlb_ensemble_run": ([_P, C.c_int], C.c_int),
+    "mlb_ensemble_netmoment": ([_P, _D], C.c_int),
+    "mlb_ensemble_info": ([_P, C.POINTER(C.c_longlong), _I, _D], C.c_int),
+    "mlb_ensemble_get_stream": ([_P, C.POINTER(_P)], C.c_int),
 }
 EXPORTED = tuple(_SIGS)
 
@@ -994,6 +1003,76 @@ class Plan:
             self._h = None
 
     close = __del__
+
+
+class _EnsCfg(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("gamma", C.c_double), ("dt", C.c_double), ("J", C.c_double),
+                ("pbc", C.c_int * 3), ("K", C.c_double), ("axis", C.c_double * 3), ("T", C.c_double),
+                ("seed", C.c_uint64), ("B", C.c_double * 3), ("dB", C.c_double * 3), ("g", C.c_double),
+                ("open_xy", C.c_int), ("llg", C.c_int)]
+
+
+class Ensemble:
+    """Replicas of uneven sizes stepped together: packed by size class, one
+    launch per phase, graph-captured (the batched op:apply({ss1, ...}) form
+    for systems that share one operator set)."""
+
+    def __init__(self, dims):
+        _ensure_init()
+        d = np.ascontiguousarray(np.asarray(dims, dtype=np.int32).reshape(-1, 3))
+        self.dims = [tuple(int(v) for v in row) for row in d]
+        h = _P()
+        _ck(_lib.mlb_ensemble_create(len(d), d.ctypes.data_as(_I), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_ensemble_destroy(h)
+            self._h = None
+
+    def configure(self, alpha=0.1, dt=0.01, gamma=1.0, J=1.0, pbc=(0, 0, 0), K=0.0, axis=(0, 0, 1), T=0.0,
+                  seed=0, B=(0, 0, 0), dB=(0, 0, 0), g=0.0, open_xy=True, llg="Cartesian"):
+        c = _EnsCfg()
+        c.alpha, c.gamma, c.dt, c.J, c.K, c.T, c.g = alpha, gamma, dt, J, K, T, g
+        for i in range(3):
+            c.pbc[i] = int(bool(pbc[i]))
+            c.axis[i] = axis[i]
+            c.B[i] = B[i]
+            c.dB[i] = dB[i]
+        c.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        c.open_xy = int(bool(open_xy))
+        c.llg = 0 if llg == "Cartesian" else 1
+        _ck(_lib.mlb_ensemble_configure(self._h, C.byref(c)))
+
+    def setSpins(self, rep, x, y, z):
+        n = int(np.prod(self.dims[rep]))
+        x, y, z = _f64(x, n), _f64(y, n), _f64(z, n)
+        _ck(_lib.mlb_ensemble_set_spins(self._h, int(rep), _dp(x), _dp(y), _dp(z)))
+
+    def spins(self, rep):
+        n = int(np.prod(self.dims[rep]))
+        x, y, z = np.zeros(n), np.zeros(n), np.zeros(n)
+        _ck(_lib.mlb_ensemble_get_spins(self._h, int(rep), _dp(x), _dp(y), _dp(z)))
+        return x, y, z
+
+    def run(self, nsteps):
+        _ck(_lib.mlb_ensemble_run(self._h, int(nsteps)))
+
+    def netMoment(self):
+        out = np.zeros((len(self.dims), 8))
+        _ck(_lib.mlb_ensemble_netmoment(self._h, _dp(out)))
+        return out
+
+    def info(self):
+        n, bs, t = C.c_longlong(), C.c_int(), C.c_double()
+        _ck(_lib.mlb_ensemble_info(self._h, C.byref(n), C.byref(bs), C.byref(t)))
+        return {"sites": n.value, "block_size": bs.value, "time": t.value}
+
+    def stream(self):
+        out = _P()
+        _ck(_lib.mlb_ensemble_get_stream(self._h, C.byref(out)))
+        return out.value or 0
 
 
 def run(ss, ops, llg, nsteps):

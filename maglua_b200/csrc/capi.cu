@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <new>
 #include <set>
@@ -543,6 +544,7 @@ void plan_sizes(mlb_op* op, ConvPlan& P)
         k.Pz = op->nz == 1 ? 1 : nice_len(2 * op->nz - 1);
     }
     k.Kx = k.Px / 2 + 1;
+    k.nrep = 1;
     int ty = 16;
     while (ty > 1 && (size_t)2 * ty * k.Px * sizeof(float2) > 96 * 1024) ty /= 2;
     k.ty = ty;
@@ -1403,6 +1405,227 @@ void plan_launch(mlb_plan* p, int nsteps)
     }
     s->dry = false;
     advance_sweep(p->ops.data(), (int)p->ops.size());
+}
+
+// ------------------------------------------------------------------ packed ensembles
+struct EnsClass {
+    int nx, ny, nz, nrep;
+    long long base;             // first packed site of the class
+    mlb_op* dip = nullptr;      // tensor spectrum holder for this size
+};
+
+void ens_free_graphs(mlb_ensemble* e);
+
+} // namespace
+
+struct mlb_ensemble {
+    int nrep = 0;
+    long long ntot = 0;
+    std::vector<int> pos;            // user replica -> packed replica index
+    std::vector<int4> rinfo_h;       // packed order: {nx, ny, nz, first site}
+    std::vector<EnsClass> cls;
+    float* sp[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int cur = 0;
+    float* H[3] = {nullptr, nullptr, nullptr};
+    float ms = 0.f;
+    bool have_ms = false;
+    mlb_ensemble_cfg cfg;
+    bool configured = false;
+    DevStep* dstep = nullptr;
+    cudaStream_t st = nullptr, own = nullptr;
+    int4* rinfo = nullptr;
+    int* brep = nullptr;
+    int* bstart = nullptr;
+    int nblk = 0;
+    int bs = 0;                       // fused-kernel block size (autotuned)
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    double time = 0.0;
+    uint64_t counter = 0;
+    double B[3] = {0, 0, 0};
+    double* mom = nullptr;
+};
+
+namespace {
+
+std::map<std::string, int> g_ens_tuned;   // class signature -> block size
+
+void ens_free_graphs(mlb_ensemble* e)
+{
+    for (int q = 0; q < 2; q++) {
+        if (e->exec[q]) cudaGraphExecDestroy(e->exec[q]);
+        e->exec[q] = nullptr;
+    }
+}
+
+void ens_block_table(mlb_ensemble* e, int bs)
+{
+    std::vector<int> br, bstv;
+    for (int r = 0; r < e->nrep; r++) {
+        const int4 ri = e->rinfo_h[r];
+        const int n = ri.x * ri.y * ri.z;
+        for (int s0 = 0; s0 < n; s0 += bs) { br.push_back(r); bstv.push_back(s0); }
+    }
+    cudaFree(e->brep);
+    cudaFree(e->bstart);
+    e->brep = nullptr; e->bstart = nullptr;
+    CK(cudaMalloc(&e->brep, sizeof(int) * br.size()));
+    CK(cudaMalloc(&e->bstart, sizeof(int) * br.size()));
+    CK(cudaMemcpy(e->brep, br.data(), sizeof(int) * br.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->bstart, bstv.data(), sizeof(int) * bstv.size(), cudaMemcpyHostToDevice));
+    e->nblk = (int)br.size();
+    e->bs = bs;
+}
+
+FastK ens_fastk(mlb_ensemble* e)
+{
+    const mlb_ensemble_cfg& c = e->cfg;
+    const double ms = e->ms, a = c.alpha, g = c.gamma, dt = c.dt;
+    FastK F;
+    memset(&F, 0, sizeof(F));
+    F.ex = c.J != 0.0;
+    for (int d = 0; d < 6; d++) F.J[d] = (float)(c.J / (ms * ms));
+    for (int q = 0; q < 3; q++) F.pbc[q] = c.pbc[q] ? 1 : 0;
+    const double al = std::sqrt(c.axis[0] * c.axis[0] + c.axis[1] * c.axis[1] + c.axis[2] * c.axis[2]);
+    F.ani = c.K != 0.0 && al > 0;
+    if (F.ani) {
+        for (int q = 0; q < 3; q++) F.axis[q] = (float)(c.axis[q] / al);
+        F.ani_c = (float)(2.0 * c.K / (ms * ms));
+    }
+    F.th = c.T != 0.0 && g > 0;
+    if (F.th) {
+        F.sigma = (float)std::sqrt((2.0 * a * c.T) / (ms * dt * g));
+        F.seed = c.seed;
+        F.counter = 0;
+        F.dctr = &e->dstep->th_counter;
+    }
+    F.Bdev = e->dstep->B;
+    F.addw = 1.f;
+    F.llg_type = c.llg == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
+    F.tof = 1;
+    F.renorm = 1;
+    F.dt_zero = dt == 0.0;
+    F.dt = (float)dt;
+    F.precess = 1.f;
+    F.ms = (float)ms;
+    const double gaa = g / (1.0 + a * a);
+    if (F.llg_type == LLG_CART) {
+        F.c_prec = (float)-gaa;
+        F.c_damp = (float)((a / ms) * gaa);
+    } else {
+        F.c_damp = (float)(a / ms);
+        F.c_rot = (float)(0.5 * g * dt / (1.0 + a * a));
+    }
+    return F;
+}
+
+void ens_enqueue_step(mlb_ensemble* e, int q)
+{
+    const float* s[3] = {e->sp[q][0], e->sp[q][1], e->sp[q][2]};
+    float* o[3] = {e->sp[1 - q][0], e->sp[1 - q][1], e->sp[1 - q][2]};
+    const float* add[3] = {nullptr, nullptr, nullptr};
+    if (e->cfg.g != 0.0) {
+        for (EnsClass& c : e->cls) {
+            ConvPlan& P = *c.dip->plan;
+            const float* cs[3] = {s[0] + c.base, s[1] + c.base, s[2] + c.base};
+            float* ch[3] = {e->H[0] + c.base, e->H[1] + c.base, e->H[2] + c.base};
+            CK(mlb::launch_conv_fast(P.k, P.L, P.tw.p, cs, P.spec.p, P.ten6.p, ch, e->st));
+        }
+        for (int q3 = 0; q3 < 3; q3++) add[q3] = e->H[q3];
+    }
+    EnsLaunch E{e->nblk, e->bs, e->brep, e->bstart, e->rinfo};
+    CK(mlb::launch_fused_ens(ens_fastk(e), E, s, add, o, e->st));
+    CK(mlb::launch_advance_step(e->dstep, e->st));
+}
+
+// Block size of the fused ensemble kernel: time each candidate on the
+// current state (the kernel only writes the other spin buffer) and keep the
+// fastest; remembered per class signature for the process.
+void ens_autotune(mlb_ensemble* e)
+{
+    std::string sig;
+    for (EnsClass& c : e->cls)
+        sig += std::to_string(c.nx) + "x" + std::to_string(c.ny) + "x" + std::to_string(c.nz) + ":" + std::to_string(c.nrep) + ";";
+    auto it = g_ens_tuned.find(sig);
+    if (it != g_ens_tuned.end()) { ens_block_table(e, it->second); return; }
+    const int cand[3] = {128, 256, 512};
+    float best = 1e30f;
+    int best_bs = 256;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    const float* s[3] = {e->sp[e->cur][0], e->sp[e->cur][1], e->sp[e->cur][2]};
+    float* o[3] = {e->sp[1 - e->cur][0], e->sp[1 - e->cur][1], e->sp[1 - e->cur][2]};
+    const float* add[3] = {nullptr, nullptr, nullptr};
+    if (e->cfg.g != 0.0) for (int q = 0; q < 3; q++) add[q] = e->H[q];
+    for (int bs : cand) {
+        ens_block_table(e, bs);
+        EnsLaunch E{e->nblk, e->bs, e->brep, e->bstart, e->rinfo};
+        const FastK F = ens_fastk(e);
+        CK(mlb::launch_fused_ens(F, E, s, add, o, e->st));
+        CK(cudaEventRecord(a, e->st));
+        for (int k = 0; k < 10; k++) CK(mlb::launch_fused_ens(F, E, s, add, o, e->st));
+        CK(cudaEventRecord(b, e->st));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        if (ms < best) { best = ms; best_bs = bs; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    g_ens_tuned[sig] = best_bs;
+    ens_block_table(e, best_bs);
+}
+
+void ens_prepare(mlb_ensemble* e)
+{
+    if (!e->configured) fail(MLB_ESTATE, "ensemble not configured");
+    if (!e->have_ms) fail(MLB_ESTATE, "ensemble spins not set");
+    if (e->exec[0]) return;
+    const mlb_ensemble_cfg& c = e->cfg;
+    if (c.g != 0.0) {
+        for (EnsClass& k : e->cls) {
+            if (!k.dip) {
+                k.dip = new mlb_op();
+                k.dip->kind = MLB_OP_DIPOLE;
+                k.dip->nx = k.nx; k.dip->ny = k.ny; k.dip->nz = k.nz;
+                k.dip->slot = "Dipole";
+            }
+            k.dip->open[0] = c.open_xy ? 1 : 0;
+            k.dip->open[1] = c.open_xy ? 1 : 0;
+            k.dip->open[2] = 1;
+            k.dip->t6_valid = false;
+            k.dip->plan_dirty = true;
+            build_plan(k.dip, e->st);
+            ConvPlan& P = *k.dip->plan;
+            if (!mlb::conv_fast_ok(P.k)) fail(MLB_EUNSUP, "ensemble size class outside the fast FFT sizes");
+            P.k.nrep = k.nrep;
+            P.k.g = (float)(c.g / ((double)P.k.Px * P.k.Py * P.k.Pz));
+            P.spec.alloc((size_t)P.k.Kx * 3 * k.nz * k.ny * k.nrep);
+        }
+    }
+    ens_autotune(e);
+    CK(cudaStreamSynchronize(e->st));
+    for (int q = 0; q < 2; q++) {
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+        bool ok = true;
+        std::string why;
+        try {
+            ens_enqueue_step(e, q);
+        } catch (Err& er) {
+            ok = false;
+            why = er.msg;
+        }
+        cudaError_t ce = cudaStreamEndCapture(e->st, &graph);
+        if (!ok || ce != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            ens_free_graphs(e);
+            fail(MLB_ESTATE, "ensemble capture failed: " + (ok ? std::string(cudaGetErrorString(ce)) : why));
+        }
+        ce = cudaGraphInstantiate(&e->exec[q], graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) { ens_free_graphs(e); fail(MLB_ECUDA, cudaGetErrorString(ce)); }
+    }
 }
 
 } // namespace
@@ -2352,6 +2575,195 @@ int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps)
             advance_sweep(ops, nops);
         }
     });
+}
+
+
+// ---------------------------------------------------------------- ensembles
+int mlb_ensemble_create(int nrep, const int* dims, mlb_ensemble** out)
+{
+    return guard([&] {
+        if (nrep < 1 || !dims) fail(MLB_EINVAL, "ensemble needs replicas");
+        std::unique_ptr<mlb_ensemble> e(new mlb_ensemble());
+        e->nrep = nrep;
+        // size classes in order of first appearance; replicas packed by class
+        std::vector<int> cls_of(nrep);
+        for (int r = 0; r < nrep; r++) {
+            const int nx = dims[3 * r], ny = dims[3 * r + 1], nz = dims[3 * r + 2];
+            if (nx < 1 || ny < 1 || nz < 1) fail(MLB_EINVAL, "dimensions must be positive");
+            int k = -1;
+            for (size_t j = 0; j < e->cls.size(); j++)
+                if (e->cls[j].nx == nx && e->cls[j].ny == ny && e->cls[j].nz == nz) k = (int)j;
+            if (k < 0) {
+                EnsClass c;
+                c.nx = nx; c.ny = ny; c.nz = nz; c.nrep = 0; c.base = 0;
+                e->cls.push_back(c);
+                k = (int)e->cls.size() - 1;
+            }
+            cls_of[r] = k;
+            e->cls[k].nrep++;
+        }
+        long long base = 0;
+        for (EnsClass& c : e->cls) { c.base = base; base += (long long)c.nx * c.ny * c.nz * c.nrep; }
+        if (base > (1LL << 31) - 1) fail(MLB_EUNSUP, "more than 2^31-1 sites in one ensemble");
+        e->ntot = base;
+        std::vector<int> fill(e->cls.size(), 0);
+        e->pos.resize(nrep);
+        e->rinfo_h.resize(nrep);
+        int packed = 0;
+        std::vector<int> first(e->cls.size(), 0);
+        for (size_t k = 0; k < e->cls.size(); k++) { first[k] = packed; packed += e->cls[k].nrep; }
+        for (int r = 0; r < nrep; r++) {
+            const int k = cls_of[r];
+            const int p = first[k] + fill[k];
+            const EnsClass& c = e->cls[k];
+            e->pos[r] = p;
+            e->rinfo_h[p] = make_int4(c.nx, c.ny, c.nz, (int)(c.base + (long long)fill[k] * c.nx * c.ny * c.nz));
+            fill[k]++;
+        }
+        CK(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
+        e->st = e->own;
+        for (int b = 0; b < 2; b++)
+            for (int c = 0; c < 3; c++) {
+                CK(cudaMalloc(&e->sp[b][c], sizeof(float) * e->ntot));
+                CK(cudaMemset(e->sp[b][c], 0, sizeof(float) * e->ntot));
+            }
+        for (int c = 0; c < 3; c++) {
+            CK(cudaMalloc(&e->H[c], sizeof(float) * e->ntot));
+            CK(cudaMemset(e->H[c], 0, sizeof(float) * e->ntot));
+        }
+        CK(cudaMalloc(&e->rinfo, sizeof(int4) * nrep));
+        CK(cudaMemcpy(e->rinfo, e->rinfo_h.data(), sizeof(int4) * nrep, cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&e->dstep, sizeof(DevStep)));
+        CK(cudaMemset(e->dstep, 0, sizeof(DevStep)));
+        CK(cudaMalloc(&e->mom, sizeof(double) * 6 * nrep));
+        memset(&e->cfg, 0, sizeof(e->cfg));
+        *out = e.release();
+    });
+}
+
+int mlb_ensemble_destroy(mlb_ensemble* e)
+{
+    return guard([&] {
+        if (!e) return;
+        cudaStreamSynchronize(e->st);
+        ens_free_graphs(e);
+        for (int b = 0; b < 2; b++)
+            for (int c = 0; c < 3; c++) cudaFree(e->sp[b][c]);
+        for (int c = 0; c < 3; c++) cudaFree(e->H[c]);
+        cudaFree(e->rinfo); cudaFree(e->brep); cudaFree(e->bstart); cudaFree(e->dstep); cudaFree(e->mom);
+        for (EnsClass& c : e->cls) delete c.dip;
+        if (e->own) cudaStreamDestroy(e->own);
+        delete e;
+    });
+}
+
+int mlb_ensemble_configure(mlb_ensemble* e, const mlb_ensemble_cfg* cfg)
+{
+    return guard([&] {
+        if (cfg->llg != MLB_LLG_CARTESIAN && cfg->llg != MLB_LLG_QUATERNION) fail(MLB_EINVAL, "unknown LLG type");
+        e->cfg = *cfg;
+        e->configured = true;
+        e->counter = 0;
+        for (int a = 0; a < 3; a++) e->B[a] = cfg->B[a];
+        ens_free_graphs(e);
+    });
+}
+
+int mlb_ensemble_set_spins(mlb_ensemble* e, int rep, const double* x, const double* y, const double* z)
+{
+    return guard([&] {
+        if (rep < 0 || rep >= e->nrep) fail(MLB_ERANGE, "replica index");
+        const int4 ri = e->rinfo_h[e->pos[rep]];
+        const int n = ri.x * ri.y * ri.z;
+        std::vector<float> f[3];
+        const double* src[3] = {x, y, z};
+        float m0 = -1.f;
+        for (int i = 0; i < n; i++) {
+            const float m = (float)std::sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+            if (m0 < 0) m0 = m;
+            if (std::fabs(m - m0) > 1e-6f * std::max(1.f, m0)) fail(MLB_EUNSUP, "ensemble spins must share one length");
+        }
+        if (e->have_ms && std::fabs(m0 - e->ms) > 1e-6f * std::max(1.f, m0))
+            fail(MLB_EUNSUP, "ensemble spins must share one length");
+        e->ms = m0;
+        e->have_ms = true;
+        CK(cudaStreamSynchronize(e->st));
+        for (int c = 0; c < 3; c++) {
+            f[c].resize(n);
+            for (int i = 0; i < n; i++) f[c][i] = (float)src[c][i];
+            CK(cudaMemcpy(e->sp[e->cur][c] + ri.w, f[c].data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+        }
+    });
+}
+
+int mlb_ensemble_get_spins(mlb_ensemble* e, int rep, double* x, double* y, double* z)
+{
+    return guard([&] {
+        if (rep < 0 || rep >= e->nrep) fail(MLB_ERANGE, "replica index");
+        const int4 ri = e->rinfo_h[e->pos[rep]];
+        const int n = ri.x * ri.y * ri.z;
+        std::vector<float> f(n);
+        double* dst[3] = {x, y, z};
+        CK(cudaStreamSynchronize(e->st));
+        for (int c = 0; c < 3; c++) {
+            CK(cudaMemcpy(f.data(), e->sp[e->cur][c] + ri.w, sizeof(float) * n, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < n; i++) dst[c][i] = f[i];
+        }
+    });
+}
+
+int mlb_ensemble_run(mlb_ensemble* e, int nsteps)
+{
+    return guard([&] {
+        if (nsteps <= 0) return;
+        ens_prepare(e);
+        DevStep h;
+        memset(&h, 0, sizeof(h));
+        h.th_counter = e->counter;
+        for (int a = 0; a < 3; a++) { h.B[a] = (float)e->B[a]; h.dB[a] = (float)e->cfg.dB[a]; }
+        CK(cudaMemcpyAsync(e->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, e->st));
+        const bool cart = e->cfg.llg != MLB_LLG_QUATERNION;
+        for (int k = 0; k < nsteps; k++) {
+            CK(cudaGraphLaunch(e->exec[e->cur], e->st));
+            e->cur = 1 - e->cur;
+            if (!cart || e->cfg.dt != 0.0) e->time = e->time + e->cfg.dt;
+            for (int a = 0; a < 3; a++) e->B[a] += e->cfg.dB[a];
+        }
+        e->counter += (uint64_t)nsteps;
+    });
+}
+
+int mlb_ensemble_netmoment(mlb_ensemble* e, double* out8)
+{
+    return guard([&] {
+        const float* s[3] = {e->sp[e->cur][0], e->sp[e->cur][1], e->sp[e->cur][2]};
+        CK(mlb::launch_ens_moments(e->rinfo, e->nrep, s, e->mom, e->st));
+        std::vector<double> m(6 * (size_t)e->nrep);
+        CK(cudaMemcpyAsync(m.data(), e->mom, sizeof(double) * m.size(), cudaMemcpyDeviceToHost, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        for (int r = 0; r < e->nrep; r++) {
+            const double* v = &m[6 * (size_t)e->pos[r]];
+            double* o = out8 + 8 * (size_t)r;
+            o[0] = v[0]; o[1] = v[1]; o[2] = v[2];
+            o[3] = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            o[4] = v[3]; o[5] = v[4]; o[6] = v[5];
+            o[7] = std::sqrt(v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
+        }
+    });
+}
+
+int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, double* time)
+{
+    return guard([&] {
+        if (nsites) *nsites = e->ntot;
+        if (block_size) *block_size = e->bs;
+        if (time) *time = e->time;
+    });
+}
+
+int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
+{
+    return guard([&] { *stream = (void*)e->st; });
 }
 
 } // extern "C"

@@ -68,9 +68,11 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][PX]
     float2* B = A + X::BUF;         // [L][PX]
-    const int comp = blockIdx.z, zz = blockIdx.y;
+    const int comp = blockIdx.z % 3, rep = blockIdx.z / 3, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
-    const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + (size_t)zz * c.ny * c.nx;
+    const size_t nsite = (size_t)c.nx * c.ny * c.nz;
+    spec += (size_t)rep * c.Kx * 3 * c.nz * c.ny;
+    const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + rep * nsite + (size_t)zz * c.ny * c.nx;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     constexpr int IT = (X::LINE + NT - 1) / NT;
     float2 v[IT];
@@ -122,10 +124,12 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][PX] lines
     float2* B = A + X::BUF;         // [ROWS][KX] spectra, then scratch
-    const int comp = blockIdx.z, zz = blockIdx.y;
+    const int comp = blockIdx.z % 3, rep = blockIdx.z / 3, zz = blockIdx.y;
     const int row0 = blockIdx.x * X::ROWS;
     const int rows_here = min(X::ROWS, c.ny - row0);
-    float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + (size_t)zz * c.ny * c.nx;
+    const size_t nsite = (size_t)c.nx * c.ny * c.nz;
+    spec += (size_t)rep * c.Kx * 3 * c.nz * c.ny;
+    float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + rep * nsite + (size_t)zz * c.ny * c.nx;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     constexpr int IS = (X::SPEC + NT - 1) / NT;
     {
@@ -178,21 +182,24 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
 // One CTA per kx.  y transforms of the 3*nz data lines by TPL threads each
 // (in rounds), z transforms + tensor multiply with one thread per
 // (component, ky) column, inverse y transforms.
-template <int PY>
+// threads per CTA: 768, or 384 when the z columns are 32 long (registers)
+template <int PY, int PZ>
 struct YZT {
-    static constexpr int N = 768;
+    static constexpr int N = PZ >= 32 ? 384 : 768;
 };
 
 template <int PY, int PZ>
-__global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
-                                                    float2* __restrict__ spec, const float* __restrict__ ten6)
+__global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
+                                                               float2* __restrict__ spec, const float* __restrict__ ten6)
 {
+    constexpr int NT = YZT<PY, PZ>::N;
     constexpr int TPL = fr::Tpl<PY>::V;
-    constexpr int LPR = 768 / TPL;   // lines per round
+    constexpr int LPR = NT / TPL;    // lines per round
     extern __shared__ float2 sm[];
     const int kx = blockIdx.x;
     const int nz = c.nz, ny = c.ny;
     const int nlines = 3 * nz;
+    spec += (size_t)blockIdx.y * c.Kx * 3 * nz * ny;
     float2* P = sm;                          // [3][nz][PY]
     float2* Pb = P + (size_t)nlines * PY;    // scratch [3][nz][PY]
     float2* Q = Pb + (size_t)nlines * PY;    // [3][PZ][PY]
@@ -208,17 +215,17 @@ __global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __res
     float2* sp = spec + (size_t)kx * nlines * ny;
     {
         // at most 3*PZ*PY elements (nz <= PZ): unrolled gather, then store
-        constexpr int IG = (3 * PZ * PY + 767) / 768;
+        constexpr int IG = (3 * PZ * PY + NT - 1) / NT;
         float2 v[IG];
 #pragma unroll
         for (int it = 0; it < IG; it++) {
-            const int idx = threadIdx.x + it * 768;
+            const int idx = threadIdx.x + it * NT;
             const int l = idx / PY, y = idx % PY;
             v[it] = (l < nlines && y < ny) ? sp[(size_t)l * ny + y] : make_float2(0.f, 0.f);
         }
 #pragma unroll
         for (int it = 0; it < IG; it++) {
-            const int idx = threadIdx.x + it * 768;
+            const int idx = threadIdx.x + it * NT;
             if (idx < nlines * PY) P[idx] = v[it];
         }
     }
@@ -267,10 +274,10 @@ __global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __res
         Y = fr::sm_fft<PY, +1, TPL>(P, Pb, l < nlines ? l : 0, tl, twl, l < nlines);
     }
     {
-        constexpr int IG = (3 * PZ * PY + 767) / 768;
+        constexpr int IG = (3 * PZ * PY + NT - 1) / NT;
 #pragma unroll
         for (int it = 0; it < IG; it++) {
-            const int idx = threadIdx.x + it * 768;
+            const int idx = threadIdx.x + it * NT;
             const int l = idx / PY, y = idx % PY;
             if (l < nlines && y < ny) sp[(size_t)l * ny + y] = Y[idx];
         }
@@ -281,19 +288,18 @@ __global__ void __launch_bounds__(768, 1) k_yz_fast(ConvK c, const float2* __res
 // Uniform-parameter systems: ms, alpha, gamma, anisotropy and thermal scale
 // the same on every site, exchange as a six-direction stencil.  Constants
 // are folded on the host (FastK).
+// One site of the fused step.  (x, y, z) are the site's coordinates inside
+// its lattice of NX x NY x NZ sites and i its index in the (packed) arrays;
+// neighbours are addressed relative to i, so several lattices can share the
+// arrays back to back.
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __restrict__ sx, const float* __restrict__ sy,
-                                                    const float* __restrict__ sz, const float* __restrict__ ax,
-                                                    const float* __restrict__ ay, const float* __restrict__ az,
-                                                    float* __restrict__ ox, float* __restrict__ oy,
-                                                    float* __restrict__ oz)
+__device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                           const float* __restrict__ sx, const float* __restrict__ sy,
+                                           const float* __restrict__ sz, const float* __restrict__ ax,
+                                           const float* __restrict__ ay, const float* __restrict__ az,
+                                           float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= F.nx || y >= F.ny) return;
-    const int nxy = F.nx * F.ny;
-    const int i = x + F.nx * y + nxy * z;
+    const int nxy = NX * NY;
     const float Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
     float Hx, Hy, Hz;
     if (F.Bdev) { Hx = F.Bdev[0]; Hy = F.Bdev[1]; Hz = F.Bdev[2]; }
@@ -309,12 +315,12 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
                 ex += (J) * __ldg(sx + f); ey += (J) * __ldg(sy + f); ez += (J) * __ldg(sz + f);   \
             }                                                                                      \
         }
-        MLB_NB(x + 1 < F.nx, F.pbc[0], 1, 1 - F.nx, F.J[0])
-        MLB_NB(x > 0, F.pbc[0], -1, F.nx - 1, F.J[1])
-        MLB_NB(y + 1 < F.ny, F.pbc[1], F.nx, F.nx - nxy, F.J[2])
-        MLB_NB(y > 0, F.pbc[1], -F.nx, nxy - F.nx, F.J[3])
-        MLB_NB(z + 1 < F.nz, F.pbc[2], nxy, nxy - nxy * F.nz, F.J[4])
-        MLB_NB(z > 0, F.pbc[2], -nxy, nxy * F.nz - nxy, F.J[5])
+        MLB_NB(x + 1 < NX, F.pbc[0], 1, 1 - NX, F.J[0])
+        MLB_NB(x > 0, F.pbc[0], -1, NX - 1, F.J[1])
+        MLB_NB(y + 1 < NY, F.pbc[1], NX, NX - nxy, F.J[2])
+        MLB_NB(y > 0, F.pbc[1], -NX, nxy - NX, F.J[3])
+        MLB_NB(z + 1 < NZ, F.pbc[2], nxy, nxy - nxy * NZ, F.J[4])
+        MLB_NB(z > 0, F.pbc[2], -nxy, nxy * NZ - nxy, F.J[5])
 #undef MLB_NB
         Hx += ex; Hy += ey; Hz += ez;
     }
@@ -392,6 +398,70 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
     ox[i] = nx_; oy[i] = ny_; oz[i] = nz_;
 }
 
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
+__global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __restrict__ sx, const float* __restrict__ sy,
+                                                    const float* __restrict__ sz, const float* __restrict__ ax,
+                                                    const float* __restrict__ ay, const float* __restrict__ az,
+                                                    float* __restrict__ ox, float* __restrict__ oy,
+                                                    float* __restrict__ oz)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= F.nx || y >= F.ny) return;
+    const int i = x + F.nx * (y + F.ny * z);
+    fused_site<LT, EXS, ANI, TH, ADD>(F, F.nx, F.ny, F.nz, x, y, z, i, sx, sy, sz, ax, ay, az, ox, oy, oz);
+}
+
+// Packed ensemble: block b covers sites [bstart[b], bstart[b] + blockDim) of
+// replica brep[b]; rinfo[r] = {nx, ny, nz, first packed site}.
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
+__global__ void k_fused_ens(FastK F, const int* __restrict__ brep, const int* __restrict__ bstart,
+                            const int4* __restrict__ rinfo, const float* __restrict__ sx,
+                            const float* __restrict__ sy, const float* __restrict__ sz,
+                            const float* __restrict__ ax, const float* __restrict__ ay,
+                            const float* __restrict__ az, float* __restrict__ ox, float* __restrict__ oy,
+                            float* __restrict__ oz)
+{
+    const int4 r = __ldg(rinfo + __ldg(brep + blockIdx.x));
+    const int local = __ldg(bstart + blockIdx.x) + threadIdx.x;
+    const int n = r.x * r.y * r.z;
+    if (local >= n) return;
+    const int x = local % r.x;
+    const int y = (local / r.x) % r.y;
+    const int z = local / (r.x * r.y);
+    fused_site<LT, EXS, ANI, TH, ADD>(F, r.x, r.y, r.z, x, y, z, r.w + local, sx, sy, sz, ax, ay, az, ox, oy, oz);
+}
+
+// FP64 per-replica sums (x, y, z, x^2, y^2, z^2): one block per replica.
+__global__ void __launch_bounds__(256) k_ens_moments(const int4* __restrict__ rinfo, const float* __restrict__ sx,
+                                                     const float* __restrict__ sy, const float* __restrict__ sz,
+                                                     double* __restrict__ out)
+{
+    const int4 r = rinfo[blockIdx.x];
+    const int n = r.x * r.y * r.z;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const double a = sx[r.w + k], b = sy[r.w + k], c = sz[r.w + k];
+        acc[0] += a; acc[1] += b; acc[2] += c;
+        acc[3] += a * a; acc[4] += b * b; acc[5] += c * c;
+    }
+    __shared__ double sh[6][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[q][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) v += sh[threadIdx.x][k];
+        out[blockIdx.x * 6 + threadIdx.x] = v;
+    }
+}
+
 // ------------------------------------------------------------------ dispatch
 namespace mlb {
 
@@ -405,7 +475,7 @@ static size_t yz_fast_smem(int PY, int PZ, int nz)
 
 bool conv_fast_ok(const ConvK& c)
 {
-    if (c.general || !pow2_in(c.Px, 16, 512) || !pow2_in(c.Py, 16, 512) || !pow2_in(c.Pz, 1, 16)) return false;
+    if (c.general || !pow2_in(c.Px, 16, 512) || !pow2_in(c.Py, 16, 512) || !pow2_in(c.Pz, 1, 32)) return false;
     return yz_fast_smem(c.Py, c.Pz, c.nz) <= 227 * 1024;
 }
 
@@ -414,7 +484,7 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
                             cudaStream_t st, bool fwd)
 {
     using X = XCfg<PX>;
-    dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3);
+    dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3 * c.nrep);
     const size_t smem = X::SMEM;
     if (fwd) {
         k_fx_fast<PX><<<grid, 256, smem, st>>>(c, tw, s[0], s[1], s[2], spec);
@@ -442,7 +512,7 @@ template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
     const size_t smem = yz_fast_smem(PY, PZ, c.nz);
-    k_yz_fast<PY, PZ><<<c.Kx, YZT<PY>::N, smem, st>>>(c, twy, spec, ten6);
+    k_yz_fast<PY, PZ><<<dim3(c.Kx, c.nrep), YZT<PY, PZ>::N, smem, st>>>(c, twy, spec, ten6);
     return cudaGetLastError();
 }
 
@@ -455,6 +525,7 @@ static cudaError_t launch_yz_py(const ConvK& c, const float2* twy, float2* spec,
     case 4: return launch_yz_t<PY, 4>(c, twy, spec, ten6, st);
     case 8: return launch_yz_t<PY, 8>(c, twy, spec, ten6, st);
     case 16: return launch_yz_t<PY, 16>(c, twy, spec, ten6, st);
+    case 32: return launch_yz_t<PY, 32>(c, twy, spec, ten6, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -490,7 +561,8 @@ static cudaError_t cfg_yz()
     if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 2>, a, 227 * 1024)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 4>, a, 227 * 1024)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 8>, a, 227 * 1024)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_yz_fast<PY, 16>, a, 227 * 1024);
+    if ((e = cudaFuncSetAttribute(k_yz_fast<PY, 16>, a, 227 * 1024)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_yz_fast<PY, 32>, a, 227 * 1024);
 }
 
 cudaError_t conv_fast_configure()
@@ -557,6 +629,51 @@ static void fused_ex(const FastK& F, const float* s[3], const float* a[3], float
 {
     if (F.ex) fused_ani<LT, true>(F, s, a, o, st);
     else fused_ani<LT, false>(F, s, a, o, st);
+}
+
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
+static void ens_t(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+{
+    k_fused_ens<LT, EXS, ANI, TH, ADD><<<E.nblk, E.bs, 0, st>>>(F, E.brep, E.bstart, E.rinfo, s[0], s[1], s[2], a[0], a[1],
+                                                               a[2], o[0], o[1], o[2]);
+}
+template <int LT, bool EXS, bool ANI, bool TH>
+static void ens_add(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+{
+    if (a[0]) ens_t<LT, EXS, ANI, TH, true>(F, E, s, a, o, st);
+    else ens_t<LT, EXS, ANI, TH, false>(F, E, s, a, o, st);
+}
+template <int LT, bool EXS, bool ANI>
+static void ens_th(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+{
+    if (F.th) ens_add<LT, EXS, ANI, true>(F, E, s, a, o, st);
+    else ens_add<LT, EXS, ANI, false>(F, E, s, a, o, st);
+}
+template <int LT, bool EXS>
+static void ens_ani(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+{
+    if (F.ani) ens_th<LT, EXS, true>(F, E, s, a, o, st);
+    else ens_th<LT, EXS, false>(F, E, s, a, o, st);
+}
+
+cudaError_t launch_fused_ens(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3],
+                             cudaStream_t st)
+{
+    Prof pf("k_fused_ens", st);
+    if (F.llg_type == LLG_CART) {
+        if (F.ex) ens_ani<LLG_CART, true>(F, E, s, a, o, st);
+        else ens_ani<LLG_CART, false>(F, E, s, a, o, st);
+    } else {
+        if (F.ex) ens_ani<LLG_QUAT, true>(F, E, s, a, o, st);
+        else ens_ani<LLG_QUAT, false>(F, E, s, a, o, st);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ens_moments(const int4* rinfo, int nrep, const float* s[3], double* out, cudaStream_t st)
+{
+    k_ens_moments<<<nrep, 256, 0, st>>>(rinfo, s[0], s[1], s[2], out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fused_fast(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)

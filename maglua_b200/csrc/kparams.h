@@ -117,6 +117,7 @@ struct ConvK {
     int general;             // 0: 6 real tensor entries per k, 1: 9 complex
     float g;                 // strength * global_scale / (Px*Py*Pz)
     int fx, fy, fz;          // FftLen indices
+    int nrep;                // replicas of this size packed back to back (1 for a system)
 };
 
 // Fused step for uniform-parameter systems (k_fused_fast): every constant
@@ -138,4 +139,12 @@ struct FastK {
     float addw;
     int llg_type, tof, renorm, dt_zero;
     float dt, precess, c_prec, c_damp, c_rot, ms;
+};
+
+// Block table of the packed-ensemble fused kernel.
+struct EnsLaunch {
+    int nblk, bs;
+    const int* brep;
+    const int* bstart;
+    const int4* rinfo;
 };

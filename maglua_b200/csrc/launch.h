@@ -44,6 +44,9 @@ bool conv_fast_ok(const ConvK& c);
 cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                              const float* ten6, float* h[3], cudaStream_t st);
 cudaError_t launch_fused_fast(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st);
+cudaError_t launch_fused_ens(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3],
+                             cudaStream_t st);
+cudaError_t launch_ens_moments(const int4* rinfo, int nrep, const float* s[3], double* out, cudaStream_t st);
 void prof_begin();
 int prof_end(int cap, char* names, double* ms, int* launches);
 cudaError_t launch_fused(const FusedK& P, float dt_sys, cudaStream_t st);

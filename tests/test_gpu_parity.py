@@ -564,3 +564,61 @@ def test_plan_matches_calls_and_recaptures(M):
     np.testing.assert_array_equal(res[0], res[3])
     np.testing.assert_array_equal(res[1], res[4])
     assert res[2] == res[5]
+
+
+# ---------------------------------------------------------------- ensembles
+def _single(M, dims, s, cfg, nsteps):
+    n = int(np.prod(dims))
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    ss.setAlpha(cfg["alpha"])
+    ss.setTimeStep(cfg["dt"])
+    ex = M.Exchange(ss)
+    ex.addPaths(*O.nn_paths(*dims, pbc=cfg["pbc"]))
+    ani = M.Anisotropy(ss)
+    ani.addMany(np.arange(n), np.tile(cfg["axis"], (n, 1)), np.full(n, cfg["K"]))
+    z = M.AppliedField(ss)
+    z.set(*cfg["B"])
+    z.setSweep(*cfg["dB"])
+    dip = M.Dipole(ss)
+    dip.setOpen(True, True, True)
+    dip.setStrength(cfg["g"])
+    l = M.LLG.new(cfg["llg"])
+    M.run(ss, [ex, ani, z, dip], l, nsteps)
+    return np.stack(ss.spinArrays()[:3]), ss.time()
+
+
+@pytest.mark.parametrize("llg", ["Cartesian", "Quaternion"])
+def test_ensemble_matches_single_systems(M, llg):
+    dims = [(16, 16, 4), (8, 8, 2), (32, 16, 1), (16, 16, 4), (8, 8, 2)]
+    cfg = dict(alpha=0.1, dt=0.01, pbc=(0, 0, 0), K=0.2, axis=(0, 0, 1.0), B=(0.0, 0.05, -0.1),
+               dB=(0.0, 0.0, -1e-3), g=0.05, llg=llg)
+    e = M.Ensemble(dims)
+    e.configure(alpha=cfg["alpha"], dt=cfg["dt"], J=1.0, pbc=cfg["pbc"], K=cfg["K"], axis=cfg["axis"], T=0.0,
+                B=cfg["B"], dB=cfg["dB"], g=cfg["g"], open_xy=True, llg=llg)
+    starts = [random_spins(int(np.prod(d)), 50 + r) for r, d in enumerate(dims)]
+    for r, s in enumerate(starts):
+        e.setSpins(r, *s)
+    e.run(7)
+    e.run(33)
+    assert e.info()["time"] == pytest.approx(0.4)
+    for r, d in enumerate(dims):
+        ref, t = _single(M, d, starts[r], cfg, 40)
+        got = np.stack(e.spins(r))
+        assert np.abs(got - ref).max() <= 1e-5, (r, np.abs(got - ref).max())
+    nm = e.netMoment()
+    x, y, z = e.spins(1)
+    np.testing.assert_allclose(nm[1, :3], [x.sum(), y.sum(), z.sum()], rtol=1e-9, atol=1e-9)
+
+
+def test_ensemble_thermal_replicas_independent(M):
+    dims = [(16, 16, 4)] * 4
+    e = M.Ensemble(dims)
+    e.configure(alpha=0.1, dt=0.01, J=1.0, K=0.2, T=0.2, seed=3, g=0.0)
+    s = np.stack([np.zeros(1024), np.zeros(1024), np.ones(1024)])
+    for r in range(4):
+        e.setSpins(r, *s)
+    e.run(50)
+    a, b = np.stack(e.spins(0)), np.stack(e.spins(1))
+    assert np.abs(a - b).max() > 1e-3      # different noise per replica
+    assert np.allclose(np.sqrt((a ** 2).sum(0)), 1.0, atol=1e-5)
