@@ -59,6 +59,14 @@ int mlb_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
  * M/cpu/core/spinsystem.h:33-140; methods spinsystem.cpp:3233-3318 and
  * spinsystem_luafuncs.lua. */
 int mlb_system_create(int nx, int ny, int nz, mlb_system** out);      /* SpinSystem.new(nx,ny,nz) */
+/* The same with the state precision chosen: real_bytes 4 (FP32, the
+ * default and the only width the specialised step kernels take) or 8 (FP64
+ * state, fields and LLG, as the reference's CPU build computes them; the
+ * general kernels only).  No counterpart in the reference, whose CPU build
+ * is FP64 and whose cuda32 build is FP32 by compile-time choice
+ * (M/cuda32 versus M/cpu). */
+int mlb_system_create_ex(int nx, int ny, int nz, int real_bytes, mlb_system** out);
+int mlb_system_real_bytes(const mlb_system* s, int* real_bytes);
 int mlb_system_destroy(mlb_system* s);                                 /* __gc */
 int mlb_system_dims(const mlb_system* s, int out[3]);                  /* nx(), ny(), nz() */
 /* Launch on this stream from now on (NULL = the system's own stream). */

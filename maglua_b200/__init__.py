@@ -47,6 +47,8 @@ _SIGS = {
     "mlb_profile_end": ([C.c_int, C.c_char_p, _D, _I, _I], C.c_int),
     "mlb_philox4x32_10": ([C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], C.c_int),
     "mlb_system_create": ([C.c_int, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_system_create_ex": ([C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_system_real_bytes": ([_P, C.POINTER(C.c_int)], C.c_int),
     "mlb_system_destroy": ([_P], C.c_int),
     "mlb_system_dims": ([_P, _I], C.c_int),
     "mlb_system_set_stream": ([_P, _P], C.c_int),
@@ -218,18 +220,27 @@ class SpinSystem:
 
     ALPHA, GAMMA, DT, TIME = 0, 1, 2, 3
 
-    def __init__(self, nx, ny=1, nz=1):
+    def __init__(self, nx, ny=1, nz=1, precision="f32"):
+        """precision "f32" (default) or "f64": the width of the spins, fields
+        and LLG arithmetic on the device."""
         _ensure_init()
         if isinstance(nx, SpinSystem):
             nx, ny, nz = nx.nx(), nx.ny(), nx.nz()
         elif hasattr(nx, "__len__"):
             nx, ny, nz = _site3(nx)
+        rb = {"f32": 4, "f64": 8}.get(precision)
+        if rb is None:
+            raise MagLuaError(-1, "precision must be 'f32' or 'f64'")
         h = _P()
-        _ck(_lib.mlb_system_create(int(nx), int(ny), int(nz), C.byref(h)))
+        _ck(_lib.mlb_system_create_ex(int(nx), int(ny), int(nz), rb, C.byref(h)))
         self._h = h
         self._dims = (int(nx), int(ny), int(nz))
+        self._precision = precision
 
-    new = classmethod(lambda cls, *a: cls(*a))
+    new = classmethod(lambda cls, *a, **k: cls(*a, **k))
+
+    def precision(self):
+        return self._precision
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -454,7 +465,7 @@ class SpinSystem:
         _ck(_lib.mlb_system_copy(dst._h, self._h, 0))
 
     def copy(self):
-        c = SpinSystem(*self._dims)
+        c = SpinSystem(*self._dims, precision=self._precision)
         self.copyTo(c)
         return c
 

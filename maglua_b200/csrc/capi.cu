@@ -1,7 +1,8 @@
 // capi.cu -- host layer behind include/mlb200.h.
 //
 // Object model (mirrors MagLua's SpinSystem / SpinOperation / LLG classes):
-//   * mlb_system: FP32 SoA spins in two generations (ping-pong buffers), ms,
+//   * mlb_system: SoA spins (FP32, or FP64 for systems created with 8-byte
+//     reals) in two generations (ping-pong buffers), ms,
 //     per-site alpha/gamma, named field slots ("Total" is slot 0).
 //   * Field slots are evaluated lazily.  A slot is ZERO, DATA (device arrays
 //     hold its value), LAZY (a base -- zero or its arrays -- plus operator terms
@@ -154,10 +155,11 @@ void append_twiddles(std::vector<C>& pool, int n)
 struct ConvPlan {
     ConvK k;
     FftLen L[3];
-    DBuf<float2> tw;
-    DBuf<float2> spec;
-    DBuf<float> ten6;
-    DBuf<float2> ten9;
+    int rb = 4;          // bytes per real of the arrays below (state precision)
+    DBuf<char> tw;       // complex twiddles per axis
+    DBuf<char> spec;     // SPEC[kx][c][z][y] (complex)
+    DBuf<char> ten6;     // TEN6[kx][kz][ky][6] (real)
+    DBuf<char> ten9;     // TEN9[kx][kz][ky][9] (complex)
     double max_imag = 0; // largest |Im| of the FP64 tensor transform (6-component)
 };
 
@@ -168,7 +170,7 @@ struct Term {
     mlb_op* op;
     int weight;
     uint64_t counter;
-    float B[3];
+    double B[3];
     double T;
     double gs;
     double dt_sys;
@@ -178,7 +180,7 @@ enum { ST_ZERO = 0, ST_DATA = 1, ST_LAZY = 2, ST_SUM = 3 };
 
 struct Slot {
     std::string name;
-    float* h[3] = {nullptr, nullptr, nullptr};
+    void* h[3] = {nullptr, nullptr, nullptr};
     bool used = false;
     int state = ST_ZERO;
     bool base_data = false;
@@ -189,16 +191,17 @@ struct Slot {
 
 struct mlb_system {
     int nx, ny, nz, n;
-    float* sp[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int rb = 4;                     // bytes per real of every state array (4 or 8)
+    void* sp[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
     long long gen = 0;
-    float* ms = nullptr;
-    std::vector<float> ms_host;
+    void* ms = nullptr;
+    std::vector<double> ms_host;    // ms as stored on the device (rounded to rb)
     bool ms_dirty = true;
     bool ms_uniform = true;
-    float ms_u = 0.f;
-    float* sa = nullptr;
-    float* sg = nullptr;
+    double ms_u = 0.0;
+    void* sa = nullptr;
+    void* sg = nullptr;
     double alpha = 1.0, gamma = 1.0, dt = 1.0, time = 0.0;
     std::vector<Slot> slots;
     cudaStream_t own = nullptr;
@@ -225,7 +228,7 @@ struct mlb_op {
     bool ex_dirty = true;
     ExchangeK exk{};
     DBuf<int> eptr, ecol;
-    DBuf<float> eval;
+    DBuf<double> eval;
     // anisotropies: per op site + parameters
     std::vector<int> asite;
     std::vector<double> apar; // generic: axis3,K ; uni: axis3,K1,K2 ; cubic: axes9,K3
@@ -234,17 +237,17 @@ struct mlb_op {
     UniK unik{};
     CubK cubk{};
     DBuf<int> aptr;
-    DBuf<float> aaxes, aK;
+    DBuf<double> aaxes, aK;
     double gs_compiled = -1;
     // thermal
     double T = 0.0;
     std::vector<double> tscale;
-    DBuf<float> dscale;
+    DBuf<double> dscale;
     bool tscale_dirty = false;
     uint64_t seed = 0;
     uint64_t counter = 0;
     bool inject_pending = false;
-    DBuf<float> inj[3];
+    DBuf<double> inj[3];
     // applied field
     double B[3] = {0, 0, 0};
     double dB[3] = {0, 0, 0};
@@ -309,14 +312,48 @@ int slot_register(mlb_system* s, const char* name)
 void slot_alloc(mlb_system* s, Slot& sl)
 {
     if (sl.h[0]) return;
-    for (int c = 0; c < 3; c++) CK(cudaMalloc(&sl.h[c], sizeof(float) * std::max(1, s->n)));
+    for (int c = 0; c < 3; c++) CK(cudaMalloc(&sl.h[c], (size_t)s->rb * std::max(1, s->n)));
 }
+
+// Byte offset of element i of a state array.
+inline void* elem(void* p, size_t i, int rb) { return static_cast<char*>(p) + i * (size_t)rb; }
+
+// Host values in FP64 -> n reals of width rb on the device (stream order).
+void put_reals(mlb_system* s, void* dst, const double* src, size_t n)
+{
+    if (n == 0) return;
+    if (s->rb == 8) {
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+        return;
+    }
+    std::vector<float> f(n);
+    for (size_t i = 0; i < n; i++) f[i] = (float)src[i];
+    CK(cudaMemcpyAsync(dst, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s->st));
+}
+
+// n reals of width rb on the device -> FP64 host values (synchronises).
+void get_reals(mlb_system* s, double* dst, const void* src, size_t n)
+{
+    if (n == 0) return;
+    if (s->rb == 8) {
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        return;
+    }
+    std::vector<float> f(n);
+    CK(cudaMemcpyAsync(f.data(), src, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (size_t i = 0; i < n; i++) dst[i] = f[i];
+}
+
+// Value as stored at width rb.
+inline double round_to(double v, int rb) { return rb == 8 ? v : (double)(float)v; }
 
 void refresh_ms(mlb_system* s)
 {
     if (!s->ms_dirty) return;
     s->ms_uniform = true;
-    s->ms_u = s->n ? s->ms_host[0] : 0.f;
+    s->ms_u = s->n ? s->ms_host[0] : 0.0;
     for (int i = 1; i < s->n; i++)
         if (s->ms_host[i] != s->ms_u) { s->ms_uniform = false; break; }
     s->ms_dirty = false;
@@ -330,7 +367,7 @@ SysK sysk(mlb_system* s, int buf)
     k.x = s->sp[buf][0]; k.y = s->sp[buf][1]; k.z = s->sp[buf][2];
     k.ms = s->ms; k.ms_u = s->ms_u; k.ms_uniform = s->ms_uniform ? 1 : 0;
     k.site_alpha = s->sa; k.site_gamma = s->sg;
-    k.alpha = (float)s->alpha; k.gamma = (float)s->gamma;
+    k.alpha = s->alpha; k.gamma = s->gamma;
     return k;
 }
 
@@ -414,7 +451,7 @@ void compile_exchange(mlb_op* op)
     }
     if (stencil) {
         k.mode = EX_STENCIL;
-        for (int d = 0; d < 6; d++) k.J[d] = seen[d] ? (float)Jd[d] : 0.f;
+        for (int d = 0; d < 6; d++) k.J[d] = seen[d] ? Jd[d] : 0.0;
         for (int a = 0; a < 3; a++) k.pbc[a] = pbc[a];
         op->eptr.release(); op->ecol.release(); op->eval.release();
     } else if (np > 0) {
@@ -423,17 +460,17 @@ void compile_exchange(mlb_op* op)
         for (size_t p = 0; p < np; p++) cnt[op->et[p] + 1]++;
         for (int i = 0; i < n; i++) cnt[i + 1] += cnt[i];
         std::vector<int> col(np);
-        std::vector<float> val(np);
+        std::vector<double> val(np);
         std::vector<int> pos(cnt.begin(), cnt.end() - 1);
         for (size_t p = 0; p < np; p++) {
             const int q = pos[op->et[p]]++;
             col[q] = op->ef[p];
-            val[q] = (float)op->eJ[p];
+            val[q] = op->eJ[p];
         }
         op->eptr.alloc(n + 1); op->ecol.alloc(np); op->eval.alloc(np);
         CK(cudaMemcpy(op->eptr.p, cnt.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(op->ecol.p, col.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(op->eval.p, val.data(), sizeof(float) * np, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->eval.p, val.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
         k.ptr = op->eptr.p; k.col = op->ecol.p; k.val = op->eval.p;
     } else {
         k.mode = EX_NONE;
@@ -469,24 +506,24 @@ void compile_aniso(mlb_op* op)
         std::vector<int> cnt(n + 1, 0);
         for (size_t j = 0; j < no; j++) cnt[op->asite[j] + 1]++;
         for (int i = 0; i < n; i++) cnt[i + 1] += cnt[i];
-        std::vector<float> ax(no * nax), kk(no * nk);
+        std::vector<double> ax(no * nax), kk(no * nk);
         std::vector<int> pos(cnt.begin(), cnt.end() - 1);
         for (size_t j = 0; j < no; j++) {
             const int q = pos[op->asite[j]]++;
-            for (int a = 0; a < nax; a++) ax[q * nax + a] = (float)op->apar[j * npar + a];
-            for (int a = 0; a < nk; a++) kk[q * nk + a] = (float)(op->apar[j * npar + nax + a] * gs);
+            for (int a = 0; a < nax; a++) ax[q * nax + a] = op->apar[j * npar + a];
+            for (int a = 0; a < nk; a++) kk[q * nk + a] = op->apar[j * npar + nax + a] * gs;
         }
         op->aptr.alloc(n + 1); op->aaxes.alloc(ax.size()); op->aK.alloc(kk.size());
         CK(cudaMemcpy(op->aptr.p, cnt.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(op->aaxes.p, ax.data(), sizeof(float) * ax.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(op->aK.p, kk.data(), sizeof(float) * kk.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->aaxes.p, ax.data(), sizeof(double) * ax.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(op->aK.p, kk.data(), sizeof(double) * kk.size(), cudaMemcpyHostToDevice));
     }
     if (op->kind == MLB_OP_ANISOTROPY) {
         AniK k{};
         k.mode = mode;
         if (mode == ANI_UNIFORM) {
-            for (int a = 0; a < 3; a++) k.axis[a] = (float)op->apar[a];
-            k.K = (float)(op->apar[3] * gs);
+            for (int a = 0; a < 3; a++) k.axis[a] = op->apar[a];
+            k.K = op->apar[3] * gs;
         } else if (mode == ANI_CSR) { k.ptr = op->aptr.p; k.axes = op->aaxes.p; k.Ks = op->aK.p; }
         op->anik = k;
     } else if (op->kind == MLB_OP_UNIAXIAL) {
@@ -494,8 +531,8 @@ void compile_aniso(mlb_op* op)
         k.mode = mode;
         k.quirk = op->quirks ? 1 : 0;
         if (mode == ANI_UNIFORM) {
-            for (int a = 0; a < 3; a++) k.axis[a] = (float)op->apar[a];
-            k.K1 = (float)(op->apar[3] * gs); k.K2 = (float)(op->apar[4] * gs);
+            for (int a = 0; a < 3; a++) k.axis[a] = op->apar[a];
+            k.K1 = op->apar[3] * gs; k.K2 = op->apar[4] * gs;
         } else if (mode == ANI_CSR) { k.ptr = op->aptr.p; k.axes = op->aaxes.p; k.K12 = op->aK.p; }
         op->unik = k;
     } else {
@@ -503,8 +540,8 @@ void compile_aniso(mlb_op* op)
         k.mode = mode;
         k.quirk = op->quirks ? 1 : 0;
         if (mode == ANI_UNIFORM) {
-            for (int a = 0; a < 9; a++) k.axes[a] = (float)op->apar[a];
-            for (int a = 0; a < 3; a++) k.K[a] = (float)(op->apar[9 + a] * gs);
+            for (int a = 0; a < 9; a++) k.axes[a] = op->apar[a];
+            for (int a = 0; a < 3; a++) k.K[a] = op->apar[9 + a] * gs;
         } else if (mode == ANI_CSR) { k.ptr = op->aptr.p; k.axs = op->aaxes.p; k.Ks = op->aK.p; }
         op->cubk = k;
     }
@@ -516,10 +553,8 @@ void compile_thermal_scale(mlb_op* op)
 {
     if (!op->tscale_dirty) return;
     const int n = op->nx * op->ny * op->nz;
-    std::vector<float> f(n);
-    for (int i = 0; i < n; i++) f[i] = (float)op->tscale[i];
     op->dscale.alloc(n);
-    CK(cudaMemcpy(op->dscale.p, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(op->dscale.p, op->tscale.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
     op->tscale_dirty = false;
 }
 
@@ -529,6 +564,7 @@ bool is_conv(int kind) { return kind == MLB_OP_DIPOLE || kind == MLB_OP_LONGRANG
 void plan_sizes(mlb_op* op, ConvPlan& P)
 {
     ConvK& k = P.k;
+    const size_t cb = (size_t)2 * P.rb;   // bytes per complex value
     k.nx = op->nx; k.ny = op->ny; k.nz = op->nz;
     if (op->kind == MLB_OP_LONGRANGE3D) {
         k.Px = op->nx; k.Py = op->ny; k.Pz = op->nz;
@@ -546,12 +582,16 @@ void plan_sizes(mlb_op* op, ConvPlan& P)
     k.Kx = k.Px / 2 + 1;
     k.nrep = 1;
     int ty = 16;
-    while (ty > 1 && (size_t)2 * ty * k.Px * sizeof(float2) > 96 * 1024) ty /= 2;
+    while (ty > 1 && (size_t)2 * ty * k.Px * cb > 96 * 1024) ty /= 2;
     k.ty = ty;
-    if ((size_t)6 * k.Py * k.Pz * sizeof(float2) > 227 * 1024)
+    // the power-of-two FP32 fast path has its own limits; the general
+    // kernels hold a whole padded (y,z) plane of three components twice
+    if (P.rb == 4 && mlb::conv_fast_ok(k)) return;
+    if ((size_t)6 * k.Py * k.Pz * cb > 227 * 1024)
         fail(MLB_EUNSUP, "padded (y,z) plane " + std::to_string(k.Py) + "x" + std::to_string(k.Pz) +
-                             " exceeds the shared-memory plane of this build");
-    if ((size_t)2 * k.Px * sizeof(float2) > 96 * 1024) fail(MLB_EUNSUP, "x length too large");
+                             " exceeds the shared-memory plane of this build at " + std::to_string(8 * P.rb) +
+                             "-bit precision");
+    if ((size_t)2 * k.Px * cb > 96 * 1024) fail(MLB_EUNSUP, "x length too large");
 }
 
 void ensure_t6_layout(mlb_op* op)
@@ -561,11 +601,13 @@ void ensure_t6_layout(mlb_op* op)
         if (op->t6[q].size() != ne) op->t6[q].assign(ne, 0.0);
 }
 
-// Build or rebuild the tensor spectrum of op (FP64 on the GPU).
-void build_plan(mlb_op* op, cudaStream_t st)
+// Build or rebuild the tensor spectrum of op (FP64 on the GPU), stored at
+// rb bytes per real for the systems it is applied to.
+void build_plan(mlb_op* op, cudaStream_t st, int rb)
 {
-    if (!op->plan_dirty && op->plan) return;
+    if (!op->plan_dirty && op->plan && op->plan->rb == rb) return;
     std::unique_ptr<ConvPlan> P(new ConvPlan());
+    P->rb = rb;
     plan_sizes(op, *P);
     ConvK& k = P->k;
     const int Px = k.Px, Py = k.Py, Pz = k.Pz;
@@ -578,8 +620,13 @@ void build_plan(mlb_op* op, cudaStream_t st)
         append_twiddles(twf, lens[a]);
         append_twiddles(twd, lens[a]);
     }
-    P->tw.alloc(twf.size());
-    CK(cudaMemcpy(P->tw.p, twf.data(), sizeof(float2) * twf.size(), cudaMemcpyHostToDevice));
+    if (rb == 8) {
+        P->tw.alloc(sizeof(double2) * twd.size());
+        CK(cudaMemcpy(P->tw.p, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice));
+    } else {
+        P->tw.alloc(sizeof(float2) * twf.size());
+        CK(cudaMemcpy(P->tw.p, twf.data(), sizeof(float2) * twf.size(), cudaMemcpyHostToDevice));
+    }
     DBuf<double2> twdd;
     twdd.alloc(twd.size());
     CK(cudaMemcpy(twdd.p, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice));
@@ -637,17 +684,17 @@ void build_plan(mlb_op* op, cudaStream_t st)
     }
     CK(mlb::launch_fft3d_d(W.p, ncomp, Px, Py, Pz, P->L, twdd.p, -1, st));
     if (k.general) {
-        P->ten9.alloc((size_t)k.Kx * Py * Pz * 9);
-        CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, st));
+        P->ten9.alloc((size_t)k.Kx * Py * Pz * 9 * 2 * rb);
+        CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, rb, st));
     } else {
-        P->ten6.alloc((size_t)k.Kx * Py * Pz * 6);
+        P->ten6.alloc((size_t)k.Kx * Py * Pz * 6 * rb);
         DBuf<double> mi;
         mi.alloc(1);
         CK(cudaMemsetAsync(mi.p, 0, sizeof(double), st));
-        CK(mlb::launch_tensor_pack6(W.p, Px, Py, Pz, k.Kx, P->ten6.p, mi.p, st));
+        CK(mlb::launch_tensor_pack6(W.p, Px, Py, Pz, k.Kx, P->ten6.p, mi.p, rb, st));
         CK(cudaMemcpyAsync(&P->max_imag, mi.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     }
-    P->spec.alloc((size_t)k.Kx * 3 * op->nz * op->ny);
+    P->spec.alloc((size_t)k.Kx * 3 * op->nz * op->ny * 2 * rb);
     CK(cudaStreamSynchronize(st));
     op->plan = std::move(P);
     op->plan_dirty = false;
@@ -664,7 +711,7 @@ struct TermsBuild {
 void terms_init(TermsK& T)
 {
     memset(&T, 0, sizeof(T));
-    T.ex_gs = 1.f;
+    T.ex_gs = 1.0;
 }
 
 // Add one recorded term to T; false when T already holds a different op
@@ -676,7 +723,7 @@ bool terms_add(TermsK& T, const Term& t, bool th_sub, mlb_system* s, bool captur
     case MLB_OP_EXCHANGE:
         if (T.ex.mode != EX_NONE) return false;
         T.ex = op->exk;
-        T.ex_gs = (float)(op->gs * t.weight);
+        T.ex_gs = op->gs * t.weight;
         return true;
     case MLB_OP_ANISOTROPY:
         if (T.ani.mode != ANI_NONE) return false;
@@ -693,7 +740,7 @@ bool terms_add(TermsK& T, const Term& t, bool th_sub, mlb_system* s, bool captur
     case MLB_OP_THERMAL:
         if (T.th.mode != TH_NONE || !th_sub) return false;
         T.th.mode = TH_PHILOX;
-        T.th.T = (float)(t.T * t.gs);
+        T.th.T = t.T * t.gs;
         T.th.scale = op->tscale.empty() ? nullptr : op->dscale.p;
         T.th.seed = op->seed;
         // captured steps read the counter from the device step block
@@ -710,7 +757,7 @@ bool terms_add(TermsK& T, const Term& t, bool th_sub, mlb_system* s, bool captur
     return false;
 }
 
-bool add_addend(TermsK& T, float* const h[3], float w, bool thermal)
+bool add_addend(TermsK& T, void* const h[3], double w, bool thermal)
 {
     if (T.nadd >= MLB_MAX_ADDENDS) return false;
     for (int c = 0; c < 3; c++) T.add[T.nadd][c] = h[c];
@@ -736,7 +783,7 @@ void before_mutate(mlb_system* s, int si)
 void eval_into(mlb_system* s, int buf, const TermsK& T, double dt_sys, Slot& out, int acc)
 {
     slot_alloc(s, out);
-    CK(mlb::launch_eval(sysk(s, buf), T, (float)dt_sys, out.h, acc, s->st));
+    CK(mlb::launch_eval(sysk(s, buf), T, dt_sys, out.h, acc, s->rb, s->st));
 }
 
 // Evaluate a LAZY slot into its arrays (state becomes DATA).
@@ -748,7 +795,7 @@ void materialize_lazy(mlb_system* s, int si)
     // terms one kind at a time so any combination is handled
     slot_alloc(s, sl);
     if (!sl.base_data) {
-        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(sl.h[c], 0, sizeof(float) * s->n, s->st));
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(sl.h[c], 0, (size_t)s->rb * s->n, s->st));
     }
     for (const Term& t : sl.terms) {
         TermsK T;
@@ -786,7 +833,7 @@ void build_sum_terms(mlb_system* s, const std::vector<int>& list, TermsK& T, lon
                 bool ok = x.gen == gen;
                 TermsK T2 = T;
                 double dts = dt_sys;
-                if (ok && x.base_data) ok = add_addend(T2, x.h, 1.f, is_th);
+                if (ok && x.base_data) ok = add_addend(T2, x.h, 1.0, is_th);
                 for (const Term& t : x.terms) {
                     if (!ok) break;
                     const bool th_here = t.op->kind == MLB_OP_THERMAL;
@@ -803,7 +850,7 @@ void build_sum_terms(mlb_system* s, const std::vector<int>& list, TermsK& T, lon
                 T = T2;
                 dt_sys = dts;
             } else if (x.state == ST_DATA) {
-                if (!add_addend(T, x.h, 1.f, is_th)) fail(MLB_EUNSUP, "too many materialised field slots in one sum");
+                if (!add_addend(T, x.h, 1.0, is_th)) fail(MLB_EUNSUP, "too many materialised field slots in one sum");
             }
         }
         if (!restart) return;
@@ -819,7 +866,7 @@ void materialize(mlb_system* s, int si)
         return;
     case ST_ZERO:
         slot_alloc(s, sl);
-        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(sl.h[c], 0, sizeof(float) * s->n, s->st));
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(sl.h[c], 0, (size_t)s->rb * s->n, s->st));
         sl.state = ST_DATA;
         return;
     case ST_LAZY:
@@ -934,7 +981,7 @@ void op_apply(mlb_op* op, mlb_system* s)
             TermsK T;
             terms_init(T);
             T.th.mode = TH_INJECT;
-            T.th.T = (float)(op->T * op->gs);
+            T.th.T = op->T * op->gs;
             T.th.scale = op->tscale.empty() ? nullptr : op->dscale.p;
             T.th.nx = op->inj[0].p; T.th.ny = op->inj[1].p; T.th.nz = op->inj[2].p;
             sl.terms.clear();
@@ -950,27 +997,35 @@ void op_apply(mlb_op* op, mlb_system* s)
     }
     case MLB_OP_APPLIEDFIELD:
         sl.used = true;
-        for (int a = 0; a < 3; a++) t.B[a] = (float)(op->B[a] * op->gs);
+        for (int a = 0; a < 3; a++) t.B[a] = op->B[a] * op->gs;
         sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
         return;
     case MLB_OP_DIPOLE:
     case MLB_OP_LONGRANGE:
     case MLB_OP_LONGRANGE3D: {
-        if (s->capturing && op->plan_dirty) fail(MLB_ESTATE, "tensor changed during capture");
-        build_plan(op, s->st);
+        if (s->capturing && (op->plan_dirty || !op->plan || op->plan->rb != s->rb))
+            fail(MLB_ESTATE, "tensor changed during capture");
+        build_plan(op, s->st, s->rb);
         sl.used = true;
         sl.terms.clear();
         sl.base_data = false;
         slot_alloc(s, sl);
         ConvPlan& P = *op->plan;
-        P.k.g = (float)(op->g * op->gs / ((double)P.k.Px * P.k.Py * P.k.Pz));
+        P.k.g = op->g * op->gs / ((double)P.k.Px * P.k.Py * P.k.Pz);
         sl.state = ST_DATA;
         if (s->dry) return;
-        const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
-        if (mlb::conv_fast_ok(P.k))
-            CK(mlb::launch_conv_fast(P.k, P.L, P.tw.p, sp, P.spec.p, P.ten6.p, sl.h, s->st));
-        else
-            CK(mlb::launch_conv(P.k, P.L[0], P.L[1], P.L[2], P.tw.p, sp, P.spec.p, P.ten6.p, P.ten9.p, sl.h, s->st));
+        if (s->rb == 4 && mlb::conv_fast_ok(P.k)) {
+            const float* sp[3] = {static_cast<const float*>(s->sp[s->cur][0]), static_cast<const float*>(s->sp[s->cur][1]),
+                                  static_cast<const float*>(s->sp[s->cur][2])};
+            float* h[3] = {static_cast<float*>(sl.h[0]), static_cast<float*>(sl.h[1]), static_cast<float*>(sl.h[2])};
+            CK(mlb::launch_conv_fast(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), sp,
+                                     reinterpret_cast<float2*>(P.spec.p), reinterpret_cast<const float*>(P.ten6.p), h,
+                                     s->st));
+        } else {
+            const void* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+            CK(mlb::launch_conv(P.k, P.L[0], P.L[1], P.L[2], P.tw.p, sp, P.spec.p, P.ten6.p, P.ten9.p, sl.h, s->rb,
+                                s->st));
+        }
         sl.state = ST_DATA;
         return;
     }
@@ -985,9 +1040,9 @@ LlgK llgk(const mlb_llg* l, double dt)
     k.type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
     k.thermal_only_first_term = l->tof;
     k.renorm = l->disable_renorm ? 0 : 1;
-    k.precess = (float)l->precess;
-    k.damp = (float)l->damp;
-    k.dt = (float)dt;
+    k.precess = l->precess;
+    k.damp = l->damp;
+    k.dt = dt;
     k.dt_zero = dt == 0.0 ? 1 : 0;
     return k;
 }
@@ -997,7 +1052,7 @@ LlgK llgk(const mlb_llg* l, double dt)
 bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, double dt_sys, FastK& F)
 {
     refresh_ms(s);
-    if (!s->ms_uniform || !(s->ms_u > 0.f) || s->sa || s->sg) return false;
+    if (s->rb != 4 || !s->ms_uniform || !(s->ms_u > 0.0) || s->sa || s->sg) return false;
     if (T.ex.mode == EX_CSR || T.ani.mode == ANI_CSR || T.uni.mode != ANI_NONE || T.cub.mode != ANI_NONE) return false;
     if (T.th.mode == TH_INJECT || (T.th.mode == TH_PHILOX && T.th.scale)) return false;
     if (T.nadd > 1 || (T.nadd == 1 && T.add_is_thermal[0])) return false;
@@ -1012,19 +1067,19 @@ bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, dou
     }
     F.ani = T.ani.mode == ANI_UNIFORM;
     if (F.ani) {
-        for (int c = 0; c < 3; c++) F.axis[c] = T.ani.axis[c];
+        for (int c = 0; c < 3; c++) F.axis[c] = (float)T.ani.axis[c];
         F.ani_c = (float)(2.0 * (double)T.ani.K / (ms * ms));
     }
-    F.th = T.th.mode == TH_PHILOX && T.th.T != 0.f && g > 0;
+    F.th = T.th.mode == TH_PHILOX && T.th.T != 0.0 && g > 0;
     if (F.th) {
         F.sigma = (float)std::sqrt((2.0 * a * (double)T.th.T) / (ms * dt_sys * g));
         F.seed = T.th.seed; F.counter = T.th.counter; F.dctr = T.th.dctr;
     }
     if (T.zee.on) {
-        for (int c = 0; c < 3; c++) F.B[c] = T.zee.B[c];
+        for (int c = 0; c < 3; c++) F.B[c] = (float)T.zee.B[c];
         F.Bdev = T.zee.Bdev;
     }
-    F.addw = T.nadd == 1 ? T.addw[0] : 0.f;
+    F.addw = T.nadd == 1 ? (float)T.addw[0] : 0.f;
     F.llg_type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
     F.tof = l->tof;
     F.renorm = l->disable_renorm ? 0 : 1;
@@ -1069,17 +1124,21 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         return false;
     }
     if (th >= 0 && !th_in && s->slots[th].state == ST_DATA) {
-        if (!add_addend(T, s->slots[th].h, 0.f, true)) return false;
+        if (!add_addend(T, s->slots[th].h, 0.0, true)) return false;
     }
     const int nb = 1 - s->cur;
     FastK F;
     if (s->dry) {
         // bookkeeping only: the kernels of this step ran in a captured graph
     } else if (fast_fused(s, T, l, dt, dt_sys, F)) {
-        const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+        const float* sp[3];
         const float* ad[3] = {nullptr, nullptr, nullptr};
-        if (T.nadd == 1) for (int c = 0; c < 3; c++) ad[c] = T.add[0][c];
-        float* out[3] = {s->sp[nb][0], s->sp[nb][1], s->sp[nb][2]};
+        float* out[3];
+        for (int c = 0; c < 3; c++) {
+            sp[c] = static_cast<const float*>(s->sp[s->cur][c]);
+            out[c] = static_cast<float*>(s->sp[nb][c]);
+            if (T.nadd == 1) ad[c] = static_cast<const float*>(T.add[0][c]);
+        }
         CK(mlb::launch_fused_fast(F, sp, ad, out, s->st));
     } else {
         FusedK P;
@@ -1087,7 +1146,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         P.terms = T;
         P.llg = llgk(l, dt);
         P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
-        CK(mlb::launch_fused(P, (float)dt_sys, s->st));
+        CK(mlb::launch_fused(P, dt_sys, s->rb, s->st));
     }
     if (s->capturing) CK(mlb::launch_advance_step(s->dstep, s->st));
     s->cur = nb;
@@ -1100,6 +1159,7 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
     if (from->nx != dmdt->nx || from->nx != to->nx || from->ny != dmdt->ny || from->ny != to->ny ||
         from->nz != dmdt->nz || from->nz != to->nz)
         fail(MLB_EINVAL, "SpinSystems of different sizes");
+    if (from->rb != dmdt->rb || from->rb != to->rb) fail(MLB_EINVAL, "SpinSystems of different precisions");
     const double dt = scale * dmdt->dt;
     const bool cart = l->kind != MLB_LLG_QUATERNION;
     bool done = false;
@@ -1114,7 +1174,7 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
         materialize_all(to);
         if (to != dmdt) { materialize(dmdt, 0); if (th >= 0) materialize(dmdt, th); }
         if (from != to && !(cart && dt == 0.0)) {
-            CK(cudaMemcpyAsync(to->ms, from->ms, sizeof(float) * from->n, cudaMemcpyDeviceToDevice, to->st));
+            CK(cudaMemcpyAsync(to->ms, from->ms, (size_t)from->rb * from->n, cudaMemcpyDeviceToDevice, to->st));
             to->ms_host = from->ms_host;
             to->ms_dirty = true;
         }
@@ -1122,13 +1182,13 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
             CK(cudaStreamSynchronize(from->st));
             CK(cudaStreamSynchronize(dmdt->st));
         }
-        const float* m[3] = {dmdt->sp[dmdt->cur][0], dmdt->sp[dmdt->cur][1], dmdt->sp[dmdt->cur][2]};
-        const float* H[3] = {dmdt->slots[0].h[0], dmdt->slots[0].h[1], dmdt->slots[0].h[2]};
-        const float* Ht[3] = {nullptr, nullptr, nullptr};
+        const void* m[3] = {dmdt->sp[dmdt->cur][0], dmdt->sp[dmdt->cur][1], dmdt->sp[dmdt->cur][2]};
+        const void* H[3] = {dmdt->slots[0].h[0], dmdt->slots[0].h[1], dmdt->slots[0].h[2]};
+        const void* Ht[3] = {nullptr, nullptr, nullptr};
         if (th >= 0) for (int c = 0; c < 3; c++) Ht[c] = dmdt->slots[th].h[c];
-        float* out[3] = {to->sp[to->cur][0], to->sp[to->cur][1], to->sp[to->cur][2]};
-        CK(mlb::launch_llg(sysk(from, from->cur), m, H, Ht, dmdt->sa, dmdt->sg, (float)dmdt->alpha,
-                           (float)dmdt->gamma, llgk(l, dt), out, to->st));
+        void* out[3] = {to->sp[to->cur][0], to->sp[to->cur][1], to->sp[to->cur][2]};
+        CK(mlb::launch_llg(sysk(from, from->cur), m, H, Ht, dmdt->sa, dmdt->sg, dmdt->alpha, dmdt->gamma,
+                           llgk(l, dt), out, to->rb, to->st));
     }
     if (cart) {
         if (dt != 0.0 && advance) to->time = from->time + dt;
@@ -1166,23 +1226,25 @@ void spins_changing(mlb_system* s)
     materialize_all(s);
 }
 
-mlb_system* make_system(int nx, int ny, int nz)
+mlb_system* make_system(int nx, int ny, int nz, int rb)
 {
+    if (rb != 4 && rb != 8) fail(MLB_EINVAL, "bytes per real must be 4 or 8");
     if (nx < 1 || ny < 1 || nz < 1) fail(MLB_EINVAL, "dimensions must be positive");
     const long long n = (long long)nx * ny * nz;
     if (n > (1LL << 31) - 1) fail(MLB_EUNSUP, "more than 2^31-1 sites");
     std::unique_ptr<mlb_system> s(new mlb_system());
     s->nx = nx; s->ny = ny; s->nz = nz; s->n = (int)n;
+    s->rb = rb;
     CK(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking));
     s->st = s->own;
     for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++) {
-            CK(cudaMalloc(&s->sp[b][c], sizeof(float) * n));
-            CK(cudaMemset(s->sp[b][c], 0, sizeof(float) * n));
+            CK(cudaMalloc(&s->sp[b][c], (size_t)rb * n));
+            CK(cudaMemset(s->sp[b][c], 0, (size_t)rb * n));
         }
-    CK(cudaMalloc(&s->ms, sizeof(float) * n));
-    CK(cudaMemset(s->ms, 0, sizeof(float) * n));
-    s->ms_host.assign(n, 0.f);
+    CK(cudaMalloc(&s->ms, (size_t)rb * n));
+    CK(cudaMemset(s->ms, 0, (size_t)rb * n));
+    s->ms_host.assign(n, 0.0);
     s->ms_dirty = true;
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
@@ -1214,7 +1276,7 @@ void free_system(mlb_system* s)
     delete s;
 }
 
-void upload_site_array(mlb_system* s, float** dst, const double* a)
+void upload_site_array(mlb_system* s, void** dst, const double* a)
 {
     spins_changing(s);
     if (!a) {
@@ -1222,10 +1284,8 @@ void upload_site_array(mlb_system* s, float** dst, const double* a)
         *dst = nullptr;
         return;
     }
-    std::vector<float> f(s->n);
-    for (int i = 0; i < s->n; i++) f[i] = (float)a[i];
-    if (!*dst) CK(cudaMalloc(dst, sizeof(float) * s->n));
-    CK(cudaMemcpyAsync(*dst, f.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+    if (!*dst) CK(cudaMalloc(dst, (size_t)s->rb * s->n));
+    put_reals(s, *dst, a, s->n);
     CK(cudaStreamSynchronize(s->st));
 }
 
@@ -1272,7 +1332,7 @@ void load_state(mlb_system* s, const std::vector<mlb_op*>& ops, const HostState&
     s->cur = h.cur; s->gen = h.gen; s->time = h.time; s->last_fused = h.last_fused;
     for (size_t i = 0; i < s->slots.size(); i++) {
         Slot& x = s->slots[i];
-        float* keep[3] = {x.h[0], x.h[1], x.h[2]};
+        void* keep[3] = {x.h[0], x.h[1], x.h[2]};
         if (i < h.slots.size()) {
             const bool had = h.slots[i].h[0] != nullptr;
             x = h.slots[i];
@@ -1384,7 +1444,7 @@ void plan_launch(mlb_plan* p, int nsteps)
     for (mlb_op* o : p->ops) {
         if (o->kind == MLB_OP_THERMAL) h.th_counter = o->counter;
         if (o->kind == MLB_OP_APPLIEDFIELD)
-            for (int a = 0; a < 3; a++) { h.B[a] = (float)(o->B[a] * o->gs); h.dB[a] = (float)(o->dB[a] * o->gs); }
+            for (int a = 0; a < 3; a++) { h.B[a] = o->B[a] * o->gs; h.dB[a] = o->dB[a] * o->gs; }
     }
     CK(cudaMemcpyAsync(s->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
     for (int k = 0; k < nsteps; k++) {
@@ -1528,7 +1588,9 @@ void ens_enqueue_step(mlb_ensemble* e, int q)
             ConvPlan& P = *c.dip->plan;
             const float* cs[3] = {s[0] + c.base, s[1] + c.base, s[2] + c.base};
             float* ch[3] = {e->H[0] + c.base, e->H[1] + c.base, e->H[2] + c.base};
-            CK(mlb::launch_conv_fast(P.k, P.L, P.tw.p, cs, P.spec.p, P.ten6.p, ch, e->st));
+            CK(mlb::launch_conv_fast(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), cs,
+                                     reinterpret_cast<float2*>(P.spec.p), reinterpret_cast<const float*>(P.ten6.p), ch,
+                                     e->st));
         }
         for (int q3 = 0; q3 < 3; q3++) add[q3] = e->H[q3];
     }
@@ -1595,12 +1657,12 @@ void ens_prepare(mlb_ensemble* e)
             k.dip->open[2] = 1;
             k.dip->t6_valid = false;
             k.dip->plan_dirty = true;
-            build_plan(k.dip, e->st);
+            build_plan(k.dip, e->st, 4);
             ConvPlan& P = *k.dip->plan;
             if (!mlb::conv_fast_ok(P.k)) fail(MLB_EUNSUP, "ensemble size class outside the fast FFT sizes");
             P.k.nrep = k.nrep;
-            P.k.g = (float)(c.g / ((double)P.k.Px * P.k.Py * P.k.Pz));
-            P.spec.alloc((size_t)P.k.Kx * 3 * k.nz * k.ny * k.nrep);
+            P.k.g = c.g / ((double)P.k.Px * P.k.Py * P.k.Pz);
+            P.spec.alloc((size_t)P.k.Kx * 3 * k.nz * k.ny * k.nrep * sizeof(float2));
         }
     }
     ens_autotune(e);
@@ -1668,8 +1730,21 @@ int mlb_system_create(int nx, int ny, int nz, mlb_system** out)
 {
     return guard([&] {
         if (!out) fail(MLB_EINVAL, "null output");
-        *out = make_system(nx, ny, nz);
+        *out = make_system(nx, ny, nz, 4);
     });
+}
+
+int mlb_system_create_ex(int nx, int ny, int nz, int real_bytes, mlb_system** out)
+{
+    return guard([&] {
+        if (!out) fail(MLB_EINVAL, "null output");
+        *out = make_system(nx, ny, nz, real_bytes);
+    });
+}
+
+int mlb_system_real_bytes(const mlb_system* s, int* out)
+{
+    return guard([&] { *out = s->rb; });
 }
 
 int mlb_system_destroy(mlb_system* s)
@@ -1710,11 +1785,11 @@ int mlb_system_set_spin(mlb_system* s, int idx, double sx, double sy, double sz)
         g_version++;
         if (idx < 0 || idx >= s->n) fail(MLB_ERANGE, "site outside the SpinSystem");
         spins_changing(s);
-        const float v[3] = {(float)sx, (float)sy, (float)sz};
-        for (int c = 0; c < 3; c++)
-            CK(cudaMemcpyAsync(s->sp[s->cur][c] + idx, &v[c], sizeof(float), cudaMemcpyHostToDevice, s->st));
-        s->ms_host[idx] = (float)std::sqrt(sx * sx + sy * sy + sz * sz);
-        CK(cudaMemcpyAsync(s->ms + idx, &s->ms_host[idx], sizeof(float), cudaMemcpyHostToDevice, s->st));
+        const double v[3] = {sx, sy, sz};
+        for (int c = 0; c < 3; c++) put_reals(s, elem(s->sp[s->cur][c], idx, s->rb), &v[c], 1);
+        const double m = std::sqrt(sx * sx + sy * sy + sz * sz);
+        put_reals(s, elem(s->ms, idx, s->rb), &m, 1);
+        s->ms_host[idx] = round_to(m, s->rb);
         s->ms_dirty = true;
         CK(cudaStreamSynchronize(s->st));
     });
@@ -1724,11 +1799,8 @@ int mlb_system_get_spin(mlb_system* s, int idx, double out4[4])
 {
     return guard([&] {
         if (idx < 0 || idx >= s->n) fail(MLB_ERANGE, "site outside the SpinSystem");
-        float v[3];
-        for (int c = 0; c < 3; c++)
-            CK(cudaMemcpyAsync(&v[c], s->sp[s->cur][c] + idx, sizeof(float), cudaMemcpyDeviceToHost, s->st));
-        CK(cudaStreamSynchronize(s->st));
-        out4[0] = v[0]; out4[1] = v[1]; out4[2] = v[2]; out4[3] = s->ms_host[idx];
+        for (int c = 0; c < 3; c++) get_reals(s, &out4[c], elem(s->sp[s->cur][c], idx, s->rb), 1);
+        out4[3] = s->ms_host[idx];
     });
 }
 
@@ -1738,16 +1810,12 @@ int mlb_system_set_spins(mlb_system* s, const double* x, const double* y, const 
         g_version++;
         if (!x || !y || !z) fail(MLB_EINVAL, "null spin array");
         spins_changing(s);
-        std::vector<float> f[3];
         const double* src[3] = {x, y, z};
-        for (int c = 0; c < 3; c++) {
-            f[c].resize(s->n);
-            for (int i = 0; i < s->n; i++) f[c][i] = (float)src[c][i];
-            CK(cudaMemcpyAsync(s->sp[s->cur][c], f[c].data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
-        }
+        for (int c = 0; c < 3; c++) put_reals(s, s->sp[s->cur][c], src[c], s->n);
         for (int i = 0; i < s->n; i++)
-            s->ms_host[i] = ms ? (float)ms[i] : (float)std::sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
-        CK(cudaMemcpyAsync(s->ms, s->ms_host.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+            s->ms_host[i] = ms ? ms[i] : std::sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+        put_reals(s, s->ms, s->ms_host.data(), s->n);
+        for (int i = 0; i < s->n; i++) s->ms_host[i] = round_to(s->ms_host[i], s->rb);
         s->ms_dirty = true;
         CK(cudaStreamSynchronize(s->st));
     });
@@ -1756,14 +1824,9 @@ int mlb_system_set_spins(mlb_system* s, const double* x, const double* y, const 
 int mlb_system_get_spins(mlb_system* s, double* x, double* y, double* z, double* ms)
 {
     return guard([&] {
-        std::vector<float> f(s->n);
         double* dst[3] = {x, y, z};
-        for (int c = 0; c < 3; c++) {
-            if (!dst[c]) continue;
-            CK(cudaMemcpyAsync(f.data(), s->sp[s->cur][c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
-            CK(cudaStreamSynchronize(s->st));
-            for (int i = 0; i < s->n; i++) dst[c][i] = f[i];
-        }
+        for (int c = 0; c < 3; c++)
+            if (dst[c]) get_reals(s, dst[c], s->sp[s->cur][c], s->n);
         if (ms)
             for (int i = 0; i < s->n; i++) ms[i] = s->ms_host[i];
     });
@@ -1775,15 +1838,24 @@ int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const f
         g_version++;
         spins_changing(s);
         const float* src[3] = {x, y, z};
-        for (int c = 0; c < 3; c++)
-            CK(cudaMemcpyAsync(s->sp[s->cur][c], src[c], sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
-        if (ms) {
-            CK(cudaMemcpyAsync(s->ms, ms, sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
-            if (memcmp(s->ms_host.data(), ms, sizeof(float) * s->n) != 0) {
-                memcpy(s->ms_host.data(), ms, sizeof(float) * s->n);
-                s->ms_dirty = true;
+        if (s->rb == 4) {
+            for (int c = 0; c < 3; c++)
+                CK(cudaMemcpyAsync(s->sp[s->cur][c], src[c], sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+            if (ms) CK(cudaMemcpyAsync(s->ms, ms, sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
+        } else {
+            std::vector<double> d(s->n);
+            for (int c = 0; c < 3; c++) {
+                for (int i = 0; i < s->n; i++) d[i] = src[c][i];
+                put_reals(s, s->sp[s->cur][c], d.data(), s->n);
+            }
+            if (ms) {
+                for (int i = 0; i < s->n; i++) d[i] = ms[i];
+                put_reals(s, s->ms, d.data(), s->n);
             }
         }
+        if (ms)
+            for (int i = 0; i < s->n; i++)
+                if (s->ms_host[i] != (double)ms[i]) { s->ms_host[i] = ms[i]; s->ms_dirty = true; }
     });
 }
 
@@ -1791,8 +1863,18 @@ int mlb_system_download_f32(mlb_system* s, float* x, float* y, float* z)
 {
     return guard([&] {
         float* dst[3] = {x, y, z};
-        for (int c = 0; c < 3; c++)
-            if (dst[c]) CK(cudaMemcpyAsync(dst[c], s->sp[s->cur][c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
+        if (s->rb == 4) {
+            for (int c = 0; c < 3; c++)
+                if (dst[c])
+                    CK(cudaMemcpyAsync(dst[c], s->sp[s->cur][c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
+        } else {
+            std::vector<double> d(s->n);
+            for (int c = 0; c < 3; c++) {
+                if (!dst[c]) continue;
+                get_reals(s, d.data(), s->sp[s->cur][c], s->n);
+                for (int i = 0; i < s->n; i++) dst[c][i] = (float)d[i];
+            }
+        }
     });
 }
 
@@ -1862,13 +1944,13 @@ int mlb_system_sum_fields_custom(mlb_system* s, const char* dest, int n, const c
         before_mutate(s, d);
         // materialise the sources and the destination, then a weighted sum
         std::vector<int> idx;
-        std::vector<float> ww;
+        std::vector<double> ww;
         for (int k = 0; k < n; k++) {
             const int j = slot_find(s, src[k]);
             if (j < 0 || !s->slots[j].used) continue;
             materialize(s, j);
             idx.push_back(j);
-            ww.push_back((float)(w ? w[k] : 1.0));
+            ww.push_back(w ? w[k] : 1.0);
         }
         Slot& out = s->slots[d];
         out.terms.clear();
@@ -1901,14 +1983,9 @@ int mlb_system_get_field(mlb_system* s, const char* slot, double* hx, double* hy
         const int j = slot_find(s, slot);
         if (j < 0) fail(MLB_ENOTFOUND, std::string("Unknown field type `") + slot + "'");
         materialize(s, j);
-        std::vector<float> f(s->n);
         double* dst[3] = {hx, hy, hz};
-        for (int c = 0; c < 3; c++) {
-            if (!dst[c]) continue;
-            CK(cudaMemcpyAsync(f.data(), s->slots[j].h[c], sizeof(float) * s->n, cudaMemcpyDeviceToHost, s->st));
-            CK(cudaStreamSynchronize(s->st));
-            for (int i = 0; i < s->n; i++) dst[c][i] = f[i];
-        }
+        for (int c = 0; c < 3; c++)
+            if (dst[c]) get_reals(s, dst[c], s->slots[j].h[c], s->n);
     });
 }
 
@@ -1919,14 +1996,10 @@ int mlb_system_set_field(mlb_system* s, const char* slot, const double* hx, cons
         const int j = slot_register(s, slot);
         before_mutate(s, j);
         materialize(s, j);
-        std::vector<float> f(s->n);
         const double* src[3] = {hx, hy, hz};
-        for (int c = 0; c < 3; c++) {
-            if (!src[c]) continue;
-            for (int i = 0; i < s->n; i++) f[i] = (float)src[c][i];
-            CK(cudaMemcpyAsync(s->slots[j].h[c], f.data(), sizeof(float) * s->n, cudaMemcpyHostToDevice, s->st));
-            CK(cudaStreamSynchronize(s->st));
-        }
+        for (int c = 0; c < 3; c++)
+            if (src[c]) put_reals(s, s->slots[j].h[c], src[c], s->n);
+        CK(cudaStreamSynchronize(s->st));
     });
 }
 
@@ -1957,7 +2030,7 @@ int mlb_system_netmoment(mlb_system* s, double m, double out8[8])
 {
     return guard([&] {
         CK(mlb::launch_netmoment(s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2], s->n, m, s->red, s->red_nb,
-                                 s->redout, s->st));
+                                 s->redout, s->rb, s->st));
         double r[6];
         CK(cudaMemcpyAsync(r, s->redout, sizeof(r), cudaMemcpyDeviceToHost, s->st));
         CK(cudaStreamSynchronize(s->st));
@@ -1974,9 +2047,9 @@ int mlb_system_field_dot(mlb_system* s, const char* slot, double* out)
         const int j = slot_find(s, slot);
         if (j < 0) fail(MLB_ENOTFOUND, std::string("Unknown field type `") + slot + "'");
         materialize(s, j);
-        const float* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
-        const float* h[3] = {s->slots[j].h[0], s->slots[j].h[1], s->slots[j].h[2]};
-        CK(mlb::launch_dot(sp, h, s->n, s->red, s->red_nb, s->redout, s->st));
+        const void* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+        const void* h[3] = {s->slots[j].h[0], s->slots[j].h[1], s->slots[j].h[2]};
+        CK(mlb::launch_dot(sp, h, s->n, s->red, s->red_nb, s->redout, s->rb, s->st));
         CK(cudaMemcpyAsync(out, s->redout, sizeof(double), cudaMemcpyDeviceToHost, s->st));
         CK(cudaStreamSynchronize(s->st));
     });
@@ -1987,13 +2060,14 @@ int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
     return guard([&] {
         g_version++;
         if (dst->nx != src->nx || dst->ny != src->ny || dst->nz != src->nz) fail(MLB_EINVAL, "size mismatch");
+        if (dst->rb != src->rb) fail(MLB_EINVAL, "precision mismatch");
         if (dst == src) return;
+        const size_t bytes = (size_t)src->rb * src->n;
         spins_changing(dst);
         CK(cudaStreamSynchronize(src->st));
         for (int c = 0; c < 3; c++)
-            CK(cudaMemcpyAsync(dst->sp[dst->cur][c], src->sp[src->cur][c], sizeof(float) * src->n,
-                               cudaMemcpyDeviceToDevice, dst->st));
-        CK(cudaMemcpyAsync(dst->ms, src->ms, sizeof(float) * src->n, cudaMemcpyDeviceToDevice, dst->st));
+            CK(cudaMemcpyAsync(dst->sp[dst->cur][c], src->sp[src->cur][c], bytes, cudaMemcpyDeviceToDevice, dst->st));
+        CK(cudaMemcpyAsync(dst->ms, src->ms, bytes, cudaMemcpyDeviceToDevice, dst->st));
         dst->ms_host = src->ms_host;
         dst->ms_dirty = true;
         dst->alpha = src->alpha; dst->gamma = src->gamma; dst->dt = src->dt; dst->time = src->time;
@@ -2001,12 +2075,12 @@ int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
         upload_site_array(dst, &dst->sa, nullptr);
         upload_site_array(dst, &dst->sg, nullptr);
         if (src->sa) {
-            CK(cudaMalloc(&dst->sa, sizeof(float) * src->n));
-            CK(cudaMemcpy(dst->sa, src->sa, sizeof(float) * src->n, cudaMemcpyDeviceToDevice));
+            CK(cudaMalloc(&dst->sa, bytes));
+            CK(cudaMemcpy(dst->sa, src->sa, bytes, cudaMemcpyDeviceToDevice));
         }
         if (src->sg) {
-            CK(cudaMalloc(&dst->sg, sizeof(float) * src->n));
-            CK(cudaMemcpy(dst->sg, src->sg, sizeof(float) * src->n, cudaMemcpyDeviceToDevice));
+            CK(cudaMalloc(&dst->sg, bytes));
+            CK(cudaMemcpy(dst->sg, src->sg, bytes, cudaMemcpyDeviceToDevice));
         }
         if (with_fields) {
             materialize_all(src);
@@ -2018,7 +2092,7 @@ int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
                 if (x.state == ST_DATA) {
                     slot_alloc(dst, y);
                     for (int c = 0; c < 3; c++)
-                        CK(cudaMemcpy(y.h[c], x.h[c], sizeof(float) * src->n, cudaMemcpyDeviceToDevice));
+                        CK(cudaMemcpy(y.h[c], x.h[c], bytes, cudaMemcpyDeviceToDevice));
                     y.state = ST_DATA;
                 }
             }
@@ -2304,11 +2378,9 @@ int mlb_thermal_inject(mlb_op* op, const double* nx, const double* ny, const dou
         if (op->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "not a Thermal operator");
         const int n = op->nx * op->ny * op->nz;
         const double* src[3] = {nx, ny, nz};
-        std::vector<float> f(n);
         for (int c = 0; c < 3; c++) {
             op->inj[c].alloc(n);
-            for (int i = 0; i < n; i++) f[i] = (float)src[c][i];
-            CK(cudaMemcpy(op->inj[c].p, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(op->inj[c].p, src[c], sizeof(double) * n, cudaMemcpyHostToDevice));
         }
         op->inject_pending = true;
     });
@@ -2401,7 +2473,7 @@ int mlb_longrange_set_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double 
         if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
             cudaStream_t st;
             CK(cudaStreamCreate(&st));
-            build_plan(op, st);
+            build_plan(op, st, op->plan ? op->plan->rb : 4);
             cudaStreamDestroy(st);
         }
         ensure_t6_layout(op);
@@ -2423,7 +2495,7 @@ int mlb_longrange_get_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double*
         if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
             cudaStream_t st;
             CK(cudaStreamCreate(&st));
-            build_plan(op, st);
+            build_plan(op, st, op->plan ? op->plan->rb : 4);
             cudaStreamDestroy(st);
         }
         ensure_t6_layout(op);
@@ -2440,7 +2512,7 @@ int mlb_longrange_get_tensor(mlb_op* op, double* const t6[6])
             if (op->open[0] || op->open[1]) fail(MLB_EUNSUP, "open-boundary tensor has no reference layout");
             cudaStream_t st;
             CK(cudaStreamCreate(&st));
-            build_plan(op, st);
+            build_plan(op, st, op->plan ? op->plan->rb : 4);
             cudaStreamDestroy(st);
         }
         ensure_t6_layout(op);
@@ -2720,7 +2792,7 @@ int mlb_ensemble_run(mlb_ensemble* e, int nsteps)
         DevStep h;
         memset(&h, 0, sizeof(h));
         h.th_counter = e->counter;
-        for (int a = 0; a < 3; a++) { h.B[a] = (float)e->B[a]; h.dB[a] = (float)e->cfg.dB[a]; }
+        for (int a = 0; a < 3; a++) { h.B[a] = e->B[a]; h.dB[a] = e->cfg.dB[a]; }
         CK(cudaMemcpyAsync(e->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, e->st));
         const bool cart = e->cfg.llg != MLB_LLG_QUATERNION;
         for (int k = 0; k < nsteps; k++) {

@@ -302,7 +302,7 @@ __device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int N
     const int nxy = NX * NY;
     const float Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
     float Hx, Hy, Hz;
-    if (F.Bdev) { Hx = F.Bdev[0]; Hy = F.Bdev[1]; Hz = F.Bdev[2]; }
+    if (F.Bdev) { Hx = (float)F.Bdev[0]; Hy = (float)F.Bdev[1]; Hz = (float)F.Bdev[2]; }
     else { Hx = F.B[0]; Hy = F.B[1]; Hz = F.B[2]; }
     if (EXS) {
         float ex = 0.f, ey = 0.f, ez = 0.f;

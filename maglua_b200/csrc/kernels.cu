@@ -23,28 +23,39 @@
 #include <stdio.h>
 
 // ------------------------------------------------------------ helpers
-__device__ __forceinline__ float ms_at(const SysK& s, int i) { return s.ms_uniform ? s.ms_u : __ldg(s.ms + i); }
-__device__ __forceinline__ float alpha_at(const SysK& s, int i) { return s.site_alpha ? __ldg(s.site_alpha + i) : s.alpha; }
-__device__ __forceinline__ float gamma_at(const SysK& s, int i) { return s.site_gamma ? __ldg(s.site_gamma + i) : s.gamma; }
-__device__ __forceinline__ float3 f3(float a, float b, float c) { return make_float3(a, b, c); }
-__device__ __forceinline__ float3 add3(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
-__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
-__device__ __forceinline__ float3 scl3(float a, float3 b) { return f3(a * b.x, a * b.y, a * b.z); }
-__device__ __forceinline__ float3 cross3(float3 a, float3 b)
+template <typename R>
+struct V3 {
+    R x, y, z;
+};
+template <typename R> __device__ __forceinline__ V3<R> v3(R a, R b, R c) { V3<R> v; v.x = a; v.y = b; v.z = c; return v; }
+template <typename R> __device__ __forceinline__ V3<R> add3(V3<R> a, V3<R> b) { return v3<R>(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <typename R> __device__ __forceinline__ V3<R> sub3(V3<R> a, V3<R> b) { return v3<R>(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <typename R> __device__ __forceinline__ V3<R> scl3(R a, V3<R> b) { return v3<R>(a * b.x, a * b.y, a * b.z); }
+template <typename R> __device__ __forceinline__ V3<R> cross3(V3<R> a, V3<R> b)
 {
-    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    return v3<R>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-__device__ __forceinline__ float3 spin_at(const SysK& s, int i)
+template <typename R> __device__ __forceinline__ R ldr(const void* p, int i) { return __ldg(static_cast<const R*>(p) + i); }
+template <typename R> __device__ __forceinline__ R ms_at(const SysK& s, int i) { return s.ms_uniform ? (R)s.ms_u : ldr<R>(s.ms, i); }
+template <typename R> __device__ __forceinline__ R alpha_at(const SysK& s, int i) { return s.site_alpha ? ldr<R>(s.site_alpha, i) : (R)s.alpha; }
+template <typename R> __device__ __forceinline__ R gamma_at(const SysK& s, int i) { return s.site_gamma ? ldr<R>(s.site_gamma, i) : (R)s.gamma; }
+template <typename R> __device__ __forceinline__ V3<R> spin_at(const SysK& s, int i)
 {
-    return f3(__ldg(s.x + i), __ldg(s.y + i), __ldg(s.z + i));
+    return v3<R>(ldr<R>(s.x, i), ldr<R>(s.y, i), ldr<R>(s.z, i));
 }
+template <typename R> __device__ __forceinline__ R rsq(R v);
+template <> __device__ __forceinline__ float rsq<float>(float v) { return sqrtf(v); }
+template <> __device__ __forceinline__ double rsq<double>(double v) { return sqrt(v); }
+__device__ __forceinline__ void sincos_r(float v, float* s, float* c) { sincosf(v, s, c); }
+__device__ __forceinline__ void sincos_r(double v, double* s, double* c) { sincos(v, s, c); }
 
 // ------------------------------------------------------------ field terms
 // Exchange: h_t += J s_f / (m_f m_t) (normalised) or J s_f / m_f, only for
 // m_f != 0 (M/cpu/exchange/spinoperationexchange.cpp:134-213).
-__device__ __forceinline__ float3 ex_term(const ExchangeK& e, const SysK& s, int i, float mt)
+template <typename R>
+__device__ __forceinline__ V3<R> ex_term(const ExchangeK& e, const SysK& s, int i, R mt)
 {
-    float3 h = f3(0.f, 0.f, 0.f);
+    V3<R> h = v3<R>(0, 0, 0);
     if (e.mode == EX_STENCIL) {
         const int ix = i % s.nx;
         const int iy = (i / s.nx) % s.ny;
@@ -52,8 +63,8 @@ __device__ __forceinline__ float3 ex_term(const ExchangeK& e, const SysK& s, int
         const int nxy = s.nx * s.ny;
 #pragma unroll
         for (int d = 0; d < 6; d++) {
-            const float J = e.J[d];
-            if (J == 0.f) continue;
+            const R J = (R)e.J[d];
+            if (J == (R)0) continue;
             const int ax = d >> 1;
             const int sg = (d & 1) ? -1 : 1;
             int c = ax == 0 ? ix : (ax == 1 ? iy : iz);
@@ -64,23 +75,23 @@ __device__ __forceinline__ float3 ex_term(const ExchangeK& e, const SysK& s, int
                 c = c < 0 ? c + n : c - n;
             }
             const int f = ax == 0 ? (i - ix + c) : (ax == 1 ? (i + (c - iy) * s.nx) : (i + (c - iz) * nxy));
-            const float mf = ms_at(s, f);
-            if (mf != 0.f) {
-                const float3 sf = spin_at(s, f);
-                const float den = e.normalize ? mf * mt : mf;
-                h = add3(h, f3(sf.x * J / den, sf.y * J / den, sf.z * J / den));
+            const R mf = ms_at<R>(s, f);
+            if (mf != (R)0) {
+                const V3<R> sf = spin_at<R>(s, f);
+                const R den = e.normalize ? mf * mt : mf;
+                h = add3(h, v3<R>(sf.x * J / den, sf.y * J / den, sf.z * J / den));
             }
         }
     } else if (e.mode == EX_CSR) {
         const int p0 = __ldg(e.ptr + i), p1 = __ldg(e.ptr + i + 1);
         for (int p = p0; p < p1; p++) {
             const int f = __ldg(e.col + p);
-            const float J = __ldg(e.val + p);
-            const float mf = ms_at(s, f);
-            if (mf != 0.f) {
-                const float3 sf = spin_at(s, f);
-                const float den = e.normalize ? mf * mt : mf;
-                h = add3(h, f3(sf.x * J / den, sf.y * J / den, sf.z * J / den));
+            const R J = (R)__ldg(e.val + p);
+            const R mf = ms_at<R>(s, f);
+            if (mf != (R)0) {
+                const V3<R> sf = spin_at<R>(s, f);
+                const R den = e.normalize ? mf * mt : mf;
+                h = add3(h, v3<R>(sf.x * J / den, sf.y * J / den, sf.z * J / den));
             }
         }
     }
@@ -89,83 +100,94 @@ __device__ __forceinline__ float3 ex_term(const ExchangeK& e, const SysK& s, int
 
 // Anisotropy: H = 2K (s.n)/ms^2 n for ms > 0
 // (M/cpu/anisotropy/spinoperationanisotropy.cpp:247-283).
-__device__ __forceinline__ float3 ani_one(float3 sp, float ms, const float* n, float K)
+template <typename R>
+__device__ __forceinline__ V3<R> ani_one(V3<R> sp, R ms, R n0, R n1, R n2, R K)
 {
-    const float sda = sp.x * n[0] + sp.y * n[1] + sp.z * n[2];
-    const float v = 2.0f * K * sda / (ms * ms);
-    return f3(n[0] * v, n[1] * v, n[2] * v);
+    const R sda = sp.x * n0 + sp.y * n1 + sp.z * n2;
+    const R v = (R)2 * K * sda / (ms * ms);
+    return v3<R>(n0 * v, n1 * v, n2 * v);
 }
-__device__ __forceinline__ float3 ani_term(const AniK& a, float3 sp, float ms, int i)
+template <typename R>
+__device__ __forceinline__ V3<R> ani_term(const AniK& a, V3<R> sp, R ms, int i)
 {
-    float3 h = f3(0.f, 0.f, 0.f);
-    if (!(ms > 0.f)) return h;
-    if (a.mode == ANI_UNIFORM) return ani_one(sp, ms, a.axis, a.K);
+    V3<R> h = v3<R>(0, 0, 0);
+    if (!(ms > (R)0)) return h;
+    if (a.mode == ANI_UNIFORM) return ani_one<R>(sp, ms, (R)a.axis[0], (R)a.axis[1], (R)a.axis[2], (R)a.K);
     if (a.mode == ANI_CSR) {
         const int p0 = __ldg(a.ptr + i), p1 = __ldg(a.ptr + i + 1);
-        for (int p = p0; p < p1; p++) {
-            const float n[3] = {__ldg(a.axes + 3 * p), __ldg(a.axes + 3 * p + 1), __ldg(a.axes + 3 * p + 2)};
-            h = add3(h, ani_one(sp, ms, n, __ldg(a.Ks + p)));
-        }
+        for (int p = p0; p < p1; p++)
+            h = add3(h, ani_one<R>(sp, ms, (R)__ldg(a.axes + 3 * p), (R)__ldg(a.axes + 3 * p + 1),
+                                   (R)__ldg(a.axes + 3 * p + 2), (R)__ldg(a.Ks + p)));
     }
     return h;
 }
 
 // Uniaxial: [2K1 u + 4K2 u^3] n with u = s.n of the unit spin; quirk keeps
 // the reference's sz*nx (..._uniaxial.cpp:250-298, :287).
-__device__ __forceinline__ float3 uni_one(float3 u3, const float* n, float K1, float K2, int quirk)
+template <typename R>
+__device__ __forceinline__ V3<R> uni_one(V3<R> u3, R n0, R n1, R n2, R K1, R K2, int quirk)
 {
-    const float u = u3.x * n[0] + u3.y * n[1] + u3.z * (quirk ? n[0] : n[2]);
-    const float mag = 2.0f * K1 * u + 4.0f * K2 * (u * u * u);
-    return f3(n[0] * mag, n[1] * mag, n[2] * mag);
+    const R u = u3.x * n0 + u3.y * n1 + u3.z * (quirk ? n0 : n2);
+    const R mag = (R)2 * K1 * u + (R)4 * K2 * (u * u * u);
+    return v3<R>(n0 * mag, n1 * mag, n2 * mag);
 }
-__device__ __forceinline__ float3 uni_term(const UniK& a, float3 sp, float ms, int i)
+template <typename R>
+__device__ __forceinline__ V3<R> uni_term(const UniK& a, V3<R> sp, R ms, int i)
 {
-    float3 h = f3(0.f, 0.f, 0.f);
-    if (!(ms > 0.f) || a.mode == ANI_NONE) return h;
-    const float3 u = f3(sp.x / ms, sp.y / ms, sp.z / ms);
-    if (a.mode == ANI_UNIFORM) return uni_one(u, a.axis, a.K1, a.K2, a.quirk);
+    V3<R> h = v3<R>(0, 0, 0);
+    if (!(ms > (R)0) || a.mode == ANI_NONE) return h;
+    const V3<R> u = v3<R>(sp.x / ms, sp.y / ms, sp.z / ms);
+    if (a.mode == ANI_UNIFORM)
+        return uni_one<R>(u, (R)a.axis[0], (R)a.axis[1], (R)a.axis[2], (R)a.K1, (R)a.K2, a.quirk);
     const int p0 = __ldg(a.ptr + i), p1 = __ldg(a.ptr + i + 1);
-    for (int p = p0; p < p1; p++) {
-        const float n[3] = {__ldg(a.axes + 3 * p), __ldg(a.axes + 3 * p + 1), __ldg(a.axes + 3 * p + 2)};
-        h = add3(h, uni_one(u, n, __ldg(a.K12 + 2 * p), __ldg(a.K12 + 2 * p + 1), a.quirk));
-    }
+    for (int p = p0; p < p1; p++)
+        h = add3(h, uni_one<R>(u, (R)__ldg(a.axes + 3 * p), (R)__ldg(a.axes + 3 * p + 1), (R)__ldg(a.axes + 3 * p + 2),
+                               (R)__ldg(a.K12 + 2 * p), (R)__ldg(a.K12 + 2 * p + 1), a.quirk));
     return h;
 }
 
 // Cubic (..._cubic.cpp:308-390); quirk keeps (n2s2 + n3s3) in the first K1 term.
-__device__ __forceinline__ float3 cub_one(float3 s, const float* n, const float* K, int quirk)
+template <typename R>
+__device__ __forceinline__ V3<R> cub_one(V3<R> s, const R* n, const R* K, int quirk)
 {
-    const float n1s = n[0] * s.x + n[1] * s.y + n[2] * s.z;
-    const float n2s = n[3] * s.x + n[4] * s.y + n[5] * s.z;
-    const float n3s = n[6] * s.x + n[7] * s.y + n[8] * s.z;
-    const float n1s2 = n1s * n1s, n2s2 = n2s * n2s, n3s2 = n3s * n3s;
-    const float n1s3 = n1s2 * n1s, n2s3 = n2s2 * n2s, n3s3 = n3s2 * n3s;
-    const float n1s4 = n1s2 * n1s2, n2s4 = n2s2 * n2s2, n3s4 = n3s2 * n3s2;
-    const float q = quirk ? n3s3 : n3s2;
-    const float a1 = 2.0f * K[0] * n1s * (n2s2 + q), a2 = 2.0f * K[0] * n2s * (n1s2 + n3s2), a3 = 2.0f * K[0] * n3s * (n1s2 + n2s2);
-    const float p = n1s * n2s * n3s;
-    const float b1 = 2.0f * K[1] * p * n2s * n3s, b2 = 2.0f * K[1] * p * n1s * n3s, b3 = 2.0f * K[1] * p * n1s * n2s;
-    const float c1 = 4.0f * K[2] * n1s3 * (n2s4 + n3s4), c2 = 4.0f * K[2] * n2s3 * (n1s4 + n3s4), c3 = 4.0f * K[2] * n3s3 * (n1s4 + n2s4);
-    float3 h;
+    const R n1s = n[0] * s.x + n[1] * s.y + n[2] * s.z;
+    const R n2s = n[3] * s.x + n[4] * s.y + n[5] * s.z;
+    const R n3s = n[6] * s.x + n[7] * s.y + n[8] * s.z;
+    const R n1s2 = n1s * n1s, n2s2 = n2s * n2s, n3s2 = n3s * n3s;
+    const R n1s3 = n1s2 * n1s, n2s3 = n2s2 * n2s, n3s3 = n3s2 * n3s;
+    const R n1s4 = n1s2 * n1s2, n2s4 = n2s2 * n2s2, n3s4 = n3s2 * n3s2;
+    const R q = quirk ? n3s3 : n3s2;
+    const R a1 = (R)2 * K[0] * n1s * (n2s2 + q), a2 = (R)2 * K[0] * n2s * (n1s2 + n3s2), a3 = (R)2 * K[0] * n3s * (n1s2 + n2s2);
+    const R p = n1s * n2s * n3s;
+    const R b1 = (R)2 * K[1] * p * n2s * n3s, b2 = (R)2 * K[1] * p * n1s * n3s, b3 = (R)2 * K[1] * p * n1s * n2s;
+    const R c1 = (R)4 * K[2] * n1s3 * (n2s4 + n3s4), c2 = (R)4 * K[2] * n2s3 * (n1s4 + n3s4), c3 = (R)4 * K[2] * n3s3 * (n1s4 + n2s4);
+    V3<R> h;
     h.x = (n[0] * a1 + n[3] * a2 + n[6] * a3) + (n[0] * b1 + n[3] * b2 + n[6] * b3) + (n[0] * c1 + n[3] * c2 + n[6] * c3);
     h.y = (n[1] * a1 + n[4] * a2 + n[7] * a3) + (n[1] * b1 + n[4] * b2 + n[7] * b3) + (n[1] * c1 + n[4] * c2 + n[7] * c3);
     h.z = (n[2] * a1 + n[5] * a2 + n[8] * a3) + (n[2] * b1 + n[5] * b2 + n[8] * b3) + (n[2] * c1 + n[5] * c2 + n[8] * c3);
     return h;
 }
-__device__ __forceinline__ float3 cub_term(const CubK& a, float3 sp, float ms, int i)
+template <typename R>
+__device__ __forceinline__ V3<R> cub_term(const CubK& a, V3<R> sp, R ms, int i)
 {
-    float3 h = f3(0.f, 0.f, 0.f);
-    if (!(ms > 0.f) || a.mode == ANI_NONE) return h;
-    const float3 u = f3(sp.x / ms, sp.y / ms, sp.z / ms);
-    if (a.mode == ANI_UNIFORM) return cub_one(u, a.axes, a.K, a.quirk);
+    V3<R> h = v3<R>(0, 0, 0);
+    if (!(ms > (R)0) || a.mode == ANI_NONE) return h;
+    const V3<R> u = v3<R>(sp.x / ms, sp.y / ms, sp.z / ms);
+    R n[9], K[3];
+    if (a.mode == ANI_UNIFORM) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) n[q] = (R)a.axes[q];
+#pragma unroll
+        for (int q = 0; q < 3; q++) K[q] = (R)a.K[q];
+        return cub_one<R>(u, n, K, a.quirk);
+    }
     const int p0 = __ldg(a.ptr + i), p1 = __ldg(a.ptr + i + 1);
     for (int p = p0; p < p1; p++) {
-        float n[9], K[3];
 #pragma unroll
-        for (int q = 0; q < 9; q++) n[q] = __ldg(a.axs + 9 * p + q);
+        for (int q = 0; q < 9; q++) n[q] = (R)__ldg(a.axs + 9 * p + q);
 #pragma unroll
-        for (int q = 0; q < 3; q++) K[q] = __ldg(a.Ks + 3 * p + q);
-        h = add3(h, cub_one(u, n, K, a.quirk));
+        for (int q = 0; q < 3; q++) K[q] = (R)__ldg(a.Ks + 3 * p + q);
+        h = add3(h, cub_one<R>(u, n, K, a.quirk));
     }
     return h;
 }
@@ -173,51 +195,58 @@ __device__ __forceinline__ float3 cub_term(const CubK& a, float3 sp, float ms, i
 // Thermal: sigma = sqrt(2 alpha T scale / (ms dt gamma)) times N(0,1) per
 // component, zero where ms == 0, T == 0 or gamma <= 0
 // (M/cpu/thermal/spinoperationthermal.cpp:135-191).
-__device__ __forceinline__ float3 th_term(const ThermalK& t, const SysK& s, float dt_sys, int i, float ms)
+template <typename R>
+__device__ __forceinline__ V3<R> th_term(const ThermalK& t, const SysK& s, R dt_sys, int i, R ms)
 {
-    float3 h = f3(0.f, 0.f, 0.f);
-    if (t.mode == TH_NONE || ms == 0.f || t.T == 0.f) return h;
-    const float a = alpha_at(s, i), g = gamma_at(s, i);
-    if (!(g > 0.f)) return h;
-    const float sc = t.scale ? __ldg(t.scale + i) : 1.0f;
-    const float sd = sqrtf((2.0f * a * t.T * sc) / (ms * dt_sys * g));
-    float3 n;
+    V3<R> h = v3<R>(0, 0, 0);
+    if (t.mode == TH_NONE || ms == (R)0 || t.T == 0.0) return h;
+    const R a = alpha_at<R>(s, i), g = gamma_at<R>(s, i);
+    if (!(g > (R)0)) return h;
+    const R sc = t.scale ? (R)__ldg(t.scale + i) : (R)1;
+    const R sd = rsq<R>(((R)2 * a * (R)t.T * sc) / (ms * dt_sys * g));
+    V3<R> n;
     if (t.mode == TH_PHILOX) {
         const uint64_t ctr = t.counter + (t.dctr ? *t.dctr : 0ull);
-        n = philox_normal3(t.seed, ctr, (uint32_t)i, 0x6d6c6232u);
+        const float3 f = philox_normal3(t.seed, ctr, (uint32_t)i, 0x6d6c6232u);
+        n = v3<R>((R)f.x, (R)f.y, (R)f.z);
     } else {
-        n = f3(__ldg(t.nx + i), __ldg(t.ny + i), __ldg(t.nz + i));
+        n = v3<R>((R)__ldg(t.nx + i), (R)__ldg(t.ny + i), (R)__ldg(t.nz + i));
     }
-    return f3(sd * n.x, sd * n.y, sd * n.z);
+    return v3<R>(sd * n.x, sd * n.y, sd * n.z);
 }
 
-struct Fields { float3 H; float3 Hth; };
+template <typename R>
+struct Fields {
+    V3<R> H;
+    V3<R> Hth;
+};
 
 // Every term of TermsK at site i.  H is the would-be "Total" slot, Hth the
 // "Thermal" slot that LLG subtracts (llgcartesian.cpp:160-172).
-__device__ __forceinline__ Fields eval_terms(const TermsK& T, const SysK& s, float dt_sys, int i)
+template <typename R>
+__device__ __forceinline__ Fields<R> eval_terms(const TermsK& T, const SysK& s, R dt_sys, int i)
 {
-    const float ms = ms_at(s, i);
-    const float3 sp = spin_at(s, i);
-    float3 H = f3(0.f, 0.f, 0.f);
-    float3 Hth = f3(0.f, 0.f, 0.f);
-    if (T.ex.mode != EX_NONE) H = add3(H, scl3(T.ex_gs, ex_term(T.ex, s, i, ms)));
-    if (T.ani.mode != ANI_NONE) H = add3(H, ani_term(T.ani, sp, ms, i));
-    if (T.uni.mode != ANI_NONE) H = add3(H, uni_term(T.uni, sp, ms, i));
-    if (T.cub.mode != ANI_NONE) H = add3(H, cub_term(T.cub, sp, ms, i));
-    if (T.th.mode != TH_NONE) { Hth = th_term(T.th, s, dt_sys, i, ms); H = add3(H, Hth); }
+    const R ms = ms_at<R>(s, i);
+    const V3<R> sp = spin_at<R>(s, i);
+    V3<R> H = v3<R>(0, 0, 0);
+    V3<R> Hth = v3<R>(0, 0, 0);
+    if (T.ex.mode != EX_NONE) H = add3(H, scl3((R)T.ex_gs, ex_term<R>(T.ex, s, i, ms)));
+    if (T.ani.mode != ANI_NONE) H = add3(H, ani_term<R>(T.ani, sp, ms, i));
+    if (T.uni.mode != ANI_NONE) H = add3(H, uni_term<R>(T.uni, sp, ms, i));
+    if (T.cub.mode != ANI_NONE) H = add3(H, cub_term<R>(T.cub, sp, ms, i));
+    if (T.th.mode != TH_NONE) { Hth = th_term<R>(T.th, s, dt_sys, i, ms); H = add3(H, Hth); }
     if (T.zee.on) {
-        const float3 B = T.zee.Bdev ? f3(T.zee.Bdev[0], T.zee.Bdev[1], T.zee.Bdev[2])
-                                    : f3(T.zee.B[0], T.zee.B[1], T.zee.B[2]);
+        const V3<R> B = T.zee.Bdev ? v3<R>((R)T.zee.Bdev[0], (R)T.zee.Bdev[1], (R)T.zee.Bdev[2])
+                                   : v3<R>((R)T.zee.B[0], (R)T.zee.B[1], (R)T.zee.B[2]);
         H = add3(H, B);
     }
     for (int a = 0; a < T.nadd; a++) {
-        const float3 v = f3(__ldg(T.add[a][0] + i), __ldg(T.add[a][1] + i), __ldg(T.add[a][2] + i));
-        const float w = T.addw[a];
-        H = add3(H, f3(w * v.x, w * v.y, w * v.z));
+        const V3<R> v = v3<R>(ldr<R>(T.add[a][0], i), ldr<R>(T.add[a][1], i), ldr<R>(T.add[a][2], i));
+        const R w = (R)T.addw[a];
+        H = add3(H, v3<R>(w * v.x, w * v.y, w * v.z));
         if (T.add_is_thermal[a]) Hth = add3(Hth, v);
     }
-    Fields f;
+    Fields<R> f;
     f.H = H;
     f.Hth = Hth;
     return f;
@@ -227,121 +256,129 @@ __device__ __forceinline__ Fields eval_terms(const TermsK& T, const SysK& s, flo
 // Cartesian Euler step (M/cpu/llg/llgcartesian.cpp:90-278) or quaternion
 // rotation (M/cpu/llg/llgquat.cpp:126-378) for one site with ms > 0.
 // S: from-spin, M: dmdt-spin, H: Total, Hth: Thermal.
-__device__ __forceinline__ float3 llg_site(const LlgK& L, float3 S, float3 M, float3 H, float3 Hth,
-                                           float ms, float a, float g)
+template <typename R>
+__device__ __forceinline__ V3<R> llg_site(const LlgK& L, V3<R> S, V3<R> M, V3<R> H, V3<R> Hth, R ms, R a, R g)
 {
+    const R dt = (R)L.dt, p = (R)L.precess, d = (R)L.damp;
     if (L.type == LLG_CART) {
         if (L.dt_zero) return S;
-        const float gaa = g / (1.0f + a * a);
-        float3 MH, MMH;
+        const R gaa = g / ((R)1 + a * a);
         if (L.thermal_only_first_term) {
-            const float3 h = sub3(H, Hth);
-            const float3 Mh = cross3(M, h);
-            MMH = cross3(M, Mh);
-            MH = cross3(M, H);
-            const float3 dM = sub3(scl3(L.precess * -gaa, MH), scl3(L.damp * (a / ms) * gaa, MMH));
-            return add3(S, scl3(L.dt, dM));
+            const V3<R> h = sub3(H, Hth);
+            const V3<R> Mh = cross3(M, h);
+            const V3<R> MMH = cross3(M, Mh);
+            const V3<R> MH = cross3(M, H);
+            const V3<R> dM = sub3(scl3(p * -gaa, MH), scl3(d * (a / ms) * gaa, MMH));
+            return add3(S, scl3(dt, dM));
         }
-        MH = cross3(M, H);
-        MMH = cross3(M, MH);
-        const float3 dM = sub3(scl3(-gaa, MH), scl3((a / ms) * gaa, MMH));
-        return add3(S, scl3(L.dt, dM));
+        const V3<R> MH = cross3(M, H);
+        const V3<R> MMH = cross3(M, MH);
+        const V3<R> dM = sub3(scl3(-gaa, MH), scl3((a / ms) * gaa, MMH));
+        return add3(S, scl3(dt, dM));
     }
     // quaternion
-    const float inv = 1.0f / ms;
-    float3 Hp;
+    const R inv = (R)1 / ms;
+    V3<R> Hp;
     if (L.thermal_only_first_term) {
-        const float3 h = sub3(H, Hth);
-        const float3 Sh = cross3(M, h);
-        Hp = add3(scl3(L.precess, H), scl3(L.damp * a * inv, Sh));
+        const V3<R> h = sub3(H, Hth);
+        const V3<R> Sh = cross3(M, h);
+        Hp = add3(scl3(p, H), scl3(d * a * inv, Sh));
     } else {
-        const float3 SH = cross3(S, H);
+        const V3<R> SH = cross3(S, H);
         Hp = add3(H, scl3(a * inv, SH));
     }
-    const float HLen = sqrtf(Hp.x * Hp.x + Hp.y * Hp.y + Hp.z * Hp.z);
-    if (!(HLen > 0.f)) return S;
-    const float iHLen = 1.0f / HLen;
-    const float ra = 1.0f * g * HLen / (1.0f + a * a);
-    float sint, cost;
-    sincosf(0.5f * ra * L.dt, &sint, &cost);
+    const R HLen = rsq<R>(Hp.x * Hp.x + Hp.y * Hp.y + Hp.z * Hp.z);
+    if (!(HLen > (R)0)) return S;
+    const R iHLen = (R)1 / HLen;
+    const R ra = (R)1 * g * HLen / ((R)1 + a * a);
+    R sint, cost;
+    sincos_r(((R)0.5) * ra * dt, &sint, &cost);
     // qRot = (cost, sint * Hp/|Hp|); qRes = qRot * (0,S) * conj(qRot)
-    const float qw = cost, qx = sint * Hp.x * iHLen, qy = sint * Hp.y * iHLen, qz = sint * Hp.z * iHLen;
-    // t = qRot * (0, S)
-    const float tw = -qx * S.x - qy * S.y - qz * S.z;
-    const float tx = qw * S.x + qy * S.z - qz * S.y;
-    const float ty = qw * S.y + qz * S.x - qx * S.z;
-    const float tz = qw * S.z + qx * S.y - qy * S.x;
-    // r = t * conj(qRot), conj = (qw, -qx, -qy, -qz)
-    const float cx = -qx, cy = -qy, cz = -qz;
-    float3 r;
+    const R qw = cost, qx = sint * Hp.x * iHLen, qy = sint * Hp.y * iHLen, qz = sint * Hp.z * iHLen;
+    const R tw = -qx * S.x - qy * S.y - qz * S.z;
+    const R tx = qw * S.x + qy * S.z - qz * S.y;
+    const R ty = qw * S.y + qz * S.x - qx * S.z;
+    const R tz = qw * S.z + qx * S.y - qy * S.x;
+    const R cx = -qx, cy = -qy, cz = -qz;
+    V3<R> r;
     r.x = tw * cx + qw * tx + ty * cz - tz * cy;
     r.y = tw * cy + qw * ty + tz * cx - tx * cz;
     r.z = tw * cz + qw * tz + tx * cy - ty * cx;
     return r;
 }
 
-__device__ __forceinline__ float3 renorm(float3 v, float ms)
+template <typename R>
+__device__ __forceinline__ V3<R> renorm(V3<R> v, R ms)
 {
-    const float mm = v.x * v.x + v.y * v.y + v.z * v.z;
-    if (mm != 0.f) {
-        const float inv = ms / sqrtf(mm);
-        return f3(v.x * inv, v.y * inv, v.z * inv);
+    const R mm = v.x * v.x + v.y * v.y + v.z * v.z;
+    if (mm != (R)0) {
+        const R inv = ms / rsq<R>(mm);
+        return v3<R>(v.x * inv, v.y * inv, v.z * inv);
     }
     return v;
 }
 
 // ------------------------------------------------------------ kernels
-__global__ void __launch_bounds__(256) k_fused_step(FusedK P, float dt_sys)
+template <typename R>
+__global__ void __launch_bounds__(256) k_fused_step(FusedK P, double dt_sys)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.sys.n) return;
-    const float ms = ms_at(P.sys, i);
-    const float3 S = spin_at(P.sys, i);
-    float3 out = S;
-    if (ms > 0.f) {
-        const Fields F = eval_terms(P.terms, P.sys, dt_sys, i);
-        out = llg_site(P.llg, S, S, F.H, F.Hth, ms, alpha_at(P.sys, i), gamma_at(P.sys, i));
+    const R ms = ms_at<R>(P.sys, i);
+    const V3<R> S = spin_at<R>(P.sys, i);
+    V3<R> out = S;
+    if (ms > (R)0) {
+        const Fields<R> F = eval_terms<R>(P.terms, P.sys, (R)dt_sys, i);
+        out = llg_site<R>(P.llg, S, S, F.H, F.Hth, ms, alpha_at<R>(P.sys, i), gamma_at<R>(P.sys, i));
     }
-    if (P.llg.renorm) out = renorm(out, ms);
-    P.ox[i] = out.x;
-    P.oy[i] = out.y;
-    P.oz[i] = out.z;
+    if (P.llg.renorm) out = renorm<R>(out, ms);
+    static_cast<R*>(P.ox)[i] = out.x;
+    static_cast<R*>(P.oy)[i] = out.y;
+    static_cast<R*>(P.oz)[i] = out.z;
 }
 
 // out = (accumulate ? out : 0) + terms
-__global__ void __launch_bounds__(256) k_eval_terms(SysK s, TermsK T, float dt_sys, float* hx, float* hy,
-                                                    float* hz, int accumulate)
+template <typename R>
+__global__ void __launch_bounds__(256) k_eval_terms(SysK s, TermsK T, double dt_sys, void* hx_, void* hy_,
+                                                    void* hz_, int accumulate)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
-    const Fields F = eval_terms(T, s, dt_sys, i);
+    R* hx = static_cast<R*>(hx_);
+    R* hy = static_cast<R*>(hy_);
+    R* hz = static_cast<R*>(hz_);
+    const Fields<R> F = eval_terms<R>(T, s, (R)dt_sys, i);
     if (accumulate) { hx[i] += F.H.x; hy[i] += F.H.y; hz[i] += F.H.z; }
     else { hx[i] = F.H.x; hy[i] = F.H.y; hz[i] = F.H.z; }
 }
 
 // Stand-alone LLG: from (spins+ms), dmdt spins M, Total H, optional Thermal.
 // Sites with ms <= 0 keep the destination's current value.
-__global__ void __launch_bounds__(256) k_llg(SysK from, const float* mx, const float* my, const float* mz,
-                                             const float* hx, const float* hy, const float* hz,
-                                             const float* tx, const float* ty, const float* tz,
-                                             const float* dsa, const float* dsg, float da, float dg,
-                                             LlgK L, float* ox, float* oy, float* oz)
+template <typename R>
+__global__ void __launch_bounds__(256) k_llg(SysK from, const void* mx, const void* my, const void* mz,
+                                             const void* hx, const void* hy, const void* hz,
+                                             const void* tx, const void* ty, const void* tz,
+                                             const void* dsa, const void* dsg, double da, double dg,
+                                             LlgK L, void* ox_, void* oy_, void* oz_)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= from.n) return;
-    const float ms = ms_at(from, i);
-    float3 out = f3(ox[i], oy[i], oz[i]);
+    R* ox = static_cast<R*>(ox_);
+    R* oy = static_cast<R*>(oy_);
+    R* oz = static_cast<R*>(oz_);
+    const R ms = ms_at<R>(from, i);
+    V3<R> out = v3<R>(ox[i], oy[i], oz[i]);
     if (L.type == LLG_CART && L.dt_zero) {
-        out = spin_at(from, i);
-    } else if (ms > 0.f) {
-        const float3 S = spin_at(from, i);
-        const float3 M = f3(mx[i], my[i], mz[i]);
-        const float3 H = f3(hx[i], hy[i], hz[i]);
-        const float3 Ht = tx ? f3(tx[i], ty[i], tz[i]) : f3(0.f, 0.f, 0.f);
-        const float a = dsa ? dsa[i] : da, g = dsg ? dsg[i] : dg;
-        out = llg_site(L, S, M, H, Ht, ms, a, g);
+        out = spin_at<R>(from, i);
+    } else if (ms > (R)0) {
+        const V3<R> S = spin_at<R>(from, i);
+        const V3<R> M = v3<R>(ldr<R>(mx, i), ldr<R>(my, i), ldr<R>(mz, i));
+        const V3<R> H = v3<R>(ldr<R>(hx, i), ldr<R>(hy, i), ldr<R>(hz, i));
+        const V3<R> Ht = tx ? v3<R>(ldr<R>(tx, i), ldr<R>(ty, i), ldr<R>(tz, i)) : v3<R>(0, 0, 0);
+        const R a = dsa ? ldr<R>(dsa, i) : (R)da, g = dsg ? ldr<R>(dsg, i) : (R)dg;
+        out = llg_site<R>(L, S, M, H, Ht, ms, a, g);
     }
-    if (L.renorm) out = renorm(out, ms);
+    if (L.renorm) out = renorm<R>(out, ms);
     ox[i] = out.x; oy[i] = out.y; oz[i] = out.z;
 }
 
@@ -353,9 +390,13 @@ __global__ void k_advance_step(DevStep* d)
 }
 
 // FP64 partial sums for netMoment: per block (sum v*m, sum (v*m)^2) x 3.
-__global__ void __launch_bounds__(256) k_netmoment_partial(const float* x, const float* y, const float* z,
+template <typename R>
+__global__ void __launch_bounds__(256) k_netmoment_partial(const void* x_, const void* y_, const void* z_,
                                                            int n, double m, double* part)
 {
+    const R* x = static_cast<const R*>(x_);
+    const R* y = static_cast<const R*>(y_);
+    const R* z = static_cast<const R*>(z_);
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double a = (double)x[i] * m, b = (double)y[i] * m, c = (double)z[i] * m;
@@ -390,10 +431,17 @@ __global__ void k_partial_final(const double* part, int nb, int nq, double* out)
 }
 
 // FP64 sum of s . h over sites (energy-style dot product).
-__global__ void __launch_bounds__(256) k_dot_partial(const float* x, const float* y, const float* z,
-                                                     const float* hx, const float* hy, const float* hz,
+template <typename R>
+__global__ void __launch_bounds__(256) k_dot_partial(const void* x_, const void* y_, const void* z_,
+                                                     const void* hx_, const void* hy_, const void* hz_,
                                                      int n, double* part)
 {
+    const R* x = static_cast<const R*>(x_);
+    const R* y = static_cast<const R*>(y_);
+    const R* z = static_cast<const R*>(z_);
+    const R* hx = static_cast<const R*>(hx_);
+    const R* hy = static_cast<const R*>(hy_);
+    const R* hz = static_cast<const R*>(hz_);
     double acc = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         acc += (double)x[i] * hx[i] + (double)y[i] * hy[i] + (double)z[i] * hz[i];
@@ -411,28 +459,31 @@ __global__ void __launch_bounds__(256) k_dot_partial(const float* x, const float
 // ------------------------------------------------------------ dipole convolution
 // Forward x pass: rows (y0..y0+ty) of layer z, three components, zero-padded
 // to Px, complex FFT, first Kx bins written to SPEC[kx][c][z][y].
-__global__ void __launch_bounds__(256) k_conv_fx(ConvK c, FftLen Lx, const float2* tw, const float* sx,
-                                                 const float* sy, const float* sz, float2* spec)
+template <typename R>
+__global__ void __launch_bounds__(256) k_conv_fx(ConvK c, FftLen Lx, const typename CT<R>::T* tw, const void* sx,
+                                                 const void* sy, const void* sz, typename CT<R>::T* spec)
 {
-    extern __shared__ float2 smf[];
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* smf = reinterpret_cast<C*>(smraw);
     const int y0 = blockIdx.x * c.ty, zz = blockIdx.y;
     const int rows = min(c.ty, c.ny - y0);
-    float2* A = smf;
-    float2* B = smf + c.ty * c.Px;
+    C* A = smf;
+    C* B = smf + c.ty * c.Px;
     LineGeo g;
     g.nlines = rows; g.lpg = 1 << 30; g.gstride = 0; g.ls = c.Px; g.es = 1; g.line_fast = 0;
     for (int comp = 0; comp < 3; comp++) {
-        const float* src = comp == 0 ? sx : (comp == 1 ? sy : sz);
+        const R* src = static_cast<const R*>(comp == 0 ? sx : (comp == 1 ? sy : sz));
         for (int t = threadIdx.x; t < rows * c.Px; t += blockDim.x) {
             const int r = t / c.Px, x = t % c.Px;
-            const float v = x < c.nx ? __ldg(src + ((size_t)zz * c.ny + y0 + r) * c.nx + x) : 0.f;
-            A[r * c.Px + x] = make_float2(v, 0.f);
+            const R v = x < c.nx ? __ldg(src + ((size_t)zz * c.ny + y0 + r) * c.nx + x) : (R)0;
+            A[r * c.Px + x] = cmk<C>(v, (R)0);
         }
         __syncthreads();
-        const float2* R = c.Px > 1 ? cta_fft<float2>(A, B, g, Lx, tw, -1) : A;
+        const C* Rl = c.Px > 1 ? cta_fft<C>(A, B, g, Lx, tw, -1) : A;
         for (int t = threadIdx.x; t < c.Kx * rows; t += blockDim.x) {
             const int kx = t / rows, r = t % rows;
-            spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + y0 + r] = R[r * c.Px + kx];
+            spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + y0 + r] = Rl[r * c.Px + kx];
         }
         __syncthreads();
     }
@@ -440,17 +491,20 @@ __global__ void __launch_bounds__(256) k_conv_fx(ConvK c, FftLen Lx, const float
 
 // Per-kx (y,z) plane: forward FFT in y then z (zero padded), tensor
 // multiply, inverse z then y, write back the data rows.
-__global__ void __launch_bounds__(512) k_conv_yz(ConvK c, FftLen Ly, FftLen Lz, const float2* tw,
-                                                 float2* spec, const float* ten6, const float2* ten9)
+template <typename R>
+__global__ void __launch_bounds__(512) k_conv_yz(ConvK c, FftLen Ly, FftLen Lz, const typename CT<R>::T* tw,
+                                                 typename CT<R>::T* spec, const R* ten6, const typename CT<R>::T* ten9)
 {
-    extern __shared__ float2 smf[];
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* smf = reinterpret_cast<C*>(smraw);
     const int kx = blockIdx.x;
     const int PP = c.Py * c.Pz;
-    float2* A = smf;
-    float2* B = smf + 3 * PP;
-    for (int t = threadIdx.x; t < 6 * PP; t += blockDim.x) smf[t] = make_float2(0.f, 0.f);
+    C* A = smf;
+    C* B = smf + 3 * PP;
+    for (int t = threadIdx.x; t < 6 * PP; t += blockDim.x) smf[t] = cmk<C>((R)0, (R)0);
     __syncthreads();
-    float2* sp = spec + (size_t)kx * 3 * c.nz * c.ny;
+    C* sp = spec + (size_t)kx * 3 * c.nz * c.ny;
     const int NZY = c.nz * c.ny;
     for (int t = threadIdx.x; t < 3 * NZY; t += blockDim.x) {
         const int comp = t / NZY, rem = t % NZY, z = rem / c.ny, y = rem % c.ny;
@@ -459,37 +513,37 @@ __global__ void __launch_bounds__(512) k_conv_yz(ConvK c, FftLen Ly, FftLen Lz, 
     __syncthreads();
     LineGeo gy; gy.nlines = 3 * c.nz; gy.lpg = c.nz; gy.gstride = PP; gy.ls = c.Py; gy.es = 1; gy.line_fast = 0;
     LineGeo gz; gz.nlines = 3 * c.Py; gz.lpg = c.Py; gz.gstride = PP; gz.ls = 1; gz.es = c.Py; gz.line_fast = 1;
-    float2* cur = A;
-    float2* oth = B;
-    if (c.Py > 1) { cur = cta_fft<float2>(cur, oth, gy, Ly, tw, -1); oth = cur == A ? B : A; }
-    if (c.Pz > 1) { cur = cta_fft<float2>(cur, oth, gz, Lz, tw, -1); oth = cur == A ? B : A; }
-    const float gg = c.g;
+    C* cur = A;
+    C* oth = B;
+    if (c.Py > 1) { cur = cta_fft<C>(cur, oth, gy, Ly, tw, -1); oth = cur == A ? B : A; }
+    if (c.Pz > 1) { cur = cta_fft<C>(cur, oth, gz, Lz, tw, -1); oth = cur == A ? B : A; }
+    const R gg = (R)c.g;
     if (!c.general) {
-        const float* T = ten6 + (size_t)kx * PP * 6;
+        const R* T = ten6 + (size_t)kx * PP * 6;
         for (int t = threadIdx.x; t < PP; t += blockDim.x) {
-            const float t0 = __ldg(T + 6 * t), t1 = __ldg(T + 6 * t + 1), t2 = __ldg(T + 6 * t + 2);
-            const float t3 = __ldg(T + 6 * t + 3), t4 = __ldg(T + 6 * t + 4), t5 = __ldg(T + 6 * t + 5);
-            const float2 s0 = cur[t], s1 = cur[PP + t], s2 = cur[2 * PP + t];
-            cur[t] = make_float2(gg * (t0 * s0.x + t1 * s1.x + t2 * s2.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2.y));
-            cur[PP + t] = make_float2(gg * (t1 * s0.x + t3 * s1.x + t4 * s2.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2.y));
-            cur[2 * PP + t] = make_float2(gg * (t2 * s0.x + t4 * s1.x + t5 * s2.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2.y));
+            const R t0 = __ldg(T + 6 * t), t1 = __ldg(T + 6 * t + 1), t2 = __ldg(T + 6 * t + 2);
+            const R t3 = __ldg(T + 6 * t + 3), t4 = __ldg(T + 6 * t + 4), t5 = __ldg(T + 6 * t + 5);
+            const C s0 = cur[t], s1 = cur[PP + t], s2 = cur[2 * PP + t];
+            cur[t] = cmk<C>(gg * (t0 * s0.x + t1 * s1.x + t2 * s2.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2.y));
+            cur[PP + t] = cmk<C>(gg * (t1 * s0.x + t3 * s1.x + t4 * s2.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2.y));
+            cur[2 * PP + t] = cmk<C>(gg * (t2 * s0.x + t4 * s1.x + t5 * s2.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2.y));
         }
     } else {
-        const float2* T = ten9 + (size_t)kx * PP * 9;
+        const C* T = ten9 + (size_t)kx * PP * 9;
         for (int t = threadIdx.x; t < PP; t += blockDim.x) {
-            const float2 s[3] = {cur[t], cur[PP + t], cur[2 * PP + t]};
+            const C s[3] = {cur[t], cur[PP + t], cur[2 * PP + t]};
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                float2 acc = make_float2(0.f, 0.f);
+                C acc = cmk<C>((R)0, (R)0);
 #pragma unroll
                 for (int b = 0; b < 3; b++) acc = cadd(acc, cmul(T[9 * t + 3 * a + b], s[b]));
-                cur[a * PP + t] = make_float2(gg * acc.x, gg * acc.y);
+                cur[a * PP + t] = cmk<C>(gg * acc.x, gg * acc.y);
             }
         }
     }
     __syncthreads();
-    if (c.Pz > 1) { cur = cta_fft<float2>(cur, oth, gz, Lz, tw, +1); oth = cur == A ? B : A; }
-    if (c.Py > 1) { cur = cta_fft<float2>(cur, oth, gy, Ly, tw, +1); oth = cur == A ? B : A; }
+    if (c.Pz > 1) { cur = cta_fft<C>(cur, oth, gz, Lz, tw, +1); oth = cur == A ? B : A; }
+    if (c.Py > 1) { cur = cta_fft<C>(cur, oth, gy, Ly, tw, +1); oth = cur == A ? B : A; }
     for (int t = threadIdx.x; t < 3 * NZY; t += blockDim.x) {
         const int comp = t / NZY, rem = t % NZY, z = rem / c.ny, y = rem % c.ny;
         sp[t] = cur[comp * PP + z * c.Py + y];
@@ -498,19 +552,22 @@ __global__ void __launch_bounds__(512) k_conv_yz(ConvK c, FftLen Ly, FftLen Lz, 
 
 // Inverse x pass: Hermitian completion, complex inverse FFT, real part of
 // the first nx points written to the field slot.
-__global__ void __launch_bounds__(256) k_conv_ix(ConvK c, FftLen Lx, const float2* tw, const float2* spec,
-                                                 float* hx, float* hy, float* hz)
+template <typename R>
+__global__ void __launch_bounds__(256) k_conv_ix(ConvK c, FftLen Lx, const typename CT<R>::T* tw, const typename CT<R>::T* spec,
+                                                 void* hx, void* hy, void* hz)
 {
-    extern __shared__ float2 smf[];
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* smf = reinterpret_cast<C*>(smraw);
     const int y0 = blockIdx.x * c.ty, zz = blockIdx.y;
     const int rows = min(c.ty, c.ny - y0);
-    float2* A = smf;
-    float2* B = smf + c.ty * c.Px;
+    C* A = smf;
+    C* B = smf + c.ty * c.Px;
     LineGeo g;
     g.nlines = rows; g.lpg = 1 << 30; g.gstride = 0; g.ls = c.Px; g.es = 1; g.line_fast = 0;
     const int nh = c.Px - c.Kx;
     for (int comp = 0; comp < 3; comp++) {
-        float* dst = comp == 0 ? hx : (comp == 1 ? hy : hz);
+        R* dst = static_cast<R*>(comp == 0 ? hx : (comp == 1 ? hy : hz));
         for (int t = threadIdx.x; t < c.Kx * rows; t += blockDim.x) {
             const int kx = t / rows, r = t % rows;
             A[r * c.Px + kx] = spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + y0 + r];
@@ -521,10 +578,10 @@ __global__ void __launch_bounds__(256) k_conv_ix(ConvK c, FftLen Lx, const float
             A[r * c.Px + k] = cconj(A[r * c.Px + c.Px - k]);
         }
         __syncthreads();
-        const float2* R = c.Px > 1 ? cta_fft<float2>(A, B, g, Lx, tw, +1) : A;
+        const C* Rl = c.Px > 1 ? cta_fft<C>(A, B, g, Lx, tw, +1) : A;
         for (int t = threadIdx.x; t < rows * c.nx; t += blockDim.x) {
             const int r = t / c.nx, x = t % c.nx;
-            dst[((size_t)zz * c.ny + y0 + r) * c.nx + x] = R[r * c.Px + x].x;
+            dst[((size_t)zz * c.ny + y0 + r) * c.nx + x] = Rl[r * c.Px + x].x;
         }
         __syncthreads();
     }
@@ -679,9 +736,10 @@ __global__ void k_fft_lines(C* data, int Px, int Py, int Pz, int ax, FftLen L, c
     for (int t = threadIdx.x; t < L.n; t += blockDim.x) d[(size_t)t * es] = R[t];
 }
 
-// Real symmetric tensor: TEN6[kx][kz][ky][q] = Re W_q(kx,ky,kz) (float).
-__global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, float* ten6,
-                               double* maxim)
+// Real symmetric tensor: TEN6[kx][kz][ky][q] = Re W_q(kx,ky,kz) in the
+// state precision R.
+template <typename R>
+__global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, R* ten6, double* maxim)
 {
     const long long total = (long long)Kx * Py * Pz;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -694,7 +752,7 @@ __global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx,
     double mi = 0;
     for (int q = 0; q < 6; q++) {
         const double2 v = W[q * plane + off];
-        ten6[(size_t)e * 6 + q] = (float)v.x;
+        ten6[(size_t)e * 6 + q] = (R)v.x;
         mi = fmax(mi, fabs(v.y));
     }
     if (maxim) {
@@ -704,7 +762,8 @@ __global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx,
 }
 
 // General 9-component complex tensor: TEN9[kx][kz][ky][q].
-__global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, float2* ten9)
+template <typename R>
+__global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, typename CT<R>::T* ten9)
 {
     const long long total = (long long)Kx * Py * Pz;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -716,7 +775,7 @@ __global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx,
     const size_t off = ((size_t)kz * Py + ky) * Px + kx;
     for (int q = 0; q < 9; q++) {
         const double2 v = W[q * plane + off];
-        ten9[(size_t)e * 9 + q] = make_float2((float)v.x, (float)v.y);
+        ten9[(size_t)e * 9 + q] = cmk<typename CT<R>::T>((R)v.x, (R)v.y);
     }
 }
 
@@ -805,30 +864,39 @@ int prof_end(int cap, char* names, double* ms, int* launches)
 
 static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
-cudaError_t launch_fused(const FusedK& P, float dt_sys, cudaStream_t st)
+cudaError_t launch_fused(const FusedK& P, double dt_sys, int rb, cudaStream_t st)
 {
     if (P.sys.n == 0) return cudaSuccess;
     Prof pf("k_fused_step", st);
-    k_fused_step<<<blocks_for(P.sys.n, 256), 256, 0, st>>>(P, dt_sys);
+    if (rb == 8) k_fused_step<double><<<blocks_for(P.sys.n, 256), 256, 0, st>>>(P, dt_sys);
+    else k_fused_step<float><<<blocks_for(P.sys.n, 256), 256, 0, st>>>(P, dt_sys);
     return cudaGetLastError();
 }
 
-cudaError_t launch_eval(const SysK& s, const TermsK& T, float dt_sys, float* h[3], int acc, cudaStream_t st)
+cudaError_t launch_eval(const SysK& s, const TermsK& T, double dt_sys, void* const h[3], int acc, int rb,
+                        cudaStream_t st)
 {
     if (s.n == 0) return cudaSuccess;
     Prof pf("k_eval_terms", st);
-    k_eval_terms<<<blocks_for(s.n, 256), 256, 0, st>>>(s, T, dt_sys, h[0], h[1], h[2], acc);
+    if (rb == 8) k_eval_terms<double><<<blocks_for(s.n, 256), 256, 0, st>>>(s, T, dt_sys, h[0], h[1], h[2], acc);
+    else k_eval_terms<float><<<blocks_for(s.n, 256), 256, 0, st>>>(s, T, dt_sys, h[0], h[1], h[2], acc);
     return cudaGetLastError();
 }
 
-cudaError_t launch_llg(const SysK& from, const float* m[3], const float* H[3], const float* Ht[3],
-                       const float* dsa, const float* dsg, float da, float dg, const LlgK& L,
-                       float* out[3], cudaStream_t st)
+cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* const H[3], const void* const Ht[3],
+                       const void* dsa, const void* dsg, double da, double dg, const LlgK& L,
+                       void* const out[3], int rb, cudaStream_t st)
 {
     if (from.n == 0) return cudaSuccess;
     Prof pf("k_llg", st);
-    k_llg<<<blocks_for(from.n, 256), 256, 0, st>>>(from, m[0], m[1], m[2], H[0], H[1], H[2], Ht[0], Ht[1],
-                                                   Ht[2], dsa, dsg, da, dg, L, out[0], out[1], out[2]);
+    if (rb == 8)
+        k_llg<double><<<blocks_for(from.n, 256), 256, 0, st>>>(from, m[0], m[1], m[2], H[0], H[1], H[2], Ht[0],
+                                                               Ht[1], Ht[2], dsa, dsg, da, dg, L, out[0], out[1],
+                                                               out[2]);
+    else
+        k_llg<float><<<blocks_for(from.n, 256), 256, 0, st>>>(from, m[0], m[1], m[2], H[0], H[1], H[2], Ht[0],
+                                                              Ht[1], Ht[2], dsa, dsg, da, dg, L, out[0], out[1],
+                                                              out[2]);
     return cudaGetLastError();
 }
 
@@ -838,54 +906,75 @@ cudaError_t launch_advance_step(DevStep* d, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_netmoment(const float* x, const float* y, const float* z, int n, double m,
-                             double* part, int nb, double* out, cudaStream_t st)
+cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
+                             double* out, int rb, cudaStream_t st)
 {
-    k_netmoment_partial<<<nb, 256, 0, st>>>(x, y, z, n, m, part);
+    if (rb == 8) k_netmoment_partial<double><<<nb, 256, 0, st>>>(x, y, z, n, m, part);
+    else k_netmoment_partial<float><<<nb, 256, 0, st>>>(x, y, z, n, m, part);
     k_partial_final<<<1, 32, 0, st>>>(part, nb, 6, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_dot(const float* s[3], const float* h[3], int n, double* part, int nb, double* out,
-                       cudaStream_t st)
+cudaError_t launch_dot(const void* const s[3], const void* const h[3], int n, double* part, int nb, double* out,
+                       int rb, cudaStream_t st)
 {
-    k_dot_partial<<<nb, 256, 0, st>>>(s[0], s[1], s[2], h[0], h[1], h[2], n, part);
+    if (rb == 8) k_dot_partial<double><<<nb, 256, 0, st>>>(s[0], s[1], s[2], h[0], h[1], h[2], n, part);
+    else k_dot_partial<float><<<nb, 256, 0, st>>>(s[0], s[1], s[2], h[0], h[1], h[2], n, part);
     k_partial_final<<<1, 32, 0, st>>>(part, nb, 1, out);
     return cudaGetLastError();
 }
 
-size_t conv_x_smem(const ConvK& c) { return (size_t)2 * c.ty * c.Px * sizeof(float2); }
-size_t conv_yz_smem(const ConvK& c) { return (size_t)6 * c.Py * c.Pz * sizeof(float2); }
+size_t conv_x_smem(const ConvK& c, int rb) { return (size_t)2 * c.ty * c.Px * 2 * rb; }
+size_t conv_yz_smem(const ConvK& c, int rb) { return (size_t)6 * c.Py * c.Pz * 2 * rb; }
+
+template <typename K>
+static cudaError_t max_smem(K kern)
+{
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
 
 cudaError_t conv_configure()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_conv_yz, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_fx, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_conv_ix, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_fft_lines<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    return e;
+    cudaError_t e;
+    if ((e = max_smem(k_conv_yz<float>)) != cudaSuccess) return e;
+    if ((e = max_smem(k_conv_yz<double>)) != cudaSuccess) return e;
+    if ((e = max_smem(k_conv_fx<float>)) != cudaSuccess) return e;
+    if ((e = max_smem(k_conv_fx<double>)) != cudaSuccess) return e;
+    if ((e = max_smem(k_conv_ix<float>)) != cudaSuccess) return e;
+    if ((e = max_smem(k_conv_ix<double>)) != cudaSuccess) return e;
+    return max_smem(k_fft_lines<double2>);
 }
 
-cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz,
-                        const float2* tw, const float* s[3], float2* spec, const float* ten6,
-                        const float2* ten9, float* h[3], cudaStream_t st)
+template <typename R>
+static void conv_generic(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz, const void* tw_,
+                         const void* const s[3], void* spec_, const void* ten6, const void* ten9, void* const h[3],
+                         cudaStream_t st)
 {
+    typedef typename CT<R>::T C;
+    const C* tw = static_cast<const C*>(tw_);
+    C* spec = static_cast<C*>(spec_);
     dim3 gx(blocks_for(c.ny, c.ty), c.nz);
     {
         Prof pf("k_conv_fx", st);
-        k_conv_fx<<<gx, 256, conv_x_smem(c), st>>>(c, Lx, tw, s[0], s[1], s[2], spec);
+        k_conv_fx<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, Lx, tw, s[0], s[1], s[2], spec);
     }
     {
         Prof pf("k_conv_yz", st);
-        k_conv_yz<<<c.Kx, 512, conv_yz_smem(c), st>>>(c, Ly, Lz, tw, spec, ten6, ten9);
+        k_conv_yz<R><<<c.Kx, 512, conv_yz_smem(c, sizeof(R)), st>>>(c, Ly, Lz, tw, spec, static_cast<const R*>(ten6),
+                                                                    static_cast<const C*>(ten9));
     }
     {
         Prof pf("k_conv_ix", st);
-        k_conv_ix<<<gx, 256, conv_x_smem(c), st>>>(c, Lx, tw, spec, h[0], h[1], h[2]);
+        k_conv_ix<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, Lx, tw, spec, h[0], h[1], h[2]);
     }
+}
+
+cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz, const void* tw,
+                        const void* const s[3], void* spec, const void* ten6, const void* ten9, void* const h[3],
+                        int rb, cudaStream_t st)
+{
+    if (rb == 8) conv_generic<double>(c, Lx, Ly, Lz, tw, s, spec, ten6, ten9, h, st);
+    else conv_generic<float>(c, Lx, Ly, Lz, tw, s, spec, ten6, ten9, h, st);
     return cudaGetLastError();
 }
 
@@ -935,18 +1024,27 @@ cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const 
     return cudaSuccess;
 }
 
-cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, float* ten6, double* maxim,
-                                cudaStream_t st)
+cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
+                                int rb, cudaStream_t st)
 {
     const long long total = (long long)Kx * Py * Pz;
-    k_tensor_pack6<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten6, maxim);
+    if (rb == 8)
+        k_tensor_pack6<double><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<double*>(ten6),
+                                                                       maxim);
+    else
+        k_tensor_pack6<float><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<float*>(ten6),
+                                                                      maxim);
     return cudaGetLastError();
 }
 
-cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, float2* ten9, cudaStream_t st)
+cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb,
+                                cudaStream_t st)
 {
     const long long total = (long long)Kx * Py * Pz;
-    k_tensor_pack9<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten9);
+    if (rb == 8)
+        k_tensor_pack9<double><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<double2*>(ten9));
+    else
+        k_tensor_pack9<float><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<float2*>(ten9));
     return cudaGetLastError();
 }
 

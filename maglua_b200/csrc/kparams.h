@@ -1,6 +1,6 @@
 // kparams.h -- plain-old-data launch parameters shared by the host layer
-// (capi.cu) and the kernels (kernels.cu).  Device pointers only; FP32 state,
-// FP64 where noted.
+// (capi.cu) and the kernels (kernels.cu, conv_fast.cu).  Device pointers
+// only.
 #pragma once
 #include <stdint.h>
 
@@ -16,85 +16,88 @@ enum { ANI_NONE = 0, ANI_UNIFORM = 1, ANI_CSR = 2 };
 enum { TH_NONE = 0, TH_PHILOX = 1, TH_INJECT = 2 };
 enum { LLG_CART = 0, LLG_QUAT = 1 };
 
+// Operator parameters are FP64 (host values); kernels compute in the
+// system's precision R (float or double) and convert on use.  State arrays
+// (spins, ms, slots, per-site alpha/gamma) are untyped device pointers of R.
 struct ExchangeK {
     int mode;
     int normalize;
-    float J[6];            // (+x,-x,+y,-y,+z,-z): source offset from target, times global_scale
+    double J[6];           // (+x,-x,+y,-y,+z,-z): source offset from target
     int pbc[3];
     const int* ptr;        // CSR (n+1)
     const int* col;        // source sites
-    const float* val;      // J * global_scale
+    const double* val;     // J per pathway
 };
 
 // Generic Anisotropy (H = 2K (s.n)/ms^2 n)
 struct AniK {
     int mode;
-    float axis[3]; float K;        // uniform (K already times global_scale)
-    const int* ptr; const float* axes; const float* Ks;   // CSR: axes 3/op, K 1/op
+    double axis[3]; double K;                    // uniform (K times global_scale)
+    const int* ptr; const double* axes; const double* Ks;   // CSR: axes 3/op, K 1/op
 };
 // Uniaxial (H = [2K1 u + 4K2 u^3] n, u from unit spin)
 struct UniK {
     int mode; int quirk;
-    float axis[3]; float K1, K2;
-    const int* ptr; const float* axes; const float* K12;  // axes 3/op, K 2/op
+    double axis[3]; double K1, K2;
+    const int* ptr; const double* axes; const double* K12;  // axes 3/op, K 2/op
 };
 // Cubic
 struct CubK {
     int mode; int quirk;
-    float axes[9]; float K[3];
-    const int* ptr; const float* axs; const float* Ks;    // axes 9/op, K 3/op
+    double axes[9]; double K[3];
+    const int* ptr; const double* axs; const double* Ks;    // axes 9/op, K 3/op
 };
 struct ThermalK {
     int mode;
-    float T;                  // temperature * global_scale
-    const float* scale;       // per-site scale or null
+    double T;                 // temperature * global_scale
+    const double* scale;      // per-site scale or null
     uint64_t seed;
     uint64_t counter;         // host part of the Philox counter
     const uint64_t* dctr;     // device step counter added to it (null = 0)
-    const float* nx; const float* ny; const float* nz;   // injected normals
+    const double* nx; const double* ny; const double* nz;   // injected normals
 };
 struct ZeemanK {
     int on;
-    float B[3];               // times global_scale
-    const float* Bdev;        // captured steps: B read from the device step block
+    double B[3];              // times global_scale
+    const double* Bdev;       // captured steps: B read from the device step block
 };
 
 // Parameters a captured step reads on the device and advances once per step
 // (k_advance_step): the Thermal counter and the applied field with its sweep.
 struct DevStep {
     uint64_t th_counter;
-    float B[3];
-    float dB[3];
+    double B[3];
+    double dB[3];
 };
 
 struct SysK {
     int nx, ny, nz, n;
-    const float* x; const float* y; const float* z;   // spins read
-    const float* ms; float ms_u; int ms_uniform;
-    const float* site_alpha; const float* site_gamma;
-    float alpha, gamma;
+    const void* x; const void* y; const void* z;   // spins read (R)
+    const void* ms; double ms_u; int ms_uniform;
+    const void* site_alpha; const void* site_gamma;
+    double alpha, gamma;
 };
 
 // Which terms a kernel evaluates, in slot order for the sum.
 struct TermsK {
-    ExchangeK ex; float ex_gs;   // (unused)
+    ExchangeK ex; double ex_gs;   // exchange scale (global_scale x applies)
     AniK ani;
     UniK uni;
     CubK cub;
     ThermalK th;
     ZeemanK zee;
     int nadd;
-    const float* add[MLB_MAX_ADDENDS][3];   // materialised slot arrays added to Total
-    float addw[MLB_MAX_ADDENDS];
-    int add_is_thermal[MLB_MAX_ADDENDS];    // this addend is the Thermal slot
+    const void* add[MLB_MAX_ADDENDS][3];   // materialised slot arrays added to Total (R)
+    double addw[MLB_MAX_ADDENDS];
+    int add_is_thermal[MLB_MAX_ADDENDS];   // this addend is the Thermal slot
 };
 
 struct LlgK {
     int type;
     int thermal_only_first_term;
     int renorm;
-    float precess, damp;
-    float dt;                 // scale * dmdt->dt
+    double precess, damp;
+    double dt;                // scale * dmdt->dt
     int dt_zero;
 };
 
@@ -103,7 +106,7 @@ struct FusedK {
     SysK sys;
     TermsK terms;
     LlgK llg;
-    float* ox; float* oy; float* oz;
+    void* ox; void* oy; void* oz;
 };
 
 // ------------------------------------------------------------- dipole
@@ -115,7 +118,7 @@ struct ConvK {
     int Kx;
     int ty;                  // rows per CTA in the x passes
     int general;             // 0: 6 real tensor entries per k, 1: 9 complex
-    float g;                 // strength * global_scale / (Px*Py*Pz)
+    double g;                // strength * global_scale / (Px*Py*Pz)
     int fx, fy, fz;          // FftLen indices
     int nrep;                // replicas of this size packed back to back (1 for a system)
 };
@@ -135,7 +138,7 @@ struct FastK {
     uint64_t seed, counter;
     const uint64_t* dctr;
     float B[3];               // Zeeman (Bdev when read from the device step block)
-    const float* Bdev;
+    const double* Bdev;
     float addw;
     int llg_type, tof, renorm, dt_zero;
     float dt, precess, c_prec, c_damp, c_rot, ms;

@@ -49,22 +49,24 @@ cudaError_t launch_fused_ens(const FastK& F, const EnsLaunch& E, const float* s[
 cudaError_t launch_ens_moments(const int4* rinfo, int nrep, const float* s[3], double* out, cudaStream_t st);
 void prof_begin();
 int prof_end(int cap, char* names, double* ms, int* launches);
-cudaError_t launch_fused(const FusedK& P, float dt_sys, cudaStream_t st);
-cudaError_t launch_eval(const SysK& s, const TermsK& T, float dt_sys, float* h[3], int acc, cudaStream_t st);
-cudaError_t launch_llg(const SysK& from, const float* m[3], const float* H[3], const float* Ht[3],
-                       const float* dsa, const float* dsg, float da, float dg, const LlgK& L,
-                       float* out[3], cudaStream_t st);
+// Generic kernels: rb = bytes per real of the state arrays (4 or 8).
+cudaError_t launch_fused(const FusedK& P, double dt_sys, int rb, cudaStream_t st);
+cudaError_t launch_eval(const SysK& s, const TermsK& T, double dt_sys, void* const h[3], int acc, int rb,
+                        cudaStream_t st);
+cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* const H[3], const void* const Ht[3],
+                       const void* dsa, const void* dsg, double da, double dg, const LlgK& L,
+                       void* const out[3], int rb, cudaStream_t st);
 cudaError_t launch_advance_step(DevStep* d, cudaStream_t st);
-cudaError_t launch_netmoment(const float* x, const float* y, const float* z, int n, double m,
-                             double* part, int nb, double* out, cudaStream_t st);
-cudaError_t launch_dot(const float* s[3], const float* h[3], int n, double* part, int nb, double* out,
-                       cudaStream_t st);
-size_t conv_x_smem(const ConvK& c);
-size_t conv_yz_smem(const ConvK& c);
+cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
+                             double* out, int rb, cudaStream_t st);
+cudaError_t launch_dot(const void* const s[3], const void* const h[3], int n, double* part, int nb, double* out,
+                       int rb, cudaStream_t st);
+size_t conv_x_smem(const ConvK& c, int rb);
+size_t conv_yz_smem(const ConvK& c, int rb);
 cudaError_t conv_configure();
-cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz,
-                        const float2* tw, const float* s[3], float2* spec, const float* ten6,
-                        const float2* ten9, float* h[3], cudaStream_t st);
+cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, const FftLen& Lz, const void* tw,
+                        const void* const s[3], void* spec, const void* ten6, const void* ten9, void* const h[3],
+                        int rb, cudaStream_t st);
 cudaError_t launch_tensor_lattice(int nx, int ny, int nz, const int gmax[4], const double ABC[9], int Px,
                                   int Py, int Pz, int zsign, double2* W, cudaStream_t st);
 cudaError_t launch_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, int Pz, int zsign,
@@ -73,7 +75,8 @@ cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int 
                                double2* W, cudaStream_t st);
 cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const FftLen L[3],
                            const double2* tw, int sign, cudaStream_t st);
-cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, float* ten6, double* maxim,
+cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
+                                int rb, cudaStream_t st);
+cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb,
                                 cudaStream_t st);
-cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, float2* ten9, cudaStream_t st);
 } // namespace mlb

@@ -34,7 +34,7 @@ def rel_err(a, b):
 class Pair:
     """Oracle and product objects for the same lattice."""
 
-    def __init__(self, nx, ny, nz, spins, alpha=0.1, dt=0.01, gamma=1.0):
+    def __init__(self, nx, ny, nz, spins, alpha=0.1, dt=0.01, gamma=1.0, precision="f32"):
         import maglua_b200 as M
         self.M = M
         self.dims = (nx, ny, nz)
@@ -42,7 +42,7 @@ class Pair:
         self.o = O.SpinSystem(nx, ny, nz)
         self.o.set_spins(*spins)
         self.o.alpha, self.o.dt, self.o.gamma = alpha, dt, gamma
-        self.g = M.SpinSystem(nx, ny, nz)
+        self.g = M.SpinSystem(nx, ny, nz, precision=precision)
         self.g.setSpinArrays(*spins)
         self.g.setAlpha(alpha)
         self.g.setTimeStep(dt)

@@ -349,10 +349,9 @@ def _golden():
         return json.load(f)
 
 
-def _c1_gpu(M, kind):
+def _c1_gpu(M, kind, precision="f32"):
     from golden.make_golden import c1_spins, NX, NY, NZ, J, K, G, ALPHA, DT
-    n = NX * NY * NZ
-    p = Pair(NX, NY, NZ, c1_spins(), alpha=ALPHA, dt=DT)
+    p = Pair(NX, NY, NZ, c1_spins(), alpha=ALPHA, dt=DT, precision=precision)
     p.exchange(J=J, paths=O.nn_paths(NX, NY, NZ, J=J, dirs=4))
     p.anisotropy(axis=(0, 0, 1), K=K)
     p.dipole(g=G)
