@@ -269,6 +269,26 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
  * issuing those calls one by one. */
 int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
 
+/* ---------------------------------------------------------------- no-allocation dipole field
+ * No counterpart in the reference (LongRange::init allocates the FFT work
+ * arrays per operator, M/cpu/longrange/spinoperationlongrange.cpp:98-139).
+ * The Dipole / LongRange field of FP32 device spin arrays (sx, sy, sz: nx*ny*nz
+ * each, layout x + nx*(y + ny*z)) into FP32 device field arrays (hx, hy, hz),
+ * scaled by the operator's strength, on `stream` (NULL = the legacy default
+ * stream), with no device or host allocation: the spectrum scratch is a
+ * static device array of MLB_NOALLOC_SCRATCH_BYTES (16 MiB), enough for
+ * Kx*3*nz*ny complex FP32 values with Kx = Px/2+1 (256x256x8 needs 6.3 MB).
+ * Larger lattices return MLB_ERANGE.  The operator's tensor spectrum must
+ * already exist (apply the operator once to an FP32 SpinSystem of its size;
+ * that call allocates), else MLB_ESTATE.  The first call on each device looks
+ * up the scratch's address with cudaGetSymbolAddress with that device
+ * current; make it before any stream capture.  Every call shares the one
+ * scratch: calls that overlap in time (two streams, two threads) race on it
+ * and must be serialised by the caller. */
+#define MLB_NOALLOC_SCRATCH_BYTES 16777216u
+int mlb_dipole_field_noalloc(mlb_op* op, const float* sx, const float* sy, const float* sz, float* hx, float* hy,
+                             float* hz, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,6 +118,7 @@ _SIGS = {
     "mlb_llg_set_flags": ([_P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
     "mlb_llg_apply": ([_P, _P, C.c_double, _P, _P, C.c_int], C.c_int),
     "mlb_run": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int], C.c_int),
+    "mlb_dipole_field_noalloc": ([_P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
     "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
     "mlb_plan_kernel_times": ([_P, C.c_int, C.c_char_p, _D, _I], C.c_int),

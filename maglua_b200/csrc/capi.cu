@@ -2839,3 +2839,74 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------- no-allocation dipole field
+// Spectrum scratch of mlb_dipole_field_noalloc: a file-scope device array,
+// so the call allocates nothing.  Nothing in it needs to start at zero: the
+// forward x pass writes every spectrum element (kx < Px/2+1, all three
+// components, every data row) before the (y,z) pass and the inverse x pass
+// read it.
+static __device__ __align__(256) unsigned char g_noalloc_spec[MLB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+void* g_noalloc_addr[kNoallocMaxDevices] = {};   // device address of g_noalloc_spec per device
+
+// Address of the scratch on the current device, looked up on the first call
+// made with that device current (the lookup may load this library's device
+// code, so that first call belongs before any stream capture).
+void* noalloc_scratch()
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocMaxDevices) fail(MLB_EUNSUP, "device ordinal beyond the scratch table");
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_spec);
+        if (e != cudaSuccess || !p)
+            fail(MLB_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    return g_noalloc_addr[dev];
+}
+} // namespace
+
+extern "C" int mlb_dipole_field_noalloc(mlb_op* op, const float* sx, const float* sy, const float* sz, float* hx,
+                                        float* hy, float* hz, void* stream)
+{
+    return guard([&] {
+        if (!op) fail(MLB_EINVAL, "null operator");
+        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE)
+            fail(MLB_EINVAL, "not a Dipole or LongRange operator");
+        // size check first, from the plan geometry alone (nothing allocated)
+        ConvPlan geo;
+        geo.rb = 4;
+        plan_sizes(op, geo);
+        const size_t need = (size_t)geo.k.Kx * 3 * op->nz * op->ny * sizeof(float2);
+        if (need > (size_t)MLB_NOALLOC_SCRATCH_BYTES)
+            fail(MLB_ERANGE, "spectrum of " + std::to_string(need) + " bytes for " + std::to_string(op->nx) + "x" +
+                                 std::to_string(op->ny) + "x" + std::to_string(op->nz) + " exceeds the " +
+                                 std::to_string((unsigned long long)MLB_NOALLOC_SCRATCH_BYTES) +
+                                 "-byte static scratch of mlb_dipole_field_noalloc");
+        if (!op->plan || op->plan_dirty || op->plan->rb != 4)
+            fail(MLB_ESTATE, "tensor spectrum not built for FP32: apply the operator to an FP32 SpinSystem once "
+                             "(that call allocates) before calling mlb_dipole_field_noalloc");
+        if (!sx || !sy || !sz || !hx || !hy || !hz) fail(MLB_EINVAL, "null spin or field array");
+        void* scratch = noalloc_scratch();
+        const ConvPlan& P = *op->plan;
+        ConvK k = P.k;
+        k.nrep = 1;
+        k.g = op->g * op->gs / ((double)k.Px * k.Py * k.Pz);
+        cudaStream_t st = (cudaStream_t)stream;
+        const float* sp[3] = {sx, sy, sz};
+        float* h[3] = {hx, hy, hz};
+        if (mlb::conv_fast_ok(k)) {
+            CK(mlb::launch_conv_fast(k, P.L, reinterpret_cast<const float2*>(P.tw.p), sp,
+                                     static_cast<float2*>(scratch), reinterpret_cast<const float*>(P.ten6.p), h, st));
+        } else {
+            const void* spv[3] = {sx, sy, sz};
+            void* hv[3] = {hx, hy, hz};
+            CK(mlb::launch_conv(k, P.L[0], P.L[1], P.L[2], P.tw.p, spv, scratch, P.ten6.p, P.ten9.p, hv, 4, st));
+        }
+    });
+}
