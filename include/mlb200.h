@@ -269,6 +269,58 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
  * issuing those calls one by one. */
 int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
 
+/* ---------------------------------------------------------------- learned dipolar surrogate
+ * B200 extension, no counterpart in the reference.  A linear spectral-conv
+ * network on the in-plane grid, with the (component, z) pairs as 3*nz
+ * channels, predicts the Dipole/LongRange field change dH from the spin
+ * change m - m0 since the last exact evaluation (M/cpu/longrange/
+ * spinoperationlongrange.cpp:354-440 computes the exact field):
+ *   dH[co](s) = sum_{|ox|,|oy| <= radius} sum_ci W[o][co][ci] (m - m0)[ci](s + o)
+ *             + sum_{kx < modes_x, ky in the modes_y lowest |ky|}
+ *                 w_kx/(nx ny) Re(e^{i k.s} sum_ci R_k[co][ci] (m - m0)^_k[ci])
+ * evaluated in BF16 on the tcgen05 tensor cores with FP32 accumulation.
+ * Needs an FP32 system, periodic in-plane lattice, nx a multiple of 128, ny
+ * a multiple of 8 (of 4 when 3*nz > 16), 3*nz <= 32, modes_x, modes_y <= 16,
+ * radius <= 3.  Parameters: W [(2r+1)^2][C][C], R [modes_x][modes_y][C][C][2]
+ * (C = 3*nz), FP32 on the host side. */
+typedef struct mlb_surrogate mlb_surrogate;
+int mlb_surrogate_create(mlb_op* dipole, int modes_x, int modes_y, int radius, mlb_surrogate** out);
+int mlb_surrogate_destroy(mlb_surrogate* s);
+/* out: C, CP (padded channels), modes_x, modes_y, radius, number of W values, number of R values (floats) */
+int mlb_surrogate_sizes(const mlb_surrogate* s, int out[7]);
+int mlb_surrogate_get_params(mlb_surrogate* s, float* w, float* r);
+int mlb_surrogate_set_params(mlb_surrogate* s, const float* w, const float* r);
+/* Exact evaluation every k steps and whenever the estimated relative field
+ * error eps * |dH| / |H| exceeds tol (eps: the validated relative error of
+ * the predicted update, set by mlb_surrogate_validate or here when > 0). */
+int mlb_surrogate_set_schedule(mlb_surrogate* s, int k, double tol, double eps);
+/* Online training on the plain method: nsteps canonical steps of ss with
+ * ops (which hold the surrogate's operator) and l; every step that is not
+ * the first of a window of `window` steps is one Adam step on the pair
+ * (m - m0, H - H0) with learning rate lr.  loss_out[0]: mean relative loss
+ * |dH_pred - dH|^2 / |dH|^2 over the last quarter of the iterations. */
+int mlb_surrogate_train(mlb_surrogate* s, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps,
+                        int window, double lr, double* loss_out);
+/* nsteps plain steps; at every step inside a window of `window` steps the
+ * surrogate's field is compared with the exact one.  out: mean and max of
+ * |dH_pred - dH|/|dH|, mean and max of |H_pred - H|/|H|, mean and max of
+ * |H0 - H|/|H| (the field without the surrogate).  Sets eps to the max of
+ * the first pair. */
+int mlb_surrogate_validate(mlb_surrogate* s, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps,
+                           int window, double out[6]);
+/* nsteps canonical steps (captured) with the surrogate standing in for its
+ * operator between exact evaluations. */
+int mlb_surrogate_run(mlb_surrogate* s, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
+/* out: exact evaluations, surrogate evaluations, failed residual checks of
+ * the last run; *last_bound: the last estimated relative field error. */
+int mlb_surrogate_stats(mlb_surrogate* s, long long out[3], double* last_bound);
+/* Host-array forms for checks: x (3 arrays of nx*ny*nz, SpinSystem layout)
+ * -> dh = net(x); and the gradients of L = |net(x) - t|^2 / |t|^2 with
+ * respect to W and R (p: the prediction the gradients used; may be NULL). */
+int mlb_surrogate_forward(mlb_surrogate* s, const float* const x[3], float* const dh[3]);
+int mlb_surrogate_gradients(mlb_surrogate* s, const float* const x[3], const float* const t[3], float* dw, float* dr,
+                            float* const p[3], double* loss);
+
 /* ---------------------------------------------------------------- no-allocation dipole field
  * No counterpart in the reference (LongRange::init allocates the FFT work
  * arrays per operator, M/cpu/longrange/spinoperationlongrange.cpp:98-139).

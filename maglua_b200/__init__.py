@@ -119,6 +119,18 @@ _SIGS = {
     "mlb_llg_apply": ([_P, _P, C.c_double, _P, _P, C.c_int], C.c_int),
     "mlb_run": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int], C.c_int),
     "mlb_dipole_field_noalloc": ([_P, _P, _P, _P, _P, _P, _P, _P], C.c_int),
+    "mlb_surrogate_create": ([_P, C.c_int, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_surrogate_destroy": ([_P], C.c_int),
+    "mlb_surrogate_sizes": ([_P, _I], C.c_int),
+    "mlb_surrogate_get_params": ([_P, _F, _F], C.c_int),
+    "mlb_surrogate_set_params": ([_P, _F, _F], C.c_int),
+    "mlb_surrogate_set_schedule": ([_P, C.c_int, C.c_double, C.c_double], C.c_int),
+    "mlb_surrogate_train": ([_P, _P, C.POINTER(_P), C.c_int, _P, C.c_int, C.c_int, C.c_double, _D], C.c_int),
+    "mlb_surrogate_validate": ([_P, _P, C.POINTER(_P), C.c_int, _P, C.c_int, C.c_int, _D], C.c_int),
+    "mlb_surrogate_run": ([_P, _P, C.POINTER(_P), C.c_int, _P, C.c_int], C.c_int),
+    "mlb_surrogate_stats": ([_P, C.POINTER(C.c_longlong), _D], C.c_int),
+    "mlb_surrogate_forward": ([_P, C.POINTER(_F), C.POINTER(_F)], C.c_int),
+    "mlb_surrogate_gradients": ([_P, C.POINTER(_F), C.POINTER(_F), _F, _F, C.POINTER(_F), _D], C.c_int),
     "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
     "mlb_plan_kernel_times": ([_P, C.c_int, C.c_char_p, _D, _I], C.c_int),
@@ -1085,6 +1097,102 @@ class Ensemble:
         out = _P()
         _ck(_lib.mlb_ensemble_get_stream(self._h, C.byref(out)))
         return out.value or 0
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fptrs(arrs):
+    return (_F * 3)(*[a.ctypes.data_as(_F) for a in arrs])
+
+
+class Surrogate:
+    """Learned dipolar surrogate bound to a Dipole or LongRange operator (a
+    B200 extension without a reference counterpart): a linear spectral-conv
+    network predicting the field change from the spin change since the last
+    exact evaluation, BF16 on the tensor cores."""
+
+    def __init__(self, op, modes=(16, 16), radius=2):
+        _ensure_init()
+        h = _P()
+        _ck(_lib.mlb_surrogate_create(op._h, int(modes[0]), int(modes[1]), int(radius), C.byref(h)))
+        self._h = h
+        self._op = op
+        self.dims = tuple(op._dims)
+        out = (C.c_int * 7)()
+        _ck(_lib.mlb_surrogate_sizes(h, out))
+        self.C, self.CP, self.mx, self.my, self.radius, self.nw, self.nr = list(out)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_surrogate_destroy(h)
+            self._h = None
+
+    def params(self):
+        w = np.zeros(self.nw, np.float32)
+        r = np.zeros(self.nr, np.float32)
+        _ck(_lib.mlb_surrogate_get_params(self._h, w.ctypes.data_as(_F), r.ctypes.data_as(_F)))
+        dia = 2 * self.radius + 1
+        W = w.reshape(dia * dia, self.C, self.C).astype(np.float64)
+        R = r.reshape(self.mx, self.my, self.C, self.C, 2).astype(np.float64)
+        return W, R[..., 0] + 1j * R[..., 1]
+
+    def setParams(self, W, R):
+        w = _f32(np.asarray(W).reshape(-1))
+        Rc = np.asarray(R)
+        r = _f32(np.stack([Rc.real, Rc.imag], axis=-1).reshape(-1))
+        _ck(_lib.mlb_surrogate_set_params(self._h, w.ctypes.data_as(_F), r.ctypes.data_as(_F)))
+
+    def setSchedule(self, k, tol=1e-3, eps=0.0):
+        _ck(_lib.mlb_surrogate_set_schedule(self._h, int(k), float(tol), float(eps)))
+
+    def forward(self, x):
+        xs = [_f32(x[c]) for c in range(3)]
+        out = [np.zeros_like(xs[0]) for _ in range(3)]
+        _ck(_lib.mlb_surrogate_forward(self._h, _fptrs(xs), _fptrs(out)))
+        return np.stack(out)
+
+    def gradients(self, x, t):
+        xs = [_f32(x[c]) for c in range(3)]
+        ts = [_f32(t[c]) for c in range(3)]
+        p = [np.zeros_like(xs[0]) for _ in range(3)]
+        dw = np.zeros(self.nw, np.float32)
+        dr = np.zeros(self.nr, np.float32)
+        loss = C.c_double()
+        _ck(_lib.mlb_surrogate_gradients(self._h, _fptrs(xs), _fptrs(ts), dw.ctypes.data_as(_F),
+                                         dr.ctypes.data_as(_F), _fptrs(p), C.byref(loss)))
+        dia = 2 * self.radius + 1
+        dR = dr.reshape(self.mx, self.my, self.C, self.C, 2).astype(np.float64)
+        return (dw.reshape(dia * dia, self.C, self.C).astype(np.float64), dR[..., 0] + 1j * dR[..., 1],
+                np.stack(p), loss.value)
+
+    @staticmethod
+    def _ops(ops):
+        return (_P * len(ops))(*[o._h for o in ops])
+
+    def train(self, ss, ops, llg, nsteps, window=10, lr=1e-3):
+        loss = C.c_double()
+        _ck(_lib.mlb_surrogate_train(self._h, ss._h, self._ops(ops), len(ops), llg._h, int(nsteps), int(window),
+                                     float(lr), C.byref(loss)))
+        return loss.value
+
+    def validate(self, ss, ops, llg, nsteps, window=10):
+        out = np.zeros(6)
+        _ck(_lib.mlb_surrogate_validate(self._h, ss._h, self._ops(ops), len(ops), llg._h, int(nsteps), int(window),
+                                        _dp(out)))
+        keys = ["dh_mean", "dh_max", "field_mean", "field_max", "field_without_mean", "field_without_max"]
+        return dict(zip(keys, out.tolist()))
+
+    def run(self, ss, ops, llg, nsteps):
+        _ck(_lib.mlb_surrogate_run(self._h, ss._h, self._ops(ops), len(ops), llg._h, int(nsteps)))
+
+    def stats(self):
+        out = (C.c_longlong * 3)()
+        b = C.c_double()
+        _ck(_lib.mlb_surrogate_stats(self._h, out, C.byref(b)))
+        return {"exact": out[0], "surrogate": out[1], "failed": out[2], "last_bound": b.value}
 
 
 def run(ss, ops, llg, nsteps):

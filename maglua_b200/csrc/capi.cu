@@ -213,6 +213,7 @@ struct mlb_system {
     bool capturing = false;
     bool dry = false;               // replay host bookkeeping without launching
     bool last_fused = false;
+    mlb_surrogate* sur = nullptr;   // learned surrogate standing in for its operator (surrogate runs)
 };
 
 struct mlb_op {
@@ -581,6 +582,7 @@ void plan_sizes(mlb_op* op, ConvPlan& P)
     }
     k.Kx = k.Px / 2 + 1;
     k.nrep = 1;
+    k.run_if = nullptr;
     int ty = 16;
     while (ty > 1 && (size_t)2 * ty * k.Px * cb > 96 * 1024) ty /= 2;
     k.ty = ty;
@@ -931,6 +933,12 @@ void check_dims(const mlb_op* op, const mlb_system* s)
         fail(MLB_EINVAL, "operator and SpinSystem sizes differ");
 }
 
+// Learned-surrogate hooks (defined with mlb_surrogate below): the operator's
+// field for this step from the surrogate or, when the device schedule asks
+// for it, the exact convolution; and the end-of-step schedule update.
+bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl);
+void sur_advance(mlb_system* s);
+
 void op_apply(mlb_op* op, mlb_system* s)
 {
     check_dims(op, s);
@@ -1014,6 +1022,7 @@ void op_apply(mlb_op* op, mlb_system* s)
         P.k.g = op->g * op->gs / ((double)P.k.Px * P.k.Py * P.k.Pz);
         sl.state = ST_DATA;
         if (s->dry) return;
+        if (s->sur && sur_hook(op, s, sl)) return;
         if (s->rb == 4 && mlb::conv_fast_ok(P.k)) {
             const float* sp[3] = {static_cast<const float*>(s->sp[s->cur][0]), static_cast<const float*>(s->sp[s->cur][1]),
                                   static_cast<const float*>(s->sp[s->cur][2])};
@@ -1295,6 +1304,7 @@ void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
     for (int i = 0; i < nops; i++) op_apply(ops[i], s);
     sum_fields(s);
     llg_apply(l, s, 1.0, s, s, 1);
+    if (s->sur && !s->dry) sur_advance(s);
 }
 
 void advance_sweep(mlb_op* const* ops, int nops)
@@ -1723,6 +1733,7 @@ int mlb_init(int device)
         CK(mlb::conv_configure());
         CK(mlb::fftreg_init());
         CK(mlb::conv_fast_configure());
+        CK(mlb::sur_configure());
     });
 }
 
@@ -2836,6 +2847,533 @@ int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, doubl
 int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
 {
     return guard([&] { *stream = (void*)e->st; });
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- learned surrogate
+struct mlb_surrogate {
+    mlb_op* op = nullptr;
+    int nx = 0, ny = 0, nz = 0, n = 0;
+    SurK k{};
+    int nw = 0, nr = 0;
+    double g_train = 0.0;       // operator strength x global scale the parameters were trained at
+    int adam_step = 0;
+    int kint = 10;              // exact evaluation every kint steps
+    double tol = 1e-3;          // bound on the estimated relative field error
+    double eps = 0.1;           // validated relative error of the predicted update
+    DBuf<float> w, r, gw, gr, mw, vw, mr, vr;
+    DBuf<uint8_t> wc, Fc;
+    DBuf<__nv_bfloat16> F;
+    DBuf<float2> twy, Xp, Yh, Zh, Gh;
+    DBuf<uint4> Xb;             // BF16 input records [CP/8][ny][nx] for the output kernel
+    DBuf<uint8_t> Zb;           // per-row B tiles of the mixed spectrum [ny][CP x 32 BF16]
+    DBuf<unsigned int> ycnt;    // per-kx arrival counters of the y-DFT
+    DBuf<float> m0[3], h0[3], P[3], G[3], part;
+    DBuf<double> lpart, lsum;
+    DBuf<int> err;
+    DBuf<SurDev> dev;
+    int lnb = 1;
+    long long stats[3] = {0, 0, 0};
+    double last_bound = 0.0;
+};
+
+namespace {
+
+uint16_t host_bf16(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+    const uint32_t lsb = (u >> 16) & 1u;
+    u += 0x7fffu + lsb;           // round to nearest even
+    return (uint16_t)(u >> 16);
+}
+
+void sur_upload_w(mlb_surrogate* S, const std::vector<float>& w)
+{
+    const int C = S->k.C, CP = S->k.CP, no = (2 * S->k.rad + 1) * (2 * S->k.rad + 1);
+    std::vector<uint16_t> t((size_t)no * CP * CP, 0);
+    for (int o = 0; o < no; o++)
+        for (int co = 0; co < C; co++)
+            for (int ci = 0; ci < C; ci++) {
+                const size_t byte = (size_t)(co >> 3) * (CP / 8) * 128 + (ci >> 3) * 128 + (co & 7) * 16 + (ci & 7) * 2;
+                t[(size_t)o * CP * CP + byte / 2] = host_bf16(w[((size_t)o * C + co) * C + ci]);
+            }
+    CK(cudaMemcpy(S->wc.p, t.data(), t.size() * 2, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S->w.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice));
+}
+
+void sur_check_err(mlb_surrogate* S)
+{
+    int e = 0;
+    CK(cudaMemcpy(&e, S->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        CK(cudaMemset(S->err.p, 0, sizeof(int)));
+        fail(MLB_ECUDA, "tensor-core completion wait gave up (results of that launch are invalid)");
+    }
+}
+
+// dH (mode 1) or H0 + ratio dH (mode 0, with residual statistics in dev) for
+// a = m, b = m0 (b may be null: the input is a itself).
+void sur_forward(mlb_surrogate* S, const float* const a[3], const float* const b[3], int mode,
+                 const float* const h0[3], float* const out[3], SurDev* dev, const int* skip, float ratio,
+                 cudaStream_t st)
+{
+    SurK k = S->k;
+    k.skip_if = skip;
+    k.ratio = ratio;
+    CK(mlb::launch_sur_xdft(k, a, b, S->F.p, S->Xp.p, S->Xb.p, S->err.p, st));
+    CK(mlb::launch_sur_ydft(k, S->Xp.p, S->twy.p, reinterpret_cast<const float2*>(S->r.p), S->Yh.p, S->Zh.p,
+                            S->ycnt.p, st));
+    CK(mlb::launch_sur_zrows(k, S->Zh.p, S->twy.p, S->Zb.p, st));
+    CK(mlb::launch_sur_out(k, S->Xb.p, h0, out, S->wc.p, S->Fc.p, S->Zb.p, dev, S->err.p, mode, st));
+}
+
+// Loss, gradients and one Adam step for the pair (a - b, hx - h0) (h0 may be
+// null: target hx); leaves sum T^2, sum (P - T)^2, sum hx^2 in lsum.
+void sur_train_iter(mlb_surrogate* S, const float* const a[3], const float* const b[3], const float* const hx[3],
+                    const float* const h0[3], double lr, bool update, cudaStream_t st)
+{
+    float* P[3] = {S->P[0].p, S->P[1].p, S->P[2].p};
+    float* G[3] = {S->G[0].p, S->G[1].p, S->G[2].p};
+    const float* Gc[3] = {G[0], G[1], G[2]};
+    sur_forward(S, a, b, 1, nullptr, P, nullptr, nullptr, 1.f, st);
+    const float* Pc[3] = {P[0], P[1], P[2]};
+    CK(mlb::launch_sur_loss(S->n, Pc, hx, h0, G, S->lpart.p, S->lnb, S->lsum.p, st));
+    SurK k = S->k;
+    k.skip_if = nullptr;
+    CK(mlb::launch_sur_xdft(k, Gc, nullptr, S->F.p, S->Xp.p, nullptr, S->err.p, st));
+    CK(mlb::launch_sur_ydft(k, S->Xp.p, S->twy.p, nullptr, S->Gh.p, nullptr, S->ycnt.p, st));
+    CK(mlb::launch_sur_grad_r(k, S->Gh.p, S->Yh.p, reinterpret_cast<float2*>(S->gr.p), st));
+    CK(mlb::launch_sur_grad_w(k, a, b, Gc, S->part.p, S->gw.p, st));
+    if (!update) return;
+    S->adam_step++;
+    CK(mlb::launch_sur_adam(S->w.p, S->r.p, S->gw.p, S->gr.p, S->mw.p, S->vw.p, S->mr.p, S->vr.p, S->wc.p,
+                            S->lsum.p, (float)lr, S->adam_step, S->nw, S->nr, S->k.C, S->k.CP, st));
+}
+
+void sur_check_use(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int nops)
+{
+    if (ss->rb != 4) fail(MLB_EUNSUP, "the surrogate runs on FP32 systems");
+    if (ss->nx != S->nx || ss->ny != S->ny || ss->nz != S->nz) fail(MLB_EINVAL, "surrogate and SpinSystem sizes differ");
+    bool found = false;
+    for (int i = 0; i < nops; i++) {
+        check_dims(ops[i], ss);
+        if (ops[i] == S->op) found = true;
+    }
+    if (!found) fail(MLB_EINVAL, "the surrogate's operator is not among the step's operators");
+}
+
+void sur_snapshot_now(mlb_surrogate* S, mlb_system* ss, const Slot& sl)
+{
+    for (int c = 0; c < 3; c++) {
+        CK(cudaMemcpyAsync(S->m0[c].p, ss->sp[ss->cur][c], sizeof(float) * S->n, cudaMemcpyDeviceToDevice, ss->st));
+        CK(cudaMemcpyAsync(S->h0[c].p, sl.h[c], sizeof(float) * S->n, cudaMemcpyDeviceToDevice, ss->st));
+    }
+}
+
+// One canonical step with the hook point after the operators: f(step) runs
+// with the surrogate operator's exact field in its slot.
+template <class Fn>
+void plain_step_with(mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, mlb_surrogate* S, Fn&& f)
+{
+    reset_fields(ss);
+    for (int i = 0; i < nops; i++) op_apply(ops[i], ss);
+    const int si = slot_find(ss, S->op->slot.c_str());
+    materialize(ss, si);
+    f(ss->slots[si]);
+    sum_fields(ss);
+    llg_apply(l, ss, 1.0, ss, ss, 1);
+    advance_sweep(ops, nops);
+}
+
+} // namespace
+
+namespace {
+
+bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl)
+{
+    mlb_surrogate* S = s->sur;
+    if (S->op != op || s->rb != 4) return false;
+    SurDev* d = S->dev.p;
+    const float* a[3];
+    const float* b[3] = {S->m0[0].p, S->m0[1].p, S->m0[2].p};
+    const float* h0[3] = {S->h0[0].p, S->h0[1].p, S->h0[2].p};
+    float* out[3];
+    for (int c = 0; c < 3; c++) {
+        a[c] = static_cast<const float*>(s->sp[s->cur][c]);
+        out[c] = static_cast<float*>(sl.h[c]);
+    }
+    const float ratio = S->g_train > 0 ? (float)(op->g * op->gs / S->g_train) : 1.f;
+    sur_forward(S, a, b, 0, h0, out, d, &d->exact, ratio, s->st);
+    // exact passes, run only when the schedule or the residual check asks
+    ConvPlan& P = *op->plan;
+    ConvK kk = P.k;
+    kk.run_if = &d->exact;
+    if (mlb::conv_fast_ok(kk)) {
+        CK(mlb::launch_conv_fast(kk, P.L, reinterpret_cast<const float2*>(P.tw.p), a,
+                                 reinterpret_cast<float2*>(P.spec.p), reinterpret_cast<const float*>(P.ten6.p), out,
+                                 s->st));
+    } else {
+        const void* av[3] = {a[0], a[1], a[2]};
+        void* ov[3] = {out[0], out[1], out[2]};
+        CK(mlb::launch_conv(kk, P.L[0], P.L[1], P.L[2], P.tw.p, av, P.spec.p, P.ten6.p, P.ten9.p, ov, 4, s->st));
+    }
+    const float* hc[3] = {out[0], out[1], out[2]};
+    float* sm[3] = {S->m0[0].p, S->m0[1].p, S->m0[2].p};
+    float* sh[3] = {S->h0[0].p, S->h0[1].p, S->h0[2].p};
+    CK(mlb::launch_sur_snapshot(d, S->n, a, hc, sm, sh, s->st));
+    return true;
+}
+
+void sur_advance(mlb_system* s) { CK(mlb::launch_sur_advance(s->sur->dev.p, s->st)); }
+
+} // namespace
+
+extern "C" {
+
+int mlb_surrogate_create(mlb_op* op, int mx, int my, int rad, mlb_surrogate** out)
+{
+    return guard([&] {
+        if (!op || !out) fail(MLB_EINVAL, "null argument");
+        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE)
+            fail(MLB_EINVAL, "the surrogate stands in for a Dipole or LongRange operator");
+        const int nx = op->nx, ny = op->ny, nz = op->nz, C = 3 * nz;
+        if (C > 32) fail(MLB_EUNSUP, "more than 10 layers in z");
+        const int CP = C <= 16 ? 16 : 32;
+        if (nx % 128 != 0) fail(MLB_EUNSUP, "nx must be a multiple of 128");
+        if (ny % (128 / CP) != 0 || ny % 4 != 0) fail(MLB_EUNSUP, "ny must be a multiple of 8 (of 4 above 16 channels)");
+        if (mx < 1 || mx > 16 || mx > nx / 2) fail(MLB_EINVAL, "modes_x must be in 1..16 and at most nx/2");
+        if (my < 2 || my > 16 || my % 2 || my > ny) fail(MLB_EINVAL, "modes_y must be even, in 2..16, at most ny");
+        if (rad < 0 || rad > 3) fail(MLB_EINVAL, "radius must be in 0..3");
+        if (mlb::sur_out_smem(CP, rad) > 226 * 1024) fail(MLB_EUNSUP, "stencil too large for shared memory");
+        std::unique_ptr<mlb_surrogate> S(new mlb_surrogate());
+        S->op = op;
+        S->nx = nx; S->ny = ny; S->nz = nz; S->n = nx * ny * nz;
+        SurK& k = S->k;
+        k.nx = nx; k.ny = ny; k.nz = nz; k.C = C; k.CP = CP; k.mx = mx; k.my = my; k.rad = rad;
+        k.nxc = nx / 64; k.skip_if = nullptr; k.ratio = 1.f;
+        const int dia = 2 * rad + 1;
+        S->nw = dia * dia * C * C;
+        S->nr = mx * my * C * C * 2;
+        for (DBuf<float>* b : {&S->w, &S->gw, &S->mw, &S->vw}) { b->alloc(S->nw); CK(cudaMemset(b->p, 0, sizeof(float) * S->nw)); }
+        for (DBuf<float>* b : {&S->r, &S->gr, &S->mr, &S->vr}) { b->alloc(S->nr); CK(cudaMemset(b->p, 0, sizeof(float) * S->nr)); }
+        S->wc.alloc((size_t)dia * dia * CP * CP * 2);
+        CK(cudaMemset(S->wc.p, 0, S->wc.n));
+        // forward x-DFT rows [2 kx + ri][x] and inverse rows in the canonical A layout
+        std::vector<uint16_t> F((size_t)32 * nx, 0), Fc((size_t)nx * 32, 0);
+        for (int kx = 0; kx < mx; kx++)
+            for (int x = 0; x < nx; x++) {
+                const double th = 2.0 * M_PI * (double)((long long)kx * x % nx) / nx;
+                const uint16_t c = host_bf16((float)std::cos(th)), s = host_bf16((float)-std::sin(th));
+                F[(size_t)(2 * kx) * nx + x] = c;
+                F[(size_t)(2 * kx + 1) * nx + x] = s;
+                for (int ri = 0; ri < 2; ri++) {
+                    const int kk = 2 * kx + ri;
+                    const size_t byte = (size_t)(x >> 3) * 512 + (kk >> 3) * 128 + (x & 7) * 16 + (kk & 7) * 2;
+                    Fc[byte / 2] = ri ? s : c;
+                }
+            }
+        S->F.alloc(F.size());
+        CK(cudaMemcpy(S->F.p, F.data(), F.size() * 2, cudaMemcpyHostToDevice));
+        S->Fc.alloc(Fc.size() * 2);
+        CK(cudaMemcpy(S->Fc.p, Fc.data(), Fc.size() * 2, cudaMemcpyHostToDevice));
+        std::vector<float2> twy((size_t)my * ny);
+        for (int j = 0; j < my; j++) {
+            const int ky = j < my / 2 ? j : ny - my + j;
+            for (int y = 0; y < ny; y++) {
+                const double th = 2.0 * M_PI * (double)((long long)ky * y % ny) / ny;
+                twy[(size_t)j * ny + y] = make_float2((float)std::cos(th), (float)-std::sin(th));
+            }
+        }
+        S->twy.alloc(twy.size());
+        CK(cudaMemcpy(S->twy.p, twy.data(), sizeof(float2) * twy.size(), cudaMemcpyHostToDevice));
+        S->Xp.alloc((size_t)k.nxc * mx * C * ny);
+        S->Yh.alloc((size_t)mx * my * C);
+        S->Gh.alloc((size_t)mx * my * C);
+        S->Zh.alloc((size_t)mx * my * C);
+        S->Xb.alloc((size_t)(CP / 8) * nx * ny);
+        S->Zb.alloc((size_t)ny * CP * 64);
+        S->ycnt.alloc(16);
+        CK(cudaMemset(S->ycnt.p, 0, sizeof(unsigned int) * 16));
+        if (mlb::sur_ydft_smem(k) > 226 * 1024) fail(MLB_EUNSUP, "ny too large for the y-DFT of this build");
+        for (int c = 0; c < 3; c++) {
+            for (DBuf<float>* b : {&S->m0[c], &S->h0[c], &S->P[c], &S->G[c]}) {
+                b->alloc(S->n);
+                CK(cudaMemset(b->p, 0, sizeof(float) * S->n));
+            }
+        }
+        S->part.alloc((size_t)(nx / 128) * (ny / 4) * S->nw);
+        S->lnb = (int)std::min<long long>(1024, std::max<long long>(1, (3LL * S->n + 255) / 256));
+        S->lpart.alloc((size_t)S->lnb * 3);
+        S->lsum.alloc(3);
+        S->err.alloc(1);
+        CK(cudaMemset(S->err.p, 0, sizeof(int)));
+        S->dev.alloc(1);
+        SurDev h{};
+        h.exact = 1;
+        h.k = S->kint;
+        h.eps = (float)S->eps;
+        h.tol = (float)S->tol;
+        CK(cudaMemcpy(S->dev.p, &h, sizeof(h), cudaMemcpyHostToDevice));
+        CK(cudaDeviceSynchronize());
+        *out = S.release();
+    });
+}
+
+int mlb_surrogate_destroy(mlb_surrogate* s)
+{
+    return guard([&] {
+        for (mlb_system* x : g_systems)
+            if (x->sur == s) x->sur = nullptr;
+        cudaDeviceSynchronize();
+        delete s;
+    });
+}
+
+int mlb_surrogate_sizes(const mlb_surrogate* s, int out[7])
+{
+    return guard([&] {
+        out[0] = s->k.C; out[1] = s->k.CP; out[2] = s->k.mx; out[3] = s->k.my; out[4] = s->k.rad;
+        out[5] = s->nw; out[6] = s->nr;
+    });
+}
+
+int mlb_surrogate_get_params(mlb_surrogate* s, float* w, float* r)
+{
+    return guard([&] {
+        if (w) CK(cudaMemcpy(w, s->w.p, sizeof(float) * s->nw, cudaMemcpyDeviceToHost));
+        if (r) CK(cudaMemcpy(r, s->r.p, sizeof(float) * s->nr, cudaMemcpyDeviceToHost));
+    });
+}
+
+int mlb_surrogate_set_params(mlb_surrogate* s, const float* w, const float* r)
+{
+    return guard([&] {
+        g_version++;
+        if (w) sur_upload_w(s, std::vector<float>(w, w + s->nw));
+        if (r) CK(cudaMemcpy(s->r.p, r, sizeof(float) * s->nr, cudaMemcpyHostToDevice));
+        if (s->g_train == 0.0) s->g_train = s->op->g * s->op->gs;
+        CK(cudaDeviceSynchronize());
+    });
+}
+
+int mlb_surrogate_set_schedule(mlb_surrogate* s, int k, double tol, double eps)
+{
+    return guard([&] {
+        g_version++;
+        if (k < 1) fail(MLB_EINVAL, "k must be at least 1");
+        s->kint = k;
+        s->tol = tol;
+        if (eps > 0) s->eps = eps;
+    });
+}
+
+int mlb_surrogate_forward(mlb_surrogate* s, const float* const x[3], float* const dh[3])
+{
+    return guard([&] {
+        const size_t bytes = sizeof(float) * s->n;
+        for (int c = 0; c < 3; c++) CK(cudaMemcpy(s->m0[c].p, x[c], bytes, cudaMemcpyHostToDevice));
+        const float* a[3] = {s->m0[0].p, s->m0[1].p, s->m0[2].p};
+        float* P[3] = {s->P[0].p, s->P[1].p, s->P[2].p};
+        sur_forward(s, a, nullptr, 1, nullptr, P, nullptr, nullptr, 1.f, 0);
+        CK(cudaDeviceSynchronize());
+        sur_check_err(s);
+        for (int c = 0; c < 3; c++) CK(cudaMemcpy(dh[c], P[c], bytes, cudaMemcpyDeviceToHost));
+    });
+}
+
+int mlb_surrogate_gradients(mlb_surrogate* s, const float* const x[3], const float* const t[3], float* dw, float* dr,
+                            float* const p[3], double* loss)
+{
+    return guard([&] {
+        const size_t bytes = sizeof(float) * s->n;
+        for (int c = 0; c < 3; c++) {
+            CK(cudaMemcpy(s->m0[c].p, x[c], bytes, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(s->h0[c].p, t[c], bytes, cudaMemcpyHostToDevice));
+        }
+        const float* a[3] = {s->m0[0].p, s->m0[1].p, s->m0[2].p};
+        const float* hx[3] = {s->h0[0].p, s->h0[1].p, s->h0[2].p};
+        sur_train_iter(s, a, nullptr, hx, nullptr, 0.0, false, 0);
+        CK(cudaDeviceSynchronize());
+        sur_check_err(s);
+        double sums[3];
+        CK(cudaMemcpy(sums, s->lsum.p, sizeof(sums), cudaMemcpyDeviceToHost));
+        const double sc = sums[0] > 0 ? 1.0 / sums[0] : 0.0;
+        if (dw) {
+            CK(cudaMemcpy(dw, s->gw.p, sizeof(float) * s->nw, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < s->nw; i++) dw[i] = (float)(dw[i] * sc);
+        }
+        if (dr) {
+            CK(cudaMemcpy(dr, s->gr.p, sizeof(float) * s->nr, cudaMemcpyDeviceToHost));
+            for (int i = 0; i < s->nr; i++) dr[i] = (float)(dr[i] * sc);
+        }
+        if (p)
+            for (int c = 0; c < 3; c++)
+                if (p[c]) CK(cudaMemcpy(p[c], s->P[c].p, bytes, cudaMemcpyDeviceToHost));
+        if (loss) *loss = sums[1] * sc;
+    });
+}
+
+int mlb_surrogate_train(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps,
+                        int window, double lr, double* loss_out)
+{
+    return guard([&] {
+        sur_check_use(S, ss, ops, nops);
+        if (window < 2) fail(MLB_EINVAL, "window must be at least 2");
+        g_version++;
+        S->g_train = S->op->g * S->op->gs;
+        std::vector<double> hist;
+        DBuf<double> dh;
+        dh.alloc((size_t)3 * std::max(1, nsteps));
+        int it = 0;
+        for (int step = 0; step < nsteps; step++) {
+            plain_step_with(ss, ops, nops, l, S, [&](Slot& sl) {
+                if (step % window == 0) {
+                    sur_snapshot_now(S, ss, sl);
+                    return;
+                }
+                const float* a[3];
+                const float* b[3] = {S->m0[0].p, S->m0[1].p, S->m0[2].p};
+                const float* hx[3];
+                const float* h0[3] = {S->h0[0].p, S->h0[1].p, S->h0[2].p};
+                for (int c = 0; c < 3; c++) {
+                    a[c] = static_cast<const float*>(ss->sp[ss->cur][c]);
+                    hx[c] = static_cast<const float*>(sl.h[c]);
+                }
+                sur_train_iter(S, a, b, hx, h0, lr, true, ss->st);
+                CK(cudaMemcpyAsync(dh.p + 3 * (size_t)it, S->lsum.p, sizeof(double) * 3, cudaMemcpyDeviceToDevice,
+                                   ss->st));
+                it++;
+            });
+        }
+        CK(cudaStreamSynchronize(ss->st));
+        sur_check_err(S);
+        hist.resize((size_t)3 * it);
+        if (it) CK(cudaMemcpy(hist.data(), dh.p, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost));
+        double acc = 0;
+        int cnt = 0;
+        for (int i = it - std::max(1, it / 4); i < it; i++) {
+            if (i < 0 || hist[3 * i] <= 0) continue;
+            acc += hist[3 * i + 1] / hist[3 * i];
+            cnt++;
+        }
+        if (loss_out) *loss_out = cnt ? acc / cnt : 0.0;
+    });
+}
+
+int mlb_surrogate_validate(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps,
+                           int window, double out[6])
+{
+    return guard([&] {
+        sur_check_use(S, ss, ops, nops);
+        if (window < 2) fail(MLB_EINVAL, "window must be at least 2");
+        double sum[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+        int cnt = 0;
+        const float ratio = S->g_train > 0 ? (float)(S->op->g * S->op->gs / S->g_train) : 1.f;
+        for (int step = 0; step < nsteps; step++) {
+            plain_step_with(ss, ops, nops, l, S, [&](Slot& sl) {
+                if (step % window == 0) {
+                    sur_snapshot_now(S, ss, sl);
+                    return;
+                }
+                const float* a[3];
+                const float* b[3] = {S->m0[0].p, S->m0[1].p, S->m0[2].p};
+                const float* hx[3];
+                const float* h0[3] = {S->h0[0].p, S->h0[1].p, S->h0[2].p};
+                float* P[3] = {S->P[0].p, S->P[1].p, S->P[2].p};
+                float* G[3] = {S->G[0].p, S->G[1].p, S->G[2].p};
+                for (int c = 0; c < 3; c++) {
+                    a[c] = static_cast<const float*>(ss->sp[ss->cur][c]);
+                    hx[c] = static_cast<const float*>(sl.h[c]);
+                }
+                sur_forward(S, a, b, 1, nullptr, P, nullptr, nullptr, ratio, ss->st);
+                const float* Pc[3] = {P[0], P[1], P[2]};
+                CK(mlb::launch_sur_loss(S->n, Pc, hx, h0, G, S->lpart.p, S->lnb, S->lsum.p, ss->st));
+                double s3[3];
+                CK(cudaMemcpyAsync(s3, S->lsum.p, sizeof(s3), cudaMemcpyDeviceToHost, ss->st));
+                CK(cudaStreamSynchronize(ss->st));
+                if (s3[0] <= 0 || s3[2] <= 0) return;
+                const double e[3] = {std::sqrt(s3[1] / s3[0]), std::sqrt(s3[1] / s3[2]), std::sqrt(s3[0] / s3[2])};
+                for (int q = 0; q < 3; q++) { sum[q] += e[q]; mx[q] = std::max(mx[q], e[q]); }
+                cnt++;
+            });
+        }
+        sur_check_err(S);
+        for (int q = 0; q < 3; q++) {
+            out[2 * q] = cnt ? sum[q] / cnt : 0.0;
+            out[2 * q + 1] = mx[q];
+        }
+        if (cnt) S->eps = mx[0];
+    });
+}
+
+int mlb_surrogate_run(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps)
+{
+    return guard([&] {
+        sur_check_use(S, ss, ops, nops);
+        if (nsteps <= 0) return;
+        if (!S->op->plan || S->op->plan_dirty || S->op->plan->rb != 4) {
+            // build the tensor outside any capture
+            build_plan(S->op, ss->st, 4);
+        }
+        SurDev h{};
+        h.exact = 1;
+        h.k = S->kint;
+        h.eps = (float)S->eps;
+        h.tol = (float)S->tol;
+        CK(cudaMemcpyAsync(S->dev.p, &h, sizeof(h), cudaMemcpyHostToDevice, ss->st));
+        CK(cudaStreamSynchronize(ss->st));
+        ss->sur = S;
+        g_version++;
+        try {
+            bool done = false;
+            if (nsteps >= 3) {
+                mlb_plan p;
+                p.s = ss;
+                p.ops.assign(ops, ops + nops);
+                p.l = l;
+                bool ok = true;
+                try {
+                    plan_capture(&p);
+                } catch (Err&) {
+                    ok = false;
+                }
+                if (ok) {
+                    plan_launch(&p, nsteps);
+                    done = true;
+                }
+                plan_release(&p);
+            }
+            if (!done)
+                for (int k = 0; k < nsteps; k++) {
+                    do_step(ss, ops, nops, l);
+                    advance_sweep(ops, nops);
+                }
+        } catch (...) {
+            ss->sur = nullptr;
+            g_version++;
+            throw;
+        }
+        ss->sur = nullptr;
+        g_version++;
+        CK(cudaStreamSynchronize(ss->st));
+        CK(cudaMemcpy(&h, S->dev.p, sizeof(h), cudaMemcpyDeviceToHost));
+        S->stats[0] = h.nexact;
+        S->stats[1] = h.nsur - h.nfail;
+        S->stats[2] = h.nfail;
+        S->last_bound = h.last_bound;
+        sur_check_err(S);
+    });
+}
+
+int mlb_surrogate_stats(mlb_surrogate* s, long long out[3], double* last_bound)
+{
+    return guard([&] {
+        for (int q = 0; q < 3; q++) out[q] = s->stats[q];
+        if (last_bound) *last_bound = s->last_bound;
+    });
 }
 
 } // extern "C"

@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
                                                  const float* __restrict__ sy, const float* __restrict__ sz,
                                                  float2* __restrict__ spec)
 {
+    if (c.run_if && *c.run_if == 0) return;
     using X = XCfg<PX>;
     constexpr int NT = X::NT;
     extern __shared__ float2 sm[];
@@ -118,6 +119,7 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
                                                  float* __restrict__ hx, float* __restrict__ hy,
                                                  float* __restrict__ hz)
 {
+    if (c.run_if && *c.run_if == 0) return;
     using X = XCfg<PX>;
     constexpr int KX = X::KX, NT = X::NT;
     extern __shared__ float2 sm[];
@@ -192,6 +194,7 @@ template <int PY, int PZ>
 __global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
                                                                float2* __restrict__ spec, const float* __restrict__ ten6)
 {
+    if (c.run_if && *c.run_if == 0) return;
     constexpr int NT = YZT<PY, PZ>::N;
     constexpr int TPL = fr::Tpl<PY>::V;
     constexpr int LPR = NT / TPL;    // lines per round

@@ -463,6 +463,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_conv_fx(ConvK c, FftLen Lx, const typename CT<R>::T* tw, const void* sx,
                                                  const void* sy, const void* sz, typename CT<R>::T* spec)
 {
+    if (c.run_if && *c.run_if == 0) return;
     typedef typename CT<R>::T C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* smf = reinterpret_cast<C*>(smraw);
@@ -495,6 +496,7 @@ template <typename R>
 __global__ void __launch_bounds__(512) k_conv_yz(ConvK c, FftLen Ly, FftLen Lz, const typename CT<R>::T* tw,
                                                  typename CT<R>::T* spec, const R* ten6, const typename CT<R>::T* ten9)
 {
+    if (c.run_if && *c.run_if == 0) return;
     typedef typename CT<R>::T C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* smf = reinterpret_cast<C*>(smraw);
@@ -556,6 +558,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_conv_ix(ConvK c, FftLen Lx, const typename CT<R>::T* tw, const typename CT<R>::T* spec,
                                                  void* hx, void* hy, void* hz)
 {
+    if (c.run_if && *c.run_if == 0) return;
     typedef typename CT<R>::T C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* smf = reinterpret_cast<C*>(smraw);
@@ -903,6 +906,12 @@ cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* con
 cudaError_t launch_advance_step(DevStep* d, cudaStream_t st)
 {
     k_advance_step<<<1, 1, 0, st>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st)
+{
+    k_partial_final<<<1, 32, 0, st>>>(part, nb, nq, out);
     return cudaGetLastError();
 }
 

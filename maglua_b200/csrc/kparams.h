@@ -121,6 +121,7 @@ struct ConvK {
     double g;                // strength * global_scale / (Px*Py*Pz)
     int fx, fy, fz;          // FftLen indices
     int nrep;                // replicas of this size packed back to back (1 for a system)
+    const int* run_if;       // when set, the passes run only while *run_if != 0
 };
 
 // Fused step for uniform-parameter systems (k_fused_fast): every constant
@@ -142,6 +143,36 @@ struct FastK {
     float addw;
     int llg_type, tof, renorm, dt_zero;
     float dt, precess, c_prec, c_damp, c_rot, ms;
+};
+
+// ------------------------------------------------------------- learned surrogate
+// Linear spectral-conv network on the in-plane grid (ny x nx) with the
+// (component, z) pairs as channels: ch = c * nz + z, C = 3 nz real channels
+// padded to CP.  Output channel co at site s:
+//   sum_{o, ci} W[o][co][ci] X[ci][s + o]                      (stencil, |o_x|,|o_y| <= rad)
+// + sum_{kx < mx, ky} w_kx / (nx ny) Re(e^{i k.s} sum_ci R_k[co][ci] Xhat_k[ci])
+// with Xhat the 2D DFT of X restricted to the retained modes.
+struct SurK {
+    int nx, ny, nz;
+    int C, CP;
+    int mx, my;               // kx < mx; ky in {0..my/2-1} and {ny-my/2..ny-1}
+    int rad;
+    int nxc;                  // 128-wide x chunks of the x-DFT (nx / 128)
+    const int* skip_if;       // kernels return at once while *skip_if != 0
+    float ratio;              // strength now / strength at training
+};
+
+// Device state of a surrogate-driven run (one block per surrogate).
+struct SurDev {
+    int exact;                // this step evaluates the exact convolution
+    int cycle;                // steps since the last exact evaluation
+    int k;                    // exact evaluation every k steps
+    int nexact, nfail, nsur;  // counters: exact steps, failed residual checks, surrogate steps
+    float eps;                // validation relative error of the predicted update
+    float tol;                // bound on the estimated relative field error
+    float last_bound;
+    unsigned int arrivals;    // CTAs of the output kernel done this step
+    double sums[2];           // sum dH^2, sum H^2 of this step
 };
 
 // Block table of the packed-ensemble fused kernel.

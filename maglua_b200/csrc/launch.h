@@ -1,5 +1,6 @@
 // launch.h -- host-callable launchers for the kernels in kernels.cu.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "device.cuh"
@@ -57,6 +58,7 @@ cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* con
                        const void* dsa, const void* dsg, double da, double dg, const LlgK& L,
                        void* const out[3], int rb, cudaStream_t st);
 cudaError_t launch_advance_step(DevStep* d, cudaStream_t st);
+cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st);
 cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
                              double* out, int rb, cudaStream_t st);
 cudaError_t launch_dot(const void* const s[3], const void* const h[3], int n, double* part, int nb, double* out,
@@ -79,4 +81,28 @@ cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx
                                 int rb, cudaStream_t st);
 cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb,
                                 cudaStream_t st);
+// Learned surrogate (surrogate.cu).
+size_t sur_out_smem(int CP, int rad);
+size_t sur_gw_smem(int C, int rad);
+size_t sur_ydft_smem(const SurK& k);
+cudaError_t sur_configure();
+cudaError_t launch_sur_xdft(const SurK& k, const float* const a[3], const float* const b[3],
+                            const __nv_bfloat16* F, float2* Xp, uint4* Xb, int* err, cudaStream_t st);
+cudaError_t launch_sur_ydft(const SurK& k, const float2* Xp, const float2* twy, const float2* R, float2* Yh,
+                            float2* Zh, unsigned int* cnt, cudaStream_t st);
+cudaError_t launch_sur_zrows(const SurK& k, const float2* Zh, const float2* twy, uint8_t* Zb, cudaStream_t st);
+cudaError_t launch_sur_out(const SurK& k, const uint4* Xb, const float* const h0[3], float* const out[3],
+                           const uint8_t* Wc, const uint8_t* Fc, const uint8_t* Zb, SurDev* dev, int* err, int mode,
+                           cudaStream_t st);
+cudaError_t launch_sur_snapshot(SurDev* d, int n, const float* const m[3], const float* const h[3],
+                                float* const sm[3], float* const sh[3], cudaStream_t st);
+cudaError_t launch_sur_advance(SurDev* d, cudaStream_t st);
+cudaError_t launch_sur_loss(int n, const float* const P[3], const float* const X[3], const float* const H0[3],
+                            float* const G[3], double* part, int nb, double* out, cudaStream_t st);
+cudaError_t launch_sur_grad_w(const SurK& k, const float* const a[3], const float* const b[3],
+                              const float* const g[3], float* part, float* gw, cudaStream_t st);
+cudaError_t launch_sur_grad_r(const SurK& k, const float2* Gh, const float2* Xh, float2* dR, cudaStream_t st);
+cudaError_t launch_sur_adam(float* w, float* r, const float* gw, const float* gr, float* mw, float* vw, float* mr,
+                            float* vr, uint8_t* wc, const double* sums, float lr, int step, int nw, int nr, int C,
+                            int CP, cudaStream_t st);
 } // namespace mlb

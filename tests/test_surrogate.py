@@ -1,0 +1,180 @@
+"""Learned dipolar surrogate (no reference counterpart): the tcgen05 BF16
+forward and the FP32 training kernels against the FP64 CPU reference of the
+network (oracle/surrogate.py), online training on pairs from the plain
+method, what the trained network gains over holding the field between exact
+evaluations, and the captured run with its exact schedule and residual
+check.
+
+Tolerances: the stencil branch with BF16-representable inputs and weights is
+exact up to FP32 accumulation (1e-5); the spectral branch rounds its DFT rows
+and mixed spectrum to BF16 (2e-2); the stencil gradient is FP32 (1e-4); the
+mode gradient uses a BF16 transform of G (2e-2).
+"""
+import numpy as np
+import pytest
+
+from oracle import surrogate as OS
+from helpers import random_spins, rel_err
+
+
+def crel(a, b):
+    return rel_err(np.stack([np.real(a), np.imag(a)]), np.stack([np.real(b), np.imag(b)]))
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (128, 16, 2)
+N = DIMS[0] * DIMS[1] * DIMS[2]
+C = 3 * DIMS[2]
+MODES = (8, 8)
+RAD = 2
+
+
+@pytest.fixture(scope="module")
+def M():
+    import maglua_b200 as M
+    M.init(0)
+    return M
+
+
+def bf16(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _sur(M, dims=DIMS, modes=MODES, radius=RAD):
+    d = M.Dipole(*dims)
+    d.setStrength(0.05)
+    return M.Surrogate(d, modes, radius), d
+
+
+def _random_params(seed, scale_w=0.1, scale_r=0.3):
+    r = np.random.default_rng(seed)
+    W = r.normal(size=((2 * RAD + 1) ** 2, C, C)) * scale_w
+    R = (r.normal(size=(MODES[0], MODES[1], C, C)) + 1j * r.normal(size=(MODES[0], MODES[1], C, C))) * scale_r
+    return W, R
+
+
+def test_stencil_branch_layout_exact(M):
+    S, _ = _sur(M)
+    W, _ = _random_params(1)
+    W = bf16(W)
+    R = np.zeros((MODES[0], MODES[1], C, C), complex)
+    S.setParams(W, R)
+    x = bf16(np.random.default_rng(2).normal(size=(3, N)))
+    got = S.forward(x)
+    ref = OS.forward(x, W, R, DIMS, MODES[0], MODES[1], RAD)
+    assert rel_err(got, ref) <= 1e-5
+
+
+def test_spectral_branch(M):
+    S, _ = _sur(M)
+    _, R = _random_params(3)
+    W = np.zeros(((2 * RAD + 1) ** 2, C, C))
+    S.setParams(W, R)
+    x = np.random.default_rng(4).normal(size=(3, N))
+    got = S.forward(x)
+    ref = OS.forward(x.astype(np.float32), W, R.astype(np.complex64), DIMS, MODES[0], MODES[1], RAD)
+    assert rel_err(got, ref) <= 2e-2
+
+
+def test_full_forward_two_calls(M):
+    S, _ = _sur(M)
+    W, R = _random_params(5)
+    S.setParams(W, R)
+    Wr, Rr = S.params()
+    x = np.random.default_rng(6).normal(size=(3, N))
+    ref = OS.forward(x.astype(np.float32), Wr, Rr, DIMS, MODES[0], MODES[1], RAD)
+    a = S.forward(x)
+    b = S.forward(x)
+    assert np.array_equal(a, b)
+    assert rel_err(a, ref) <= 2e-2
+
+
+def test_gradients_against_cpu_reference(M):
+    S, _ = _sur(M)
+    W, R = _random_params(7)
+    S.setParams(W, R)
+    Wr, Rr = S.params()
+    r = np.random.default_rng(8)
+    x = r.normal(size=(3, N)).astype(np.float32)
+    t = r.normal(size=(3, N)).astype(np.float32)
+    dW, dR, P, loss = S.gradients(x, t)
+    # backward kernels on the device's own prediction
+    L1, dW1, dR1, _ = OS.loss_and_gradients(x, t, Wr, Rr, DIMS, MODES[0], MODES[1], RAD, pred=P)
+    assert loss == pytest.approx(L1, rel=1e-6)
+    assert rel_err(dW, dW1) <= 1e-4
+    assert crel(dR, dR1) <= 2e-2
+    # end to end against the FP64 network
+    L2, dW2, dR2, P2 = OS.loss_and_gradients(x, t, Wr, Rr, DIMS, MODES[0], MODES[1], RAD)
+    assert rel_err(P, P2) <= 2e-2
+    assert rel_err(dW, dW2) <= 3e-2
+    assert crel(dR, dR2) <= 3e-2
+
+
+def _film(M, dims, seed, T=0.1):
+    n = int(np.prod(dims))
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*random_spins(n, seed))
+    ss.setAlpha(0.02)
+    ss.setTimeStep(0.005)
+    ex = M.Exchange(ss)
+    import oracle as O
+    f, to, j = O.nn_paths(*dims, J=1.0, pbc=(1, 1, 0))
+    ex.addPaths(f, to, j)
+    ani = M.Anisotropy(ss)
+    ani.addMany(np.arange(n, dtype=np.int32), np.tile([0.0, 0.0, 1.0], (n, 1)), np.full(n, 0.02))
+    dip = M.Dipole(ss)
+    dip.setStrength(0.05)
+    ops = [ex, ani, dip]
+    if T > 0:
+        th = M.Thermal(ss)
+        th.setTemperature(T)
+        th.setSeed(seed)
+        ops.append(th)
+    return ss, ops, dip
+
+
+def test_training_gains_over_holding_the_field(M):
+    dims = (128, 128, 2)
+    ss, ops, dip = _film(M, dims, 101)
+    S = M.Surrogate(dip, (16, 16), 2)
+    llg = M.LLG.new("Quaternion")
+    loss = S.train(ss, ops, llg, 600, window=10, lr=2e-3)
+    v = S.validate(ss, ops, llg, 100, window=10)
+    assert loss < 0.2, loss
+    # the trained network's field is closer to the exact one than the field
+    # held from the last exact evaluation (the method without it)
+    assert v["field_mean"] * 4 < v["field_without_mean"], v
+    assert v["dh_mean"] < 0.5, v
+
+
+def test_run_with_zero_tolerance_equals_plain_run(M):
+    dims = (128, 32, 2)
+    ss, ops, dip = _film(M, dims, 202, T=0.0)
+    ref, ops_r, dip_r = _film(M, dims, 202, T=0.0)
+    S = M.Surrogate(dip, (8, 8), RAD)
+    W, R = _random_params(9)
+    S.setParams(W * 1e-2, R * 1e-2)
+    S.setSchedule(4, tol=0.0, eps=1.0)    # every residual check fails: every step exact
+    llg = M.LLG.new("Quaternion")
+    S.run(ss, ops, llg, 12)
+    M.run(ref, ops_r, M.LLG.new("Quaternion"), 12)
+    a = np.stack(ss.spinArrays()[:3])
+    b = np.stack(ref.spinArrays()[:3])
+    assert np.array_equal(a, b)
+    st = S.stats()
+    assert st["exact"] == 12 and st["surrogate"] == 0
+
+
+def test_run_schedule_counts_and_stays_close(M):
+    dims = (128, 128, 2)
+    ss, ops, dip = _film(M, dims, 303)
+    S = M.Surrogate(dip, (16, 16), 2)
+    llg = M.LLG.new("Quaternion")
+    S.train(ss, ops, llg, 300, window=5, lr=2e-3)
+    S.setSchedule(5, tol=1.0)             # no residual failures at this bound
+    S.run(ss, ops, llg, 40)
+    st = S.stats()
+    assert st["exact"] == 8 and st["surrogate"] == 32 and st["failed"] == 0, st
