@@ -309,8 +309,14 @@ int mlb_surrogate_train(mlb_surrogate* s, mlb_system* ss, mlb_op* const* ops, in
 int mlb_surrogate_validate(mlb_surrogate* s, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps,
                            int window, double out[6]);
 /* nsteps canonical steps (captured) with the surrogate standing in for its
- * operator between exact evaluations. */
+ * operator between exact evaluations: attach, run, detach. */
 int mlb_surrogate_run(mlb_surrogate* s, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
+/* From attach to detach every step of ss (eager calls, mlb_run, plans
+ * captured meanwhile) takes the surrogate's operator field from the
+ * surrogate, with the device schedule restarted (first step exact).  detach
+ * collects the statistics of mlb_surrogate_stats. */
+int mlb_surrogate_attach(mlb_surrogate* s, mlb_system* ss);
+int mlb_surrogate_detach(mlb_system* ss);
 /* out: exact evaluations, surrogate evaluations, failed residual checks of
  * the last run; *last_bound: the last estimated relative field error. */
 int mlb_surrogate_stats(mlb_surrogate* s, long long out[3], double* last_bound);

@@ -128,6 +128,8 @@ _SIGS = {
     "mlb_surrogate_train": ([_P, _P, C.POINTER(_P), C.c_int, _P, C.c_int, C.c_int, C.c_double, _D], C.c_int),
     "mlb_surrogate_validate": ([_P, _P, C.POINTER(_P), C.c_int, _P, C.c_int, C.c_int, _D], C.c_int),
     "mlb_surrogate_run": ([_P, _P, C.POINTER(_P), C.c_int, _P, C.c_int], C.c_int),
+    "mlb_surrogate_attach": ([_P, _P], C.c_int),
+    "mlb_surrogate_detach": ([_P], C.c_int),
     "mlb_surrogate_stats": ([_P, C.POINTER(C.c_longlong), _D], C.c_int),
     "mlb_surrogate_forward": ([_P, C.POINTER(_F), C.POINTER(_F)], C.c_int),
     "mlb_surrogate_gradients": ([_P, C.POINTER(_F), C.POINTER(_F), _F, _F, C.POINTER(_F), _D], C.c_int),
@@ -1187,6 +1189,12 @@ class Surrogate:
 
     def run(self, ss, ops, llg, nsteps):
         _ck(_lib.mlb_surrogate_run(self._h, ss._h, self._ops(ops), len(ops), llg._h, int(nsteps)))
+
+    def attach(self, ss):
+        _ck(_lib.mlb_surrogate_attach(self._h, ss._h))
+
+    def detach(self, ss):
+        _ck(_lib.mlb_surrogate_detach(ss._h))
 
     def stats(self):
         out = (C.c_longlong * 3)()

@@ -3095,9 +3095,11 @@ int mlb_surrogate_create(mlb_op* op, int mx, int my, int rad, mlb_surrogate** ou
         S->Zh.alloc((size_t)mx * my * C);
         S->Xb.alloc((size_t)(CP / 8) * nx * ny);
         S->Zb.alloc((size_t)ny * CP * 64);
+        CK(cudaMemset(S->Zb.p, 0, S->Zb.n));
         S->ycnt.alloc(16);
         CK(cudaMemset(S->ycnt.p, 0, sizeof(unsigned int) * 16));
-        if (mlb::sur_ydft_smem(k) > 226 * 1024) fail(MLB_EUNSUP, "ny too large for the y-DFT of this build");
+        if (mlb::sur_ydft_smem(k) > 128 * 1024) fail(MLB_EUNSUP, "ny too large for the y-DFT of this build");
+        if (sizeof(float2) * (mx * my * C + my * 4) > 128 * 1024) fail(MLB_EUNSUP, "too many retained modes");
         for (int c = 0; c < 3; c++) {
             for (DBuf<float>* b : {&S->m0[c], &S->h0[c], &S->P[c], &S->G[c]}) {
                 b->alloc(S->n);
@@ -3309,15 +3311,15 @@ int mlb_surrogate_validate(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops,
     });
 }
 
-int mlb_surrogate_run(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps)
+int mlb_surrogate_attach(mlb_surrogate* S, mlb_system* ss)
 {
     return guard([&] {
-        sur_check_use(S, ss, ops, nops);
-        if (nsteps <= 0) return;
-        if (!S->op->plan || S->op->plan_dirty || S->op->plan->rb != 4) {
-            // build the tensor outside any capture
-            build_plan(S->op, ss->st, 4);
-        }
+        if (ss->rb != 4) fail(MLB_EUNSUP, "the surrogate runs on FP32 systems");
+        if (ss->nx != S->nx || ss->ny != S->ny || ss->nz != S->nz)
+            fail(MLB_EINVAL, "surrogate and SpinSystem sizes differ");
+        if (ss->sur && ss->sur != S) fail(MLB_ESTATE, "another surrogate is attached to this system");
+        // the tensor spectrum is built outside any capture
+        if (!S->op->plan || S->op->plan_dirty || S->op->plan->rb != 4) build_plan(S->op, ss->st, 4);
         SurDev h{};
         h.exact = 1;
         h.k = S->kint;
@@ -3327,6 +3329,34 @@ int mlb_surrogate_run(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int 
         CK(cudaStreamSynchronize(ss->st));
         ss->sur = S;
         g_version++;
+    });
+}
+
+int mlb_surrogate_detach(mlb_system* ss)
+{
+    return guard([&] {
+        mlb_surrogate* S = ss->sur;
+        if (!S) return;
+        ss->sur = nullptr;
+        g_version++;
+        CK(cudaStreamSynchronize(ss->st));
+        SurDev h;
+        CK(cudaMemcpy(&h, S->dev.p, sizeof(h), cudaMemcpyDeviceToHost));
+        S->stats[0] = h.nexact;
+        S->stats[1] = h.nsur - h.nfail;
+        S->stats[2] = h.nfail;
+        S->last_bound = h.last_bound;
+        sur_check_err(S);
+    });
+}
+
+int mlb_surrogate_run(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps)
+{
+    return guard([&] {
+        sur_check_use(S, ss, ops, nops);
+        if (nsteps <= 0) return;
+        int rc = mlb_surrogate_attach(S, ss);
+        if (rc) fail(rc, g_err);
         try {
             bool done = false;
             if (nsteps >= 3) {
@@ -3356,15 +3386,8 @@ int mlb_surrogate_run(mlb_surrogate* S, mlb_system* ss, mlb_op* const* ops, int 
             g_version++;
             throw;
         }
-        ss->sur = nullptr;
-        g_version++;
-        CK(cudaStreamSynchronize(ss->st));
-        CK(cudaMemcpy(&h, S->dev.p, sizeof(h), cudaMemcpyDeviceToHost));
-        S->stats[0] = h.nexact;
-        S->stats[1] = h.nsur - h.nfail;
-        S->stats[2] = h.nfail;
-        S->last_bound = h.last_bound;
-        sur_check_err(S);
+        rc = mlb_surrogate_detach(ss);
+        if (rc) fail(rc, g_err);
     });
 }
 

@@ -174,8 +174,8 @@ __global__ void __launch_bounds__(256) k_sur_xdft(SurK k, const float* a0, const
 // grid (mx, C), 256 threads: the x chunks' partial sums of line (kx, ci) are
 // staged once, then Yh[kx][j][ci] = sum_y line[y] twy[j][y]
 // (twy = e^{-2 pi i ky_j y / ny}).  When R is given, the last CTA of each kx
-// to finish (cnt[kx] counts them and is reset) mixes the modes of that kx:
-// Zh[kx][j][co] = sum_ci R[kx][j][co][ci] Yh[kx][j][ci].
+// to finish (cnt[kx] counts them and is reset) mixes the modes of that kx,
+//   Zh[kx][j][co] = sum_ci R[kx][j][co][ci] Yh[kx][j][ci].
 __global__ void __launch_bounds__(256) k_sur_ydft(SurK k, const float2* __restrict__ Xp,
                                                   const float2* __restrict__ twy, const float2* __restrict__ R,
                                                   float2* __restrict__ Yh, float2* __restrict__ Zh,
@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(256) k_sur_ydft(SurK k, const float2* __restri
     if (k.skip_if && *k.skip_if) return;
     extern __shared__ float2 line[];      // [ny]
     __shared__ int last;
+    __shared__ float2 zh[16 * 32];        // [j][co] of this kx
     const int kx = blockIdx.x, ci = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int y = threadIdx.x; y < k.ny; y += blockDim.x) {
         float2 acc = make_float2(0.f, 0.f);
@@ -197,12 +198,14 @@ __global__ void __launch_bounds__(256) k_sur_ydft(SurK k, const float2* __restri
     __syncthreads();
     for (int j = warp; j < k.my; j += 8) {
         float re = 0.f, im = 0.f;
-        const float2* w = twy + (size_t)j * k.ny;
-#pragma unroll 4
+        // twiddles by recurrence from this lane's first one: t(y + 32) = t(y) t(32)
+        float2 t = lane < k.ny ? __ldg(twy + (size_t)j * k.ny + lane) : make_float2(1.f, 0.f);
+        const float2 st = __ldg(twy + (size_t)j * k.ny + (32 % k.ny));
         for (int y = lane; y < k.ny; y += 32) {
-            const float2 a = line[y], t = __ldg(w + y);
+            const float2 a = line[y];
             re += a.x * t.x - a.y * t.y;
             im += a.x * t.y + a.y * t.x;
+            t = make_float2(t.x * st.x - t.y * st.y, t.x * st.y + t.y * st.x);
         }
         for (int s = 16; s > 0; s >>= 1) {
             re += __shfl_xor_sync(0xffffffffu, re, s);
@@ -227,9 +230,11 @@ __global__ void __launch_bounds__(256) k_sur_ydft(SurK k, const float2* __restri
             re += a.x * b.x - a.y * b.y;
             im += a.x * b.y + a.y * b.x;
         }
-        Zh[((size_t)kx * k.my + j) * k.C + co] = make_float2(re, im);
+        zh[o] = make_float2(re, im);
     }
     if (threadIdx.x == 0) cnt[kx] = 0u;
+    __syncthreads();
+    for (int o = threadIdx.x; o < k.my * k.C; o += blockDim.x) Zh[(size_t)kx * k.my * k.C + o] = zh[o];
 }
 
 // ------------------------------------------------------------------ inverse y-DFT
@@ -241,32 +246,29 @@ __global__ void __launch_bounds__(256) k_sur_zrows(SurK k, const float2* __restr
                                                    const float2* __restrict__ twy, uint8_t* __restrict__ Zb)
 {
     if (k.skip_if && *k.skip_if) return;
-    extern __shared__ float2 zh[];        // [mx][my][C], then [my][ZR] twiddles
-    float2* tw = zh + (size_t)k.mx * k.my * k.C;
-    for (int o = threadIdx.x; o < k.mx * k.my * k.C; o += blockDim.x) zh[o] = Zh[o];
+    extern __shared__ float2 zs[];        // [mx][my][C], then [my][ZR] twiddles
+    float2* tw = zs + (size_t)k.mx * k.my * k.C;
+    for (int o = threadIdx.x; o < k.mx * k.my * k.C; o += blockDim.x) zs[o] = __ldg(Zh + o);
     for (int o = threadIdx.x; o < k.my * ZR; o += blockDim.x)
         tw[o] = __ldg(twy + (size_t)(o / ZR) * k.ny + blockIdx.x * ZR + o % ZR);
     __syncthreads();
     const float inv = 1.f / ((float)k.nx * (float)k.ny);
-    const int tile = k.CP * 64;           // bytes of one row's B tile
-    for (int o = threadIdx.x; o < ZR * k.CP * 16; o += blockDim.x) {
-        const int kx = o % 16, co = (o / 16) % k.CP, yl = o / (16 * k.CP);
+    const int tile = k.CP * 64;
+    for (int o = threadIdx.x; o < ZR * k.C * k.mx; o += blockDim.x) {
+        const int co = o % k.C, kx = (o / k.C) % k.mx, yl = o / (k.mx * k.C);
         const int y = blockIdx.x * ZR + yl;
         float re = 0.f, im = 0.f;
-        if (co < k.C && kx < k.mx) {
-            for (int j = 0; j < k.my; j++) {
-                const float2 z = zh[((size_t)kx * k.my + j) * k.C + co];
-                const float2 w = tw[j * ZR + yl];   // conjugated below
-                re += z.x * w.x + z.y * w.y;
-                im += z.y * w.x - z.x * w.y;
-            }
-            const float s = (kx == 0 ? 1.f : 2.f) * inv;
-            re *= s;
-            im *= s;
+#pragma unroll 4
+        for (int j = 0; j < k.my; j++) {
+            const float2 z = zs[((size_t)kx * k.my + j) * k.C + co];
+            const float2 w = tw[j * ZR + yl];   // conjugated: e^{+i ...}
+            re += z.x * w.x + z.y * w.y;
+            im += z.y * w.x - z.x * w.y;
         }
+        const float s = (kx == 0 ? 1.f : 2.f) * inv;
         const int kk = 2 * kx;
         *reinterpret_cast<uint32_t*>(Zb + (size_t)y * tile + (co >> 3) * 512 + (kk >> 3) * 128 + (co & 7) * 16 +
-                                     (kk & 7) * 2) = pack2(re, im);
+                                     (kk & 7) * 2) = pack2(s * re, s * im);
     }
 }
 
@@ -643,8 +645,8 @@ cudaError_t sur_configure()
     if ((e = out_attr<32, 0>()) || (e = out_attr<32, 1>()) || (e = out_attr<32, 2>()) || (e = out_attr<32, 3>())) return e;
     if ((e = cudaFuncSetAttribute(k_sur_xdft<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
     if ((e = cudaFuncSetAttribute(k_sur_xdft<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(k_sur_zrows, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
-    if ((e = cudaFuncSetAttribute(k_sur_ydft, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+    if ((e = cudaFuncSetAttribute(k_sur_ydft, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024))) return e;
+    if ((e = cudaFuncSetAttribute(k_sur_zrows, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024))) return e;
     return cudaFuncSetAttribute(k_sur_grad_w, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
 }
 
@@ -678,6 +680,7 @@ cudaError_t launch_sur_zrows(const SurK& k, const float2* Zh, const float2* twy,
     k_sur_zrows<<<k.ny / ZR, 256, sizeof(float2) * (k.mx * k.my * k.C + k.my * ZR), st>>>(k, Zh, twy, Zb);
     return cudaGetLastError();
 }
+
 
 cudaError_t launch_sur_out(const SurK& k, const uint4* Xb, const float* const h0[3], float* const out[3],
                            const uint8_t* Wc, const uint8_t* Fc, const uint8_t* Zb, SurDev* dev, int* err, int mode,
