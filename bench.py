@@ -128,7 +128,8 @@ def algorithmic_bytes():
     spin-step figure B = 36 + 24 + (K/N)(24 + 48*2) with K = (Px/2+1)*Py*Pz:
     fused stencil/LLG 36 B/site; forward x pass 12 B/site + 24 B/k;
     (y,z) pass with the tensor multiply 24+24+24 B/k; inverse x pass 24 B/k
-    + 12 B/site."""
+    + 12 B/site.  The fused x pass (inverse x, step, forward x of the new
+    spins) carries the three: 48 B/k + 60 B/site."""
     n = NX * NY * NZ
     Px, Py, Pz = NX, NY, 16
     Kk = (Px // 2 + 1) * Py * Pz
@@ -137,6 +138,7 @@ def algorithmic_bytes():
         "k_conv_fx": 12 * n + 24 * Kk,
         "k_conv_yz": 72 * Kk,
         "k_conv_ix": 24 * Kk + 12 * n,
+        "k_xstep": 48 * Kk + 60 * n,
     }, (36 + 24) * n + Kk * (24 + 48 * 2), n, Kk
 
 
@@ -172,7 +174,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -252,7 +254,7 @@ def cpu_baseline(procs=1, target_s=15.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

@@ -161,6 +161,9 @@ struct ConvPlan {
     DBuf<char> ten6;     // TEN6[kx][kz][ky][6] (real)
     DBuf<char> ten9;     // TEN9[kx][kz][ky][9] (complex)
     double max_imag = 0; // largest |Im| of the FP64 tensor transform (6-component)
+    // SPEC holds the forward x transform of the spins of the system whose
+    // spec_token equals this one (set by the fused x pass; 0 = none)
+    unsigned long long spec_token = 0;
 };
 
 } // namespace
@@ -214,6 +217,14 @@ struct mlb_system {
     bool dry = false;               // replay host bookkeeping without launching
     bool last_fused = false;
     mlb_surrogate* sur = nullptr;   // learned surrogate standing in for its operator (surrogate runs)
+    // Inside do_step the inverse x pass of a fast-path convolution waits for
+    // the LLG update, which runs it fused with the step (launch_xstep).
+    bool defer_x = false;
+    mlb_op* pend_op = nullptr;      // operator whose inverse x pass is pending
+    int pend_si = -1;               // and its slot
+    bool cap_carry = false;         // capture: assume SPEC holds the current spins' x transform
+    mlb_op* cap_xstep = nullptr;    // capture: the convolution whose x pass the captured step fused
+    unsigned long long spec_token = 0;   // matches ConvPlan::spec_token while that holds
 };
 
 struct mlb_op {
@@ -272,14 +283,18 @@ struct mlb_llg {
     double precess = 1.0, damp = 1.0;
 };
 
-// A captured step (two graphs, one per spin-buffer parity).
+// A captured step: one graph per spin-buffer parity q and per carry c
+// (index q + 2 c); c = 1 when the convolution's SPEC already holds the
+// forward x transform of the current spins (left there by the previous
+// step's fused x pass), so the step starts at the (y,z) pass.
 struct mlb_plan {
     mlb_system* s = nullptr;
     std::vector<mlb_op*> ops;
     mlb_llg* l = nullptr;
     bool timing = false;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    std::vector<mlb::ProfCaptured> ev[2];
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<mlb::ProfCaptured> ev[4];
+    mlb_op* carry_op = nullptr;   // the convolution whose SPEC a step leaves carried (null: none)
     std::vector<mlb::ProfCaptured>* last = nullptr;
     unsigned long long version = 0;
 };
@@ -287,6 +302,7 @@ struct mlb_plan {
 namespace {
 
 std::set<mlb_system*> g_systems;
+unsigned long long g_spec_token = 0;
 // bumped by every parameter setter; a plan captured under an older value
 // is captured again before its next launch
 unsigned long long g_version = 1;
@@ -939,10 +955,25 @@ void check_dims(const mlb_op* op, const mlb_system* s)
 bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl);
 void sur_advance(mlb_system* s);
 
+// Run a deferred inverse x pass on its own (the step took another path).
+void flush_pending(mlb_system* s)
+{
+    if (!s->pend_op) return;
+    mlb_op* op = s->pend_op;
+    Slot& sl = s->slots[s->pend_si];
+    s->pend_op = nullptr;
+    s->pend_si = -1;
+    ConvPlan& P = *op->plan;
+    float* h[3] = {static_cast<float*>(sl.h[0]), static_cast<float*>(sl.h[1]), static_cast<float*>(sl.h[2])};
+    CK(mlb::launch_conv_fast_ix(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), reinterpret_cast<float2*>(P.spec.p),
+                                h, s->st));
+}
+
 void op_apply(mlb_op* op, mlb_system* s)
 {
     check_dims(op, s);
     const int si = slot_register(s, op->slot.c_str());
+    if (s->pend_op && (is_conv(op->kind) || si == s->pend_si)) flush_pending(s);
     before_mutate(s, si);
     Slot& sl = s->slots[si];
     Term t{};
@@ -1027,10 +1058,24 @@ void op_apply(mlb_op* op, mlb_system* s)
             const float* sp[3] = {static_cast<const float*>(s->sp[s->cur][0]), static_cast<const float*>(s->sp[s->cur][1]),
                                   static_cast<const float*>(s->sp[s->cur][2])};
             float* h[3] = {static_cast<float*>(sl.h[0]), static_cast<float*>(sl.h[1]), static_cast<float*>(sl.h[2])};
+            if (s->defer_x && P.k.nrep == 1 && !P.k.general) {
+                // forward x pass only when SPEC does not already hold it
+                const bool carry = s->capturing ? s->cap_carry
+                                                : (s->spec_token != 0 && s->spec_token == P.spec_token);
+                CK(mlb::launch_conv_fast_fyz(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), sp,
+                                             reinterpret_cast<float2*>(P.spec.p),
+                                             reinterpret_cast<const float*>(P.ten6.p), !carry, s->st));
+                if (!s->capturing) P.spec_token = 0;
+                s->pend_op = op;
+                s->pend_si = si;
+                return;
+            }
+            if (!s->capturing) P.spec_token = 0;
             CK(mlb::launch_conv_fast(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), sp,
                                      reinterpret_cast<float2*>(P.spec.p), reinterpret_cast<const float*>(P.ten6.p), h,
                                      s->st));
         } else {
+            if (!s->capturing) P.spec_token = 0;
             const void* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
             CK(mlb::launch_conv(P.k, P.L[0], P.L[1], P.L[2], P.tw.p, sp, P.spec.p, P.ten6.p, P.ten9.p, sl.h, s->rb,
                                 s->st));
@@ -1130,13 +1175,18 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
     build_sum_terms(s, list, T, gen, dt_sys, s->capturing, th);
     if (gen != s->gen) {
         if (s->capturing) fail(MLB_ESTATE, "step is not fusable");
+        flush_pending(s);
         return false;
     }
     if (th >= 0 && !th_in && s->slots[th].state == ST_DATA) {
-        if (!add_addend(T, s->slots[th].h, 0.0, true)) return false;
+        if (!add_addend(T, s->slots[th].h, 0.0, true)) {
+            flush_pending(s);
+            return false;
+        }
     }
     const int nb = 1 - s->cur;
     FastK F;
+    bool carried = false;   // SPEC ends holding the new spins' x transform
     if (s->dry) {
         // bookkeeping only: the kernels of this step ran in a captured graph
     } else if (fast_fused(s, T, l, dt, dt_sys, F)) {
@@ -1148,8 +1198,29 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
             out[c] = static_cast<float*>(s->sp[nb][c]);
             if (T.nadd == 1) ad[c] = static_cast<const float*>(T.add[0][c]);
         }
-        CK(mlb::launch_fused_fast(F, sp, ad, out, s->st));
+        ConvPlan* CP = s->pend_op ? s->pend_op->plan.get() : nullptr;
+        mlb_op* pend_op_was = s->pend_op;
+        if (CP && T.nadd == 1 && T.add[0][0] == s->slots[s->pend_si].h[0] && mlb::xstep_ok(CP->k, F)) {
+            float* h[3] = {static_cast<float*>(s->slots[s->pend_si].h[0]),
+                           static_cast<float*>(s->slots[s->pend_si].h[1]),
+                           static_cast<float*>(s->slots[s->pend_si].h[2])};
+            s->pend_op = nullptr;
+            s->pend_si = -1;
+            CK(mlb::launch_xstep(CP->k, CP->L, reinterpret_cast<const float2*>(CP->tw.p),
+                                 reinterpret_cast<float2*>(CP->spec.p), F, true, sp, h, out, s->st));
+            carried = true;
+            if (s->capturing) {
+                s->cap_xstep = pend_op_was;
+            } else {
+                CP->spec_token = ++g_spec_token;
+                s->spec_token = CP->spec_token;
+            }
+        } else {
+            flush_pending(s);
+            CK(mlb::launch_fused_fast(F, sp, ad, out, s->st));
+        }
     } else {
+        flush_pending(s);
         FusedK P;
         P.sys = sysk(s, s->cur);
         P.terms = T;
@@ -1158,6 +1229,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         CK(mlb::launch_fused(P, dt_sys, s->rb, s->st));
     }
     if (s->capturing) CK(mlb::launch_advance_step(s->dstep, s->st));
+    if (!carried && !s->capturing && !s->dry) s->spec_token = 0;
     s->cur = nb;
     s->gen++;
     return true;
@@ -1175,7 +1247,11 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
     if (from == dmdt && dmdt == to) done = llg_fused(l, from, dt);
     from->last_fused = done;
     if (!done) {
+        flush_pending(from);
+        if (dmdt != from) flush_pending(dmdt);
+        if (to != from && to != dmdt) flush_pending(to);
         if (from->capturing) fail(MLB_ESTATE, "step is not fusable");
+        to->spec_token = 0;
         materialize(dmdt, 0);
         const int th = slot_find(dmdt, "Thermal");
         if (th >= 0) materialize(dmdt, th);
@@ -1232,7 +1308,9 @@ void reset_fields(mlb_system* s)
 void spins_changing(mlb_system* s)
 {
     // lazy records read the current buffer, which is about to change
+    flush_pending(s);
     materialize_all(s);
+    s->spec_token = 0;
 }
 
 mlb_system* make_system(int nx, int ny, int nz, int rb)
@@ -1298,12 +1376,29 @@ void upload_site_array(mlb_system* s, void** dst, const double* a)
     CK(cudaStreamSynchronize(s->st));
 }
 
+// The canonical script step.  Nothing outside runs between its calls, so the
+// inverse x pass of a fast-path convolution may wait for the LLG update
+// (defer_x) and run fused with it.
 void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
 {
     reset_fields(s);
-    for (int i = 0; i < nops; i++) op_apply(ops[i], s);
-    sum_fields(s);
-    llg_apply(l, s, 1.0, s, s, 1);
+    s->defer_x = !s->sur;
+    try {
+        for (int i = 0; i < nops; i++) op_apply(ops[i], s);
+        sum_fields(s);
+        llg_apply(l, s, 1.0, s, s, 1);
+    } catch (...) {
+        s->defer_x = false;
+        try {
+            flush_pending(s);
+        } catch (...) {
+            s->pend_op = nullptr;
+            s->pend_si = -1;
+        }
+        throw;
+    }
+    s->defer_x = false;
+    flush_pending(s);
     if (s->sur && !s->dry) sur_advance(s);
 }
 
@@ -1361,7 +1456,7 @@ void load_state(mlb_system* s, const std::vector<mlb_op*>& ops, const HostState&
 
 void plan_release(mlb_plan* p)
 {
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < 4; q++) {
         if (p->exec[q]) cudaGraphExecDestroy(p->exec[q]);
         p->exec[q] = nullptr;
         for (ProfCaptured& r : p->ev[q]) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
@@ -1393,11 +1488,15 @@ void plan_capture(mlb_plan* p)
         if (!s->last_fused) fail(MLB_ESTATE, "step is not fusable");
         load_state(s, p->ops, h0);
         CK(cudaStreamSynchronize(s->st));
-        for (int q = 0; q < 2; q++) {
-            s->cur = q;
+        p->carry_op = nullptr;
+        for (int q = 0; q < 4; q++) {
+            if (q >= 2 && !p->carry_op) break;   // no fused x pass: no carried variant
+            s->cur = q & 1;
+            s->cap_carry = q >= 2;
             cudaGraph_t graph = nullptr;
             CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
             s->capturing = true;
+            s->cap_xstep = nullptr;
             if (p->timing) mlb::prof_set_capture_sink(&p->ev[q]);
             bool ok = true;
             std::string why;
@@ -1409,6 +1508,12 @@ void plan_capture(mlb_plan* p)
             }
             mlb::prof_set_capture_sink(nullptr);
             s->capturing = false;
+            s->cap_carry = false;
+            if (q < 2) {
+                // the carried variants exist only when both parities end in the fused x pass
+                if (q == 0) p->carry_op = s->cap_xstep;
+                else if (p->carry_op != s->cap_xstep) p->carry_op = nullptr;
+            }
             cudaError_t e = cudaStreamEndCapture(s->st, &graph);
             if (!ok || e != cudaSuccess) {
                 if (graph) cudaGraphDestroy(graph);
@@ -1423,6 +1528,7 @@ void plan_capture(mlb_plan* p)
     } catch (...) {
         s->dry = false;
         s->capturing = false;
+        s->cap_carry = false;
         mlb::prof_set_capture_sink(nullptr);
         load_state(s, p->ops, h0);
         throw;
@@ -1457,9 +1563,17 @@ void plan_launch(mlb_plan* p, int nsteps)
             for (int a = 0; a < 3; a++) { h.B[a] = o->B[a] * o->gs; h.dB[a] = o->dB[a] * o->gs; }
     }
     CK(cudaMemcpyAsync(s->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
+    ConvPlan* CP = p->carry_op ? p->carry_op->plan.get() : nullptr;
     for (int k = 0; k < nsteps; k++) {
-        CK(cudaGraphLaunch(p->exec[s->cur], s->st));
-        p->last = &p->ev[s->cur];
+        const bool carry = CP && s->spec_token != 0 && s->spec_token == CP->spec_token;
+        const int gi = s->cur + (carry ? 2 : 0);
+        CK(cudaGraphLaunch(p->exec[gi], s->st));
+        p->last = &p->ev[gi];
+        if (CP) {
+            // the step's fused x pass left SPEC holding the new spins' transform
+            CP->spec_token = ++g_spec_token;
+            s->spec_token = CP->spec_token;
+        }
         if (k < nsteps - 1) {
             advance_host(p);
             advance_sweep(p->ops.data(), (int)p->ops.size());
@@ -3009,6 +3123,7 @@ bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl)
     sur_forward(S, a, b, 0, h0, out, d, &d->exact, ratio, s->st);
     // exact passes, run only when the schedule or the residual check asks
     ConvPlan& P = *op->plan;
+    if (!s->capturing) P.spec_token = 0;
     ConvK kk = P.k;
     kk.run_if = &d->exact;
     if (mlb::conv_fast_ok(kk)) {

@@ -295,12 +295,13 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const fl
 // its lattice of NX x NY x NZ sites and i its index in the (packed) arrays;
 // neighbours are addressed relative to i, so several lattices can share the
 // arrays back to back.
+// The new spin of the site is returned in (rx, ry, rz); (Ax, Ay, Az) is the
+// materialised addend (the dipole slot), used when ADD.
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
-                                           const float* __restrict__ sx, const float* __restrict__ sy,
-                                           const float* __restrict__ sz, const float* __restrict__ ax,
-                                           const float* __restrict__ ay, const float* __restrict__ az,
-                                           float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz)
+__device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                             const float* __restrict__ sx, const float* __restrict__ sy,
+                                             const float* __restrict__ sz, float Ax, float Ay, float Az, float& rx,
+                                             float& ry, float& rz)
 {
     const int nxy = NX * NY;
     const float Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
@@ -339,7 +340,7 @@ __device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int N
         Hx += Tx; Hy += Ty; Hz += Tz;
     }
     if (ADD) {
-        Hx += F.addw * __ldg(ax + i); Hy += F.addw * __ldg(ay + i); Hz += F.addw * __ldg(az + i);
+        Hx += F.addw * Ax; Hy += F.addw * Ay; Hz += F.addw * Az;
     }
     float nx_, ny_, nz_;
     if (LT == LLG_CART) {
@@ -398,7 +399,21 @@ __device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int N
             nx_ *= inv; ny_ *= inv; nz_ *= inv;
         }
     }
-    ox[i] = nx_; oy[i] = ny_; oz[i] = nz_;
+    rx = nx_; ry = ny_; rz = nz_;
+}
+
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
+__device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                           const float* __restrict__ sx, const float* __restrict__ sy,
+                                           const float* __restrict__ sz, const float* __restrict__ ax,
+                                           const float* __restrict__ ay, const float* __restrict__ az,
+                                           float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz)
+{
+    float Ax = 0.f, Ay = 0.f, Az = 0.f;
+    if (ADD) { Ax = __ldg(ax + i); Ay = __ldg(ay + i); Az = __ldg(az + i); }
+    float rx, ry, rz;
+    fused_site_v<LT, EXS, ANI, TH, ADD>(F, NX, NY, NZ, x, y, z, i, sx, sy, sz, Ax, Ay, Az, rx, ry, rz);
+    ox[i] = rx; oy[i] = ry; oz[i] = rz;
 }
 
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
@@ -414,6 +429,138 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
     if (x >= F.nx || y >= F.ny) return;
     const int i = x + F.nx * (y + F.ny * z);
     fused_site<LT, EXS, ANI, TH, ADD>(F, F.nx, F.ny, F.nz, x, y, z, i, sx, sy, sz, ax, ay, az, ox, oy, oz);
+}
+
+// ------------------------------------------------------------------ fused x pass of a step
+// One CTA owns ROWS consecutive rows (y0 .. y0 + ROWS - 1) of one layer z, all
+// three components, and runs on them, in shared memory:
+//   1. the inverse x transform of the (y,z)-pass output (two rows per
+//      complex line, Hermitian completion) -> the dipole field of the rows,
+//      written to its slot;
+//   2. the fused field terms + LLG update of the rows' sites with that field
+//      as the addend -> the new spins (exchange neighbours read from the
+//      current spin arrays, which no CTA writes);
+//   3. (fwd) the forward x transform of the new spins (two rows per complex
+//      line, split) -> the spectrum rows of the next step.
+// The spectrum rows a CTA reads in 1 and writes in 3 are its own.  Every
+// arithmetic step repeats k_ix_fast, fused_site and k_fx_fast operation for
+// operation, so the result is bitwise that of the three separate kernels.
+template <int PX>
+struct XSCfg {
+    static constexpr int NT = 384;
+    static constexpr int TPL = fr::Tpl<PX>::V;
+    static constexpr int L = NT / TPL;                 // complex lines = 3 ROWS / 2
+    static constexpr int ROWS = 2 * L / 3;
+    static constexpr int R2 = ROWS / 2;
+    static constexpr int KX = PX / 2 + 1;
+    static constexpr int LINE = L * PX;
+    static constexpr int SPEC = 3 * ROWS * KX;
+    static constexpr int BUF = LINE > SPEC ? LINE : SPEC;
+    static constexpr int SMEM = (PX + 2 * BUF) * 8;
+    static_assert(L % 3 == 0 && ROWS % 2 == 0, "line layout");
+};
+
+template <int PX, int LT, bool EXS, bool ANI, bool TH>
+__global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, const float2* __restrict__ tw,
+                                                  float2* __restrict__ spec, const float* __restrict__ sx,
+                                                  const float* __restrict__ sy, const float* __restrict__ sz,
+                                                  float* __restrict__ hx, float* __restrict__ hy,
+                                                  float* __restrict__ hz, float* __restrict__ ox,
+                                                  float* __restrict__ oy, float* __restrict__ oz)
+{
+    using X = XSCfg<PX>;
+    constexpr int KX = X::KX, NT = X::NT, ROWS = X::ROWS, R2 = X::R2;
+    extern __shared__ float2 sm[];
+    float2* twl = sm;               // [PX]
+    float2* A = twl + PX;           // [L][PX] lines
+    float2* B = A + X::BUF;         // [3][ROWS][KX] spectra, then scratch
+    const int zz = blockIdx.y;
+    const int row0 = blockIdx.x * ROWS;
+    const int rows_here = min(ROWS, c.ny - row0);
+    const int nx = c.nx, ny = c.ny, nz = c.nz;
+    for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
+    // 1. spectrum rows SPEC[kx][comp][zz][row0 + row] -> B[(comp ROWS + row) KX + kx]
+    constexpr int IS = (X::SPEC + NT - 1) / NT;
+    {
+        float2 v[IS];
+#pragma unroll
+        for (int it = 0; it < IS; it++) {
+            const int idx = threadIdx.x + it * NT;
+            const int kx = idx / (3 * ROWS), rem = idx % (3 * ROWS);
+            const int comp = rem / ROWS, row = rem % ROWS;
+            v[it] = make_float2(0.f, 0.f);
+            if (idx < X::SPEC && row < rows_here)
+                v[it] = spec[(((size_t)kx * 3 + comp) * nz + zz) * ny + row0 + row];
+        }
+#pragma unroll
+        for (int it = 0; it < IS; it++) {
+            const int idx = threadIdx.x + it * NT;
+            const int kx = idx / (3 * ROWS), rem = idx % (3 * ROWS);
+            if (idx < X::SPEC) B[rem * KX + kx] = v[it];
+        }
+    }
+    __syncthreads();
+    // line l = comp R2 + p: Z[k] = S_row(2p)[k] + i S_row(2p+1)[k], Hermitian completion
+    constexpr int IL = (X::LINE + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < IL; it++) {
+        const int idx = threadIdx.x + it * NT;
+        if (idx >= X::LINE) continue;
+        const int l = idx / PX, k = idx % PX;
+        const int comp = l / R2, p = l % R2;
+        const float2* Sa = B + (comp * ROWS + 2 * p) * KX;
+        const float2* Sb = Sa + KX;
+        float2 a, b;
+        if (k < KX) { a = Sa[k]; b = Sb[k]; }
+        else { a = cconj(Sa[PX - k]); b = cconj(Sb[PX - k]); }
+        A[idx] = make_float2(a.x - b.y, a.y + b.x);
+    }
+    __syncthreads();
+    const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
+    const float2* R = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
+    float2* W = (R == A) ? B : A;   // free buffer: the new spins' lines (FWD)
+    const float* Rf = reinterpret_cast<const float*>(R);
+    float* Wf = reinterpret_cast<float*>(W);
+    // 2. field of the rows to the slot, then the step of every site
+    const size_t layer = (size_t)zz * ny * nx;
+    constexpr int IO = (ROWS * PX + NT - 1) / NT;
+#pragma unroll 1
+    for (int it = 0; it < IO; it++) {
+        const int idx = threadIdx.x + it * NT;
+        const int row = idx / PX, x = idx % PX;
+        const int fo = 2 * (((row >> 1)) * PX + x) + (row & 1);   // float offset of (row, x) in component 0's lines
+        const bool live = idx < ROWS * PX && row < rows_here && x < nx;
+        float rx = 0.f, ry = 0.f, rz = 0.f;
+        if (live) {
+            const float Ax = Rf[fo], Ay = Rf[fo + 2 * R2 * PX], Az = Rf[fo + 4 * R2 * PX];
+            const int y = row0 + row;
+            const size_t i = layer + (size_t)y * nx + x;
+            hx[i] = Ax; hy[i] = Ay; hz[i] = Az;
+            fused_site_v<LT, EXS, ANI, TH, true>(F, nx, ny, nz, x, y, zz, (int)i, sx, sy, sz, Ax, Ay, Az, rx, ry, rz);
+            ox[i] = rx; oy[i] = ry; oz[i] = rz;
+        }
+        if (fwd && idx < ROWS * PX) {
+            Wf[fo] = rx; Wf[fo + 2 * R2 * PX] = ry; Wf[fo + 4 * R2 * PX] = rz;
+        }
+    }
+    if (!fwd) return;
+    __syncthreads();
+    // 3. forward transform of the new spins' lines, split into the two rows
+    const float2* Q = fr::sm_fft<PX, -1, X::TPL>(W, const_cast<float2*>(R), l, tl, twl, true);
+    constexpr int IQ = (X::SPEC + NT - 1) / NT;
+#pragma unroll
+    for (int it = 0; it < IQ; it++) {
+        const int idx = threadIdx.x + it * NT;
+        const int kx = idx / (3 * ROWS), rem = idx % (3 * ROWS);
+        const int comp = rem / ROWS, row = rem % ROWS;
+        if (idx >= X::SPEC || row >= rows_here) continue;
+        const float2* Z = Q + (comp * R2 + (row >> 1)) * PX;
+        const float2 zk = Z[kx], zn = Z[(PX - kx) & (PX - 1)];
+        float2 o;
+        if ((row & 1) == 0) o = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+        else o = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+        spec[(((size_t)kx * 3 + comp) * nz + zz) * ny + row0 + row] = o;
+    }
 }
 
 // Packed ensemble: block b covers sites [bstart[b], bstart[b] + blockDim) of
@@ -568,6 +715,9 @@ static cudaError_t cfg_yz()
     return cudaFuncSetAttribute(k_yz_fast<PY, 32>, a, 227 * 1024);
 }
 
+template <int PX>
+static cudaError_t cfg_xs();
+
 cudaError_t conv_fast_configure()
 {
     cudaError_t e;
@@ -576,6 +726,8 @@ cudaError_t conv_fast_configure()
         return e;
     if ((e = cfg_yz<16>()) || (e = cfg_yz<32>()) || (e = cfg_yz<64>()) || (e = cfg_yz<128>()) || (e = cfg_yz<256>()) ||
         (e = cfg_yz<512>()))
+        return e;
+    if ((e = cfg_xs<32>()) || (e = cfg_xs<64>()) || (e = cfg_xs<128>()) || (e = cfg_xs<256>()) || (e = cfg_xs<512>()))
         return e;
     return cudaSuccess;
 }
@@ -599,6 +751,95 @@ cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw
         e = launch_x_any(c, tw + L[0].tw_off, s, spec, h, st, false);
     }
     return e;
+}
+
+// ------------------------------------------------------------------ fused x pass dispatch
+cudaError_t launch_conv_fast_fyz(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
+                                 const float* ten6, bool with_fx, cudaStream_t st)
+{
+    cudaError_t e = cudaSuccess;
+    if (with_fx) {
+        Prof pf("k_conv_fx", st);
+        e = launch_x_any(c, tw + L[0].tw_off, s, spec, nullptr, st, true);
+    }
+    if (e != cudaSuccess) return e;
+    Prof pf("k_conv_yz", st);
+    return launch_yz_any(c, tw + L[1].tw_off, spec, ten6, st);
+}
+
+cudaError_t launch_conv_fast_ix(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, float* h[3],
+                                cudaStream_t st)
+{
+    Prof pf("k_conv_ix", st);
+    return launch_x_any(c, tw + L[0].tw_off, nullptr, spec, h, st, false);
+}
+
+bool xstep_ok(const ConvK& c, const FastK& F)
+{
+    return c.nrep == 1 && F.ex && (c.Px == 32 || c.Px == 64 || c.Px == 128 || c.Px == 256 || c.Px == 512);
+}
+
+template <int PX, int LT, bool ANI, bool TH>
+static void xstep_t(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec, const float* s[3],
+                    float* h[3], float* o[3], cudaStream_t st)
+{
+    using X = XSCfg<PX>;
+    dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 1);
+    k_xstep<PX, LT, true, ANI, TH><<<grid, X::NT, X::SMEM, st>>>(c, F, fwd, tw, spec, s[0], s[1], s[2], h[0], h[1],
+                                                               h[2], o[0], o[1], o[2]);
+}
+template <int PX, int LT>
+static void xstep_lt(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec, const float* s[3],
+                     float* h[3], float* o[3], cudaStream_t st)
+{
+    if (F.ani) {
+        if (F.th) xstep_t<PX, LT, true, true>(c, F, fwd, tw, spec, s, h, o, st);
+        else xstep_t<PX, LT, true, false>(c, F, fwd, tw, spec, s, h, o, st);
+    } else {
+        if (F.th) xstep_t<PX, LT, false, true>(c, F, fwd, tw, spec, s, h, o, st);
+        else xstep_t<PX, LT, false, false>(c, F, fwd, tw, spec, s, h, o, st);
+    }
+}
+template <int PX>
+static void xstep_px(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec, const float* s[3],
+                     float* h[3], float* o[3], cudaStream_t st)
+{
+    if (F.llg_type == LLG_CART) xstep_lt<PX, LLG_CART>(c, F, fwd, tw, spec, s, h, o, st);
+    else xstep_lt<PX, LLG_QUAT>(c, F, fwd, tw, spec, s, h, o, st);
+}
+
+cudaError_t launch_xstep(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const FastK& F,
+                         bool fwd, const float* s[3], float* h[3], float* o[3], cudaStream_t st)
+{
+    Prof pf(fwd ? "k_xstep" : "k_xstep_ix", st);
+    const float2* t = tw + L[0].tw_off;
+    switch (c.Px) {
+    case 32: xstep_px<32>(c, F, fwd, t, spec, s, h, o, st); break;
+    case 64: xstep_px<64>(c, F, fwd, t, spec, s, h, o, st); break;
+    case 128: xstep_px<128>(c, F, fwd, t, spec, s, h, o, st); break;
+    case 256: xstep_px<256>(c, F, fwd, t, spec, s, h, o, st); break;
+    case 512: xstep_px<512>(c, F, fwd, t, spec, s, h, o, st); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <int PX, int LT, bool ANI, bool TH>
+static cudaError_t cfg_xs1()
+{
+    return cudaFuncSetAttribute(k_xstep<PX, LT, true, ANI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                XSCfg<PX>::SMEM);
+}
+template <int PX>
+static cudaError_t cfg_xs()
+{
+    cudaError_t e;
+    if ((e = cfg_xs1<PX, LLG_CART, false, false>()) || (e = cfg_xs1<PX, LLG_CART, false, true>()) ||
+        (e = cfg_xs1<PX, LLG_CART, true, false>()) || (e = cfg_xs1<PX, LLG_CART, true, true>()) ||
+        (e = cfg_xs1<PX, LLG_QUAT, false, false>()) || (e = cfg_xs1<PX, LLG_QUAT, false, true>()) ||
+        (e = cfg_xs1<PX, LLG_QUAT, true, false>()) || (e = cfg_xs1<PX, LLG_QUAT, true, true>()))
+        return e;
+    return cudaSuccess;
 }
 
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>

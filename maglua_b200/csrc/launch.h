@@ -44,6 +44,16 @@ cudaError_t conv_fast_configure();
 bool conv_fast_ok(const ConvK& c);
 cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                              const float* ten6, float* h[3], cudaStream_t st);
+// The (y,z) pass, optionally preceded by the forward x pass, without the
+// inverse x pass: the fused x pass (launch_xstep) completes the step.
+cudaError_t launch_conv_fast_fyz(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
+                                 const float* ten6, bool with_fx, cudaStream_t st);
+cudaError_t launch_conv_fast_ix(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, float* h[3],
+                                cudaStream_t st);
+bool xstep_ok(const ConvK& c, const FastK& F);
+// Inverse x pass + fused step (+ forward x pass of the new spins when fwd).
+cudaError_t launch_xstep(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const FastK& F,
+                         bool fwd, const float* s[3], float* h[3], float* o[3], cudaStream_t st);
 cudaError_t launch_fused_fast(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st);
 cudaError_t launch_fused_ens(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3],
                              cudaStream_t st);

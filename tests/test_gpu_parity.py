@@ -556,7 +556,8 @@ def test_plan_matches_calls_and_recaptures(M):
             th.setTemperature(0.6)      # changes the captured constants: recapture
             plan.launch(4)
             kt = plan.kernelTimes()
-            assert "k_fused_step" in kt and all(v > 0 for v in kt.values())
+            # the fused x pass: (y,z) pass + one kernel for inverse x, step, forward x
+            assert "k_xstep" in kt and "k_conv_yz" in kt and all(v > 0 for v in kt.values())
         res.append(np.stack(ss.spinArrays()[:3]))
         res.append(np.stack(ss.fieldArrays("Total")))
         res.append(ss.time())

@@ -1,0 +1,181 @@
+"""The fused x pass of a step (inverse x transform of the dipole spectrum,
+field terms + LLG update, forward x transform of the new spins in one
+kernel) against the same step issued as the reference's individual calls
+(M/cpu/core/spinsystem_luafuncs.lua resetFields / op:apply / sumFields,
+M/cpu/llg/llg.cpp apply), which run the separate inverse-x, fused-step and
+forward-x kernels.  Both orders perform the same float operations, so the
+spins, the Total field and the Dipole slot must agree bitwise; so must every
+path that invalidates the spectrum carried from one step to the next
+(spins set from the host, an individual call in between, two systems
+sharing one Dipole operator)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import random_spins, tilted_spins
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    import maglua_b200 as M
+    M.init(0)
+    return M
+
+
+def build(M, dims, spins, llg="Quaternion", T=0.5, ani=True, open_xy=False, dip_op=None):
+    n = int(np.prod(dims))
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*spins)
+    ss.setAlpha(0.05)
+    ss.setTimeStep(0.005)
+    ex = M.Exchange(ss)
+    ex.addPaths(*O.nn_paths(*dims, pbc=(0, 0, 0) if open_xy else (1, 1, 0)))
+    ops = [ex]
+    if ani:
+        a = M.Anisotropy(ss)
+        a.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.05))
+        ops.append(a)
+    if T > 0:
+        th = M.Thermal(ss, M.Random.Philox(11))
+        th.setTemperature(T)
+        ops.append(th)
+    z = M.AppliedField(ss)
+    z.set(0.1, 0, 0.02)
+    ops.append(z)
+    dip = dip_op
+    if dip is None:
+        dip = M.Dipole(ss)
+        dip.setStrength(0.03)
+        if open_xy:
+            dip.setOpen(True, True, True)
+    ops.append(dip)
+    return ss, ops, M.LLG.new(llg)
+
+
+def calls(ss, ops, l, k):
+    for _ in range(k):
+        ss.resetFields()
+        for op in ops:
+            op.apply(ss)
+        ss.sumFields()
+        l.apply(ss)
+
+
+def state(ss):
+    return (np.stack(ss.spinArrays()[:3]), np.stack(ss.fieldArrays("Total")), np.stack(ss.fieldArrays("Dipole")))
+
+
+def assert_same(a, b):
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+CASES = [
+    # dims, llg, T, anisotropy, open in-plane
+    ((64, 20, 3), "Quaternion", 0.5, True, False),     # 20 rows: a partial row band
+    ((32, 16, 2), "Cartesian", 0.0, False, True),      # open x/y: padded x = 64
+    ((128, 16, 1), "Cartesian", 0.5, True, False),
+    ((256, 24, 2), "Quaternion", 0.0, True, False),
+    ((512, 8, 2), "Quaternion", 0.5, False, False),
+    ((96, 8, 2), "Quaternion", 0.5, True, False),      # x length without the fused pass
+]
+
+
+@pytest.mark.parametrize("dims,llg,T,ani,open_xy", CASES)
+def test_run_equals_calls_bitwise(M, dims, llg, T, ani, open_xy):
+    n = int(np.prod(dims))
+    s0 = random_spins(n, 41)
+    out = []
+    for mode in ("calls", "run", "plan"):
+        ss, ops, l = build(M, dims, s0, llg, T, ani, open_xy)
+        if mode == "calls":
+            calls(ss, ops, l, 7)
+        elif mode == "run":
+            M.run(ss, ops, l, 2)      # eager steps (below the capture threshold)
+            M.run(ss, ops, l, 5)      # captured steps
+        else:
+            p = M.Plan(ss, ops, l)
+            p.launch(3)
+            p.launch(4)
+        out.append(state(ss))
+    assert_same(out[0], out[1])
+    assert_same(out[0], out[2])
+
+
+def test_carried_spectrum_invalidated_by_host_writes(M):
+    dims = (64, 16, 2)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 42)
+    res = []
+    for mode in ("calls", "run"):
+        ss, ops, l = build(M, dims, s0)
+        step = (lambda k: calls(ss, ops, l, k)) if mode == "calls" else (lambda k: M.run(ss, ops, l, k))
+        step(4)
+        ss.setSpin((3, 5, 2), (0.6, 0.0, 0.8))
+        step(4)
+        x, y, z, _ = ss.spinArrays()
+        ss.setSpinArrays(z, x, y)
+        step(1)
+        step(3)
+        res.append(state(ss))
+    assert_same(res[0], res[1])
+
+
+def test_individual_calls_between_runs(M):
+    dims = (128, 8, 2)
+    n = int(np.prod(dims))
+    s0 = random_spins(n, 43)
+    res = []
+    for mode in ("calls", "mixed"):
+        ss, ops, l = build(M, dims, s0, llg="Cartesian")
+        if mode == "calls":
+            calls(ss, ops, l, 10)
+        else:
+            M.run(ss, ops, l, 4)
+            calls(ss, ops, l, 2)
+            p = M.Plan(ss, ops, l)
+            p.launch(3)
+            calls(ss, ops, l, 1)
+        res.append(state(ss))
+    assert_same(res[0], res[1])
+
+
+def test_two_systems_share_one_dipole(M):
+    dims = (64, 16, 2)
+    n = int(np.prod(dims))
+    sa, sb = random_spins(n, 44), tilted_spins(n, 45)
+    res = []
+    for mode in ("calls", "run"):
+        dip = M.Dipole(*dims)
+        dip.setStrength(0.03)
+        A = build(M, dims, sa, dip_op=dip)
+        B = build(M, dims, sb, dip_op=dip)
+        for k in range(3):
+            for ss, ops, l in (A, B):
+                if mode == "calls":
+                    calls(ss, ops, l, 3)
+                else:
+                    M.run(ss, ops, l, 3)
+        res.append(state(A[0]) + state(B[0]))
+    assert_same(res[0], res[1])
+
+
+def test_run_matches_oracle(M):
+    """The fused pass against the FP64 oracle (T = 0, 30 steps)."""
+    dims = (64, 24, 2)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 46, deg=20.0)
+    ss, ops, l = build(M, dims, s0, llg="Quaternion", T=0.0)
+    M.run(ss, ops, l, 30)
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s0)
+    o.alpha, o.dt = 0.05, 0.005
+    f, t, j = O.nn_paths(*dims, pbc=(1, 1, 0))
+    sites = np.arange(n, dtype=np.int32)
+    lr = O.LongRange(*dims, O.dipole_tensor(*dims))
+    O.run_steps(o, 30, paths=(f, t, j), ani=(sites, np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.05)),
+                B=(0.1, 0, 0.02), lr=lr, g=0.03, llg="Quaternion")
+    err = float(np.abs(np.stack(ss.spinArrays()[:3]) - o.spins()).max())
+    assert err < 2e-6, err
