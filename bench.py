@@ -312,28 +312,26 @@ def main():
 
     # warm-up (tensor setup, graph capture)
     M.run(ss, ops, llg, args.warmup)
-    plan = M.Plan(ss, ops, llg, timing=True)
-    plan.launch(2)
+    plan_nt = M.Plan(ss, ops, llg, timing=False)
+    plan_nt.launch(2)
     ss.synchronize()
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.zero_()          # write 1 GiB (> L2)
+            sweep.sum()            # read 512 MiB: evicts the dirty flush lines
 
     # timed region: one captured step per launch, per-step events, L2 flush
     # (write then read sweep) before every step, outside the events
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kern_ms = {}
-    kern_n = {}
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
     for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()          # write 1 GiB (> L2)
-            sweep.sum()            # read 512 MiB: evicts the dirty flush lines
+        flush_l2()
         evs[k][0].record(stream)
-        plan.launch(1)
+        plan_nt.launch(1)
         evs[k][1].record(stream)
-        for nm, ms in plan.kernelTimes().items():
-            kern_ms[nm] = kern_ms.get(nm, 0.0) + ms
-            kern_n[nm] = kern_n.get(nm, 0) + 1
     ss.synchronize()
     barrier()
     clk = clocks.stop()
@@ -345,10 +343,23 @@ def main():
         total_ms = float(t.item())
     value = world * n * args.steps / (total_ms * 1e-3)
 
+    # per-kernel times: the same step captured with event nodes around each
+    # kernel (the nodes add a little time of their own), same flushes
+    plan = M.Plan(ss, ops, llg, timing=True)
+    plan.launch(2)
+    kern_ms = {}
+    kern_n = {}
+    ksteps = min(args.steps, 200)
+    for k in range(ksteps):
+        flush_l2()
+        plan.launch(1)
+        for nm, ms in plan.kernelTimes().items():
+            kern_ms[nm] = kern_ms.get(nm, 0.0) + ms
+            kern_n[nm] = kern_n.get(nm, 0) + 1
+    ss.synchronize()
+
     # steady state without flushes (L2-resident state), same plan
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    plan_nt = M.Plan(ss, ops, llg, timing=False)
-    plan_nt.launch(2)
     barrier()
     e0.record(stream)
     plan_nt.launch(args.steps)
@@ -407,9 +418,9 @@ def main():
     cpu = None
     if not args.no_cpu and world == 1:
         cpu = cpu_baseline(procs=1, target_s=15.0)
-    # our kernels in the timed region: the step kernels plus one step-block
-    # advance per step
-    launches = sum(kern_n.values()) + args.steps
+    # our kernels in the timed region: the step kernels (counted per step in
+    # the timing pass) plus one step-block advance per step
+    launches = int(round(sum(kern_n.values()) / ksteps * args.steps)) + args.steps
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

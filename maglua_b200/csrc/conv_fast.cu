@@ -62,6 +62,8 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
                                                  const float* __restrict__ sy, const float* __restrict__ sz,
                                                  float2* __restrict__ spec)
 {
+    pdl_trigger();
+    pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
     using X = XCfg<PX>;
     constexpr int NT = X::NT;
@@ -119,6 +121,8 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
                                                  float* __restrict__ hx, float* __restrict__ hy,
                                                  float* __restrict__ hz)
 {
+    pdl_trigger();
+    pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
     using X = XCfg<PX>;
     constexpr int KX = X::KX, NT = X::NT;
@@ -194,7 +198,6 @@ template <int PY, int PZ>
 __global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
                                                                float2* __restrict__ spec, const float* __restrict__ ten6)
 {
-    if (c.run_if && *c.run_if == 0) return;
     constexpr int NT = YZT<PY, PZ>::N;
     constexpr int TPL = fr::Tpl<PY>::V;
     constexpr int LPR = NT / TPL;    // lines per round
@@ -208,6 +211,8 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const fl
     float2* Q = Pb + (size_t)nlines * PY;    // [3][PZ][PY]
     float2* twl = Q + (size_t)3 * PZ * PY;   // [PY]
     const float* Tk = ten6 + (size_t)kx * PZ * PY * 6;
+    // the tensor and twiddles are constants of the plan: fetch them while
+    // the previous kernel finishes
     if (threadIdx.x == 0) {
         // pull this kx's tensor chunk into L2 while the y transforms run
         const unsigned bytes = (unsigned)(PZ * PY * 6 * sizeof(float));
@@ -215,6 +220,9 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const fl
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tk), "r"(bytes) : "memory");
     }
     for (int k = threadIdx.x; k < PY; k += blockDim.x) twl[k] = twy[k];
+    pdl_trigger();
+    pdl_wait();
+    if (c.run_if && *c.run_if == 0) return;
     float2* sp = spec + (size_t)kx * nlines * ny;
     {
         // at most 3*PZ*PY elements (nz <= PZ): unrolled gather, then store
@@ -479,6 +487,8 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
     const int rows_here = min(ROWS, c.ny - row0);
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
+    pdl_trigger();
+    pdl_wait();
     // 1. spectrum rows SPEC[kx][comp][zz][row0 + row] -> B[(comp ROWS + row) KX + kx]
     constexpr int IS = (X::SPEC + NT - 1) / NT;
     {
@@ -637,9 +647,9 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
     dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3 * c.nrep);
     const size_t smem = X::SMEM;
     if (fwd) {
-        k_fx_fast<PX><<<grid, 256, smem, st>>>(c, tw, s[0], s[1], s[2], spec);
+        return launch_pdl(k_fx_fast<PX>, grid, dim3(256), smem, st, c, tw, s[0], s[1], s[2], spec);
     } else {
-        k_ix_fast<PX><<<grid, 256, smem, st>>>(c, tw, spec, h[0], h[1], h[2]);
+        return launch_pdl(k_ix_fast<PX>, grid, dim3(256), smem, st, c, tw, spec, h[0], h[1], h[2]);
     }
     return cudaGetLastError();
 }
@@ -662,8 +672,7 @@ template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
     const size_t smem = yz_fast_smem(PY, PZ, c.nz);
-    k_yz_fast<PY, PZ><<<dim3(c.Kx, c.nrep), YZT<PY, PZ>::N, smem, st>>>(c, twy, spec, ten6);
-    return cudaGetLastError();
+    return launch_pdl(k_yz_fast<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZT<PY, PZ>::N), smem, st, c, twy, spec, ten6);
 }
 
 template <int PY>
@@ -698,9 +707,13 @@ static cudaError_t launch_yz_any(const ConvK& c, const float2* twy, float2* spec
 template <int PX>
 static cudaError_t cfg_x()
 {
+    const cudaFuncAttribute co = cudaFuncAttributePreferredSharedMemoryCarveout;
+    const int mx = (int)cudaSharedmemCarveoutMaxShared;
     cudaError_t e = cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess || (e = cudaFuncSetAttribute(k_fx_fast<PX>, co, mx)) != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    return cudaFuncSetAttribute(k_ix_fast<PX>, co, mx);
 }
 template <int PY>
 static cudaError_t cfg_yz()
@@ -780,32 +793,31 @@ bool xstep_ok(const ConvK& c, const FastK& F)
 }
 
 template <int PX, int LT, bool ANI, bool TH>
-static void xstep_t(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec, const float* s[3],
-                    float* h[3], float* o[3], cudaStream_t st)
+static cudaError_t xstep_t(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec,
+                           const float* s[3], float* h[3], float* o[3], cudaStream_t st)
 {
     using X = XSCfg<PX>;
     dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 1);
-    k_xstep<PX, LT, true, ANI, TH><<<grid, X::NT, X::SMEM, st>>>(c, F, fwd, tw, spec, s[0], s[1], s[2], h[0], h[1],
-                                                               h[2], o[0], o[1], o[2]);
+    return launch_pdl(k_xstep<PX, LT, true, ANI, TH>, grid, dim3(X::NT), (size_t)X::SMEM, st, c, F, fwd, tw, spec,
+                      s[0], s[1], s[2], h[0], h[1], h[2], o[0], o[1], o[2]);
 }
 template <int PX, int LT>
-static void xstep_lt(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec, const float* s[3],
-                     float* h[3], float* o[3], cudaStream_t st)
+static cudaError_t xstep_lt(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec,
+                            const float* s[3], float* h[3], float* o[3], cudaStream_t st)
 {
     if (F.ani) {
-        if (F.th) xstep_t<PX, LT, true, true>(c, F, fwd, tw, spec, s, h, o, st);
-        else xstep_t<PX, LT, true, false>(c, F, fwd, tw, spec, s, h, o, st);
-    } else {
-        if (F.th) xstep_t<PX, LT, false, true>(c, F, fwd, tw, spec, s, h, o, st);
-        else xstep_t<PX, LT, false, false>(c, F, fwd, tw, spec, s, h, o, st);
+        if (F.th) return xstep_t<PX, LT, true, true>(c, F, fwd, tw, spec, s, h, o, st);
+        return xstep_t<PX, LT, true, false>(c, F, fwd, tw, spec, s, h, o, st);
     }
+    if (F.th) return xstep_t<PX, LT, false, true>(c, F, fwd, tw, spec, s, h, o, st);
+    return xstep_t<PX, LT, false, false>(c, F, fwd, tw, spec, s, h, o, st);
 }
 template <int PX>
-static void xstep_px(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec, const float* s[3],
-                     float* h[3], float* o[3], cudaStream_t st)
+static cudaError_t xstep_px(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec,
+                            const float* s[3], float* h[3], float* o[3], cudaStream_t st)
 {
-    if (F.llg_type == LLG_CART) xstep_lt<PX, LLG_CART>(c, F, fwd, tw, spec, s, h, o, st);
-    else xstep_lt<PX, LLG_QUAT>(c, F, fwd, tw, spec, s, h, o, st);
+    if (F.llg_type == LLG_CART) return xstep_lt<PX, LLG_CART>(c, F, fwd, tw, spec, s, h, o, st);
+    return xstep_lt<PX, LLG_QUAT>(c, F, fwd, tw, spec, s, h, o, st);
 }
 
 cudaError_t launch_xstep(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const FastK& F,
@@ -814,21 +826,23 @@ cudaError_t launch_xstep(const ConvK& c, const FftLen L[3], const float2* tw, fl
     Prof pf(fwd ? "k_xstep" : "k_xstep_ix", st);
     const float2* t = tw + L[0].tw_off;
     switch (c.Px) {
-    case 32: xstep_px<32>(c, F, fwd, t, spec, s, h, o, st); break;
-    case 64: xstep_px<64>(c, F, fwd, t, spec, s, h, o, st); break;
-    case 128: xstep_px<128>(c, F, fwd, t, spec, s, h, o, st); break;
-    case 256: xstep_px<256>(c, F, fwd, t, spec, s, h, o, st); break;
-    case 512: xstep_px<512>(c, F, fwd, t, spec, s, h, o, st); break;
-    default: return cudaErrorInvalidValue;
+    case 32: return xstep_px<32>(c, F, fwd, t, spec, s, h, o, st);
+    case 64: return xstep_px<64>(c, F, fwd, t, spec, s, h, o, st);
+    case 128: return xstep_px<128>(c, F, fwd, t, spec, s, h, o, st);
+    case 256: return xstep_px<256>(c, F, fwd, t, spec, s, h, o, st);
+    case 512: return xstep_px<512>(c, F, fwd, t, spec, s, h, o, st);
     }
-    return cudaGetLastError();
+    return cudaErrorInvalidValue;
 }
 
 template <int PX, int LT, bool ANI, bool TH>
 static cudaError_t cfg_xs1()
 {
-    return cudaFuncSetAttribute(k_xstep<PX, LT, true, ANI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                XSCfg<PX>::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_xstep<PX, LT, true, ANI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         XSCfg<PX>::SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_xstep<PX, LT, true, ANI, TH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared);
 }
 template <int PX>
 static cudaError_t cfg_xs()

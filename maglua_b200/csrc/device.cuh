@@ -9,6 +9,15 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Programmatic dependent launch (kernels launched with launch_pdl): a kernel
+// may be scheduled while the previous kernel of its stream finishes.
+// pdl_wait() returns once that kernel has completed and its writes are
+// visible; nothing a predecessor writes may be read before it.
+// pdl_trigger() lets the next kernel be scheduled.  Both are no-ops for a
+// kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 #ifndef MLB_HD
 #define MLB_HD __host__ __device__ __forceinline__
 #endif

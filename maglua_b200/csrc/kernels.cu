@@ -385,6 +385,7 @@ __global__ void __launch_bounds__(256) k_llg(SysK from, const void* mx, const vo
 // One step of the device step block: next Thermal counter, swept field.
 __global__ void k_advance_step(DevStep* d)
 {
+    pdl_wait();   // the step's kernels read d until they complete
     d->th_counter += 1ull;
     for (int a = 0; a < 3; a++) d->B[a] += d->dB[a];
 }
@@ -905,8 +906,7 @@ cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* con
 
 cudaError_t launch_advance_step(DevStep* d, cudaStream_t st)
 {
-    k_advance_step<<<1, 1, 0, st>>>(d);
-    return cudaGetLastError();
+    return launch_pdl(k_advance_step, dim3(1), dim3(1), 0, st, d);
 }
 
 cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st)

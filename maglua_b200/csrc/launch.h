@@ -9,6 +9,27 @@
 #include <vector>
 
 namespace mlb {
+// Launch with programmatic stream serialization: the kernel's CTAs may be
+// scheduled before the previous kernel of the stream has finished (they
+// wait in pdl_wait()), which hides the launch latency between the kernels
+// of a step.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args)
+{
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg;
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // Kernel timing: 1 = eager profiling (mlb_profile_begin/end), 2 = event
 // nodes inside a graph being captured for a plan with timing, 0 = off.
 struct ProfCaptured {
