@@ -122,6 +122,74 @@ def run_batched(M, torch, steps, warmup):
             "l2": "working set larger than L2 (no flush)"}
 
 
+# ----------------------------------------------------------------- learned surrogate
+SUR_DIMS = (512, 512, 4)
+SUR_WORKLOAD = ("film 512x512x4, periodic x/y, open z (z padded to 8), J=1, K=0.02 z, g=0.05, T=0.1, "
+                "alpha=0.02, dt=0.005, LLG.Quaternion; spins from a seeded random start relaxed 200 steps; "
+                "surrogate: linear spectral-conv net (BF16 tcgen05, 16x16 modes, radius-2 stencil) trained "
+                "online on the plain method")
+
+
+def run_surrogate(M, torch, steps, flush_l2=None):
+    """Plain fused FFT path vs the learned surrogate on the 512x512x4 film:
+    spin-steps/s of both on the same system, and the surrogate's relative
+    dipolar-field error against the exact FFT field (the device FP32 field,
+    itself within 1e-5 of the FP64 oracle) at each exact-evaluation period k."""
+    import oracle as O  # noqa: F401  (nn_paths only: set-up, not timed)
+    dims = SUR_DIMS
+    n = int(np.prod(dims))
+    r = np.random.default_rng(1000)
+    v = r.normal(size=(3, n))
+    v /= np.linalg.norm(v, axis=0)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*v)
+    ss.setAlpha(0.02)
+    ss.setTimeStep(0.005)
+    ex = M.Exchange(ss)
+    ex.addPaths(*nn_paths(*dims))
+    ani = M.Anisotropy(ss)
+    ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.02))
+    th = M.Thermal(ss, M.Random.Philox(1000))
+    th.setTemperature(0.1)
+    dip = M.Dipole(ss)
+    dip.setStrength(0.05)
+    ops = [ex, ani, th, dip]
+    llg = M.LLG.new("Quaternion")
+    M.run(ss, ops, llg, 200)
+    st = torch.cuda.ExternalStream(ss.stream())
+
+    def timed(fn, k):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ss.synchronize()
+        a.record(st)
+        fn(k)
+        b.record(st)
+        ss.synchronize()
+        return a.elapsed_time(b) / k
+
+    plan = M.Plan(ss, ops, llg)
+    plan.launch(3)
+    plain_ms = timed(plan.launch, steps)
+    S = M.Surrogate(dip, (16, 16), 2)
+    t0 = time.perf_counter()
+    loss = S.train(ss, ops, llg, 1000, window=10, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    out = {"workload": SUR_WORKLOAD, "sites": n, "plain": {"value": n / (plain_ms * 1e-3), "ms_per_step": plain_ms},
+           "train": {"steps": 1000, "seconds": train_s, "final_rel_loss": loss}, "by_k": {}}
+    for k in (5, 10, 20):
+        val = S.validate(ss, ops, llg, 4 * k, window=k)
+        S.setSchedule(k, tol=1e-3)
+        S.run(ss, ops, llg, k)
+        ms = timed(lambda m: S.run(ss, ops, llg, m), max(steps, 10 * k))
+        st_ = S.stats()
+        out["by_k"][str(k)] = {"value": n / (ms * 1e-3), "ms_per_step": ms, "speedup_vs_plain": plain_ms / ms,
+                               "field_rel_err_mean": val["field_mean"], "field_rel_err_max": val["field_max"],
+                               "field_rel_err_without_net_mean": val["field_without_mean"],
+                               "exact": st_["exact"], "surrogate": st_["surrogate"], "failed_checks": st_["failed"]}
+    out["l2"] = "working set about 100 MB: L2-resident, no flush (both paths measured the same way)"
+    return out
+
+
 # ----------------------------------------------------------------- algorithmic bytes
 def algorithmic_bytes():
     """Per-launch algorithmic bytes of each kernel, split from the per
@@ -258,6 +326,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate comparison")
     ap.add_argument("--ncu-steps", type=int, default=0,
                     help="profiling driver: run this many eager steps of the workload and exit (for ncu)")
     args = ap.parse_args()
@@ -388,6 +457,7 @@ def main():
     e2e_val = world * n * args.steps / e2e_s
 
     batched = run_batched(M, torch, args.steps, args.warmup)
+    surrogate = run_surrogate(M, torch, min(args.steps, 200)) if not args.no_surrogate else None
 
     if rank != 0:
         if dist:
@@ -441,6 +511,7 @@ def main():
                                      "how": "the same captured step launched back to back, no flush"},
         "cpu_baseline": cpu,
         "batched_ensemble": batched,
+        "surrogate": surrogate,
     }
     print(json.dumps(line), flush=True)
     if dist:

@@ -160,6 +160,7 @@ struct ConvPlan {
     DBuf<char> spec;     // SPEC[kx][c][z][y] (complex)
     DBuf<char> ten6;     // TEN6[kx][kz][ky][6] (real)
     DBuf<char> ten9;     // TEN9[kx][kz][ky][9] (complex)
+    DBuf<char> spec2;    // split passes: S2[kx][ky][c][z] (complex)
     double max_imag = 0; // largest |Im| of the FP64 tensor transform (6-component)
     // SPEC holds the forward x transform of the spins of the system whose
     // spec_token equals this one (set by the fused x pass; 0 = none)
@@ -602,13 +603,20 @@ void plan_sizes(mlb_op* op, ConvPlan& P)
     int ty = 16;
     while (ty > 1 && (size_t)2 * ty * k.Px * cb > 96 * 1024) ty /= 2;
     k.ty = ty;
+    k.split = 0;
+    k.spec2 = nullptr;
     // the power-of-two FP32 fast path has its own limits; the general
-    // kernels hold a whole padded (y,z) plane of three components twice
+    // kernels hold a whole padded (y,z) plane of three components twice;
+    // larger planes take the split (y,z) passes
     if (P.rb == 4 && mlb::conv_fast_ok(k)) return;
-    if ((size_t)6 * k.Py * k.Pz * cb > 227 * 1024)
-        fail(MLB_EUNSUP, "padded (y,z) plane " + std::to_string(k.Py) + "x" + std::to_string(k.Pz) +
-                             " exceeds the shared-memory plane of this build at " + std::to_string(8 * P.rb) +
-                             "-bit precision");
+    if ((size_t)6 * k.Py * k.Pz * cb > 227 * 1024) {
+        k.split = 1;
+        if (mlb::split_smem(k, P.rb) > 227 * 1024)
+            fail(MLB_EUNSUP, "padded lengths " + std::to_string(k.Py) + "x" + std::to_string(k.Pz) +
+                                 " exceed the split passes of this build at " + std::to_string(8 * P.rb) +
+                                 "-bit precision");
+        if (P.rb == 4 && mlb::conv_fast_ok(k)) return;
+    }
     if ((size_t)2 * k.Px * cb > 96 * 1024) fail(MLB_EUNSUP, "x length too large");
 }
 
@@ -703,16 +711,20 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
     CK(mlb::launch_fft3d_d(W.p, ncomp, Px, Py, Pz, P->L, twdd.p, -1, st));
     if (k.general) {
         P->ten9.alloc((size_t)k.Kx * Py * Pz * 9 * 2 * rb);
-        CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, rb, st));
+        CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, rb, k.split, st));
     } else {
         P->ten6.alloc((size_t)k.Kx * Py * Pz * 6 * rb);
         DBuf<double> mi;
         mi.alloc(1);
         CK(cudaMemsetAsync(mi.p, 0, sizeof(double), st));
-        CK(mlb::launch_tensor_pack6(W.p, Px, Py, Pz, k.Kx, P->ten6.p, mi.p, rb, st));
+        CK(mlb::launch_tensor_pack6(W.p, Px, Py, Pz, k.Kx, P->ten6.p, mi.p, rb, k.split, st));
         CK(cudaMemcpyAsync(&P->max_imag, mi.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     P->spec.alloc((size_t)k.Kx * 3 * op->nz * op->ny * 2 * rb);
+    if (k.split) {
+        P->spec2.alloc((size_t)k.Kx * Py * 3 * op->nz * 2 * rb);
+        k.spec2 = P->spec2.p;
+    }
     CK(cudaStreamSynchronize(st));
     op->plan = std::move(P);
     op->plan_dirty = false;
@@ -3558,6 +3570,9 @@ extern "C" int mlb_dipole_field_noalloc(mlb_op* op, const float* sx, const float
         ConvPlan geo;
         geo.rb = 4;
         plan_sizes(op, geo);
+        if (geo.k.split)
+            fail(MLB_EUNSUP, "a (y,z) plane larger than shared memory needs the split passes' second spectrum "
+                             "buffer, which mlb_dipole_field_noalloc does not provide");
         const size_t need = (size_t)geo.k.Kx * 3 * op->nz * op->ny * sizeof(float2);
         if (need > (size_t)MLB_NOALLOC_SCRATCH_BYTES)
             fail(MLB_ERANGE, "spectrum of " + std::to_string(need) + " bytes for " + std::to_string(op->nx) + "x" +

@@ -635,8 +635,23 @@ static size_t yz_fast_smem(int PY, int PZ, int nz)
 
 bool conv_fast_ok(const ConvK& c)
 {
-    if (c.general || !pow2_in(c.Px, 16, 512) || !pow2_in(c.Py, 16, 512) || !pow2_in(c.Pz, 1, 32)) return false;
+    if (c.general || !pow2_in(c.Px, 16, 512)) return false;
+    // large planes: fast x passes around the split (y,z) passes
+    if (c.split) return true;
+    if (!pow2_in(c.Py, 16, 512) || !pow2_in(c.Pz, 1, 32)) return false;
     return yz_fast_smem(c.Py, c.Pz, c.nz) <= 227 * 1024;
+}
+
+static cudaError_t launch_yz_any(const ConvK& c, const float2* twy, float2* spec, const float* ten6,
+                                 cudaStream_t st);
+
+// (y,z) pass of the fast path: the whole-plane kernel, or the split passes
+static cudaError_t yz_pass(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const float* ten6,
+                           cudaStream_t st)
+{
+    if (c.split) return launch_conv_split_yz(c, L[1], L[2], tw, spec, ten6, nullptr, 4, st);
+    Prof pf("k_conv_yz", st);
+    return launch_yz_any(c, tw + L[1].tw_off, spec, ten6, st);
 }
 
 template <int PX>
@@ -754,10 +769,7 @@ cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw
         e = launch_x_any(c, tw + L[0].tw_off, s, spec, h, st, true);
     }
     if (e != cudaSuccess) return e;
-    {
-        Prof pf("k_conv_yz", st);
-        e = launch_yz_any(c, tw + L[1].tw_off, spec, ten6, st);
-    }
+    e = yz_pass(c, L, tw, spec, ten6, st);
     if (e != cudaSuccess) return e;
     {
         Prof pf("k_conv_ix", st);
@@ -776,8 +788,7 @@ cudaError_t launch_conv_fast_fyz(const ConvK& c, const FftLen L[3], const float2
         e = launch_x_any(c, tw + L[0].tw_off, s, spec, nullptr, st, true);
     }
     if (e != cudaSuccess) return e;
-    Prof pf("k_conv_yz", st);
-    return launch_yz_any(c, tw + L[1].tw_off, spec, ten6, st);
+    return yz_pass(c, L, tw, spec, ten6, st);
 }
 
 cudaError_t launch_conv_fast_ix(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, float* h[3],

@@ -19,6 +19,8 @@
 
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 #include <stdint.h>
 #include <stdio.h>
 
@@ -741,9 +743,9 @@ __global__ void k_fft_lines(C* data, int Px, int Py, int Pz, int ax, FftLen L, c
 }
 
 // Real symmetric tensor: TEN6[kx][kz][ky][q] = Re W_q(kx,ky,kz) in the
-// state precision R.
+// state precision R (kmaj: TEN6[kx][ky][kz][q], the split-pass layout).
 template <typename R>
-__global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, R* ten6, double* maxim)
+__global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, R* ten6, double* maxim, int kmaj)
 {
     const long long total = (long long)Kx * Py * Pz;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -753,10 +755,11 @@ __global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx,
     const int kz = rem / Py, ky = rem % Py;
     const size_t plane = (size_t)Px * Py * Pz;
     const size_t off = ((size_t)kz * Py + ky) * Px + kx;
+    const size_t o = kmaj ? ((size_t)kx * Py + ky) * Pz + kz : (size_t)e;
     double mi = 0;
     for (int q = 0; q < 6; q++) {
         const double2 v = W[q * plane + off];
-        ten6[(size_t)e * 6 + q] = (R)v.x;
+        ten6[o * 6 + q] = (R)v.x;
         mi = fmax(mi, fabs(v.y));
     }
     if (maxim) {
@@ -765,9 +768,10 @@ __global__ void k_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx,
     }
 }
 
-// General 9-component complex tensor: TEN9[kx][kz][ky][q].
+// General 9-component complex tensor: TEN9[kx][kz][ky][q] (kmaj:
+// TEN9[kx][ky][kz][q]).
 template <typename R>
-__global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, typename CT<R>::T* ten9)
+__global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, typename CT<R>::T* ten9, int kmaj)
 {
     const long long total = (long long)Kx * Py * Pz;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -777,9 +781,132 @@ __global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx,
     const int kz = rem / Py, ky = rem % Py;
     const size_t plane = (size_t)Px * Py * Pz;
     const size_t off = ((size_t)kz * Py + ky) * Px + kx;
+    const size_t o = kmaj ? ((size_t)kx * Py + ky) * Pz + kz : (size_t)e;
     for (int q = 0; q < 9; q++) {
         const double2 v = W[q * plane + off];
-        ten9[(size_t)e * 9 + q] = cmk<typename CT<R>::T>((R)v.x, (R)v.y);
+        ten9[o * 9 + q] = cmk<typename CT<R>::T>((R)v.x, (R)v.y);
+    }
+}
+
+// ------------------------------------------------------------ split (y,z) passes
+// For (y,z) planes larger than one CTA's shared memory (a 256^3 open cube
+// pads to 512 x 512 planes): the plane pass of k_conv_yz done as three
+// passes through S2[kx][ky][comp][z] (data layers z < nz only).
+//   k_split_y   CTA (kx, comp, SPLIT_ZB data layers): y FFT of the layers'
+//               rows (zero-padded to Py), stored ky-major in S2;
+//   k_split_z   CTA (kx, ky): z FFT of the three components' columns
+//               (zero-padded to Pz), tensor multiply (ky-major tensor),
+//               inverse z FFT, data layers back to S2;
+//   k_split_yi  CTA (kx, comp, SPLIT_ZB layers): inverse y FFT, data rows to
+//               SPEC[kx][comp][z][y].
+// The arithmetic per element is that of k_conv_yz: same FFTs, same multiply.
+constexpr int SPLIT_ZB = 8;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_split_y(ConvK c, FftLen Ly, const typename CT<R>::T* tw,
+                                                 const typename CT<R>::T* spec, typename CT<R>::T* s2)
+{
+    if (c.run_if && *c.run_if == 0) return;
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw);
+    C* B = A + SPLIT_ZB * c.Py;
+    const int kx = blockIdx.x, comp = blockIdx.y, z0 = blockIdx.z * SPLIT_ZB;
+    const int nl = min(SPLIT_ZB, c.nz - z0);
+    const C* src = spec + (((size_t)kx * 3 + comp) * c.nz + z0) * c.ny;
+    for (int t = threadIdx.x; t < nl * c.Py; t += blockDim.x) {
+        const int l = t / c.Py, y = t % c.Py;
+        A[t] = y < c.ny ? src[(size_t)l * c.ny + y] : cmk<C>((R)0, (R)0);
+    }
+    __syncthreads();
+    LineGeo g;
+    g.nlines = nl; g.lpg = 1 << 30; g.gstride = 0; g.ls = c.Py; g.es = 1; g.line_fast = 0;
+    const C* Rl = c.Py > 1 ? cta_fft<C>(A, B, g, Ly, tw, -1) : A;
+    for (int t = threadIdx.x; t < nl * c.Py; t += blockDim.x) {
+        const int l = t % nl, ky = t / nl;
+        s2[(((size_t)kx * c.Py + ky) * 3 + comp) * c.nz + z0 + l] = Rl[l * c.Py + ky];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_split_z(ConvK c, FftLen Lz, const typename CT<R>::T* tw,
+                                                 typename CT<R>::T* s2, const R* ten6, const typename CT<R>::T* ten9)
+{
+    if (c.run_if && *c.run_if == 0) return;
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw);
+    C* B = A + 3 * c.Pz;
+    const int kx = blockIdx.x, ky = blockIdx.y;
+    const int Pz = c.Pz;
+    C* col = s2 + ((size_t)kx * c.Py + ky) * 3 * c.nz;
+    for (int t = threadIdx.x; t < 3 * Pz; t += blockDim.x) {
+        const int comp = t / Pz, z = t % Pz;
+        A[t] = z < c.nz ? col[comp * c.nz + z] : cmk<C>((R)0, (R)0);
+    }
+    __syncthreads();
+    LineGeo g;
+    g.nlines = 3; g.lpg = 1 << 30; g.gstride = 0; g.ls = Pz; g.es = 1; g.line_fast = 0;
+    C* cur = A;
+    C* oth = B;
+    if (Pz > 1) { cur = cta_fft<C>(cur, oth, g, Lz, tw, -1); oth = cur == A ? B : A; }
+    const R gg = (R)c.g;
+    const size_t tb = ((size_t)kx * c.Py + ky) * Pz;
+    if (!c.general) {
+        for (int t = threadIdx.x; t < Pz; t += blockDim.x) {
+            const R* T = ten6 + (tb + t) * 6;
+            const R t0 = __ldg(T), t1 = __ldg(T + 1), t2 = __ldg(T + 2);
+            const R t3 = __ldg(T + 3), t4 = __ldg(T + 4), t5 = __ldg(T + 5);
+            const C s0 = cur[t], s1 = cur[Pz + t], s2v = cur[2 * Pz + t];
+            cur[t] = cmk<C>(gg * (t0 * s0.x + t1 * s1.x + t2 * s2v.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2v.y));
+            cur[Pz + t] = cmk<C>(gg * (t1 * s0.x + t3 * s1.x + t4 * s2v.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2v.y));
+            cur[2 * Pz + t] =
+                cmk<C>(gg * (t2 * s0.x + t4 * s1.x + t5 * s2v.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2v.y));
+        }
+    } else {
+        for (int t = threadIdx.x; t < Pz; t += blockDim.x) {
+            const C* T = ten9 + (tb + t) * 9;
+            const C s[3] = {cur[t], cur[Pz + t], cur[2 * Pz + t]};
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                C acc = cmk<C>((R)0, (R)0);
+#pragma unroll
+                for (int b = 0; b < 3; b++) acc = cadd(acc, cmul(T[3 * a + b], s[b]));
+                cur[a * Pz + t] = cmk<C>(gg * acc.x, gg * acc.y);
+            }
+        }
+    }
+    __syncthreads();
+    if (Pz > 1) { cur = cta_fft<C>(cur, oth, g, Lz, tw, +1); }
+    for (int t = threadIdx.x; t < 3 * c.nz; t += blockDim.x) {
+        const int comp = t / c.nz, z = t % c.nz;
+        col[t] = cur[comp * Pz + z];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_split_yi(ConvK c, FftLen Ly, const typename CT<R>::T* tw,
+                                                  const typename CT<R>::T* s2, typename CT<R>::T* spec)
+{
+    if (c.run_if && *c.run_if == 0) return;
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* A = reinterpret_cast<C*>(smraw);
+    C* B = A + SPLIT_ZB * c.Py;
+    const int kx = blockIdx.x, comp = blockIdx.y, z0 = blockIdx.z * SPLIT_ZB;
+    const int nl = min(SPLIT_ZB, c.nz - z0);
+    for (int t = threadIdx.x; t < nl * c.Py; t += blockDim.x) {
+        const int l = t % nl, ky = t / nl;
+        A[l * c.Py + ky] = s2[(((size_t)kx * c.Py + ky) * 3 + comp) * c.nz + z0 + l];
+    }
+    __syncthreads();
+    LineGeo g;
+    g.nlines = nl; g.lpg = 1 << 30; g.gstride = 0; g.ls = c.Py; g.es = 1; g.line_fast = 0;
+    const C* Rl = c.Py > 1 ? cta_fft<C>(A, B, g, Ly, tw, +1) : A;
+    C* dst = spec + (((size_t)kx * 3 + comp) * c.nz + z0) * c.ny;
+    for (int t = threadIdx.x; t < nl * c.ny; t += blockDim.x) {
+        const int l = t / c.ny, y = t % c.ny;
+        dst[(size_t)l * c.ny + y] = Rl[l * c.Py + y];
     }
 }
 
@@ -951,6 +1078,9 @@ cudaError_t conv_configure()
     if ((e = max_smem(k_conv_fx<double>)) != cudaSuccess) return e;
     if ((e = max_smem(k_conv_ix<float>)) != cudaSuccess) return e;
     if ((e = max_smem(k_conv_ix<double>)) != cudaSuccess) return e;
+    if ((e = max_smem(k_split_y<float>)) || (e = max_smem(k_split_y<double>)) || (e = max_smem(k_split_yi<float>)) ||
+        (e = max_smem(k_split_yi<double>)) || (e = max_smem(k_split_z<float>)) || (e = max_smem(k_split_z<double>)))
+        return e;
     return max_smem(k_fft_lines<double2>);
 }
 
@@ -967,7 +1097,9 @@ static void conv_generic(const ConvK& c, const FftLen& Lx, const FftLen& Ly, con
         Prof pf("k_conv_fx", st);
         k_conv_fx<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, Lx, tw, s[0], s[1], s[2], spec);
     }
-    {
+    if (c.split) {
+        launch_conv_split_yz(c, Ly, Lz, tw_, spec_, ten6, ten9, (int)sizeof(R), st);
+    } else {
         Prof pf("k_conv_yz", st);
         k_conv_yz<R><<<c.Kx, 512, conv_yz_smem(c, sizeof(R)), st>>>(c, Ly, Lz, tw, spec, static_cast<const R*>(ten6),
                                                                     static_cast<const C*>(ten9));
@@ -1034,26 +1166,60 @@ cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const 
 }
 
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
-                                int rb, cudaStream_t st)
+                                int rb, int kmaj, cudaStream_t st)
 {
     const long long total = (long long)Kx * Py * Pz;
     if (rb == 8)
         k_tensor_pack6<double><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<double*>(ten6),
-                                                                       maxim);
+                                                                       maxim, kmaj);
     else
         k_tensor_pack6<float><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<float*>(ten6),
-                                                                      maxim);
+                                                                      maxim, kmaj);
     return cudaGetLastError();
 }
 
-cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb,
+cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb, int kmaj,
                                 cudaStream_t st)
 {
     const long long total = (long long)Kx * Py * Pz;
     if (rb == 8)
-        k_tensor_pack9<double><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<double2*>(ten9));
+        k_tensor_pack9<double><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<double2*>(ten9),
+                                                                       kmaj);
     else
-        k_tensor_pack9<float><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<float2*>(ten9));
+        k_tensor_pack9<float><<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, static_cast<float2*>(ten9),
+                                                                      kmaj);
+    return cudaGetLastError();
+}
+
+size_t split_smem(const ConvK& c, int rb)
+{
+    const size_t cb = (size_t)2 * rb;
+    return std::max((size_t)2 * SPLIT_ZB * c.Py * cb, (size_t)6 * c.Pz * cb);
+}
+
+template <typename R>
+static void split_t(const ConvK& c, const FftLen& Ly, const FftLen& Lz, const void* tw_, void* spec_,
+                    const void* ten6, const void* ten9, cudaStream_t st)
+{
+    typedef typename CT<R>::T C;
+    const C* tw = static_cast<const C*>(tw_);
+    C* spec = static_cast<C*>(spec_);
+    C* s2 = static_cast<C*>(c.spec2);
+    const size_t cb = 2 * sizeof(R);
+    dim3 gy(c.Kx, 3, (c.nz + SPLIT_ZB - 1) / SPLIT_ZB);
+    const size_t smy = (size_t)2 * SPLIT_ZB * c.Py * cb;
+    k_split_y<R><<<gy, 256, smy, st>>>(c, Ly, tw, spec, s2);
+    k_split_z<R><<<dim3(c.Kx, c.Py), 256, (size_t)6 * c.Pz * cb, st>>>(c, Lz, tw, s2, static_cast<const R*>(ten6),
+                                                                       static_cast<const C*>(ten9));
+    k_split_yi<R><<<gy, 256, smy, st>>>(c, Ly, tw, s2, spec);
+}
+
+cudaError_t launch_conv_split_yz(const ConvK& c, const FftLen& Ly, const FftLen& Lz, const void* tw, void* spec,
+                                 const void* ten6, const void* ten9, int rb, cudaStream_t st)
+{
+    Prof pf("k_conv_yz_split", st);
+    if (rb == 8) split_t<double>(c, Ly, Lz, tw, spec, ten6, ten9, st);
+    else split_t<float>(c, Ly, Lz, tw, spec, ten6, ten9, st);
     return cudaGetLastError();
 }
 

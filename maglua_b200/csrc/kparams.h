@@ -122,6 +122,12 @@ struct ConvK {
     int fx, fy, fz;          // FftLen indices
     int nrep;                // replicas of this size packed back to back (1 for a system)
     const int* run_if;       // when set, the passes run only while *run_if != 0
+    // Planes too large for one CTA's shared memory: the (y,z) pass runs as
+    // three passes (y, z with the tensor multiply, inverse y) through spec2,
+    // S2[kx][ky][comp][z] (data layers only), and the tensor is stored
+    // ky-major, TEN[kx][ky][kz][q].
+    int split;
+    void* spec2;
 };
 
 // Fused step for uniform-parameter systems (k_fused_fast): every constant

@@ -109,9 +109,13 @@ cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int 
 cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const FftLen L[3],
                            const double2* tw, int sign, cudaStream_t st);
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
-                                int rb, cudaStream_t st);
-cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb,
+                                int rb, int kmaj, cudaStream_t st);
+cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb, int kmaj,
                                 cudaStream_t st);
+// Split (y,z) passes for planes larger than shared memory (c.split, c.spec2).
+size_t split_smem(const ConvK& c, int rb);
+cudaError_t launch_conv_split_yz(const ConvK& c, const FftLen& Ly, const FftLen& Lz, const void* tw, void* spec,
+                                 const void* ten6, const void* ten9, int rb, cudaStream_t st);
 // Learned surrogate (surrogate.cu).
 size_t sur_out_smem(int CP, int rad);
 size_t sur_gw_smem(int C, int rad);

@@ -115,6 +115,8 @@ lib.orc_lr_apply.argtypes = [C.c_void_p, _PSS, C.c_char_p, C.c_double, C.c_doubl
 lib.orc_lr_free.argtypes = [C.c_void_p]
 lib.orc_longrange3d_apply.argtypes = [_PSS, _D * 9, C.c_double, C.c_double]
 lib.orc_dipole_direct.argtypes = [_PSS, _D, C.c_double, C.c_int, C.c_int, C.c_int, _D, _D, _D]
+lib.orc_dipole_direct_sites.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_double,
+                                        C.POINTER(C.c_longlong), C.c_int, _D]
 lib.orc_llg_default.argtypes = [C.POINTER(_LLG)]
 lib.orc_llg_cart_apply.argtypes = [C.POINTER(_LLG), _PSS, C.c_double, _PSS, _PSS, C.c_int]
 lib.orc_llg_quat_apply.argtypes = [C.POINTER(_LLG), _PSS, C.c_double, _PSS, _PSS, C.c_int]
@@ -352,6 +354,18 @@ def longrange3d_apply(ss, T9, g, gscale=1.0):
     T9 = [_f64(t).reshape(-1) for t in T9]
     arr = (_D * 9)(*[_dp(t) for t in T9])
     lib.orc_longrange3d_apply(ss.p, arr, g, gscale)
+
+
+def dipole_direct_sites(dims, spins, g, sites, ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
+    """Open-boundary direct dipole sum at the listed target sites only
+    (3 x len(sites)); spins are 3 arrays of nx*ny*nz in SpinSystem order."""
+    nx, ny, nz = dims
+    x, y, z = (_f64(a) for a in spins)
+    st = np.ascontiguousarray(sites, dtype=np.int64)
+    out = np.zeros(3 * len(st))
+    lib.orc_dipole_direct_sites(nx, ny, nz, _dp(x), _dp(y), _dp(z), _dp(_f64(ABC)), g,
+                                st.ctypes.data_as(C.POINTER(C.c_longlong)), len(st), _dp(out))
+    return out.reshape(-1, 3).T
 
 
 def dipole_direct(ss, g, periodic=(0, 0, 0), ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):

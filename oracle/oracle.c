@@ -827,6 +827,33 @@ void orc_dipole_direct(const orc_ss* ss, const double ABC[9], double g,
     }
 }
 
+/* The same open-boundary direct sum at chosen target sites only, over
+ * spin arrays given directly (for lattices too large for the O(N^2) form):
+ * out[3*q + a] = g * sum_s Gamma(r_t - r_s) m_s for target t = sites[q]. */
+void orc_dipole_direct_sites(int nx, int ny, int nz, const double* x, const double* y, const double* z,
+                             const double ABC[9], double g, const long long* sites, int nsites, double* out)
+{
+    const long long n = (long long)nx * ny * nz;
+    for (int q = 0; q < nsites; q++) {
+        const long long t = sites[q];
+        const int tx = (int)(t % nx), ty = (int)((t / nx) % ny), tz = (int)(t / ((long long)nx * ny));
+        double ax = 0, ay = 0, az = 0;
+        for (long long s = 0; s < n; s++) {
+            const int sx = (int)(s % nx), sy = (int)((s / nx) % ny), sz = (int)(s / ((long long)nx * ny));
+            const int dx = tx - sx, dy = ty - sy, dz = tz - sz;
+            const double rx = dx * ABC[0] + dy * ABC[3] + dz * ABC[6];
+            const double ry = dx * ABC[1] + dy * ABC[4] + dz * ABC[7];
+            const double rz = dx * ABC[2] + dy * ABC[5] + dz * ABC[8];
+            double G[6];
+            gamma_dip(rx, ry, rz, G);
+            ax += G[0] * x[s] + G[1] * y[s] + G[2] * z[s];
+            ay += G[1] * x[s] + G[3] * y[s] + G[4] * z[s];
+            az += G[2] * x[s] + G[4] * y[s] + G[5] * z[s];
+        }
+        out[3 * q] = g * ax; out[3 * q + 1] = g * ay; out[3 * q + 2] = g * az;
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* LLG                                                                  */
 /* ------------------------------------------------------------------ */

@@ -100,6 +100,8 @@ void    orc_lr_free(orc_lr* c);
  * T9 = {XX,XY,XZ,YX,YY,YZ,ZX,ZY,ZZ}, each nx*ny*nz, cyclic. */
 void orc_longrange3d_apply(orc_ss* ss, double* const T9[9], double g, double gscale);
 /* Physical open-boundary direct sum h_t = g * sum_s Gamma(r_t - r_s) s_s (no images). */
+void orc_dipole_direct_sites(int nx, int ny, int nz, const double* x, const double* y, const double* z,
+                             const double ABC[9], double g, const long long* sites, int nsites, double* out);
 void orc_dipole_direct(const orc_ss* ss, const double ABC[9], double g,
                        int px, int py, int pz, double* hx, double* hy, double* hz);
 
