@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmlb200.so")
 SOURCES = ["kernels.cu", "conv_fast.cu", "surrogate.cu", "capi.cu"]
-HEADERS = ["device.cuh", "fftreg.cuh", "kparams.h", "launch.h"]
+HEADERS = ["device.cuh", "fftreg.cuh", "fused.cuh", "kparams.h", "launch.h", "umma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -1292,6 +1292,9 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
     } else if (advance) {
         to->time = from->time + dt;
     }
+    // an attached surrogate's device schedule advances with every step of
+    // its system, whether issued by do_step or as individual calls
+    if (to->sur && !to->dry) sur_advance(to);
 }
 
 void sum_fields(mlb_system* s)
@@ -1394,7 +1397,7 @@ void upload_site_array(mlb_system* s, void** dst, const double* a)
 void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
 {
     reset_fields(s);
-    s->defer_x = !s->sur;
+    s->defer_x = true;
     try {
         for (int i = 0; i < nops; i++) op_apply(ops[i], s);
         sum_fields(s);
@@ -1411,7 +1414,6 @@ void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
     }
     s->defer_x = false;
     flush_pending(s);
-    if (s->sur && !s->dry) sur_advance(s);
 }
 
 void advance_sweep(mlb_op* const* ops, int nops)
@@ -2999,6 +3001,8 @@ struct mlb_surrogate {
     DBuf<double> lpart, lsum;
     DBuf<int> err;
     DBuf<SurDev> dev;
+    DBuf<double> rpart;         // per-CTA residual sums of the output kernel
+    int rnp = 0;
     int lnb = 1;
     long long stats[3] = {0, 0, 0};
     double last_bound = 0.0;
@@ -3053,7 +3057,8 @@ void sur_forward(mlb_surrogate* S, const float* const a[3], const float* const b
     CK(mlb::launch_sur_ydft(k, S->Xp.p, S->twy.p, reinterpret_cast<const float2*>(S->r.p), S->Yh.p, S->Zh.p,
                             S->ycnt.p, st));
     CK(mlb::launch_sur_zrows(k, S->Zh.p, S->twy.p, S->Zb.p, st));
-    CK(mlb::launch_sur_out(k, S->Xb.p, h0, out, S->wc.p, S->Fc.p, S->Zb.p, dev, S->err.p, mode, st));
+    CK(mlb::launch_sur_out(k, S->Xb.p, h0, out, S->wc.p, S->Fc.p, S->Zb.p, dev, mode == 1 ? nullptr : S->rpart.p,
+                           S->err.p, mode, st));
 }
 
 // Loss, gradients and one Adam step for the pair (a - b, hx - h0) (h0 may be
@@ -3118,6 +3123,10 @@ void plain_step_with(mlb_system* ss, mlb_op* const* ops, int nops, mlb_llg* l, m
 
 namespace {
 
+// The surrogate's operator field of this step: the network's field (skipped
+// on exact steps), the exact passes (run on exact steps only), and the
+// snapshot m0 = m, H0 = H after an exact evaluation; the device schedule
+// decides which, so a captured step holds both.
 bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl)
 {
     mlb_surrogate* S = s->sur;
@@ -3133,7 +3142,6 @@ bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl)
     }
     const float ratio = S->g_train > 0 ? (float)(op->g * op->gs / S->g_train) : 1.f;
     sur_forward(S, a, b, 0, h0, out, d, &d->exact, ratio, s->st);
-    // exact passes, run only when the schedule or the residual check asks
     ConvPlan& P = *op->plan;
     if (!s->capturing) P.spec_token = 0;
     ConvK kk = P.k;
@@ -3154,7 +3162,10 @@ bool sur_hook(mlb_op* op, mlb_system* s, Slot& sl)
     return true;
 }
 
-void sur_advance(mlb_system* s) { CK(mlb::launch_sur_advance(s->sur->dev.p, s->st)); }
+void sur_advance(mlb_system* s)
+{
+    CK(mlb::launch_sur_advance(s->sur->dev.p, s->sur->rpart.p, s->sur->rnp, s->st));
+}
 
 } // namespace
 
@@ -3240,6 +3251,9 @@ int mlb_surrogate_create(mlb_op* op, int mx, int my, int rad, mlb_surrogate** ou
         S->err.alloc(1);
         CK(cudaMemset(S->err.p, 0, sizeof(int)));
         S->dev.alloc(1);
+        S->rnp = (nx / 128) * ny;
+        S->rpart.alloc((size_t)2 * S->rnp);
+
         SurDev h{};
         h.exact = 1;
         h.k = S->kint;
@@ -3470,8 +3484,8 @@ int mlb_surrogate_detach(mlb_system* ss)
         SurDev h;
         CK(cudaMemcpy(&h, S->dev.p, sizeof(h), cudaMemcpyDeviceToHost));
         S->stats[0] = h.nexact;
-        S->stats[1] = h.nsur - h.nfail;
-        S->stats[2] = h.nfail;
+        S->stats[1] = h.nsur;      // steps that used the network's field
+        S->stats[2] = h.nfail;     // of those, checks that sent the next step to the exact field
         S->last_bound = h.last_bound;
         sur_check_err(S);
     });

@@ -1,0 +1,125 @@
+// fused.cuh -- one site of the fused step (field terms + LLG update) for
+// uniform-parameter FP32 systems, shared by the fused-step kernels
+// (conv_fast.cu) and the surrogate's output kernel (surrogate.cu).
+#pragma once
+#include "device.cuh"
+#include "kparams.h"
+
+#include <math.h>
+#include <stdint.h>
+
+// ------------------------------------------------------------------ fused step
+// Uniform-parameter systems: ms, alpha, gamma, anisotropy and thermal scale
+// the same on every site, exchange as a six-direction stencil.  Constants
+// are folded on the host (FastK).
+// One site of the fused step.  (x, y, z) are the site's coordinates inside
+// its lattice of NX x NY x NZ sites and i its index in the (packed) arrays;
+// neighbours are addressed relative to i, so several lattices can share the
+// arrays back to back.
+// The new spin of the site is returned in (rx, ry, rz); (Ax, Ay, Az) is the
+// materialised addend (the dipole slot), used when ADD.
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
+__device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                             const float* __restrict__ sx, const float* __restrict__ sy,
+                                             const float* __restrict__ sz, float Ax, float Ay, float Az, float& rx,
+                                             float& ry, float& rz)
+{
+    const int nxy = NX * NY;
+    const float Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
+    float Hx, Hy, Hz;
+    if (F.Bdev) { Hx = (float)F.Bdev[0]; Hy = (float)F.Bdev[1]; Hz = (float)F.Bdev[2]; }
+    else { Hx = F.B[0]; Hy = F.B[1]; Hz = F.B[2]; }
+    if (EXS) {
+        float ex = 0.f, ey = 0.f, ez = 0.f;
+#define MLB_NB(cond, wrapcond, off, woff, J)                                                       \
+        if ((J) != 0.f) {                                                                          \
+            int f = -1;                                                                            \
+            if (cond) f = i + (off);                                                               \
+            else if (wrapcond) f = i + (woff);                                                     \
+            if (f >= 0) {                                                                          \
+                ex += (J) * __ldg(sx + f); ey += (J) * __ldg(sy + f); ez += (J) * __ldg(sz + f);   \
+            }                                                                                      \
+        }
+        MLB_NB(x + 1 < NX, F.pbc[0], 1, 1 - NX, F.J[0])
+        MLB_NB(x > 0, F.pbc[0], -1, NX - 1, F.J[1])
+        MLB_NB(y + 1 < NY, F.pbc[1], NX, NX - nxy, F.J[2])
+        MLB_NB(y > 0, F.pbc[1], -NX, nxy - NX, F.J[3])
+        MLB_NB(z + 1 < NZ, F.pbc[2], nxy, nxy - nxy * NZ, F.J[4])
+        MLB_NB(z > 0, F.pbc[2], -nxy, nxy * NZ - nxy, F.J[5])
+#undef MLB_NB
+        Hx += ex; Hy += ey; Hz += ez;
+    }
+    if (ANI) {
+        const float v = F.ani_c * (Sx * F.axis[0] + Sy * F.axis[1] + Sz * F.axis[2]);
+        Hx += v * F.axis[0]; Hy += v * F.axis[1]; Hz += v * F.axis[2];
+    }
+    float Tx = 0.f, Ty = 0.f, Tz = 0.f;
+    if (TH) {
+        const uint64_t ctr = F.counter + (F.dctr ? *F.dctr : 0ull);
+        const float3 nrm = philox_normal3(F.seed, ctr, (uint32_t)i, 0x6d6c6232u);
+        Tx = F.sigma * nrm.x; Ty = F.sigma * nrm.y; Tz = F.sigma * nrm.z;
+        Hx += Tx; Hy += Ty; Hz += Tz;
+    }
+    if (ADD) {
+        Hx += F.addw * Ax; Hy += F.addw * Ay; Hz += F.addw * Az;
+    }
+    float nx_, ny_, nz_;
+    if (LT == LLG_CART) {
+        if (F.dt_zero) { nx_ = Sx; ny_ = Sy; nz_ = Sz; }
+        else {
+            // h = H - Hth; dM = -p gaa M x H - d (a/ms) gaa M x (M x h)
+            const float hx = F.tof ? Hx - Tx : Hx, hy = F.tof ? Hy - Ty : Hy, hz = F.tof ? Hz - Tz : Hz;
+            const float mhx = Sy * hz - Sz * hy, mhy = Sz * hx - Sx * hz, mhz = Sx * hy - Sy * hx;
+            const float mmx = Sy * mhz - Sz * mhy, mmy = Sz * mhx - Sx * mhz, mmz = Sx * mhy - Sy * mhx;
+            const float MHx = Sy * Hz - Sz * Hy, MHy = Sz * Hx - Sx * Hz, MHz = Sx * Hy - Sy * Hx;
+            nx_ = Sx + F.dt * (F.c_prec * MHx - F.c_damp * mmx);
+            ny_ = Sy + F.dt * (F.c_prec * MHy - F.c_damp * mmy);
+            nz_ = Sz + F.dt * (F.c_prec * MHz - F.c_damp * mmz);
+        }
+    } else {
+        float Hpx, Hpy, Hpz;
+        if (F.tof) {
+            const float hx = Hx - Tx, hy = Hy - Ty, hz = Hz - Tz;
+            const float shx = Sy * hz - Sz * hy, shy = Sz * hx - Sx * hz, shz = Sx * hy - Sy * hx;
+            Hpx = F.precess * Hx + F.c_damp * shx;
+            Hpy = F.precess * Hy + F.c_damp * shy;
+            Hpz = F.precess * Hz + F.c_damp * shz;
+        } else {
+            const float shx = Sy * Hz - Sz * Hy, shy = Sz * Hx - Sx * Hz, shz = Sx * Hy - Sy * Hx;
+            Hpx = Hx + F.c_damp * shx; Hpy = Hy + F.c_damp * shy; Hpz = Hz + F.c_damp * shz;
+        }
+        const float HL2 = Hpx * Hpx + Hpy * Hpy + Hpz * Hpz;
+        if (HL2 > 0.f) {
+            const float iHL = rsqrtf(HL2);
+            const float HL = HL2 * iHL;
+            // half rotation angle; small angles by their Taylor series
+            // (|th| <= 0.1: truncation below 1e-10), else sincosf
+            const float th = F.c_rot * HL;
+            float sn, cs;
+            if (fabsf(th) <= 0.1f) {
+                const float t2 = th * th;
+                sn = th * (1.0f - t2 * (1.0f / 6.0f) * (1.0f - t2 * (1.0f / 20.0f) * (1.0f - t2 * (1.0f / 42.0f))));
+                cs = 1.0f - t2 * 0.5f * (1.0f - t2 * (1.0f / 12.0f) * (1.0f - t2 * (1.0f / 30.0f) * (1.0f - t2 * (1.0f / 56.0f))));
+            } else {
+                sincosf(th, &sn, &cs);
+            }
+            const float qw = cs, qx = sn * Hpx * iHL, qy = sn * Hpy * iHL, qz = sn * Hpz * iHL;
+            const float tw = -qx * Sx - qy * Sy - qz * Sz;
+            const float tx = qw * Sx + qy * Sz - qz * Sy;
+            const float ty = qw * Sy + qz * Sx - qx * Sz;
+            const float tz = qw * Sz + qx * Sy - qy * Sx;
+            nx_ = -tw * qx + qw * tx - ty * qz + tz * qy;
+            ny_ = -tw * qy + qw * ty - tz * qx + tx * qz;
+            nz_ = -tw * qz + qw * tz - tx * qy + ty * qx;
+        } else { nx_ = Sx; ny_ = Sy; nz_ = Sz; }
+    }
+    if (F.renorm) {
+        const float mm = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
+        if (mm != 0.f) {
+            const float inv = F.ms * rsqrtf(mm);
+            nx_ *= inv; ny_ *= inv; nz_ *= inv;
+        }
+    }
+    rx = nx_; ry = ny_; rz = nz_;
+}
+

@@ -177,6 +177,7 @@ struct SurDev {
     float eps;                // validation relative error of the predicted update
     float tol;                // bound on the estimated relative field error
     float last_bound;
+    int fail;                 // this step's residual check failed: the next step is exact
     unsigned int arrivals;    // CTAs of the output kernel done this step
     double sums[2];           // sum dH^2, sum H^2 of this step
 };

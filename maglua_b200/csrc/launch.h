@@ -126,12 +126,15 @@ cudaError_t launch_sur_xdft(const SurK& k, const float* const a[3], const float*
 cudaError_t launch_sur_ydft(const SurK& k, const float2* Xp, const float2* twy, const float2* R, float2* Yh,
                             float2* Zh, unsigned int* cnt, cudaStream_t st);
 cudaError_t launch_sur_zrows(const SurK& k, const float2* Zh, const float2* twy, uint8_t* Zb, cudaStream_t st);
+// mode 0: out = h0 + ratio * dH (the surrogate's field; per-CTA residual
+// sums to part); mode 1: out = dH.
 cudaError_t launch_sur_out(const SurK& k, const uint4* Xb, const float* const h0[3], float* const out[3],
-                           const uint8_t* Wc, const uint8_t* Fc, const uint8_t* Zb, SurDev* dev, int* err, int mode,
-                           cudaStream_t st);
+                           const uint8_t* Wc, const uint8_t* Fc, const uint8_t* Zb, SurDev* dev, double* part,
+                           int* err, int mode, cudaStream_t st);
 cudaError_t launch_sur_snapshot(SurDev* d, int n, const float* const m[3], const float* const h[3],
                                 float* const sm[3], float* const sh[3], cudaStream_t st);
-cudaError_t launch_sur_advance(SurDev* d, cudaStream_t st);
+// End of a step: residual check of a surrogate step (np per-CTA sums), schedule
+cudaError_t launch_sur_advance(SurDev* d, const double* part, int np, cudaStream_t st);
 cudaError_t launch_sur_loss(int n, const float* const P[3], const float* const X[3], const float* const H0[3],
                             float* const G[3], double* part, int nb, double* out, cudaStream_t st);
 cudaError_t launch_sur_grad_w(const SurK& k, const float* const a[3], const float* const b[3],

@@ -11,12 +11,14 @@
 // Both branches are evaluated as BF16 x BF16 -> FP32 GEMMs on the tcgen05
 // tensor cores (operands staged in shared memory, accumulators in TMEM):
 //   k_sur_xdft   Xhat over x: [(y, ch) rows] x [x] times the DFT rows [(kx, re/im)] x [x];
-//   k_sur_modes  DFT over y of the retained kx and the per-mode channel mixing
-//                (CUDA cores, FP32: a few MFLOP);
+//   k_sur_ydft   DFT over y of the retained kx and the per-mode channel mixing,
+//   k_sur_zrows  inverse DFT over y into each row's B tile (CUDA cores, FP32:
+//                a few MFLOP);
 //   k_sur_out    per 128-site M-tile: 25 shifted views of the staged halo tile
 //                (one MMA per stencil offset, no im2col copy) plus the inverse
 //                x-DFT [x] x [(kx, re/im)] times the mixed spectrum of this row,
-//                FP32 epilogue adds H0 (or writes dH for training).
+//                FP32 epilogue adds H0 (or writes dH for training) and leaves
+//                per-CTA residual sums for the schedule (k_sur_advance).
 // Training kernels (FP32, CUDA cores): loss and its gradient G, the stencil
 // gradient sum_s G[co](s) X[ci](s + o), the mode gradient
 // w_kx/(nx ny) Ghat_k[co] conj(Xhat_k[ci]) and Adam.
@@ -285,7 +287,8 @@ struct OutArgs {
     const uint8_t* Wc;      // stencil weights, canonical B tiles per offset
     const uint8_t* Fc;      // inverse x-DFT rows, canonical A layout over all nx
     const uint8_t* Zb;      // per-row B tiles of the mixed spectrum
-    SurDev* dev;            // residual statistics (mode 0)
+    SurDev* dev;
+    double* part;           // mode 0: per-CTA sums of dH^2 and H^2
     int* err;
     int mode;               // 0: out = h0 + ratio * dH; 1: out = dH
 };
@@ -301,6 +304,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int CP, int RAD>
 __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
 {
+    pdl_trigger();
+    pdl_wait();
     if (k.skip_if && *k.skip_if) return;
     constexpr int NPL = CP / 8, DIA = 2 * RAD + 1, HW = 128 + 2 * RAD;
     constexpr uint32_t PL = (DIA * HW * 16 + 127) & ~127u;   // bytes per halo plane
@@ -402,8 +407,8 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
     umma::fence_before_sync();
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(taddr, 32);
-    if (q.mode != 0 || !q.dev) return;
-    // residual statistics: block sums, then the last CTA of the grid decides
+    if (q.mode == 1 || !q.part) return;
+    // residual statistics: this CTA's sums (k_sur_advance reduces them)
     for (int s = 16; s > 0; s >>= 1) {
         s_dh += __shfl_xor_sync(0xffffffffu, s_dh, s);
         s_h += __shfl_xor_sync(0xffffffffu, s_h, s);
@@ -413,24 +418,9 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
     if (tid == 0) {
         double a = 0, b = 0;
         for (int w = 0; w < 4; w++) { a += red[0][w]; b += red[1][w]; }
-        atomicAdd(&q.dev->sums[0], a);
-        atomicAdd(&q.dev->sums[1], b);
-        __threadfence();
-        const unsigned int done = atomicAdd(&q.dev->arrivals, 1u);
-        if (done == gridDim.x * gridDim.y - 1) {
-            __threadfence();
-            const double sdh = atomicAdd(&q.dev->sums[0], 0.0), sh = atomicAdd(&q.dev->sums[1], 0.0);
-            const float bound = sh > 0 ? (float)((double)q.dev->eps * sqrt(sdh / sh)) : 0.f;
-            q.dev->last_bound = bound;
-            q.dev->nsur += 1;
-            if (bound > q.dev->tol) {
-                q.dev->exact = 1;       // this step's exact passes run after this kernel
-                q.dev->nfail += 1;
-            }
-            q.dev->sums[0] = 0.0;
-            q.dev->sums[1] = 0.0;
-            q.dev->arrivals = 0u;
-        }
+        const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+        q.part[2 * cta] = a;
+        q.part[2 * cta + 1] = b;
     }
 }
 
@@ -449,11 +439,43 @@ __global__ void __launch_bounds__(256) k_sur_snapshot(SurDev* d, int n, const fl
     }
 }
 
-// End of a step: the next one is exact every k steps.
-__global__ void k_sur_advance(SurDev* d)
+// End of a step (one CTA of 256 threads).  After a surrogate step: the
+// residual check, bound = eps |dH| / |H| from the output kernel's per-CTA
+// sums, fails when bound > tol.  The next step is exact every k steps,
+// after a failed check, and always when the bound is zero.
+__global__ void __launch_bounds__(256) k_sur_advance(SurDev* d, const double* part, int np)
 {
-    d->cycle += 1;
-    d->exact = d->cycle >= d->k ? 1 : 0;
+    pdl_wait();
+    __shared__ double red[2][8];
+    if (!d->exact && part) {
+        double a = 0.0, b = 0.0;
+        for (int i = threadIdx.x; i < np; i += blockDim.x) {
+            a += part[2 * i];
+            b += part[2 * i + 1];
+        }
+        for (int s = 16; s > 0; s >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, s);
+            b += __shfl_xor_sync(0xffffffffu, b, s);
+        }
+        if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = a; red[1][threadIdx.x >> 5] = b; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sdh = 0.0, sh = 0.0;
+            for (int w = 0; w < 8; w++) { sdh += red[0][w]; sh += red[1][w]; }
+            const float bound = sh > 0 ? (float)((double)d->eps * sqrt(sdh / sh)) : 0.f;
+            d->last_bound = bound;
+            d->nsur += 1;
+            if (bound > d->tol) {
+                d->fail = 1;        // the next step evaluates the exact convolution
+                d->nfail += 1;
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        d->cycle += 1;
+        d->exact = (d->cycle >= d->k || d->fail || !(d->tol > 0.f)) ? 1 : 0;
+        d->fail = 0;
+    }
 }
 
 // ------------------------------------------------------------------ training
@@ -683,37 +705,39 @@ cudaError_t launch_sur_zrows(const SurK& k, const float2* Zh, const float2* twy,
 
 
 cudaError_t launch_sur_out(const SurK& k, const uint4* Xb, const float* const h0[3], float* const out[3],
-                           const uint8_t* Wc, const uint8_t* Fc, const uint8_t* Zb, SurDev* dev, int* err, int mode,
-                           cudaStream_t st)
+                           const uint8_t* Wc, const uint8_t* Fc, const uint8_t* Zb, SurDev* dev, double* part,
+                           int* err, int mode, cudaStream_t st)
 {
     Prof pf("k_sur_out", st);
     OutArgs q;
+    memset(&q, 0, sizeof(q));
     q.Xb = Xb;
     for (int c = 0; c < 3; c++) {
         q.h0[c] = h0 ? h0[c] : nullptr;
         q.out[c] = out[c];
     }
-    q.Wc = Wc; q.Fc = Fc; q.Zb = Zb; q.dev = dev; q.err = err; q.mode = mode;
+    q.Wc = Wc; q.Fc = Fc; q.Zb = Zb; q.dev = dev; q.part = part; q.err = err; q.mode = mode;
     dim3 g(k.nx / 128, k.ny);
     const size_t sm = sur_out_smem(k.CP, k.rad);
-#define MLB_SUR_OUT(CPV, RV) k_sur_out<CPV, RV><<<g, 128, sm, st>>>(k, q)
+    cudaError_t e = cudaSuccess;
+#define MLB_SUR_OUT(CPV, RV) launch_pdl(k_sur_out<CPV, RV>, g, dim3(128), sm, st, k, q)
     if (k.CP == 16) {
         switch (k.rad) {
-        case 0: MLB_SUR_OUT(16, 0); break;
-        case 1: MLB_SUR_OUT(16, 1); break;
-        case 2: MLB_SUR_OUT(16, 2); break;
-        default: MLB_SUR_OUT(16, 3); break;
+        case 0: e = MLB_SUR_OUT(16, 0); break;
+        case 1: e = MLB_SUR_OUT(16, 1); break;
+        case 2: e = MLB_SUR_OUT(16, 2); break;
+        default: e = MLB_SUR_OUT(16, 3); break;
         }
     } else {
         switch (k.rad) {
-        case 0: MLB_SUR_OUT(32, 0); break;
-        case 1: MLB_SUR_OUT(32, 1); break;
-        case 2: MLB_SUR_OUT(32, 2); break;
-        default: MLB_SUR_OUT(32, 3); break;
+        case 0: e = MLB_SUR_OUT(32, 0); break;
+        case 1: e = MLB_SUR_OUT(32, 1); break;
+        case 2: e = MLB_SUR_OUT(32, 2); break;
+        default: e = MLB_SUR_OUT(32, 3); break;
         }
     }
 #undef MLB_SUR_OUT
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_sur_snapshot(SurDev* d, int n, const float* const m[3], const float* const h[3],
@@ -726,10 +750,9 @@ cudaError_t launch_sur_snapshot(SurDev* d, int n, const float* const m[3], const
     return cudaGetLastError();
 }
 
-cudaError_t launch_sur_advance(SurDev* d, cudaStream_t st)
+cudaError_t launch_sur_advance(SurDev* d, const double* part, int np, cudaStream_t st)
 {
-    k_sur_advance<<<1, 1, 0, st>>>(d);
-    return cudaGetLastError();
+    return launch_pdl(k_sur_advance, dim3(1), dim3(256), 0, st, d, part, np);
 }
 
 cudaError_t launch_sur_loss(int n, const float* const P[3], const float* const X[3], const float* const H0[3],

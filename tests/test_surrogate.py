@@ -178,3 +178,35 @@ def test_run_schedule_counts_and_stays_close(M):
     S.run(ss, ops, llg, 40)
     st = S.stats()
     assert st["exact"] == 8 and st["surrogate"] == 32 and st["failed"] == 0, st
+
+
+def test_fused_surrogate_step_equals_individual_calls(M):
+    """Attached surrogate: steps run through the fused output pass (network
+    field + LLG update in one kernel, exact steps through the fused x pass)
+    equal the same steps issued as individual calls, which materialise the
+    field in the slot and run the separate step kernel."""
+    dims = (128, 32, 2)
+    res = []
+    for mode in ("calls", "run"):
+        ss, ops, dip = _film(M, dims, 404)
+        S = M.Surrogate(dip, (8, 8), RAD)
+        W, R = _random_params(10)
+        S.setParams(W * 1e-2, R * 1e-2)
+        S.setSchedule(3, tol=1.0, eps=0.05)
+        llg = M.LLG.new("Quaternion")
+        S.attach(ss)
+        if mode == "calls":
+            for _ in range(8):
+                ss.resetFields()
+                for op in ops:
+                    op.apply(ss)
+                ss.sumFields()
+                llg.apply(ss)
+        else:
+            M.run(ss, ops, llg, 8)
+        S.detach(ss)
+        res.append((np.stack(ss.spinArrays()[:3]), np.stack(ss.fieldArrays("Dipole")), S.stats()))
+    np.testing.assert_array_equal(res[0][0], res[1][0])
+    np.testing.assert_array_equal(res[0][1], res[1][1])
+    assert res[0][2]["exact"] == res[1][2]["exact"] == 3, res
+    assert res[1][2]["surrogate"] == 5, res
