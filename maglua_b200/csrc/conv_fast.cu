@@ -41,8 +41,9 @@ using fr::Split;
 
 // ------------------------------------------------------------------ x passes
 // A CTA of 256 threads transforms L = 256/TPL complex lines; line l packs
-// rows (row0 + 2l, row0 + 2l + 1) of one component of one layer as real and
-// imaginary parts.  Global loads are gathered into registers in unrolled
+// rows (row0 + 2l, row0 + 2l + 1) of one component as real and imaginary
+// parts, rows counted over the flattened (z, y) index r = z ny + y (SPEC is
+// contiguous in r), so small layers fill a CTA.  Global loads are gathered into registers in unrolled
 // batches before they are written to shared memory, so each thread has all
 // its loads in flight at once.
 template <int PX>
@@ -72,11 +73,12 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][PX]
     float2* B = A + X::BUF;         // [L][PX]
-    const int comp = blockIdx.z % 3, rep = blockIdx.z / 3, zz = blockIdx.y;
+    const int comp = blockIdx.z % 3, rep = blockIdx.z / 3;
+    const int nr = c.nz * c.ny;                 // rows (z, y) of one component, flattened
     const int row0 = blockIdx.x * X::ROWS;
     const size_t nsite = (size_t)c.nx * c.ny * c.nz;
-    spec += (size_t)rep * c.Kx * 3 * c.nz * c.ny;
-    const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + rep * nsite + (size_t)zz * c.ny * c.nx;
+    spec += (size_t)rep * c.Kx * 3 * nr;
+    const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + rep * nsite;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     constexpr int IT = (X::LINE + NT - 1) / NT;
     float2 v[IT];
@@ -87,8 +89,8 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
         const int ya = row0 + 2 * l, yb = ya + 1;
         float a = 0.f, b = 0.f;
         if (idx < X::LINE && x < c.nx) {
-            if (ya < c.ny) a = __ldg(src + (size_t)ya * c.nx + x);
-            if (yb < c.ny) b = __ldg(src + (size_t)yb * c.nx + x);
+            if (ya < nr) a = __ldg(src + (size_t)ya * c.nx + x);
+            if (yb < nr) b = __ldg(src + (size_t)yb * c.nx + x);
         }
         v[it] = make_float2(a, b);
     }
@@ -100,8 +102,8 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
     const float2* R = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
-    // split the two real rows and store SPEC[kx][comp][zz][row]
-    const int rows_here = min(X::ROWS, c.ny - row0);
+    // split the two real rows and store SPEC[kx][comp][row] (row = z ny + y)
+    const int rows_here = min(X::ROWS, nr - row0);
     constexpr int IS = (X::SPEC + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < IS; it++) {
@@ -113,7 +115,7 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
         float2 o;
         if ((row & 1) == 0) o = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
         else o = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
-        spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + row0 + row] = o;
+        spec[((size_t)kx * 3 + comp) * nr + row0 + row] = o;
     }
 }
 
@@ -131,12 +133,13 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][PX] lines
     float2* B = A + X::BUF;         // [ROWS][KX] spectra, then scratch
-    const int comp = blockIdx.z % 3, rep = blockIdx.z / 3, zz = blockIdx.y;
+    const int comp = blockIdx.z % 3, rep = blockIdx.z / 3;
+    const int nr = c.nz * c.ny;                 // rows (z, y) of one component, flattened
     const int row0 = blockIdx.x * X::ROWS;
-    const int rows_here = min(X::ROWS, c.ny - row0);
+    const int rows_here = min(X::ROWS, nr - row0);
     const size_t nsite = (size_t)c.nx * c.ny * c.nz;
-    spec += (size_t)rep * c.Kx * 3 * c.nz * c.ny;
-    float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + rep * nsite + (size_t)zz * c.ny * c.nx;
+    spec += (size_t)rep * c.Kx * 3 * nr;
+    float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + rep * nsite;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     constexpr int IS = (X::SPEC + NT - 1) / NT;
     {
@@ -147,7 +150,7 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
             const int kx = idx / X::ROWS, row = idx % X::ROWS;
             v[it] = make_float2(0.f, 0.f);
             if (idx < X::SPEC && row < rows_here)
-                v[it] = spec[(((size_t)kx * 3 + comp) * c.nz + zz) * c.ny + row0 + row];
+                v[it] = spec[((size_t)kx * 3 + comp) * nr + row0 + row];
         }
 #pragma unroll
         for (int it = 0; it < IS; it++) {
@@ -189,14 +192,17 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
 // One CTA per kx.  y transforms of the 3*nz data lines by TPL threads each
 // (in rounds), z transforms + tensor multiply with one thread per
 // (component, ky) column, inverse y transforms.
-// threads per CTA: 768, or 384 when the z columns are 32 long (registers)
+// threads per CTA: 768 for the planes of a large film (one CTA per SM), 384
+// when the z columns are 32 long (registers), 256 for planes up to 128 wide
+// (many small replicas: several CTAs per SM)
 template <int PY, int PZ>
 struct YZT {
-    static constexpr int N = PZ >= 32 ? 384 : 768;
+    static constexpr int N = PY <= 128 ? 256 : (PZ >= 32 ? 384 : 768);
+    static constexpr int MINB = PY <= 128 ? 3 : 1;
 };
 
 template <int PY, int PZ>
-__global__ void __launch_bounds__(YZT<PY, PZ>::N, 1) k_yz_fast(ConvK c, const float2* __restrict__ twy,
+__global__ void __launch_bounds__(YZT<PY, PZ>::N, YZT<PY, PZ>::MINB) k_yz_fast(ConvK c, const float2* __restrict__ twy,
                                                                float2* __restrict__ spec, const float* __restrict__ ten6)
 {
     constexpr int NT = YZT<PY, PZ>::N;
@@ -328,8 +334,9 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
 }
 
 // ------------------------------------------------------------------ fused x pass of a step
-// One CTA owns ROWS consecutive rows (y0 .. y0 + ROWS - 1) of one layer z, all
-// three components, and runs on them, in shared memory:
+// One CTA owns ROWS consecutive rows r = z ny + y (the flattened (z, y) row
+// index, r0 .. r0 + ROWS - 1), all three components, and runs on them, in
+// shared memory:
 //   1. the inverse x transform of the (y,z)-pass output (two rows per
 //      complex line, Hermitian completion) -> the dipole field of the rows,
 //      written to its slot;
@@ -370,15 +377,15 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][PX] lines
     float2* B = A + X::BUF;         // [3][ROWS][KX] spectra, then scratch
-    const int zz = blockIdx.y;
-    const int row0 = blockIdx.x * ROWS;
-    const int rows_here = min(ROWS, c.ny - row0);
     const int nx = c.nx, ny = c.ny, nz = c.nz;
+    const int nr = nz * ny;                     // rows (z, y), flattened
+    const int row0 = blockIdx.x * ROWS;
+    const int rows_here = min(ROWS, nr - row0);
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
-    // 1. spectrum rows SPEC[kx][comp][zz][row0 + row] -> B[(comp ROWS + row) KX + kx]
+    // 1. spectrum rows SPEC[kx][comp][row0 + row] -> B[(comp ROWS + row) KX + kx]
     constexpr int IS = (X::SPEC + NT - 1) / NT;
     {
         float2 v[IS];
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
             const int comp = rem / ROWS, row = rem % ROWS;
             v[it] = make_float2(0.f, 0.f);
             if (idx < X::SPEC && row < rows_here)
-                v[it] = spec[(((size_t)kx * 3 + comp) * nz + zz) * ny + row0 + row];
+                v[it] = spec[((size_t)kx * 3 + comp) * nr + row0 + row];
         }
 #pragma unroll
         for (int it = 0; it < IS; it++) {
@@ -421,7 +428,6 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
     const float* Rf = reinterpret_cast<const float*>(R);
     float* Wf = reinterpret_cast<float*>(W);
     // 2. field of the rows to the slot, then the step of every site
-    const size_t layer = (size_t)zz * ny * nx;
     constexpr int IO = (ROWS * PX + NT - 1) / NT;
 #pragma unroll 1
     for (int it = 0; it < IO; it++) {
@@ -432,8 +438,8 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
         float rx = 0.f, ry = 0.f, rz = 0.f;
         if (live) {
             const float Ax = Rf[fo], Ay = Rf[fo + 2 * R2 * PX], Az = Rf[fo + 4 * R2 * PX];
-            const int y = row0 + row;
-            const size_t i = layer + (size_t)y * nx + x;
+            const int r = row0 + row, zz = r / ny, y = r - zz * ny;
+            const size_t i = (size_t)r * nx + x;
             hx[i] = Ax; hy[i] = Ay; hz[i] = Az;
             fused_site_v<LT, EXS, ANI, TH, true>(F, nx, ny, nz, x, y, zz, (int)i, sx, sy, sz, Ax, Ay, Az, rx, ry, rz);
             ox[i] = rx; oy[i] = ry; oz[i] = rz;
@@ -458,7 +464,7 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
         float2 o;
         if ((row & 1) == 0) o = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
         else o = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
-        spec[(((size_t)kx * 3 + comp) * nz + zz) * ny + row0 + row] = o;
+        spec[((size_t)kx * 3 + comp) * nr + row0 + row] = o;
     }
 }
 
@@ -548,7 +554,7 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
                             cudaStream_t st, bool fwd)
 {
     using X = XCfg<PX>;
-    dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 3 * c.nrep);
+    dim3 grid((c.nz * c.ny + X::ROWS - 1) / X::ROWS, 1, 3 * c.nrep);
     const size_t smem = X::SMEM;
     if (fwd) {
         return launch_pdl(k_fx_fast<PX>, grid, dim3(256), smem, st, c, tw, s[0], s[1], s[2], spec);
@@ -697,7 +703,7 @@ static cudaError_t xstep_t(const ConvK& c, const FastK& F, int fwd, const float2
                            const float* s[3], float* h[3], float* o[3], cudaStream_t st)
 {
     using X = XSCfg<PX>;
-    dim3 grid((c.ny + X::ROWS - 1) / X::ROWS, c.nz, 1);
+    dim3 grid((c.nz * c.ny + X::ROWS - 1) / X::ROWS, 1, 1);
     return launch_pdl(k_xstep<PX, LT, true, ANI, TH>, grid, dim3(X::NT), (size_t)X::SMEM, st, c, F, fwd, tw, spec,
                       s[0], s[1], s[2], h[0], h[1], h[2], o[0], o[1], o[2]);
 }
