@@ -49,7 +49,7 @@ def tilted_spins(n, seed, deg=5.0):
 
 def nn_paths(nx, ny, nz, pbc=(1, 1, 0)):
     """Pathways of the canonical setup loop ex:add({i,j,k},{i+-1,...},J)."""
-    idx = np.arange(nx * ny * nz).reshape(nz, ny, nx)
+    idx = np.arange(nx * ny * nz, dtype=np.int32).reshape(nz, ny, nx)
     frm, to = [], []
     for ax, n in ((2, nx), (1, ny), (0, nz)):
         for sgn in (1, -1):
@@ -190,6 +190,75 @@ def run_surrogate(M, torch, steps, flush_l2=None):
     return out
 
 
+# ----------------------------------------------------------------- 256^3 open cube
+CUBE_DIMS = (256, 256, 256)
+CUBE_WORKLOAD = ("256^3 simple-cubic cube, open boundaries (512^3 padded transform, split (y,z) passes), "
+                 "J=1, cubic anisotropy K_c=0.05 (axes x, y, z), g=0.03, T=0.3, alpha=0.05, dt=0.005, "
+                 "LLG.Quaternion; spins +z with a seeded 20-degree tilt")
+
+
+def run_cube(M, torch, steps=20):
+    """Configuration 5 on one GPU: FP32 and FP64 step rates, and the FP32
+    fields and energies of one state against the FP64 run's (both from the
+    same spins: the FP64 state after 2 steps, rounded to FP32)."""
+    dims = CUBE_DIMS
+    n = int(np.prod(dims))
+    f, t, j = nn_paths(*dims, pbc=(0, 0, 0))
+    s0 = tilted_spins(n, 5, deg=20.0)
+
+    def build(prec, spins):
+        ss = M.SpinSystem(*dims, precision=prec)
+        ss.setSpinArrays(*spins)
+        ss.setAlpha(0.05)
+        ss.setTimeStep(0.005)
+        ex = M.Exchange(ss)
+        ex.addPaths(f, t, j)
+        cub = M.AnisotropyCubic(ss)
+        cub.addMany(np.arange(n), np.tile([1.0, 0, 0], (n, 1)), np.tile([0, 1.0, 0], (n, 1)),
+                    np.tile([0.05, 0, 0], (n, 1)))
+        th = M.Thermal(ss, M.Random.Philox(5))
+        th.setTemperature(0.3)
+        dip = M.Dipole(ss)
+        dip.setStrength(0.03)
+        dip.setOpen(True, True, True)
+        return ss, [ex, cub, th, dip], M.LLG.new("Quaternion")
+
+    def timed(ss, fn, k):
+        st = torch.cuda.ExternalStream(ss.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ss.synchronize()
+        a.record(st)
+        fn(k)
+        b.record(st)
+        ss.synchronize()
+        return a.elapsed_time(b) / k
+
+    d, dops, dl = build("f64", s0)
+    M.run(d, dops, dl, 2)
+    f64_ms = timed(d, lambda k: M.run(d, dops, dl, k), 3)
+    x, y, z, _ = d.spinArrays()
+    g, gops, gl = build("f32", np.stack([x, y, z]))
+    for ss in (d, g):
+        ops = dops if ss is d else gops
+        ss.resetFields()
+        for op in ops[:2] + ops[3:]:
+            op.apply(ss)
+        ss.sumFields()
+    hd, hg = np.stack(d.fieldArrays("Dipole")), np.stack(g.fieldArrays("Dipole"))
+    out = {"workload": CUBE_WORKLOAD, "sites": n,
+           "dipole_field_rel_err_f32_vs_f64": float(np.linalg.norm(hg - hd) / np.linalg.norm(hd)), "energy_rel_err": {}}
+    for nm in ("Exchange", "CubicAnisotropy", "Dipole"):
+        ed, eg = d.fieldDot(nm), g.fieldDot(nm)
+        out["energy_rel_err"][nm] = abs(eg - ed) / abs(ed)
+    del d, dops, hd, hg
+    M.run(g, gops, gl, 3)
+    f32_ms = timed(g, lambda k: M.run(g, gops, gl, k), steps)
+    out["f32"] = {"value": n / (f32_ms * 1e-3), "ms_per_step": f32_ms}
+    out["f64"] = {"value": n / (f64_ms * 1e-3), "ms_per_step": f64_ms}
+    out["l2"] = "working set several GB: larger than L2 (no flush)"
+    return out
+
+
 # ----------------------------------------------------------------- algorithmic bytes
 def algorithmic_bytes():
     """Per-launch algorithmic bytes of each kernel, split from the per
@@ -327,6 +396,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate comparison")
+    ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 open-cube precision study")
     ap.add_argument("--ncu-steps", type=int, default=0,
                     help="profiling driver: run this many eager steps of the workload and exit (for ncu)")
     args = ap.parse_args()
@@ -458,6 +528,7 @@ def main():
 
     batched = run_batched(M, torch, args.steps, args.warmup)
     surrogate = run_surrogate(M, torch, min(args.steps, 200)) if not args.no_surrogate else None
+    cube = run_cube(M, torch) if not args.no_cube else None
 
     if rank != 0:
         if dist:
@@ -512,6 +583,7 @@ def main():
         "cpu_baseline": cpu,
         "batched_ensemble": batched,
         "surrogate": surrogate,
+        "cube_256": cube,
     }
     print(json.dumps(line), flush=True)
     if dist:
