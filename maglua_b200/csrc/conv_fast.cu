@@ -302,6 +302,126 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, YZT<PY, PZ>::MINB) k_yz_fast(C
     }
 }
 
+// ------------------------------------------------------------------ (y,z) pass, register form
+// For the planes of a large film (Py 256 or 512, Pz <= 16): one CTA of 384
+// threads per kx.  The y transforms of the 3 nz data lines are four-step
+// register FFTs (fr::line_fft: T lanes per line, E = Py/T points per lane, one
+// warp-synchronous exchange); lane t of a line loads x[t + T j] straight from
+// SPEC and stores its outputs in natural order to the plane P[3][nz][Py].
+// Then each thread takes whole ky columns: the z transforms of the three
+// components (zero-padded to Pz), the 3x3 real tensor multiply and the inverse
+// z transforms in registers, data layers back to P.  The inverse y transforms
+// read P and store the data rows straight to SPEC.  Shared-memory traffic is
+// about a third of the Stockham form's, with no z-spectrum buffer.
+template <int PY, int PZ>
+struct YZR {
+    static constexpr int NT = 384;
+    static constexpr int T = fr::Split<PY>::T;
+    static constexpr int E = fr::Split<PY>::E;
+    static constexpr int LPR = NT / T;                  // lines per round
+    static constexpr int EX = E * (T + 1);              // exchange elements per line
+    static size_t smem(int nz) { return ((size_t)3 * nz * PY + (size_t)LPR * EX + PY) * sizeof(float2); }
+};
+
+template <int PY, int PZ>
+__global__ void __launch_bounds__(384, 1) k_yz_reg(ConvK c, const float2* __restrict__ twy,
+                                                   float2* __restrict__ spec, const float* __restrict__ ten6)
+{
+    using Y = YZR<PY, PZ>;
+    constexpr int NT = Y::NT, T = Y::T, E = Y::E;
+    extern __shared__ float2 sm[];
+    const int kx = blockIdx.x;
+    const int nz = c.nz, ny = c.ny;
+    const int nlines = 3 * nz;
+    float2* P = sm;                                // [3][nz][PY]
+    float2* ex = P + (size_t)nlines * PY;          // [LPR][EX]
+    float2* twl = ex + (size_t)Y::LPR * Y::EX;     // [PY]
+    const float* Tk = ten6 + (size_t)kx * PZ * PY * 6;
+    if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(PZ * PY * 6 * sizeof(float));
+        if ((((uintptr_t)Tk) & 15) == 0 && (bytes & 15) == 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tk), "r"(bytes) : "memory");
+    }
+    for (int k = threadIdx.x; k < PY; k += NT) twl[k] = twy[k];
+    pdl_trigger();
+    pdl_wait();
+    if (c.run_if && *c.run_if == 0) return;
+    float2* sp = spec + (size_t)kx * nlines * ny;
+    __syncthreads();
+    const int lr = threadIdx.x / T, t = threadIdx.x % T;
+    const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << (((threadIdx.x & 31) / T) * T));
+    float2* exl = ex + (size_t)lr * Y::EX;
+    // forward y transforms: SPEC rows -> P (natural order)
+    for (int l0 = 0; l0 < nlines; l0 += Y::LPR) {
+        const int l = l0 + lr;
+        const bool act = l < nlines;   // whole T-lane groups share act
+        if (act) {
+            float2 v[E];
+#pragma unroll
+            for (int j = 0; j < E; j++) {
+                const int y = t + T * j;
+                v[j] = y < ny ? sp[(size_t)l * ny + y] : make_float2(0.f, 0.f);
+            }
+            fr::line_fft<PY, -1, float2>(v, exl, t, mask, twl);
+#pragma unroll
+            for (int r = 0; r < E; r++) P[(size_t)l * PY + fr::out_index<PY>(t, r)] = v[r];
+        }
+    }
+    __syncthreads();
+    // z transforms, tensor multiply, inverse z transforms: one ky column per thread
+    const float gg = c.g;
+    for (int ky = threadIdx.x; ky < PY; ky += NT) {
+        float2 s0[PZ], s1[PZ], s2[PZ];
+#pragma unroll
+        for (int z = 0; z < PZ; z++) {
+            const bool in = z < nz;
+            s0[z] = in ? P[((size_t)0 * nz + z) * PY + ky] : make_float2(0.f, 0.f);
+            s1[z] = in ? P[((size_t)1 * nz + z) * PY + ky] : make_float2(0.f, 0.f);
+            s2[z] = in ? P[((size_t)2 * nz + z) * PY + ky] : make_float2(0.f, 0.f);
+        }
+        fr::RegFFT<PZ, -1, float2>::run(s0);
+        fr::RegFFT<PZ, -1, float2>::run(s1);
+        fr::RegFFT<PZ, -1, float2>::run(s2);
+#pragma unroll
+        for (int kz = 0; kz < PZ; kz++) {
+            const float* Tp = Tk + ((size_t)kz * PY + ky) * 6;
+            const float t0 = __ldg(Tp) * gg, t1 = __ldg(Tp + 1) * gg, t2 = __ldg(Tp + 2) * gg;
+            const float t3 = __ldg(Tp + 3) * gg, t4 = __ldg(Tp + 4) * gg, t5 = __ldg(Tp + 5) * gg;
+            const float2 a = s0[kz], b = s1[kz], d = s2[kz];
+            s0[kz] = make_float2(t0 * a.x + t1 * b.x + t2 * d.x, t0 * a.y + t1 * b.y + t2 * d.y);
+            s1[kz] = make_float2(t1 * a.x + t3 * b.x + t4 * d.x, t1 * a.y + t3 * b.y + t4 * d.y);
+            s2[kz] = make_float2(t2 * a.x + t4 * b.x + t5 * d.x, t2 * a.y + t4 * b.y + t5 * d.y);
+        }
+        fr::RegFFT<PZ, +1, float2>::run(s0);
+        fr::RegFFT<PZ, +1, float2>::run(s1);
+        fr::RegFFT<PZ, +1, float2>::run(s2);
+#pragma unroll
+        for (int z = 0; z < PZ; z++) {
+            if (z < nz) {
+                P[((size_t)0 * nz + z) * PY + ky] = s0[z];
+                P[((size_t)1 * nz + z) * PY + ky] = s1[z];
+                P[((size_t)2 * nz + z) * PY + ky] = s2[z];
+            }
+        }
+    }
+    __syncthreads();
+    // inverse y transforms: P -> SPEC data rows
+    for (int l0 = 0; l0 < nlines; l0 += Y::LPR) {
+        const int l = l0 + lr;
+        if (l < nlines) {
+            float2 v[E];
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = P[(size_t)l * PY + t + T * j];
+            fr::line_fft<PY, +1, float2>(v, exl, t, mask, twl);
+#pragma unroll
+            for (int r = 0; r < E; r++) {
+                const int y = fr::out_index<PY>(t, r);
+                if (y < ny) sp[(size_t)l * ny + y] = v[r];
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ fused step
 // (fused_site_v, the per-site arithmetic, is in fused.cuh)
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
@@ -522,6 +642,15 @@ namespace mlb {
 
 static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
+// the register (y,z) kernel: a single film's planes of width 256 or 512,
+// z padded to at most 16, and the plane in shared memory
+static bool yz_reg_ok(int PY, int PZ, const ConvK& c)
+{
+    if (c.nrep != 1 || (PY != 256 && PY != 512) || PZ > 16) return false;
+    const size_t sm = PY == 256 ? YZR<256, 16>::smem(c.nz) : YZR<512, 16>::smem(c.nz);
+    return sm <= 227 * 1024;
+}
+
 // shared memory of k_yz_fast: data rows and scratch, z spectra, twiddles
 static size_t yz_fast_smem(int PY, int PZ, int nz)
 {
@@ -581,6 +710,10 @@ static cudaError_t launch_x_any(const ConvK& c, const float2* tw, const float* s
 template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
+    if (yz_reg_ok(PY, PZ, c)) {
+        return launch_pdl(k_yz_reg<(PY >= 256 ? PY : 256), (PZ <= 16 ? PZ : 16)>, dim3(c.Kx), dim3(384),
+                          YZR<(PY >= 256 ? PY : 256), (PZ <= 16 ? PZ : 16)>::smem(c.nz), st, c, twy, spec, ten6);
+    }
     const size_t smem = yz_fast_smem(PY, PZ, c.nz);
     return launch_pdl(k_yz_fast<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZT<PY, PZ>::N), smem, st, c, twy, spec, ten6);
 }
@@ -641,6 +774,18 @@ static cudaError_t cfg_yz()
 template <int PX>
 static cudaError_t cfg_xs();
 
+template <int PY>
+static cudaError_t cfg_yzr()
+{
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 1>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 2>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 4>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 8>, a, 227 * 1024)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_yz_reg<PY, 16>, a, 227 * 1024);
+}
+
 cudaError_t conv_fast_configure()
 {
     cudaError_t e;
@@ -652,6 +797,7 @@ cudaError_t conv_fast_configure()
         return e;
     if ((e = cfg_xs<32>()) || (e = cfg_xs<64>()) || (e = cfg_xs<128>()) || (e = cfg_xs<256>()) || (e = cfg_xs<512>()))
         return e;
+    if ((e = cfg_yzr<256>()) || (e = cfg_yzr<512>())) return e;
     return cudaSuccess;
 }
 

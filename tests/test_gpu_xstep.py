@@ -179,3 +179,46 @@ def test_run_matches_oracle(M):
                 B=(0.1, 0, 0.02), lr=lr, g=0.03, llg="Quaternion")
     err = float(np.abs(np.stack(ss.spinArrays()[:3]) - o.spins()).max())
     assert err < 2e-6, err
+
+
+@pytest.mark.parametrize("dims,open_xy", [((32, 256, 4), False), ((16, 512, 2), False), ((8, 128, 3), True)])
+def test_wide_plane_dipole_field(M, dims, open_xy):
+    """Planes 256 and 512 wide (the register (y,z) kernel): dipole field
+    against the oracle, reference-mode lattice sum or open direct sum."""
+    from helpers import Pair
+    n = int(np.prod(dims))
+    p = Pair(*dims, random_spins(n, 47, lengths=True))
+    p.dipole(g=0.4, open_xy=open_xy)
+    p.o.reset_fields()
+    for f in p.oapply:
+        f(p.o)
+    p.g.resetFields()
+    for op in p.ops:
+        op.apply(p.g)
+    h = np.stack(p.g.fieldArrays("Dipole"))
+    ref = p.o.field("Dipole")
+    assert float(np.linalg.norm(h - ref) / np.linalg.norm(ref)) <= 1e-5
+
+
+def test_wide_plane_steps_match_calls_and_oracle(M):
+    dims = (32, 256, 4)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 48, deg=20.0)
+    out = []
+    for mode in ("calls", "run"):
+        ss, ops, l = build(M, dims, s0, llg="Quaternion", T=0.0)
+        if mode == "calls":
+            calls(ss, ops, l, 6)
+        else:
+            M.run(ss, ops, l, 6)
+        out.append(state(ss))
+    assert_same(out[0], out[1])
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s0)
+    o.alpha, o.dt = 0.05, 0.005
+    f, t, j = O.nn_paths(*dims, pbc=(1, 1, 0))
+    sites = np.arange(n, dtype=np.int32)
+    lr = O.LongRange(*dims, O.dipole_tensor(*dims))
+    O.run_steps(o, 6, paths=(f, t, j), ani=(sites, np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.05)),
+                B=(0.1, 0, 0.02), lr=lr, g=0.03, llg="Quaternion")
+    assert float(np.abs(out[1][0] - o.spins()).max()) < 1e-6
