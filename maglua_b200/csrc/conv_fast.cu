@@ -439,7 +439,7 @@ __device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int N
 }
 
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __restrict__ sx, const float* __restrict__ sy,
+__global__ void __launch_bounds__(256) k_fused_fast(FastK F0, const float* __restrict__ sx, const float* __restrict__ sy,
                                                     const float* __restrict__ sz, const float* __restrict__ ax,
                                                     const float* __restrict__ ay, const float* __restrict__ az,
                                                     float* __restrict__ ox, float* __restrict__ oy,
@@ -448,7 +448,8 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastK F, const float* __rest
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
-    if (x >= F.nx || y >= F.ny) return;
+    if (x >= F0.nx || y >= F0.ny) return;
+    const FastK F = fastk_resolved(F0);
     const int i = x + F.nx * (y + F.ny * z);
     fused_site<LT, EXS, ANI, TH, ADD>(F, F.nx, F.ny, F.nz, x, y, z, i, sx, sy, sz, ax, ay, az, ox, oy, oz);
 }
@@ -484,7 +485,7 @@ struct XSCfg {
 };
 
 template <int PX, int LT, bool EXS, bool ANI, bool TH>
-__global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, const float2* __restrict__ tw,
+__global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, const float2* __restrict__ tw,
                                                   float2* __restrict__ spec, const float* __restrict__ sx,
                                                   const float* __restrict__ sy, const float* __restrict__ sz,
                                                   float* __restrict__ hx, float* __restrict__ hy,
@@ -505,6 +506,7 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F, int fwd, con
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
+    const FastK F = fastk_resolved(F0);
     // 1. spectrum rows SPEC[kx][comp][row0 + row] -> B[(comp ROWS + row) KX + kx]
     constexpr int IS = (X::SPEC + NT - 1) / NT;
     {

@@ -8,6 +8,22 @@
 #include <math.h>
 #include <stdint.h>
 
+// The step block's per-step values (swept field, thermal counter) read once
+// per thread instead of once per site: the same values, so the same results.
+__device__ __forceinline__ FastK fastk_resolved(const FastK& F)
+{
+    FastK G = F;
+    if (F.Bdev) {
+        G.B[0] = (float)F.Bdev[0]; G.B[1] = (float)F.Bdev[1]; G.B[2] = (float)F.Bdev[2];
+        G.Bdev = nullptr;
+    }
+    if (F.dctr) {
+        G.counter = F.counter + *F.dctr;
+        G.dctr = nullptr;
+    }
+    return G;
+}
+
 // ------------------------------------------------------------------ fused step
 // Uniform-parameter systems: ms, alpha, gamma, anisotropy and thermal scale
 // the same on every site, exchange as a six-direction stencil.  Constants
