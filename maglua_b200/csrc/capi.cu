@@ -211,6 +211,13 @@ struct mlb_system {
     cudaStream_t own = nullptr;
     cudaStream_t st = nullptr;
     DevStep* dstep = nullptr;       // device step block (captured steps)
+    DevStep dstep_mirror{};         // what the device block holds, when dstep_known
+    bool dstep_known = false;
+    // netMoment: reduction + copy to pinned memory captured once per spin
+    // buffer (and per length argument m)
+    cudaGraphExec_t nm_exec[2] = {nullptr, nullptr};
+    double nm_m[2] = {0.0, 0.0};
+    double* nm_host = nullptr;      // pinned, 6 doubles
     double* red = nullptr;
     double* redout = nullptr;
     int red_nb = 1;
@@ -1350,6 +1357,7 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     s->ms_dirty = true;
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
+    CK(cudaMallocHost(&s->nm_host, sizeof(double) * 6));
     s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
     CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
     CK(cudaMalloc(&s->redout, sizeof(double) * 8));
@@ -1370,6 +1378,9 @@ void free_system(mlb_system* s)
     cudaFree(s->sa);
     cudaFree(s->sg);
     cudaFree(s->dstep);
+    for (int q = 0; q < 2; q++)
+        if (s->nm_exec[q]) cudaGraphExecDestroy(s->nm_exec[q]);
+    cudaFreeHost(s->nm_host);
     cudaFree(s->red);
     cudaFree(s->redout);
     for (Slot& x : s->slots)
@@ -1576,7 +1587,19 @@ void plan_launch(mlb_plan* p, int nsteps)
         if (o->kind == MLB_OP_APPLIEDFIELD)
             for (int a = 0; a < 3; a++) { h.B[a] = o->B[a] * o->gs; h.dB[a] = o->dB[a] * o->gs; }
     }
-    CK(cudaMemcpyAsync(s->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
+    // upload only what the device block does not already hold (consecutive
+    // launches: the steps advanced it exactly as the host mirror below)
+    if (!s->dstep_known || memcmp(&h, &s->dstep_mirror, sizeof(h)) != 0) {
+        // (a pageable source is staged before cudaMemcpyAsync returns)
+        CK(cudaMemcpyAsync(s->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
+        s->dstep_mirror = h;
+    }
+    // the device advances the block once per step (k_advance_step)
+    for (int k = 0; k < nsteps; k++) {
+        s->dstep_mirror.th_counter += 1ull;
+        for (int a = 0; a < 3; a++) s->dstep_mirror.B[a] += s->dstep_mirror.dB[a];
+    }
+    s->dstep_known = true;
     ConvPlan* CP = p->carry_op ? p->carry_op->plan.get() : nullptr;
     for (int k = 0; k < nsteps; k++) {
         const bool carry = CP && s->spec_token != 0 && s->spec_token == CP->spec_token;
@@ -2168,11 +2191,31 @@ int mlb_system_ensure_slot(mlb_system* s, const char* slot)
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8])
 {
     return guard([&] {
-        CK(mlb::launch_netmoment(s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2], s->n, m, s->red, s->red_nb,
-                                 s->redout, s->rb, s->st));
-        double r[6];
-        CK(cudaMemcpyAsync(r, s->redout, sizeof(r), cudaMemcpyDeviceToHost, s->st));
+        const int q = s->cur;
+        if (!s->nm_exec[q] || s->nm_m[q] != m) {
+            // capture the reduction and the copy to pinned memory once
+            if (s->nm_exec[q]) { cudaGraphExecDestroy(s->nm_exec[q]); s->nm_exec[q] = nullptr; }
+            CK(cudaStreamSynchronize(s->st));
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = mlb::launch_netmoment(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, s->red, s->red_nb,
+                                                  s->redout, s->rb, s->st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(s->nm_host, s->redout, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->st);
+            cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
+            if (e == cudaSuccess) e = e2;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&s->nm_exec[q], g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                fail(MLB_ECUDA, std::string("netMoment graph: ") + cudaGetErrorString(e));
+            }
+            s->nm_m[q] = m;
+        }
+        CK(cudaGraphLaunch(s->nm_exec[q], s->st));
         CK(cudaStreamSynchronize(s->st));
+        double r[6];
+        for (int k = 0; k < 6; k++) r[k] = s->nm_host[k];
         out8[0] = r[0]; out8[1] = r[1]; out8[2] = r[2];
         out8[3] = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
         out8[4] = r[3]; out8[5] = r[4]; out8[6] = r[5];
