@@ -422,14 +422,22 @@ __global__ void __launch_bounds__(256) k_netmoment_partial(const void* x_, const
     }
 }
 
-// out[q] = sum_b part[b*nq + q], fixed order (deterministic).
-__global__ void k_partial_final(const double* part, int nb, int nq, double* out)
+// out[q] = sum_b part[b*nq + q]: block q (256 threads), thread t sums
+// b = t, t + 256, ... in order, then a fixed shuffle and warp tree
+// (deterministic, independent of timing).
+__global__ void __launch_bounds__(256) k_partial_final(const double* part, int nb, int nq, double* out)
 {
-    const int q = threadIdx.x;
-    if (q < nq) {
-        double v = 0;
-        for (int b = 0; b < nb; b++) v += part[b * nq + q];
-        out[q] = v;
+    const int q = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ double sh[8];
+    double v = 0;
+    for (int b = threadIdx.x; b < nb; b += 256) v += part[b * nq + q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int k = 0; k < 8; k++) s += sh[k];
+        out[q] = s;
     }
 }
 
@@ -1038,7 +1046,7 @@ cudaError_t launch_advance_step(DevStep* d, cudaStream_t st)
 
 cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st)
 {
-    k_partial_final<<<1, 32, 0, st>>>(part, nb, nq, out);
+    k_partial_final<<<nq, 256, 0, st>>>(part, nb, nq, out);
     return cudaGetLastError();
 }
 
@@ -1047,7 +1055,7 @@ cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n,
 {
     if (rb == 8) k_netmoment_partial<double><<<nb, 256, 0, st>>>(x, y, z, n, m, part);
     else k_netmoment_partial<float><<<nb, 256, 0, st>>>(x, y, z, n, m, part);
-    k_partial_final<<<1, 32, 0, st>>>(part, nb, 6, out);
+    k_partial_final<<<6, 256, 0, st>>>(part, nb, 6, out);
     return cudaGetLastError();
 }
 
@@ -1056,7 +1064,7 @@ cudaError_t launch_dot(const void* const s[3], const void* const h[3], int n, do
 {
     if (rb == 8) k_dot_partial<double><<<nb, 256, 0, st>>>(s[0], s[1], s[2], h[0], h[1], h[2], n, part);
     else k_dot_partial<float><<<nb, 256, 0, st>>>(s[0], s[1], s[2], h[0], h[1], h[2], n, part);
-    k_partial_final<<<1, 32, 0, st>>>(part, nb, 1, out);
+    k_partial_final<<<1, 256, 0, st>>>(part, nb, 1, out);
     return cudaGetLastError();
 }
 
