@@ -269,6 +269,21 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
  * issuing those calls one by one. */
 int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
 
+/* ---------------------------------------------------------------- Runge-Kutta integrators
+ * Replaces the script M/common/scripts/RungeKutta.lua:57-215
+ * (make_rk_step_function(ss, type, {ops}, llg, temp) and its step function):
+ * type is one of "RK1", "RK2", "K3", "RK4", "RK3", "RK4_38", "RK6", "BS3"
+ * (the script's Butcher tables; another name is MLB_EINVAL with the script's
+ * message).  ops make the deterministic field (resetFields, apply each,
+ * sumFields); temp (may be NULL) is a Thermal operator applied after the
+ * stages with llg:apply(ss, false).  The stage systems are copies of ss made
+ * here (fields included), on ss's stream.  mlb_rk_step runs nsteps steps. */
+typedef struct mlb_rk mlb_rk;
+int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops, mlb_llg* l, mlb_op* temp,
+                  mlb_rk** out);
+int mlb_rk_step(mlb_rk* r, int nsteps);
+int mlb_rk_destroy(mlb_rk* r);
+
 /* ---------------------------------------------------------------- learned dipolar surrogate
  * B200 extension, no counterpart in the reference.  A linear spectral-conv
  * network on the in-plane grid, with the (component, z) pairs as 3*nz

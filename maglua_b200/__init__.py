@@ -133,6 +133,9 @@ _SIGS = {
     "mlb_surrogate_stats": ([_P, C.POINTER(C.c_longlong), _D], C.c_int),
     "mlb_surrogate_forward": ([_P, C.POINTER(_F), C.POINTER(_F)], C.c_int),
     "mlb_surrogate_gradients": ([_P, C.POINTER(_F), C.POINTER(_F), _F, _F, C.POINTER(_F), _D], C.c_int),
+    "mlb_rk_create": ([_P, C.c_char_p, C.POINTER(_P), C.c_int, _P, _P, C.POINTER(_P)], C.c_int),
+    "mlb_rk_step": ([_P, C.c_int], C.c_int),
+    "mlb_rk_destroy": ([_P], C.c_int),
     "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
     "mlb_plan_kernel_times": ([_P, C.c_int, C.c_char_p, _D, _I], C.c_int),
@@ -1201,6 +1204,33 @@ class Surrogate:
         b = C.c_double()
         _ck(_lib.mlb_surrogate_stats(self._h, out, C.byref(b)))
         return {"exact": out[0], "surrogate": out[1], "failed": out[2], "last_bound": b.value}
+
+
+class RungeKutta:
+    """make_rk_step_function(ss, type, {ops}, llg, temp) of the reference's
+    RungeKutta.lua, run natively: step(n) advances ss by n steps of the
+    Butcher scheme `kind` (RK1, RK2, K3, RK4, RK3, RK4_38, RK6, BS3) with the
+    field of ops and the optional Thermal operator temp applied after the
+    stages."""
+
+    def __init__(self, ss, kind, ops, llg, temp=None):
+        arr = (_P * len(ops))(*[o._h for o in ops])
+        h = _P()
+        _ck(_lib.mlb_rk_create(ss._h, kind.encode(), arr, len(ops), llg._h, temp._h if temp is not None else None,
+                               C.byref(h)))
+        self._h = h
+        self._keep = (ss, list(ops), llg, temp)
+
+    def step(self, n=1):
+        _ck(_lib.mlb_rk_step(self._h, int(n)))
+
+    __call__ = step
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.mlb_rk_destroy(h)
+            self._h = None
 
 
 def run(ss, ops, llg, nsteps):

@@ -3022,6 +3022,144 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
 
 } // extern "C"
 
+// ---------------------------------------------------------------- Runge-Kutta integrators
+// The reference's make_rk_step_function (M/common/scripts/RungeKutta.lua:
+// 57-215) as native host code over the same operations: per step the field
+// of the base system, one stage system per Butcher row (a copy of the base
+// system, RungeKutta.lua:182-185), each row applied as a chain of
+// llg:apply(src, factor, dmdt, dst) calls (istep, :186-193), and the optional
+// thermal kick llg:apply(ss, false) (:206-211).  Every call is the library's
+// own entry (op_apply, llg_apply), so the time bookkeeping and the arithmetic
+// are those of the scripted loop.
+struct mlb_rk {
+    mlb_system* ss = nullptr;
+    std::vector<mlb_system*> k;          // stage systems 2..nstep (owned)
+    std::vector<mlb_op*> ops;            // the deterministic field: resetFields, apply each, sumFields
+    mlb_llg* l = nullptr;
+    mlb_op* temp = nullptr;              // optional Thermal operator
+    std::vector<std::vector<double>> bt; // Butcher rows (the c column is not used)
+};
+
+namespace {
+
+bool rk_table(const std::string& name, std::vector<std::vector<double>>& bt)
+{
+    // RungeKutta.lua:100-158
+    if (name == "RK1") bt = {{1.0}};
+    else if (name == "RK2") bt = {{0.5}, {0.0, 1.0}};
+    else if (name == "K3") bt = {{0.5}, {-1.0, 2.0}, {1.0 / 6, 2.0 / 3, 1.0 / 6}};
+    else if (name == "RK4") bt = {{0.5}, {0.0, 0.5}, {0.0, 0.0, 1.0}, {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6}};
+    else if (name == "RK3") bt = {{1.0 / 3}, {0.0, 2.0 / 3}, {0.25, 0.0, 0.75}};
+    else if (name == "RK4_38") bt = {{1.0 / 3}, {-1.0 / 3, 1.0}, {1.0, -1.0, 1.0}, {1.0 / 8, 3.0 / 8, 3.0 / 8, 1.0 / 8}};
+    else if (name == "RK6")
+        bt = {{1.0 / 3},
+              {0.0, 2.0 / 3},
+              {1.0 / 12, 4.0 / 12, -1.0 / 12},
+              {-1.0 / 16, 18.0 / 16, -3.0 / 16, -6.0 / 16},
+              {0.0, 9.0 / 8, -3.0 / 8, -6.0 / 8, 4.0 / 8},
+              {9.0 / 44, -36.0 / 44, 63.0 / 44, 72.0 / 44, 0.0, -64.0 / 44},
+              {11.0 / 120, 0.0, 81.0 / 120, 81.0 / 120, -32.0 / 120, -32.0 / 120, 11.0 / 120}};
+    else if (name == "BS3") bt = {{0.5}, {0.0, 0.75}, {2.0 / 9, 1.0 / 3, 4.0 / 9}, {7.0 / 24, 0.25, 1.0 / 3, 1.0 / 8}};
+    else return false;
+    return true;
+}
+
+void rk_field(mlb_rk* r, mlb_system* s)
+{
+    reset_fields(s);
+    for (mlb_op* op : r->ops) op_apply(op, s);
+    sum_fields(s);
+}
+
+// istep (RungeKutta.lua:186-193): one Butcher row into dst
+void rk_row(mlb_rk* r, mlb_system* src, const std::vector<double>& f, mlb_system* dst)
+{
+    const int nstep = (int)r->bt.size();
+    llg_apply(r->l, src, f[0], src, dst, 1);
+    for (int i = 2; i <= nstep; i++)
+        if (i <= (int)f.size() && f[i - 1] != 0.0) llg_apply(r->l, dst, f[i - 1], r->k[i - 2], dst, 1);
+}
+
+// sfunc (RungeKutta.lua:194-213)
+void rk_step(mlb_rk* r)
+{
+    const int nstep = (int)r->bt.size();
+    mlb_system* ss = r->ss;
+    rk_field(r, ss);
+    for (int i = 1; i <= nstep - 1; i++) {
+        mlb_system* d = r->k[i - 1];   // ss_k[i+1]
+        d->dt = ss->dt;
+        rk_row(r, ss, r->bt[i - 1], d);
+        rk_field(r, d);
+    }
+    rk_row(r, ss, r->bt[nstep - 1], ss);
+    if (r->temp) {
+        reset_fields(ss);
+        op_apply(r->temp, ss);
+        sum_fields(ss);
+        llg_apply(r->l, ss, 1.0, ss, ss, 0);
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops, mlb_llg* l, mlb_op* temp,
+                  mlb_rk** out)
+{
+    return guard([&] {
+        if (!ss || !l || !out || !type || (nops > 0 && !ops)) fail(MLB_EINVAL, "null argument");
+        std::unique_ptr<mlb_rk> r(new mlb_rk());
+        if (!rk_table(type, r->bt))
+            fail(MLB_EINVAL, "RK type must be one of \"RK1\", \"RK2\", \"K3\", \"RK4\", \"RK3\", \"RK4_38\", \"RK6\", \"BS3\"");
+        for (int i = 0; i < nops; i++) {
+            check_dims(ops[i], ss);
+            r->ops.push_back(ops[i]);
+        }
+        if (temp) {
+            if (temp->kind != MLB_OP_THERMAL) fail(MLB_EINVAL, "the optional operator must be a Thermal");
+            check_dims(temp, ss);
+        }
+        r->ss = ss;
+        r->l = l;
+        r->temp = temp;
+        // stage systems: copies of the base system on its stream (ss_k[i] = ss_k[1]:copy())
+        const int nstep = (int)r->bt.size();
+        try {
+            for (int i = 2; i <= nstep; i++) {
+                mlb_system* c = make_system(ss->nx, ss->ny, ss->nz, ss->rb);
+                r->k.push_back(c);
+                int rc = mlb_system_copy(c, ss, 1);
+                if (rc) fail(rc, g_err);
+                c->st = ss->st;
+            }
+        } catch (...) {
+            for (mlb_system* c : r->k) free_system(c);
+            throw;
+        }
+        *out = r.release();
+    });
+}
+
+int mlb_rk_step(mlb_rk* r, int nsteps)
+{
+    return guard([&] {
+        for (int k = 0; k < nsteps; k++) rk_step(r);
+    });
+}
+
+int mlb_rk_destroy(mlb_rk* r)
+{
+    return guard([&] {
+        if (!r) return;
+        for (mlb_system* c : r->k) free_system(c);
+        delete r;
+    });
+}
+
+} // extern "C"
+
 // ---------------------------------------------------------------- learned surrogate
 struct mlb_surrogate {
     mlb_op* op = nullptr;

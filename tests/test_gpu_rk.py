@@ -1,0 +1,125 @@
+"""Runge-Kutta integrators (mlb_rk_*) against the reference script they
+replace, M/common/scripts/RungeKutta.lua:57-215 (make_rk_step_function and
+its step function), restated below in Python over the FP64 oracle's own
+operators and LLG (llg:apply(src, factor, dmdt, dst) with the reference's
+argument meaning).  Fields ≤ 1e-5, so a short FP32 trajectory stays within
+1e-5 of the FP64 one; the time bookkeeping must agree exactly."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import Pair, tilted_spins
+
+pytestmark = pytest.mark.gpu
+
+# RungeKutta.lua:100-158 (the c column is not used by the script)
+BUTCHER = {
+    "RK1": [[1.0]],
+    "RK2": [[0.5], [0.0, 1.0]],
+    "K3": [[0.5], [-1.0, 2.0], [1 / 6, 2 / 3, 1 / 6]],
+    "RK4": [[0.5], [0.0, 0.5], [0.0, 0.0, 1.0], [1 / 6, 1 / 3, 1 / 3, 1 / 6]],
+    "RK3": [[1 / 3], [0.0, 2 / 3], [0.25, 0.0, 0.75]],
+    "RK4_38": [[1 / 3], [-1 / 3, 1.0], [1.0, -1.0, 1.0], [1 / 8, 3 / 8, 3 / 8, 1 / 8]],
+    "RK6": [[1 / 3], [0.0, 2 / 3], [1 / 12, 4 / 12, -1 / 12], [-1 / 16, 18 / 16, -3 / 16, -6 / 16],
+            [0.0, 9 / 8, -3 / 8, -6 / 8, 4 / 8], [9 / 44, -36 / 44, 63 / 44, 72 / 44, 0.0, -64 / 44],
+            [11 / 120, 0.0, 81 / 120, 81 / 120, -32 / 120, -32 / 120, 11 / 120]],
+    "BS3": [[0.5], [0.0, 0.75], [2 / 9, 1 / 3, 4 / 9], [7 / 24, 0.25, 1 / 3, 1 / 8]],
+}
+
+
+@pytest.fixture(scope="module")
+def M():
+    import maglua_b200 as M
+    M.init(0)
+    return M
+
+
+def oracle_copy(o):
+    c = O.SpinSystem(o.nx, o.ny, o.nz)
+    c.set_spins(*o.spins())
+    c.alpha, c.gamma, c.dt, c.time = o.alpha, o.gamma, o.dt, o.time
+    return c
+
+
+def oracle_rk_steps(p, kind, llg, nsteps):
+    """make_rk_step_function(ss, kind, field, llg) and nsteps calls of the
+    step function, on the oracle system p.o."""
+    bt = BUTCHER[kind]
+    nstep = len(bt)
+    ss = p.o
+    k = [ss] + [oracle_copy(ss) for _ in range(nstep - 1)]
+
+    def field(s):
+        s.reset_fields()
+        for f in p.oapply:
+            f(s)
+        s.sum_fields()
+
+    def istep(src, factors, dst):
+        llg.apply(src, factors[0], src, dst)
+        for i in range(2, nstep + 1):
+            if i <= len(factors) and factors[i - 1] != 0:
+                llg.apply(dst, factors[i - 1], k[i - 1], dst)
+
+    for _ in range(nsteps):
+        field(ss)
+        for i in range(1, nstep):
+            k[i].dt = ss.dt
+            istep(ss, bt[i - 1], k[i])
+            field(k[i])
+        istep(ss, bt[nstep - 1], ss)
+
+
+@pytest.mark.parametrize("kind,llg", [("RK1", "Cartesian"), ("RK2", "Quaternion"), ("K3", "Cartesian"),
+                                      ("RK3", "Quaternion"), ("RK4", "Quaternion"), ("RK4", "Cartesian"),
+                                      ("RK4_38", "Cartesian"), ("RK6", "Quaternion"), ("BS3", "Quaternion")])
+def test_rk_matches_oracle(M, kind, llg):
+    dims = (16, 12, 2)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 70, deg=25.0)
+    p = Pair(*dims, s0, alpha=0.1, dt=0.02)
+    p.exchange(J=1.0, pbc=(1, 1, 0))
+    p.anisotropy(axis=(0, 0, 1), K=0.1)
+    p.zeeman((0.05, 0.0, 0.02))
+    p.dipole(g=0.05)
+    rk = M.RungeKutta(p.g, kind, p.ops, M.LLG.new(llg))
+    rk.step(4)
+    rk.step(6)
+    oracle_rk_steps(p, kind, O.LLG(llg), 10)
+    got = np.stack(p.g.spinArrays()[:3])
+    err = float(np.abs(got - p.o.spins()).max())
+    assert err < 1e-5, err
+    assert p.g.time() == pytest.approx(p.o.time, rel=1e-12, abs=1e-12)
+
+
+def test_rk_thermal_kick_keeps_unit_spins(M):
+    """The optional thermal step (RungeKutta.lua:206-211): llg:apply(ss, false)
+    after the stages leaves the time unadvanced by the kick and the spins
+    normalised."""
+    dims = (32, 16, 1)
+    n = int(np.prod(dims))
+    out = []
+    for T in (0.2, None):
+        ss = M.SpinSystem(*dims)
+        ss.setSpinArrays(*tilted_spins(n, 71))
+        ss.setAlpha(0.1)
+        ss.setTimeStep(0.01)
+        ex = M.Exchange(ss)
+        ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 1)))
+        th = None
+        if T is not None:
+            th = M.Thermal(ss, M.Random.Philox(3))
+            th.setTemperature(T)
+        rk = M.RungeKutta(ss, "RK4", [ex], M.LLG.new("Quaternion"), temp=th)
+        rk.step(20)
+        x, y, z, _ = ss.spinArrays()
+        assert np.allclose(np.sqrt(x * x + y * y + z * z), 1.0, atol=1e-5)
+        assert ss.time() == pytest.approx(20 * 0.01, rel=1e-12)
+        out.append(np.stack([x, y, z]))
+    assert np.abs(out[0] - out[1]).max() > 1e-3   # the kicks moved the spins
+
+
+def test_rk_rejects_unknown_scheme(M):
+    ss = M.SpinSystem(4, 4, 1)
+    with pytest.raises(M.MagLuaError, match="RK type must be one of"):
+        M.RungeKutta(ss, "RK5", [], M.LLG.new("Cartesian"))
