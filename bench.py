@@ -190,6 +190,31 @@ def run_surrogate(M, torch, steps, flush_l2=None):
     return out
 
 
+# ----------------------------------------------------------------- Runge-Kutta
+def run_rk(M, torch, steps=20):
+    """The 256x256x8 film stepped by the native RK4 scheme (RungeKutta.lua's
+    make_rk_step_function with the deterministic operators as the field and
+    the Thermal operator as the kick): spin-steps/s of full RK4 steps (four
+    field evaluations each)."""
+    ss, ops, _ = build_system(M, 0)
+    th = [o for o in ops if isinstance(o, M.Thermal)][0]
+    det = [o for o in ops if o is not th]
+    rk = M.RungeKutta(ss, "RK4", det, M.LLG.new("Quaternion"), temp=th)
+    rk.step(3)
+    st = torch.cuda.ExternalStream(ss.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ss.synchronize()
+    a.record(st)
+    rk.step(steps)
+    b.record(st)
+    ss.synchronize()
+    ms = a.elapsed_time(b) / steps
+    n = NX * NY * NZ
+    return {"workload": WORKLOAD.replace("LLG.Quaternion", "RK4 (LLG.Quaternion stages) + thermal kick"),
+            "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "how": "mlb_rk_step: eager launches (no graph capture), L2 not flushed"}
+
+
 # ----------------------------------------------------------------- 256^3 open cube
 CUBE_DIMS = (256, 256, 256)
 CUBE_WORKLOAD = ("256^3 simple-cubic cube, open boundaries (512^3 padded transform, split (y,z) passes), "
@@ -529,6 +554,7 @@ def main():
     batched = run_batched(M, torch, args.steps, args.warmup)
     surrogate = run_surrogate(M, torch, min(args.steps, 200)) if not args.no_surrogate else None
     cube = run_cube(M, torch) if not args.no_cube else None
+    rk = run_rk(M, torch)
 
     if rank != 0:
         if dist:
@@ -584,6 +610,7 @@ def main():
         "batched_ensemble": batched,
         "surrogate": surrogate,
         "cube_256": cube,
+        "rk4": rk,
     }
     print(json.dumps(line), flush=True)
     if dist:

@@ -202,6 +202,9 @@ struct mlb_system {
     void* ms = nullptr;
     std::vector<double> ms_host;    // ms as stored on the device (rounded to rb)
     bool ms_dirty = true;
+    // identifies the moment magnitudes held (device ms and ms_host): equal
+    // tokens, equal magnitudes; a new one whenever they are set
+    unsigned long long ms_token = 0;
     bool ms_uniform = true;
     double ms_u = 0.0;
     void* sa = nullptr;
@@ -310,6 +313,7 @@ struct mlb_plan {
 namespace {
 
 std::set<mlb_system*> g_systems;
+unsigned long long g_ms_token = 0;
 unsigned long long g_spec_token = 0;
 // bumped by every parameter setter; a plan captured under an older value
 // is captured again before its next launch
@@ -1277,10 +1281,13 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
         // the destination's spins change in place: settle its lazy fields
         materialize_all(to);
         if (to != dmdt) { materialize(dmdt, 0); if (th >= 0) materialize(dmdt, th); }
-        if (from != to && !(cart && dt == 0.0)) {
+        if (from != to && !(cart && dt == 0.0) && to->ms_token != from->ms_token) {
+            // the new spins carry the source's magnitudes (skipped when the
+            // destination already holds them, e.g. the copies of RK stages)
             CK(cudaMemcpyAsync(to->ms, from->ms, (size_t)from->rb * from->n, cudaMemcpyDeviceToDevice, to->st));
             to->ms_host = from->ms_host;
             to->ms_dirty = true;
+            to->ms_token = from->ms_token;
         }
         if (from->st != to->st || dmdt->st != to->st) {
             CK(cudaStreamSynchronize(from->st));
@@ -1355,6 +1362,7 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     CK(cudaMemset(s->ms, 0, (size_t)rb * n));
     s->ms_host.assign(n, 0.0);
     s->ms_dirty = true;
+    s->ms_token = ++g_ms_token;
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
     CK(cudaMallocHost(&s->nm_host, sizeof(double) * 6));
@@ -1953,6 +1961,7 @@ int mlb_system_set_spin(mlb_system* s, int idx, double sx, double sy, double sz)
         put_reals(s, elem(s->ms, idx, s->rb), &m, 1);
         s->ms_host[idx] = round_to(m, s->rb);
         s->ms_dirty = true;
+        s->ms_token = ++g_ms_token;
         CK(cudaStreamSynchronize(s->st));
     });
 }
@@ -1979,6 +1988,7 @@ int mlb_system_set_spins(mlb_system* s, const double* x, const double* y, const 
         put_reals(s, s->ms, s->ms_host.data(), s->n);
         for (int i = 0; i < s->n; i++) s->ms_host[i] = round_to(s->ms_host[i], s->rb);
         s->ms_dirty = true;
+        s->ms_token = ++g_ms_token;
         CK(cudaStreamSynchronize(s->st));
     });
 }
@@ -2015,9 +2025,12 @@ int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const f
                 put_reals(s, s->ms, d.data(), s->n);
             }
         }
-        if (ms)
+        if (ms) {
+            bool changed = false;
             for (int i = 0; i < s->n; i++)
-                if (s->ms_host[i] != (double)ms[i]) { s->ms_host[i] = ms[i]; s->ms_dirty = true; }
+                if (s->ms_host[i] != (double)ms[i]) { s->ms_host[i] = ms[i]; changed = true; }
+            if (changed) { s->ms_dirty = true; s->ms_token = ++g_ms_token; }
+        }
     });
 }
 
@@ -2252,6 +2265,7 @@ int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
         CK(cudaMemcpyAsync(dst->ms, src->ms, bytes, cudaMemcpyDeviceToDevice, dst->st));
         dst->ms_host = src->ms_host;
         dst->ms_dirty = true;
+        dst->ms_token = src->ms_token;
         dst->alpha = src->alpha; dst->gamma = src->gamma; dst->dt = src->dt; dst->time = src->time;
         CK(cudaStreamSynchronize(dst->st));
         upload_site_array(dst, &dst->sa, nullptr);

@@ -313,9 +313,9 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, YZT<PY, PZ>::MINB) k_yz_fast(C
 // z transforms in registers, data layers back to P.  The inverse y transforms
 // read P and store the data rows straight to SPEC.  Shared-memory traffic is
 // about a third of the Stockham form's, with no z-spectrum buffer.
-template <int PY, int PZ>
+template <int PY, int PZ, int NTH = 384>
 struct YZR {
-    static constexpr int NT = 384;
+    static constexpr int NT = NTH;
     static constexpr int T = fr::Split<PY>::T;
     static constexpr int E = fr::Split<PY>::E;
     static constexpr int LPR = NT / T;                  // lines per round
@@ -323,11 +323,12 @@ struct YZR {
     static size_t smem(int nz) { return ((size_t)3 * nz * PY + (size_t)LPR * EX + PY) * sizeof(float2); }
 };
 
-template <int PY, int PZ>
-__global__ void __launch_bounds__(384, 1) k_yz_reg(ConvK c, const float2* __restrict__ twy,
-                                                   float2* __restrict__ spec, const float* __restrict__ ten6)
+template <int PY, int PZ, int NTH>
+__global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, const float2* __restrict__ twy,
+                                                                    float2* __restrict__ spec,
+                                                                    const float* __restrict__ ten6)
 {
-    using Y = YZR<PY, PZ>;
+    using Y = YZR<PY, PZ, NTH>;
     constexpr int NT = Y::NT, T = Y::T, E = Y::E;
     extern __shared__ float2 sm[];
     const int kx = blockIdx.x;
@@ -346,7 +347,8 @@ __global__ void __launch_bounds__(384, 1) k_yz_reg(ConvK c, const float2* __rest
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
-    float2* sp = spec + (size_t)kx * nlines * ny;
+    // replica blockIdx.y of a packed size class (one for a single film)
+    float2* sp = spec + (size_t)blockIdx.y * c.Kx * nlines * ny + (size_t)kx * nlines * ny;
     __syncthreads();
     const int lr = threadIdx.x / T, t = threadIdx.x % T;
     const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << (((threadIdx.x & 31) / T) * T));
@@ -644,12 +646,20 @@ namespace mlb {
 
 static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
-// the register (y,z) kernel: a single film's planes of width 256 or 512,
-// z padded to at most 16, and the plane in shared memory
+// the register (y,z) kernel: planes of width 64 to 512 with z padded to at
+// most 16 and the plane in shared memory (384 threads for a film's 256- and
+// 512-wide planes, 128 for the small planes of packed replicas)
 static bool yz_reg_ok(int PY, int PZ, const ConvK& c)
 {
-    if (c.nrep != 1 || (PY != 256 && PY != 512) || PZ > 16) return false;
-    const size_t sm = PY == 256 ? YZR<256, 16>::smem(c.nz) : YZR<512, 16>::smem(c.nz);
+    if (PZ > 16) return false;
+    size_t sm;
+    switch (PY) {
+    case 64: sm = YZR<64, 16, 128>::smem(c.nz); break;
+    case 128: sm = YZR<128, 16, 128>::smem(c.nz); break;
+    case 256: sm = YZR<256, 16, 384>::smem(c.nz); break;
+    case 512: sm = YZR<512, 16, 384>::smem(c.nz); break;
+    default: return false;
+    }
     return sm <= 227 * 1024;
 }
 
@@ -712,9 +722,16 @@ static cudaError_t launch_x_any(const ConvK& c, const float2* tw, const float* s
 template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
-    if (yz_reg_ok(PY, PZ, c)) {
-        return launch_pdl(k_yz_reg<(PY >= 256 ? PY : 256), (PZ <= 16 ? PZ : 16)>, dim3(c.Kx), dim3(384),
-                          YZR<(PY >= 256 ? PY : 256), (PZ <= 16 ? PZ : 16)>::smem(c.nz), st, c, twy, spec, ten6);
+    constexpr int RPZ = PZ <= 16 ? PZ : 16;
+    if constexpr (PY >= 256) {
+        if (yz_reg_ok(PY, PZ, c))
+            return launch_pdl(k_yz_reg<PY, RPZ, 384>, dim3(c.Kx, c.nrep), dim3(384), YZR<PY, RPZ, 384>::smem(c.nz), st,
+                              c, twy, spec, ten6);
+    } else if constexpr (PY >= 64) {
+        // small planes (packed replicas): 128-thread CTAs, several per SM
+        if (yz_reg_ok(PY, PZ, c))
+            return launch_pdl(k_yz_reg<PY, RPZ, 128>, dim3(c.Kx, c.nrep), dim3(128), YZR<PY, RPZ, 128>::smem(c.nz), st,
+                              c, twy, spec, ten6);
     }
     const size_t smem = yz_fast_smem(PY, PZ, c.nz);
     return launch_pdl(k_yz_fast<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZT<PY, PZ>::N), smem, st, c, twy, spec, ten6);
@@ -776,16 +793,16 @@ static cudaError_t cfg_yz()
 template <int PX>
 static cudaError_t cfg_xs();
 
-template <int PY>
+template <int PY, int NTH>
 static cudaError_t cfg_yzr()
 {
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 1>, a, 227 * 1024)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 2>, a, 227 * 1024)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 4>, a, 227 * 1024)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 8>, a, 227 * 1024)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_yz_reg<PY, 16>, a, 227 * 1024);
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 1, NTH>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 2, NTH>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 4, NTH>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_reg<PY, 8, NTH>, a, 227 * 1024)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_yz_reg<PY, 16, NTH>, a, 227 * 1024);
 }
 
 cudaError_t conv_fast_configure()
@@ -799,7 +816,8 @@ cudaError_t conv_fast_configure()
         return e;
     if ((e = cfg_xs<32>()) || (e = cfg_xs<64>()) || (e = cfg_xs<128>()) || (e = cfg_xs<256>()) || (e = cfg_xs<512>()))
         return e;
-    if ((e = cfg_yzr<256>()) || (e = cfg_yzr<512>())) return e;
+    if ((e = cfg_yzr<64, 128>()) || (e = cfg_yzr<128, 128>()) || (e = cfg_yzr<256, 384>()) || (e = cfg_yzr<512, 384>()))
+        return e;
     return cudaSuccess;
 }
 
