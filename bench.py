@@ -424,14 +424,46 @@ def main():
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 open-cube precision study")
     ap.add_argument("--ncu-steps", type=int, default=0,
                     help="profiling driver: run this many eager steps of the workload and exit (for ncu)")
+    ap.add_argument("--ncu-surrogate", type=int, default=0,
+                    help="profiling driver: this many surrogate steps on the 512x512x4 film (small random "
+                         "network weights, every step after the first a surrogate step) and exit")
+    ap.add_argument("--ncu-ensemble", type=int, default=0,
+                    help="profiling driver: this many captured steps of the packed ensemble and exit")
     args = ap.parse_args()
-    if args.ncu_steps:
+    if args.ncu_steps or args.ncu_surrogate or args.ncu_ensemble:
         import maglua_b200 as M
         M.init(int(os.environ.get("LOCAL_RANK", "0")))
-        ss, ops, llg = build_system(M, 0)
-        for _ in range(args.ncu_steps):
-            M.run(ss, ops, llg, 1)
-        ss.synchronize()
+        if args.ncu_steps:
+            ss, ops, llg = build_system(M, 0)
+            for _ in range(args.ncu_steps):
+                M.run(ss, ops, llg, 1)
+            ss.synchronize()
+        if args.ncu_surrogate:
+            dims = SUR_DIMS
+            n = int(np.prod(dims))
+            ss = M.SpinSystem(*dims)
+            ss.setSpinArrays(*tilted_spins(n, 9, deg=30.0))
+            ss.setAlpha(0.02)
+            ss.setTimeStep(0.005)
+            ex = M.Exchange(ss)
+            ex.addPaths(*nn_paths(*dims))
+            dip = M.Dipole(ss)
+            dip.setStrength(0.05)
+            ops, llg = [ex, dip], M.LLG.new("Quaternion")
+            S = M.Surrogate(dip, (16, 16), 2)
+            r = np.random.default_rng(9)
+            W = r.normal(size=(25, S.C, S.C)) * 1e-3
+            R = (r.normal(size=(16, 16, S.C, S.C)) + 1j * r.normal(size=(16, 16, S.C, S.C))) * 1e-3
+            S.setParams(W, R)
+            S.setSchedule(1 << 30, tol=1e30, eps=1e-6)
+            S.attach(ss)
+            for _ in range(args.ncu_surrogate):
+                M.run(ss, ops, llg, 1)
+            S.detach(ss)
+            ss.synchronize()
+        if args.ncu_ensemble:
+            import torch
+            run_batched(M, torch, args.ncu_ensemble, 3)
         return
     args.warmup = max(3, args.warmup)
 
