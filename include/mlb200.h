@@ -114,9 +114,13 @@ int mlb_system_ensure_slot(mlb_system* s, const char* slot);          /* _ensure
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8]);
 /* sum_i s_i . h_slot,i in FP64 (the fieldArray:dot(spinArray) energy pattern). */
 int mlb_system_field_dot(mlb_system* s, const char* slot, double* out);
-/* copyTo / copySpinsTo (:1846-1898): spins, ms, scalars (and fields when
- * with_fields). */
+/* copyTo (with_fields: spins, ms, per-site alpha/gamma, alpha, gamma, dt,
+ * time and the fields; SpinSystem::copyFrom, spinsystem.cpp:310-391) or
+ * copySpinsTo (without: spins and ms only; copySpinsFrom, :393-409). */
 int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields);
+/* diff (spinsystem.cpp:301-307, l_getdiff :2145-2160): sum_i |a_i - b_i| of
+ * each component and the length of that vector, FP64. */
+int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4]);
 
 /* ---------------------------------------------------------------- operators
  * SpinOperation base, M/cpu/core/spinoperation.h:28-72. */
@@ -282,7 +286,22 @@ typedef struct mlb_rk mlb_rk;
 int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops, mlb_llg* l, mlb_op* temp,
                   mlb_rk** out);
 int mlb_rk_step(mlb_rk* r, int nsteps);
+/* The step function called on another system of the same size, as the
+ * script's step(ss_input, skip_temperature) (RungeKutta.lua:194-213). */
+int mlb_rk_step_on(mlb_rk* r, mlb_system* ss, int skip_temperature);
 int mlb_rk_destroy(mlb_rk* r);
+
+/* Replaces M/common/scripts/AdaptiveTimeStep.lua:9-110
+ * (make_adapt_step_function(ss, step, tolerance, llg, temp) and its step
+ * function) over a Runge-Kutta scheme: one step of dt against two of dt/2
+ * on copies of ss, compared with SpinSystem:diff; *accepted = 1 when the
+ * difference is below tolerance (ss takes the half-step result and dt grows),
+ * else 0 (ss unchanged, dt halves).  temp (may be NULL, then l may be NULL)
+ * is the Thermal kick applied after an accepted step. */
+typedef struct mlb_adapt mlb_adapt;
+int mlb_adapt_create(mlb_system* ss, mlb_rk* step, double tolerance, mlb_llg* l, mlb_op* temp, mlb_adapt** out);
+int mlb_adapt_step(mlb_adapt* a, int* accepted);
+int mlb_adapt_destroy(mlb_adapt* a);
 
 /* ---------------------------------------------------------------- learned dipolar surrogate
  * B200 extension, no counterpart in the reference.  A linear spectral-conv

@@ -135,6 +135,11 @@ _SIGS = {
     "mlb_surrogate_gradients": ([_P, C.POINTER(_F), C.POINTER(_F), _F, _F, C.POINTER(_F), _D], C.c_int),
     "mlb_rk_create": ([_P, C.c_char_p, C.POINTER(_P), C.c_int, _P, _P, C.POINTER(_P)], C.c_int),
     "mlb_rk_step": ([_P, C.c_int], C.c_int),
+    "mlb_rk_step_on": ([_P, _P, C.c_int], C.c_int),
+    "mlb_adapt_create": ([_P, _P, C.c_double, _P, _P, C.POINTER(_P)], C.c_int),
+    "mlb_adapt_step": ([_P, _I], C.c_int),
+    "mlb_adapt_destroy": ([_P], C.c_int),
+    "mlb_system_diff": ([_P, _P, _D], C.c_int),
     "mlb_rk_destroy": ([_P], C.c_int),
     "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
@@ -481,6 +486,12 @@ class SpinSystem:
 
     def copySpinsTo(self, dst):
         _ck(_lib.mlb_system_copy(dst._h, self._h, 0))
+
+    def diff(self, other):
+        """(dx, dy, dz, |d|) with d_c = sum_i |self_c,i - other_c,i| (l_getdiff)."""
+        out = np.zeros(4)
+        _ck(_lib.mlb_system_diff(self._h, other._h, _dp(out)))
+        return tuple(out)
 
     def copy(self):
         c = SpinSystem(*self._dims, precision=self._precision)
@@ -1224,12 +1235,44 @@ class RungeKutta:
     def step(self, n=1):
         _ck(_lib.mlb_rk_step(self._h, int(n)))
 
-    __call__ = step
+    def __call__(self, ss=None, skip_temperature=False):
+        """The script's step(ss_input, skip_temperature)."""
+        if ss is None:
+            self.step(1)
+        else:
+            _ck(_lib.mlb_rk_step_on(self._h, ss._h, int(bool(skip_temperature))))
+        return True
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h and _lib is not None:
             _lib.mlb_rk_destroy(h)
+            self._h = None
+
+
+class AdaptiveTimeStep:
+    """make_adapt_step_function(ss, step, tolerance, llg, temp) of the
+    reference's AdaptiveTimeStep.lua over a RungeKutta scheme: step() makes
+    one adaptive step of ss and returns whether it was accepted."""
+
+    def __init__(self, ss, rk, tolerance, llg=None, temp=None):
+        h = _P()
+        _ck(_lib.mlb_adapt_create(ss._h, rk._h, float(tolerance), llg._h if llg is not None else None,
+                                  temp._h if temp is not None else None, C.byref(h)))
+        self._h = h
+        self._keep = (ss, rk, llg, temp)
+
+    def step(self):
+        ok = C.c_int()
+        _ck(_lib.mlb_adapt_step(self._h, C.byref(ok)))
+        return bool(ok.value)
+
+    __call__ = step
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.mlb_adapt_destroy(h)
             self._h = None
 
 

@@ -1413,6 +1413,40 @@ void upload_site_array(mlb_system* s, void** dst, const double* a)
 // The canonical script step.  Nothing outside runs between its calls, so the
 // inverse x pass of a fast-path convolution may wait for the LLG update
 // (defer_x) and run fused with it.
+// copySpinsFrom (spinsystem.cpp:393-409): spins and moment magnitudes.
+void copy_spins(mlb_system* dst, mlb_system* src)
+{
+    if (dst == src) return;
+    const size_t bytes = (size_t)src->rb * src->n;
+    spins_changing(dst);
+    if (src->st != dst->st) CK(cudaStreamSynchronize(src->st));
+    for (int c = 0; c < 3; c++)
+        CK(cudaMemcpyAsync(dst->sp[dst->cur][c], src->sp[src->cur][c], bytes, cudaMemcpyDeviceToDevice, dst->st));
+    if (dst->ms_token != src->ms_token) {
+        CK(cudaMemcpyAsync(dst->ms, src->ms, bytes, cudaMemcpyDeviceToDevice, dst->st));
+        dst->ms_host = src->ms_host;
+        dst->ms_dirty = true;
+        dst->ms_token = src->ms_token;
+    }
+}
+
+// SpinSystem::diff (spinsystem.cpp:301-307): sum_i |a_i - b_i| per component
+// and the length of that vector, FP64 on the device.
+void system_diff(mlb_system* a, mlb_system* b, double out4[4])
+{
+    if (a->nx != b->nx || a->ny != b->ny || a->nz != b->nz) fail(MLB_EINVAL, "size mismatch");
+    if (a->rb != b->rb) fail(MLB_EINVAL, "precision mismatch");
+    if (a->st != b->st) CK(cudaStreamSynchronize(b->st));
+    const void* pa[3] = {a->sp[a->cur][0], a->sp[a->cur][1], a->sp[a->cur][2]};
+    const void* pb[3] = {b->sp[b->cur][0], b->sp[b->cur][1], b->sp[b->cur][2]};
+    CK(mlb::launch_diff(pa, pb, a->n, a->red, a->red_nb, a->redout, a->rb, a->st));
+    double r[3];
+    CK(cudaMemcpyAsync(r, a->redout, sizeof(r), cudaMemcpyDeviceToHost, a->st));
+    CK(cudaStreamSynchronize(a->st));
+    out4[0] = r[0]; out4[1] = r[1]; out4[2] = r[2];
+    out4[3] = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+}
+
 void do_step(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l)
 {
     reset_fields(s);
@@ -2250,6 +2284,11 @@ int mlb_system_field_dot(mlb_system* s, const char* slot, double* out)
     });
 }
 
+int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4])
+{
+    return guard([&] { system_diff(a, b, out4); });
+}
+
 int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
 {
     return guard([&] {
@@ -2257,15 +2296,9 @@ int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
         if (dst->nx != src->nx || dst->ny != src->ny || dst->nz != src->nz) fail(MLB_EINVAL, "size mismatch");
         if (dst->rb != src->rb) fail(MLB_EINVAL, "precision mismatch");
         if (dst == src) return;
+        copy_spins(dst, src);
+        if (!with_fields) return;   // copySpinsTo: spins and magnitudes only
         const size_t bytes = (size_t)src->rb * src->n;
-        spins_changing(dst);
-        CK(cudaStreamSynchronize(src->st));
-        for (int c = 0; c < 3; c++)
-            CK(cudaMemcpyAsync(dst->sp[dst->cur][c], src->sp[src->cur][c], bytes, cudaMemcpyDeviceToDevice, dst->st));
-        CK(cudaMemcpyAsync(dst->ms, src->ms, bytes, cudaMemcpyDeviceToDevice, dst->st));
-        dst->ms_host = src->ms_host;
-        dst->ms_dirty = true;
-        dst->ms_token = src->ms_token;
         dst->alpha = src->alpha; dst->gamma = src->gamma; dst->dt = src->dt; dst->time = src->time;
         CK(cudaStreamSynchronize(dst->st));
         upload_site_array(dst, &dst->sa, nullptr);
@@ -3094,11 +3127,11 @@ void rk_row(mlb_rk* r, mlb_system* src, const std::vector<double>& f, mlb_system
         if (i <= (int)f.size() && f[i - 1] != 0.0) llg_apply(r->l, dst, f[i - 1], r->k[i - 2], dst, 1);
 }
 
-// sfunc (RungeKutta.lua:194-213)
-void rk_step(mlb_rk* r)
+// sfunc (RungeKutta.lua:194-213) on the base system ss (the script's
+// ss_input, default the system the scheme was made for)
+void rk_step(mlb_rk* r, mlb_system* ss, bool skip_temperature)
 {
     const int nstep = (int)r->bt.size();
-    mlb_system* ss = r->ss;
     rk_field(r, ss);
     for (int i = 1; i <= nstep - 1; i++) {
         mlb_system* d = r->k[i - 1];   // ss_k[i+1]
@@ -3107,7 +3140,7 @@ void rk_step(mlb_rk* r)
         rk_field(r, d);
     }
     rk_row(r, ss, r->bt[nstep - 1], ss);
-    if (r->temp) {
+    if (r->temp && !skip_temperature) {
         reset_fields(ss);
         op_apply(r->temp, ss);
         sum_fields(ss);
@@ -3159,7 +3192,16 @@ int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops
 int mlb_rk_step(mlb_rk* r, int nsteps)
 {
     return guard([&] {
-        for (int k = 0; k < nsteps; k++) rk_step(r);
+        for (int k = 0; k < nsteps; k++) rk_step(r, r->ss, false);
+    });
+}
+
+int mlb_rk_step_on(mlb_rk* r, mlb_system* ss, int skip_temperature)
+{
+    return guard([&] {
+        if (ss->nx != r->ss->nx || ss->ny != r->ss->ny || ss->nz != r->ss->nz || ss->rb != r->ss->rb)
+            fail(MLB_EINVAL, "SpinSystem differs in size or precision from the scheme's");
+        rk_step(r, ss, skip_temperature != 0);
     });
 }
 
@@ -3169,6 +3211,114 @@ int mlb_rk_destroy(mlb_rk* r)
         if (!r) return;
         for (mlb_system* c : r->k) free_system(c);
         delete r;
+    });
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- adaptive time step
+// make_adapt_step_function (M/common/scripts/AdaptiveTimeStep.lua:9-110)
+// over a Runge-Kutta scheme: a full step of dt on one copy and two steps of
+// dt/2 on another, compared with SpinSystem::diff; accepted when the
+// difference is below the tolerance (the half-step result is kept, the time
+// step grows by 1 + clamp(e^2, 0.1, 0.5) - 0.1 with e = (tol - diff)/tol),
+// otherwise the time step halves.  The optional dynamics function of the
+// script is not part of this entry.
+struct mlb_adapt {
+    mlb_system* ss = nullptr;
+    mlb_system* s2 = nullptr;   // full step (owned copy)
+    mlb_system* s3 = nullptr;   // two half steps (owned copy)
+    mlb_rk* step = nullptr;
+    double tol = 0.0;
+    mlb_llg* l = nullptr;
+    mlb_op* temp = nullptr;
+};
+
+namespace {
+
+bool adapt_step(mlb_adapt* a)
+{
+    mlb_system* s = a->ss;
+    mlb_system* s2 = a->s2;
+    mlb_system* s3 = a->s3;
+    s2->time = s->time;
+    s3->time = s->time;
+    s2->dt = s->dt;
+    s3->dt = s->dt / 2;
+    copy_spins(s2, s);
+    copy_spins(s3, s);
+    rk_step(a->step, s2, true);
+    rk_step(a->step, s3, true);
+    rk_step(a->step, s3, true);
+    double d4[4];
+    system_diff(s2, s3, d4);
+    const bool same = d4[3] < a->tol;
+    double ee = (a->tol - d4[3]) / a->tol;
+    if (same) {
+        copy_spins(s, s3);
+        if (a->temp) {
+            reset_fields(s);
+            op_apply(a->temp, s);
+            sum_fields(s);
+            llg_apply(a->l, s, 1.0, s, s, 0);
+        }
+        s->time = s3->time;
+        ee = ee * ee;
+        if (ee > 0.5) ee = 0.5;
+        if (ee < 0.1) ee = 0.1;
+        s->dt = s->dt * (1 + ee - 0.1);
+    } else {
+        s->dt = s->dt * 0.5;
+    }
+    return same;
+}
+
+} // namespace
+
+extern "C" {
+
+int mlb_adapt_create(mlb_system* ss, mlb_rk* step, double tolerance, mlb_llg* l, mlb_op* temp, mlb_adapt** out)
+{
+    return guard([&] {
+        if (!ss || !step || !out) fail(MLB_EINVAL, "null argument");
+        if (ss->nx != step->ss->nx || ss->ny != step->ss->ny || ss->nz != step->ss->nz || ss->rb != step->ss->rb)
+            fail(MLB_EINVAL, "SpinSystem differs in size or precision from the scheme's");
+        if (temp && (temp->kind != MLB_OP_THERMAL || !l)) fail(MLB_EINVAL, "a Thermal operator needs the LLG operator");
+        std::unique_ptr<mlb_adapt> a(new mlb_adapt());
+        a->ss = ss;
+        a->step = step;
+        a->tol = tolerance;
+        a->l = l;
+        a->temp = temp;
+        for (mlb_system** c : {&a->s2, &a->s3}) {
+            *c = make_system(ss->nx, ss->ny, ss->nz, ss->rb);
+            int rc = mlb_system_copy(*c, ss, 1);
+            if (rc) {
+                free_system(a->s2);
+                free_system(a->s3);
+                fail(rc, g_err);
+            }
+            (*c)->st = ss->st;
+        }
+        *out = a.release();
+    });
+}
+
+int mlb_adapt_step(mlb_adapt* a, int* accepted)
+{
+    return guard([&] {
+        const bool ok = adapt_step(a);
+        if (accepted) *accepted = ok ? 1 : 0;
+    });
+}
+
+int mlb_adapt_destroy(mlb_adapt* a)
+{
+    return guard([&] {
+        if (!a) return;
+        free_system(a->s2);
+        free_system(a->s3);
+        delete a;
     });
 }
 

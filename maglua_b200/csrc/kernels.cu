@@ -422,6 +422,33 @@ __global__ void __launch_bounds__(256) k_netmoment_partial(const void* x_, const
     }
 }
 
+// FP64 partial sums of |a - b| per component (SpinSystem::diff,
+// spinsystem.cpp:301-307 with dArray::diffSum).
+template <typename R>
+__global__ void __launch_bounds__(256) k_diff_partial(const void* ax_, const void* ay_, const void* az_,
+                                                      const void* bx_, const void* by_, const void* bz_, int n,
+                                                      double* part)
+{
+    const R* a[3] = {static_cast<const R*>(ax_), static_cast<const R*>(ay_), static_cast<const R*>(az_)};
+    const R* b[3] = {static_cast<const R*>(bx_), static_cast<const R*>(by_), static_cast<const R*>(bz_)};
+    double acc[3] = {0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; c++) acc[c] += fabs((double)a[c][i] - (double)b[c][i]);
+    __shared__ double sh[3][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int q = 0; q < 3; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[q][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) v += sh[threadIdx.x][k];
+        part[blockIdx.x * 3 + threadIdx.x] = v;
+    }
+}
+
 // out[q] = sum_b part[b*nq + q]: block q (256 threads), thread t sums
 // b = t, t + 256, ... in order, then a fixed shuffle and warp tree
 // (deterministic, independent of timing).
@@ -1056,6 +1083,15 @@ cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n,
     if (rb == 8) k_netmoment_partial<double><<<nb, 256, 0, st>>>(x, y, z, n, m, part);
     else k_netmoment_partial<float><<<nb, 256, 0, st>>>(x, y, z, n, m, part);
     k_partial_final<<<6, 256, 0, st>>>(part, nb, 6, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diff(const void* const a[3], const void* const b[3], int n, double* part, int nb, double* out,
+                        int rb, cudaStream_t st)
+{
+    if (rb == 8) k_diff_partial<double><<<nb, 256, 0, st>>>(a[0], a[1], a[2], b[0], b[1], b[2], n, part);
+    else k_diff_partial<float><<<nb, 256, 0, st>>>(a[0], a[1], a[2], b[0], b[1], b[2], n, part);
+    k_partial_final<<<3, 256, 0, st>>>(part, nb, 3, out);
     return cudaGetLastError();
 }
 

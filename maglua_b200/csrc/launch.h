@@ -94,6 +94,8 @@ cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n,
                              double* out, int rb, cudaStream_t st);
 cudaError_t launch_dot(const void* const s[3], const void* const h[3], int n, double* part, int nb, double* out,
                        int rb, cudaStream_t st);
+cudaError_t launch_diff(const void* const a[3], const void* const b[3], int n, double* part, int nb, double* out,
+                        int rb, cudaStream_t st);
 size_t conv_x_smem(const ConvK& c, int rb);
 size_t conv_yz_smem(const ConvK& c, int rb);
 cudaError_t conv_configure();

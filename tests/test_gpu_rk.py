@@ -123,3 +123,110 @@ def test_rk_rejects_unknown_scheme(M):
     ss = M.SpinSystem(4, 4, 1)
     with pytest.raises(M.MagLuaError, match="RK type must be one of"):
         M.RungeKutta(ss, "RK5", [], M.LLG.new("Cartesian"))
+
+
+class OracleRK:
+    """The script's step function sfunc(ss_input) on the oracle: stage copies
+    made once from the base system (RungeKutta.lua:182-185)."""
+
+    def __init__(self, p, kind, llg):
+        self.p, self.bt, self.llg = p, BUTCHER[kind], llg
+        self.k = [None] + [oracle_copy(p.o) for _ in range(len(self.bt) - 1)]
+
+    def field(self, s):
+        s.reset_fields()
+        for f in self.p.oapply:
+            f(s)
+        s.sum_fields()
+
+    def __call__(self, ss):
+        bt, nstep, llg = self.bt, len(self.bt), self.llg
+        k = [ss] + self.k[1:]
+
+        def istep(src, factors, dst):
+            llg.apply(src, factors[0], src, dst)
+            for i in range(2, nstep + 1):
+                if i <= len(factors) and factors[i - 1] != 0:
+                    llg.apply(dst, factors[i - 1], k[i - 1], dst)
+
+        self.field(ss)
+        for i in range(1, nstep):
+            k[i].dt = ss.dt
+            istep(ss, bt[i - 1], k[i])
+            self.field(k[i])
+        istep(ss, bt[nstep - 1], ss)
+
+
+def test_diff_and_copy_spins(M):
+    dims = (12, 10, 3)
+    n = int(np.prod(dims))
+    from helpers import random_spins
+    a, b = M.SpinSystem(*dims), M.SpinSystem(*dims)
+    sa, sb = random_spins(n, 72), random_spins(n, 73)
+    a.setSpinArrays(*sa)
+    b.setSpinArrays(*sb)
+    b.setAlpha(0.3)
+    b.setTimeStep(0.07)
+    b.setTime(1.5)
+    ga = np.stack(a.spinArrays()[:3])
+    gb = np.stack(b.spinArrays()[:3])
+    d = np.abs(ga - gb).sum(axis=1)
+    got = a.diff(b)
+    np.testing.assert_allclose(got[:3], d, rtol=1e-12)
+    assert got[3] == pytest.approx(np.sqrt((d ** 2).sum()), rel=1e-12)
+    # copySpinsTo (copySpinsFrom, spinsystem.cpp:393-409): spins and magnitudes only
+    a.copySpinsTo(b)
+    np.testing.assert_array_equal(np.stack(b.spinArrays()), np.stack(a.spinArrays()))
+    assert (b.alpha(), b.timeStep(), b.time()) == (0.3, 0.07, 1.5)
+    assert a.diff(b)[3] == 0.0
+
+
+@pytest.mark.parametrize("kind,tol", [("RK2", 2e-3), ("RK4", 1e-4)])
+def test_adaptive_time_step_matches_oracle(M, kind, tol):
+    """make_adapt_step_function (AdaptiveTimeStep.lua:9-110) natively against
+    the script restated over the oracle: the accept/reject sequence, the time
+    steps and the trajectory."""
+    dims = (16, 12, 2)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 74, deg=30.0)
+    p = Pair(*dims, s0, alpha=0.2, dt=0.08)
+    p.exchange(J=1.0, pbc=(1, 1, 0))
+    p.anisotropy(axis=(0, 0, 1), K=0.2)
+    p.dipole(g=0.05)
+    rk = M.RungeKutta(p.g, kind, p.ops, M.LLG.new("Quaternion"))
+    ad = M.AdaptiveTimeStep(p.g, rk, tol)
+    got = []
+    for _ in range(12):
+        got.append((ad.step(), p.g.timeStep(), p.g.time()))
+    # oracle
+    o = p.o
+    step = OracleRK(p, kind, O.LLG("Quaternion"))
+    s2, s3 = oracle_copy(o), oracle_copy(o)
+    ref = []
+    for _ in range(12):
+        s2.time = s3.time = o.time
+        s2.dt, s3.dt = o.dt, o.dt / 2
+        s2.set_spins(*o.spins())
+        s3.set_spins(*o.spins())
+        step(s2)
+        step(s3)
+        step(s3)
+        d = np.abs(s2.spins() - s3.spins()).sum(axis=1)
+        dxyz = float(np.sqrt((d ** 2).sum()))
+        same = dxyz < tol
+        ee = (tol - dxyz) / tol
+        if same:
+            o.set_spins(*s3.spins())
+            o.time = s3.time
+            ee = min(max(ee * ee, 0.1), 0.5)
+            o.dt = o.dt * (1 + ee - 0.1)
+        else:
+            o.dt = o.dt * 0.5
+        ref.append((same, o.dt, o.time))
+    assert [g[0] for g in got] == [r[0] for r in ref], (got, ref)
+    assert any(not r[0] for r in ref) and any(r[0] for r in ref)   # both branches taken
+    for g, r in zip(got, ref):
+        assert g[1] == pytest.approx(r[1], rel=1e-4)
+        assert g[2] == pytest.approx(r[2], rel=1e-4, abs=1e-9)
+    err = float(np.abs(np.stack(p.g.spinArrays()[:3]) - o.spins()).max())
+    assert err < 2e-5, err
