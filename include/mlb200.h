@@ -273,6 +273,15 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
  * issuing those calls one by one. */
 int mlb_run(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int nsteps);
 
+/* The Dipole tensor cache files WAB_<nx>x<ny>.<v>.lua of the reference
+ * (M/cpu/dipole/dipolesupport.cpp:256-643; written by dipole_write_matrix,
+ * checked by dipoleParamsMatch, loaded by dipoleLoad :717-851).  write: the
+ * operator's reference-layout tensor (computed first for a Dipole);
+ * read: a file whose nx, ny, nz, gmax and unit cell match the operator
+ * (MLB_EINVAL otherwise) becomes its tensor, so the lattice sum is skipped. */
+int mlb_dipole_write_wab(mlb_op* op, const char* filename);
+int mlb_dipole_read_wab(mlb_op* op, const char* filename);
+
 /* ---------------------------------------------------------------- Runge-Kutta integrators
  * Replaces the script M/common/scripts/RungeKutta.lua:57-215
  * (make_rk_step_function(ss, type, {ops}, llg, temp) and its step function):

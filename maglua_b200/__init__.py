@@ -140,6 +140,8 @@ _SIGS = {
     "mlb_adapt_step": ([_P, _I], C.c_int),
     "mlb_adapt_destroy": ([_P], C.c_int),
     "mlb_system_diff": ([_P, _P, _D], C.c_int),
+    "mlb_dipole_write_wab": ([_P, C.c_char_p], C.c_int),
+    "mlb_dipole_read_wab": ([_P, C.c_char_p], C.c_int),
     "mlb_rk_destroy": ([_P], C.c_int),
     "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
@@ -860,6 +862,22 @@ class LongRange(SpinOperation):
         ptrs = (_D * 6)(*[_dp(a) for a in arrs])
         _ck(_lib.mlb_longrange_get_tensor(self._h, ptrs))
         return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
+
+
+def _wab_methods(cls):
+    def writeWAB(self, filename):
+        """Write the tensor as the reference's WAB_<nx>x<ny>.<v>.lua cache file."""
+        _ck(_lib.mlb_dipole_write_wab(self._h, str(filename).encode()))
+
+    def readWAB(self, filename):
+        """Take the tensor from a WAB file whose parameters match this operator."""
+        _ck(_lib.mlb_dipole_read_wab(self._h, str(filename).encode()))
+
+    cls.writeWAB, cls.readWAB = writeWAB, readWAB
+    return cls
+
+
+LongRange = _wab_methods(LongRange)
 
 
 class Dipole(LongRange):

@@ -3069,6 +3069,241 @@ int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
 
 } // extern "C"
 
+// ---------------------------------------------------------------- WAB tensor files
+// The Dipole tensor cache of the reference (M/cpu/dipole/dipolesupport.cpp:
+// 256-643): a Lua file with gmax, nx, ny, nz, the unit cell ABC and, per z
+// offset k = -(nz-1) .. nz-1 and component XX, XY, XZ, YY, YZ, ZZ, either
+// "NAME[k] = 0" (an all-zero layer) or "NAME[k] = [[" ny lines of nx
+// comma-separated numbers "]]", followed by a Lua function parse() that turns
+// the strings into tables (the reference's loader runs the file and calls
+// it).  The writer here produces that layout with a parse() of its own; the
+// reader parses the data lines directly (no Lua needed) and accepts a file
+// only when nx, ny, nz, gmax and ABC match the operator, as dipoleParamsMatch
+// (:456-560) does.
+namespace {
+
+const char* const kWabNames[6] = {"XX", "XY", "XZ", "YY", "YZ", "ZZ"};
+
+void wab_write_layer(FILE* f, const char* name, int k, const double* M, int nx, int ny)
+{
+    fprintf(f, "\n");
+    bool zero = true;
+    for (int i = 0; i < nx * ny && zero; i++) zero = M[i] == 0.0;
+    if (zero) {
+        fprintf(f, "%s[%i] = 0\n", name, k);
+        return;
+    }
+    fprintf(f, "%s[%i] = [[\n", name, k);
+    for (int j = 0; j < ny; j++) {
+        for (int i = 0; i < nx; i++) {
+            const bool last = i == nx - 1 && j == ny - 1;
+            const double v = M[i + j * nx];
+            if (v == 0.0) fprintf(f, "0%s", last ? "" : ",");
+            else fprintf(f, "% .16g%s", v, last ? "" : ",");
+        }
+        fprintf(f, "\n");
+    }
+    fprintf(f, "]]\n\n");
+}
+
+// Lua that turns each "[[...]]" layer into M[row][col] tables and a "0" layer
+// into a table of zeros, written after the data.
+const char* const kWabParse =
+    "\n"
+    "local function rows_of(text)\n"
+    "\tlocal M = {}\n"
+    "\tfor line in string.gmatch(text, \"[^\\n]+\") do\n"
+    "\t\tlocal row = {}\n"
+    "\t\tfor v in string.gmatch(line, \"[^,%s]+\") do row[#row + 1] = tonumber(v) end\n"
+    "\t\tif #row > 0 then M[#M + 1] = row end\n"
+    "\tend\n"
+    "\treturn M\n"
+    "end\n"
+    "\n"
+    "local function layer(v)\n"
+    "\tif v == 0 then\n"
+    "\t\tlocal zrow = setmetatable({}, {__index = function() return 0 end})\n"
+    "\t\treturn setmetatable({}, {__index = function() return zrow end})\n"
+    "\tend\n"
+    "\treturn rows_of(v)\n"
+    "end\n"
+    "\n"
+    "function parse()\n"
+    "\tfor _, t in ipairs({XX, XY, XZ, YY, YZ, ZZ}) do\n"
+    "\t\tfor k, v in pairs(t) do t[k] = layer(v) end\n"
+    "\tend\n"
+    "end\n";
+
+bool wab_near(double a, double b) { return fabs(a - b) <= 0.5 * (fabs(a) + fabs(b)) * 1e-6; }
+
+// numbers after `key` up to the end of its statement (a line for scalars, the
+// closing braces for tables)
+bool wab_numbers_after(const std::string& t, const char* key, std::vector<double>& out, bool& huge)
+{
+    out.clear();
+    huge = false;
+    size_t p = t.find(key);
+    if (p == std::string::npos) return false;
+    p = t.find('=', p);
+    if (p == std::string::npos) return false;
+    size_t e = t.find('\n', p);
+    // tables may span lines: stop at the brace that closes the first one
+    size_t q = p + 1;
+    while (q < t.size() && (t[q] == ' ' || t[q] == '\t')) q++;
+    if (q < t.size() && t[q] == '{') {
+        int depth = 0;
+        for (size_t r = q; r < t.size(); r++) {
+            if (t[r] == '{') depth++;
+            else if (t[r] == '}' && --depth == 0) { e = r + 1; break; }
+        }
+    }
+    std::string s = t.substr(p + 1, e == std::string::npos ? std::string::npos : e - p - 1);
+    // drop comments
+    for (size_t c = s.find("--"); c != std::string::npos; c = s.find("--")) {
+        const size_t n = s.find('\n', c);
+        s.erase(c, n == std::string::npos ? std::string::npos : n - c);
+    }
+    if (s.find("math.huge") != std::string::npos) huge = true;
+    const char* c = s.c_str();
+    while (*c) {
+        if ((*c >= '0' && *c <= '9') || *c == '-' || *c == '+' || *c == '.') {
+            char* end = nullptr;
+            const double v = strtod(c, &end);
+            if (end == c) { c++; continue; }
+            out.push_back(v);
+            c = end;
+        } else {
+            c++;
+        }
+    }
+    return true;
+}
+
+} // namespace
+
+extern "C" {
+
+int mlb_dipole_write_wab(mlb_op* op, const char* filename)
+{
+    return guard([&] {
+        if (!op || !filename) fail(MLB_EINVAL, "null argument");
+        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE)
+            fail(MLB_EINVAL, "not a Dipole or LongRange operator");
+        if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) build_plan(op, nullptr, 4);   // the lattice sum
+        ensure_t6_layout(op);
+        FILE* f = fopen(filename, "w");
+        if (!f) fail(MLB_EINVAL, std::string("cannot write ") + filename);
+        fprintf(f, "-- This file contains dipole interaction matrices\n\n");
+        fprintf(f, "gmax = {%i, %i, %i, %i} -- radial max, maxX, maxY, maxZ\n", op->gmax[0], op->gmax[1], op->gmax[2],
+                op->gmax[3]);
+        fprintf(f, "nx, ny, nz = %i, %i, %i\n", op->nx, op->ny, op->nz);
+        const double* A = op->ABC;
+        fprintf(f, "ABC = {{%g, %g, %g}, --unit cell\n       {%g, %g, %g},\n       {%g, %g, %g}}\n\n", A[0], A[1],
+                A[2], A[3], A[4], A[5], A[6], A[7], A[8]);
+        fprintf(f, "XX={} XY={} XZ={} YY={} YZ={} ZZ={}\n");
+        const size_t layer = (size_t)op->nx * op->ny;
+        for (int c = 0; c < 2 * op->nz - 1; c++)
+            for (int q = 0; q < 6; q++)
+                wab_write_layer(f, kWabNames[q], c - op->nz + 1, op->t6[q].data() + c * layer, op->nx, op->ny);
+        fprintf(f, "%s", kWabParse);
+        const bool ok = ferror(f) == 0;
+        fclose(f);
+        if (!ok) fail(MLB_EINVAL, std::string("error writing ") + filename);
+    });
+}
+
+int mlb_dipole_read_wab(mlb_op* op, const char* filename)
+{
+    return guard([&] {
+        if (!op || !filename) fail(MLB_EINVAL, "null argument");
+        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE)
+            fail(MLB_EINVAL, "not a Dipole or LongRange operator");
+        FILE* f = fopen(filename, "rb");
+        if (!f) fail(MLB_ENOTFOUND, std::string("cannot read ") + filename);
+        std::string t;
+        char buf[65536];
+        size_t got;
+        while ((got = fread(buf, 1, sizeof(buf), f)) > 0) t.append(buf, got);
+        fclose(f);
+        // header
+        std::vector<double> v;
+        bool huge = false;
+        if (!wab_numbers_after(t, "nx, ny, nz", v, huge) || v.size() != 3 || (int)v[0] != op->nx ||
+            (int)v[1] != op->ny || (int)v[2] != op->nz)
+            fail(MLB_EINVAL, "WAB file: nx, ny, nz differ from the operator's");
+        if (!wab_numbers_after(t, "gmax", v, huge)) fail(MLB_EINVAL, "WAB file: no gmax");
+        if (huge) fail(MLB_EUNSUP, "WAB file with infinite gmax (extrapolated sums are not supported)");
+        if (v.size() == 1) v.assign(4, v[0]);   // old files: one radius
+        if (v.size() != 4) fail(MLB_EINVAL, "WAB file: malformed gmax");
+        for (int i = 0; i < 4; i++)
+            if ((int)v[i] != op->gmax[i]) fail(MLB_EINVAL, "WAB file: gmax differs from the operator's");
+        if (!wab_numbers_after(t, "ABC", v, huge) || v.size() != 9) fail(MLB_EINVAL, "WAB file: malformed ABC");
+        for (int i = 0; i < 9; i++)
+            if (!wab_near(v[i], op->ABC[i])) fail(MLB_EINVAL, "WAB file: unit cell differs from the operator's");
+        // layers
+        const size_t layer = (size_t)op->nx * op->ny;
+        std::vector<double> t6[6];
+        for (int q = 0; q < 6; q++) t6[q].assign(layer * (2 * op->nz - 1), 0.0);
+        std::vector<char> seen((size_t)6 * (2 * op->nz - 1), 0);
+        size_t pos = t.find("XX={}");
+        if (pos == std::string::npos) fail(MLB_EINVAL, "WAB file: no tensor tables");
+        for (;;) {
+            size_t best = std::string::npos;
+            int q = -1;
+            for (int c = 0; c < 6; c++) {
+                const std::string key = std::string("\n") + kWabNames[c] + "[";
+                const size_t p = t.find(key, pos);
+                if (p < best) { best = p; q = c; }
+            }
+            if (best == std::string::npos) break;
+            size_t p = best + 4;   // after "\nXX["
+            char* end = nullptr;
+            const long k = strtol(t.c_str() + p, &end, 10);
+            p = end - t.c_str();
+            const size_t eq = t.find('=', p);
+            if (eq == std::string::npos || k < -(op->nz - 1) || k > op->nz - 1)
+                fail(MLB_EINVAL, "WAB file: malformed layer index");
+            const int c = (int)k + op->nz - 1;
+            size_t r = eq + 1;
+            while (r < t.size() && (t[r] == ' ' || t[r] == '\t')) r++;
+            if (t.compare(r, 2, "[[") == 0) {
+                const size_t close = t.find("]]", r + 2);
+                if (close == std::string::npos) fail(MLB_EINVAL, "WAB file: unterminated layer");
+                const char* s = t.c_str() + r + 2;
+                const char* stop = t.c_str() + close;
+                size_t i = 0;
+                while (s < stop) {
+                    if (*s == ',' || *s == ' ' || *s == '\n' || *s == '\r' || *s == '\t') { s++; continue; }
+                    char* e2 = nullptr;
+                    const double x = strtod(s, &e2);
+                    if (e2 == s) fail(MLB_EINVAL, "WAB file: malformed number");
+                    if (i >= layer) fail(MLB_EINVAL, "WAB file: layer larger than nx*ny");
+                    t6[q][c * layer + i++] = x;
+                    s = e2;
+                }
+                if (i != layer) fail(MLB_EINVAL, "WAB file: layer smaller than nx*ny");
+                pos = close + 2;
+            } else {
+                char* e2 = nullptr;
+                const double x = strtod(t.c_str() + r, &e2);
+                if (e2 == t.c_str() + r || x != 0.0) fail(MLB_EINVAL, "WAB file: malformed zero layer");
+                pos = e2 - t.c_str();
+            }
+            seen[(size_t)q * (2 * op->nz - 1) + c] = 1;
+        }
+        for (char x : seen)
+            if (!x) fail(MLB_EINVAL, "WAB file: missing layers");
+        materialize_users(op);
+        for (int q = 0; q < 6; q++) op->t6[q].swap(t6[q]);
+        op->t6_valid = true;
+        op->t6_edited = op->kind == MLB_OP_LONGRANGE;
+        op->plan_dirty = true;
+        g_version++;
+    });
+}
+
+} // extern "C"
+
 // ---------------------------------------------------------------- Runge-Kutta integrators
 // The reference's make_rk_step_function (M/common/scripts/RungeKutta.lua:
 // 57-215) as native host code over the same operations: per step the field
