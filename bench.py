@@ -222,31 +222,45 @@ CUBE_WORKLOAD = ("256^3 simple-cubic cube, open boundaries (512^3 padded transfo
                  "LLG.Quaternion; spins +z with a seeded 20-degree tilt")
 
 
+def cube_system(M, prec, spins):
+    """The open cube of CUBE_DIMS sites with its operators and integrator."""
+    dims = CUBE_DIMS
+    n = int(np.prod(dims))
+    f, t, j = nn_paths(*dims, pbc=(0, 0, 0))
+    ss = M.SpinSystem(*dims, precision=prec)
+    ss.setSpinArrays(*spins)
+    ss.setAlpha(0.05)
+    ss.setTimeStep(0.005)
+    ex = M.Exchange(ss)
+    ex.addPaths(f, t, j)
+    cub = M.AnisotropyCubic(ss)
+    cub.addMany(np.arange(n), np.tile([1.0, 0, 0], (n, 1)), np.tile([0, 1.0, 0], (n, 1)),
+                np.tile([0.05, 0, 0], (n, 1)))
+    th = M.Thermal(ss, M.Random.Philox(5))
+    th.setTemperature(0.3)
+    dip = M.Dipole(ss)
+    dip.setStrength(0.03)
+    dip.setOpen(True, True, True)
+    return ss, [ex, cub, th, dip], M.LLG.new("Quaternion")
+
+
+def run_cube_steps(M, nsteps):
+    """Profiling driver: eager FP32 steps of the cube."""
+    n = int(np.prod(CUBE_DIMS))
+    ss, ops, llg = cube_system(M, "f32", tilted_spins(n, 5, deg=20.0))
+    for _ in range(nsteps):
+        M.run(ss, ops, llg, 1)
+    ss.synchronize()
+
+
 def run_cube(M, torch, steps=20):
     """Configuration 5 on one GPU: FP32 and FP64 step rates, and the FP32
     fields and energies of one state against the FP64 run's (both from the
     same spins: the FP64 state after 2 steps, rounded to FP32)."""
     dims = CUBE_DIMS
     n = int(np.prod(dims))
-    f, t, j = nn_paths(*dims, pbc=(0, 0, 0))
     s0 = tilted_spins(n, 5, deg=20.0)
-
-    def build(prec, spins):
-        ss = M.SpinSystem(*dims, precision=prec)
-        ss.setSpinArrays(*spins)
-        ss.setAlpha(0.05)
-        ss.setTimeStep(0.005)
-        ex = M.Exchange(ss)
-        ex.addPaths(f, t, j)
-        cub = M.AnisotropyCubic(ss)
-        cub.addMany(np.arange(n), np.tile([1.0, 0, 0], (n, 1)), np.tile([0, 1.0, 0], (n, 1)),
-                    np.tile([0.05, 0, 0], (n, 1)))
-        th = M.Thermal(ss, M.Random.Philox(5))
-        th.setTemperature(0.3)
-        dip = M.Dipole(ss)
-        dip.setStrength(0.03)
-        dip.setOpen(True, True, True)
-        return ss, [ex, cub, th, dip], M.LLG.new("Quaternion")
+    build = lambda prec, spins: cube_system(M, prec, spins)   # noqa: E731
 
     def timed(ss, fn, k):
         st = torch.cuda.ExternalStream(ss.stream())
@@ -429,7 +443,17 @@ def main():
                          "network weights, every step after the first a surrogate step) and exit")
     ap.add_argument("--ncu-ensemble", type=int, default=0,
                     help="profiling driver: this many captured steps of the packed ensemble and exit")
+    ap.add_argument("--ncu-cube", type=int, default=0,
+                    help="profiling driver: this many eager FP32 steps of the open cube (edge --cube-edge) and exit")
+    ap.add_argument("--cube-edge", type=int, default=256, help="edge of the cube for --ncu-cube")
     args = ap.parse_args()
+    if args.ncu_cube:
+        import maglua_b200 as M
+        M.init(int(os.environ.get("LOCAL_RANK", "0")))
+        global CUBE_DIMS
+        CUBE_DIMS = (args.cube_edge,) * 3
+        run_cube_steps(M, args.ncu_cube)
+        return
     if args.ncu_steps or args.ncu_surrogate or args.ncu_ensemble:
         import maglua_b200 as M
         M.init(int(os.environ.get("LOCAL_RANK", "0")))

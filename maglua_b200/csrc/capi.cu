@@ -1130,7 +1130,9 @@ bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, dou
 {
     refresh_ms(s);
     if (s->rb != 4 || !s->ms_uniform || !(s->ms_u > 0.0) || s->sa || s->sg) return false;
-    if (T.ex.mode == EX_CSR || T.ani.mode == ANI_CSR || T.uni.mode != ANI_NONE || T.cub.mode != ANI_NONE) return false;
+    if (T.ex.mode == EX_CSR || T.ani.mode == ANI_CSR || T.uni.mode != ANI_NONE) return false;
+    // one uniform cubic axis set alone (no simple anisotropy beside it)
+    if (T.cub.mode == ANI_CSR || (T.cub.mode == ANI_UNIFORM && T.ani.mode != ANI_NONE)) return false;
     if (T.th.mode == TH_INJECT || (T.th.mode == TH_PHILOX && T.th.scale)) return false;
     if (T.nadd > 1 || (T.nadd == 1 && T.add_is_thermal[0])) return false;
     const double ms = s->ms_u, a = s->alpha, g = s->gamma;
@@ -1142,10 +1144,16 @@ bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, dou
         for (int d = 0; d < 6; d++) F.J[d] = (float)((double)T.ex.J[d] * T.ex_gs / den);
         for (int c = 0; c < 3; c++) F.pbc[c] = T.ex.pbc[c];
     }
-    F.ani = T.ani.mode == ANI_UNIFORM;
+    F.ani = T.ani.mode == ANI_UNIFORM ? 1 : 0;
     if (F.ani) {
         for (int c = 0; c < 3; c++) F.axis[c] = (float)T.ani.axis[c];
         F.ani_c = (float)(2.0 * (double)T.ani.K / (ms * ms));
+    }
+    if (T.cub.mode == ANI_UNIFORM) {
+        F.ani = 2;
+        for (int q = 0; q < 9; q++) F.cub_n[q] = (float)T.cub.axes[q];
+        for (int q = 0; q < 3; q++) F.cub_K[q] = (float)T.cub.K[q];
+        F.cub_quirk = T.cub.quirk;
     }
     F.th = T.th.mode == TH_PHILOX && T.th.T != 0.0 && g > 0;
     if (F.th) {

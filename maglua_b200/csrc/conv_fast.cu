@@ -424,6 +424,268 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
     }
 }
 
+// ------------------------------------------------------------------ split (y,z) passes, FP32
+// Planes larger than shared memory (a 256^3 open cube pads to 512 x 512):
+// the (y,z) pass as three passes through S2[kx][ky][comp][z] (data layers
+// z < nz only; the layout of the generic split kernels in kernels.cu), each
+// line transformed in registers by a T-lane group (fr::line_fft):
+//   k_sy_fast   CTA (kx, comp, LN data layers): y transforms of the layers'
+//               rows, zero-padded to PY; transposed in shared memory so that
+//               each ky stores LN consecutive z;
+//   k_sz_fast   CTA (kx, COLS ky columns): z transforms of the columns' three
+//               components, zero-padded to PZ; 3x3 tensor multiply (ky-major
+//               real tensor, scaled by the strength); inverse z transforms,
+//               data layers back to S2;
+//   k_syi_fast  CTA (kx, comp, LN layers): inverse y transforms, data rows
+//               to SPEC[kx][comp][z][y].
+// Each shared-memory line buffer serves as the four-step exchange buffer
+// and, between transforms, as the line's natural-order spectrum.
+constexpr int SPL_NT = 256;   // threads of the y passes
+constexpr int SPZ_NT = 192;   // threads of the z pass (a multiple of 3 lines)
+
+template <int PY>
+struct SPY {
+    static constexpr int T = fr::Split<PY>::T, E = fr::Split<PY>::E;
+    static constexpr int LN = SPL_NT / T;     // data layers per CTA
+    static constexpr int EX = E * (T + 1);    // exchange elements per line
+    static constexpr int TS = LN + 1;         // transpose row stride, [ky][layer]
+    static constexpr int BUF = LN * EX > PY * TS ? LN * EX : PY * TS;
+    static constexpr size_t SMEM = (size_t)(PY + BUF) * sizeof(float2);
+};
+
+template <int PZ>
+struct SPZ {
+    static constexpr int T = fr::Split<PZ>::T, E = fr::Split<PZ>::E;
+    static constexpr int LN = SPZ_NT / T;     // lines per CTA
+    static constexpr int COLS = LN / 3;       // ky columns per CTA
+    static constexpr int EX = E * (T + 1);    // >= PZ: exchange, then spectrum
+    static constexpr size_t SMEM = (size_t)(PZ + LN * EX) * sizeof(float2);
+};
+
+// lanes of this thread's T-lane group within its warp
+__device__ __forceinline__ unsigned group_mask(int T)
+{
+    return T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << (((threadIdx.x & 31) / T) * T));
+}
+
+template <int PY>
+__global__ void __launch_bounds__(SPL_NT, 2) k_sy_fast(ConvK c, const float2* __restrict__ twy,
+                                                       const float2* __restrict__ spec, float2* __restrict__ s2)
+{
+    using Y = SPY<PY>;
+    constexpr int T = Y::T, E = Y::E, LN = Y::LN;
+    extern __shared__ float2 sm[];
+    float2* twl = sm;
+    float2* buf = sm + PY;
+    for (int k = threadIdx.x; k < PY; k += SPL_NT) twl[k] = twy[k];
+    pdl_trigger();
+    pdl_wait();
+    if (c.run_if && *c.run_if == 0) return;
+    const int nz = c.nz, ny = c.ny;
+    const int kx = blockIdx.x, comp = blockIdx.y, z0 = blockIdx.z * LN;
+    const int lr = threadIdx.x / T, t = threadIdx.x % T;
+    const int nl = min(LN, nz - z0);
+    const bool act = lr < nl;   // whole T-lane groups share act
+    __syncthreads();
+    float2 v[E];
+    if (act) {
+        const float2* src = spec + (((size_t)kx * 3 + comp) * nz + z0 + lr) * ny;
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int y = t + T * j;
+            v[j] = y < ny ? src[y] : make_float2(0.f, 0.f);
+        }
+        fr::line_fft<PY, -1, float2>(v, buf + (size_t)lr * Y::EX, t, group_mask(T), twl);
+    }
+    __syncthreads();   // exchange buffers -> transpose buffer
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < E; r++) buf[fr::out_index<PY>(t, r) * Y::TS + lr] = v[r];
+    }
+    __syncthreads();
+    // S2[kx][ky][comp][z0 + l]: LN consecutive threads store one ky's layers
+    const int l = threadIdx.x % LN, kq = threadIdx.x / LN;
+    float2* dst = s2 + ((size_t)kx * PY * 3 + comp) * nz + z0 + l;
+    if (l < nl) {
+#pragma unroll 4
+        for (int k = 0; k < PY / T; k++) {
+            const int ky = kq + T * k;
+            dst[(size_t)ky * 3 * nz] = buf[ky * Y::TS + l];
+        }
+    }
+}
+
+template <int PZ>
+__global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __restrict__ twz,
+                                                       float2* __restrict__ s2, const float* __restrict__ ten6)
+{
+    using Z = SPZ<PZ>;
+    constexpr int T = Z::T, E = Z::E, COLS = Z::COLS, EX = Z::EX;
+    extern __shared__ float2 sm[];
+    float2* twl = sm;
+    float2* buf = sm + PZ;
+    for (int k = threadIdx.x; k < PZ; k += SPZ_NT) twl[k] = twz[k];
+    pdl_trigger();
+    pdl_wait();
+    if (c.run_if && *c.run_if == 0) return;
+    const int nz = c.nz, Py = c.Py;
+    const int kx = blockIdx.x, ky0 = blockIdx.y * COLS;
+    const int lr = threadIdx.x / T, t = threadIdx.x % T;
+    const int col = lr / 3, comp = lr - 3 * col;
+    const bool act = lr < 3 * COLS && ky0 + col < Py;   // whole T-lane groups share act
+    const unsigned mask = group_mask(T);
+    float2* exl = buf + (size_t)lr * EX;
+    float2* colp = s2 + (((size_t)kx * Py + ky0 + col) * 3 + comp) * nz;
+    __syncthreads();
+    float2 v[E];
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int z = t + T * j;
+            v[j] = z < nz ? colp[z] : make_float2(0.f, 0.f);
+        }
+        fr::line_fft<PZ, -1, float2>(v, exl, t, mask, twl);
+#pragma unroll
+        for (int r = 0; r < E; r++) exl[fr::out_index<PZ>(t, r)] = v[r];
+    }
+    __syncthreads();
+    // tensor multiply, point p = (column, kz): consecutive threads take
+    // consecutive kz, so the tensor rows [kx][ky][kz][6] stream contiguously
+    const float gg = c.g;
+    const int ncol = min(COLS, Py - ky0);
+    const float* Tb = ten6 + ((size_t)kx * Py + ky0) * PZ * 6;
+    for (int p = threadIdx.x; p < ncol * PZ; p += SPZ_NT) {
+        const int cl = p / PZ, kz = p % PZ;
+        const float* Tp = Tb + (size_t)p * 6;
+        const float t0 = __ldg(Tp), t1 = __ldg(Tp + 1), t2 = __ldg(Tp + 2);
+        const float t3 = __ldg(Tp + 3), t4 = __ldg(Tp + 4), t5 = __ldg(Tp + 5);
+        float2* b = buf + (size_t)cl * 3 * EX + kz;
+        const float2 s0 = b[0], s1 = b[EX], s2v = b[2 * EX];
+        b[0] = make_float2(gg * (t0 * s0.x + t1 * s1.x + t2 * s2v.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2v.y));
+        b[EX] = make_float2(gg * (t1 * s0.x + t3 * s1.x + t4 * s2v.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2v.y));
+        b[2 * EX] =
+            make_float2(gg * (t2 * s0.x + t4 * s1.x + t5 * s2v.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2v.y));
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = exl[t + T * j];
+        __syncwarp(mask);   // every lane has read the spectrum before the exchange overwrites it
+        fr::line_fft<PZ, +1, float2>(v, exl, t, mask, twl);
+#pragma unroll
+        for (int r = 0; r < E; r++) {
+            const int z = fr::out_index<PZ>(t, r);
+            if (z < nz) colp[z] = v[r];
+        }
+    }
+}
+
+template <int PY>
+__global__ void __launch_bounds__(SPL_NT, 2) k_syi_fast(ConvK c, const float2* __restrict__ twy,
+                                                        const float2* __restrict__ s2, float2* __restrict__ spec)
+{
+    using Y = SPY<PY>;
+    constexpr int T = Y::T, E = Y::E, LN = Y::LN;
+    extern __shared__ float2 sm[];
+    float2* twl = sm;
+    float2* buf = sm + PY;
+    for (int k = threadIdx.x; k < PY; k += SPL_NT) twl[k] = twy[k];
+    pdl_trigger();
+    pdl_wait();
+    if (c.run_if && *c.run_if == 0) return;
+    const int nz = c.nz, ny = c.ny;
+    const int kx = blockIdx.x, comp = blockIdx.y, z0 = blockIdx.z * LN;
+    const int nl = min(LN, nz - z0);
+    {
+        const int l = threadIdx.x % LN, kq = threadIdx.x / LN;
+        const float2* src = s2 + ((size_t)kx * PY * 3 + comp) * nz + z0 + l;
+        if (l < nl) {
+#pragma unroll 4
+            for (int k = 0; k < PY / T; k++) {
+                const int ky = kq + T * k;
+                buf[ky * Y::TS + l] = src[(size_t)ky * 3 * nz];
+            }
+        }
+    }
+    __syncthreads();
+    const int lr = threadIdx.x / T, t = threadIdx.x % T;
+    const bool act = lr < nl;
+    float2 v[E];
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = buf[(t + T * j) * Y::TS + lr];
+    }
+    __syncthreads();   // transpose buffer -> exchange buffers
+    if (act) {
+        fr::line_fft<PY, +1, float2>(v, buf + (size_t)lr * Y::EX, t, group_mask(T), twl);
+        float2* dst = spec + (((size_t)kx * 3 + comp) * nz + z0 + lr) * ny;
+#pragma unroll
+        for (int r = 0; r < E; r++) {
+            const int y = fr::out_index<PY>(t, r);
+            if (y < ny) dst[y] = v[r];
+        }
+    }
+}
+
+static bool split_fast_ok(const ConvK& c)
+{
+    auto p2 = [](int v) { return v >= 32 && v <= 512 && (v & (v - 1)) == 0; };
+    return c.nrep == 1 && p2(c.Py) && p2(c.Pz);
+}
+
+template <int PY, int PZ>
+static cudaError_t launch_split_t(const ConvK& c, const float2* twy, const float2* twz, float2* spec,
+                                  const float* ten6, cudaStream_t st)
+{
+    using Y = SPY<PY>;
+    using Z = SPZ<PZ>;
+    float2* s2 = static_cast<float2*>(c.spec2);
+    const dim3 gy(c.Kx, 3, (c.nz + Y::LN - 1) / Y::LN);
+    cudaError_t e = mlb::launch_pdl(k_sy_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)spec, s2);
+    if (e != cudaSuccess) return e;
+    e = mlb::launch_pdl(k_sz_fast<PZ>, dim3(c.Kx, (c.Py + Z::COLS - 1) / Z::COLS), dim3(SPZ_NT), Z::SMEM, st, c, twz,
+                        s2, ten6);
+    if (e != cudaSuccess) return e;
+    return mlb::launch_pdl(k_syi_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)s2, spec);
+}
+
+template <int PY>
+static cudaError_t launch_split_py(const ConvK& c, const float2* twy, const float2* twz, float2* spec,
+                                   const float* ten6, cudaStream_t st)
+{
+    switch (c.Pz) {
+    case 32: return launch_split_t<PY, 32>(c, twy, twz, spec, ten6, st);
+    case 64: return launch_split_t<PY, 64>(c, twy, twz, spec, ten6, st);
+    case 128: return launch_split_t<PY, 128>(c, twy, twz, spec, ten6, st);
+    case 256: return launch_split_t<PY, 256>(c, twy, twz, spec, ten6, st);
+    case 512: return launch_split_t<PY, 512>(c, twy, twz, spec, ten6, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+static cudaError_t launch_split_fast(const ConvK& c, const float2* twy, const float2* twz, float2* spec,
+                                     const float* ten6, cudaStream_t st)
+{
+    switch (c.Py) {
+    case 32: return launch_split_py<32>(c, twy, twz, spec, ten6, st);
+    case 64: return launch_split_py<64>(c, twy, twz, spec, ten6, st);
+    case 128: return launch_split_py<128>(c, twy, twz, spec, ten6, st);
+    case 256: return launch_split_py<256>(c, twy, twz, spec, ten6, st);
+    case 512: return launch_split_py<512>(c, twy, twz, spec, ten6, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int P>
+static cudaError_t cfg_split()
+{
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_sy_fast<P>, a, (int)SPY<P>::SMEM)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_syi_fast<P>, a, (int)SPY<P>::SMEM)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_sz_fast<P>, a, (int)SPZ<P>::SMEM);
+}
+
 // ------------------------------------------------------------------ fused step
 // (fused_site_v, the per-site arithmetic, is in fused.cuh)
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
@@ -685,7 +947,11 @@ static cudaError_t launch_yz_any(const ConvK& c, const float2* twy, float2* spec
 static cudaError_t yz_pass(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const float* ten6,
                            cudaStream_t st)
 {
-    if (c.split) return launch_conv_split_yz(c, L[1], L[2], tw, spec, ten6, nullptr, 4, st);
+    if (c.split) {
+        if (!split_fast_ok(c)) return launch_conv_split_yz(c, L[1], L[2], tw, spec, ten6, nullptr, 4, st);
+        Prof pf("k_conv_yz_split", st);
+        return launch_split_fast(c, tw + L[1].tw_off, tw + L[2].tw_off, spec, ten6, st);
+    }
     Prof pf("k_conv_yz", st);
     return launch_yz_any(c, tw + L[1].tw_off, spec, ten6, st);
 }
@@ -817,6 +1083,9 @@ cudaError_t conv_fast_configure()
     if ((e = cfg_xs<32>()) || (e = cfg_xs<64>()) || (e = cfg_xs<128>()) || (e = cfg_xs<256>()) || (e = cfg_xs<512>()))
         return e;
     if ((e = cfg_yzr<64, 128>()) || (e = cfg_yzr<128, 128>()) || (e = cfg_yzr<256, 384>()) || (e = cfg_yzr<512, 384>()))
+        return e;
+    if ((e = cfg_split<32>()) || (e = cfg_split<64>()) || (e = cfg_split<128>()) || (e = cfg_split<256>()) ||
+        (e = cfg_split<512>()))
         return e;
     return cudaSuccess;
 }

@@ -24,6 +24,29 @@ __device__ __forceinline__ FastK fastk_resolved(const FastK& F)
     return G;
 }
 
+// Cubic anisotropy field of one axis set at the reduced moment (sx, sy, sz)
+// = S / ms (M/cpu/anisotropy/..._cubic.cpp:308-390): axes n[0..2], n[3..5],
+// n[6..8], constants K[0..2]; quirk keeps (n2s2 + n3s3) in the first K1 term.
+template <typename R>
+__device__ __forceinline__ void cubic_field(R sx, R sy, R sz, const R* n, const R* K, int quirk, R& hx, R& hy,
+                                            R& hz)
+{
+    const R n1s = n[0] * sx + n[1] * sy + n[2] * sz;
+    const R n2s = n[3] * sx + n[4] * sy + n[5] * sz;
+    const R n3s = n[6] * sx + n[7] * sy + n[8] * sz;
+    const R n1s2 = n1s * n1s, n2s2 = n2s * n2s, n3s2 = n3s * n3s;
+    const R n1s3 = n1s2 * n1s, n2s3 = n2s2 * n2s, n3s3 = n3s2 * n3s;
+    const R n1s4 = n1s2 * n1s2, n2s4 = n2s2 * n2s2, n3s4 = n3s2 * n3s2;
+    const R q = quirk ? n3s3 : n3s2;
+    const R a1 = (R)2 * K[0] * n1s * (n2s2 + q), a2 = (R)2 * K[0] * n2s * (n1s2 + n3s2), a3 = (R)2 * K[0] * n3s * (n1s2 + n2s2);
+    const R p = n1s * n2s * n3s;
+    const R b1 = (R)2 * K[1] * p * n2s * n3s, b2 = (R)2 * K[1] * p * n1s * n3s, b3 = (R)2 * K[1] * p * n1s * n2s;
+    const R c1 = (R)4 * K[2] * n1s3 * (n2s4 + n3s4), c2 = (R)4 * K[2] * n2s3 * (n1s4 + n3s4), c3 = (R)4 * K[2] * n3s3 * (n1s4 + n2s4);
+    hx = (n[0] * a1 + n[3] * a2 + n[6] * a3) + (n[0] * b1 + n[3] * b2 + n[6] * b3) + (n[0] * c1 + n[3] * c2 + n[6] * c3);
+    hy = (n[1] * a1 + n[4] * a2 + n[7] * a3) + (n[1] * b1 + n[4] * b2 + n[7] * b3) + (n[1] * c1 + n[4] * c2 + n[7] * c3);
+    hz = (n[2] * a1 + n[5] * a2 + n[8] * a3) + (n[2] * b1 + n[5] * b2 + n[8] * b3) + (n[2] * c1 + n[5] * c2 + n[8] * c3);
+}
+
 // ------------------------------------------------------------------ fused step
 // Uniform-parameter systems: ms, alpha, gamma, anisotropy and thermal scale
 // the same on every site, exchange as a six-direction stencil.  Constants
@@ -66,8 +89,15 @@ __device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int
         Hx += ex; Hy += ey; Hz += ez;
     }
     if (ANI) {
-        const float v = F.ani_c * (Sx * F.axis[0] + Sy * F.axis[1] + Sz * F.axis[2]);
-        Hx += v * F.axis[0]; Hy += v * F.axis[1]; Hz += v * F.axis[2];
+        if (F.ani == 2) {
+            // one uniform cubic axis set
+            float cx, cy, cz;
+            cubic_field<float>(Sx / F.ms, Sy / F.ms, Sz / F.ms, F.cub_n, F.cub_K, F.cub_quirk, cx, cy, cz);
+            Hx += cx; Hy += cy; Hz += cz;
+        } else {
+            const float v = F.ani_c * (Sx * F.axis[0] + Sy * F.axis[1] + Sz * F.axis[2]);
+            Hx += v * F.axis[0]; Hy += v * F.axis[1]; Hz += v * F.axis[2];
+        }
     }
     float Tx = 0.f, Ty = 0.f, Tz = 0.f;
     if (TH) {

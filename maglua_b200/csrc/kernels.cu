@@ -14,6 +14,7 @@
 // Reference semantics are cited per device function (paths relative to the
 // reference project, M/ = src/modules/).
 #include "device.cuh"
+#include "fused.cuh"
 #include "kparams.h"
 #include "launch.h"
 
@@ -148,25 +149,12 @@ __device__ __forceinline__ V3<R> uni_term(const UniK& a, V3<R> sp, R ms, int i)
     return h;
 }
 
-// Cubic (..._cubic.cpp:308-390); quirk keeps (n2s2 + n3s3) in the first K1 term.
+// Cubic (..._cubic.cpp:308-390): cubic_field (fused.cuh) on a V3.
 template <typename R>
 __device__ __forceinline__ V3<R> cub_one(V3<R> s, const R* n, const R* K, int quirk)
 {
-    const R n1s = n[0] * s.x + n[1] * s.y + n[2] * s.z;
-    const R n2s = n[3] * s.x + n[4] * s.y + n[5] * s.z;
-    const R n3s = n[6] * s.x + n[7] * s.y + n[8] * s.z;
-    const R n1s2 = n1s * n1s, n2s2 = n2s * n2s, n3s2 = n3s * n3s;
-    const R n1s3 = n1s2 * n1s, n2s3 = n2s2 * n2s, n3s3 = n3s2 * n3s;
-    const R n1s4 = n1s2 * n1s2, n2s4 = n2s2 * n2s2, n3s4 = n3s2 * n3s2;
-    const R q = quirk ? n3s3 : n3s2;
-    const R a1 = (R)2 * K[0] * n1s * (n2s2 + q), a2 = (R)2 * K[0] * n2s * (n1s2 + n3s2), a3 = (R)2 * K[0] * n3s * (n1s2 + n2s2);
-    const R p = n1s * n2s * n3s;
-    const R b1 = (R)2 * K[1] * p * n2s * n3s, b2 = (R)2 * K[1] * p * n1s * n3s, b3 = (R)2 * K[1] * p * n1s * n2s;
-    const R c1 = (R)4 * K[2] * n1s3 * (n2s4 + n3s4), c2 = (R)4 * K[2] * n2s3 * (n1s4 + n3s4), c3 = (R)4 * K[2] * n3s3 * (n1s4 + n2s4);
     V3<R> h;
-    h.x = (n[0] * a1 + n[3] * a2 + n[6] * a3) + (n[0] * b1 + n[3] * b2 + n[6] * b3) + (n[0] * c1 + n[3] * c2 + n[6] * c3);
-    h.y = (n[1] * a1 + n[4] * a2 + n[7] * a3) + (n[1] * b1 + n[4] * b2 + n[7] * b3) + (n[1] * c1 + n[4] * c2 + n[7] * c3);
-    h.z = (n[2] * a1 + n[5] * a2 + n[8] * a3) + (n[2] * b1 + n[5] * b2 + n[8] * b3) + (n[2] * c1 + n[5] * c2 + n[8] * c3);
+    cubic_field<R>(s.x, s.y, s.z, n, K, quirk, h.x, h.y, h.z);
     return h;
 }
 template <typename R>

@@ -137,9 +137,12 @@ struct FastK {
     int ex;                   // six-direction stencil present
     float J[6];               // J * scale / ms^2 (normalised) or / ms
     int pbc[3];
-    int ani;
+    int ani;                  // 0 none, 1 uniaxial (axis, ani_c), 2 cubic (cub_*)
     float axis[3];
     float ani_c;              // 2 K scale / ms^2
+    float cub_n[9];           // cubic axes n1, n2, n3
+    float cub_K[3];           // cubic K1, K2, K3 (times the global scale)
+    int cub_quirk;
     int th;
     float sigma;              // sqrt(2 alpha T scale / (ms dt gamma))
     uint64_t seed, counter;

@@ -62,6 +62,20 @@ def test_split_fp32_reference_mode(M):
     assert rel_err(h, o.field("Dipole")) <= FIELD_TOL
 
 
+def test_split_fp32_non_power_of_two_plane(M):
+    # periodic y of 40 rows (Py = 40), open z padded to 128: the generic FP32
+    # split passes around the fast x passes
+    dims = (16, 40, 64)
+    n = int(np.prod(dims))
+    s = random_spins(n, 67)
+    h = _dipole_field(M, dims, s, 0.3, open_xy=False, trunc=8)
+    lr = O.LongRange(*dims, O.dipole_tensor(*dims, gmax=(8, 8, 8, 8)))
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    lr.apply(o, 0.3)
+    assert rel_err(h, o.field("Dipole")) <= FIELD_TOL
+
+
 def test_split_fp64_open_direct_sum(M):
     dims = (8, 64, 12)   # plane 128 x 24 at 16 bytes per complex: split
     n = int(np.prod(dims))
