@@ -215,6 +215,48 @@ def run_rk(M, torch, steps=20):
             "how": "mlb_rk_step: eager launches (no graph capture), L2 not flushed"}
 
 
+# ----------------------------------------------------------------- LongRange2D / Dipole2D
+def run_lr2d(M, torch, calls=20):
+    """Dipole2D on the 256x256x8 film (builder truncation 25 x 8 x 8 x 8):
+    field evaluations per second and the layer-mixing kernel against the
+    HBM roofline.  Algorithmic bytes per evaluation: spins in and field out
+    (24 B/site), the x passes' spectrum write and read and the mixing pass's
+    read and write (4 x 24 B per (kx, y, z)), and the tensor spectrum
+    (9 complex per (kx, ky, source, destination))."""
+    ss, _, _ = build_system(M, 0)
+    dip = M.Dipole2D(ss)
+    dip.setTruncation(25, 8, 8, 8)
+    dip.apply(ss)
+    for _ in range(3):
+        dip.apply(ss)
+    st = torch.cuda.ExternalStream(ss.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ss.synchronize()
+    a.record(st)
+    for _ in range(calls):
+        dip.apply(ss)
+    b.record(st)
+    ss.synchronize()
+    ms = a.elapsed_time(b) / calls
+    with M.profile() as prof:
+        for _ in range(calls):
+            dip.apply(ss)
+        ss.synchronize()
+    n = NX * NY * NZ
+    K = (NX // 2 + 1) * NY * NZ
+    q_bytes = 72 * NZ * K
+    total = 24 * n + 96 * K + q_bytes
+    kern = {k: {"avg_us": 1e3 * t / c, "launches": c} for k, (t, c) in prof.kernels.items()}
+    out = {"workload": "Dipole2D (layer-pair tensors, periodic in-plane) on the 256x256x8 film, FP32",
+           "evaluations_per_s": 1e3 / ms, "ms_per_evaluation": ms,
+           "algorithmic_bytes_per_evaluation": total, "achieved_gbs": total / (ms * 1e-3) / 1e9,
+           "kernels": kern, "how": "eager mlb_op_apply calls, CUDA events on the system's stream"}
+    if "k_lr2d_y" in kern:
+        mix = 48 * K + q_bytes
+        out["k_lr2d_y_gbs"] = mix / (kern["k_lr2d_y"]["avg_us"] * 1e-6) / 1e9
+    return out
+
+
 # ----------------------------------------------------------------- 256^3 open cube
 CUBE_DIMS = (256, 256, 256)
 CUBE_WORKLOAD = ("256^3 simple-cubic cube, open boundaries (512^3 padded transform, split (y,z) passes), "
@@ -611,6 +653,7 @@ def main():
     surrogate = run_surrogate(M, torch, min(args.steps, 200)) if not args.no_surrogate else None
     cube = run_cube(M, torch) if not args.no_cube else None
     rk = run_rk(M, torch)
+    lr2d = run_lr2d(M, torch)
 
     if rank != 0:
         if dist:
@@ -667,6 +710,7 @@ def main():
         "surrogate": surrogate,
         "cube_256": cube,
         "rk4": rk,
+        "dipole2d": lr2d,
     }
     print(json.dumps(line), flush=True)
     if dist:

@@ -133,6 +133,8 @@ int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4]);
 #define MLB_OP_DIPOLE 7         /* M/cpu/dipole */
 #define MLB_OP_LONGRANGE 8      /* M/cpu/longrange (user tensor) */
 #define MLB_OP_LONGRANGE3D 9    /* M/cpu/longrange3d */
+#define MLB_OP_LONGRANGE2D 10   /* M/cpu/longrange2d (layer-pair tensors) */
+#define MLB_OP_DIPOLE2D 11      /* M/cpu/dipole2d (LongRange2D + tensor builder) */
 int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out);     /* X.new(nx,ny,nz) */
 int mlb_op_destroy(mlb_op* op);
 int mlb_op_kind(const mlb_op* op, int* kind);
@@ -199,6 +201,36 @@ int mlb_longrange_get_tensor(mlb_op* op, double* const t6[6]);
 /* LongRange3D (spinoperationlongrange3d.cpp:312-424, setMatrix): component
  * ab = 3*a + b in XX..ZZ order, array nx*ny*nz. */
 int mlb_longrange3d_set_tensor(mlb_op* op, int ab, const double* t);
+/* LongRange2D (spinoperationlongrange2d.cpp:201-230 getLAB/setLAB, :430-530
+ * apply, :532-590 layer scales, :605-640 flags).  Layers are 0-based here
+ * (1-based in the Lua API); ab = 3*a + b in XX..ZZ order; each array is
+ * nx*ny, element (x, y) at x + nx*y.  The arrays are copied in and out.
+ * apply reads the arrays set for (dest s, src d) to make the field of layer
+ * d from layer s, as the reference's apply does (qAB[s][d]); the field of
+ * layer d is scaled by dst_field[d] * global scale and each source layer's
+ * moments by src_moment[s].  At apply, new data required fails with
+ * MLB_ESTATE ("make data function not set") for LongRange2D and runs the
+ * builder for Dipole2D; compile required re-transforms the arrays (setting
+ * an array alone does not mark it, as in the reference).  At most 64 layers;
+ * 6*nz*ny complex values of the state precision must fit 227 KB. */
+int mlb_longrange2d_set_tensor(mlb_op* op, int dest, int src, int ab, const double* t);   /* setTensorArray */
+int mlb_longrange2d_get_tensor(mlb_op* op, int dest, int src, int ab, double* t);         /* tensorArray */
+int mlb_longrange2d_set_layer_scales(mlb_op* op, int layer, double src_moment, double dst_field);
+int mlb_longrange2d_get_layer_scales(const mlb_op* op, int layer, double* src_moment, double* dst_field);
+/* setNewDataRequired / setCompileRequired (a negative value leaves a flag) */
+int mlb_longrange2d_set_required(mlb_op* op, int new_data, int compile);
+int mlb_longrange2d_get_required(const mlb_op* op, int* new_data, int* compile);
+/* Dipole2D builder state (dip2d_luafuncs.lua:6-26 defaults, :48-162
+ * setUnitCell / setOffset / setTruncation) and makeData (:540-660).  As in
+ * the reference, changing the builder state does not mark new data
+ * required. */
+int mlb_dipole2d_set_unit_cell(mlb_op* op, int layer, const double ABC[9]);
+int mlb_dipole2d_get_unit_cell(const mlb_op* op, int layer, double ABC[9]);
+int mlb_dipole2d_set_offset(mlb_op* op, int layer, const double off[3]);
+int mlb_dipole2d_get_offset(const mlb_op* op, int layer, double off[3]);
+int mlb_dipole2d_set_truncation(mlb_op* op, const int t[4]);     /* radial, x, y, z */
+int mlb_dipole2d_get_truncation(const mlb_op* op, int t[4]);
+int mlb_dipole2d_make_data(mlb_op* op);
 
 /* ---------------------------------------------------------------- LLG
  * M/cpu/llg/llg.cpp:91-171, llgcartesian.cpp:90-278, llgquat.cpp:126-378. */

@@ -113,6 +113,19 @@ _SIGS = {
     "mlb_longrange_get_matrix": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, _D], C.c_int),
     "mlb_longrange_get_tensor": ([_P, _D * 6], C.c_int),
     "mlb_longrange3d_set_tensor": ([_P, C.c_int, _D], C.c_int),
+    "mlb_longrange2d_set_tensor": ([_P, C.c_int, C.c_int, C.c_int, _D], C.c_int),
+    "mlb_longrange2d_get_tensor": ([_P, C.c_int, C.c_int, C.c_int, _D], C.c_int),
+    "mlb_longrange2d_set_layer_scales": ([_P, C.c_int, C.c_double, C.c_double], C.c_int),
+    "mlb_longrange2d_get_layer_scales": ([_P, C.c_int, _D, _D], C.c_int),
+    "mlb_longrange2d_set_required": ([_P, C.c_int, C.c_int], C.c_int),
+    "mlb_longrange2d_get_required": ([_P, _I, _I], C.c_int),
+    "mlb_dipole2d_set_unit_cell": ([_P, C.c_int, _D], C.c_int),
+    "mlb_dipole2d_get_unit_cell": ([_P, C.c_int, _D], C.c_int),
+    "mlb_dipole2d_set_offset": ([_P, C.c_int, _D], C.c_int),
+    "mlb_dipole2d_get_offset": ([_P, C.c_int, _D], C.c_int),
+    "mlb_dipole2d_set_truncation": ([_P, _I], C.c_int),
+    "mlb_dipole2d_get_truncation": ([_P, _I], C.c_int),
+    "mlb_dipole2d_make_data": ([_P], C.c_int),
     "mlb_llg_create": ([C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_llg_destroy": ([_P], C.c_int),
     "mlb_llg_set_flags": ([_P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
@@ -905,6 +918,164 @@ class LongRange3D(SpinOperation):
         n = self._dims[0] * self._dims[1] * self._dims[2]
         a = _f64(arr, n)
         _ck(_lib.mlb_longrange3d_set_tensor(self._h, _AB9[ab.upper()], _dp(a)))
+
+
+class LongRange2D(SpinOperation):
+    """LongRange2D (M/cpu/longrange2d): in-plane periodic convolution with a
+    9-component tensor array per (destination, source) layer pair, a
+    source-moment scale per source layer and a destination-field scale per
+    destination layer (spinoperationlongrange2d.cpp:430-530).  Layers are
+    1-based, as in the Lua API.  New data is required at first: apply then
+    calls the function given to setMakeDataFunction (fails without one);
+    after setTensorArray, call setCompileRequired() so that apply
+    re-transforms the arrays, as in the reference."""
+    KIND = 10
+
+    def _init_extra(self, rest):
+        self._make = None
+
+    def _layer(self, layer):
+        layer = int(layer)
+        if layer < 1 or layer > self._dims[2]:
+            raise MagLuaError(-1, "Invalid Layer")
+        return layer - 1
+
+    def setTensorArray(self, dest, src, ab, arr):
+        a = _f64(arr, self._dims[0] * self._dims[1])
+        _ck(_lib.mlb_longrange2d_set_tensor(self._h, self._layer(dest), self._layer(src), _AB9[ab.upper()[:2]],
+                                            _dp(a)))
+
+    def tensorArray(self, dest, src, ab):
+        """Copy of the (dest, src) array of component ab, shape (ny, nx)."""
+        out = np.zeros(self._dims[0] * self._dims[1])
+        _ck(_lib.mlb_longrange2d_get_tensor(self._h, self._layer(dest), self._layer(src), _AB9[ab.upper()[:2]],
+                                            _dp(out)))
+        return out.reshape(self._dims[1], self._dims[0])
+
+    def getMatrix(self, dest, src, x, y, ab):
+        """Element (x, y) (1-based) of the (dest, src) array of component ab
+        (longrange2d_luafuncs.lua:6-9)."""
+        return float(self.tensorArray(dest, src, ab)[int(y) - 1, int(x) - 1])
+
+    def _scales(self, layer):
+        a, b = C.c_double(), C.c_double()
+        _ck(_lib.mlb_longrange2d_get_layer_scales(self._h, self._layer(layer), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def setSourceMomentScale(self, layer, v):
+        _, d = self._scales(layer)
+        _ck(_lib.mlb_longrange2d_set_layer_scales(self._h, self._layer(layer), float(v), d))
+
+    def sourceMomentScale(self, layer):
+        return self._scales(layer)[0]
+
+    def setDestinationFieldScale(self, layer, v):
+        sm, _ = self._scales(layer)
+        _ck(_lib.mlb_longrange2d_set_layer_scales(self._h, self._layer(layer), sm, float(v)))
+
+    def destinationFieldScale(self, layer):
+        return self._scales(layer)[1]
+
+    def setStrength(self, *a):
+        raise MagLuaError(-1, "setStrength is depreciated. Please use setSourceMomentScale and setDestinationFieldScale.")
+
+    def strength(self, *a):
+        raise MagLuaError(-1, "strength is depreciated. Please use sourceMomentScale and sestinationFieldScale.")
+
+    def setNewDataRequired(self, on=True):
+        _ck(_lib.mlb_longrange2d_set_required(self._h, int(bool(on)), -1))
+
+    def setCompileRequired(self, on=True):
+        _ck(_lib.mlb_longrange2d_set_required(self._h, -1, int(bool(on))))
+
+    def _required(self):
+        a, b = C.c_int(), C.c_int()
+        _ck(_lib.mlb_longrange2d_get_required(self._h, C.byref(a), C.byref(b)))
+        return bool(a.value), bool(b.value)
+
+    def newDataRequired(self):
+        return self._required()[0]
+
+    def compileRequired(self):
+        return self._required()[1]
+
+    def setMakeDataFunction(self, fn):
+        """fn(op) fills the tensor arrays when new data is required
+        (spinoperationlongrange2d.cpp:366-385)."""
+        if not callable(fn):
+            raise MagLuaError(-1, "function required as argument")
+        self._make = fn
+
+    def makeData(self):
+        if self.newDataRequired():
+            self._make_now()
+
+    def _make_now(self):
+        if self._make is None:
+            raise MagLuaError(-4, "make data function not set")
+        self.setNewDataRequired(False)
+        self._make(self)
+        self.setCompileRequired(True)
+
+    def apply(self, ss):
+        if self._make is not None and self.newDataRequired():
+            self._make_now()
+        super().apply(ss)
+
+
+class Dipole2D(LongRange2D):
+    """Dipole2D (M/cpu/dipole2d): LongRange2D whose arrays come from the
+    point-dipole builder of dip2d_luafuncs.lua:540-660 (unit cell and offset
+    per layer, truncation), run natively on the first apply."""
+    KIND = 11
+
+    def setUnitCell(self, layer, A, B=None, Cv=None):
+        if B is None:
+            A, B, Cv = A[0], A[1], A[2]
+        abc = np.asarray([*A, *B, *Cv], dtype=np.float64)
+        _ck(_lib.mlb_dipole2d_set_unit_cell(self._h, self._layer(layer), _dp(abc)))
+
+    def unitCell(self, layer):
+        out = np.zeros(9)
+        _ck(_lib.mlb_dipole2d_get_unit_cell(self._h, self._layer(layer), _dp(out)))
+        return list(out[0:3]), list(out[3:6]), list(out[6:9])
+
+    def setOffset(self, layer, v):
+        a = np.asarray(v, dtype=np.float64)
+        _ck(_lib.mlb_dipole2d_set_offset(self._h, self._layer(layer), _dp(a)))
+
+    def offset(self, layer=None):
+        if layer is None:
+            return [self.offset(z + 1) for z in range(self._dims[2])]
+        out = np.zeros(3)
+        _ck(_lib.mlb_dipole2d_get_offset(self._h, self._layer(layer), _dp(out)))
+        return list(out)
+
+    def truncation(self):
+        t = (C.c_int * 4)()
+        _ck(_lib.mlb_dipole2d_get_truncation(self._h, t))
+        return tuple(t)
+
+    def setTruncation(self, trunc=None, tx=None, ty=None, tz=None):
+        cur = list(self.truncation())
+        for i, v in enumerate((trunc, tx, ty, tz)):
+            if v is not None:
+                cur[i] = int(v)
+        _ck(_lib.mlb_dipole2d_set_truncation(self._h, (C.c_int * 4)(*cur)))
+
+    def _make_now(self):
+        if self._make is not None:
+            return super()._make_now()
+        _ck(_lib.mlb_dipole2d_make_data(self._h))
+
+    def makeData(self):
+        if self.newDataRequired():
+            self._make_now()
+
+    def apply(self, ss):
+        if self.newDataRequired():
+            self._make_now()
+        SpinOperation.apply(self, ss)
 
 
 # ====================================================================== LLG

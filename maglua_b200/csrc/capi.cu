@@ -167,6 +167,17 @@ struct ConvPlan {
     unsigned long long spec_token = 0;
 };
 
+// LongRange2D / Dipole2D: the per-kx layer-mixing convolution and its
+// tensor spectrum Q[kx][ky][s][d][9] (complex, state precision).
+struct LR2DPlan {
+    ConvK k;
+    FftLen L[3];
+    int rb = 4;
+    DBuf<char> tw;
+    DBuf<char> spec;
+    DBuf<char> Q;
+};
+
 } // namespace
 
 // ====================================================================== objects
@@ -285,6 +296,18 @@ struct mlb_op {
     std::vector<double> t9[9];
     bool plan_dirty = true;
     std::unique_ptr<ConvPlan> plan;
+    // LongRange2D / Dipole2D: the arrays set for (dest i, src j), component
+    // ab, at [((i nz + j) 9 + ab) nx ny + y nx + x] (allocated on first use);
+    // per-layer source-moment and destination-field scales; the reference's
+    // newDataRequired / compileRequired flags
+    std::vector<double> t2;
+    std::vector<double> lr2_src, lr2_dst;
+    bool lr2_newdata = true, lr2_compile = true;
+    // Dipole2D builder: unit cell A, B, C per layer, offset per layer,
+    // truncation {radial, x, y, z}
+    std::vector<double> d2_abc, d2_off;
+    int d2_trunc[4] = {25, 25, 25, 25};
+    std::unique_ptr<LR2DPlan> lr2;
 };
 
 struct mlb_llg {
@@ -741,6 +764,156 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
     op->plan_dirty = false;
 }
 
+// ------------------------------------------------------------------ LongRange2D / Dipole2D
+bool is_lr2d(int kind) { return kind == MLB_OP_LONGRANGE2D || kind == MLB_OP_DIPOLE2D; }
+
+void ensure_t2(mlb_op* op)
+{
+    const size_t n = (size_t)op->nz * op->nz * 9 * op->nx * op->ny;
+    if (op->t2.size() != n) op->t2.assign(n, 0.0);
+}
+
+// Point-dipole tensor elements of the Dipole2D builder (demag.cpp:3-56):
+// d2_xx(X, Y, Z) = -(1/r^3 - 3 X X / r^5), d2_xy(X, Y, Z) = 3 X Y / r^5 with
+// r = |(X, Y, Z)| summed in argument order, zero at r < 1e-80; the other
+// seven elements are these two with permuted arguments.
+double d2_xx(double X, double Y, double Z)
+{
+    const double r = std::sqrt(X * X + Y * Y + Z * Z);
+    if (r < 1e-80) return 0.0;
+    const double ir = 1.0 / r;
+    const double ir3 = ir * ir * ir;
+    const double ir5 = ir3 * ir * ir;
+    return -1.0 * (ir3 - 3.0 * X * X * ir5);
+}
+double d2_xy(double X, double Y, double Z)
+{
+    const double r = std::sqrt(X * X + Y * Y + Z * Z);
+    if (r < 1e-80) return 0.0;
+    const double ir = 1.0 / r;
+    const double ir3 = ir * ir * ir;
+    const double ir5 = ir3 * ir * ir;
+    return -1.0 * (-3.0 * X * Y * ir5);
+}
+
+// Dipole2D makeData (dip2d_luafuncs.lua:540-660): zero every array, then for
+// each (dest, src) with |src - dest| <= truncation z and each (X, Y) in the x
+// and y truncation ranges add the nine elements of r = p_src - p_dest at
+// (X mod nx, Y mod ny), positions from idx2pos (:516-538).  Both positions
+// are taken at the same (X, Y), so r is the offset between the layers alone,
+// and idx2pos takes the x part of the B step from B's y component; both as
+// in the reference.
+void dipole2d_make(mlb_op* op)
+{
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    ensure_t2(op);
+    std::fill(op->t2.begin(), op->t2.end(), 0.0);
+    const size_t plane = (size_t)nx * ny;
+    auto pos = [&](int i, int j, int layer, double out[3]) {
+        double dz[3] = {0, 0, 0};
+        for (int Z = 0; Z < layer; Z++)
+            for (int c = 0; c < 3; c++) dz[c] = dz[c] + op->d2_abc[Z * 9 + 6 + c];
+        const double* A = &op->d2_abc[0];
+        const double* B = &op->d2_abc[3];
+        const double di[3] = {i * A[0], i * A[1], i * A[2]};
+        const double dj[3] = {j * B[1], j * B[1], j * B[2]};
+        const double* off = &op->d2_off[layer * 3];
+        for (int c = 0; c < 3; c++) out[c] = di[c] + dj[c] + dz[c] + off[c];
+    };
+    const int tX = op->d2_trunc[1], tY = op->d2_trunc[2], tZ = op->d2_trunc[3];
+    for (int d = 0; d < nz; d++)
+        for (int sidx = 0; sidx < nz; sidx++) {
+            if (std::abs(sidx - d) > tZ) continue;
+            double* T = &op->t2[((size_t)d * nz + sidx) * 9 * plane];
+            for (int X = -tX; X <= tX; X++)
+                for (int Y = -tY; Y <= tY; Y++) {
+                    double pd[3], ps[3];
+                    pos(X, Y, d, pd);
+                    pos(X, Y, sidx, ps);
+                    const double rx = ps[0] - pd[0], ry = ps[1] - pd[1], rz = ps[2] - pd[2];
+                    int x = X, y = Y;
+                    if (x < 0) x += 100000 * nx;
+                    if (y < 0) y += 100000 * ny;
+                    x %= nx;
+                    y %= ny;
+                    // NXX NXY NXZ / NYX NYY NYZ / NZX NZY NZZ
+                    const double v[9] = {d2_xx(rx, ry, rz), d2_xy(rx, ry, rz), d2_xy(rx, rz, ry),
+                                         d2_xy(ry, rx, rz), d2_xx(ry, rx, rz), d2_xy(ry, rz, rx),
+                                         d2_xy(rz, rx, ry), d2_xy(rz, ry, rx), d2_xx(rz, rx, ry)};
+                    const size_t at = (size_t)y * nx + x;
+                    for (int ab = 0; ab < 9; ab++) T[ab * plane + at] += v[ab];
+                }
+        }
+    op->lr2_newdata = false;
+    op->lr2_compile = true;
+}
+
+// compile (spinoperationlongrange2d.cpp:387-430): 2D transforms of every
+// array in FP64 on the GPU, divided by nx ny, stored in the state precision
+// rb.  The layer pairs go through a bounded FP64 work buffer in batches.
+void build_lr2d(mlb_op* op, cudaStream_t st, int rb)
+{
+    if (!op->lr2_compile && op->lr2 && op->lr2->rb == rb) return;
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    if (nz > MLB_LR2D_MAXZ) fail(MLB_EUNSUP, "LongRange2D supports at most 64 layers");
+    std::unique_ptr<LR2DPlan> P(new LR2DPlan());
+    P->rb = rb;
+    ConvK& k = P->k;
+    memset(&k, 0, sizeof(k));
+    k.nx = nx; k.ny = ny; k.nz = nz;
+    k.Px = nx; k.Py = ny; k.Pz = 1;
+    k.Kx = nx / 2 + 1;
+    k.general = 1;
+    k.nrep = 1;
+    const size_t cb = (size_t)2 * rb;
+    int ty = 16;
+    while (ty > 1 && (size_t)2 * ty * k.Px * cb > 96 * 1024) ty /= 2;
+    k.ty = ty;
+    if ((size_t)2 * k.Px * cb > 96 * 1024) fail(MLB_EUNSUP, "x length too large");
+    if (mlb::lr2d_smem(k, rb) > 227 * 1024)
+        fail(MLB_EUNSUP, "LongRange2D: 3 nz ny spectrum values per kx exceed shared memory at " +
+                             std::to_string(8 * rb) + "-bit precision");
+    std::vector<float2> twf;
+    std::vector<double2> twd;
+    const int lens[3] = {nx, ny, 1};
+    for (int a = 0; a < 3; a++) {
+        P->L[a] = make_len(lens[a], (int)twf.size());
+        append_twiddles(twf, lens[a]);
+        append_twiddles(twd, lens[a]);
+    }
+    if (rb == 8) {
+        P->tw.alloc(sizeof(double2) * twd.size());
+        CK(cudaMemcpy(P->tw.p, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice));
+    } else {
+        P->tw.alloc(sizeof(float2) * twf.size());
+        CK(cudaMemcpy(P->tw.p, twf.data(), sizeof(float2) * twf.size(), cudaMemcpyHostToDevice));
+    }
+    DBuf<double2> twdd;
+    twdd.alloc(twd.size());
+    CK(cudaMemcpy(twdd.p, twd.data(), sizeof(double2) * twd.size(), cudaMemcpyHostToDevice));
+    ensure_t2(op);
+    const size_t plane = (size_t)nx * ny;
+    const int npair = nz * nz;
+    P->Q.alloc((size_t)k.Kx * ny * npair * 9 * cb);
+    // batch of layer pairs whose FP64 transforms fit 256 MB
+    int bp = (int)std::max<size_t>(1, ((size_t)256 << 20) / (plane * 9 * sizeof(double2)));
+    bp = std::min(bp, npair);
+    DBuf<double2> W;
+    W.alloc(plane * 9 * bp);
+    std::vector<double2> h(plane * 9 * bp);
+    for (int p0 = 0; p0 < npair; p0 += bp) {
+        const int np = std::min(bp, npair - p0);
+        for (size_t i = 0; i < plane * 9 * np; i++) h[i] = make_double2(op->t2[(size_t)p0 * 9 * plane + i], 0.0);
+        CK(cudaMemcpyAsync(W.p, h.data(), sizeof(double2) * plane * 9 * np, cudaMemcpyHostToDevice, st));
+        CK(mlb::launch_fft3d_d(W.p, 9 * np, nx, ny, 1, P->L, twdd.p, -1, st));
+        CK(mlb::launch_lr2d_pack(W.p, nx, ny, nz, p0, np, P->Q.p, rb, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    P->spec.alloc((size_t)k.Kx * 3 * nz * ny * cb);
+    op->lr2 = std::move(P);
+    op->lr2_compile = false;
+}
+
 // ------------------------------------------------------------------ lazy evaluation
 struct TermsBuild {
     TermsK T;
@@ -996,7 +1169,7 @@ void op_apply(mlb_op* op, mlb_system* s)
 {
     check_dims(op, s);
     const int si = slot_register(s, op->slot.c_str());
-    if (s->pend_op && (is_conv(op->kind) || si == s->pend_si)) flush_pending(s);
+    if (s->pend_op && (is_conv(op->kind) || is_lr2d(op->kind) || si == s->pend_si)) flush_pending(s);
     before_mutate(s, si);
     Slot& sl = s->slots[si];
     Term t{};
@@ -1062,6 +1235,35 @@ void op_apply(mlb_op* op, mlb_system* s)
         for (int a = 0; a < 3; a++) t.B[a] = op->B[a] * op->gs;
         sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
         return;
+    case MLB_OP_LONGRANGE2D:
+    case MLB_OP_DIPOLE2D: {
+        // apply (spinoperationlongrange2d.cpp:430-530): makeNewData when new
+        // data is required, compile when required, then the convolution
+        if (op->lr2_newdata) {
+            if (s->capturing) fail(MLB_ESTATE, "tensor changed during capture");
+            if (op->kind != MLB_OP_DIPOLE2D) fail(MLB_ESTATE, "make data function not set");
+            dipole2d_make(op);
+        }
+        if (s->capturing && (op->lr2_compile || !op->lr2 || op->lr2->rb != s->rb))
+            fail(MLB_ESTATE, "tensor changed during capture");
+        build_lr2d(op, s->st, s->rb);
+        sl.used = true;
+        sl.terms.clear();
+        sl.base_data = false;
+        slot_alloc(s, sl);
+        sl.state = ST_DATA;
+        if (s->dry) return;
+        LR2DPlan& P = *op->lr2;
+        LR2DScale sc;
+        memset(&sc, 0, sizeof(sc));
+        for (int z = 0; z < op->nz; z++) {
+            sc.src[z] = op->lr2_src[z];
+            sc.dst[z] = op->lr2_dst[z] * op->gs;
+        }
+        const void* sp[3] = {s->sp[s->cur][0], s->sp[s->cur][1], s->sp[s->cur][2]};
+        CK(mlb::launch_lr2d(P.k, P.L, P.tw.p, sp, P.spec.p, P.Q.p, sc, sl.h, s->rb, s->st));
+        return;
+    }
     case MLB_OP_DIPOLE:
     case MLB_OP_LONGRANGE:
     case MLB_OP_LONGRANGE3D: {
@@ -1154,6 +1356,7 @@ bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, dou
         for (int q = 0; q < 9; q++) F.cub_n[q] = (float)T.cub.axes[q];
         for (int q = 0; q < 3; q++) F.cub_K[q] = (float)T.cub.K[q];
         F.cub_quirk = T.cub.quirk;
+        F.cub_ims = (float)(1.0 / ms);
     }
     F.th = T.th.mode == TH_PHILOX && T.th.T != 0.0 && g > 0;
     if (F.th) {
@@ -2356,7 +2559,16 @@ int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out)
         case MLB_OP_DIPOLE: op->slot = "Dipole"; break;
         case MLB_OP_LONGRANGE: op->slot = "LongRange"; break;
         case MLB_OP_LONGRANGE3D: op->slot = "LongRange3D"; break;
+        case MLB_OP_LONGRANGE2D: op->slot = "LongRange2D"; break;
+        case MLB_OP_DIPOLE2D: op->slot = "Dipole2D"; break;
         default: fail(MLB_EINVAL, "unknown operator kind");
+        }
+        if (is_lr2d(kind)) {
+            op->lr2_src.assign(nz, 1.0);
+            op->lr2_dst.assign(nz, 1.0);
+            op->d2_abc.assign((size_t)nz * 9, 0.0);
+            for (int z = 0; z < nz; z++) op->d2_abc[z * 9] = op->d2_abc[z * 9 + 4] = op->d2_abc[z * 9 + 8] = 1.0;
+            op->d2_off.assign((size_t)nz * 3, 0.0);
         }
         *out = op.release();
     });
@@ -2768,6 +2980,145 @@ int mlb_longrange3d_set_tensor(mlb_op* op, int ab, const double* t)
         const size_t n = (size_t)op->nx * op->ny * op->nz;
         op->t9[ab].assign(t, t + n);
         op->plan_dirty = true;
+    });
+}
+
+// ---------------------------------------------------------------- LongRange2D / Dipole2D
+static void need_lr2d(const mlb_op* op)
+{
+    if (!op || !is_lr2d(op->kind)) fail(MLB_EINVAL, "not a LongRange2D operator");
+}
+static void need_layer(const mlb_op* op, int layer)
+{
+    if (layer < 0 || layer >= op->nz) fail(MLB_EINVAL, "Invalid Layer");
+}
+
+int mlb_longrange2d_set_tensor(mlb_op* op, int dest, int src, int ab, const double* t)
+{
+    return guard([&] {
+        g_version++;
+        need_lr2d(op);
+        need_layer(op, dest);
+        need_layer(op, src);
+        if (ab < 0 || ab > 8) fail(MLB_EINVAL, "tensor component must be 0..8");
+        ensure_t2(op);
+        const size_t plane = (size_t)op->nx * op->ny;
+        std::copy(t, t + plane, op->t2.begin() + (((size_t)dest * op->nz + src) * 9 + ab) * plane);
+    });
+}
+
+int mlb_longrange2d_get_tensor(mlb_op* op, int dest, int src, int ab, double* t)
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, dest);
+        need_layer(op, src);
+        if (ab < 0 || ab > 8) fail(MLB_EINVAL, "tensor component must be 0..8");
+        ensure_t2(op);
+        const size_t plane = (size_t)op->nx * op->ny;
+        const double* a = op->t2.data() + (((size_t)dest * op->nz + src) * 9 + ab) * plane;
+        std::copy(a, a + plane, t);
+    });
+}
+
+int mlb_longrange2d_set_layer_scales(mlb_op* op, int layer, double src_moment, double dst_field)
+{
+    return guard([&] {
+        g_version++;
+        need_lr2d(op);
+        need_layer(op, layer);
+        op->lr2_src[layer] = src_moment;
+        op->lr2_dst[layer] = dst_field;
+    });
+}
+
+int mlb_longrange2d_get_layer_scales(const mlb_op* op, int layer, double* src_moment, double* dst_field)
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        *src_moment = op->lr2_src[layer];
+        *dst_field = op->lr2_dst[layer];
+    });
+}
+
+int mlb_longrange2d_set_required(mlb_op* op, int new_data, int compile)
+{
+    return guard([&] {
+        g_version++;
+        need_lr2d(op);
+        if (new_data >= 0) op->lr2_newdata = new_data != 0;
+        if (compile >= 0) op->lr2_compile = compile != 0;
+    });
+}
+
+int mlb_longrange2d_get_required(const mlb_op* op, int* new_data, int* compile)
+{
+    return guard([&] {
+        need_lr2d(op);
+        *new_data = op->lr2_newdata ? 1 : 0;
+        *compile = op->lr2_compile ? 1 : 0;
+    });
+}
+
+int mlb_dipole2d_set_unit_cell(mlb_op* op, int layer, const double ABC[9])
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        std::copy(ABC, ABC + 9, op->d2_abc.begin() + (size_t)layer * 9);
+    });
+}
+
+int mlb_dipole2d_get_unit_cell(const mlb_op* op, int layer, double ABC[9])
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        std::copy(op->d2_abc.begin() + (size_t)layer * 9, op->d2_abc.begin() + (size_t)layer * 9 + 9, ABC);
+    });
+}
+
+int mlb_dipole2d_set_offset(mlb_op* op, int layer, const double off[3])
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        std::copy(off, off + 3, op->d2_off.begin() + (size_t)layer * 3);
+    });
+}
+
+int mlb_dipole2d_get_offset(const mlb_op* op, int layer, double off[3])
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        std::copy(op->d2_off.begin() + (size_t)layer * 3, op->d2_off.begin() + (size_t)layer * 3 + 3, off);
+    });
+}
+
+int mlb_dipole2d_set_truncation(mlb_op* op, const int t[4])
+{
+    return guard([&] {
+        need_lr2d(op);
+        for (int i = 0; i < 4; i++) op->d2_trunc[i] = t[i];
+    });
+}
+
+int mlb_dipole2d_get_truncation(const mlb_op* op, int t[4])
+{
+    return guard([&] {
+        need_lr2d(op);
+        for (int i = 0; i < 4; i++) t[i] = op->d2_trunc[i];
+    });
+}
+
+int mlb_dipole2d_make_data(mlb_op* op)
+{
+    return guard([&] {
+        g_version++;
+        if (!op || op->kind != MLB_OP_DIPOLE2D) fail(MLB_EINVAL, "not a Dipole2D operator");
+        dipole2d_make(op);
     });
 }
 

@@ -524,12 +524,21 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     extern __shared__ float2 sm[];
     float2* twl = sm;
     float2* buf = sm + PZ;
+    const int nz = c.nz, Py = c.Py;
+    const int kx = blockIdx.x, ky0 = blockIdx.y * COLS;
+    const int ncol = min(COLS, Py - ky0);
+    const float* Tb = ten6 + ((size_t)kx * Py + ky0) * PZ * 6;
+    if (threadIdx.x == 0) {
+        // the columns' tensor rows (constant across steps) start towards L2
+        // while the z transforms run
+        const unsigned bytes = (unsigned)(ncol * PZ * 6 * sizeof(float));
+        if ((((uintptr_t)Tb) & 15) == 0 && (bytes & 15) == 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tb), "r"(bytes) : "memory");
+    }
     for (int k = threadIdx.x; k < PZ; k += SPZ_NT) twl[k] = twz[k];
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
-    const int nz = c.nz, Py = c.Py;
-    const int kx = blockIdx.x, ky0 = blockIdx.y * COLS;
     const int lr = threadIdx.x / T, t = threadIdx.x % T;
     const int col = lr / 3, comp = lr - 3 * col;
     const bool act = lr < 3 * COLS && ky0 + col < Py;   // whole T-lane groups share act
@@ -552,8 +561,6 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     // tensor multiply, point p = (column, kz): consecutive threads take
     // consecutive kz, so the tensor rows [kx][ky][kz][6] stream contiguously
     const float gg = c.g;
-    const int ncol = min(COLS, Py - ky0);
-    const float* Tb = ten6 + ((size_t)kx * Py + ky0) * PZ * 6;
     for (int p = threadIdx.x; p < ncol * PZ; p += SPZ_NT) {
         const int cl = p / PZ, kz = p % PZ;
         const float* Tp = Tb + (size_t)p * 6;
@@ -581,7 +588,7 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
 }
 
 template <int PY>
-__global__ void __launch_bounds__(SPL_NT, 2) k_syi_fast(ConvK c, const float2* __restrict__ twy,
+__global__ void __launch_bounds__(SPL_NT, 3) k_syi_fast(ConvK c, const float2* __restrict__ twy,
                                                         const float2* __restrict__ s2, float2* __restrict__ spec)
 {
     using Y = SPY<PY>;
@@ -1109,6 +1116,16 @@ cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw
 }
 
 // ------------------------------------------------------------------ fused x pass dispatch
+bool x_fast_ok(const ConvK& c) { return pow2_in(c.Px, 16, 512) && c.Px == c.nx; }
+
+cudaError_t launch_x_pass_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
+                               float* h[3], bool fwd, cudaStream_t st)
+{
+    if (!x_fast_ok(c)) return cudaErrorInvalidValue;
+    Prof pf(fwd ? "k_conv_fx" : "k_conv_ix", st);
+    return launch_x_any(c, tw + L[0].tw_off, s, spec, h, st, fwd);
+}
+
 cudaError_t launch_conv_fast_fyz(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                                  const float* ten6, bool with_fx, cudaStream_t st)
 {

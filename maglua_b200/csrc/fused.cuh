@@ -92,7 +92,8 @@ __device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int
         if (F.ani == 2) {
             // one uniform cubic axis set
             float cx, cy, cz;
-            cubic_field<float>(Sx / F.ms, Sy / F.ms, Sz / F.ms, F.cub_n, F.cub_K, F.cub_quirk, cx, cy, cz);
+            cubic_field<float>(Sx * F.cub_ims, Sy * F.cub_ims, Sz * F.cub_ims, F.cub_n, F.cub_K, F.cub_quirk, cx,
+                               cy, cz);
             Hx += cx; Hy += cy; Hz += cz;
         } else {
             const float v = F.ani_c * (Sx * F.axis[0] + Sy * F.axis[1] + Sz * F.axis[2]);

@@ -811,6 +811,57 @@ __global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx,
     }
 }
 
+// ------------------------------------------------------------ LongRange2D
+// Layer-pair convolution, periodic in x and y (spinoperationlongrange2d.cpp:
+// 430-530).  Between the x passes of the dipole convolution (k_conv_fx,
+// k_conv_ix with Px = nx), one CTA per kx:
+//   y transforms of the 3 nz spectrum rows (comp, z);
+//   for each ky, destination layer d and component a:
+//     H_a[d] = dst[d] * sum_s src[s] sum_b Q[kx][ky][s][d][a][b] M_b[s]
+//   (Q: 2D transform over nx ny of the arrays set for (s, d), divided by
+//   nx ny -- the reference's apply reads its tensors [s][d]);
+//   inverse y transforms back to SPEC.
+template <typename R>
+__global__ void __launch_bounds__(512) k_lr2d_y(ConvK c, FftLen Ly, const typename CT<R>::T* tw,
+                                                typename CT<R>::T* spec, const typename CT<R>::T* Q, LR2DScale sc)
+{
+    if (c.run_if && *c.run_if == 0) return;
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* smf = reinterpret_cast<C*>(smraw);
+    const int kx = blockIdx.x, ny = c.ny, nz = c.nz;
+    const int NL = 3 * nz;   // lines (comp, z), rows of SPEC[kx]
+    C* A = smf;
+    C* B = smf + (size_t)NL * ny;
+    C* sp = spec + (size_t)kx * NL * ny;
+    for (int t = threadIdx.x; t < NL * ny; t += blockDim.x) A[t] = sp[t];
+    __syncthreads();
+    LineGeo g;
+    g.nlines = NL; g.lpg = 1 << 30; g.gstride = 0; g.ls = ny; g.es = 1; g.line_fast = 0;
+    C* cur = ny > 1 ? cta_fft<C>(A, B, g, Ly, tw, -1) : A;
+    C* oth = cur == A ? B : A;
+    const C* Qk = Q + (size_t)kx * ny * nz * nz * 9;
+    for (int t = threadIdx.x; t < NL * ny; t += blockDim.x) {
+        const int a = t % 3, rest = t / 3, d = rest % nz, ky = rest / nz;
+        C acc = cmk<C>((R)0, (R)0);
+        for (int s = 0; s < nz; s++) {
+            const C* q = Qk + (((size_t)ky * nz + s) * nz + d) * 9 + 3 * a;
+            const R w = (R)sc.src[s];
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const C m = cur[((size_t)b * nz + s) * ny + ky];
+                const C qq = q[b];
+                acc = cadd(acc, cmul(cmk<C>(w * qq.x, w * qq.y), m));
+            }
+        }
+        const R wd = (R)sc.dst[d];
+        oth[((size_t)a * nz + d) * ny + ky] = cmk<C>(wd * acc.x, wd * acc.y);
+    }
+    __syncthreads();
+    cur = ny > 1 ? cta_fft<C>(oth, cur, g, Ly, tw, +1) : oth;
+    for (int t = threadIdx.x; t < NL * ny; t += blockDim.x) sp[t] = cur[t];
+}
+
 // ------------------------------------------------------------ split (y,z) passes
 // For (y,z) planes larger than one CTA's shared memory (a 256^3 open cube
 // pads to 512 x 512 planes): the plane pass of k_conv_yz done as three
@@ -1113,6 +1164,7 @@ cudaError_t conv_configure()
     if ((e = max_smem(k_split_y<float>)) || (e = max_smem(k_split_y<double>)) || (e = max_smem(k_split_yi<float>)) ||
         (e = max_smem(k_split_yi<double>)) || (e = max_smem(k_split_z<float>)) || (e = max_smem(k_split_z<double>)))
         return e;
+    if ((e = max_smem(k_lr2d_y<float>)) || (e = max_smem(k_lr2d_y<double>))) return e;
     return max_smem(k_fft_lines<double2>);
 }
 
@@ -1195,6 +1247,83 @@ cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const 
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// LongRange2D tensor: Q[kx][ky][s][d][ab] = W_{(s d ab)}(kx, ky) / (nx ny) for
+// the layer pairs p0 .. p0 + np - 1 (p = s nz + d), W holding their
+// transforms [(p - p0) 9 + ab][ky][kx] over the full x length.
+template <typename R>
+__global__ void k_lr2d_pack(const double2* W, int nx, int ny, int nz, int Kx, int p0, int np,
+                            typename CT<R>::T* Q)
+{
+    const long long total = (long long)Kx * ny * np * 9;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int ab = (int)(e % 9);
+    long long r = e / 9;
+    const int pl = (int)(r % np);
+    r /= np;
+    const int ky = (int)(r % ny), kx = (int)(r / ny);
+    const double inv = 1.0 / ((double)nx * ny);
+    const double2 v = W[((size_t)pl * 9 + ab) * nx * ny + (size_t)ky * nx + kx];
+    const size_t o = (((size_t)kx * ny + ky) * nz * nz + p0 + pl) * 9 + ab;
+    Q[o] = cmk<typename CT<R>::T>((R)(v.x * inv), (R)(v.y * inv));
+}
+
+cudaError_t launch_lr2d_pack(const double2* W, int nx, int ny, int nz, int p0, int np, void* Q, int rb,
+                             cudaStream_t st)
+{
+    const int Kx = nx / 2 + 1;
+    const long long total = (long long)Kx * ny * np * 9;
+    if (rb == 8)
+        k_lr2d_pack<double><<<blocks_for(total, 256), 256, 0, st>>>(W, nx, ny, nz, Kx, p0, np, static_cast<double2*>(Q));
+    else
+        k_lr2d_pack<float><<<blocks_for(total, 256), 256, 0, st>>>(W, nx, ny, nz, Kx, p0, np, static_cast<float2*>(Q));
+    return cudaGetLastError();
+}
+
+size_t lr2d_smem(const ConvK& c, int rb) { return (size_t)6 * c.nz * c.ny * 2 * rb; }
+
+// x passes: the FP32 power-of-two kernels of conv_fast.cu where they apply
+// (x_fast_ok), else the generic mixed-radix ones
+template <typename R>
+static void lr2d_t(const ConvK& c, const FftLen L[3], const void* tw_, const void* const s[3], void* spec_,
+                   const void* Q, const LR2DScale& sc, void* const h[3], cudaStream_t st)
+{
+    typedef typename CT<R>::T C;
+    const C* tw = static_cast<const C*>(tw_);
+    C* spec = static_cast<C*>(spec_);
+    dim3 gx(blocks_for(c.ny, c.ty), c.nz);
+    const bool fast = sizeof(R) == 4 && x_fast_ok(c);
+    const float* sf[3] = {static_cast<const float*>(s[0]), static_cast<const float*>(s[1]),
+                          static_cast<const float*>(s[2])};
+    float* hf[3] = {static_cast<float*>(h[0]), static_cast<float*>(h[1]), static_cast<float*>(h[2])};
+    if (fast) {
+        launch_x_pass_fast(c, L, reinterpret_cast<const float2*>(tw), sf, reinterpret_cast<float2*>(spec), hf, true,
+                           st);
+    } else {
+        Prof pf("k_conv_fx", st);
+        k_conv_fx<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, L[0], tw, s[0], s[1], s[2], spec);
+    }
+    {
+        Prof pf("k_lr2d_y", st);
+        k_lr2d_y<R><<<c.Kx, 512, lr2d_smem(c, sizeof(R)), st>>>(c, L[1], tw, spec, static_cast<const C*>(Q), sc);
+    }
+    if (fast) {
+        launch_x_pass_fast(c, L, reinterpret_cast<const float2*>(tw), sf, reinterpret_cast<float2*>(spec), hf, false,
+                           st);
+    } else {
+        Prof pf("k_conv_ix", st);
+        k_conv_ix<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, L[0], tw, spec, h[0], h[1], h[2]);
+    }
+}
+
+cudaError_t launch_lr2d(const ConvK& c, const FftLen L[3], const void* tw, const void* const s[3], void* spec,
+                        const void* Q, const LR2DScale& sc, void* const h[3], int rb, cudaStream_t st)
+{
+    if (rb == 8) lr2d_t<double>(c, L, tw, s, spec, Q, sc, h, st);
+    else lr2d_t<float>(c, L, tw, s, spec, Q, sc, h, st);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,

@@ -130,6 +130,15 @@ struct ConvK {
     void* spec2;
 };
 
+// LongRange2D layer scales (spinoperationlongrange2d.cpp:430-530): the
+// source-moment scale of each source layer and the destination-field scale
+// of each destination layer times the operator's global scale.
+#define MLB_LR2D_MAXZ 64
+struct LR2DScale {
+    double src[MLB_LR2D_MAXZ];
+    double dst[MLB_LR2D_MAXZ];
+};
+
 // Fused step for uniform-parameter systems (k_fused_fast): every constant
 // folded on the host.
 struct FastK {
@@ -143,6 +152,7 @@ struct FastK {
     float cub_n[9];           // cubic axes n1, n2, n3
     float cub_K[3];           // cubic K1, K2, K3 (times the global scale)
     int cub_quirk;
+    float cub_ims;            // 1 / ms (the reduced moment S / ms)
     int th;
     float sigma;              // sqrt(2 alpha T scale / (ms dt gamma))
     uint64_t seed, counter;

@@ -63,6 +63,11 @@ struct Prof {
 cudaError_t fftreg_init();
 cudaError_t conv_fast_configure();
 bool conv_fast_ok(const ConvK& c);
+// FP32 x passes alone (power-of-two periodic x, 16..512): the forward
+// transform of the spins to SPEC (fwd) or the inverse to the field h.
+bool x_fast_ok(const ConvK& c);
+cudaError_t launch_x_pass_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
+                               float* h[3], bool fwd, cudaStream_t st);
 cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                              const float* ten6, float* h[3], cudaStream_t st);
 // The (y,z) pass, optionally preceded by the forward x pass, without the
@@ -108,6 +113,14 @@ cudaError_t launch_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, in
                                       const double2* W, double* out, cudaStream_t st);
 cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int Px, int Py, int Pz,
                                double2* W, cudaStream_t st);
+// LongRange2D: x passes around the per-kx layer mixing (k_lr2d_y); the
+// tensor spectrum Q[kx][ky][s][d][9] packed from FP64 transforms of the
+// layer pairs p0 .. p0 + np - 1.
+size_t lr2d_smem(const ConvK& c, int rb);
+cudaError_t launch_lr2d(const ConvK& c, const FftLen L[3], const void* tw, const void* const s[3], void* spec,
+                        const void* Q, const LR2DScale& sc, void* const h[3], int rb, cudaStream_t st);
+cudaError_t launch_lr2d_pack(const double2* W, int nx, int ny, int nz, int p0, int np, void* Q, int rb,
+                             cudaStream_t st);
 cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const FftLen L[3],
                            const double2* tw, int sign, cudaStream_t st);
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,

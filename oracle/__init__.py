@@ -5,6 +5,7 @@ Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
 this package; the product (maglua_b200) never does.
 """
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -373,6 +374,89 @@ def dipole_direct(ss, g, periodic=(0, 0, 0), ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
     hx, hy, hz = np.zeros(ss.n), np.zeros(ss.n), np.zeros(ss.n)
     lib.orc_dipole_direct(ss.p, _dp(abc), g, *[int(p) for p in periodic], _dp(hx), _dp(hy), _dp(hz))
     return np.stack([hx, hy, hz])
+
+
+# ---------------------------------------------------------------- LongRange2D / Dipole2D
+def longrange2d_apply(spins, T, src_scale, dst_scale, gscale=1.0):
+    """LongRange2D compile and apply (spinoperationlongrange2d.cpp:387-530).
+    spins (3, nz, ny, nx); T (nz, nz, 9, ny, nx), T[i][j][ab] the array set
+    for (dest i, src j).  compile: q = 2D transform of each array / (nx ny);
+    apply: H_a[d] = sum_s src_scale[s] sum_b q[s][d][a b] M_b[s] (the
+    tensors read [s][d]), unnormalised inverse transform, real part, times
+    dst_scale[d] * gscale.  Returns (3, nz, ny, nx)."""
+    spins = np.asarray(spins, dtype=np.float64)
+    T = np.asarray(T, dtype=np.float64)
+    _, nz, ny, nx = spins.shape
+    q = np.fft.fft2(T, axes=(-2, -1)) / (nx * ny)
+    S = np.fft.fft2(spins, axes=(-2, -1))
+    H = np.zeros((3, nz, ny, nx), dtype=complex)
+    for a in range(3):
+        for d in range(nz):
+            for s_ in range(nz):
+                for b in range(3):
+                    H[a, d] += src_scale[s_] * q[s_, d, 3 * a + b] * S[b, s_]
+    h = np.fft.ifft2(H, axes=(-2, -1)).real * (nx * ny)
+    return h * (np.asarray(dst_scale, dtype=np.float64) * gscale)[None, :, None, None]
+
+
+def _d2_xx(X, Y, Z):
+    r = math.sqrt(X * X + Y * Y + Z * Z)
+    if r < 1e-80:
+        return 0.0
+    ir = 1.0 / r
+    ir3 = ir * ir * ir
+    ir5 = ir3 * ir * ir
+    return -1.0 * (ir3 - 3.0 * X * X * ir5)
+
+
+def _d2_xy(X, Y, Z):
+    r = math.sqrt(X * X + Y * Y + Z * Z)
+    if r < 1e-80:
+        return 0.0
+    ir = 1.0 / r
+    ir3 = ir * ir * ir
+    ir5 = ir3 * ir * ir
+    return -1.0 * (-3.0 * X * Y * ir5)
+
+
+def dipole2d_tensor(nx, ny, nz, abc, off, trunc):
+    """Dipole2D makeData (dip2d_luafuncs.lua:516-660, elements demag.cpp:
+    3-56), pure Python: abc (nz, 3, 3) unit cell A, B, C per layer, off
+    (nz, 3), trunc (radial, x, y, z).  Returns T (nz, nz, 9, ny, nx)
+    indexed [dest][src][ab]."""
+    abc = np.asarray(abc, dtype=np.float64).reshape(nz, 3, 3)
+    off = np.asarray(off, dtype=np.float64).reshape(nz, 3)
+    T = np.zeros((nz, nz, 9, ny, nx))
+
+    def idx2pos(i, j, layer):
+        dz = [0.0, 0.0, 0.0]
+        for Z in range(layer):
+            c = abc[Z][2]
+            dz = [dz[0] + float(c[0]), dz[1] + float(c[1]), dz[2] + float(c[2])]
+        A, B = abc[0][0], abc[0][1]
+        di = [i * float(A[0]), i * float(A[1]), i * float(A[2])]
+        dj = [j * float(B[1]), j * float(B[1]), j * float(B[2])]
+        o = off[layer]
+        return [di[k] + dj[k] + dz[k] + float(o[k]) for k in range(3)]
+
+    tX, tY, tZ = int(trunc[1]), int(trunc[2]), int(trunc[3])
+    for d in range(nz):
+        for s_ in range(nz):
+            if abs(s_ - d) > tZ:
+                continue
+            for X in range(-tX, tX + 1):
+                for Y in range(-tY, tY + 1):
+                    pd, ps = idx2pos(X, Y, d), idx2pos(X, Y, s_)
+                    rx, ry, rz = ps[0] - pd[0], ps[1] - pd[1], ps[2] - pd[2]
+                    x = X + 100000 * nx if X < 0 else X
+                    y = Y + 100000 * ny if Y < 0 else Y
+                    x, y = x % nx, y % ny
+                    v = (_d2_xx(rx, ry, rz), _d2_xy(rx, ry, rz), _d2_xy(rx, rz, ry),
+                         _d2_xy(ry, rx, rz), _d2_xx(ry, rx, rz), _d2_xy(ry, rz, rx),
+                         _d2_xy(rz, rx, ry), _d2_xy(rz, ry, rx), _d2_xx(rz, rx, ry))
+                    for ab in range(9):
+                        T[d, s_, ab, y, x] += v[ab]
+    return T
 
 
 def fft1d(data, sign):

@@ -242,3 +242,28 @@ def test_golden_fixtures_reproduce():
     for key, val in fresh.items():
         ref = gold[key]
         np.testing.assert_allclose(np.asarray(val), np.asarray(ref), rtol=1e-12, atol=1e-13, err_msg=key)
+
+
+def test_longrange2d_oracle_is_the_circular_convolution():
+    """The transform-based LongRange2D oracle against the real-space sum it
+    stands for: H_a[d](r) = dst[d] g sum_s src[s] sum_b sum_r' T[s][d][ab](r - r')
+    M_b[s](r'), periodic in x and y."""
+    nx, ny, nz = 5, 4, 2
+    r = np.random.default_rng(88)
+    T = r.normal(size=(nz, nz, 9, ny, nx))
+    S = r.normal(size=(3, nz, ny, nx))
+    src, dst = np.array([0.7, 1.3]), np.array([1.1, 0.4])
+    h = O.longrange2d_apply(S, T, src, dst, 0.5)
+    ref = np.zeros_like(h)
+    for a in range(3):
+        for d in range(nz):
+            for y in range(ny):
+                for x in range(nx):
+                    acc = 0.0
+                    for s_ in range(nz):
+                        for b in range(3):
+                            for yp in range(ny):
+                                for xp in range(nx):
+                                    acc += src[s_] * T[s_, d, 3 * a + b, (y - yp) % ny, (x - xp) % nx] * S[b, s_, yp, xp]
+                    ref[a, d, y, x] = dst[d] * 0.5 * acc
+    np.testing.assert_allclose(h, ref, rtol=1e-12, atol=1e-12)
