@@ -135,6 +135,7 @@ int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4]);
 #define MLB_OP_LONGRANGE3D 9    /* M/cpu/longrange3d */
 #define MLB_OP_LONGRANGE2D 10   /* M/cpu/longrange2d (layer-pair tensors) */
 #define MLB_OP_DIPOLE2D 11      /* M/cpu/dipole2d (LongRange2D + tensor builder) */
+#define MLB_OP_MAGNETOSTATICS2D 12 /* M/cpu/magnetostatics2d (LongRange2D + prism tensors) */
 int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out);     /* X.new(nx,ny,nz) */
 int mlb_op_destroy(mlb_op* op);
 int mlb_op_kind(const mlb_op* op, int* kind);
@@ -231,6 +232,14 @@ int mlb_dipole2d_get_offset(const mlb_op* op, int layer, double off[3]);
 int mlb_dipole2d_set_truncation(mlb_op* op, const int t[4]);     /* radial, x, y, z */
 int mlb_dipole2d_get_truncation(const mlb_op* op, int t[4]);
 int mlb_dipole2d_make_data(mlb_op* op);
+/* Magnetostatics2D: the same unit-cell and truncation state (the mlb_dipole2d
+ * calls, offsets unused) plus a grain size per layer (mag2d_luafuncs.lua:
+ * 93-122, default 1 x 1 x 1); mlb_dipole2d_make_data runs its builder
+ * (:598-744): minus the demagnetising tensor of a source and a destination
+ * prism (Newell's f and g, demag.cpp:196-350), summed over the in-plane
+ * images within the truncations. */
+int mlb_magnetostatics2d_set_grain_size(mlb_op* op, int layer, const double g[3]);
+int mlb_magnetostatics2d_get_grain_size(const mlb_op* op, int layer, double g[3]);
 
 /* ---------------------------------------------------------------- LLG
  * M/cpu/llg/llg.cpp:91-171, llgcartesian.cpp:90-278, llgquat.cpp:126-378. */

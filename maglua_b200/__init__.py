@@ -126,6 +126,8 @@ _SIGS = {
     "mlb_dipole2d_set_truncation": ([_P, _I], C.c_int),
     "mlb_dipole2d_get_truncation": ([_P, _I], C.c_int),
     "mlb_dipole2d_make_data": ([_P], C.c_int),
+    "mlb_magnetostatics2d_set_grain_size": ([_P, C.c_int, _D], C.c_int),
+    "mlb_magnetostatics2d_get_grain_size": ([_P, C.c_int, _D], C.c_int),
     "mlb_llg_create": ([C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_llg_destroy": ([_P], C.c_int),
     "mlb_llg_set_flags": ([_P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
@@ -1076,6 +1078,44 @@ class Dipole2D(LongRange2D):
         if self.newDataRequired():
             self._make_now()
         SpinOperation.apply(self, ss)
+
+
+class Magnetostatics2D(Dipole2D):
+    """Magnetostatics2D (M/cpu/magnetostatics2d): LongRange2D whose arrays
+    are minus the demagnetising tensors of prism-shaped grains (Newell's f
+    and g), summed over the in-plane images within the truncations
+    (mag2d_luafuncs.lua:598-744), built natively on the first apply.  The
+    user applies the 1/V source scale and 4 pi destination scale."""
+    KIND = 12
+
+    def setOffset(self, layer, v):
+        raise MagLuaError(-1, "Magnetostatics2D has no per-layer offset")
+
+    def setGrainSize(self, layer, X, Y=None, Z=None):
+        if Y is None:
+            X, Y, Z = X
+        g = np.asarray([X, Y, Z], dtype=np.float64)
+        _ck(_lib.mlb_magnetostatics2d_set_grain_size(self._h, self._layer(layer), _dp(g)))
+
+    def grainSize(self, layer):
+        """x, y, z and the volume (mag2d_luafuncs.lua:109-122)."""
+        g = np.zeros(3)
+        _ck(_lib.mlb_magnetostatics2d_get_grain_size(self._h, self._layer(layer), _dp(g)))
+        return float(g[0]), float(g[1]), float(g[2]), float(g[0] * g[1] * g[2])
+
+    def getMatrix(self, dest, src, ab, x, y):
+        """Element at 0-based offsets (x, y) of the (dest, src) array of
+        component ab, data made first if needed (mag2d_luafuncs.lua:32-45)."""
+        self.makeData()
+        return float(self.tensorArray(dest, src, ab)[int(y), int(x)])
+
+    def setMatrix(self, dest, src, ab, x, y, v):
+        """mag2d_luafuncs.lua:47-62: set one element, compile required."""
+        self.makeData()
+        a = self.tensorArray(dest, src, ab)
+        a[int(y), int(x)] = float(v)
+        self.setTensorArray(dest, src, ab, a.reshape(-1))
+        self.setCompileRequired(True)
 
 
 # ====================================================================== LLG

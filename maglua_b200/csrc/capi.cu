@@ -33,6 +33,8 @@
 #include <string>
 #include <strings.h>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 namespace {
 
@@ -305,7 +307,7 @@ struct mlb_op {
     bool lr2_newdata = true, lr2_compile = true;
     // Dipole2D builder: unit cell A, B, C per layer, offset per layer,
     // truncation {radial, x, y, z}
-    std::vector<double> d2_abc, d2_off;
+    std::vector<double> d2_abc, d2_off, d2_grain;
     int d2_trunc[4] = {25, 25, 25, 25};
     std::unique_ptr<LR2DPlan> lr2;
 };
@@ -765,7 +767,10 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
 }
 
 // ------------------------------------------------------------------ LongRange2D / Dipole2D
-bool is_lr2d(int kind) { return kind == MLB_OP_LONGRANGE2D || kind == MLB_OP_DIPOLE2D; }
+bool is_lr2d(int kind)
+{
+    return kind == MLB_OP_LONGRANGE2D || kind == MLB_OP_DIPOLE2D || kind == MLB_OP_MAGNETOSTATICS2D;
+}
 
 void ensure_t2(mlb_op* op)
 {
@@ -844,6 +849,136 @@ void dipole2d_make(mlb_op* op)
                     for (int ab = 0; ab < 9; ab++) T[ab * plane + at] += v[ab];
                 }
         }
+    op->lr2_newdata = false;
+    op->lr2_compile = true;
+}
+
+// Magnetostatics2D element functions: Newell's f and g (Newell, Williams
+// and Dunlop, J. Geophys. Res. 98, 9551 (1993)) written with logarithms,
+// log(num/den) and atan2 taken as 0 where the reference's helpers do
+// (demag.cpp:190-210), and the 64-term combination for a source prism d1 and
+// a destination prism d2 at offset (X, Y, Z) divided by 4 pi |d2|
+// (demag.cpp:256-280, after Donahue).
+double ms_log(double num, double den) { return (num == 0 || den == 0) ? 0.0 : std::log(num / den); }
+double ms_atan(double num, double den) { return (num == 0 && den == 0) ? 0.0 : std::atan2(num, den); }
+
+double ms_f(double X, double Y, double Z)
+{
+    const double x = std::fabs(X), y = std::fabs(Y), z = std::fabs(Z);
+    const double xx = x * x, yy = y * y, zz = z * z;
+    const double R = std::sqrt(xx + yy + zz);
+    return (2 * xx - yy - zz) * R / 6 - x * y * z * ms_atan(y * z, x * R) +
+           (y / 4) * (zz - xx) * ms_log((y + R) * (y + R), xx + zz) +
+           (z / 4) * (yy - xx) * ms_log((z + R) * (z + R), xx + yy);
+}
+
+double ms_g(double X, double Y, double Z)
+{
+    const double x = std::fabs(X), y = std::fabs(Y), z = std::fabs(Z);
+    const double xx = x * x, yy = y * y, zz = z * z;
+    const double R = std::sqrt(xx + yy + zz);
+    const double sg = (X < 0 ? -1.0 : 1.0) * (Y < 0 ? -1.0 : 1.0);
+    return sg * (-x * y * R / 3 -
+                 (z / 2) * (xx * ms_atan(y * z, x * R) + yy * ms_atan(x * z, y * R) + (zz / 3) * ms_atan(x * y, z * R)) +
+                 (x * y * z / 2) * ms_log((z + R) * (z + R), xx + yy) +
+                 (y / 12) * (3 * zz - yy) * ms_log((x + R) * (x + R), yy + zz) +
+                 (x / 12) * (3 * zz - xx) * ms_log((y + R) * (y + R), xx + zz));
+}
+
+template <double (*F)(double, double, double)>
+double ms_pair(double X, double Y, double Z, const double d1[3], const double d2[3])
+{
+    const double sg[4] = {1.0, -1.0, 1.0, -1.0};
+    const double ox[4] = {0, d2[0], d2[0] - d1[0], -d1[0]};
+    const double oy[4] = {0, d2[1], d2[1] - d1[1], -d1[1]};
+    const double oz[4] = {0, d2[2], d2[2] - d1[2], -d1[2]};
+    double sum = 0;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++)
+            for (int c = 0; c < 4; c++) sum = sum + sg[a] * sg[b] * sg[c] * F(X + ox[a], Y + oy[b], Z + oz[c]);
+    return sum / (4.0 * M_PI * d2[0] * d2[1] * d2[2]);
+}
+
+// The nine elements XX..ZZ at r for source prism d1, destination prism d2
+// (demag.cpp:283-350: YY, ZZ, XZ, YZ by permuting axes; YX = XY, ZX = XZ,
+// ZY = YZ).
+void ms_elements(double rx, double ry, double rz, const double d1[3], const double d2[3], double v[9])
+{
+    auto P = [](const double* d, int i, int j, int k, double* o) { o[0] = d[i]; o[1] = d[j]; o[2] = d[k]; };
+    double a1[3], a2[3];
+    const double xx = ms_pair<ms_f>(rx, ry, rz, d1, d2);
+    const double xy = ms_pair<ms_g>(rx, ry, rz, d1, d2);
+    P(d1, 0, 2, 1, a1); P(d2, 0, 2, 1, a2);
+    const double xz = ms_pair<ms_g>(rx, rz, ry, a1, a2);
+    P(d1, 1, 0, 2, a1); P(d2, 1, 0, 2, a2);
+    const double yy = ms_pair<ms_f>(ry, rx, rz, a1, a2);
+    P(d1, 1, 2, 0, a1); P(d2, 1, 2, 0, a2);
+    const double yz = ms_pair<ms_g>(ry, rz, rx, a1, a2);
+    P(d1, 2, 1, 0, a1); P(d2, 2, 1, 0, a2);
+    const double zz = ms_pair<ms_f>(rz, ry, rx, a1, a2);
+    v[0] = xx; v[1] = xy; v[2] = xz;
+    v[3] = xy; v[4] = yy; v[5] = yz;
+    v[6] = xz; v[7] = yz; v[8] = zz;
+}
+
+// Magnetostatics2D makeData (mag2d_luafuncs.lua:598-744): zero every array;
+// for source layer z1 and destination layer z2 within truncation z, and
+// each X, Y in [-truncation, truncation] within the x and y truncations,
+// r = X A + Y B + (C_0 + .. + C_{z2-1}) - (C_0 + .. + C_{z1-1}) (A, B of the
+// first layer), add -N(r; grain z1, grain z2) at (X mod nx, Y mod ny) of the
+// arrays [z1][z2].  The layer pairs run on host threads, each pair's
+// accumulation in the reference's order.
+void magnetostatics2d_make(mlb_op* op)
+{
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    ensure_t2(op);
+    std::fill(op->t2.begin(), op->t2.end(), 0.0);
+    const size_t plane = (size_t)nx * ny;
+    const double* A = &op->d2_abc[0];
+    const double* B = &op->d2_abc[3];
+    const int mx = op->d2_trunc[0], tX = op->d2_trunc[1], tY = op->d2_trunc[2], tZ = op->d2_trunc[3];
+    auto cum = [&](int layer, double c[3]) {
+        c[0] = c[1] = c[2] = 0;
+        for (int j = 0; j < layer; j++)
+            for (int q = 0; q < 3; q++) c[q] = c[q] + op->d2_abc[j * 9 + 6 + q];
+    };
+    auto pair = [&](int z1, int z2) {
+        if (std::abs(z1 - z2) > tZ) return;
+        double c1[3], c2[3];
+        cum(z1, c1);
+        cum(z2, c2);
+        const double cx = c2[0] - c1[0], cy = c2[1] - c1[1], cz = c2[2] - c1[2];
+        const double* g1 = &op->d2_grain[z1 * 3];
+        const double* g2 = &op->d2_grain[z2 * 3];
+        double* T = &op->t2[((size_t)z1 * nz + z2) * 9 * plane];
+        for (int X = -mx; X <= mx; X++) {
+            if (std::abs(X) > tX) continue;
+            for (int Y = -mx; Y <= mx; Y++) {
+                if (std::abs(Y) > tY) continue;
+                const double rx = A[0] * X + B[0] * Y + cx;
+                const double ry = A[1] * X + B[1] * Y + cy;
+                const double rz = A[2] * X + B[2] * Y + cz;
+                int x = X, y = Y;
+                while (x < 0) x += 1000 * nx;
+                while (y < 0) y += 1000 * ny;
+                x %= nx;
+                y %= ny;
+                double v[9];
+                ms_elements(rx, ry, rz, g1, g2, v);
+                const size_t at = (size_t)y * nx + x;
+                for (int ab = 0; ab < 9; ab++) T[ab * plane + at] += -v[ab];
+            }
+        }
+    };
+    const int npair = nz * nz;
+    const int nth = std::max(1, std::min<int>(npair, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; t++)
+        pool.emplace_back([&] {
+            for (int p = next++; p < npair; p = next++) pair(p / nz, p % nz);
+        });
+    for (auto& th : pool) th.join();
     op->lr2_newdata = false;
     op->lr2_compile = true;
 }
@@ -1236,13 +1371,15 @@ void op_apply(mlb_op* op, mlb_system* s)
         sl.state = ST_LAZY; sl.base_data = false; sl.terms.assign(1, t); sl.gen = s->gen;
         return;
     case MLB_OP_LONGRANGE2D:
-    case MLB_OP_DIPOLE2D: {
+    case MLB_OP_DIPOLE2D:
+    case MLB_OP_MAGNETOSTATICS2D: {
         // apply (spinoperationlongrange2d.cpp:430-530): makeNewData when new
         // data is required, compile when required, then the convolution
         if (op->lr2_newdata) {
             if (s->capturing) fail(MLB_ESTATE, "tensor changed during capture");
-            if (op->kind != MLB_OP_DIPOLE2D) fail(MLB_ESTATE, "make data function not set");
-            dipole2d_make(op);
+            if (op->kind == MLB_OP_DIPOLE2D) dipole2d_make(op);
+            else if (op->kind == MLB_OP_MAGNETOSTATICS2D) magnetostatics2d_make(op);
+            else fail(MLB_ESTATE, "make data function not set");
         }
         if (s->capturing && (op->lr2_compile || !op->lr2 || op->lr2->rb != s->rb))
             fail(MLB_ESTATE, "tensor changed during capture");
@@ -2561,6 +2698,7 @@ int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out)
         case MLB_OP_LONGRANGE3D: op->slot = "LongRange3D"; break;
         case MLB_OP_LONGRANGE2D: op->slot = "LongRange2D"; break;
         case MLB_OP_DIPOLE2D: op->slot = "Dipole2D"; break;
+        case MLB_OP_MAGNETOSTATICS2D: op->slot = "Magnetostatics2D"; break;
         default: fail(MLB_EINVAL, "unknown operator kind");
         }
         if (is_lr2d(kind)) {
@@ -2569,6 +2707,7 @@ int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out)
             op->d2_abc.assign((size_t)nz * 9, 0.0);
             for (int z = 0; z < nz; z++) op->d2_abc[z * 9] = op->d2_abc[z * 9 + 4] = op->d2_abc[z * 9 + 8] = 1.0;
             op->d2_off.assign((size_t)nz * 3, 0.0);
+            op->d2_grain.assign((size_t)nz * 3, 1.0);
         }
         *out = op.release();
     });
@@ -3117,8 +3256,27 @@ int mlb_dipole2d_make_data(mlb_op* op)
 {
     return guard([&] {
         g_version++;
-        if (!op || op->kind != MLB_OP_DIPOLE2D) fail(MLB_EINVAL, "not a Dipole2D operator");
-        dipole2d_make(op);
+        if (op && op->kind == MLB_OP_DIPOLE2D) dipole2d_make(op);
+        else if (op && op->kind == MLB_OP_MAGNETOSTATICS2D) magnetostatics2d_make(op);
+        else fail(MLB_EINVAL, "not a Dipole2D or Magnetostatics2D operator");
+    });
+}
+
+int mlb_magnetostatics2d_set_grain_size(mlb_op* op, int layer, const double g[3])
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        std::copy(g, g + 3, op->d2_grain.begin() + (size_t)layer * 3);
+    });
+}
+
+int mlb_magnetostatics2d_get_grain_size(const mlb_op* op, int layer, double g[3])
+{
+    return guard([&] {
+        need_lr2d(op);
+        need_layer(op, layer);
+        std::copy(op->d2_grain.begin() + (size_t)layer * 3, op->d2_grain.begin() + (size_t)layer * 3 + 3, g);
     });
 }
 

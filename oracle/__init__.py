@@ -459,6 +459,107 @@ def dipole2d_tensor(nx, ny, nz, abc, off, trunc):
     return T
 
 
+def _ms_log(num, den):
+    out = np.zeros(np.broadcast(num, den).shape)
+    m = (num != 0) & (den != 0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out[m] = np.log(num[m] / den[m])
+    return out
+
+
+def _ms_atan(num, den):
+    out = np.zeros(np.broadcast(num, den).shape)
+    m = ~((num == 0) & (den == 0))
+    out[m] = np.arctan2(num[m], den[m])
+    return out
+
+
+def _ms_f(X, Y, Z):
+    """Newell's f (Newell, Williams and Dunlop 1993) in logarithms."""
+    x, y, z = np.abs(X), np.abs(Y), np.abs(Z)
+    xx, yy, zz = x * x, y * y, z * z
+    R = np.sqrt(xx + yy + zz)
+    return ((2 * xx - yy - zz) * R / 6 - x * y * z * _ms_atan(y * z, x * R)
+            + (y / 4) * (zz - xx) * _ms_log((y + R) * (y + R), xx + zz)
+            + (z / 4) * (yy - xx) * _ms_log((z + R) * (z + R), xx + yy))
+
+
+def _ms_g(X, Y, Z):
+    """Newell's g in logarithms, odd in X and in Y."""
+    x, y, z = np.abs(X), np.abs(Y), np.abs(Z)
+    xx, yy, zz = x * x, y * y, z * z
+    R = np.sqrt(xx + yy + zz)
+    sg = np.where(X < 0, -1.0, 1.0) * np.where(Y < 0, -1.0, 1.0)
+    return sg * (-x * y * R / 3
+                 - (z / 2) * (xx * _ms_atan(y * z, x * R) + yy * _ms_atan(x * z, y * R)
+                              + (zz / 3) * _ms_atan(x * y, z * R))
+                 + (x * y * z / 2) * _ms_log((z + R) * (z + R), xx + yy)
+                 + (y / 12) * (3 * zz - yy) * _ms_log((x + R) * (x + R), yy + zz)
+                 + (x / 12) * (3 * zz - xx) * _ms_log((y + R) * (y + R), xx + zz))
+
+
+def _ms_pair(fn, X, Y, Z, d1, d2):
+    sg = (1.0, -1.0, 1.0, -1.0)
+    ox = (0.0, d2[0], d2[0] - d1[0], -d1[0])
+    oy = (0.0, d2[1], d2[1] - d1[1], -d1[1])
+    oz = (0.0, d2[2], d2[2] - d1[2], -d1[2])
+    acc = np.zeros(np.shape(X))
+    for a in range(4):
+        for b in range(4):
+            for c in range(4):
+                acc = acc + sg[a] * sg[b] * sg[c] * fn(X + ox[a], Y + oy[b], Z + oz[c])
+    return acc / (4.0 * math.pi * d2[0] * d2[1] * d2[2])
+
+
+def magnetostatics2d_elements(rx, ry, rz, d1, d2):
+    """The nine prism-prism elements XX..ZZ (magnetostatics2d/demag.cpp:
+    256-350) for source prism d1 and destination prism d2 at offset r."""
+    def P(d, i, j, k):
+        return (d[i], d[j], d[k])
+    xx = _ms_pair(_ms_f, rx, ry, rz, d1, d2)
+    xy = _ms_pair(_ms_g, rx, ry, rz, d1, d2)
+    xz = _ms_pair(_ms_g, rx, rz, ry, P(d1, 0, 2, 1), P(d2, 0, 2, 1))
+    yy = _ms_pair(_ms_f, ry, rx, rz, P(d1, 1, 0, 2), P(d2, 1, 0, 2))
+    yz = _ms_pair(_ms_g, ry, rz, rx, P(d1, 1, 2, 0), P(d2, 1, 2, 0))
+    zz = _ms_pair(_ms_f, rz, ry, rx, P(d1, 2, 1, 0), P(d2, 2, 1, 0))
+    return [xx, xy, xz, xy, yy, yz, xz, yz, zz]
+
+
+def magnetostatics2d_tensor(nx, ny, nz, abc, grain, trunc):
+    """Magnetostatics2D makeData (mag2d_luafuncs.lua:598-744), vectorised
+    over the in-plane images: abc (nz, 3, 3) unit cells, grain (nz, 3),
+    trunc (radial, x, y, z).  Returns T (nz, nz, 9, ny, nx) indexed
+    [source z1][destination z2][ab], each image adding -N."""
+    abc = np.asarray(abc, dtype=np.float64).reshape(nz, 3, 3)
+    grain = np.asarray(grain, dtype=np.float64).reshape(nz, 3)
+    mx = int(trunc[0])
+    Xs = [X for X in range(-mx, mx + 1) if abs(X) <= trunc[1]]
+    Ys = [Y for Y in range(-mx, mx + 1) if abs(Y) <= trunc[2]]
+    XX, YY = np.meshgrid(np.asarray(Xs, float), np.asarray(Ys, float), indexing="ij")
+    xi = XX.astype(int) % nx
+    yi = YY.astype(int) % ny
+    A, B = abc[0][0], abc[0][1]
+    T = np.zeros((nz, nz, 9, ny, nx))
+    for z1 in range(nz):
+        c1 = np.zeros(3)
+        for j in range(z1):
+            c1 = c1 + abc[j][2]
+        for z2 in range(nz):
+            if abs(z1 - z2) > trunc[3]:
+                continue
+            c2 = np.zeros(3)
+            for j in range(z2):
+                c2 = c2 + abc[j][2]
+            c = c2 - c1
+            rx = A[0] * XX + B[0] * YY + c[0]
+            ry = A[1] * XX + B[1] * YY + c[1]
+            rz = A[2] * XX + B[2] * YY + c[2]
+            v = magnetostatics2d_elements(rx, ry, rz, grain[z1], grain[z2])
+            for k in range(9):
+                np.add.at(T[z1, z2, k], (yi, xi), -v[k])
+    return T
+
+
 def fft1d(data, sign):
     d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128)).copy()
     lib.orc_fft1d(d.view(np.float64).ctypes.data_as(_D), len(d), 1, sign)

@@ -182,3 +182,44 @@ def test_longrange2d_layer_limit(M):
     op.setNewDataRequired(False)
     with pytest.raises(M.MagLuaError, match="at most 64 layers"):
         op.apply(ss)
+
+
+def test_magnetostatics2d_field(M):
+    """Magnetostatics2D with uneven grains per layer and a sheared unit cell:
+    the native builder's arrays and the field (1/V source and 4 pi
+    destination scales, as a user sets them) against the oracle."""
+    dims = (16, 8, 2)
+    nx, ny, nz = dims
+    abc = [[[1.0, 0, 0], [0.2, 1.0, 0], [0, 0, 1.2]], [[1.0, 0, 0], [0.2, 1.0, 0], [0.1, 0, 0.9]]]
+    grain = [[0.9, 0.8, 1.0], [0.7, 0.9, 0.8]]
+    trunc = (6, 6, 5, 1)
+    s = random_spins(nx * ny * nz, 89, lengths=True)
+    ss = _system(M, dims, s)
+    mag = M.Magnetostatics2D(ss)
+    for z in range(nz):
+        mag.setUnitCell(z + 1, *abc[z])
+        mag.setGrainSize(z + 1, *grain[z])
+        vol = grain[z][0] * grain[z][1] * grain[z][2]
+        mag.setSourceMomentScale(z + 1, 1.0 / vol)
+        mag.setDestinationFieldScale(z + 1, 4 * np.pi)
+    mag.setTruncation(*trunc)
+    assert mag.grainSize(2)[3] == pytest.approx(0.7 * 0.9 * 0.8)
+    mag.apply(ss)
+    T = O.magnetostatics2d_tensor(nx, ny, nz, abc, grain, trunc)
+    for i in range(nz):
+        for j in range(nz):
+            for ab in range(9):
+                np.testing.assert_allclose(mag.tensorArray(i + 1, j + 1, AB[ab]), T[i, j, ab], rtol=1e-10,
+                                           atol=1e-11 * np.abs(T).max())
+    src = [1.0 / np.prod(g) for g in grain]
+    ref = O.longrange2d_apply(s.reshape(3, nz, ny, nx), T, src, [4 * np.pi] * nz).reshape(3, -1)
+    assert rel_err(_field(ss, "Magnetostatics2D"), ref) <= FIELD_TOL
+    # setMatrix marks compile required (mag2d_luafuncs.lua:47-62)
+    v = mag.getMatrix(1, 2, "XZ", 3, 1)
+    assert v == T[0, 1, 2, 1, 3]
+    mag.setMatrix(1, 2, "XZ", 3, 1, v + 0.5)
+    assert mag.compileRequired()
+    T[0, 1, 2, 1, 3] += 0.5
+    mag.apply(ss)
+    ref = O.longrange2d_apply(s.reshape(3, nz, ny, nx), T, src, [4 * np.pi] * nz).reshape(3, -1)
+    assert rel_err(_field(ss, "Magnetostatics2D"), ref) <= FIELD_TOL

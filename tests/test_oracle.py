@@ -267,3 +267,68 @@ def test_longrange2d_oracle_is_the_circular_convolution():
                                     acc += src[s_] * T[s_, d, 3 * a + b, (y - yp) % ny, (x - xp) % nx] * S[b, s_, yp, xp]
                     ref[a, d, y, x] = dst[d] * 0.5 * acc
     np.testing.assert_allclose(h, ref, rtol=1e-12, atol=1e-12)
+
+
+def _mag2d_fixture():
+    with open(os.path.join(GOLDEN, "mag2d_save_test.json")) as f:
+        return json.load(f)
+
+
+NAMES9 = ["XX", "XY", "XZ", "YX", "YY", "YZ", "ZX", "ZY", "ZZ"]
+
+
+def _fixture_arrays(fx):
+    out = {}
+    for key, comps in fx["arrays"].items():
+        d, s_ = (int(v) - 1 for v in key.split(","))
+        for ab, rows in comps.items():
+            out[(d, s_, NAMES9.index(ab))] = np.asarray(rows) * fx["sign_of_file"]
+    return out
+
+
+def test_magnetostatics2d_oracle_matches_reference_data_file():
+    """The Magnetostatics2D builder restated in the oracle against the
+    reference's tensor data file (dipole2d/save_test.lua, 16 x 16 x 2, 1e-6
+    cells and grains, truncation 20, values printed to 7 significant
+    digits).  The file holds +N; the current makeData adds -N."""
+    fx = _mag2d_fixture()
+    a, g = fx["unit_cell"], fx["grain"]
+    abc = np.tile(np.eye(3) * a, (2, 1, 1))
+    T = O.magnetostatics2d_tensor(16, 16, 2, abc, np.full((2, 3), g), fx["truncation"])
+    for (d, s_, ab), ref in _fixture_arrays(fx).items():
+        got = -T[d, s_, ab]
+        np.testing.assert_allclose(got, ref, rtol=1e-6, atol=2e-7 * np.abs(ref).max() + 1e-12)
+
+
+def test_magnetostatics2d_builder_in_the_library(tmp_path):
+    """The library's native builder (host code, no GPU needed) against the
+    oracle and the reference's data file."""
+    import ctypes as C
+    import maglua_b200
+    lib = maglua_b200._lib.load()
+    fx = _mag2d_fixture()
+    a, g = fx["unit_cell"], fx["grain"]
+    op = C.c_void_p()
+    assert lib.mlb_op_create(12, 16, 16, 2, C.byref(op)) == 0
+    try:
+        for z in range(2):
+            abc = (C.c_double * 9)(a, 0, 0, 0, a, 0, 0, 0, a)
+            assert lib.mlb_dipole2d_set_unit_cell(op, z, abc) == 0
+            assert lib.mlb_magnetostatics2d_set_grain_size(op, z, (C.c_double * 3)(g, g, g)) == 0
+        assert lib.mlb_dipole2d_set_truncation(op, (C.c_int * 4)(*fx["truncation"])) == 0
+        assert lib.mlb_dipole2d_make_data(op) == 0
+        T = O.magnetostatics2d_tensor(16, 16, 2, np.tile(np.eye(3) * a, (2, 1, 1)), np.full((2, 3), g),
+                                      fx["truncation"])
+        ref = _fixture_arrays(fx)
+        buf = np.zeros(256)
+        for d in range(2):
+            for s_ in range(2):
+                for ab in range(9):
+                    assert lib.mlb_longrange2d_get_tensor(op, d, s_, ab, buf.ctypes.data_as(C.POINTER(C.c_double))) == 0
+                    got = buf.reshape(16, 16)
+                    np.testing.assert_allclose(got, T[d, s_, ab], rtol=1e-11, atol=1e-11 * np.abs(T).max())
+                    if (d, s_, ab) in ref:
+                        r = ref[(d, s_, ab)]
+                        np.testing.assert_allclose(-got, r, rtol=1e-6, atol=2e-7 * np.abs(r).max() + 1e-12)
+    finally:
+        lib.mlb_op_destroy(op)
