@@ -240,6 +240,16 @@ int mlb_dipole2d_make_data(mlb_op* op);
  * images within the truncations. */
 int mlb_magnetostatics2d_set_grain_size(mlb_op* op, int layer, const double g[3]);
 int mlb_magnetostatics2d_get_grain_size(const mlb_op* op, int layer, double g[3]);
+/* Dipole2D / Magnetostatics2D tensor data files, the GAB_<nx>x<ny>x<nz>.<n>.lua
+ * and MAB_... files of dip2d_luafuncs.lua:278-500 (dip2d_save, dip2d_load)
+ * and mag2d_luafuncs.lua:278-480: write builds the arrays if new data is
+ * required and writes the reference's layout (system size, builder state,
+ * `% 16.15E` arrays [dest][src], a Lua loader); read sets the arrays, clears
+ * new data required and marks compile required only when the file's kind,
+ * size, unit cells, offsets or grain sizes and truncations match the
+ * operator's (relative 1e-8, as sameInternals); *loaded says whether it did. */
+int mlb_lr2d_write_data_file(mlb_op* op, const char* filename);
+int mlb_lr2d_read_data_file(mlb_op* op, const char* filename, int* loaded);
 
 /* ---------------------------------------------------------------- LLG
  * M/cpu/llg/llg.cpp:91-171, llgcartesian.cpp:90-278, llgquat.cpp:126-378. */

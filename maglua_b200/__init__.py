@@ -128,6 +128,8 @@ _SIGS = {
     "mlb_dipole2d_make_data": ([_P], C.c_int),
     "mlb_magnetostatics2d_set_grain_size": ([_P, C.c_int, _D], C.c_int),
     "mlb_magnetostatics2d_get_grain_size": ([_P, C.c_int, _D], C.c_int),
+    "mlb_lr2d_write_data_file": ([_P, C.c_char_p], C.c_int),
+    "mlb_lr2d_read_data_file": ([_P, C.c_char_p, _I], C.c_int),
     "mlb_llg_create": ([C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_llg_destroy": ([_P], C.c_int),
     "mlb_llg_set_flags": ([_P, C.c_int, C.c_int, C.c_double, C.c_double], C.c_int),
@@ -1069,6 +1071,18 @@ class Dipole2D(LongRange2D):
         if self._make is not None:
             return super()._make_now()
         _ck(_lib.mlb_dipole2d_make_data(self._h))
+
+    def writeDataFile(self, filename):
+        """Write the reference's tensor data file (GAB_... for Dipole2D,
+        MAB_... for Magnetostatics2D; dip2d_luafuncs.lua:278-500)."""
+        _ck(_lib.mlb_lr2d_write_data_file(self._h, os.fsencode(filename)))
+
+    def readDataFile(self, filename):
+        """Load the arrays of a tensor data file when its size and builder
+        state match this operator's; returns whether it did."""
+        ok = C.c_int()
+        _ck(_lib.mlb_lr2d_read_data_file(self._h, os.fsencode(filename), C.byref(ok)))
+        return bool(ok.value)
 
     def makeData(self):
         if self.newDataRequired():

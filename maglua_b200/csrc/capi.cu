@@ -4712,3 +4712,276 @@ extern "C" int mlb_dipole_field_noalloc(mlb_op* op, const float* sx, const float
         }
     });
 }
+
+// ====================================================================== GAB / MAB tensor files
+// Dipole2D and Magnetostatics2D data files (dip2d_luafuncs.lua:278-500,
+// mag2d_luafuncs.lua:278-480): a Lua file holding the system size, the
+// builder state and the nine arrays of every (destination, source) layer
+// pair, `% 16.15E` numbers with `0` for exact zeros, ending in a loader that
+// the reference's makeData runs (`return sameInternals, load`).  The layout
+// is the reference's so that either side can read the other's files; the
+// loader text below is this library's own.
+namespace {
+
+const char* const kLr2dLoader = R"LUA(
+-- loader: rows of comma-separated numbers -> tables indexed [y][x]
+local function rows_of(block)
+    if block == 0 then
+        local zero_row = setmetatable({}, {__index = function() return 0 end})
+        return setmetatable({}, {__index = function() return zero_row end})
+    end
+    local out = {}
+    for line in string.gmatch(block, "[^\n]+") do
+        local row = {}
+        for w in string.gmatch(line, "[^,]+") do
+            local v = tonumber(w)
+            if v then row[#row + 1] = v end
+        end
+        if #row > 0 then out[#out + 1] = row end
+    end
+    return out
+end
+
+local names = {"XX", "XY", "XZ", "YX", "YY", "YZ", "ZX", "ZY", "ZZ"}
+local blocks = {XX = XX, XY = XY, XZ = XZ, YX = YX, YY = YY, YZ = YZ, ZX = ZX, ZY = ZY, ZZ = ZZ}
+
+local function close(a, b)
+    if a == b then return true end
+    if a == nil or b == nil or a == 0 or b == 0 then return false end
+    return math.abs(a - b) / math.abs(a + b) < 1e-8
+end
+
+local function matches(op)
+    local id = op:internalData()
+    if id == nil then return false end
+    if op:nx() ~= nx or op:ny() ~= ny or op:nz() ~= nz then return false end
+    for k = 1, nz do
+        for i = 1, 3 do
+            for j = 1, 3 do
+                if not close(id.ABC[k][i][j], internal.ABC[k][i][j]) then return false end
+            end
+            local mine = (internal.offset or internal.grainSize)[k][i]
+            local theirs = ((internal.offset and id.offset) or id.grainSize)[k][i]
+            if not close(theirs, mine) then return false end
+        end
+    end
+    for _, key in ipairs({"truncation", "truncationX", "truncationY", "truncationZ"}) do
+        if not close(id[key], internal[key]) then return false end
+    end
+    return true
+end
+
+local function load(op)
+    if op:nx() ~= nx or op:ny() ~= ny or op:nz() ~= nz then
+        error("Size Mismatch", 2)
+    end
+    op:setInternalData(internal)
+    op:setNewDataRequired(false)
+    for d = 1, nz do
+        for s = 1, nz do
+            for _, ab in ipairs(names) do
+                local r = rows_of(blocks[ab][d][s])
+                local t = op:tensorArray(d, s, ab)
+                for x = 1, nx do
+                    for y = 1, ny do
+                        t:set(x, y, r[y][x])
+                    end
+                end
+            end
+        end
+    end
+    op:setCompileRequired(true)
+end
+
+return matches, load
+)LUA";
+
+const char* const kNames9[9] = {"XX", "XY", "XZ", "YX", "YY", "YZ", "ZX", "ZY", "ZZ"};
+
+std::string num14(double v)
+{
+    char b[64];
+    snprintf(b, sizeof(b), "%.14g", v);
+    return b;
+}
+
+bool same_number(double a, double b)
+{
+    if (a == b) return true;
+    if (a == 0 || b == 0) return false;
+    return std::fabs(a - b) / std::fabs(a + b) < 1e-8;
+}
+
+// numbers following `key` up to the end of its line (or of a {...} group)
+std::vector<double> numbers_on_line(const std::string& t, size_t at)
+{
+    std::vector<double> v;
+    const size_t end = t.find('\n', at);
+    const std::string line = t.substr(at, end == std::string::npos ? std::string::npos : end - at);
+    const char* p = line.c_str();
+    while (*p) {
+        if ((*p >= '0' && *p <= '9') || *p == '-' || *p == '+' || *p == '.') {
+            char* e;
+            const double x = strtod(p, &e);
+            if (e == p) { p++; continue; }
+            v.push_back(x);
+            p = e;
+        } else {
+            p++;
+        }
+    }
+    return v;
+}
+
+} // namespace
+
+extern "C" {
+
+int mlb_lr2d_write_data_file(mlb_op* op, const char* filename)
+{
+    return guard([&] {
+        if (!op || !filename) fail(MLB_EINVAL, "null argument");
+        if (op->kind != MLB_OP_DIPOLE2D && op->kind != MLB_OP_MAGNETOSTATICS2D)
+            fail(MLB_EINVAL, "not a Dipole2D or Magnetostatics2D operator");
+        const bool mag = op->kind == MLB_OP_MAGNETOSTATICS2D;
+        if (op->lr2_newdata) {
+            if (mag) magnetostatics2d_make(op);
+            else dipole2d_make(op);
+        }
+        ensure_t2(op);
+        const int nx = op->nx, ny = op->ny, nz = op->nz;
+        FILE* f = fopen(filename, "w");
+        if (!f) fail(MLB_EINVAL, std::string("cannot write ") + filename);
+        fprintf(f, "-- %s Data File\n--\nMagLua_Version = %d\n\n", mag ? "Magnetostatics2D" : "Dipole2D", mlb_version());
+        fprintf(f, "-- system size\nlocal nx, ny, nz = %d, %d, %d\n\t\n-- internal state\nlocal internal = {}\n", nx, ny,
+                nz);
+        fprintf(f, "internal.ABC = {}\ninternal.%s = {}\n", mag ? "grainSize" : "offset");
+        for (int z = 0; z < nz; z++) {
+            const double* a = &op->d2_abc[z * 9];
+            fprintf(f, "internal.ABC[%d] = {{%s, %s, %s}, {%s, %s, %s}, {%s, %s, %s}}\n", z + 1, num14(a[0]).c_str(),
+                    num14(a[1]).c_str(), num14(a[2]).c_str(), num14(a[3]).c_str(), num14(a[4]).c_str(),
+                    num14(a[5]).c_str(), num14(a[6]).c_str(), num14(a[7]).c_str(), num14(a[8]).c_str());
+        }
+        fprintf(f, "\n");
+        for (int z = 0; z < nz; z++) {
+            const double* v = mag ? &op->d2_grain[z * 3] : &op->d2_off[z * 3];
+            fprintf(f, "internal.%s[%d] = {%s, %s, %s}\n", mag ? "grainSize" : "offset", z + 1, num14(v[0]).c_str(),
+                    num14(v[1]).c_str(), num14(v[2]).c_str());
+        }
+        fprintf(f, "internal.truncation  = %d\ninternal.truncationX = %d\ninternal.truncationY = %d\n"
+                   "internal.truncationZ = %d\n\n",
+                op->d2_trunc[0], op->d2_trunc[1], op->d2_trunc[2], op->d2_trunc[3]);
+        fprintf(f, "-- interaction tensors. Format is AB[destination_layer][source_layer]\n");
+        std::string tt = "{";
+        for (int d = 0; d < nz; d++) tt += d ? ", {}" : "{}";
+        tt += "}";
+        for (int ab = 0; ab < 9; ab++) fprintf(f, "local %s = %s\n", kNames9[ab], tt.c_str());
+        fprintf(f, "\n");
+        const size_t plane = (size_t)nx * ny;
+        for (int ab = 0; ab < 9; ab++)
+            for (int d = 0; d < nz; d++)
+                for (int s = 0; s < nz; s++) {
+                    fprintf(f, "%s[%d][%d] = [[\n", kNames9[ab], d + 1, s + 1);
+                    const double* a = op->t2.data() + (((size_t)d * nz + s) * 9 + ab) * plane;
+                    for (int y = 0; y < ny; y++) {
+                        for (int x = 0; x < nx; x++) {
+                            const double v = a[(size_t)y * nx + x];
+                            if (x) fputs(", ", f);
+                            if (v == 0) fputs("0", f);
+                            else fprintf(f, "% 16.15E", v);
+                        }
+                        fputc('\n', f);
+                    }
+                    fprintf(f, "]]\n");
+                }
+        fputs(kLr2dLoader, f);
+        const bool ok = ferror(f) == 0;
+        fclose(f);
+        if (!ok) fail(MLB_EINVAL, std::string("error writing ") + filename);
+    });
+}
+
+int mlb_lr2d_read_data_file(mlb_op* op, const char* filename, int* loaded)
+{
+    return guard([&] {
+        if (!op || !filename || !loaded) fail(MLB_EINVAL, "null argument");
+        if (op->kind != MLB_OP_DIPOLE2D && op->kind != MLB_OP_MAGNETOSTATICS2D)
+            fail(MLB_EINVAL, "not a Dipole2D or Magnetostatics2D operator");
+        *loaded = 0;
+        const bool mag = op->kind == MLB_OP_MAGNETOSTATICS2D;
+        FILE* f = fopen(filename, "rb");
+        if (!f) fail(MLB_ENOTFOUND, std::string("cannot read ") + filename);
+        std::string t;
+        char buf[65536];
+        size_t got;
+        while ((got = fread(buf, 1, sizeof(buf), f)) > 0) t.append(buf, got);
+        fclose(f);
+        const int nx = op->nx, ny = op->ny, nz = op->nz;
+        // kind and size
+        if (t.find(mag ? "-- Magnetostatics2D Data File" : "-- Dipole2D Data File") == std::string::npos) return;
+        size_t at = t.find("local nx, ny, nz =");
+        if (at == std::string::npos) fail(MLB_EINVAL, "no system size in " + std::string(filename));
+        std::vector<double> dims = numbers_on_line(t, at + 18);
+        if (dims.size() < 3 || dims[0] != nx || dims[1] != ny || dims[2] != nz) return;
+        // builder state (sameInternals)
+        for (int z = 0; z < nz; z++) {
+            at = t.find("internal.ABC[" + std::to_string(z + 1) + "] =");
+            if (at == std::string::npos) return;
+            std::vector<double> a = numbers_on_line(t, t.find('=', at) + 1);
+            if (a.size() < 9) return;
+            for (int q = 0; q < 9; q++)
+                if (!same_number(a[q], op->d2_abc[z * 9 + q])) return;
+            const std::string key = mag ? "internal.grainSize[" : "internal.offset[";
+            at = t.find(key + std::to_string(z + 1) + "] =");
+            if (at == std::string::npos) return;
+            std::vector<double> v = numbers_on_line(t, t.find('=', at) + 1);
+            if (v.size() < 3) return;
+            const double* mine = mag ? &op->d2_grain[z * 3] : &op->d2_off[z * 3];
+            for (int q = 0; q < 3; q++)
+                if (!same_number(v[q], mine[q])) return;
+        }
+        const char* tkeys[4] = {"internal.truncation ", "internal.truncationX", "internal.truncationY",
+                                "internal.truncationZ"};
+        for (int q = 0; q < 4; q++) {
+            at = t.find(tkeys[q]);
+            if (at == std::string::npos) return;
+            std::vector<double> v = numbers_on_line(t, t.find('=', at) + 1);
+            if (v.empty() || !same_number(v[0], op->d2_trunc[q])) return;
+        }
+        // the arrays
+        const size_t plane = (size_t)nx * ny;
+        std::vector<double> all((size_t)nz * nz * 9 * plane, 0.0);
+        for (int ab = 0; ab < 9; ab++)
+            for (int d = 0; d < nz; d++)
+                for (int s = 0; s < nz; s++) {
+                    const std::string key =
+                        std::string(kNames9[ab]) + "[" + std::to_string(d + 1) + "][" + std::to_string(s + 1) + "] =";
+                    at = t.find(key);
+                    if (at == std::string::npos) fail(MLB_EINVAL, "no " + key + " block in " + filename);
+                    size_t p = at + key.size();
+                    while (p < t.size() && (t[p] == ' ' || t[p] == '\t')) p++;
+                    double* out = all.data() + (((size_t)d * nz + s) * 9 + ab) * plane;
+                    if (t.compare(p, 2, "[[") != 0) continue;   // `= 0`: an all-zero array
+                    const size_t e = t.find("]]", p + 2);
+                    if (e == std::string::npos) fail(MLB_EINVAL, "unterminated " + key + " block in " + filename);
+                    const char* c = t.c_str() + p + 2;
+                    const char* stop = t.c_str() + e;
+                    size_t n = 0;
+                    while (c < stop && n < plane) {
+                        char* endp;
+                        const double v = strtod(c, &endp);
+                        if (endp == c) { c++; continue; }
+                        out[n++] = v;   // row y, column x
+                        c = endp;
+                    }
+                    if (n != plane) fail(MLB_EINVAL, key + " block of " + filename + " is not nx*ny numbers");
+                }
+        g_version++;
+        op->t2.swap(all);
+        op->lr2_newdata = false;
+        op->lr2_compile = true;
+        *loaded = 1;
+    });
+}
+
+} // extern "C"

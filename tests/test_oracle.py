@@ -332,3 +332,116 @@ def test_magnetostatics2d_builder_in_the_library(tmp_path):
                         np.testing.assert_allclose(-got, r, rtol=1e-6, atol=2e-7 * np.abs(r).max() + 1e-12)
     finally:
         lib.mlb_op_destroy(op)
+
+
+def _mag2d_reference_layout_text(fx):
+    """A Magnetostatics2D data file in the layout of the reference's writer
+    (mag2d_luafuncs.lua:278-330: header, builder state, then the blocks), with
+    the fixture's arrays as [1][1], [1][2] and their layer mirrors."""
+    a, g = fx["unit_cell"], fx["grain"]
+    lines = ["-- Magnetostatics2D Data File", "--", "MagLua_Version = 400", "", "-- system size",
+             "local nx, ny, nz = 16, 16, 2", "\t", "-- internal state", "local internal = {}",
+             "internal.ABC = {}", "internal.grainSize = {}"]
+    for z in (1, 2):
+        lines.append(f"internal.ABC[{z}] = {{{{{a:g}, 0, 0}}, {{0, {a:g}, 0}}, {{0, 0, {a:g}}}}}")
+    lines.append("")
+    for z in (1, 2):
+        lines.append(f"internal.grainSize[{z}] = {{{g:g}, {g:g}, {g:g}}}")
+    for k, v in zip(["truncation ", "truncationX", "truncationY", "truncationZ"], fx["truncation"]):
+        lines.append(f"internal.{k} = {v}")
+    lines += ["", "-- interaction tensors. Format is AB[destination_layer][source_layer]"]
+    for ab in NAMES9:
+        lines.append(f"local {ab} = {{{{}}, {{}}}}")
+    arrays = {}
+    for key, comps in fx["arrays"].items():
+        d, s_ = (int(v) for v in key.split(","))
+        for ab, rows in comps.items():
+            arrays[(ab, d, s_)] = rows
+            arrays[(ab, 3 - d, 3 - s_)] = rows
+    for ab in NAMES9:
+        for d in (1, 2):
+            for s_ in (1, 2):
+                lines.append(f"{ab}[{d}][{s_}] = [[")
+                for row in arrays[(ab, d, s_)]:
+                    lines.append(", ".join("0" if v == 0 else f"{v:E}" for v in row))
+                lines.append("]]")
+    lines.append("return function() end")
+    return "\n".join(lines) + "\n", arrays
+
+
+def test_lr2d_data_files_in_the_library(tmp_path):
+    """Tensor data files (dip2d_luafuncs.lua:278-500, mag2d_luafuncs.lua:
+    278-480) through the library's host code: a file in the reference's
+    layout loads only into a matching operator; a written file reads back."""
+    import ctypes as C
+    import maglua_b200
+    lib = maglua_b200._lib.load()
+    fx = _mag2d_fixture()
+    a, g = fx["unit_cell"], fx["grain"]
+    text, arrays = _mag2d_reference_layout_text(fx)
+    ref_file = tmp_path / "MAB_16x16x2.0.lua"
+    ref_file.write_text(text)
+    dp = C.POINTER(C.c_double)
+
+    def mag_op(grain=g, trunc=fx["truncation"]):
+        op = C.c_void_p()
+        assert lib.mlb_op_create(12, 16, 16, 2, C.byref(op)) == 0
+        for z in range(2):
+            assert lib.mlb_dipole2d_set_unit_cell(op, z, (C.c_double * 9)(a, 0, 0, 0, a, 0, 0, 0, a)) == 0
+            assert lib.mlb_magnetostatics2d_set_grain_size(op, z, (C.c_double * 3)(grain, grain, grain)) == 0
+        assert lib.mlb_dipole2d_set_truncation(op, (C.c_int * 4)(*trunc)) == 0
+        return op
+
+    def tensor(op, d, s_, ab):
+        buf = np.zeros(256)
+        assert lib.mlb_longrange2d_get_tensor(op, d, s_, ab, buf.ctypes.data_as(dp)) == 0
+        return buf.reshape(16, 16)
+
+    loaded = C.c_int()
+    op = mag_op()
+    try:
+        assert lib.mlb_lr2d_read_data_file(op, str(ref_file).encode(), C.byref(loaded)) == 0 and loaded.value == 1
+        nd, cr = C.c_int(), C.c_int()
+        assert lib.mlb_longrange2d_get_required(op, C.byref(nd), C.byref(cr)) == 0
+        assert (nd.value, cr.value) == (0, 1)
+        for (ab, d, s_), rows in arrays.items():
+            np.testing.assert_array_equal(tensor(op, d - 1, s_ - 1, NAMES9.index(ab)), np.asarray(rows))
+        # written by the library, read into a fresh operator
+        out = tmp_path / "MAB_16x16x2.1.lua"
+        assert lib.mlb_lr2d_write_data_file(op, str(out).encode()) == 0
+        txt = out.read_text()
+        assert txt.startswith("-- Magnetostatics2D Data File") and "internal.grainSize[2] = {1e-06, 1e-06, 1e-06}" in txt
+        op2 = mag_op()
+        assert lib.mlb_lr2d_read_data_file(op2, str(out).encode(), C.byref(loaded)) == 0 and loaded.value == 1
+        for d in range(2):
+            for s_ in range(2):
+                for ab in range(9):
+                    np.testing.assert_allclose(tensor(op2, d, s_, ab), tensor(op, d, s_, ab), rtol=1e-15, atol=0)
+        lib.mlb_op_destroy(op2)
+        # other grain size or truncation: not loaded, arrays untouched
+        for other in (mag_op(grain=2e-6), mag_op(trunc=(25, 25, 25, 25))):
+            assert lib.mlb_lr2d_read_data_file(other, str(ref_file).encode(), C.byref(loaded)) == 0
+            assert loaded.value == 0
+            assert lib.mlb_longrange2d_get_required(other, C.byref(nd), C.byref(cr)) == 0 and nd.value == 1
+            lib.mlb_op_destroy(other)
+        # a Dipole2D operator does not take a Magnetostatics2D file
+        dop = C.c_void_p()
+        assert lib.mlb_op_create(11, 16, 16, 2, C.byref(dop)) == 0
+        assert lib.mlb_lr2d_read_data_file(dop, str(ref_file).encode(), C.byref(loaded)) == 0 and loaded.value == 0
+        # Dipole2D round trip
+        assert lib.mlb_dipole2d_set_truncation(dop, (C.c_int * 4)(25, 3, 2, 1)) == 0
+        gab = tmp_path / "GAB_16x16x2.0.lua"
+        assert lib.mlb_lr2d_write_data_file(dop, str(gab).encode()) == 0
+        dop2 = C.c_void_p()
+        assert lib.mlb_op_create(11, 16, 16, 2, C.byref(dop2)) == 0
+        assert lib.mlb_dipole2d_set_truncation(dop2, (C.c_int * 4)(25, 3, 2, 1)) == 0
+        assert lib.mlb_lr2d_read_data_file(dop2, str(gab).encode(), C.byref(loaded)) == 0 and loaded.value == 1
+        T = O.dipole2d_tensor(16, 16, 2, np.tile(np.eye(3), (2, 1, 1)), np.zeros((2, 3)), (25, 3, 2, 1))
+        for d in range(2):
+            for s_ in range(2):
+                for ab in range(9):
+                    np.testing.assert_allclose(tensor(dop2, d, s_, ab), T[d, s_, ab], rtol=1e-15, atol=0)
+        lib.mlb_op_destroy(dop)
+        lib.mlb_op_destroy(dop2)
+    finally:
+        lib.mlb_op_destroy(op)
