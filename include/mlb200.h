@@ -112,6 +112,13 @@ int mlb_system_set_slot_used(mlb_system* s, const char* slot, int used);
 int mlb_system_ensure_slot(mlb_system* s, const char* slot);          /* _ensureSlotExists */
 /* netMoment(m): 8 numbers as the Lua method (spinsystem_luafuncs.lua:17-54). */
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8]);
+/* B200 extension (no reference counterpart): netMoment without waiting.
+ * _async enqueues the reduction of the current spins and its copy into
+ * pinned slot 0 or 1 on the system's stream and returns; _wait blocks until
+ * that slot's copy has landed and fills out8 as mlb_system_netmoment does.
+ * A caller can launch the next step before reading this step's result. */
+int mlb_system_netmoment_async(mlb_system* s, double m, int slot);
+int mlb_system_netmoment_wait(mlb_system* s, int slot, double out8[8]);
 /* sum_i s_i . h_slot,i in FP64 (the fieldArray:dot(spinArray) energy pattern). */
 int mlb_system_field_dot(mlb_system* s, const char* slot, double* out);
 /* copyTo (with_fields: spins, ms, per-site alpha/gamma, alpha, gamma, dt,

@@ -129,6 +129,8 @@ _SIGS = {
     "mlb_magnetostatics2d_set_grain_size": ([_P, C.c_int, _D], C.c_int),
     "mlb_magnetostatics2d_get_grain_size": ([_P, C.c_int, _D], C.c_int),
     "mlb_lr2d_write_data_file": ([_P, C.c_char_p], C.c_int),
+    "mlb_system_netmoment_async": ([_P, C.c_double, C.c_int], C.c_int),
+    "mlb_system_netmoment_wait": ([_P, C.c_int, _D], C.c_int),
     "mlb_lr2d_read_data_file": ([_P, C.c_char_p, _I], C.c_int),
     "mlb_llg_create": ([C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_llg_destroy": ([_P], C.c_int),
@@ -492,6 +494,16 @@ class SpinSystem:
     def netMoment(self, m=1.0):
         out = np.zeros(8)
         _ck(_lib.mlb_system_netmoment(self._h, float(m), _dp(out)))
+        return tuple(out)
+
+    def netMomentAsync(self, slot, m=1.0):
+        """Enqueue netMoment of the current spins into pinned slot 0 or 1
+        without waiting; netMomentWait(slot) returns it."""
+        _ck(_lib.mlb_system_netmoment_async(self._h, float(m), int(slot)))
+
+    def netMomentWait(self, slot):
+        out = np.zeros(8)
+        _ck(_lib.mlb_system_netmoment_wait(self._h, int(slot), _dp(out)))
         return tuple(out)
 
     def fieldDot(self, name):

@@ -177,6 +177,7 @@ struct LR2DPlan {
     int rb = 4;
     DBuf<char> tw;
     DBuf<char> spec;
+    DBuf<char> spec2;    // S2[kx][ky][c][z] for the FP32 register y passes
     DBuf<char> Q;
 };
 
@@ -231,9 +232,14 @@ struct mlb_system {
     bool dstep_known = false;
     // netMoment: reduction + copy to pinned memory captured once per spin
     // buffer (and per length argument m)
-    cudaGraphExec_t nm_exec[2] = {nullptr, nullptr};
-    double nm_m[2] = {0.0, 0.0};
-    double* nm_host = nullptr;      // pinned, 6 doubles
+    // netMoment: the reduction and its copy to pinned memory captured once per
+    // spin buffer q and destination d (0: the synchronous read, 1 and 2: the
+    // two slots of mlb_system_netmoment_async, each with an event)
+    cudaGraphExec_t nm_exec[2][3] = {};
+    double nm_m[2][3] = {};
+    double* nm_host = nullptr;      // pinned, 3 x 6 doubles
+    cudaEvent_t nm_ev[2] = {nullptr, nullptr};
+    bool nm_pending[2] = {false, false};
     double* red = nullptr;
     double* redout = nullptr;
     int red_nb = 1;
@@ -1045,6 +1051,11 @@ void build_lr2d(mlb_op* op, cudaStream_t st, int rb)
         CK(cudaStreamSynchronize(st));
     }
     P->spec.alloc((size_t)k.Kx * 3 * nz * ny * cb);
+    if (rb == 4 && mlb::x_fast_ok(k) && mlb::split_y_fast_ok(k)) {
+        // FP32 power-of-two planes: y transforms through a second spectrum
+        P->spec2.alloc((size_t)k.Kx * ny * 3 * nz * cb);
+        P->k.spec2 = P->spec2.p;
+    }
     op->lr2 = std::move(P);
     op->lr2_compile = false;
 }
@@ -1713,7 +1724,7 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     s->ms_token = ++g_ms_token;
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
-    CK(cudaMallocHost(&s->nm_host, sizeof(double) * 6));
+    CK(cudaMallocHost(&s->nm_host, sizeof(double) * 18));
     s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
     CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
     CK(cudaMalloc(&s->redout, sizeof(double) * 8));
@@ -1735,7 +1746,10 @@ void free_system(mlb_system* s)
     cudaFree(s->sg);
     cudaFree(s->dstep);
     for (int q = 0; q < 2; q++)
-        if (s->nm_exec[q]) cudaGraphExecDestroy(s->nm_exec[q]);
+        for (int d = 0; d < 3; d++)
+            if (s->nm_exec[q][d]) cudaGraphExecDestroy(s->nm_exec[q][d]);
+    for (int k = 0; k < 2; k++)
+        if (s->nm_ev[k]) cudaEventDestroy(s->nm_ev[k]);
     cudaFreeHost(s->nm_host);
     cudaFree(s->red);
     cudaFree(s->redout);
@@ -2583,38 +2597,72 @@ int mlb_system_ensure_slot(mlb_system* s, const char* slot)
     return guard([&] { slot_register(s, slot); });
 }
 
+// The netMoment reduction of the current spins with its copy to pinned
+// destination d (6 doubles at nm_host + 6 d), enqueued on the system's stream
+// as one captured graph per spin buffer and destination.
+static void netmoment_enqueue(mlb_system* s, double m, int d)
+{
+    const int q = s->cur;
+    if (!s->nm_exec[q][d] || s->nm_m[q][d] != m) {
+        if (s->nm_exec[q][d]) { cudaGraphExecDestroy(s->nm_exec[q][d]); s->nm_exec[q][d] = nullptr; }
+        CK(cudaStreamSynchronize(s->st));
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = mlb::launch_netmoment(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, s->red, s->red_nb,
+                                              s->redout, s->rb, s->st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->nm_host + 6 * d, s->redout, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->st);
+        cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&s->nm_exec[q][d], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            fail(MLB_ECUDA, std::string("netMoment graph: ") + cudaGetErrorString(e));
+        }
+        s->nm_m[q][d] = m;
+    }
+    CK(cudaGraphLaunch(s->nm_exec[q][d], s->st));
+}
+
+static void netmoment_out(const double* r, double out8[8])
+{
+    out8[0] = r[0]; out8[1] = r[1]; out8[2] = r[2];
+    out8[3] = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    out8[4] = r[3]; out8[5] = r[4]; out8[6] = r[5];
+    out8[7] = std::sqrt(r[3] * r[3] + r[4] * r[4] + r[5] * r[5]);
+}
+
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8])
 {
     return guard([&] {
-        const int q = s->cur;
-        if (!s->nm_exec[q] || s->nm_m[q] != m) {
-            // capture the reduction and the copy to pinned memory once
-            if (s->nm_exec[q]) { cudaGraphExecDestroy(s->nm_exec[q]); s->nm_exec[q] = nullptr; }
-            CK(cudaStreamSynchronize(s->st));
-            cudaGraph_t g = nullptr;
-            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e = mlb::launch_netmoment(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, s->red, s->red_nb,
-                                                  s->redout, s->rb, s->st);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(s->nm_host, s->redout, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->st);
-            cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
-            if (e == cudaSuccess) e = e2;
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&s->nm_exec[q], g, 0);
-            if (g) cudaGraphDestroy(g);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                fail(MLB_ECUDA, std::string("netMoment graph: ") + cudaGetErrorString(e));
-            }
-            s->nm_m[q] = m;
-        }
-        CK(cudaGraphLaunch(s->nm_exec[q], s->st));
+        netmoment_enqueue(s, m, 0);
         CK(cudaStreamSynchronize(s->st));
         double r[6];
         for (int k = 0; k < 6; k++) r[k] = s->nm_host[k];
-        out8[0] = r[0]; out8[1] = r[1]; out8[2] = r[2];
-        out8[3] = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-        out8[4] = r[3]; out8[5] = r[4]; out8[6] = r[5];
-        out8[7] = std::sqrt(r[3] * r[3] + r[4] * r[4] + r[5] * r[5]);
+        netmoment_out(r, out8);
+    });
+}
+
+int mlb_system_netmoment_async(mlb_system* s, double m, int slot)
+{
+    return guard([&] {
+        if (slot < 0 || slot > 1) fail(MLB_EINVAL, "netMoment slot must be 0 or 1");
+        if (!s->nm_ev[slot]) CK(cudaEventCreateWithFlags(&s->nm_ev[slot], cudaEventDisableTiming));
+        netmoment_enqueue(s, m, 1 + slot);
+        CK(cudaEventRecord(s->nm_ev[slot], s->st));
+        s->nm_pending[slot] = true;
+    });
+}
+
+int mlb_system_netmoment_wait(mlb_system* s, int slot, double out8[8])
+{
+    return guard([&] {
+        if (slot < 0 || slot > 1) fail(MLB_EINVAL, "netMoment slot must be 0 or 1");
+        if (!s->nm_pending[slot]) fail(MLB_ESTATE, "no netMoment enqueued in this slot");
+        CK(cudaEventSynchronize(s->nm_ev[slot]));
+        s->nm_pending[slot] = false;
+        netmoment_out(s->nm_host + 6 * (1 + slot), out8);
     });
 }
 

@@ -683,6 +683,20 @@ static cudaError_t launch_split_fast(const ConvK& c, const float2* twy, const fl
     return cudaErrorInvalidValue;
 }
 
+// The split y passes alone (forward: SPEC -> S2 = c.spec2, inverse: S2 ->
+// SPEC) for FP32 power-of-two Py in 32..512; used by LongRange2D, whose
+// layer mixing reads S2[kx][ky][comp][z] with each k-point's 3 nz values
+// contiguous.
+template <int PY>
+static cudaError_t launch_split_y_t(const ConvK& c, const float2* twy, float2* spec, bool fwd, cudaStream_t st)
+{
+    using Y = SPY<PY>;
+    float2* s2 = static_cast<float2*>(c.spec2);
+    const dim3 gy(c.Kx, 3, (c.nz + Y::LN - 1) / Y::LN);
+    if (fwd) return mlb::launch_pdl(k_sy_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)spec, s2);
+    return mlb::launch_pdl(k_syi_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)s2, spec);
+}
+
 template <int P>
 static cudaError_t cfg_split()
 {
@@ -949,6 +963,27 @@ bool conv_fast_ok(const ConvK& c)
 
 static cudaError_t launch_yz_any(const ConvK& c, const float2* twy, float2* spec, const float* ten6,
                                  cudaStream_t st);
+
+bool split_y_fast_ok(const ConvK& c)
+{
+    return c.nrep == 1 && c.Py >= 32 && c.Py <= 512 && (c.Py & (c.Py - 1)) == 0;
+}
+
+cudaError_t launch_split_y_fast(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, bool fwd,
+                                cudaStream_t st)
+{
+    const float2* twy = tw + L[1].tw_off;
+    Prof pf(fwd ? "k_sy_fast" : "k_syi_fast", st);
+    switch (c.Py) {
+    case 32: return launch_split_y_t<32>(c, twy, spec, fwd, st);
+    case 64: return launch_split_y_t<64>(c, twy, spec, fwd, st);
+    case 128: return launch_split_y_t<128>(c, twy, spec, fwd, st);
+    case 256: return launch_split_y_t<256>(c, twy, spec, fwd, st);
+    case 512: return launch_split_y_t<512>(c, twy, spec, fwd, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
 
 // (y,z) pass of the fast path: the whole-plane kernel, or the split passes
 static cudaError_t yz_pass(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const float* ten6,

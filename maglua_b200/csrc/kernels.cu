@@ -813,24 +813,31 @@ __global__ void k_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx,
 
 // ------------------------------------------------------------ LongRange2D
 // Layer-pair convolution, periodic in x and y (spinoperationlongrange2d.cpp:
-// 430-530).  Between the x passes of the dipole convolution (k_conv_fx,
-// k_conv_ix with Px = nx), one CTA per kx:
-//   y transforms of the 3 nz spectrum rows (comp, z);
-//   for each ky, destination layer d and component a:
-//     H_a[d] = dst[d] * sum_s src[s] sum_b Q[kx][ky][s][d][a][b] M_b[s]
-//   (Q: 2D transform over nx ny of the arrays set for (s, d), divided by
-//   nx ny -- the reference's apply reads its tensors [s][d]);
-//   inverse y transforms back to SPEC.
+// 430-530), between the x passes of the dipole convolution (k_conv_fx,
+// k_conv_ix with Px = nx):
+//   k_lr2d_ffty  one CTA per kx: the y transforms of the 3 nz spectrum rows
+//                (comp, z) in shared memory, in place (sign -1 forward, +1
+//                inverse);
+//   k_lr2d_mix   CTA (kx, LR2D_KB consecutive ky): for each ky, destination
+//                layer d and component a,
+//                  H_a[d] = dst[d] * sum_s src[s] sum_b Q[kx][ky][s][d][ab] M_b[s]
+//                (Q: the 2D transforms over nx ny of the arrays set for
+//                (s, d), divided by nx ny -- the reference's apply reads its
+//                tensors [s][d]).  Each CTA reads and writes only its own ky
+//                columns, so the mixing runs in place; many CTAs per kx keep
+//                the tensor stream (9 nz^2 complex per k-point) near the
+//                HBM roofline.
+constexpr int LR2D_KB = 8;
+
 template <typename R>
-__global__ void __launch_bounds__(512) k_lr2d_y(ConvK c, FftLen Ly, const typename CT<R>::T* tw,
-                                                typename CT<R>::T* spec, const typename CT<R>::T* Q, LR2DScale sc)
+__global__ void __launch_bounds__(512) k_lr2d_ffty(ConvK c, FftLen Ly, const typename CT<R>::T* tw,
+                                                   typename CT<R>::T* spec, int sign)
 {
-    if (c.run_if && *c.run_if == 0) return;
     typedef typename CT<R>::T C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* smf = reinterpret_cast<C*>(smraw);
-    const int kx = blockIdx.x, ny = c.ny, nz = c.nz;
-    const int NL = 3 * nz;   // lines (comp, z), rows of SPEC[kx]
+    const int kx = blockIdx.x, ny = c.ny;
+    const int NL = 3 * c.nz;
     C* A = smf;
     C* B = smf + (size_t)NL * ny;
     C* sp = spec + (size_t)kx * NL * ny;
@@ -838,28 +845,85 @@ __global__ void __launch_bounds__(512) k_lr2d_y(ConvK c, FftLen Ly, const typena
     __syncthreads();
     LineGeo g;
     g.nlines = NL; g.lpg = 1 << 30; g.gstride = 0; g.ls = ny; g.es = 1; g.line_fast = 0;
-    C* cur = ny > 1 ? cta_fft<C>(A, B, g, Ly, tw, -1) : A;
-    C* oth = cur == A ? B : A;
-    const C* Qk = Q + (size_t)kx * ny * nz * nz * 9;
-    for (int t = threadIdx.x; t < NL * ny; t += blockDim.x) {
-        const int a = t % 3, rest = t / 3, d = rest % nz, ky = rest / nz;
+    const C* cur = cta_fft<C>(A, B, g, Ly, tw, sign);
+    for (int t = threadIdx.x; t < NL * ny; t += blockDim.x) sp[t] = cur[t];
+}
+
+// The mixing on the split layout S2[kx][ky][comp][z] (FP32 power-of-two
+// ny, after k_sy_fast): a CTA's KB k-points are one contiguous block.
+__global__ void __launch_bounds__(256) k_lr2d_mix_s2(ConvK c, float2* s2, const float2* Q, LR2DScale sc)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float2* Mk = reinterpret_cast<float2*>(smraw);   // [j][b][s]
+    float2* Hk = Mk + (size_t)3 * c.nz * LR2D_KB;      // [j][a][d]
+    const int kx = blockIdx.x, ky0 = blockIdx.y * LR2D_KB, ny = c.ny, nz = c.nz;
+    const int nk = min(LR2D_KB, ny - ky0);
+    const int NL = 3 * nz;
+    pdl_wait();
+    float2* base = s2 + ((size_t)kx * ny + ky0) * NL;
+    for (int t = threadIdx.x; t < NL * nk; t += blockDim.x) Mk[t] = base[t];
+    __syncthreads();
+    const float2* Qk = Q + ((size_t)kx * ny + ky0) * nz * nz * 9;
+    for (int t = threadIdx.x; t < NL * nk; t += blockDim.x) {
+        const int a = t % 3, rest = t / 3, d = rest % nz, j = rest / nz;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int s = 0; s < nz; s++) {
+            const float2* q = Qk + (((size_t)j * nz + s) * nz + d) * 9 + 3 * a;
+            const float w = (float)sc.src[s];
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const float2 m = Mk[(size_t)j * NL + b * nz + s];
+                const float2 qq = q[b];
+                acc = cadd(acc, cmul(make_float2(w * qq.x, w * qq.y), m));
+            }
+        }
+        const float wd = (float)sc.dst[d];
+        Hk[(size_t)j * NL + a * nz + d] = make_float2(wd * acc.x, wd * acc.y);
+    }
+    __syncthreads();
+    pdl_trigger();
+    for (int t = threadIdx.x; t < NL * nk; t += blockDim.x) base[t] = Hk[t];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_lr2d_mix(ConvK c, typename CT<R>::T* spec, const typename CT<R>::T* Q,
+                                                  LR2DScale sc)
+{
+    typedef typename CT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* Mk = reinterpret_cast<C*>(smraw);          // [b nz + s][LR2D_KB]: the CTA's spectrum columns
+    C* Hk = Mk + (size_t)3 * c.nz * LR2D_KB;      // [a nz + d][LR2D_KB]: its output
+    const int kx = blockIdx.x, ky0 = blockIdx.y * LR2D_KB, ny = c.ny, nz = c.nz;
+    const int nk = min(LR2D_KB, ny - ky0);
+    const int NL = 3 * nz;
+    C* sp = spec + (size_t)kx * NL * ny + ky0;
+    for (int t = threadIdx.x; t < NL * LR2D_KB; t += blockDim.x) {
+        const int line = t / LR2D_KB, j = t % LR2D_KB;
+        if (j < nk) Mk[t] = sp[(size_t)line * ny + j];
+    }
+    __syncthreads();
+    const C* Qk = Q + ((size_t)kx * ny + ky0) * nz * nz * 9;
+    for (int t = threadIdx.x; t < NL * nk; t += blockDim.x) {
+        const int a = t % 3, rest = t / 3, d = rest % nz, j = rest / nz;
         C acc = cmk<C>((R)0, (R)0);
         for (int s = 0; s < nz; s++) {
-            const C* q = Qk + (((size_t)ky * nz + s) * nz + d) * 9 + 3 * a;
+            const C* q = Qk + (((size_t)j * nz + s) * nz + d) * 9 + 3 * a;
             const R w = (R)sc.src[s];
 #pragma unroll
             for (int b = 0; b < 3; b++) {
-                const C m = cur[((size_t)b * nz + s) * ny + ky];
+                const C m = Mk[((size_t)b * nz + s) * LR2D_KB + j];
                 const C qq = q[b];
                 acc = cadd(acc, cmul(cmk<C>(w * qq.x, w * qq.y), m));
             }
         }
         const R wd = (R)sc.dst[d];
-        oth[((size_t)a * nz + d) * ny + ky] = cmk<C>(wd * acc.x, wd * acc.y);
+        Hk[((size_t)a * nz + d) * LR2D_KB + j] = cmk<C>(wd * acc.x, wd * acc.y);
     }
     __syncthreads();
-    cur = ny > 1 ? cta_fft<C>(oth, cur, g, Ly, tw, +1) : oth;
-    for (int t = threadIdx.x; t < NL * ny; t += blockDim.x) sp[t] = cur[t];
+    for (int t = threadIdx.x; t < NL * LR2D_KB; t += blockDim.x) {
+        const int line = t / LR2D_KB, j = t % LR2D_KB;
+        if (j < nk) sp[(size_t)line * ny + j] = Hk[t];
+    }
 }
 
 // ------------------------------------------------------------ split (y,z) passes
@@ -1164,7 +1228,9 @@ cudaError_t conv_configure()
     if ((e = max_smem(k_split_y<float>)) || (e = max_smem(k_split_y<double>)) || (e = max_smem(k_split_yi<float>)) ||
         (e = max_smem(k_split_yi<double>)) || (e = max_smem(k_split_z<float>)) || (e = max_smem(k_split_z<double>)))
         return e;
-    if ((e = max_smem(k_lr2d_y<float>)) || (e = max_smem(k_lr2d_y<double>))) return e;
+    if ((e = max_smem(k_lr2d_mix_s2)) || (e = max_smem(k_lr2d_ffty<float>)) || (e = max_smem(k_lr2d_ffty<double>)) ||
+        (e = max_smem(k_lr2d_mix<float>)) || (e = max_smem(k_lr2d_mix<double>)))
+        return e;
     return max_smem(k_fft_lines<double2>);
 }
 
@@ -1305,9 +1371,33 @@ static void lr2d_t(const ConvK& c, const FftLen L[3], const void* tw_, const voi
         Prof pf("k_conv_fx", st);
         k_conv_fx<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, L[0], tw, s[0], s[1], s[2], spec);
     }
+    if (fast && split_y_fast_ok(c) && c.spec2) {
+        // register y transforms through S2 and the mixing on that layout
+        float2* sp2 = reinterpret_cast<float2*>(spec);
+        launch_split_y_fast(c, L, reinterpret_cast<const float2*>(tw), sp2, true, st);
+        {
+            Prof pf("k_lr2d_mix", st);
+            const size_t sm = (size_t)6 * c.nz * LR2D_KB * sizeof(float2);
+            launch_pdl(k_lr2d_mix_s2, dim3(c.Kx, (c.ny + LR2D_KB - 1) / LR2D_KB), dim3(256), sm, st, c,
+                       static_cast<float2*>(c.spec2), reinterpret_cast<const float2*>(Q), sc);
+        }
+        launch_split_y_fast(c, L, reinterpret_cast<const float2*>(tw), sp2, false, st);
+        launch_x_pass_fast(c, L, reinterpret_cast<const float2*>(tw), sf, sp2, hf, false, st);
+        return;
+    }
+    if (c.ny > 1) {
+        Prof pf("k_lr2d_ffty", st);
+        k_lr2d_ffty<R><<<c.Kx, 512, lr2d_smem(c, sizeof(R)), st>>>(c, L[1], tw, spec, -1);
+    }
     {
-        Prof pf("k_lr2d_y", st);
-        k_lr2d_y<R><<<c.Kx, 512, lr2d_smem(c, sizeof(R)), st>>>(c, L[1], tw, spec, static_cast<const C*>(Q), sc);
+        Prof pf("k_lr2d_mix", st);
+        const size_t sm = (size_t)6 * c.nz * LR2D_KB * sizeof(C);
+        k_lr2d_mix<R><<<dim3(c.Kx, (c.ny + LR2D_KB - 1) / LR2D_KB), 256, sm, st>>>(c, spec, static_cast<const C*>(Q),
+                                                                                    sc);
+    }
+    if (c.ny > 1) {
+        Prof pf("k_lr2d_ffty", st);
+        k_lr2d_ffty<R><<<c.Kx, 512, lr2d_smem(c, sizeof(R)), st>>>(c, L[1], tw, spec, +1);
     }
     if (fast) {
         launch_x_pass_fast(c, L, reinterpret_cast<const float2*>(tw), sf, reinterpret_cast<float2*>(spec), hf, false,

@@ -66,6 +66,11 @@ bool conv_fast_ok(const ConvK& c);
 // FP32 x passes alone (power-of-two periodic x, 16..512): the forward
 // transform of the spins to SPEC (fwd) or the inverse to the field h.
 bool x_fast_ok(const ConvK& c);
+// The FP32 split y passes alone: SPEC -> S2 (c.spec2) forward, S2 -> SPEC
+// inverse, power-of-two Py 32..512.
+bool split_y_fast_ok(const ConvK& c);
+cudaError_t launch_split_y_fast(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, bool fwd,
+                                cudaStream_t st);
 cudaError_t launch_x_pass_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                                float* h[3], bool fwd, cudaStream_t st);
 cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
@@ -113,7 +118,8 @@ cudaError_t launch_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, in
                                       const double2* W, double* out, cudaStream_t st);
 cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int Px, int Py, int Pz,
                                double2* W, cudaStream_t st);
-// LongRange2D: x passes around the per-kx layer mixing (k_lr2d_y); the
+// LongRange2D: x passes around the y transforms and the layer mixing
+// (k_lr2d_ffty, k_lr2d_mix); the
 // tensor spectrum Q[kx][ky][s][d][9] packed from FP64 transforms of the
 // layer pairs p0 .. p0 + np - 1.
 size_t lr2d_smem(const ConvK& c, int rb);

@@ -43,7 +43,7 @@ def _field(ss, name):
 
 
 @pytest.mark.parametrize("dims,precision", [((16, 12, 3), "f32"), ((12, 10, 2), "f32"), ((16, 8, 4), "f64"),
-                                            ((32, 32, 1), "f32")])
+                                            ((32, 32, 1), "f32"), ((64, 32, 3), "f32"), ((32, 64, 5), "f32")])
 def test_longrange2d_random_tensors(M, dims, precision):
     nx, ny, nz = dims
     r = np.random.default_rng(81)
@@ -144,7 +144,7 @@ def test_dipole2d_builder_and_field(M):
 
 def test_longrange2d_in_steps(M):
     """The operator inside captured steps: the same spins as individual calls."""
-    dims = (32, 16, 2)
+    dims = (32, 32, 2)
     nx, ny, nz = dims
     n = nx * ny * nz
     s0 = tilted_spins(n, 86, deg=20.0)
