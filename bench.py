@@ -258,6 +258,31 @@ def run_lr2d(M, torch, calls=20):
     return out
 
 
+# ----------------------------------------------------------------- DipoleEwald3D
+def run_ewald(M, edge=32):
+    """The Ewald tensor of an edge^3 simple-cubic lattice (NSites 10: 9261
+    real and reciprocal terms per element, 9 elements per site) computed on
+    the GPU (one FP64 thread per element), against the library's host path
+    timed on a sample of elements (the reference evaluates elements one by
+    one on the CPU)."""
+    ew = M.DipoleEwald3D(edge, edge, edge)
+    ew.calculateTensorElement("XX", (1, 0, 0))   # the eta search
+    t0 = time.perf_counter()
+    ew.tensorArrays()
+    gpu_s = time.perf_counter() - t0
+    k = 12
+    t0 = time.perf_counter()
+    for i in range(k):
+        ew.calculateTensorElement(["XX", "XY", "ZZ"][i % 3], (i % edge, (3 * i) % edge, (5 * i) % edge))
+    host_per = (time.perf_counter() - t0) / k
+    n_el = 9 * edge ** 3
+    return {"workload": f"DipoleEwald3D tensor of a {edge}^3 simple-cubic lattice, NSites 10, FP64",
+            "elements": n_el, "gpu_seconds": gpu_s, "host_seconds_per_element": host_per,
+            "host_seconds_estimate": host_per * n_el, "speedup": host_per * n_el / gpu_s,
+            "how": "wall clock around mlb_ewald3d_tensor (kernel + copy of 9 x edge^3 doubles) vs "
+                   "mlb_ewald3d_element on one host thread"}
+
+
 # ----------------------------------------------------------------- 256^3 open cube
 CUBE_DIMS = (256, 256, 256)
 CUBE_WORKLOAD = ("256^3 simple-cubic cube, open boundaries (512^3 padded transform, split (y,z) passes), "
@@ -660,6 +685,7 @@ def main():
     cube = run_cube(M, torch) if not args.no_cube else None
     rk = run_rk(M, torch)
     lr2d = run_lr2d(M, torch)
+    ewald = run_ewald(M)
 
     if rank != 0:
         if dist:
@@ -718,6 +744,7 @@ def main():
         "cube_256": cube,
         "rk4": rk,
         "dipole2d": lr2d,
+        "ewald3d": ewald,
     }
     print(json.dumps(line), flush=True)
     if dist:

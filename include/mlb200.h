@@ -258,6 +258,38 @@ int mlb_magnetostatics2d_get_grain_size(const mlb_op* op, int layer, double g[3]
 int mlb_lr2d_write_data_file(mlb_op* op, const char* filename);
 int mlb_lr2d_read_data_file(mlb_op* op, const char* filename, int* loaded);
 
+/* ---------------------------------------------------------------- DipoleEwald3D
+ * M/cpu/ewald3d/ewald3d.cpp: the dipolar tensor G_ab(r) of a periodic
+ * lattice of nx x ny x nz unit cells by Ewald summation in FP64 (the
+ * tensor source of LongRange3D in make_tensor.lua, which stores -G).
+ * Defaults: cubic unit cell, NSites 10, tau 1e-3.  eta (the real/reciprocal
+ * split) is searched at the first element after the geometry, tau or NSites
+ * changed, as calcTensorElement does it: G_xx's N -> N + 1 shell at r = a1
+ * minimised by golden sections with the shell count taken from the integer
+ * part of tau (findEta(a1, tau), ewald3d.cpp:30) and tolerance 1e-3;
+ * MLB_ESTATE when the search does not converge.  setTau ignores tau <= 0 and
+ * setNSites n <= 1, as the reference.  ab = 3*a + b in XX..ZZ order. */
+typedef struct mlb_ewald3d mlb_ewald3d;
+int mlb_ewald3d_create(int nx, int ny, int nz, mlb_ewald3d** out);       /* DipoleEwald3D.new(nx,ny,nz) */
+int mlb_ewald3d_destroy(mlb_ewald3d* e);
+int mlb_ewald3d_set_unit_cell(mlb_ewald3d* e, const double a[3], const double b[3], const double c[3]);
+int mlb_ewald3d_get_unit_cell(const mlb_ewald3d* e, double abc[9]);
+int mlb_ewald3d_set_lattice_size(mlb_ewald3d* e, int nx, int ny, int nz);
+int mlb_ewald3d_get_lattice_size(const mlb_ewald3d* e, int n3[3]);
+int mlb_ewald3d_set_tau(mlb_ewald3d* e, double tau);
+int mlb_ewald3d_get_tau(const mlb_ewald3d* e, double* tau);
+int mlb_ewald3d_set_nsites(mlb_ewald3d* e, int n);
+int mlb_ewald3d_get_nsites(const mlb_ewald3d* e, int* n);
+int mlb_ewald3d_get_eta(const mlb_ewald3d* e, double* eta);
+int mlb_ewald3d_get_volume(const mlb_ewald3d* e, double* v);           /* volume: supercell |u1.(u2 x u3)| */
+/* calculateTensorElement(AB, {x,y,z}) at r = x a + y b + z c (host) */
+int mlb_ewald3d_element(mlb_ewald3d* e, int ab, const int r3[3], double* out);
+/* calculateTensorElementRealR(AB, {rx,ry,rz}) (host) */
+int mlb_ewald3d_element_real(mlb_ewald3d* e, int ab, const double r[3], double* out);
+/* B200 extension: every element of the lattice, out9[ab][x + nx*(y + ny*z)]
+ * = calculateTensorElement(ab, {x,y,z}), one GPU thread per element (FP64). */
+int mlb_ewald3d_tensor(mlb_ewald3d* e, double* out9);
+
 /* ---------------------------------------------------------------- LLG
  * M/cpu/llg/llg.cpp:91-171, llgcartesian.cpp:90-278, llgquat.cpp:126-378. */
 #define MLB_LLG_CARTESIAN 0

@@ -130,6 +130,21 @@ _SIGS = {
     "mlb_magnetostatics2d_get_grain_size": ([_P, C.c_int, _D], C.c_int),
     "mlb_lr2d_write_data_file": ([_P, C.c_char_p], C.c_int),
     "mlb_system_netmoment_async": ([_P, C.c_double, C.c_int], C.c_int),
+    "mlb_ewald3d_create": ([C.c_int, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_ewald3d_destroy": ([_P], C.c_int),
+    "mlb_ewald3d_set_unit_cell": ([_P, _D, _D, _D], C.c_int),
+    "mlb_ewald3d_get_unit_cell": ([_P, _D], C.c_int),
+    "mlb_ewald3d_set_lattice_size": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "mlb_ewald3d_get_lattice_size": ([_P, _I], C.c_int),
+    "mlb_ewald3d_set_tau": ([_P, C.c_double], C.c_int),
+    "mlb_ewald3d_get_tau": ([_P, _D], C.c_int),
+    "mlb_ewald3d_set_nsites": ([_P, C.c_int], C.c_int),
+    "mlb_ewald3d_get_nsites": ([_P, _I], C.c_int),
+    "mlb_ewald3d_get_eta": ([_P, _D], C.c_int),
+    "mlb_ewald3d_get_volume": ([_P, _D], C.c_int),
+    "mlb_ewald3d_element": ([_P, C.c_int, _I, _D], C.c_int),
+    "mlb_ewald3d_element_real": ([_P, C.c_int, _D, _D], C.c_int),
+    "mlb_ewald3d_tensor": ([_P, _D], C.c_int),
     "mlb_system_netmoment_wait": ([_P, C.c_int, _D], C.c_int),
     "mlb_lr2d_read_data_file": ([_P, C.c_char_p, _I], C.c_int),
     "mlb_llg_create": ([C.c_int, C.POINTER(_P)], C.c_int),
@@ -1142,6 +1157,109 @@ class Magnetostatics2D(Dipole2D):
         a[int(y), int(x)] = float(v)
         self.setTensorArray(dest, src, ab, a.reshape(-1))
         self.setCompileRequired(True)
+
+
+class DipoleEwald3D:
+    """DipoleEwald3D (M/cpu/ewald3d): the dipolar tensor G_ab(r) of a
+    periodic nx x ny x nz lattice by Ewald summation in FP64, element by
+    element on the host or every element of the lattice on the GPU
+    (tensorArrays).  make_tensor.lua stores -G into LongRange3D."""
+
+    def __init__(self, *args):
+        dims = self._dims_of(args)
+        h = _P()
+        _ck(_lib.mlb_ewald3d_create(int(dims[0]), int(dims[1]), int(dims[2]), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.mlb_ewald3d_destroy(h)
+            self._h = None
+
+    @classmethod
+    def new(cls, *a):
+        return cls(*a)
+
+    @staticmethod
+    def _dims_of(args):
+        if args and isinstance(args[0], SpinSystem):
+            return (args[0].nx(), args[0].ny(), args[0].nz())
+        if args and hasattr(args[0], "__len__"):
+            return (tuple(int(v) for v in args[0]) + (1, 1, 1))[:3]
+        return (tuple(int(a) for a in args) + (1, 1, 1))[:3]
+
+    def setUnitCell(self, a, b, c):
+        va, vb, vc = (np.asarray(v, dtype=np.float64) for v in (a, b, c))
+        _ck(_lib.mlb_ewald3d_set_unit_cell(self._h, _dp(va), _dp(vb), _dp(vc)))
+
+    def unitCell(self):
+        out = np.zeros(9)
+        _ck(_lib.mlb_ewald3d_get_unit_cell(self._h, _dp(out)))
+        return list(out[0:3]), list(out[3:6]), list(out[6:9])
+
+    def latticeSize(self):
+        n = (C.c_int * 3)()
+        _ck(_lib.mlb_ewald3d_get_lattice_size(self._h, n))
+        return tuple(n)
+
+    def setLatticeSize(self, *args):
+        dims = self._dims_of(args)
+        _ck(_lib.mlb_ewald3d_set_lattice_size(self._h, int(dims[0]), int(dims[1]), int(dims[2])))
+
+    def volume(self):
+        v = C.c_double()
+        _ck(_lib.mlb_ewald3d_get_volume(self._h, C.byref(v)))
+        return v.value
+
+    def tau(self):
+        v = C.c_double()
+        _ck(_lib.mlb_ewald3d_get_tau(self._h, C.byref(v)))
+        return v.value
+
+    def setTau(self, t):
+        _ck(_lib.mlb_ewald3d_set_tau(self._h, float(t)))
+
+    def NSites(self):
+        v = C.c_int()
+        _ck(_lib.mlb_ewald3d_get_nsites(self._h, C.byref(v)))
+        return v.value
+
+    def setNSites(self, n):
+        _ck(_lib.mlb_ewald3d_set_nsites(self._h, int(n)))
+
+    def eta(self):
+        v = C.c_double()
+        _ck(_lib.mlb_ewald3d_get_eta(self._h, C.byref(v)))
+        return v.value
+
+    @staticmethod
+    def _ab(AB):
+        ab = str(AB).upper()[:2]
+        if len(ab) < 2 or ab not in _AB9:
+            raise MagLuaError(-1, "first argument of calculateTensorElement must be AB pair: `XX', `XY', ... `ZZ'")
+        return _AB9[ab]
+
+    def calculateTensorElement(self, AB, xyz):
+        r = (C.c_int * 3)(*[int(v) for v in xyz])
+        out = C.c_double()
+        _ck(_lib.mlb_ewald3d_element(self._h, self._ab(AB), r, C.byref(out)))
+        return out.value
+
+    def calculateTensorElementRealR(self, AB, r):
+        rr = np.asarray(r, dtype=np.float64)
+        out = C.c_double()
+        _ck(_lib.mlb_ewald3d_element_real(self._h, self._ab(AB), _dp(rr), C.byref(out)))
+        return out.value
+
+    def tensorArrays(self):
+        """Every element of the lattice computed on the GPU: {AB: array
+        (nz, ny, nx)} with the values calculateTensorElement returns."""
+        nx, ny, nz = self.latticeSize()
+        out = np.zeros(9 * nx * ny * nz)
+        _ck(_lib.mlb_ewald3d_tensor(self._h, _dp(out)))
+        out = out.reshape(9, nz, ny, nx)
+        return {ab: out[k] for ab, k in _AB9.items()}
 
 
 # ====================================================================== LLG

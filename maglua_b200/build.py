@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmlb200.so")
-SOURCES = ["kernels.cu", "conv_fast.cu", "surrogate.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "conv_fast.cu", "surrogate.cu", "ewald.cu", "capi.cu"]
 HEADERS = ["device.cuh", "fftreg.cuh", "fused.cuh", "kparams.h", "launch.h", "umma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

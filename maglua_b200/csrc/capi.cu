@@ -5033,3 +5033,9 @@ int mlb_lr2d_read_data_file(mlb_op* op, const char* filename, int* loaded)
 }
 
 } // extern "C"
+
+namespace mlb {
+// The message mlb_last_error returns, for entry points defined in other
+// translation units (ewald.cu).
+void set_last_error(const std::string& msg) { g_err = msg; }
+} // namespace mlb

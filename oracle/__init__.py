@@ -560,6 +560,132 @@ def magnetostatics2d_tensor(nx, ny, nz, abc, grain, trunc):
     return T
 
 
+# ---------------------------------------------------------------- DipoleEwald3D
+def ewald_geometry(d, a):
+    """Supercell vectors, reciprocal vectors and volume (ewald3d.cpp:76-104)."""
+    u = [[d[i] * a[i][c] for c in range(3)] for i in range(3)]
+
+    def cross(p, q):
+        return [p[1] * q[2] - p[2] * q[1], p[2] * q[0] - p[0] * q[2], p[0] * q[1] - p[1] * q[0]]
+
+    def dot(p, q):
+        return p[0] * q[0] + p[1] * q[1] + p[2] * q[2]
+
+    c23, c31, c12 = cross(u[1], u[2]), cross(u[2], u[0]), cross(u[0], u[1])
+    vu = abs(dot(u[0], c23))
+    b = [[2.0 * math.pi * c23[c] / vu for c in range(3)], [2.0 * math.pi * c31[c] / vu for c in range(3)],
+         [2.0 * math.pi * c12[c] / vu for c in range(3)]]
+    return u, b, vu
+
+
+def _ew_term(g, alpha, beta, r, eta, n, m, k):
+    u, b, vu = g
+    eta2 = eta * eta
+    delta = 1.0 if alpha == beta else 0.0
+    Q = [n * b[0][i] + m * b[1][i] + k * b[2][i] for i in range(3)]
+    r0 = (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) == 0
+    if r0:
+        R = [n * u[0][i] + m * u[1][i] + k * u[2][i] for i in range(3)]
+    else:
+        R = [n * u[0][i] + m * u[1][i] + k * u[2][i] + r[i] for i in range(3)]
+    Q2 = Q[0] * Q[0] + Q[1] * Q[1] + Q[2] * Q[2]
+    if math.sqrt(Q2) > 0:
+        if r0:
+            rec = -4.0 * math.pi * math.exp(-Q2 / (4.0 * eta2)) * (Q2 * delta - 3 * Q[alpha] * Q[beta]) / (3.0 * vu * Q2)
+        else:
+            rq = r[0] * Q[0] + r[1] * Q[1] + r[2] * Q[2]
+            rec = 4.0 * math.pi * Q[alpha] * Q[beta] * math.cos(rq) * math.exp(-Q2 / (4.0 * eta2)) / (Q2 * vu)
+    else:
+        rec = 0.0
+    Rab = R[alpha] * R[beta]
+    R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2]
+    R1 = math.sqrt(R2)
+    R4 = R2 * R2
+    R5 = R4 * R1
+    sp = 1.772453850905516027
+    if R1 > 0:
+        if r0:
+            real = (R2 * delta - 3.0 * R[alpha] * R[beta]) * (
+                2.0 * eta * math.exp(-R2 * eta2) * (3.0 + 2.0 * R2 * eta2) / (3.0 * R4 * sp) + math.erfc(R1 * eta) / R5)
+        else:
+            real = (2.0 * eta * math.exp(-eta2 * R2) * (R2 * delta - 3.0 * Rab - 2.0 * eta2 * Rab * R2) / (sp * R4)
+                    + (R2 * delta - 3.0 * Rab) * math.erfc(eta * R1) / R5)
+    else:
+        real = 0.0
+    return real, rec
+
+
+def ewald_element(g, alpha, beta, r, eta, N):
+    """G_ab(r) (ewald3d.cpp:330-358): real and reciprocal parts summed
+    separately over n, m, k in [-N, N]."""
+    tq = tr = 0.0
+    for n in range(-N, N + 1):
+        for m in range(-N, N + 1):
+            for k in range(-N, N + 1):
+                a, b = _ew_term(g, alpha, beta, r, eta, n, m, k)
+                tr += a
+                tq += b
+    return tq + tr
+
+
+def ewald_next_shell(g, alpha, beta, r, eta, N):
+    """G(N + 1) - G(N) by its surface shell (ewald3d.cpp:361-422)."""
+    tq = tr = 0.0
+    M = N + 1
+    faces = [[(n, m, M) for n in range(-M, M + 1) for m in range(-M, M + 1)],
+             [(n, M, k) for n in range(-M, M + 1) for k in range(-N, N + 1)],
+             [(M, m, k) for m in range(-N, N + 1) for k in range(-N, N + 1)]]
+    for fi, face in enumerate(faces):
+        for t in face:
+            neg = list(t)
+            neg[2 - fi] = -neg[2 - fi]
+            a1, b1 = _ew_term(g, alpha, beta, r, eta, *t)
+            a2, b2 = _ew_term(g, alpha, beta, r, eta, *neg)
+            tr += a1
+            tq += b1
+            tr += a2
+            tq += b2
+    return tq + tr
+
+
+def ewald_find_eta(g, r3, N, tol=1e-3):
+    """Golden-section search for eta (ewald3d.cpp:109-218); None when the 100
+    levels run out."""
+    RGR, MINA = 0.3819660112501051518, 1e-10
+
+    def F(x):
+        return abs(ewald_next_shell(g, 0, 0, r3, x, N))
+
+    def rec(depth, a, fa, b, fb, c, fc):
+        if depth < 0:
+            return None
+        if a > MINA and fa < fb < fc:
+            x = c + RGR * (c - b)
+            return rec(depth - 1, b, fb, c, fc, x, F(x))
+        if fa > fb > fc:
+            x = a - RGR * (b - a)
+            return rec(depth - 1, x, F(x), a, fa, b, fb)
+        if (c - b) > (b - a):
+            x = b + RGR * (c - b)
+            if (c - a) < tol * (abs(b) + abs(x)):
+                return (c + a) * 0.5
+            fx = F(x)
+            if fx < fb:
+                return rec(depth - 1, b, fb, x, fx, c, fc)
+            return rec(depth - 1, a, fa, b, fb, x, fx)
+        x = b - RGR * (b - a)
+        if (c - a) < tol * (abs(b) + abs(x)):
+            return (c + a) * 0.5
+        fx = F(x)
+        if fx < fb:
+            return rec(depth - 1, a, fa, x, fx, b, fb)
+        return rec(depth - 1, x, fx, b, fb, c, fc)
+
+    a, c = MINA, 1000.0
+    b = a + RGR * (c - a)
+    return rec(100, a, F(a), b, F(b), c, F(c))
+
+
 def fft1d(data, sign):
     d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128)).copy()
     lib.orc_fft1d(d.view(np.float64).ctypes.data_as(_D), len(d), 1, sign)

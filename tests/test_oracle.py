@@ -445,3 +445,66 @@ def test_lr2d_data_files_in_the_library(tmp_path):
         lib.mlb_op_destroy(dop2)
     finally:
         lib.mlb_op_destroy(op)
+
+
+SHEARED = [[1, 0, 0], [0.5, 0.8, 0], [0.1, 0.2, 0.9]]
+
+
+def test_ewald_oracle_physics():
+    """Properties of the Ewald sum that hold whatever its implementation:
+    trace G(r) = -4 pi / V away from the lattice points, independence of the
+    real/reciprocal split eta, and G_aa(0) = 0 on a cubic lattice."""
+    g = O.ewald_geometry((4, 4, 4), SHEARED)
+    eta = O.ewald_find_eta(g, SHEARED[0], 0)
+    assert eta is not None and 0.5 < eta < 5
+    for r in ([0.3, -1.1, 2.0], [2.0, 2.0, 2.0]):
+        tr = sum(O.ewald_element(g, a, a, r, eta, 10) for a in range(3))
+        assert tr == pytest.approx(-4 * np.pi / g[2], rel=1e-9)
+    v = O.ewald_element(g, 0, 1, [0.3, -1.1, 2.0], eta, 10)
+    for e2 in (0.8 * eta, 1.2 * eta):
+        assert O.ewald_element(g, 0, 1, [0.3, -1.1, 2.0], e2, 10) == pytest.approx(v, rel=1e-8)
+    gc = O.ewald_geometry((3, 3, 3), np.eye(3))
+    ec = O.ewald_find_eta(gc, [1, 0, 0], 0)
+    for a in range(3):
+        assert abs(O.ewald_element(gc, a, a, [0, 0, 0], ec, 8)) < 1e-12
+
+
+def test_ewald_library_host_path():
+    """DipoleEwald3D through the library's host code (no GPU): the eta search
+    and single elements against the oracle's restatement of ewald3d.cpp."""
+    import ctypes as C
+    import maglua_b200
+    lib = maglua_b200._lib.load()
+    e = C.c_void_p()
+    assert lib.mlb_ewald3d_create(4, 4, 4, C.byref(e)) == 0
+    try:
+        d3 = lambda v: (C.c_double * 3)(*v)   # noqa: E731
+        assert lib.mlb_ewald3d_set_unit_cell(e, d3(SHEARED[0]), d3(SHEARED[1]), d3(SHEARED[2])) == 0
+        vol = C.c_double()
+        lib.mlb_ewald3d_get_volume(e, C.byref(vol))
+        g = O.ewald_geometry((4, 4, 4), SHEARED)
+        assert vol.value == g[2]
+        out = C.c_double()
+        assert lib.mlb_ewald3d_element(e, 1, (C.c_int * 3)(1, 2, 0), C.byref(out)) == 0
+        eta = C.c_double()
+        lib.mlb_ewald3d_get_eta(e, C.byref(eta))
+        eta_o = O.ewald_find_eta(g, SHEARED[0], 0)
+        assert eta.value == pytest.approx(eta_o, rel=2e-3)
+        for ab, r3 in [(1, (1, 2, 0)), (0, (0, 0, 0)), (4, (0, 0, 0)), (5, (3, 1, 2)), (7, (3, 1, 2)), (8, (2, 0, 1))]:
+            assert lib.mlb_ewald3d_element(e, ab, (C.c_int * 3)(*r3), C.byref(out)) == 0
+            r = [sum(r3[j] * SHEARED[j][i] for j in range(3)) for i in range(3)]
+            ref = O.ewald_element(g, ab // 3, ab % 3, r, eta.value, 10)
+            assert out.value == pytest.approx(ref, rel=1e-12, abs=1e-15)
+        assert lib.mlb_ewald3d_element_real(e, 2, d3([0.3, -1.1, 2.0]), C.byref(out)) == 0
+        assert out.value == pytest.approx(O.ewald_element(g, 0, 2, [0.3, -1.1, 2.0], eta.value, 10), rel=1e-12)
+        # reference setters: tau <= 0 and NSites <= 1 are ignored
+        lib.mlb_ewald3d_set_tau(e, C.c_double(-1.0))
+        lib.mlb_ewald3d_set_nsites(e, 1)
+        t, n = C.c_double(), C.c_int()
+        lib.mlb_ewald3d_get_tau(e, C.byref(t))
+        lib.mlb_ewald3d_get_nsites(e, C.byref(n))
+        assert (t.value, n.value) == (1e-3, 10)
+        assert lib.mlb_ewald3d_element(e, 9, (C.c_int * 3)(0, 0, 0), C.byref(out)) != 0
+        assert b"AB pair" in lib.mlb_last_error()
+    finally:
+        lib.mlb_ewald3d_destroy(e)
