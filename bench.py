@@ -664,7 +664,8 @@ def main():
     t0 = time.perf_counter()
     ss.uploadF32(hx, hy, hz, hm)
     # each step's netMoment is read on the host; the read of step k waits
-    # while step k + 1 is already queued on the GPU
+    # while step k + 1 is already queued on the GPU (a deeper queue measured
+    # slower: the plan's step-block upload then waits for the GPU)
     for k in range(args.steps):
         plan_nt.launch(1)
         ss.netMomentAsync(k & 1)

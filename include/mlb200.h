@@ -114,7 +114,7 @@ int mlb_system_ensure_slot(mlb_system* s, const char* slot);          /* _ensure
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8]);
 /* B200 extension (no reference counterpart): netMoment without waiting.
  * _async enqueues the reduction of the current spins and its copy into
- * pinned slot 0 or 1 on the system's stream and returns; _wait blocks until
+ * pinned slot 0..3 on the system's stream and returns; _wait blocks until
  * that slot's copy has landed and fills out8 as mlb_system_netmoment does.
  * A caller can launch the next step before reading this step's result. */
 int mlb_system_netmoment_async(mlb_system* s, double m, int slot);

@@ -512,7 +512,7 @@ class SpinSystem:
         return tuple(out)
 
     def netMomentAsync(self, slot, m=1.0):
-        """Enqueue netMoment of the current spins into pinned slot 0 or 1
+        """Enqueue netMoment of the current spins into pinned slot 0..3
         without waiting; netMomentWait(slot) returns it."""
         _ck(_lib.mlb_system_netmoment_async(self._h, float(m), int(slot)))
 

@@ -233,13 +233,13 @@ struct mlb_system {
     // netMoment: reduction + copy to pinned memory captured once per spin
     // buffer (and per length argument m)
     // netMoment: the reduction and its copy to pinned memory captured once per
-    // spin buffer q and destination d (0: the synchronous read, 1 and 2: the
-    // two slots of mlb_system_netmoment_async, each with an event)
-    cudaGraphExec_t nm_exec[2][3] = {};
-    double nm_m[2][3] = {};
-    double* nm_host = nullptr;      // pinned, 3 x 6 doubles
-    cudaEvent_t nm_ev[2] = {nullptr, nullptr};
-    bool nm_pending[2] = {false, false};
+    // spin buffer q and destination d (0: the synchronous read, 1..4: the
+    // slots of mlb_system_netmoment_async, each with an event)
+    cudaGraphExec_t nm_exec[2][5] = {};
+    double nm_m[2][5] = {};
+    double* nm_host = nullptr;      // pinned, 5 x 6 doubles
+    cudaEvent_t nm_ev[4] = {};
+    bool nm_pending[4] = {};
     double* red = nullptr;
     double* redout = nullptr;
     int red_nb = 1;
@@ -1724,7 +1724,7 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     s->ms_token = ++g_ms_token;
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
-    CK(cudaMallocHost(&s->nm_host, sizeof(double) * 18));
+    CK(cudaMallocHost(&s->nm_host, sizeof(double) * 30));
     s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
     CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
     CK(cudaMalloc(&s->redout, sizeof(double) * 8));
@@ -1746,9 +1746,9 @@ void free_system(mlb_system* s)
     cudaFree(s->sg);
     cudaFree(s->dstep);
     for (int q = 0; q < 2; q++)
-        for (int d = 0; d < 3; d++)
+        for (int d = 0; d < 5; d++)
             if (s->nm_exec[q][d]) cudaGraphExecDestroy(s->nm_exec[q][d]);
-    for (int k = 0; k < 2; k++)
+    for (int k = 0; k < 4; k++)
         if (s->nm_ev[k]) cudaEventDestroy(s->nm_ev[k]);
     cudaFreeHost(s->nm_host);
     cudaFree(s->red);
@@ -2647,7 +2647,7 @@ int mlb_system_netmoment(mlb_system* s, double m, double out8[8])
 int mlb_system_netmoment_async(mlb_system* s, double m, int slot)
 {
     return guard([&] {
-        if (slot < 0 || slot > 1) fail(MLB_EINVAL, "netMoment slot must be 0 or 1");
+        if (slot < 0 || slot > 3) fail(MLB_EINVAL, "netMoment slot must be 0..3");
         if (!s->nm_ev[slot]) CK(cudaEventCreateWithFlags(&s->nm_ev[slot], cudaEventDisableTiming));
         netmoment_enqueue(s, m, 1 + slot);
         CK(cudaEventRecord(s->nm_ev[slot], s->st));
@@ -2658,7 +2658,7 @@ int mlb_system_netmoment_async(mlb_system* s, double m, int slot)
 int mlb_system_netmoment_wait(mlb_system* s, int slot, double out8[8])
 {
     return guard([&] {
-        if (slot < 0 || slot > 1) fail(MLB_EINVAL, "netMoment slot must be 0 or 1");
+        if (slot < 0 || slot > 3) fail(MLB_EINVAL, "netMoment slot must be 0..3");
         if (!s->nm_pending[slot]) fail(MLB_ESTATE, "no netMoment enqueued in this slot");
         CK(cudaEventSynchronize(s->nm_ev[slot]));
         s->nm_pending[slot] = false;

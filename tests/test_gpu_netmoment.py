@@ -46,5 +46,5 @@ def test_netmoment_async_slots(M):
     np.testing.assert_allclose(np.asarray(sync[-1]), o.netmoment(0.5), rtol=1e-9, atol=1e-9)
     with pytest.raises(M.MagLuaError, match="no netMoment enqueued"):
         ss.netMomentWait(0)
-    with pytest.raises(M.MagLuaError, match="slot must be 0 or 1"):
-        ss.netMomentAsync(2)
+    with pytest.raises(M.MagLuaError, match="slot must be 0..3"):
+        ss.netMomentAsync(4)
