@@ -303,7 +303,7 @@ class SpinSystem:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_system_destroy(h)
             self._h = None
 
@@ -584,7 +584,7 @@ class SpinOperation:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_op_destroy(h)
             self._h = None
 
@@ -1173,7 +1173,7 @@ class DipoleEwald3D:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_ewald3d_destroy(h)
             self._h = None
 
@@ -1282,7 +1282,7 @@ class _LLGBase:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_llg_destroy(h)
             self._h = None
 
@@ -1411,7 +1411,7 @@ class Plan:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_plan_destroy(h)
             self._h = None
 
@@ -1440,7 +1440,7 @@ class Ensemble:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_ensemble_destroy(h)
             self._h = None
 
@@ -1515,7 +1515,7 @@ class Surrogate:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.mlb_surrogate_destroy(h)
             self._h = None
 
