@@ -669,6 +669,32 @@ void ensure_t6_layout(mlb_op* op)
         if (op->t6[q].size() != ne) op->t6[q].assign(ne, 0.0);
 }
 
+// The FP32 split passes with power-of-two planes (the register z pass) can
+// read a quarter tensor.
+bool quarter_ok(const ConvK& k, int rb)
+{
+    auto p2 = [](int v) { return v >= 32 && v <= 512 && (v & (v - 1)) == 0; };
+    return rb == 4 && k.split && !k.general && mlb::conv_fast_ok(k) && p2(k.Py) && p2(k.Pz);
+}
+
+// Whether the FP64 transformed tensor W holds the per-axis parities of a
+// point-dipole tensor on an orthogonal lattice to 1e-10 of its largest
+// element (rounding of the transform is ~1e-15 of it; a tensor without the
+// parities misses by O(1)).
+bool tensor_has_parities(const double2* W, const ConvK& k, cudaStream_t st)
+{
+    DBuf<unsigned long long> out;
+    out.alloc(3);
+    CK(cudaMemsetAsync(out.p, 0, sizeof(unsigned long long) * 3, st));
+    CK(mlb::launch_tensor_symcheck(W, k.Px, k.Py, k.Pz, k.Kx, out.p, st));
+    unsigned long long h[3];
+    CK(cudaMemcpyAsync(h, out.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double d[3];
+    memcpy(d, h, sizeof(d));
+    return d[0] > 0 && d[1] <= 1e-10 * d[0] && d[2] <= 1e-10 * d[0];
+}
+
 // Build or rebuild the tensor spectrum of op (FP64 on the GPU), stored at
 // rb bytes per real for the systems it is applied to.
 void build_plan(mlb_op* op, cudaStream_t st, int rb)
@@ -754,6 +780,11 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
     if (k.general) {
         P->ten9.alloc((size_t)k.Kx * Py * Pz * 9 * 2 * rb);
         CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, rb, k.split, st));
+    } else if (quarter_ok(k, rb) && tensor_has_parities(W.p, k, st)) {
+        // the split FP32 passes read a quarter of the tensor (ky <= Py/2, kz <= Pz/2)
+        k.quarter = 1;
+        P->ten6.alloc((size_t)k.Kx * (Py / 2 + 1) * (Pz / 2 + 1) * 6 * rb);
+        CK(mlb::launch_tensor_pack6q(W.p, Px, Py, Pz, k.Kx, reinterpret_cast<float*>(P->ten6.p), st));
     } else {
         P->ten6.alloc((size_t)k.Kx * Py * Pz * 6 * rb);
         DBuf<double> mi;

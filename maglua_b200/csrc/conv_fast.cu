@@ -515,23 +515,43 @@ __global__ void __launch_bounds__(SPL_NT, 2) k_sy_fast(ConvK c, const float2* __
     }
 }
 
-template <int PZ>
+// Column of local line group c in z-pass CTA b: consecutive columns, or
+// with a quarter tensor (ConvK::quarter) mirrored pairs (i, Py - i) with
+// i = b COLS/2 + c/2, the self-mirrored columns 0 and Py/2 in CTA 0.
+template <int COLS>
+__device__ __forceinline__ int sz_column(int b, int c, int Py, bool quarter)
+{
+    if (!quarter) return b * COLS + c;
+    const int i = b * (COLS / 2) + (c >> 1);
+    if (i == 0) return (c & 1) ? Py / 2 : 0;
+    return (c & 1) ? Py - i : i;
+}
+
+template <int PZ, bool QT>
 __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __restrict__ twz,
                                                        float2* __restrict__ s2, const float* __restrict__ ten6)
 {
     using Z = SPZ<PZ>;
     constexpr int T = Z::T, E = Z::E, COLS = Z::COLS, EX = Z::EX;
+    constexpr int QZ = PZ / 2 + 1;
     extern __shared__ float2 sm[];
     float2* twl = sm;
     float2* buf = sm + PZ;
     const int nz = c.nz, Py = c.Py;
-    const int kx = blockIdx.x, ky0 = blockIdx.y * COLS;
-    const int ncol = min(COLS, Py - ky0);
-    const float* Tb = ten6 + ((size_t)kx * Py + ky0) * PZ * 6;
+    const int kx = blockIdx.x, b = blockIdx.y, ky0 = b * COLS;
+    const int ncol = QT ? COLS : min(COLS, Py - ky0);
     if (threadIdx.x == 0) {
         // the columns' tensor rows (constant across steps) start towards L2
         // while the z transforms run
-        const unsigned bytes = (unsigned)(ncol * PZ * 6 * sizeof(float));
+        const float* Tb;
+        unsigned bytes;
+        if (QT) {
+            Tb = ten6 + ((size_t)kx * (Py / 2 + 1) + b * (COLS / 2)) * QZ * 6;
+            bytes = (unsigned)((COLS / 2) * QZ * 6 * sizeof(float));
+        } else {
+            Tb = ten6 + ((size_t)kx * Py + ky0) * PZ * 6;
+            bytes = (unsigned)(ncol * PZ * 6 * sizeof(float));
+        }
         if ((((uintptr_t)Tb) & 15) == 0 && (bytes & 15) == 0)
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tb), "r"(bytes) : "memory");
     }
@@ -541,10 +561,11 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     if (c.run_if && *c.run_if == 0) return;
     const int lr = threadIdx.x / T, t = threadIdx.x % T;
     const int col = lr / 3, comp = lr - 3 * col;
-    const bool act = lr < 3 * COLS && ky0 + col < Py;   // whole T-lane groups share act
+    const bool act = lr < 3 * COLS && col < ncol;   // whole T-lane groups share act
     const unsigned mask = group_mask(T);
     float2* exl = buf + (size_t)lr * EX;
-    float2* colp = s2 + (((size_t)kx * Py + ky0 + col) * 3 + comp) * nz;
+    const int kyl = sz_column<COLS>(b, col, Py, QT);
+    float2* colp = s2 + (((size_t)kx * Py + kyl) * 3 + comp) * nz;
     __syncthreads();
     float2 v[E];
     if (act) {
@@ -560,17 +581,30 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     __syncthreads();
     // tensor multiply, point p = (column, kz): consecutive threads take
     // consecutive kz, so the tensor rows [kx][ky][kz][6] stream contiguously
+    // (a quarter tensor: rows ky <= Py/2, kz <= Pz/2, mirrored with the
+    // parity signs of XY, XZ, YZ)
     const float gg = c.g;
     for (int p = threadIdx.x; p < ncol * PZ; p += SPZ_NT) {
         const int cl = p / PZ, kz = p % PZ;
-        const float* Tp = Tb + (size_t)p * 6;
-        const float t0 = __ldg(Tp), t1 = __ldg(Tp + 1), t2 = __ldg(Tp + 2);
-        const float t3 = __ldg(Tp + 3), t4 = __ldg(Tp + 4), t5 = __ldg(Tp + 5);
-        float2* b = buf + (size_t)cl * 3 * EX + kz;
-        const float2 s0 = b[0], s1 = b[EX], s2v = b[2 * EX];
-        b[0] = make_float2(gg * (t0 * s0.x + t1 * s1.x + t2 * s2v.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2v.y));
-        b[EX] = make_float2(gg * (t1 * s0.x + t3 * s1.x + t4 * s2v.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2v.y));
-        b[2 * EX] =
+        const float* Tp;
+        float sy = 1.f, sz = 1.f;
+        if (QT) {
+            const int ky = sz_column<COLS>(b, cl, Py, true);
+            const int kyq = ky <= Py / 2 ? ky : Py - ky;
+            const int kzq = kz <= PZ / 2 ? kz : PZ - kz;
+            if (ky > Py / 2) sy = -1.f;
+            if (kz > PZ / 2) sz = -1.f;
+            Tp = ten6 + (((size_t)kx * (Py / 2 + 1) + kyq) * QZ + kzq) * 6;
+        } else {
+            Tp = ten6 + (((size_t)kx * Py + ky0) * PZ + p) * 6;
+        }
+        const float t0 = __ldg(Tp), t1 = sy * __ldg(Tp + 1), t2 = sz * __ldg(Tp + 2);
+        const float t3 = __ldg(Tp + 3), t4 = sy * sz * __ldg(Tp + 4), t5 = __ldg(Tp + 5);
+        float2* bb = buf + (size_t)cl * 3 * EX + kz;
+        const float2 s0 = bb[0], s1 = bb[EX], s2v = bb[2 * EX];
+        bb[0] = make_float2(gg * (t0 * s0.x + t1 * s1.x + t2 * s2v.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2v.y));
+        bb[EX] = make_float2(gg * (t1 * s0.x + t3 * s1.x + t4 * s2v.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2v.y));
+        bb[2 * EX] =
             make_float2(gg * (t2 * s0.x + t4 * s1.x + t5 * s2v.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2v.y));
     }
     __syncthreads();
@@ -650,8 +684,14 @@ static cudaError_t launch_split_t(const ConvK& c, const float2* twy, const float
     const dim3 gy(c.Kx, 3, (c.nz + Y::LN - 1) / Y::LN);
     cudaError_t e = mlb::launch_pdl(k_sy_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)spec, s2);
     if (e != cudaSuccess) return e;
-    e = mlb::launch_pdl(k_sz_fast<PZ>, dim3(c.Kx, (c.Py + Z::COLS - 1) / Z::COLS), dim3(SPZ_NT), Z::SMEM, st, c, twz,
-                        s2, ten6);
+    if (c.quarter && c.Py % Z::COLS == 0)
+        e = mlb::launch_pdl(k_sz_fast<PZ, true>, dim3(c.Kx, c.Py / Z::COLS), dim3(SPZ_NT), Z::SMEM, st, c, twz, s2,
+                            ten6);
+    else if (c.quarter)
+        e = cudaErrorInvalidValue;
+    else
+        e = mlb::launch_pdl(k_sz_fast<PZ, false>, dim3(c.Kx, (c.Py + Z::COLS - 1) / Z::COLS), dim3(SPZ_NT), Z::SMEM, st,
+                            c, twz, s2, ten6);
     if (e != cudaSuccess) return e;
     return mlb::launch_pdl(k_syi_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)s2, spec);
 }
@@ -704,7 +744,8 @@ static cudaError_t cfg_split()
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_sy_fast<P>, a, (int)SPY<P>::SMEM)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_syi_fast<P>, a, (int)SPY<P>::SMEM)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_sz_fast<P>, a, (int)SPZ<P>::SMEM);
+    if ((e = cudaFuncSetAttribute(k_sz_fast<P, true>, a, (int)SPZ<P>::SMEM)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_sz_fast<P, false>, a, (int)SPZ<P>::SMEM);
 }
 
 // ------------------------------------------------------------------ fused step

@@ -1416,6 +1416,71 @@ cudaError_t launch_lr2d(const ConvK& c, const FftLen L[3], const void* tw, const
     return cudaGetLastError();
 }
 
+// Largest |W|, and the largest deviations from the parities T(kx, -ky, kz)
+// = s_y(q) T(kx, ky, kz) and T(kx, ky, -kz) = s_z(q) T(kx, ky, kz) of the
+// real parts of the six transformed components (XY, YZ odd in ky; XZ, YZ
+// odd in kz), as the bits of non-negative doubles.
+__global__ void k_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int Kx, unsigned long long* out)
+{
+    const long long total = (long long)6 * Kx * Py * Pz;
+    unsigned long long m[3] = {0ull, 0ull, 0ull};
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(e % 6);
+        long long r = e / 6;
+        const int kx = (int)(r % Kx);
+        r /= Kx;
+        const int ky = (int)(r % Py), kz = (int)(r / Py);
+        const size_t plane = (size_t)Px * Py * Pz;
+        const double2* Wq = W + q * plane;
+        const double v = Wq[((size_t)kz * Py + ky) * Px + kx].x;
+        const double vy = Wq[((size_t)kz * Py + (Py - ky) % Py) * Px + kx].x;
+        const double vz = Wq[((size_t)((Pz - kz) % Pz) * Py + ky) * Px + kx].x;
+        const double sy = (q == 1 || q == 4) ? -1.0 : 1.0;
+        const double sz = (q == 2 || q == 4) ? -1.0 : 1.0;
+        // non-negative doubles order as their bit patterns
+        m[0] = max(m[0], (unsigned long long)__double_as_longlong(fabs(v)));
+        m[1] = max(m[1], (unsigned long long)__double_as_longlong(fabs(vy - sy * v)));
+        m[2] = max(m[2], (unsigned long long)__double_as_longlong(fabs(vz - sz * v)));
+    }
+    for (int k = 0; k < 3; k++) {
+        unsigned long long x = m[k];
+        for (int o = 16; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if ((threadIdx.x & 31) == 0 && x) atomicMax(out + k, x);
+    }
+}
+
+// Quarter tensor TEN6Q[kx][ky <= Py/2][kz <= Pz/2][q] = Re W_q in FP32.
+__global__ void k_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten)
+{
+    const int Qy = Py / 2 + 1, Qz = Pz / 2 + 1;
+    const long long total = (long long)Kx * Qy * Qz;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int kz = (int)(e % Qz);
+    const long long r = e / Qz;
+    const int ky = (int)(r % Qy), kx = (int)(r / Qy);
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)kz * Py + ky) * Px + kx;
+    for (int q = 0; q < 6; q++) ten[e * 6 + q] = (float)W[q * plane + off].x;
+}
+
+cudaError_t launch_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int Kx, unsigned long long* out3,
+                                   cudaStream_t st)
+{
+    const long long total = (long long)6 * Kx * Py * Pz;
+    const long long nb = std::min<long long>(blocks_for(total, 256), 148LL * 8);
+    k_tensor_symcheck<<<(unsigned)nb, 256, 0, st>>>(W, Px, Py, Pz, Kx, out3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, cudaStream_t st)
+{
+    const long long total = (long long)Kx * (Py / 2 + 1) * (Pz / 2 + 1);
+    k_tensor_pack6q<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
                                 int rb, int kmaj, cudaStream_t st)
 {

@@ -128,6 +128,12 @@ struct ConvK {
     // ky-major, TEN[kx][ky][kz][q].
     int split;
     void* spec2;
+    // Split FP32 passes of a tensor with the per-axis parities of a
+    // point-dipole tensor on an orthogonal lattice (XY and YZ odd in ky, XZ
+    // and YZ odd in kz, checked on the FP64 transform): the tensor is stored
+    // for ky <= Py/2 and kz <= Pz/2 only, TEN[kx][ky][kz][q], and each z-pass
+    // CTA takes mirrored ky columns together.
+    int quarter = 0;
 };
 
 // LongRange2D layer scales (spinoperationlongrange2d.cpp:430-530): the

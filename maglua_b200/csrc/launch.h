@@ -129,6 +129,12 @@ cudaError_t launch_lr2d_pack(const double2* W, int nx, int ny, int nz, int p0, i
                              cudaStream_t st);
 cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const FftLen L[3],
                            const double2* tw, int sign, cudaStream_t st);
+// Parity check of the FP64 transformed six-component tensor (out3: max |W|,
+// largest ky- and kz-parity deviations, as double bits; zero them first)
+// and the FP32 quarter tensor of the split passes (ConvK::quarter).
+cudaError_t launch_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int Kx, unsigned long long* out3,
+                                   cudaStream_t st);
+cudaError_t launch_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, cudaStream_t st);
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
                                 int rb, int kmaj, cudaStream_t st);
 cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb, int kmaj,

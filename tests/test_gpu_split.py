@@ -48,6 +48,26 @@ def test_split_fp32_open_direct_sum(M, dims):
     assert rel_err(h, O.dipole_direct(o, 0.4)) <= FIELD_TOL
 
 
+def test_split_fp32_sheared_cell(M):
+    # a sheared unit cell: the tensor lacks the per-axis parities, so the
+    # split z pass reads the full tensor (no quarter storage)
+    dims = (8, 64, 24)
+    n = int(np.prod(dims))
+    s = random_spins(n, 68, lengths=True)
+    abc = (1.0, 0.0, 0.0, 0.3, 1.0, 0.0, 0.1, 0.2, 1.1)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    dip = M.Dipole(ss)
+    dip.setStrength(0.4)
+    dip.setOpen(True, True, True)
+    dip.setUnitCell(abc[0:3], abc[3:6], abc[6:9])
+    dip.apply(ss)
+    h = np.stack(ss.fieldArrays("Dipole"))
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    assert rel_err(h, O.dipole_direct(o, 0.4, ABC=abc)) <= FIELD_TOL
+
+
 def test_split_fp32_reference_mode(M):
     # periodic in-plane lattice sum (truncated to keep the oracle's sum short),
     # open z padded to 160: plane 32 x 160
