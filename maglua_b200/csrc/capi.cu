@@ -245,6 +245,10 @@ struct mlb_system {
     int red_nb = 1;
     bool capturing = false;
     bool dry = false;               // replay host bookkeeping without launching
+    // a system the library owns and never shows to the caller (Runge-Kutta
+    // stages, the adaptive stepper's copies): when its spins are overwritten,
+    // the fields of the old spins are dropped instead of settled
+    bool internal = false;
     bool last_fused = false;
     mlb_surrogate* sur = nullptr;   // learned surrogate standing in for its operator (surrogate runs)
     // Inside do_step the inverse x pass of a fast-path convolution waits for
@@ -1669,7 +1673,17 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
         const int th = slot_find(dmdt, "Thermal");
         if (th >= 0) materialize(dmdt, th);
         // the destination's spins change in place: settle its lazy fields
-        materialize_all(to);
+        // (an internal system's old fields are never read: drop them)
+        if (to->internal) {
+            for (Slot& x : to->slots)
+                if (x.state == ST_LAZY || x.state == ST_SUM) {
+                    x.state = ST_ZERO;
+                    x.terms.clear();
+                    x.sum_list.clear();
+                }
+        } else {
+            materialize_all(to);
+        }
         if (to != dmdt) { materialize(dmdt, 0); if (th >= 0) materialize(dmdt, th); }
         if (from != to && !(cart && dt == 0.0) && to->ms_token != from->ms_token) {
             // the new spins carry the source's magnitudes (skipped when the
@@ -4011,6 +4025,7 @@ int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops
                 int rc = mlb_system_copy(c, ss, 1);
                 if (rc) fail(rc, g_err);
                 c->st = ss->st;
+                c->internal = true;
             }
         } catch (...) {
             for (mlb_system* c : r->k) free_system(c);
@@ -4130,6 +4145,7 @@ int mlb_adapt_create(mlb_system* ss, mlb_rk* step, double tolerance, mlb_llg* l,
                 fail(rc, g_err);
             }
             (*c)->st = ss->st;
+            (*c)->internal = true;
         }
         *out = a.release();
     });
