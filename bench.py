@@ -514,7 +514,24 @@ def main():
     ap.add_argument("--ncu-cube", type=int, default=0,
                     help="profiling driver: this many eager FP32 steps of the open cube (edge --cube-edge) and exit")
     ap.add_argument("--cube-edge", type=int, default=256, help="edge of the cube for --ncu-cube")
+    ap.add_argument("--ncu-lr2d", type=int, default=0,
+                    help="profiling driver: this many Dipole2D evaluations on the 256x256x8 film and exit")
+    ap.add_argument("--ncu-ewald", type=int, default=0,
+                    help="profiling driver: the Ewald tensor of an edge^3 simple-cubic lattice (NSites 10) and exit")
     args = ap.parse_args()
+    if args.ncu_lr2d or args.ncu_ewald:
+        import maglua_b200 as M
+        M.init(int(os.environ.get("LOCAL_RANK", "0")))
+        if args.ncu_lr2d:
+            ss, _, _ = build_system(M, 0)
+            dip = M.Dipole2D(ss)
+            dip.setTruncation(25, 8, 8, 8)
+            for _ in range(args.ncu_lr2d):
+                dip.apply(ss)
+            ss.synchronize()
+        else:
+            M.DipoleEwald3D(args.ncu_ewald, args.ncu_ewald, args.ncu_ewald).tensorArrays()
+        return
     if args.ncu_cube:
         import maglua_b200 as M
         M.init(int(os.environ.get("LOCAL_RANK", "0")))
