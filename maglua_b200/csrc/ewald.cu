@@ -282,6 +282,7 @@ int mlb_ewald3d_destroy(mlb_ewald3d* e)
 int mlb_ewald3d_set_unit_cell(mlb_ewald3d* e, const double a[3], const double b[3], const double c[3])
 {
     return ew_guard([&] {
+        if (!e || !a || !b || !c) throw EwErr{MLB_EINVAL, "null argument"};
         const double* v[3] = {a, b, c};
         for (int i = 0; i < 3; i++)
             for (int k = 0; k < 3; k++) e->a[i][k] = v[i][k];
@@ -291,6 +292,7 @@ int mlb_ewald3d_set_unit_cell(mlb_ewald3d* e, const double a[3], const double b[
 
 int mlb_ewald3d_get_unit_cell(const mlb_ewald3d* e, double abc[9])
 {
+    if (!e || !abc) return MLB_EINVAL;
     for (int i = 0; i < 3; i++)
         for (int k = 0; k < 3; k++) abc[3 * i + k] = e->a[i][k];
     return MLB_OK;
@@ -299,6 +301,7 @@ int mlb_ewald3d_get_unit_cell(const mlb_ewald3d* e, double abc[9])
 int mlb_ewald3d_set_lattice_size(mlb_ewald3d* e, int nx, int ny, int nz)
 {
     return ew_guard([&] {
+        if (!e) throw EwErr{MLB_EINVAL, "null argument"};
         e->d[0] = nx > 0 ? nx : 1;
         e->d[1] = ny > 0 ? ny : 1;
         e->d[2] = nz > 0 ? nz : 1;
@@ -308,42 +311,49 @@ int mlb_ewald3d_set_lattice_size(mlb_ewald3d* e, int nx, int ny, int nz)
 
 int mlb_ewald3d_get_lattice_size(const mlb_ewald3d* e, int n3[3])
 {
+    if (!e || !n3) return MLB_EINVAL;
     for (int i = 0; i < 3; i++) n3[i] = e->d[i];
     return MLB_OK;
 }
 
 int mlb_ewald3d_set_tau(mlb_ewald3d* e, double tau)
 {
+    if (!e) return MLB_EINVAL;
     if (tau > 0) { e->tau = tau; e->good_eta = false; }
     return MLB_OK;
 }
 
 int mlb_ewald3d_get_tau(const mlb_ewald3d* e, double* tau)
 {
+    if (!e || !tau) return MLB_EINVAL;
     *tau = e->tau;
     return MLB_OK;
 }
 
 int mlb_ewald3d_set_nsites(mlb_ewald3d* e, int n)
 {
+    if (!e) return MLB_EINVAL;
     if (n > 1) { e->nsites = n; e->good_eta = false; }
     return MLB_OK;
 }
 
 int mlb_ewald3d_get_nsites(const mlb_ewald3d* e, int* n)
 {
+    if (!e || !n) return MLB_EINVAL;
     *n = e->nsites;
     return MLB_OK;
 }
 
 int mlb_ewald3d_get_eta(const mlb_ewald3d* e, double* eta)
 {
+    if (!e || !eta) return MLB_EINVAL;
     *eta = e->eta;
     return MLB_OK;
 }
 
 int mlb_ewald3d_get_volume(const mlb_ewald3d* e, double* v)
 {
+    if (!e || !v) return MLB_EINVAL;
     *v = e->g.vu;
     return MLB_OK;
 }
@@ -351,6 +361,7 @@ int mlb_ewald3d_get_volume(const mlb_ewald3d* e, double* v)
 int mlb_ewald3d_element(mlb_ewald3d* e, int ab, const int r3[3], double* out)
 {
     return ew_guard([&] {
+        if (!e || !r3 || !out) throw EwErr{MLB_EINVAL, "null argument"};
         ew_check_ab(ab);
         ew_need_eta(e);
         double r[3];
@@ -362,6 +373,7 @@ int mlb_ewald3d_element(mlb_ewald3d* e, int ab, const int r3[3], double* out)
 int mlb_ewald3d_element_real(mlb_ewald3d* e, int ab, const double r[3], double* out)
 {
     return ew_guard([&] {
+        if (!e || !r || !out) throw EwErr{MLB_EINVAL, "null argument"};
         ew_check_ab(ab);
         ew_need_eta(e);
         *out = ew_element(e->g, ab / 3, ab % 3, r, e->eta, e->nsites);
@@ -371,7 +383,7 @@ int mlb_ewald3d_element_real(mlb_ewald3d* e, int ab, const double r[3], double* 
 int mlb_ewald3d_tensor(mlb_ewald3d* e, double* out9)
 {
     return ew_guard([&] {
-        if (!out9) throw EwErr{MLB_EINVAL, "null argument"};
+        if (!e || !out9) throw EwErr{MLB_EINVAL, "null argument"};
         ew_need_eta(e);
         const long long n = (long long)e->d[0] * e->d[1] * e->d[2];
         double* dev = nullptr;
