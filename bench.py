@@ -66,9 +66,9 @@ def nn_paths(nx, ny, nz, pbc=(1, 1, 0)):
     return f, t, np.full(len(f), J)
 
 
-def build_system(M, seed):
+def build_system(M, seed, precision="f32"):
     n = NX * NY * NZ
-    ss = M.SpinSystem(NX, NY, NZ)
+    ss = M.SpinSystem(NX, NY, NZ, precision=precision)
     ss.setSpinArrays(*tilted_spins(n, seed))
     ss.setAlpha(ALPHA)
     ss.setTimeStep(DT)
@@ -213,6 +213,29 @@ def run_rk(M, torch, steps=20):
     return {"workload": WORKLOAD.replace("LLG.Quaternion", "RK4 (LLG.Quaternion stages) + thermal kick"),
             "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "how": "mlb_rk_step: eager launches (no graph capture), L2 not flushed"}
+
+
+# ----------------------------------------------------------------- FP64 film
+def run_fp64_film(M, torch, steps=20):
+    """The headline workload with FP64 state (every term, the convolution
+    and the LLG update in double, as the reference computes): captured steps,
+    no flush."""
+    ss, ops, llg = build_system(M, 0, precision="f64")
+    M.run(ss, ops, llg, 3)
+    plan = M.Plan(ss, ops, llg)
+    plan.launch(2)
+    st = torch.cuda.ExternalStream(ss.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ss.synchronize()
+    a.record(st)
+    plan.launch(steps)
+    b.record(st)
+    ss.synchronize()
+    ms = a.elapsed_time(b) / steps
+    n = NX * NY * NZ
+    return {"workload": WORKLOAD + " in FP64", "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "how": "one captured step per graph launch, back to back, CUDA events; FP64 register split (y,z) "
+                   "passes, generic FP64 x passes and fused step"}
 
 
 # ----------------------------------------------------------------- LongRange2D / Dipole2D
@@ -710,6 +733,7 @@ def main():
     cube = run_cube(M, torch) if not args.no_cube else None
     rk = run_rk(M, torch)
     lr2d = run_lr2d(M, torch)
+    fp64 = run_fp64_film(M, torch)
     ewald = run_ewald(M)
 
     if rank != 0:
@@ -768,6 +792,7 @@ def main():
         "surrogate": surrogate,
         "cube_256": cube,
         "rk4": rk,
+        "fp64_film": fp64,
         "dipole2d": lr2d,
         "ewald3d": ewald,
     }

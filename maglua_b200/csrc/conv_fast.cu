@@ -28,11 +28,15 @@ namespace mlb {
 cudaError_t fftreg_init()
 {
     float2 h[64];
+    double2 hd[64];
     for (int k = 0; k < 64; k++) {
         const double a = 2.0 * M_PI * k / 64.0;
         h[k] = make_float2((float)cos(a), (float)(-sin(a)));
+        hd[k] = make_double2(cos(a), -sin(a));
     }
-    return cudaMemcpyToSymbol(fr::c_w64, h, sizeof(h));
+    cudaError_t e = cudaMemcpyToSymbol(fr::c_w64, h, sizeof(h));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(fr::c_w64d, hd, sizeof(hd));
 }
 
 } // namespace mlb
@@ -443,23 +447,23 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
 constexpr int SPL_NT = 256;   // threads of the y passes
 constexpr int SPZ_NT = 192;   // threads of the z pass (a multiple of 3 lines)
 
-template <int PY>
+template <int PY, typename C = float2>
 struct SPY {
     static constexpr int T = fr::Split<PY>::T, E = fr::Split<PY>::E;
     static constexpr int LN = SPL_NT / T;     // data layers per CTA
     static constexpr int EX = E * (T + 1);    // exchange elements per line
     static constexpr int TS = LN + 1;         // transpose row stride, [ky][layer]
     static constexpr int BUF = LN * EX > PY * TS ? LN * EX : PY * TS;
-    static constexpr size_t SMEM = (size_t)(PY + BUF) * sizeof(float2);
+    static constexpr size_t SMEM = (size_t)(PY + BUF) * sizeof(C);
 };
 
-template <int PZ>
+template <int PZ, typename C = float2>
 struct SPZ {
     static constexpr int T = fr::Split<PZ>::T, E = fr::Split<PZ>::E;
     static constexpr int LN = SPZ_NT / T;     // lines per CTA
     static constexpr int COLS = LN / 3;       // ky columns per CTA
     static constexpr int EX = E * (T + 1);    // >= PZ: exchange, then spectrum
-    static constexpr size_t SMEM = (size_t)(PZ + LN * EX) * sizeof(float2);
+    static constexpr size_t SMEM = (size_t)(PZ + LN * EX) * sizeof(C);
 };
 
 // lanes of this thread's T-lane group within its warp
@@ -468,15 +472,20 @@ __device__ __forceinline__ unsigned group_mask(int T)
     return T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << (((threadIdx.x & 31) / T) * T));
 }
 
-template <int PY>
-__global__ void __launch_bounds__(SPL_NT, 2) k_sy_fast(ConvK c, const float2* __restrict__ twy,
-                                                       const float2* __restrict__ spec, float2* __restrict__ s2)
+// FP32 lines fit two CTAs per SM; FP64 lines hold twice the registers
+template <typename C> struct SplitOcc { static constexpr int Y = 2, YI = 3, Z = 3; };
+template <> struct SplitOcc<double2> { static constexpr int Y = 1, YI = 1, Z = 2; };
+
+template <int PY, typename C = float2>
+__global__ void __launch_bounds__(SPL_NT, SplitOcc<C>::Y) k_sy_fast(ConvK c, const C* __restrict__ twy,
+                                                                   const C* __restrict__ spec, C* __restrict__ s2)
 {
-    using Y = SPY<PY>;
+    using Y = SPY<PY, C>;
     constexpr int T = Y::T, E = Y::E, LN = Y::LN;
-    extern __shared__ float2 sm[];
-    float2* twl = sm;
-    float2* buf = sm + PY;
+    extern __shared__ __align__(16) unsigned char smraw_sy[];
+    C* sm = reinterpret_cast<C*>(smraw_sy);
+    C* twl = sm;
+    C* buf = sm + PY;
     for (int k = threadIdx.x; k < PY; k += SPL_NT) twl[k] = twy[k];
     pdl_trigger();
     pdl_wait();
@@ -487,15 +496,15 @@ __global__ void __launch_bounds__(SPL_NT, 2) k_sy_fast(ConvK c, const float2* __
     const int nl = min(LN, nz - z0);
     const bool act = lr < nl;   // whole T-lane groups share act
     __syncthreads();
-    float2 v[E];
+    C v[E];
     if (act) {
-        const float2* src = spec + (((size_t)kx * 3 + comp) * nz + z0 + lr) * ny;
+        const C* src = spec + (((size_t)kx * 3 + comp) * nz + z0 + lr) * ny;
 #pragma unroll
         for (int j = 0; j < E; j++) {
             const int y = t + T * j;
-            v[j] = y < ny ? src[y] : make_float2(0.f, 0.f);
+            v[j] = y < ny ? src[y] : cmk<C>(0, 0);
         }
-        fr::line_fft<PY, -1, float2>(v, buf + (size_t)lr * Y::EX, t, group_mask(T), twl);
+        fr::line_fft<PY, -1, C>(v, buf + (size_t)lr * Y::EX, t, group_mask(T), twl);
     }
     __syncthreads();   // exchange buffers -> transpose buffer
     if (act) {
@@ -505,7 +514,7 @@ __global__ void __launch_bounds__(SPL_NT, 2) k_sy_fast(ConvK c, const float2* __
     __syncthreads();
     // S2[kx][ky][comp][z0 + l]: LN consecutive threads store one ky's layers
     const int l = threadIdx.x % LN, kq = threadIdx.x / LN;
-    float2* dst = s2 + ((size_t)kx * PY * 3 + comp) * nz + z0 + l;
+    C* dst = s2 + ((size_t)kx * PY * 3 + comp) * nz + z0 + l;
     if (l < nl) {
 #pragma unroll 4
         for (int k = 0; k < PY / T; k++) {
@@ -527,30 +536,33 @@ __device__ __forceinline__ int sz_column(int b, int c, int Py, bool quarter)
     return (c & 1) ? Py - i : i;
 }
 
-template <int PZ, bool QT>
-__global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __restrict__ twz,
-                                                       float2* __restrict__ s2, const float* __restrict__ ten6)
+template <int PZ, bool QT, typename C = float2>
+__global__ void __launch_bounds__(SPZ_NT, SplitOcc<C>::Z) k_sz_fast(ConvK c, const C* __restrict__ twz,
+                                                                   C* __restrict__ s2,
+                                                                   const decltype(C().x)* __restrict__ ten6)
 {
-    using Z = SPZ<PZ>;
+    typedef decltype(C().x) R;
+    using Z = SPZ<PZ, C>;
     constexpr int T = Z::T, E = Z::E, COLS = Z::COLS, EX = Z::EX;
     constexpr int QZ = PZ / 2 + 1;
-    extern __shared__ float2 sm[];
-    float2* twl = sm;
-    float2* buf = sm + PZ;
+    extern __shared__ __align__(16) unsigned char smraw_sz[];
+    C* sm = reinterpret_cast<C*>(smraw_sz);
+    C* twl = sm;
+    C* buf = sm + PZ;
     const int nz = c.nz, Py = c.Py;
     const int kx = blockIdx.x, b = blockIdx.y, ky0 = b * COLS;
     const int ncol = QT ? COLS : min(COLS, Py - ky0);
     if (threadIdx.x == 0) {
         // the columns' tensor rows (constant across steps) start towards L2
         // while the z transforms run
-        const float* Tb;
+        const R* Tb;
         unsigned bytes;
         if (QT) {
             Tb = ten6 + ((size_t)kx * (Py / 2 + 1) + b * (COLS / 2)) * QZ * 6;
-            bytes = (unsigned)((COLS / 2) * QZ * 6 * sizeof(float));
+            bytes = (unsigned)((COLS / 2) * QZ * 6 * sizeof(R));
         } else {
             Tb = ten6 + ((size_t)kx * Py + ky0) * PZ * 6;
-            bytes = (unsigned)(ncol * PZ * 6 * sizeof(float));
+            bytes = (unsigned)(ncol * PZ * 6 * sizeof(R));
         }
         if ((((uintptr_t)Tb) & 15) == 0 && (bytes & 15) == 0)
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tb), "r"(bytes) : "memory");
@@ -563,18 +575,18 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     const int col = lr / 3, comp = lr - 3 * col;
     const bool act = lr < 3 * COLS && col < ncol;   // whole T-lane groups share act
     const unsigned mask = group_mask(T);
-    float2* exl = buf + (size_t)lr * EX;
+    C* exl = buf + (size_t)lr * EX;
     const int kyl = sz_column<COLS>(b, col, Py, QT);
-    float2* colp = s2 + (((size_t)kx * Py + kyl) * 3 + comp) * nz;
+    C* colp = s2 + (((size_t)kx * Py + kyl) * 3 + comp) * nz;
     __syncthreads();
-    float2 v[E];
+    C v[E];
     if (act) {
 #pragma unroll
         for (int j = 0; j < E; j++) {
             const int z = t + T * j;
-            v[j] = z < nz ? colp[z] : make_float2(0.f, 0.f);
+            v[j] = z < nz ? colp[z] : cmk<C>(0, 0);
         }
-        fr::line_fft<PZ, -1, float2>(v, exl, t, mask, twl);
+        fr::line_fft<PZ, -1, C>(v, exl, t, mask, twl);
 #pragma unroll
         for (int r = 0; r < E; r++) exl[fr::out_index<PZ>(t, r)] = v[r];
     }
@@ -583,36 +595,35 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     // consecutive kz, so the tensor rows [kx][ky][kz][6] stream contiguously
     // (a quarter tensor: rows ky <= Py/2, kz <= Pz/2, mirrored with the
     // parity signs of XY, XZ, YZ)
-    const float gg = c.g;
+    const R gg = (R)c.g;
     for (int p = threadIdx.x; p < ncol * PZ; p += SPZ_NT) {
         const int cl = p / PZ, kz = p % PZ;
-        const float* Tp;
-        float sy = 1.f, sz = 1.f;
+        const R* Tp;
+        R sy = 1, sz = 1;
         if (QT) {
             const int ky = sz_column<COLS>(b, cl, Py, true);
             const int kyq = ky <= Py / 2 ? ky : Py - ky;
             const int kzq = kz <= PZ / 2 ? kz : PZ - kz;
-            if (ky > Py / 2) sy = -1.f;
-            if (kz > PZ / 2) sz = -1.f;
+            if (ky > Py / 2) sy = -1;
+            if (kz > PZ / 2) sz = -1;
             Tp = ten6 + (((size_t)kx * (Py / 2 + 1) + kyq) * QZ + kzq) * 6;
         } else {
             Tp = ten6 + (((size_t)kx * Py + ky0) * PZ + p) * 6;
         }
-        const float t0 = __ldg(Tp), t1 = sy * __ldg(Tp + 1), t2 = sz * __ldg(Tp + 2);
-        const float t3 = __ldg(Tp + 3), t4 = sy * sz * __ldg(Tp + 4), t5 = __ldg(Tp + 5);
-        float2* bb = buf + (size_t)cl * 3 * EX + kz;
-        const float2 s0 = bb[0], s1 = bb[EX], s2v = bb[2 * EX];
-        bb[0] = make_float2(gg * (t0 * s0.x + t1 * s1.x + t2 * s2v.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2v.y));
-        bb[EX] = make_float2(gg * (t1 * s0.x + t3 * s1.x + t4 * s2v.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2v.y));
-        bb[2 * EX] =
-            make_float2(gg * (t2 * s0.x + t4 * s1.x + t5 * s2v.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2v.y));
+        const R t0 = __ldg(Tp), t1 = sy * __ldg(Tp + 1), t2 = sz * __ldg(Tp + 2);
+        const R t3 = __ldg(Tp + 3), t4 = sy * sz * __ldg(Tp + 4), t5 = __ldg(Tp + 5);
+        C* bb = buf + (size_t)cl * 3 * EX + kz;
+        const C s0 = bb[0], s1 = bb[EX], s2v = bb[2 * EX];
+        bb[0] = cmk<C>(gg * (t0 * s0.x + t1 * s1.x + t2 * s2v.x), gg * (t0 * s0.y + t1 * s1.y + t2 * s2v.y));
+        bb[EX] = cmk<C>(gg * (t1 * s0.x + t3 * s1.x + t4 * s2v.x), gg * (t1 * s0.y + t3 * s1.y + t4 * s2v.y));
+        bb[2 * EX] = cmk<C>(gg * (t2 * s0.x + t4 * s1.x + t5 * s2v.x), gg * (t2 * s0.y + t4 * s1.y + t5 * s2v.y));
     }
     __syncthreads();
     if (act) {
 #pragma unroll
         for (int j = 0; j < E; j++) v[j] = exl[t + T * j];
         __syncwarp(mask);   // every lane has read the spectrum before the exchange overwrites it
-        fr::line_fft<PZ, +1, float2>(v, exl, t, mask, twl);
+        fr::line_fft<PZ, +1, C>(v, exl, t, mask, twl);
 #pragma unroll
         for (int r = 0; r < E; r++) {
             const int z = fr::out_index<PZ>(t, r);
@@ -621,15 +632,16 @@ __global__ void __launch_bounds__(SPZ_NT, 3) k_sz_fast(ConvK c, const float2* __
     }
 }
 
-template <int PY>
-__global__ void __launch_bounds__(SPL_NT, 3) k_syi_fast(ConvK c, const float2* __restrict__ twy,
-                                                        const float2* __restrict__ s2, float2* __restrict__ spec)
+template <int PY, typename C = float2>
+__global__ void __launch_bounds__(SPL_NT, SplitOcc<C>::YI) k_syi_fast(ConvK c, const C* __restrict__ twy,
+                                                                     const C* __restrict__ s2, C* __restrict__ spec)
 {
-    using Y = SPY<PY>;
+    using Y = SPY<PY, C>;
     constexpr int T = Y::T, E = Y::E, LN = Y::LN;
-    extern __shared__ float2 sm[];
-    float2* twl = sm;
-    float2* buf = sm + PY;
+    extern __shared__ __align__(16) unsigned char smraw_syi[];
+    C* sm = reinterpret_cast<C*>(smraw_syi);
+    C* twl = sm;
+    C* buf = sm + PY;
     for (int k = threadIdx.x; k < PY; k += SPL_NT) twl[k] = twy[k];
     pdl_trigger();
     pdl_wait();
@@ -639,7 +651,7 @@ __global__ void __launch_bounds__(SPL_NT, 3) k_syi_fast(ConvK c, const float2* _
     const int nl = min(LN, nz - z0);
     {
         const int l = threadIdx.x % LN, kq = threadIdx.x / LN;
-        const float2* src = s2 + ((size_t)kx * PY * 3 + comp) * nz + z0 + l;
+        const C* src = s2 + ((size_t)kx * PY * 3 + comp) * nz + z0 + l;
         if (l < nl) {
 #pragma unroll 4
             for (int k = 0; k < PY / T; k++) {
@@ -651,15 +663,15 @@ __global__ void __launch_bounds__(SPL_NT, 3) k_syi_fast(ConvK c, const float2* _
     __syncthreads();
     const int lr = threadIdx.x / T, t = threadIdx.x % T;
     const bool act = lr < nl;
-    float2 v[E];
+    C v[E];
     if (act) {
 #pragma unroll
         for (int j = 0; j < E; j++) v[j] = buf[(t + T * j) * Y::TS + lr];
     }
     __syncthreads();   // transpose buffer -> exchange buffers
     if (act) {
-        fr::line_fft<PY, +1, float2>(v, buf + (size_t)lr * Y::EX, t, group_mask(T), twl);
-        float2* dst = spec + (((size_t)kx * 3 + comp) * nz + z0 + lr) * ny;
+        fr::line_fft<PY, +1, C>(v, buf + (size_t)lr * Y::EX, t, group_mask(T), twl);
+        C* dst = spec + (((size_t)kx * 3 + comp) * nz + z0 + lr) * ny;
 #pragma unroll
         for (int r = 0; r < E; r++) {
             const int y = fr::out_index<PY>(t, r);
@@ -668,57 +680,67 @@ __global__ void __launch_bounds__(SPL_NT, 3) k_syi_fast(ConvK c, const float2* _
     }
 }
 
-static bool split_fast_ok(const ConvK& c)
+// Sizes the register split passes take: power-of-two Py 32..512 and Pz
+// 8..512, Py a multiple of the z pass's columns per CTA.
+template <typename C>
+static bool split_fast_ok_t(const ConvK& c)
 {
-    auto p2 = [](int v) { return v >= 32 && v <= 512 && (v & (v - 1)) == 0; };
-    return c.nrep == 1 && p2(c.Py) && p2(c.Pz);
+    auto p2 = [](int v, int lo) { return v >= lo && v <= 512 && (v & (v - 1)) == 0; };
+    if (c.nrep != 1 || !p2(c.Py, 32) || !p2(c.Pz, 8)) return false;
+    const int T = c.Pz <= 4 ? 1 : (c.Pz <= 32 ? (c.Pz <= 8 ? 2 : 4) : (c.Pz <= 128 ? 8 : 16));
+    const int COLS = (SPZ_NT / T) / 3;
+    return c.Py % COLS == 0;
 }
+static bool split_fast_ok(const ConvK& c) { return split_fast_ok_t<float2>(c); }
 
-template <int PY, int PZ>
-static cudaError_t launch_split_t(const ConvK& c, const float2* twy, const float2* twz, float2* spec,
-                                  const float* ten6, cudaStream_t st)
+template <int PY, int PZ, typename C>
+static cudaError_t launch_split_t(const ConvK& c, const C* twy, const C* twz, C* spec, const decltype(C().x)* ten6,
+                                  cudaStream_t st)
 {
-    using Y = SPY<PY>;
-    using Z = SPZ<PZ>;
-    float2* s2 = static_cast<float2*>(c.spec2);
+    using Y = SPY<PY, C>;
+    using Z = SPZ<PZ, C>;
+    C* s2 = static_cast<C*>(c.spec2);
     const dim3 gy(c.Kx, 3, (c.nz + Y::LN - 1) / Y::LN);
-    cudaError_t e = mlb::launch_pdl(k_sy_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)spec, s2);
+    cudaError_t e = mlb::launch_pdl(k_sy_fast<PY, C>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const C*)spec, s2);
     if (e != cudaSuccess) return e;
     if (c.quarter && c.Py % Z::COLS == 0)
-        e = mlb::launch_pdl(k_sz_fast<PZ, true>, dim3(c.Kx, c.Py / Z::COLS), dim3(SPZ_NT), Z::SMEM, st, c, twz, s2,
+        e = mlb::launch_pdl(k_sz_fast<PZ, true, C>, dim3(c.Kx, c.Py / Z::COLS), dim3(SPZ_NT), Z::SMEM, st, c, twz, s2,
                             ten6);
     else if (c.quarter)
         e = cudaErrorInvalidValue;
     else
-        e = mlb::launch_pdl(k_sz_fast<PZ, false>, dim3(c.Kx, (c.Py + Z::COLS - 1) / Z::COLS), dim3(SPZ_NT), Z::SMEM, st,
-                            c, twz, s2, ten6);
+        e = mlb::launch_pdl(k_sz_fast<PZ, false, C>, dim3(c.Kx, (c.Py + Z::COLS - 1) / Z::COLS), dim3(SPZ_NT), Z::SMEM,
+                            st, c, twz, s2, ten6);
     if (e != cudaSuccess) return e;
-    return mlb::launch_pdl(k_syi_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)s2, spec);
+    return mlb::launch_pdl(k_syi_fast<PY, C>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const C*)s2, spec);
 }
 
-template <int PY>
-static cudaError_t launch_split_py(const ConvK& c, const float2* twy, const float2* twz, float2* spec,
-                                   const float* ten6, cudaStream_t st)
+template <int PY, typename C>
+static cudaError_t launch_split_py(const ConvK& c, const C* twy, const C* twz, C* spec, const decltype(C().x)* ten6,
+                                   cudaStream_t st)
 {
     switch (c.Pz) {
-    case 32: return launch_split_t<PY, 32>(c, twy, twz, spec, ten6, st);
-    case 64: return launch_split_t<PY, 64>(c, twy, twz, spec, ten6, st);
-    case 128: return launch_split_t<PY, 128>(c, twy, twz, spec, ten6, st);
-    case 256: return launch_split_t<PY, 256>(c, twy, twz, spec, ten6, st);
-    case 512: return launch_split_t<PY, 512>(c, twy, twz, spec, ten6, st);
+    case 8: return launch_split_t<PY, 8, C>(c, twy, twz, spec, ten6, st);
+    case 16: return launch_split_t<PY, 16, C>(c, twy, twz, spec, ten6, st);
+    case 32: return launch_split_t<PY, 32, C>(c, twy, twz, spec, ten6, st);
+    case 64: return launch_split_t<PY, 64, C>(c, twy, twz, spec, ten6, st);
+    case 128: return launch_split_t<PY, 128, C>(c, twy, twz, spec, ten6, st);
+    case 256: return launch_split_t<PY, 256, C>(c, twy, twz, spec, ten6, st);
+    case 512: return launch_split_t<PY, 512, C>(c, twy, twz, spec, ten6, st);
     }
     return cudaErrorInvalidValue;
 }
 
-static cudaError_t launch_split_fast(const ConvK& c, const float2* twy, const float2* twz, float2* spec,
-                                     const float* ten6, cudaStream_t st)
+template <typename C>
+static cudaError_t launch_split_fast(const ConvK& c, const C* twy, const C* twz, C* spec, const decltype(C().x)* ten6,
+                                     cudaStream_t st)
 {
     switch (c.Py) {
-    case 32: return launch_split_py<32>(c, twy, twz, spec, ten6, st);
-    case 64: return launch_split_py<64>(c, twy, twz, spec, ten6, st);
-    case 128: return launch_split_py<128>(c, twy, twz, spec, ten6, st);
-    case 256: return launch_split_py<256>(c, twy, twz, spec, ten6, st);
-    case 512: return launch_split_py<512>(c, twy, twz, spec, ten6, st);
+    case 32: return launch_split_py<32, C>(c, twy, twz, spec, ten6, st);
+    case 64: return launch_split_py<64, C>(c, twy, twz, spec, ten6, st);
+    case 128: return launch_split_py<128, C>(c, twy, twz, spec, ten6, st);
+    case 256: return launch_split_py<256, C>(c, twy, twz, spec, ten6, st);
+    case 512: return launch_split_py<512, C>(c, twy, twz, spec, ten6, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -733,19 +755,30 @@ static cudaError_t launch_split_y_t(const ConvK& c, const float2* twy, float2* s
     using Y = SPY<PY>;
     float2* s2 = static_cast<float2*>(c.spec2);
     const dim3 gy(c.Kx, 3, (c.nz + Y::LN - 1) / Y::LN);
-    if (fwd) return mlb::launch_pdl(k_sy_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)spec, s2);
-    return mlb::launch_pdl(k_syi_fast<PY>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)s2, spec);
+    if (fwd)
+        return mlb::launch_pdl(k_sy_fast<PY, float2>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)spec, s2);
+    return mlb::launch_pdl(k_syi_fast<PY, float2>, gy, dim3(SPL_NT), Y::SMEM, st, c, twy, (const float2*)s2, spec);
+}
+
+template <int P, typename C>
+static cudaError_t cfg_split_c()
+{
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e;
+    if constexpr (P >= 32) {
+        if ((e = cudaFuncSetAttribute(k_sy_fast<P, C>, a, (int)SPY<P, C>::SMEM)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k_syi_fast<P, C>, a, (int)SPY<P, C>::SMEM)) != cudaSuccess) return e;
+    }
+    if ((e = cudaFuncSetAttribute(k_sz_fast<P, true, C>, a, (int)SPZ<P, C>::SMEM)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_sz_fast<P, false, C>, a, (int)SPZ<P, C>::SMEM);
 }
 
 template <int P>
 static cudaError_t cfg_split()
 {
-    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_sy_fast<P>, a, (int)SPY<P>::SMEM)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_syi_fast<P>, a, (int)SPY<P>::SMEM)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_sz_fast<P, true>, a, (int)SPZ<P>::SMEM)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_sz_fast<P, false>, a, (int)SPZ<P>::SMEM);
+    cudaError_t e = cfg_split_c<P, float2>();
+    if (e != cudaSuccess) return e;
+    return cfg_split_c<P, double2>();
 }
 
 // ------------------------------------------------------------------ fused step
@@ -1005,6 +1038,17 @@ bool conv_fast_ok(const ConvK& c)
 static cudaError_t launch_yz_any(const ConvK& c, const float2* twy, float2* spec, const float* ten6,
                                  cudaStream_t st);
 
+// The register split passes for FP64 state (generic x passes around them):
+// real (6-component) tensors only.
+bool split_fast_ok_f64(const ConvK& c) { return !c.general && split_fast_ok_t<double2>(c); }
+
+cudaError_t launch_split_fast_f64(const ConvK& c, const FftLen L[3], const double2* tw, double2* spec,
+                                  const double* ten6, cudaStream_t st)
+{
+    Prof pf("k_conv_yz_split", st);
+    return launch_split_fast<double2>(c, tw + L[1].tw_off, tw + L[2].tw_off, spec, ten6, st);
+}
+
 bool split_y_fast_ok(const ConvK& c)
 {
     return c.nrep == 1 && c.Py >= 32 && c.Py <= 512 && (c.Py & (c.Py - 1)) == 0;
@@ -1033,7 +1077,7 @@ static cudaError_t yz_pass(const ConvK& c, const FftLen L[3], const float2* tw, 
     if (c.split) {
         if (!split_fast_ok(c)) return launch_conv_split_yz(c, L[1], L[2], tw, spec, ten6, nullptr, 4, st);
         Prof pf("k_conv_yz_split", st);
-        return launch_split_fast(c, tw + L[1].tw_off, tw + L[2].tw_off, spec, ten6, st);
+        return launch_split_fast<float2>(c, tw + L[1].tw_off, tw + L[2].tw_off, spec, ten6, st);
     }
     Prof pf("k_conv_yz", st);
     return launch_yz_any(c, tw + L[1].tw_off, spec, ten6, st);
@@ -1167,8 +1211,8 @@ cudaError_t conv_fast_configure()
         return e;
     if ((e = cfg_yzr<64, 128>()) || (e = cfg_yzr<128, 128>()) || (e = cfg_yzr<256, 384>()) || (e = cfg_yzr<512, 384>()))
         return e;
-    if ((e = cfg_split<32>()) || (e = cfg_split<64>()) || (e = cfg_split<128>()) || (e = cfg_split<256>()) ||
-        (e = cfg_split<512>()))
+    if ((e = cfg_split<8>()) || (e = cfg_split<16>()) || (e = cfg_split<32>()) || (e = cfg_split<64>()) ||
+        (e = cfg_split<128>()) || (e = cfg_split<256>()) || (e = cfg_split<512>()))
         return e;
     return cudaSuccess;
 }

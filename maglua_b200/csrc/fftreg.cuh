@@ -15,6 +15,7 @@ namespace fr {
 // w_64^k = exp(-2 pi i k / 64); one copy per translation unit that includes
 // this header, filled by that unit's fftreg_init().
 static __constant__ float2 c_w64[64];
+static __constant__ double2 c_w64d[64];   // the same in FP64, for double2 lines
 
 template <typename C>
 __device__ __forceinline__ C w64(int k, int sign)
@@ -24,6 +25,12 @@ __device__ __forceinline__ C w64(int k, int sign)
     c.x = w.x;
     c.y = sign > 0 ? -w.y : w.y;
     return c;
+}
+template <>
+__device__ __forceinline__ double2 w64<double2>(int k, int sign)
+{
+    const double2 w = c_w64d[k & 63];
+    return make_double2(w.x, sign > 0 ? -w.y : w.y);
 }
 
 template <int E, int SIGN, typename C>

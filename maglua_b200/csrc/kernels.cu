@@ -1248,7 +1248,12 @@ static void conv_generic(const ConvK& c, const FftLen& Lx, const FftLen& Ly, con
         k_conv_fx<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, Lx, tw, s[0], s[1], s[2], spec);
     }
     if (c.split) {
-        launch_conv_split_yz(c, Ly, Lz, tw_, spec_, ten6, ten9, (int)sizeof(R), st);
+        const FftLen L[3] = {Lx, Ly, Lz};
+        if (sizeof(R) == 8 && split_fast_ok_f64(c))
+            launch_split_fast_f64(c, L, static_cast<const double2*>(tw_), static_cast<double2*>(spec_),
+                                  static_cast<const double*>(ten6), st);
+        else
+            launch_conv_split_yz(c, Ly, Lz, tw_, spec_, ten6, ten9, (int)sizeof(R), st);
     } else {
         Prof pf("k_conv_yz", st);
         k_conv_yz<R><<<c.Kx, 512, conv_yz_smem(c, sizeof(R)), st>>>(c, Ly, Lz, tw, spec, static_cast<const R*>(ten6),

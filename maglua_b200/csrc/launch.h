@@ -66,6 +66,11 @@ bool conv_fast_ok(const ConvK& c);
 // FP32 x passes alone (power-of-two periodic x, 16..512): the forward
 // transform of the spins to SPEC (fwd) or the inverse to the field h.
 bool x_fast_ok(const ConvK& c);
+// The register split (y,z) passes for FP64 state (power-of-two planes, real
+// tensor).
+bool split_fast_ok_f64(const ConvK& c);
+cudaError_t launch_split_fast_f64(const ConvK& c, const FftLen L[3], const double2* tw, double2* spec,
+                                  const double* ten6, cudaStream_t st);
 // The FP32 split y passes alone: SPEC -> S2 (c.spec2) forward, S2 -> SPEC
 // inverse, power-of-two Py 32..512.
 bool split_y_fast_ok(const ConvK& c);

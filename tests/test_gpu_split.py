@@ -160,3 +160,44 @@ def test_cube_256_open_sampled_sites(M):
     sites = np.concatenate([corners, r.integers(0, n, 5)])
     ref = O.dipole_direct_sites(dims, s, 0.03, sites)
     assert rel_err(h[:, sites], ref) <= FIELD_TOL
+
+
+def test_split_fp64_steps_match_calls_and_oracle(M):
+    """FP64 state on a plane larger than shared memory (32 x 64 x 24,
+    periodic in-plane, z padded to 64: 64 x 64 complex doubles): the
+    register split passes in double; captured steps equal the individual
+    calls bitwise and follow the FP64 oracle."""
+    dims = (32, 64, 24)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 69, deg=15.0)
+    f, t, j = O.nn_paths(*dims, pbc=(1, 1, 0))
+    res = []
+    for mode in ("calls", "run"):
+        ss = M.SpinSystem(*dims, precision="f64")
+        ss.setSpinArrays(*s0)
+        ss.setAlpha(0.1)
+        ss.setTimeStep(0.01)
+        ex = M.Exchange(ss)
+        ex.addPaths(f, t, j)
+        dip = M.Dipole(ss)
+        dip.setStrength(0.05)
+        dip.setTruncation(12)
+        ops = [ex, dip]
+        llg = M.LLG.new("Quaternion")
+        if mode == "calls":
+            for _ in range(4):
+                ss.resetFields()
+                for op in ops:
+                    op.apply(ss)
+                ss.sumFields()
+                llg.apply(ss)
+        else:
+            M.run(ss, ops, llg, 4)
+        res.append(np.stack(ss.spinArrays()[:3]))
+    np.testing.assert_array_equal(res[0], res[1])
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s0)
+    o.alpha, o.dt = 0.1, 0.01
+    lr = O.LongRange(*dims, O.dipole_tensor(*dims, gmax=(12, 12, 12, 12)))
+    O.run_steps(o, 4, paths=(f, t, j), lr=lr, g=0.05, llg="Quaternion")
+    assert float(np.abs(res[1] - o.spins()).max()) < 1e-11
