@@ -60,43 +60,46 @@ struct XCfg {
     static constexpr int LINE = L * PX;                        // line buffer
     static constexpr int SPEC = ROWS * KX;                     // [ROWS][KX] staging
     static constexpr int BUF = LINE > SPEC ? LINE : SPEC;      // each of A, B
-    static constexpr int SMEM = (PX + 2 * BUF) * 8;            // bytes
+    static constexpr int SMEM = (PX + 2 * BUF) * 8;            // bytes (FP32)
+    static constexpr int SMEM_D = (PX + 2 * BUF) * 16;         // bytes (FP64)
 };
 
-template <int PX>
-__global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restrict__ tw, const float* __restrict__ sx,
-                                                 const float* __restrict__ sy, const float* __restrict__ sz,
-                                                 float2* __restrict__ spec)
+// R = float or double (state precision), C the matching complex type.
+template <int PX, typename R = float>
+__global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const typename CT<R>::T* __restrict__ tw,
+                                                 const R* __restrict__ sx, const R* __restrict__ sy,
+                                                 const R* __restrict__ sz, typename CT<R>::T* __restrict__ spec)
 {
+    typedef typename CT<R>::T C;
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
     using X = XCfg<PX>;
     constexpr int NT = X::NT;
-    extern __shared__ float2 sm[];
-    float2* twl = sm;               // [PX]
-    float2* A = twl + PX;           // [L][PX]
-    float2* B = A + X::BUF;         // [L][PX]
+    extern __shared__ __align__(16) unsigned char smraw_fx[];
+    C* twl = reinterpret_cast<C*>(smraw_fx);   // [PX]
+    C* A = twl + PX;                           // [L][PX]
+    C* B = A + X::BUF;                         // [L][PX]
     const int comp = blockIdx.z % 3, rep = blockIdx.z / 3;
     const int nr = c.nz * c.ny;                 // rows (z, y) of one component, flattened
     const int row0 = blockIdx.x * X::ROWS;
     const size_t nsite = (size_t)c.nx * c.ny * c.nz;
     spec += (size_t)rep * c.Kx * 3 * nr;
-    const float* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + rep * nsite;
+    const R* src = (comp == 0 ? sx : (comp == 1 ? sy : sz)) + rep * nsite;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     constexpr int IT = (X::LINE + NT - 1) / NT;
-    float2 v[IT];
+    C v[IT];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int idx = threadIdx.x + it * NT;
         const int l = idx / PX, x = idx % PX;
         const int ya = row0 + 2 * l, yb = ya + 1;
-        float a = 0.f, b = 0.f;
+        R a = 0, b = 0;
         if (idx < X::LINE && x < c.nx) {
             if (ya < nr) a = __ldg(src + (size_t)ya * c.nx + x);
             if (yb < nr) b = __ldg(src + (size_t)yb * c.nx + x);
         }
-        v[it] = make_float2(a, b);
+        v[it] = cmk<C>(a, b);
     }
 #pragma unroll
     for (int it = 0; it < IT; it++) {
@@ -105,7 +108,7 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
     }
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
-    const float2* R = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
+    const C* Rl = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
     // split the two real rows and store SPEC[kx][comp][row] (row = z ny + y)
     const int rows_here = min(X::ROWS, nr - row0);
     constexpr int IS = (X::SPEC + NT - 1) / NT;
@@ -114,45 +117,46 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const float2* __restri
         const int idx = threadIdx.x + it * NT;
         const int kx = idx / X::ROWS, row = idx % X::ROWS;
         if (idx >= X::SPEC || row >= rows_here) continue;
-        const float2* Z = R + (row >> 1) * PX;
-        const float2 zk = Z[kx], zn = Z[(PX - kx) & (PX - 1)];
-        float2 o;
-        if ((row & 1) == 0) o = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-        else o = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+        const C* Z = Rl + (row >> 1) * PX;
+        const C zk = Z[kx], zn = Z[(PX - kx) & (PX - 1)];
+        C o;
+        if ((row & 1) == 0) o = cmk<C>((R)0.5 * (zk.x + zn.x), (R)0.5 * (zk.y - zn.y));
+        else o = cmk<C>((R)0.5 * (zk.y + zn.y), (R)0.5 * (zn.x - zk.x));
         spec[((size_t)kx * 3 + comp) * nr + row0 + row] = o;
     }
 }
 
-template <int PX>
-__global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restrict__ tw, const float2* __restrict__ spec,
-                                                 float* __restrict__ hx, float* __restrict__ hy,
-                                                 float* __restrict__ hz)
+template <int PX, typename R = float>
+__global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const typename CT<R>::T* __restrict__ tw,
+                                                 const typename CT<R>::T* __restrict__ spec, R* __restrict__ hx,
+                                                 R* __restrict__ hy, R* __restrict__ hz)
 {
+    typedef typename CT<R>::T C;
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
     using X = XCfg<PX>;
     constexpr int KX = X::KX, NT = X::NT;
-    extern __shared__ float2 sm[];
-    float2* twl = sm;               // [PX]
-    float2* A = twl + PX;           // [L][PX] lines
-    float2* B = A + X::BUF;         // [ROWS][KX] spectra, then scratch
+    extern __shared__ __align__(16) unsigned char smraw_ix[];
+    C* twl = reinterpret_cast<C*>(smraw_ix);   // [PX]
+    C* A = twl + PX;                           // [L][PX] lines
+    C* B = A + X::BUF;                         // [ROWS][KX] spectra, then scratch
     const int comp = blockIdx.z % 3, rep = blockIdx.z / 3;
     const int nr = c.nz * c.ny;                 // rows (z, y) of one component, flattened
     const int row0 = blockIdx.x * X::ROWS;
     const int rows_here = min(X::ROWS, nr - row0);
     const size_t nsite = (size_t)c.nx * c.ny * c.nz;
     spec += (size_t)rep * c.Kx * 3 * nr;
-    float* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + rep * nsite;
+    R* dst = (comp == 0 ? hx : (comp == 1 ? hy : hz)) + rep * nsite;
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     constexpr int IS = (X::SPEC + NT - 1) / NT;
     {
-        float2 v[IS];
+        C v[IS];
 #pragma unroll
         for (int it = 0; it < IS; it++) {
             const int idx = threadIdx.x + it * NT;
             const int kx = idx / X::ROWS, row = idx % X::ROWS;
-            v[it] = make_float2(0.f, 0.f);
+            v[it] = cmk<C>(0, 0);
             if (idx < X::SPEC && row < rows_here)
                 v[it] = spec[((size_t)kx * 3 + comp) * nr + row0 + row];
         }
@@ -171,23 +175,23 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const float2* __restri
         const int idx = threadIdx.x + it * NT;
         if (idx >= X::LINE) continue;
         const int l = idx / PX, k = idx % PX;
-        const float2* Sa = B + (2 * l) * KX;
-        const float2* Sb = B + (2 * l + 1) * KX;
-        float2 a, b;
+        const C* Sa = B + (2 * l) * KX;
+        const C* Sb = B + (2 * l + 1) * KX;
+        C a, b;
         if (k < KX) { a = Sa[k]; b = Sb[k]; }
         else { a = cconj(Sa[PX - k]); b = cconj(Sb[PX - k]); }
-        A[idx] = make_float2(a.x - b.y, a.y + b.x);
+        A[idx] = cmk<C>(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
-    const float2* R = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
+    const C* Rl = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
     constexpr int IO = (X::ROWS * PX + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < IO; it++) {
         const int idx = threadIdx.x + it * NT;
         const int row = idx / PX, x = idx % PX;
         if (idx >= X::ROWS * PX || row >= rows_here || x >= c.nx) continue;
-        const float2 z = R[(row >> 1) * PX + x];
+        const C z = Rl[(row >> 1) * PX + x];
         dst[(size_t)(row0 + row) * c.nx + x] = (row & 1) ? z.y : z.x;
     }
 }
@@ -1091,11 +1095,36 @@ static cudaError_t launch_x(const ConvK& c, const float2* tw, const float* s[3],
     dim3 grid((c.nz * c.ny + X::ROWS - 1) / X::ROWS, 1, 3 * c.nrep);
     const size_t smem = X::SMEM;
     if (fwd) {
-        return launch_pdl(k_fx_fast<PX>, grid, dim3(256), smem, st, c, tw, s[0], s[1], s[2], spec);
+        return launch_pdl(k_fx_fast<PX, float>, grid, dim3(256), smem, st, c, tw, s[0], s[1], s[2], spec);
     } else {
-        return launch_pdl(k_ix_fast<PX>, grid, dim3(256), smem, st, c, tw, spec, h[0], h[1], h[2]);
+        return launch_pdl(k_ix_fast<PX, float>, grid, dim3(256), smem, st, c, tw, spec, h[0], h[1], h[2]);
     }
     return cudaGetLastError();
+}
+
+template <int PX>
+static cudaError_t launch_x_d(const ConvK& c, const double2* tw, const double* s[3], double2* spec, double* h[3],
+                              cudaStream_t st, bool fwd)
+{
+    using X = XCfg<PX>;
+    dim3 grid((c.nz * c.ny + X::ROWS - 1) / X::ROWS, 1, 3 * c.nrep);
+    const size_t smem = X::SMEM_D;
+    if (fwd) return launch_pdl(k_fx_fast<PX, double>, grid, dim3(256), smem, st, c, tw, s[0], s[1], s[2], spec);
+    return launch_pdl(k_ix_fast<PX, double>, grid, dim3(256), smem, st, c, tw, spec, h[0], h[1], h[2]);
+}
+
+static cudaError_t launch_x_any_d(const ConvK& c, const double2* tw, const double* s[3], double2* spec,
+                                  double* h[3], cudaStream_t st, bool fwd)
+{
+    switch (c.Px) {
+    case 16: return launch_x_d<16>(c, tw, s, spec, h, st, fwd);
+    case 32: return launch_x_d<32>(c, tw, s, spec, h, st, fwd);
+    case 64: return launch_x_d<64>(c, tw, s, spec, h, st, fwd);
+    case 128: return launch_x_d<128>(c, tw, s, spec, h, st, fwd);
+    case 256: return launch_x_d<256>(c, tw, s, spec, h, st, fwd);
+    case 512: return launch_x_d<512>(c, tw, s, spec, h, st, fwd);
+    }
+    return cudaErrorInvalidValue;
 }
 
 static cudaError_t launch_x_any(const ConvK& c, const float2* tw, const float* s[3], float2* spec, float* h[3],
@@ -1164,11 +1193,15 @@ static cudaError_t cfg_x()
 {
     const cudaFuncAttribute co = cudaFuncAttributePreferredSharedMemoryCarveout;
     const int mx = (int)cudaSharedmemCarveoutMaxShared;
-    cudaError_t e = cudaFuncSetAttribute(k_fx_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if (e != cudaSuccess || (e = cudaFuncSetAttribute(k_fx_fast<PX>, co, mx)) != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_ix_fast<PX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(k_fx_fast<PX, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess || (e = cudaFuncSetAttribute(k_fx_fast<PX, float>, co, mx)) != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_ix_fast<PX, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess || (e = cudaFuncSetAttribute(k_ix_fast<PX, float>, co, mx)) != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_fx_fast<PX, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess || (e = cudaFuncSetAttribute(k_fx_fast<PX, double>, co, mx)) != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_ix_fast<PX, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_ix_fast<PX>, co, mx);
+    return cudaFuncSetAttribute(k_ix_fast<PX, double>, co, mx);
 }
 template <int PY>
 static cudaError_t cfg_yz()
@@ -1237,6 +1270,31 @@ cudaError_t launch_conv_fast(const ConvK& c, const FftLen L[3], const float2* tw
 
 // ------------------------------------------------------------------ fused x pass dispatch
 bool x_fast_ok(const ConvK& c) { return pow2_in(c.Px, 16, 512) && c.Px == c.nx; }
+
+// The register-free Stockham x passes for FP64 state (power-of-two Px
+// 16..512, periodic or zero-padded x): 16 bytes per complex, so at most
+// (PX + 2 BUF) * 16 bytes of shared memory per CTA.
+bool x_fast_ok_f64(const ConvK& c)
+{
+    if (!pow2_in(c.Px, 16, 512) || c.nrep != 1) return false;
+    switch (c.Px) {
+    case 16: return XCfg<16>::SMEM_D <= 227 * 1024;
+    case 32: return XCfg<32>::SMEM_D <= 227 * 1024;
+    case 64: return XCfg<64>::SMEM_D <= 227 * 1024;
+    case 128: return XCfg<128>::SMEM_D <= 227 * 1024;
+    case 256: return XCfg<256>::SMEM_D <= 227 * 1024;
+    case 512: return XCfg<512>::SMEM_D <= 227 * 1024;
+    }
+    return false;
+}
+
+cudaError_t launch_x_pass_f64(const ConvK& c, const FftLen L[3], const double2* tw, const double* s[3],
+                              double2* spec, double* h[3], bool fwd, cudaStream_t st)
+{
+    if (!x_fast_ok_f64(c)) return cudaErrorInvalidValue;
+    Prof pf(fwd ? "k_conv_fx" : "k_conv_ix", st);
+    return launch_x_any_d(c, tw + L[0].tw_off, s, spec, h, st, fwd);
+}
 
 cudaError_t launch_x_pass_fast(const ConvK& c, const FftLen L[3], const float2* tw, const float* s[3], float2* spec,
                                float* h[3], bool fwd, cudaStream_t st)

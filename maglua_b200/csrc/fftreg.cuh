@@ -148,9 +148,10 @@ struct Tpl {
 
 // One radix-R Stockham stage (R = 2 or 4) of a line of N points: thread tl
 // of the line's TPL threads handles butterflies j = tl + TPL m.  tw is the
-// N-entry table exp(-2 pi i k / N) (conjugated for SIGN = +1).
-template <int N, int R, int NS, int SIGN, int TPL>
-__device__ __forceinline__ void sm_stage(const float2* src, float2* dst, int tl, const float2* tw)
+// N-entry table exp(-2 pi i k / N) (conjugated for SIGN = +1).  C is float2
+// or double2.
+template <int N, int R, int NS, int SIGN, int TPL, typename C>
+__device__ __forceinline__ void sm_stage(const C* src, C* dst, int tl, const C* tw)
 {
     constexpr int NB = N / R;
     constexpr int TWS = N / (NS * R);
@@ -159,55 +160,55 @@ __device__ __forceinline__ void sm_stage(const float2* src, float2* dst, int tl,
         const int j = tl + TPL * m;
         if (NB % TPL != 0 && j >= NB) break;
         const int jm = j & (NS - 1);
-        float2 v[R];
+        C v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            float2 x = src[j + r * NB];
+            C x = src[j + r * NB];
             if (NS > 1 && r > 0) {
-                float2 w = tw[(r * jm * TWS) & (N - 1)];
+                C w = tw[(r * jm * TWS) & (N - 1)];
                 if (SIGN > 0) w.y = -w.y;
                 x = cmul(x, w);
             }
             v[r] = x;
         }
-        if (R == 4) RegFFT<4, SIGN, float2>::run(v);
-        else RegFFT<2, SIGN, float2>::run(v);
+        if (R == 4) RegFFT<4, SIGN, C>::run(v);
+        else RegFFT<2, SIGN, C>::run(v);
         const int idxD = (j - jm) * R + jm;
 #pragma unroll
         for (int r = 0; r < R; r++) dst[idxD + r * NS] = v[r];
     }
 }
 
-template <int N, int SIGN, int TPL, int NS>
+template <int N, int SIGN, int TPL, int NS, typename C>
 struct SmStages {
     // radix-4 while four more points fit, a final radix-2 when log2(N) is odd
-    __device__ __forceinline__ static float2* run(float2* a, float2* b, int tl, const float2* tw, bool act)
+    __device__ __forceinline__ static C* run(C* a, C* b, int tl, const C* tw, bool act)
     {
         if (NS * 4 <= N) {
-            if (act) sm_stage<N, 4, NS, SIGN, TPL>(a, b, tl, tw);
+            if (act) sm_stage<N, 4, NS, SIGN, TPL, C>(a, b, tl, tw);
             __syncthreads();
-            return SmStages<N, SIGN, TPL, (NS * 4 <= N ? NS * 4 : N)>::run(b, a, tl, tw, act);
+            return SmStages<N, SIGN, TPL, (NS * 4 <= N ? NS * 4 : N), C>::run(b, a, tl, tw, act);
         } else if (NS * 2 <= N) {
-            if (act) sm_stage<N, 2, NS, SIGN, TPL>(a, b, tl, tw);
+            if (act) sm_stage<N, 2, NS, SIGN, TPL, C>(a, b, tl, tw);
             __syncthreads();
             return b;
         }
         return a;
     }
 };
-template <int N, int SIGN, int TPL>
-struct SmStages<N, SIGN, TPL, N> {
-    __device__ __forceinline__ static float2* run(float2* a, float2*, int, const float2*, bool) { return a; }
+template <int N, int SIGN, int TPL, typename C>
+struct SmStages<N, SIGN, TPL, N, C> {
+    __device__ __forceinline__ static C* run(C* a, C*, int, const C*, bool) { return a; }
 };
 
 // Transform line l (data at a + l*N, scratch at b + l*N) by its TPL threads
 // (tl = thread index within the line).  Every thread of the CTA must call
 // this (act = false for threads without a line): it synchronises the CTA
 // after each stage.  Returns the base (a or b) that holds the result.
-template <int N, int SIGN, int TPL>
-__device__ __forceinline__ float2* sm_fft(float2* a, float2* b, int l, int tl, const float2* tw, bool act)
+template <int N, int SIGN, int TPL, typename C>
+__device__ __forceinline__ C* sm_fft(C* a, C* b, int l, int tl, const C* tw, bool act)
 {
-    float2* r = SmStages<N, SIGN, TPL, 1>::run(a + (size_t)l * N, b + (size_t)l * N, tl, tw, act);
+    C* r = SmStages<N, SIGN, TPL, 1, C>::run(a + (size_t)l * N, b + (size_t)l * N, tl, tw, act);
     return r == a + (size_t)l * N ? a : b;
 }
 

@@ -1243,14 +1243,21 @@ static void conv_generic(const ConvK& c, const FftLen& Lx, const FftLen& Ly, con
     const C* tw = static_cast<const C*>(tw_);
     C* spec = static_cast<C*>(spec_);
     dim3 gx(blocks_for(c.ny, c.ty), c.nz);
-    {
+    const FftLen L3[3] = {Lx, Ly, Lz};
+    // FP64 state with a power-of-two x length: the fast x passes in double
+    const bool fx64 = sizeof(R) == 8 && x_fast_ok_f64(c);
+    const double* sd[3] = {static_cast<const double*>(s[0]), static_cast<const double*>(s[1]),
+                           static_cast<const double*>(s[2])};
+    double* hd[3] = {static_cast<double*>(h[0]), static_cast<double*>(h[1]), static_cast<double*>(h[2])};
+    if (fx64) {
+        launch_x_pass_f64(c, L3, static_cast<const double2*>(tw_), sd, static_cast<double2*>(spec_), hd, true, st);
+    } else {
         Prof pf("k_conv_fx", st);
         k_conv_fx<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, Lx, tw, s[0], s[1], s[2], spec);
     }
     if (c.split) {
-        const FftLen L[3] = {Lx, Ly, Lz};
         if (sizeof(R) == 8 && split_fast_ok_f64(c))
-            launch_split_fast_f64(c, L, static_cast<const double2*>(tw_), static_cast<double2*>(spec_),
+            launch_split_fast_f64(c, L3, static_cast<const double2*>(tw_), static_cast<double2*>(spec_),
                                   static_cast<const double*>(ten6), st);
         else
             launch_conv_split_yz(c, Ly, Lz, tw_, spec_, ten6, ten9, (int)sizeof(R), st);
@@ -1259,7 +1266,9 @@ static void conv_generic(const ConvK& c, const FftLen& Lx, const FftLen& Ly, con
         k_conv_yz<R><<<c.Kx, 512, conv_yz_smem(c, sizeof(R)), st>>>(c, Ly, Lz, tw, spec, static_cast<const R*>(ten6),
                                                                     static_cast<const C*>(ten9));
     }
-    {
+    if (fx64) {
+        launch_x_pass_f64(c, L3, static_cast<const double2*>(tw_), sd, static_cast<double2*>(spec_), hd, false, st);
+    } else {
         Prof pf("k_conv_ix", st);
         k_conv_ix<R><<<gx, 256, conv_x_smem(c, sizeof(R)), st>>>(c, Lx, tw, spec, h[0], h[1], h[2]);
     }

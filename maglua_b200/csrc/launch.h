@@ -66,6 +66,10 @@ bool conv_fast_ok(const ConvK& c);
 // FP32 x passes alone (power-of-two periodic x, 16..512): the forward
 // transform of the spins to SPEC (fwd) or the inverse to the field h.
 bool x_fast_ok(const ConvK& c);
+// The fast x passes for FP64 state (power-of-two Px 16..512).
+bool x_fast_ok_f64(const ConvK& c);
+cudaError_t launch_x_pass_f64(const ConvK& c, const FftLen L[3], const double2* tw, const double* s[3],
+                              double2* spec, double* h[3], bool fwd, cudaStream_t st);
 // The register split (y,z) passes for FP64 state (power-of-two planes, real
 // tensor).
 bool split_fast_ok_f64(const ConvK& c);
