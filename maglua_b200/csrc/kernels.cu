@@ -81,8 +81,8 @@ __device__ __forceinline__ V3<R> ex_term(const ExchangeK& e, const SysK& s, int 
             const R mf = ms_at<R>(s, f);
             if (mf != (R)0) {
                 const V3<R> sf = spin_at<R>(s, f);
-                const R den = e.normalize ? mf * mt : mf;
-                h = add3(h, v3<R>(sf.x * J / den, sf.y * J / den, sf.z * J / den));
+                const R w = J / (e.normalize ? mf * mt : mf);   // one division per neighbour
+                h = add3(h, v3<R>(sf.x * w, sf.y * w, sf.z * w));
             }
         }
     } else if (e.mode == EX_CSR) {
