@@ -706,22 +706,29 @@ def main():
         ss.netMomentAsync(k % 4)
         ss.netMomentWait(k % 4)
     ss.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    ss.uploadF32(hx, hy, hz, hm)
-    # each step's netMoment is read on the host; the read of step k waits
-    # while steps k + 1 and k + 2 are already queued on the GPU
-    depth = 2
-    for k in range(args.steps):
-        plan_nt.launch(1)
-        ss.netMomentAsync(k % 4)
-        if k >= depth:
-            ss.netMomentWait((k - depth) % 4)
-    for k in range(max(0, args.steps - depth), args.steps):
-        ss.netMomentWait(k % 4)
-    ss.downloadF32(hx, hy, hz)
-    ss.synchronize()
-    e2e_s = time.perf_counter() - t0
+
+    def e2e_run():
+        barrier()
+        t0 = time.perf_counter()
+        ss.uploadF32(hx, hy, hz, hm)
+        # each step's netMoment is read on the host; the read of step k waits
+        # while steps k + 1 and k + 2 are already queued on the GPU
+        depth = 2
+        for k in range(args.steps):
+            plan_nt.launch(1)
+            ss.netMomentAsync(k % 4)
+            if k >= depth:
+                ss.netMomentWait((k - depth) % 4)
+        for k in range(max(0, args.steps - depth), args.steps):
+            ss.netMomentWait(k % 4)
+        ss.downloadF32(hx, hy, hz)
+        ss.synchronize()
+        return time.perf_counter() - t0
+
+    # the host loop shares its cores with other work on the box: the median
+    # of three complete runs
+    e2e_runs = sorted(e2e_run() for _ in range(3))
+    e2e_s = e2e_runs[1]
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -779,7 +786,8 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": (16 * n) / args.steps,
                 "d2h_bytes_per_step": 48 + (12 * n) / args.steps,
                 "how": "C-ABI calls from host: pinned FP32 upload, per step mlb_plan_launch(1) + netMoment of that "
-                       "step read into pinned memory and waited for once two more steps are queued, final download"},
+                       "step read into pinned memory and waited for once two more steps are queued, final download; median of "
+                       "three complete runs"},
         "gpu_launches": launches,
         "roofline": roof,
         "kernels": kernels_out,

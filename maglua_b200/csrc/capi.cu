@@ -237,7 +237,9 @@ struct mlb_system {
     // slots of mlb_system_netmoment_async, each with an event)
     cudaGraphExec_t nm_exec[2][5] = {};
     double nm_m[2][5] = {};
-    double* nm_host = nullptr;      // pinned, 5 x 6 doubles
+    double* nm_host = nullptr;      // pinned, 5 x 6 doubles (the device writes them directly)
+    double* nm_host_dev = nullptr;  // the device's address of nm_host
+    unsigned* nm_counter = nullptr; // blocks done in the current netMoment launch
     cudaEvent_t nm_ev[4] = {};
     bool nm_pending[4] = {};
     double* red = nullptr;
@@ -1770,6 +1772,11 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
     CK(cudaMallocHost(&s->nm_host, sizeof(double) * 30));
+    // pinned memory is mapped for the device under unified addressing; the
+    // call fails (host side) where it is not
+    CK(cudaHostGetDevicePointer((void**)&s->nm_host_dev, s->nm_host, 0));
+    CK(cudaMalloc(&s->nm_counter, sizeof(unsigned)));
+    CK(cudaMemset(s->nm_counter, 0, sizeof(unsigned)));
     s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
     CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
     CK(cudaMalloc(&s->redout, sizeof(double) * 8));
@@ -1796,6 +1803,7 @@ void free_system(mlb_system* s)
     for (int k = 0; k < 4; k++)
         if (s->nm_ev[k]) cudaEventDestroy(s->nm_ev[k]);
     cudaFreeHost(s->nm_host);
+    cudaFree(s->nm_counter);
     cudaFree(s->red);
     cudaFree(s->redout);
     for (Slot& x : s->slots)
@@ -2653,10 +2661,10 @@ static void netmoment_enqueue(mlb_system* s, double m, int d)
         CK(cudaStreamSynchronize(s->st));
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = mlb::launch_netmoment(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, s->red, s->red_nb,
-                                              s->redout, s->rb, s->st);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(s->nm_host + 6 * d, s->redout, sizeof(double) * 6, cudaMemcpyDeviceToHost, s->st);
+        // one kernel: the last block writes the sums into the pinned slot
+        cudaError_t e = mlb::launch_netmoment_one(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, s->red,
+                                                  std::min(s->red_nb, 2 * 148), s->nm_counter, s->nm_host_dev + 6 * d, s->redout, s->rb,
+                                                  s->st);
         cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&s->nm_exec[q][d], g, 0);

@@ -410,6 +410,77 @@ __global__ void __launch_bounds__(256) k_netmoment_partial(const void* x_, const
     }
 }
 
+// netMoment in one launch: each block writes its six partials as
+// k_netmoment_partial does; the last block to finish (a device counter,
+// reset for the next launch) reduces them, one warp per quantity in a fixed
+// order, and writes the six results to out (pinned host memory the device
+// reaches directly) and out_dev.
+template <typename R>
+__global__ void __launch_bounds__(256) k_netmoment_one(const void* x_, const void* y_, const void* z_, int n,
+                                                       double m, double* part, unsigned* counter, double* out,
+                                                       double* out_dev)
+{
+    const R* x = static_cast<const R*>(x_);
+    const R* y = static_cast<const R*>(y_);
+    const R* z = static_cast<const R*>(z_);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a = (double)x[i] * m, b = (double)y[i] * m, c = (double)z[i] * m;
+        acc[0] += a; acc[1] += b; acc[2] += c;
+        acc[3] += a * a; acc[4] += b * b; acc[5] += c * c;
+    }
+    __shared__ double sh[6][8];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[q][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) v += sh[threadIdx.x][k];
+        part[blockIdx.x * 6 + threadIdx.x] = v;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // warp q sums quantity q: lane l takes blocks l, l + 32, ... in order,
+    // then a fixed shuffle tree (deterministic)
+    const int nb = gridDim.x;
+    if (w < 6) {
+        double v = 0;
+        for (int b = lane; b < nb; b += 32) v += __ldcg(part + b * 6 + w);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) {
+            out[w] = v;
+            out_dev[w] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        __threadfence_system();
+    }
+}
+
+namespace mlb {
+cudaError_t launch_netmoment_one(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
+                                 unsigned* counter, double* out_host, double* out_dev, int rb, cudaStream_t st)
+{
+    if (rb == 8)
+        k_netmoment_one<double><<<nb, 256, 0, st>>>(x, y, z, n, m, part, counter, out_host, out_dev);
+    else
+        k_netmoment_one<float><<<nb, 256, 0, st>>>(x, y, z, n, m, part, counter, out_host, out_dev);
+    return cudaGetLastError();
+}
+} // namespace mlb
+
 // FP64 partial sums of |a - b| per component (SpinSystem::diff,
 // spinsystem.cpp:301-307 with dArray::diffSum).
 template <typename R>

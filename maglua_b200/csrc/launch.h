@@ -109,6 +109,10 @@ cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* con
                        void* const out[3], int rb, cudaStream_t st);
 cudaError_t launch_advance_step(DevStep* d, cudaStream_t st);
 cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st);
+// netMoment as one launch (partials, then the last block's fixed-order
+// final sums into pinned host memory and out_dev); counter starts at 0.
+cudaError_t launch_netmoment_one(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
+                                 unsigned* counter, double* out_host, double* out_dev, int rb, cudaStream_t st);
 cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
                              double* out, int rb, cudaStream_t st);
 cudaError_t launch_dot(const void* const s[3], const void* const h[3], int n, double* part, int nb, double* out,
