@@ -424,10 +424,26 @@ __global__ void __launch_bounds__(256) k_netmoment_one(const void* x_, const voi
     const R* y = static_cast<const R*>(y_);
     const R* z = static_cast<const R*>(z_);
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double a = (double)x[i] * m, b = (double)y[i] * m, c = (double)z[i] * m;
-        acc[0] += a; acc[1] += b; acc[2] += c;
-        acc[3] += a * a; acc[4] += b * b; acc[5] += c * c;
+    // eight sites per round with their loads issued together (one memory
+    // latency per round instead of one per site); sites in increasing order
+    const int stride = gridDim.x * blockDim.x;
+    constexpr int U = 8;
+    for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
+        R xs[U], ys[U], zs[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = i0 + u * stride;
+            xs[u] = i < n ? x[i] : (R)0;
+            ys[u] = i < n ? y[i] : (R)0;
+            zs[u] = i < n ? z[i] : (R)0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (i0 + u * stride >= n) break;
+            const double a = (double)xs[u] * m, b = (double)ys[u] * m, c = (double)zs[u] * m;
+            acc[0] += a; acc[1] += b; acc[2] += c;
+            acc[3] += a * a; acc[4] += b * b; acc[5] += c * c;
+        }
     }
     __shared__ double sh[6][8];
     __shared__ bool last;
