@@ -235,7 +235,7 @@ def run_fp64_film(M, torch, steps=20):
     n = NX * NY * NZ
     return {"workload": WORKLOAD + " in FP64", "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "how": "one captured step per graph launch, back to back, CUDA events; FP64 register split (y,z) "
-                   "passes and x passes, generic FP64 fused step"}
+                   "passes, x passes and fused step"}
 
 
 # ----------------------------------------------------------------- LongRange2D / Dipole2D

@@ -1513,10 +1513,11 @@ LlgK llgk(const mlb_llg* l, double dt)
 
 // Constants of k_fused_fast when every parameter is uniform across sites;
 // false sends the step to the general fused kernel.
-bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, double dt_sys, FastK& F)
+template <typename R>
+bool fast_fused_t(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, double dt_sys, FastKT<R>& F)
 {
     refresh_ms(s);
-    if (s->rb != 4 || !s->ms_uniform || !(s->ms_u > 0.0) || s->sa || s->sg) return false;
+    if (s->rb != (int)sizeof(R) || !s->ms_uniform || !(s->ms_u > 0.0) || s->sa || s->sg) return false;
     if (T.ex.mode == EX_CSR || T.ani.mode == ANI_CSR || T.uni.mode != ANI_NONE) return false;
     // one uniform cubic axis set alone (no simple anisotropy beside it)
     if (T.cub.mode == ANI_CSR || (T.cub.mode == ANI_UNIFORM && T.ani.mode != ANI_NONE)) return false;
@@ -1528,47 +1529,52 @@ bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, dou
     F.ex = T.ex.mode == EX_STENCIL;
     if (F.ex) {
         const double den = T.ex.normalize ? ms * ms : ms;
-        for (int d = 0; d < 6; d++) F.J[d] = (float)((double)T.ex.J[d] * T.ex_gs / den);
+        for (int d = 0; d < 6; d++) F.J[d] = (R)((double)T.ex.J[d] * T.ex_gs / den);
         for (int c = 0; c < 3; c++) F.pbc[c] = T.ex.pbc[c];
     }
     F.ani = T.ani.mode == ANI_UNIFORM ? 1 : 0;
     if (F.ani) {
-        for (int c = 0; c < 3; c++) F.axis[c] = (float)T.ani.axis[c];
-        F.ani_c = (float)(2.0 * (double)T.ani.K / (ms * ms));
+        for (int c = 0; c < 3; c++) F.axis[c] = (R)T.ani.axis[c];
+        F.ani_c = (R)(2.0 * (double)T.ani.K / (ms * ms));
     }
     if (T.cub.mode == ANI_UNIFORM) {
         F.ani = 2;
-        for (int q = 0; q < 9; q++) F.cub_n[q] = (float)T.cub.axes[q];
-        for (int q = 0; q < 3; q++) F.cub_K[q] = (float)T.cub.K[q];
+        for (int q = 0; q < 9; q++) F.cub_n[q] = (R)T.cub.axes[q];
+        for (int q = 0; q < 3; q++) F.cub_K[q] = (R)T.cub.K[q];
         F.cub_quirk = T.cub.quirk;
-        F.cub_ims = (float)(1.0 / ms);
+        F.cub_ims = (R)(1.0 / ms);
     }
     F.th = T.th.mode == TH_PHILOX && T.th.T != 0.0 && g > 0;
     if (F.th) {
-        F.sigma = (float)std::sqrt((2.0 * a * (double)T.th.T) / (ms * dt_sys * g));
+        F.sigma = (R)std::sqrt((2.0 * a * (double)T.th.T) / (ms * dt_sys * g));
         F.seed = T.th.seed; F.counter = T.th.counter; F.dctr = T.th.dctr;
     }
     if (T.zee.on) {
-        for (int c = 0; c < 3; c++) F.B[c] = (float)T.zee.B[c];
+        for (int c = 0; c < 3; c++) F.B[c] = (R)T.zee.B[c];
         F.Bdev = T.zee.Bdev;
     }
-    F.addw = T.nadd == 1 ? (float)T.addw[0] : 0.f;
+    F.addw = T.nadd == 1 ? (R)T.addw[0] : 0.f;
     F.llg_type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
     F.tof = l->tof;
     F.renorm = l->disable_renorm ? 0 : 1;
     F.dt_zero = dt == 0.0;
-    F.dt = (float)dt;
-    F.precess = (float)l->precess;
-    F.ms = (float)ms;
+    F.dt = (R)dt;
+    F.precess = (R)l->precess;
+    F.ms = (R)ms;
     const double gaa = g / (1.0 + a * a);
     if (F.llg_type == LLG_CART) {
-        F.c_prec = (float)(l->tof ? l->precess * -gaa : -gaa);
-        F.c_damp = (float)(l->tof ? l->damp * (a / ms) * gaa : (a / ms) * gaa);
+        F.c_prec = (R)(l->tof ? l->precess * -gaa : -gaa);
+        F.c_damp = (R)(l->tof ? l->damp * (a / ms) * gaa : (a / ms) * gaa);
     } else {
-        F.c_damp = (float)(l->tof ? l->damp * a / ms : a / ms);
-        F.c_rot = (float)(0.5 * g * dt / (1.0 + a * a));
+        F.c_damp = (R)(l->tof ? l->damp * a / ms : a / ms);
+        F.c_rot = (R)(0.5 * g * dt / (1.0 + a * a));
     }
     return true;
+}
+
+bool fast_fused(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, double dt_sys, FastK& F)
+{
+    return fast_fused_t<float>(s, T, l, dt, dt_sys, F);
 }
 
 // Fused in-place step when Total is lazily defined; returns false when the
@@ -1605,6 +1611,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
     }
     const int nb = 1 - s->cur;
     FastK F;
+    FastKT<double> Fd;
     bool carried = false;   // SPEC ends holding the new spins' x transform
     if (s->dry) {
         // bookkeeping only: the kernels of this step ran in a captured graph
@@ -1638,6 +1645,18 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
             flush_pending(s);
             CK(mlb::launch_fused_fast(F, sp, ad, out, s->st));
         }
+    } else if (s->rb == 8 && fast_fused_t<double>(s, T, l, dt, dt_sys, Fd)) {
+        // FP64 state with uniform parameters: the fast kernel in double
+        flush_pending(s);
+        const double* sp[3];
+        const double* ad[3] = {nullptr, nullptr, nullptr};
+        double* out[3];
+        for (int c = 0; c < 3; c++) {
+            sp[c] = static_cast<const double*>(s->sp[s->cur][c]);
+            out[c] = static_cast<double*>(s->sp[nb][c]);
+            if (T.nadd == 1) ad[c] = static_cast<const double*>(T.add[0][c]);
+        }
+        CK(mlb::launch_fused_fast_f64(Fd, sp, ad, out, s->st));
     } else {
         flush_pending(s);
         FusedK P;

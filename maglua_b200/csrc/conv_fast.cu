@@ -787,34 +787,34 @@ static cudaError_t cfg_split()
 
 // ------------------------------------------------------------------ fused step
 // (fused_site_v, the per-site arithmetic, is in fused.cuh)
-template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__device__ __forceinline__ void fused_site(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
-                                           const float* __restrict__ sx, const float* __restrict__ sy,
-                                           const float* __restrict__ sz, const float* __restrict__ ax,
-                                           const float* __restrict__ ay, const float* __restrict__ az,
-                                           float* __restrict__ ox, float* __restrict__ oy, float* __restrict__ oz)
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R = float>
+__device__ __forceinline__ void fused_site(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                           const R* __restrict__ sx, const R* __restrict__ sy,
+                                           const R* __restrict__ sz, const R* __restrict__ ax,
+                                           const R* __restrict__ ay, const R* __restrict__ az,
+                                           R* __restrict__ ox, R* __restrict__ oy, R* __restrict__ oz)
 {
-    float Ax = 0.f, Ay = 0.f, Az = 0.f;
+    R Ax = 0, Ay = 0, Az = 0;
     if (ADD) { Ax = __ldg(ax + i); Ay = __ldg(ay + i); Az = __ldg(az + i); }
-    float rx, ry, rz;
+    R rx, ry, rz;
     fused_site_v<LT, EXS, ANI, TH, ADD>(F, NX, NY, NZ, x, y, z, i, sx, sy, sz, Ax, Ay, Az, rx, ry, rz);
     ox[i] = rx; oy[i] = ry; oz[i] = rz;
 }
 
-template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__global__ void __launch_bounds__(256) k_fused_fast(FastK F0, const float* __restrict__ sx, const float* __restrict__ sy,
-                                                    const float* __restrict__ sz, const float* __restrict__ ax,
-                                                    const float* __restrict__ ay, const float* __restrict__ az,
-                                                    float* __restrict__ ox, float* __restrict__ oy,
-                                                    float* __restrict__ oz)
+// R = float (FP32 state) or double (FP64 state, constants in FastKT<double>)
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R = float>
+__global__ void __launch_bounds__(256) k_fused_fast(FastKT<R> F0, const R* __restrict__ sx, const R* __restrict__ sy,
+                                                    const R* __restrict__ sz, const R* __restrict__ ax,
+                                                    const R* __restrict__ ay, const R* __restrict__ az,
+                                                    R* __restrict__ ox, R* __restrict__ oy, R* __restrict__ oz)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int z = blockIdx.z;
     if (x >= F0.nx || y >= F0.ny) return;
-    const FastK F = fastk_resolved(F0);
+    const FastKT<R> F = fastk_resolved(F0);
     const int i = x + F.nx * (y + F.ny * z);
-    fused_site<LT, EXS, ANI, TH, ADD>(F, F.nx, F.ny, F.nz, x, y, z, i, sx, sy, sz, ax, ay, az, ox, oy, oz);
+    fused_site<LT, EXS, ANI, TH, ADD, R>(F, F.nx, F.ny, F.nz, x, y, z, i, sx, sy, sz, ax, ay, az, ox, oy, oz);
 }
 
 // ------------------------------------------------------------------ fused x pass of a step
@@ -1392,34 +1392,35 @@ static cudaError_t cfg_xs()
     return cudaSuccess;
 }
 
-template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-static void fused_t(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R>
+static void fused_t(const FastKT<R>& F, const R* s[3], const R* a[3], R* o[3], cudaStream_t st)
 {
     dim3 blk(32, 8, 1);
     dim3 grid((F.nx + 31) / 32, (F.ny + 7) / 8, F.nz);
-    k_fused_fast<LT, EXS, ANI, TH, ADD><<<grid, blk, 0, st>>>(F, s[0], s[1], s[2], a[0], a[1], a[2], o[0], o[1], o[2]);
+    k_fused_fast<LT, EXS, ANI, TH, ADD, R><<<grid, blk, 0, st>>>(F, s[0], s[1], s[2], a[0], a[1], a[2], o[0], o[1],
+                                                                 o[2]);
 }
 
-template <int LT, bool EXS, bool ANI, bool TH>
-static void fused_add(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+template <int LT, bool EXS, bool ANI, bool TH, typename R>
+static void fused_add(const FastKT<R>& F, const R* s[3], const R* a[3], R* o[3], cudaStream_t st)
 {
     if (a[0]) fused_t<LT, EXS, ANI, TH, true>(F, s, a, o, st);
     else fused_t<LT, EXS, ANI, TH, false>(F, s, a, o, st);
 }
-template <int LT, bool EXS, bool ANI>
-static void fused_th(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+template <int LT, bool EXS, bool ANI, typename R>
+static void fused_th(const FastKT<R>& F, const R* s[3], const R* a[3], R* o[3], cudaStream_t st)
 {
     if (F.th) fused_add<LT, EXS, ANI, true>(F, s, a, o, st);
     else fused_add<LT, EXS, ANI, false>(F, s, a, o, st);
 }
-template <int LT, bool EXS>
-static void fused_ani(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+template <int LT, bool EXS, typename R>
+static void fused_ani(const FastKT<R>& F, const R* s[3], const R* a[3], R* o[3], cudaStream_t st)
 {
     if (F.ani) fused_th<LT, EXS, true>(F, s, a, o, st);
     else fused_th<LT, EXS, false>(F, s, a, o, st);
 }
-template <int LT>
-static void fused_ex(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+template <int LT, typename R>
+static void fused_ex(const FastKT<R>& F, const R* s[3], const R* a[3], R* o[3], cudaStream_t st)
 {
     if (F.ex) fused_ani<LT, true>(F, s, a, o, st);
     else fused_ani<LT, false>(F, s, a, o, st);
@@ -1471,6 +1472,15 @@ cudaError_t launch_ens_moments(const int4* rinfo, int nrep, const float* s[3], d
 }
 
 cudaError_t launch_fused_fast(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
+{
+    Prof pf("k_fused_step", st);
+    if (F.llg_type == LLG_CART) fused_ex<LLG_CART>(F, s, a, o, st);
+    else fused_ex<LLG_QUAT>(F, s, a, o, st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fused_fast_f64(const FastKT<double>& F, const double* s[3], const double* a[3], double* o[3],
+                                  cudaStream_t st)
 {
     Prof pf("k_fused_step", st);
     if (F.llg_type == LLG_CART) fused_ex<LLG_CART>(F, s, a, o, st);

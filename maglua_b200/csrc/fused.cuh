@@ -10,11 +10,12 @@
 
 // The step block's per-step values (swept field, thermal counter) read once
 // per thread instead of once per site: the same values, so the same results.
-__device__ __forceinline__ FastK fastk_resolved(const FastK& F)
+template <typename R>
+__device__ __forceinline__ FastKT<R> fastk_resolved(const FastKT<R>& F)
 {
-    FastK G = F;
+    FastKT<R> G = F;
     if (F.Bdev) {
-        G.B[0] = (float)F.Bdev[0]; G.B[1] = (float)F.Bdev[1]; G.B[2] = (float)F.Bdev[2];
+        G.B[0] = (R)F.Bdev[0]; G.B[1] = (R)F.Bdev[1]; G.B[2] = (R)F.Bdev[2];
         G.Bdev = nullptr;
     }
     if (F.dctr) {
@@ -57,21 +58,26 @@ __device__ __forceinline__ void cubic_field(R sx, R sy, R sz, const R* n, const 
 // arrays back to back.
 // The new spin of the site is returned in (rx, ry, rz); (Ax, Ay, Az) is the
 // materialised addend (the dipole slot), used when ADD.
-template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int NZ, int x, int y, int z, int i,
-                                             const float* __restrict__ sx, const float* __restrict__ sy,
-                                             const float* __restrict__ sz, float Ax, float Ay, float Az, float& rx,
-                                             float& ry, float& rz)
+// reciprocal square root and sine/cosine in the state precision
+__device__ __forceinline__ float fs_rsqrt(float v) { return rsqrtf(v); }
+__device__ __forceinline__ double fs_rsqrt(double v) { return rsqrt(v); }
+__device__ __forceinline__ void fs_sincos(float a, float* s, float* c) { sincosf(a, s, c); }
+__device__ __forceinline__ void fs_sincos(double a, double* s, double* c) { sincos(a, s, c); }
+
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R = float>
+__device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                             const R* __restrict__ sx, const R* __restrict__ sy,
+                                             const R* __restrict__ sz, R Ax, R Ay, R Az, R& rx, R& ry, R& rz)
 {
     const int nxy = NX * NY;
-    const float Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
-    float Hx, Hy, Hz;
-    if (F.Bdev) { Hx = (float)F.Bdev[0]; Hy = (float)F.Bdev[1]; Hz = (float)F.Bdev[2]; }
+    const R Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
+    R Hx, Hy, Hz;
+    if (F.Bdev) { Hx = (R)F.Bdev[0]; Hy = (R)F.Bdev[1]; Hz = (R)F.Bdev[2]; }
     else { Hx = F.B[0]; Hy = F.B[1]; Hz = F.B[2]; }
     if (EXS) {
-        float ex = 0.f, ey = 0.f, ez = 0.f;
+        R ex = 0, ey = 0, ez = 0;
 #define MLB_NB(cond, wrapcond, off, woff, J)                                                       \
-        if ((J) != 0.f) {                                                                          \
+        if ((J) != (R)0) {                                                                         \
             int f = -1;                                                                            \
             if (cond) f = i + (off);                                                               \
             else if (wrapcond) f = i + (woff);                                                     \
@@ -91,16 +97,16 @@ __device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int
     if (ANI) {
         if (F.ani == 2) {
             // one uniform cubic axis set
-            float cx, cy, cz;
-            cubic_field<float>(Sx * F.cub_ims, Sy * F.cub_ims, Sz * F.cub_ims, F.cub_n, F.cub_K, F.cub_quirk, cx,
-                               cy, cz);
+            R cx, cy, cz;
+            cubic_field<R>(Sx * F.cub_ims, Sy * F.cub_ims, Sz * F.cub_ims, F.cub_n, F.cub_K, F.cub_quirk, cx, cy,
+                           cz);
             Hx += cx; Hy += cy; Hz += cz;
         } else {
-            const float v = F.ani_c * (Sx * F.axis[0] + Sy * F.axis[1] + Sz * F.axis[2]);
+            const R v = F.ani_c * (Sx * F.axis[0] + Sy * F.axis[1] + Sz * F.axis[2]);
             Hx += v * F.axis[0]; Hy += v * F.axis[1]; Hz += v * F.axis[2];
         }
     }
-    float Tx = 0.f, Ty = 0.f, Tz = 0.f;
+    R Tx = 0, Ty = 0, Tz = 0;
     if (TH) {
         const uint64_t ctr = F.counter + (F.dctr ? *F.dctr : 0ull);
         const float3 nrm = philox_normal3(F.seed, ctr, (uint32_t)i, 0x6d6c6232u);
@@ -110,60 +116,61 @@ __device__ __forceinline__ void fused_site_v(const FastK& F, int NX, int NY, int
     if (ADD) {
         Hx += F.addw * Ax; Hy += F.addw * Ay; Hz += F.addw * Az;
     }
-    float nx_, ny_, nz_;
+    R nx_, ny_, nz_;
     if (LT == LLG_CART) {
         if (F.dt_zero) { nx_ = Sx; ny_ = Sy; nz_ = Sz; }
         else {
             // h = H - Hth; dM = -p gaa M x H - d (a/ms) gaa M x (M x h)
-            const float hx = F.tof ? Hx - Tx : Hx, hy = F.tof ? Hy - Ty : Hy, hz = F.tof ? Hz - Tz : Hz;
-            const float mhx = Sy * hz - Sz * hy, mhy = Sz * hx - Sx * hz, mhz = Sx * hy - Sy * hx;
-            const float mmx = Sy * mhz - Sz * mhy, mmy = Sz * mhx - Sx * mhz, mmz = Sx * mhy - Sy * mhx;
-            const float MHx = Sy * Hz - Sz * Hy, MHy = Sz * Hx - Sx * Hz, MHz = Sx * Hy - Sy * Hx;
+            const R hx = F.tof ? Hx - Tx : Hx, hy = F.tof ? Hy - Ty : Hy, hz = F.tof ? Hz - Tz : Hz;
+            const R mhx = Sy * hz - Sz * hy, mhy = Sz * hx - Sx * hz, mhz = Sx * hy - Sy * hx;
+            const R mmx = Sy * mhz - Sz * mhy, mmy = Sz * mhx - Sx * mhz, mmz = Sx * mhy - Sy * mhx;
+            const R MHx = Sy * Hz - Sz * Hy, MHy = Sz * Hx - Sx * Hz, MHz = Sx * Hy - Sy * Hx;
             nx_ = Sx + F.dt * (F.c_prec * MHx - F.c_damp * mmx);
             ny_ = Sy + F.dt * (F.c_prec * MHy - F.c_damp * mmy);
             nz_ = Sz + F.dt * (F.c_prec * MHz - F.c_damp * mmz);
         }
     } else {
-        float Hpx, Hpy, Hpz;
+        R Hpx, Hpy, Hpz;
         if (F.tof) {
-            const float hx = Hx - Tx, hy = Hy - Ty, hz = Hz - Tz;
-            const float shx = Sy * hz - Sz * hy, shy = Sz * hx - Sx * hz, shz = Sx * hy - Sy * hx;
+            const R hx = Hx - Tx, hy = Hy - Ty, hz = Hz - Tz;
+            const R shx = Sy * hz - Sz * hy, shy = Sz * hx - Sx * hz, shz = Sx * hy - Sy * hx;
             Hpx = F.precess * Hx + F.c_damp * shx;
             Hpy = F.precess * Hy + F.c_damp * shy;
             Hpz = F.precess * Hz + F.c_damp * shz;
         } else {
-            const float shx = Sy * Hz - Sz * Hy, shy = Sz * Hx - Sx * Hz, shz = Sx * Hy - Sy * Hx;
+            const R shx = Sy * Hz - Sz * Hy, shy = Sz * Hx - Sx * Hz, shz = Sx * Hy - Sy * Hx;
             Hpx = Hx + F.c_damp * shx; Hpy = Hy + F.c_damp * shy; Hpz = Hz + F.c_damp * shz;
         }
-        const float HL2 = Hpx * Hpx + Hpy * Hpy + Hpz * Hpz;
-        if (HL2 > 0.f) {
-            const float iHL = rsqrtf(HL2);
-            const float HL = HL2 * iHL;
-            // half rotation angle; small angles by their Taylor series
-            // (|th| <= 0.1: truncation below 1e-10), else sincosf
-            const float th = F.c_rot * HL;
-            float sn, cs;
-            if (fabsf(th) <= 0.1f) {
-                const float t2 = th * th;
+        const R HL2 = Hpx * Hpx + Hpy * Hpy + Hpz * Hpz;
+        if (HL2 > (R)0) {
+            const R iHL = fs_rsqrt(HL2);
+            const R HL = HL2 * iHL;
+            // half rotation angle; in FP32 small angles by their Taylor
+            // series (|th| <= 0.1: truncation below 1e-10, under FP32
+            // rounding), else (and always in FP64) sine and cosine
+            const R th = F.c_rot * HL;
+            R sn, cs;
+            if (sizeof(R) == 4 && fabs(th) <= (R)0.1) {
+                const R t2 = th * th;
                 sn = th * (1.0f - t2 * (1.0f / 6.0f) * (1.0f - t2 * (1.0f / 20.0f) * (1.0f - t2 * (1.0f / 42.0f))));
                 cs = 1.0f - t2 * 0.5f * (1.0f - t2 * (1.0f / 12.0f) * (1.0f - t2 * (1.0f / 30.0f) * (1.0f - t2 * (1.0f / 56.0f))));
             } else {
-                sincosf(th, &sn, &cs);
+                fs_sincos(th, &sn, &cs);
             }
-            const float qw = cs, qx = sn * Hpx * iHL, qy = sn * Hpy * iHL, qz = sn * Hpz * iHL;
-            const float tw = -qx * Sx - qy * Sy - qz * Sz;
-            const float tx = qw * Sx + qy * Sz - qz * Sy;
-            const float ty = qw * Sy + qz * Sx - qx * Sz;
-            const float tz = qw * Sz + qx * Sy - qy * Sx;
+            const R qw = cs, qx = sn * Hpx * iHL, qy = sn * Hpy * iHL, qz = sn * Hpz * iHL;
+            const R tw = -qx * Sx - qy * Sy - qz * Sz;
+            const R tx = qw * Sx + qy * Sz - qz * Sy;
+            const R ty = qw * Sy + qz * Sx - qx * Sz;
+            const R tz = qw * Sz + qx * Sy - qy * Sx;
             nx_ = -tw * qx + qw * tx - ty * qz + tz * qy;
             ny_ = -tw * qy + qw * ty - tz * qx + tx * qz;
             nz_ = -tw * qz + qw * tz - tx * qy + ty * qx;
         } else { nx_ = Sx; ny_ = Sy; nz_ = Sz; }
     }
     if (F.renorm) {
-        const float mm = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
-        if (mm != 0.f) {
-            const float inv = F.ms * rsqrtf(mm);
+        const R mm = nx_ * nx_ + ny_ * ny_ + nz_ * nz_;
+        if (mm != (R)0) {
+            const R inv = F.ms * fs_rsqrt(mm);
             nx_ *= inv; ny_ *= inv; nz_ *= inv;
         }
     }

@@ -147,28 +147,31 @@ struct LR2DScale {
 
 // Fused step for uniform-parameter systems (k_fused_fast): every constant
 // folded on the host.
-struct FastK {
+template <typename R>
+struct FastKT {
     int nx, ny, nz;
     int ex;                   // six-direction stencil present
-    float J[6];               // J * scale / ms^2 (normalised) or / ms
+    R J[6];                   // J * scale / ms^2 (normalised) or / ms
     int pbc[3];
     int ani;                  // 0 none, 1 uniaxial (axis, ani_c), 2 cubic (cub_*)
-    float axis[3];
-    float ani_c;              // 2 K scale / ms^2
-    float cub_n[9];           // cubic axes n1, n2, n3
-    float cub_K[3];           // cubic K1, K2, K3 (times the global scale)
+    R axis[3];
+    R ani_c;                  // 2 K scale / ms^2
+    R cub_n[9];               // cubic axes n1, n2, n3
+    R cub_K[3];               // cubic K1, K2, K3 (times the global scale)
     int cub_quirk;
-    float cub_ims;            // 1 / ms (the reduced moment S / ms)
+    R cub_ims;                // 1 / ms (the reduced moment S / ms)
     int th;
-    float sigma;              // sqrt(2 alpha T scale / (ms dt gamma))
+    R sigma;                  // sqrt(2 alpha T scale / (ms dt gamma))
     uint64_t seed, counter;
     const uint64_t* dctr;
-    float B[3];               // Zeeman (Bdev when read from the device step block)
+    R B[3];                   // Zeeman (Bdev when read from the device step block)
     const double* Bdev;
-    float addw;
+    R addw;
     int llg_type, tof, renorm, dt_zero;
-    float dt, precess, c_prec, c_damp, c_rot, ms;
+    R dt, precess, c_prec, c_damp, c_rot, ms;
 };
+// FP32 state (every fused kernel); FastKT<double> for FP64 state
+typedef FastKT<float> FastK;
 
 // ------------------------------------------------------------- learned surrogate
 // Linear spectral-conv network on the in-plane grid (ny x nx) with the

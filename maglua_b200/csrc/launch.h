@@ -95,6 +95,9 @@ bool xstep_ok(const ConvK& c, const FastK& F);
 cudaError_t launch_xstep(const ConvK& c, const FftLen L[3], const float2* tw, float2* spec, const FastK& F,
                          bool fwd, const float* s[3], float* h[3], float* o[3], cudaStream_t st);
 cudaError_t launch_fused_fast(const FastK& F, const float* s[3], const float* a[3], float* o[3], cudaStream_t st);
+// the same for FP64 state (constants in double)
+cudaError_t launch_fused_fast_f64(const FastKT<double>& F, const double* s[3], const double* a[3], double* o[3],
+                                  cudaStream_t st);
 cudaError_t launch_fused_ens(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3],
                              cudaStream_t st);
 cudaError_t launch_ens_moments(const int4* rinfo, int nrep, const float* s[3], double* out, cudaStream_t st);
