@@ -541,7 +541,17 @@ def main():
                     help="profiling driver: this many Dipole2D evaluations on the 256x256x8 film and exit")
     ap.add_argument("--ncu-ewald", type=int, default=0,
                     help="profiling driver: the Ewald tensor of an edge^3 simple-cubic lattice (NSites 10) and exit")
+    ap.add_argument("--ncu-f64", type=int, default=0,
+                    help="profiling driver: this many eager steps of the 256x256x8 film in FP64 and exit")
     args = ap.parse_args()
+    if args.ncu_f64:
+        import maglua_b200 as M
+        M.init(int(os.environ.get("LOCAL_RANK", "0")))
+        ss, ops, llg = build_system(M, 0, precision="f64")
+        for _ in range(args.ncu_f64):
+            M.run(ss, ops, llg, 1)
+        ss.synchronize()
+        return
     if args.ncu_lr2d or args.ncu_ewald:
         import maglua_b200 as M
         M.init(int(os.environ.get("LOCAL_RANK", "0")))
