@@ -592,10 +592,13 @@ ENSEMBLES = {
     "small": [(16, 16, 4), (8, 8, 2), (32, 16, 1), (16, 16, 4), (8, 8, 2)],
     # the benchmark's size classes (planes 32 to 128 wide, z padded to 4..32)
     "classes": [(32, 32, 4), (48, 48, 2), (64, 64, 4), (16, 16, 16), (48, 48, 2), (64, 64, 4), (32, 32, 4)],
+    # several replicas of a class whose z pads to 32 (the register split passes with replicas)
+    "cubes": [(16, 16, 16), (16, 16, 16), (32, 32, 4), (16, 16, 16)],
 }
 
 
-@pytest.mark.parametrize("llg,which", [("Cartesian", "small"), ("Quaternion", "small"), ("Quaternion", "classes")])
+@pytest.mark.parametrize("llg,which", [("Cartesian", "small"), ("Quaternion", "small"), ("Quaternion", "classes"),
+                                       ("Cartesian", "cubes")])
 def test_ensemble_matches_single_systems(M, llg, which):
     dims = ENSEMBLES[which]
     cfg = dict(alpha=0.1, dt=0.01, pbc=(0, 0, 0), K=0.2, axis=(0, 0, 1.0), B=(0.0, 0.05, -0.1),
