@@ -7,8 +7,7 @@ builder reproduces it with truncation 20 on every axis.  Its values carry
 the sign of a makeData that added +N; the current makeData
 (mag2d_luafuncs.lua:719-729) adds -N.
 
-Run from the repository root with the reference tree at ../reference or
-REFERENCE=<path>."""
+Reads the reference tree at /root/reference, or at REFERENCE=<path>."""
 import json
 import os
 import re
