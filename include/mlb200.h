@@ -128,6 +128,15 @@ int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields);
 /* diff (spinsystem.cpp:301-307, l_getdiff :2145-2160): sum_i |a_i - b_i| of
  * each component and the length of that vector, FP64. */
 int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4]);
+/* encode / decode (SpinSystem::encode / decode, spinsystem.cpp:669-851, as
+ * exported as a Lua value, luamigrate.cpp:265-275): the byte stream the
+ * reference's CPU build writes for a SpinSystem inside a checkpoint, so that
+ * either side reads the other's.  encode writes it into buf when cap holds
+ * it (*len = its size; buf == NULL asks for the size alone).  decode makes a
+ * new system of that state with real_bytes 4 or 8; streams whose sites
+ * carry extra data (Lua values) give MLB_EUNSUP. */
+int mlb_system_encode(mlb_system* s, void* buf, size_t cap, size_t* len);
+int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** out);
 
 /* ---------------------------------------------------------------- operators
  * SpinOperation base, M/cpu/core/spinoperation.h:28-72. */

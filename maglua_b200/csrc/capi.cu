@@ -2757,6 +2757,214 @@ int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4])
     return guard([&] { system_diff(a, b, out4); });
 }
 
+// ---------------------------------------------------------------- encode / decode
+// The LuaBaseObject byte stream of a SpinSystem as the reference's CPU build
+// writes it (SpinSystem::encode / decode, spinsystem.cpp:669-851; the
+// primitives, luabaseobject.cpp:142-205 and 250-360; an object exported as a
+// Lua value, luamigrate.cpp:75-76 and 265-275): native-endian int32, double
+// and char, no padding.  An object is LUA_TUSERDATA (7), its type id, char
+// 111 and its index in the stream's object list (or char 222 and the index
+// of an object written before), then its fields.
+namespace {
+
+const int kLuaNil = 0;
+const int kLuaUserdata = 7;
+const signed char kEncNew = 111;
+const signed char kEncOld = (signed char)222;
+
+// hash32 (factory.cpp:123-131): MurmurHash3 x86_32 (Austin Appleby's
+// published algorithm) of the type name with seed 1000, in the reference's
+// form: its tail block rotates by 16 bits where the published one rotates by
+// 15 (MurmurHash3.cpp:137-143).  Kept so that type ids match its streams.
+int32_t type_id(const char* name)
+{
+    const uint32_t c1 = 0xcc9e2d51u, c2 = 0x1b873593u;
+    auto rotl = [](uint32_t x, int r) { return (x << r) | (x >> (32 - r)); };
+    const size_t len = std::strlen(name);
+    const unsigned char* d = reinterpret_cast<const unsigned char*>(name);
+    uint32_t h = 1000;
+    const size_t nb = len / 4;
+    for (size_t i = 0; i < nb; i++) {
+        uint32_t k = (uint32_t)d[4 * i] | ((uint32_t)d[4 * i + 1] << 8) | ((uint32_t)d[4 * i + 2] << 16) |
+                     ((uint32_t)d[4 * i + 3] << 24);
+        k = rotl(k * c1, 15) * c2;
+        h = rotl(h ^ k, 13) * 5 + 0xe6546b64u;
+    }
+    const unsigned char* t = d + 4 * nb;
+    uint32_t k = 0;
+    switch (len & 3) {
+    case 3: k ^= (uint32_t)t[2] << 16; [[fallthrough]];
+    case 2: k ^= (uint32_t)t[1] << 8; [[fallthrough]];
+    case 1:
+        k ^= t[0];
+        k = rotl(k * c1, 16) * c2;
+        h ^= k;
+    }
+    h ^= (uint32_t)len;
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return (int32_t)h;
+}
+
+struct StreamOut {
+    std::vector<char> b;
+    void put(const void* p, size_t n) { b.insert(b.end(), (const char*)p, (const char*)p + n); }
+    void i32(int32_t v) { put(&v, 4); }
+    void f64(double v) { put(&v, 8); }
+    void ch(signed char v) { put(&v, 1); }
+    void header(const char* type, int idx) { i32(kLuaUserdata); i32(type_id(type)); ch(kEncNew); i32(idx); }
+    // Array<double>::encode (M/cpu/array/array_core_cpu.h:200-225): version
+    // 0, the size, then flag 1 and one value when every value compares
+    // equal, else flag 0 and all of them.
+    void darray(int idx, const mlb_system* s, const std::vector<double>& a)
+    {
+        header("Array.Double", idx);
+        ch(0);
+        i32(s->nx); i32(s->ny); i32(s->nz);
+        bool same = true;
+        for (int i = 1; i < s->n && same; i++) same = (a[i] == a[0]);
+        if (same) { i32(1); f64(a[0]); }
+        else { i32(0); put(a.data(), sizeof(double) * a.size()); }
+    }
+};
+
+struct StreamIn {
+    const char* p;
+    size_t len, pos = 0;
+    void take(void* d, size_t n)
+    {
+        if (n > len - pos) fail(MLB_EINVAL, "malformed stream: ends early");
+        std::memcpy(d, p + pos, n);
+        pos += n;
+    }
+    int32_t i32() { int32_t v; take(&v, 4); return v; }
+    double f64() { double v; take(&v, 8); return v; }
+    signed char ch() { signed char v; take(&v, 1); return v; }
+};
+
+// decodeLuaBaseObject (luabaseobject.cpp:307-360) of an Array.Double of the
+// system's size; an old-object entry refers to one decoded before.
+std::vector<double> read_darray(StreamIn& in, int nx, int ny, int nz, std::map<int, std::vector<double>>& seen)
+{
+    if (in.i32() != kLuaUserdata) fail(MLB_EINVAL, "malformed stream: expected an object");
+    if (in.i32() != type_id("Array.Double")) fail(MLB_EUNSUP, "array type other than Array.Double");
+    const signed char magic = in.ch();
+    const int idx = in.i32();
+    if (magic == kEncOld) {
+        auto it = seen.find(idx);
+        if (it == seen.end()) fail(MLB_EINVAL, "malformed stream: unknown object index");
+        return it->second;
+    }
+    if (magic != kEncNew) fail(MLB_EINVAL, "malformed stream: bad object flag");
+    if (in.ch() != 0) fail(MLB_EUNSUP, "unknown Array version");
+    const int x = in.i32(), y = in.i32(), z = in.i32();
+    if (x != nx || y != ny || z != nz) fail(MLB_EINVAL, "array size differs from the system's");
+    const size_t n = (size_t)nx * ny * nz;
+    std::vector<double> a(n);
+    const int flag = in.i32();
+    if (flag == 1) {
+        const double v = in.f64();
+        std::fill(a.begin(), a.end(), v);
+    } else if (flag == 0) {
+        in.take(a.data(), sizeof(double) * n);
+    } else {
+        fail(MLB_EINVAL, "malformed stream: bad array flag");
+    }
+    seen[idx] = a;
+    return a;
+}
+
+}  // namespace
+
+int mlb_system_encode(mlb_system* s, void* buf, size_t cap, size_t* len)
+{
+    return guard([&] {
+        if (!s || !len) fail(MLB_EINVAL, "null argument");
+        if (s->capturing) fail(MLB_ESTATE, "encode during capture");
+        std::vector<double> a[4];
+        for (int c = 0; c < 3; c++) {
+            a[c].resize(s->n);
+            get_reals(s, a[c].data(), s->sp[s->cur][c], s->n);
+        }
+        a[3] = s->ms_host;
+        StreamOut o;
+        o.header("SpinSystem", 0);
+        o.ch(0);
+        o.i32(s->nx); o.i32(s->ny); o.i32(s->nz);
+        o.f64(s->alpha); o.f64(s->dt); o.f64(s->gamma); o.f64(s->time);
+        int idx = 1;
+        for (int c = 0; c < 4; c++) o.darray(idx++, s, a[c]);
+        for (void* site : {s->sa, s->sg}) {
+            o.i32(site ? 1 : 0);
+            if (!site) continue;
+            std::vector<double> v(s->n);
+            get_reals(s, v.data(), site, s->n);
+            o.darray(idx++, s, v);
+        }
+        o.i32(0);   // no site carries extra data
+        *len = o.b.size();
+        if (!buf) return;
+        if (cap < o.b.size()) fail(MLB_EINVAL, "buffer smaller than the stream");
+        std::memcpy(buf, o.b.data(), o.b.size());
+    });
+}
+
+int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** out)
+{
+    return guard([&] {
+        if (!buf || !out) fail(MLB_EINVAL, "null argument");
+        *out = nullptr;
+        StreamIn in{static_cast<const char*>(buf), len};
+        if (in.i32() != kLuaUserdata) fail(MLB_EINVAL, "malformed stream: expected an object");
+        if (in.i32() != type_id("SpinSystem")) fail(MLB_EINVAL, "stream does not hold a SpinSystem");
+        if (in.ch() != kEncNew) fail(MLB_EINVAL, "malformed stream: bad object flag");
+        in.i32();
+        if (in.ch() != 0) fail(MLB_EUNSUP, "unknown SpinSystem version");
+        const int nx = in.i32(), ny = in.i32(), nz = in.i32();
+        if (nx <= 0 || ny <= 0 || nz <= 0) fail(MLB_EINVAL, "malformed stream: bad system size");
+        if ((long long)nx * ny * nz > (1LL << 31) - 1) fail(MLB_EUNSUP, "more than 2^31-1 sites");
+        const double alpha = in.f64(), dt = in.f64(), gamma = in.f64(), time = in.f64();
+        std::map<int, std::vector<double>> seen;
+        std::vector<double> a[4];
+        for (int c = 0; c < 4; c++) a[c] = read_darray(in, nx, ny, nz, seen);
+        std::vector<double> site[2];
+        bool has[2] = {false, false};
+        for (int k = 0; k < 2; k++) {
+            has[k] = in.i32() != 0;
+            if (has[k]) site[k] = read_darray(in, nx, ny, nz, seen);
+        }
+        // sites' extra data: Lua values, which this library does not hold;
+        // a stream whose every site has nil is accepted
+        const int nextra = in.i32();
+        if (nextra > 0) fail(MLB_EUNSUP, "sites carry extra data (Lua values)");
+        if (nextra < 0)
+            for (long long i = 0; i < (long long)nx * ny * nz; i++)
+                if (in.i32() != kLuaNil) fail(MLB_EUNSUP, "sites carry extra data (Lua values)");
+        if (in.pos != in.len) fail(MLB_EINVAL, "malformed stream: trailing bytes");
+        mlb_system* s = make_system(nx, ny, nz, real_bytes);
+        try {
+            s->alpha = alpha; s->dt = dt; s->gamma = gamma; s->time = time;
+            const double* src[3] = {a[0].data(), a[1].data(), a[2].data()};
+            for (int c = 0; c < 3; c++) put_reals(s, s->sp[s->cur][c], src[c], s->n);
+            for (int i = 0; i < s->n; i++) s->ms_host[i] = a[3][i];
+            put_reals(s, s->ms, s->ms_host.data(), s->n);
+            for (int i = 0; i < s->n; i++) s->ms_host[i] = round_to(s->ms_host[i], s->rb);
+            s->ms_dirty = true;
+            s->ms_token = ++g_ms_token;
+            if (has[0]) upload_site_array(s, &s->sa, site[0].data());
+            if (has[1]) upload_site_array(s, &s->sg, site[1].data());
+            CK(cudaStreamSynchronize(s->st));
+        } catch (...) {
+            mlb_system_destroy(s);
+            throw;
+        }
+        *out = s;
+    });
+}
+
 int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
 {
     return guard([&] {

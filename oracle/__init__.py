@@ -686,6 +686,156 @@ def ewald_find_eta(g, r3, N, tol=1e-3):
     return rec(100, a, F(a), b, F(b), c, F(c))
 
 
+# ------------------------------------------------------------ SpinSystem encode
+# The LuaBaseObject byte stream (M/common/luabaseobject/luabaseobject.cpp:
+# 142-205, 250-360): native-endian int32, double and char with no padding;
+# an object is LUA_TUSERDATA (7), its type id, then its own encode, which
+# opens with ENCODE_PREAMBLE: char 111 (new) and its index in the stream's
+# object list, or char 222 (seen before) and that index.
+
+LUA_TUSERDATA = 7
+LUA_TNIL = 0
+ENC_NEW = 111
+ENC_OLD = 222
+
+
+def type_hash32(name):
+    """hash32 (M/common/luabaseobject/factory.cpp:123-131): MurmurHash3
+    x86_32 of the type name with seed 1000 as the reference wrote it
+    (MurmurHash3.cpp:101-155), whose tail block rotates by 16 where the
+    published algorithm rotates by 15; returned as a signed int."""
+    data = name.encode()
+    c1, c2, M = 0xCC9E2D51, 0x1B873593, 0xFFFFFFFF
+    rotl = lambda x, r: ((x << r) | (x >> (32 - r))) & M
+    h = 1000
+    nb = len(data) // 4
+    for i in range(nb):
+        k = int.from_bytes(data[4 * i:4 * i + 4], "little")
+        k = rotl((k * c1) & M, 15)
+        k = (k * c2) & M
+        h = rotl(h ^ k, 13)
+        h = (h * 5 + 0xE6546B64) & M
+    tail = data[4 * nb:]
+    k = 0
+    if len(tail) >= 3:
+        k ^= tail[2] << 16
+    if len(tail) >= 2:
+        k ^= tail[1] << 8
+    if len(tail) >= 1:
+        k ^= tail[0]
+        k = rotl((k * c1) & M, 16)
+        k = (k * c2) & M
+        h ^= k
+    h ^= len(data)
+    h ^= h >> 16
+    h = (h * 0x85EBCA6B) & M
+    h ^= h >> 13
+    h = (h * 0xC2B2AE35) & M
+    h ^= h >> 16
+    return h - (1 << 32) if h >= 1 << 31 else h
+
+
+def _enc_darray(out, idx, a, dims):
+    """encodeT<dArray> (luabaseobject.h:101-106) of Array<double>::encode
+    (M/cpu/array/array_core_cpu.h:200-225): version 0, nx, ny, nz, then flag
+    1 and one double when every value compares equal, else flag 0 and the
+    values in site order."""
+    import struct
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    out += struct.pack("=iibib", LUA_TUSERDATA, type_hash32("Array.Double"), ENC_NEW, idx, 0)
+    out += struct.pack("=iii", *dims)
+    if a.size and np.all(a == a[0]):
+        out += struct.pack("=id", 1, float(a[0]))
+    else:
+        out += struct.pack("=i", 0) + a.tobytes()
+
+
+def encode_spinsystem(nx, ny, nz, alpha, dt, gamma, time, x, y, z, ms, site_alpha=None,
+                      site_gamma=None):
+    """SpinSystem::encode (M/cpu/core/spinsystem.cpp:669-757) as exported as a
+    Lua value (luamigrate.cpp:75-76, 265-275): the system's header, version 0,
+    nx, ny, nz, alpha, dt, gamma, time, the arrays x, y, z, ms, the flag and
+    array of per-site alpha, then of per-site gamma, and the count of sites
+    with extra data (0: none)."""
+    import struct
+    out = bytearray()
+    out += struct.pack("=iibib", LUA_TUSERDATA, type_hash32("SpinSystem"), ENC_NEW, 0, 0)
+    out += struct.pack("=iii", nx, ny, nz)
+    out += struct.pack("=dddd", alpha, dt, gamma, time)
+    dims = (nx, ny, nz)
+    idx = 1
+    for a in (x, y, z, ms):
+        _enc_darray(out, idx, a, dims)
+        idx += 1
+    for a in (site_alpha, site_gamma):
+        out += struct.pack("=i", 0 if a is None else 1)
+        if a is not None:
+            _enc_darray(out, idx, a, dims)
+            idx += 1
+    out += struct.pack("=i", 0)
+    return bytes(out)
+
+
+def decode_spinsystem(buf):
+    """SpinSystem::decode (spinsystem.cpp:759-851) of a stream that
+    encode_spinsystem writes, or that has sites' extra data all nil; returns
+    a dict of the scalars and arrays (site_alpha / site_gamma None when
+    absent)."""
+    import struct
+    pos = 0
+
+    def take(fmt):
+        nonlocal pos
+        v = struct.unpack_from("=" + fmt, buf, pos)
+        pos += struct.calcsize("=" + fmt)
+        return v
+
+    objs = {}
+    t, ty, magic, idx = take("iibi")
+    assert t == LUA_TUSERDATA and ty == type_hash32("SpinSystem") and magic == ENC_NEW
+    (ver,) = take("b")
+    assert ver == 0
+    nx, ny, nz = take("iii")
+    alpha, dt, gamma, time = take("dddd")
+    n = nx * ny * nz
+
+    def arr():
+        nonlocal pos
+        t, ty, magic, idx = take("iibi")
+        assert t == LUA_TUSERDATA and ty == type_hash32("Array.Double")
+        if magic == ENC_OLD:
+            return objs[idx]
+        (ver,) = take("b")
+        assert ver == 0
+        dims = take("iii")
+        assert dims == (nx, ny, nz)
+        (flag,) = take("i")
+        if flag == 1:
+            (v,) = take("d")
+            a = np.full(n, v)
+        else:
+            a = np.frombuffer(buf, dtype=np.float64, count=n, offset=pos).copy()
+            pos += 8 * n
+        objs[idx] = a
+        return a
+
+    d = dict(nx=nx, ny=ny, nz=nz, alpha=alpha, dt=dt, gamma=gamma, time=time)
+    for k in ("x", "y", "z", "ms"):
+        d[k] = arr()
+    for k in ("site_alpha", "site_gamma"):
+        (e,) = take("i")
+        d[k] = arr() if e else None
+    (ne,) = take("i")
+    if ne < 0:
+        for _ in range(n):
+            (lt,) = take("i")
+            assert lt == LUA_TNIL
+    else:
+        assert ne == 0
+    assert pos == len(buf)
+    return d
+
+
 def fft1d(data, sign):
     d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128)).copy()
     lib.orc_fft1d(d.view(np.float64).ctypes.data_as(_D), len(d), 1, sign)

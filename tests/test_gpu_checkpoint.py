@@ -1,0 +1,144 @@
+"""SpinSystem encode / decode: the byte stream of the reference's CPU build
+(spinsystem.cpp:669-851, luabaseobject.cpp:142-360), compared byte for byte
+with the oracle's restatement, decoded back, and resumed from."""
+import struct
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import random_spins
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def M():
+    import maglua_b200 as M
+    M.init(0)
+    return M
+
+
+def _state(M, dims, precision, seed, uniform_ms=False, site=False):
+    n = int(np.prod(dims))
+    s = random_spins(n, seed)
+    r = np.random.default_rng(seed + 1)
+    ms = np.full(n, 1.5) if uniform_ms else 0.5 + r.random(n)
+    ss = M.SpinSystem(*dims, precision=precision)
+    ss.setSpinArrays(s[0] * ms, s[1] * ms, s[2] * ms, ms)
+    ss.setAlpha(0.125)
+    ss.setTimeStep(0.01)
+    ss.setGamma(1.75)
+    ss.setTime(3.5)
+    sa = sg = None
+    if site:
+        sa = 0.05 + 0.1 * r.random(n)
+        sg = 1.0 + r.random(n)
+        ss.setSiteAlphaArray(sa)
+        ss.setSiteGammaArray(sg)
+        if precision == "f32":
+            sa, sg = sa.astype(np.float32).astype(np.float64), sg.astype(np.float32).astype(np.float64)
+    return ss, sa, sg
+
+
+def _oracle_stream(ss, sa=None, sg=None):
+    x, y, z, ms = ss.spinArrays()
+    nx, ny, nz = ss._dims
+    return O.encode_spinsystem(nx, ny, nz, ss.alpha(), ss.timeStep(), ss.gamma(), ss.time(), x, y, z, ms, sa, sg)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("uniform_ms,site", [(False, False), (True, False), (False, True)])
+def test_encode_matches_the_oracle_bytes(M, precision, uniform_ms, site):
+    ss, sa, sg = _state(M, (12, 10, 3), precision, 11, uniform_ms, site)
+    got = ss.encode()
+    assert got == _oracle_stream(ss, sa, sg)
+    d = O.decode_spinsystem(got)
+    assert (d["nx"], d["ny"], d["nz"]) == (12, 10, 3)
+    assert (d["alpha"], d["dt"], d["gamma"], d["time"]) == (0.125, 0.01, 1.75, 3.5)
+    # one value for a uniform array (flag 1), else every site
+    n = 12 * 10 * 3
+    arrays = 6 if site else 4
+    full = arrays - (1 if uniform_ms else 0)
+    header = 4 + 4 + 1 + 4
+    arr_head = header + 1 + 12 + 4
+    expect = header + 1 + 12 + 32 + arrays * arr_head + full * 8 * n + (arrays - full) * 8 + 4 + 4 + 4
+    assert len(got) == expect
+
+
+def test_decode_restores_the_state_exactly(M):
+    n = 9 * 7 * 2
+    s = random_spins(n, 21)
+    r = np.random.default_rng(22)
+    ms = 0.5 + r.random(n)
+    sa = 0.02 + 0.1 * r.random(n)
+    data = O.encode_spinsystem(9, 7, 2, 0.3, 0.005, 1.1, 12.25, s[0] * ms, s[1] * ms, s[2] * ms, ms, sa, None)
+    ss = M.SpinSystem.decode(data, precision="f64")
+    assert ss._dims == (9, 7, 2)
+    assert (ss.alpha(), ss.timeStep(), ss.gamma(), ss.time()) == (0.3, 0.005, 1.1, 12.25)
+    x, y, z, m = ss.spinArrays()
+    assert np.array_equal(x, s[0] * ms) and np.array_equal(y, s[1] * ms) and np.array_equal(z, s[2] * ms)
+    assert np.array_equal(m, ms)
+    # decode then encode gives the same bytes back
+    assert ss.encode() == data
+    # into FP32 state: the values rounded to float
+    s32 = M.SpinSystem.decode(data, precision="f32")
+    assert np.array_equal(s32.spinArrays()[0], (s[0] * ms).astype(np.float32).astype(np.float64))
+
+
+def test_decode_accepts_all_nil_extra_data_and_refuses_values(M):
+    n = 4 * 4 * 1
+    s = random_spins(n, 31)
+    base = O.encode_spinsystem(4, 4, 1, 1.0, 0.01, 1.0, 0.0, s[0], s[1], s[2], np.ones(n))
+    # "all sites" form (-1) with nil at every site
+    nil_all = base[:-4] + struct.pack("=i", -1) + struct.pack("=%di" % n, *([O.LUA_TNIL] * n))
+    ss = M.SpinSystem.decode(nil_all, precision="f64")
+    assert np.array_equal(ss.spinArrays()[0], s[0])
+    # a site with a Lua number: not held by this library
+    one = base[:-4] + struct.pack("=ii", 1, 3) + struct.pack("=id", 3, 2.0)
+    with pytest.raises(M.MagLuaError, match="extra data"):
+        M.SpinSystem.decode(one)
+
+
+def test_decode_rejects_malformed_streams(M):
+    n = 3 * 3 * 1
+    s = random_spins(n, 41)
+    data = O.encode_spinsystem(3, 3, 1, 1.0, 0.01, 1.0, 0.0, s[0], s[1], s[2], np.ones(n))
+    with pytest.raises(M.MagLuaError, match="ends early"):
+        M.SpinSystem.decode(data[:-9])
+    with pytest.raises(M.MagLuaError, match="trailing"):
+        M.SpinSystem.decode(data + b"\0")
+    bad = bytearray(data)
+    bad[4:8] = struct.pack("=i", O.type_hash32("Array.Double"))
+    with pytest.raises(M.MagLuaError, match="SpinSystem"):
+        M.SpinSystem.decode(bytes(bad))
+
+
+def test_resume_from_a_checkpoint_follows_the_same_trajectory(M):
+    dims = (32, 32, 4)
+    n = int(np.prod(dims))
+    ss = M.SpinSystem(*dims, precision="f64")
+    ss.setSpinArrays(*random_spins(n, 51))
+    ss.setAlpha(0.1)
+    ss.setTimeStep(0.01)
+
+    f, t, j = O.nn_paths(*dims, J=1.0, pbc=(1, 1, 0))
+
+    def ops():
+        ex = M.Exchange(*dims)
+        ex.addPaths(f, t, j)
+        ani = M.Anisotropy(*dims)
+        ani.addMany(np.arange(n, dtype=np.int32), np.tile([0.0, 0.0, 1.0], (n, 1)), np.full(n, 0.2))
+        dip = M.Dipole(*dims)
+        dip.setStrength(0.05)
+        return [ex, ani, dip]
+
+    llg = M.LLG.new("Quaternion")
+    M.run(ss, ops(), llg, 10)
+    data = ss.encode()
+    resumed = M.SpinSystem.decode(data, precision="f64")
+    assert resumed.time() == ss.time()
+    M.run(ss, ops(), llg, 15)
+    M.run(resumed, ops(), llg, 15)
+    assert ss.diff(resumed)[3] == 0.0
+    assert resumed.time() == ss.time()

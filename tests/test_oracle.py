@@ -508,3 +508,36 @@ def test_ewald_library_host_path():
         assert b"AB pair" in lib.mlb_last_error()
     finally:
         lib.mlb_ewald3d_destroy(e)
+
+
+def test_type_ids_against_the_reference_murmur():
+    """The oracle's hash32 against the ids the reference's own MurmurHash3
+    (compiled from its source) gave for these names: every tail length."""
+    with open(os.path.join(GOLDEN, "type_hashes.json")) as f:
+        fx = json.load(f)
+    assert fx["seed"] == 1000
+    for name, v in fx["hash32"].items():
+        assert O.type_hash32(name) == v, name
+
+
+def test_spinsystem_stream_round_trip_on_the_oracle():
+    """encode_spinsystem / decode_spinsystem: the field order and sizes of
+    SpinSystem::encode (spinsystem.cpp:669-757) and Array<double>::encode."""
+    import struct
+    n = 5 * 4 * 3
+    s = random_spins(n, 61)
+    ms = np.full(n, 2.0)
+    sg = np.linspace(0.5, 1.5, n)
+    data = O.encode_spinsystem(5, 4, 3, 0.2, 0.01, 1.3, 7.0, s[0], s[1], s[2], ms, None, sg)
+    t, ty, magic, idx, ver = struct.unpack_from("=iibib", data, 0)
+    assert (t, ty, magic, idx, ver) == (7, O.type_hash32("SpinSystem"), 111, 0, 0)
+    assert struct.unpack_from("=iiidddd", data, 14) == (5, 4, 3, 0.2, 0.01, 1.3, 7.0)
+    # the x array follows: its own header, index 1, then flag 0 and n doubles
+    t, ty, magic, idx, ver, ax, ay, az, flag = struct.unpack_from("=iibibiiii", data, 58)
+    assert (t, ty, magic, idx, ver, (ax, ay, az), flag) == (7, O.type_hash32("Array.Double"), 111, 1, 0,
+                                                            (5, 4, 3), 0)
+    d = O.decode_spinsystem(data)
+    assert np.array_equal(d["x"], s[0]) and np.array_equal(d["ms"], ms)
+    assert d["site_alpha"] is None and np.array_equal(d["site_gamma"], sg)
+    # the uniform ms array is one value (flag 1)
+    assert len(data) == 13 + 1 + 12 + 32 + 5 * 30 + 4 * 8 * n + 8 + 12
