@@ -132,11 +132,19 @@ int mlb_system_diff(mlb_system* a, mlb_system* b, double out4[4]);
  * exported as a Lua value, luamigrate.cpp:265-275): the byte stream the
  * reference's CPU build writes for a SpinSystem inside a checkpoint, so that
  * either side reads the other's.  encode writes it into buf when cap holds
- * it (*len = its size; buf == NULL asks for the size alone).  decode makes a
- * new system of that state with real_bytes 4 or 8; streams whose sites
- * carry extra data (Lua values) give MLB_EUNSUP. */
-int mlb_system_encode(mlb_system* s, void* buf, size_t cap, size_t* len);
-int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** out);
+ * it (*len = its size; buf == NULL asks for the size alone); first_index is
+ * the object index the system takes in the stream (0 for a stream of its
+ * own, else the count of objects the enclosing buffer has encoded so far),
+ * its arrays take the next ones.  decode makes a new system of that state
+ * with real_bytes 4 or 8; with used != NULL the stream may continue after
+ * the system and *used = the bytes read, with used == NULL it must end
+ * there.  *objects (when not NULL) = the objects the stream holds: the
+ * system and its 4 to 6 arrays, each an entry of the enclosing buffer's
+ * object list.  Streams whose sites carry extra data (Lua values) give
+ * MLB_EUNSUP. */
+int mlb_system_encode(mlb_system* s, int first_index, void* buf, size_t cap, size_t* len, int* objects);
+int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** out, size_t* used,
+                      int* objects);
 
 /* ---------------------------------------------------------------- operators
  * SpinOperation base, M/cpu/core/spinoperation.h:28-72. */

@@ -174,8 +174,8 @@ _SIGS = {
     "mlb_adapt_step": ([_P, _I], C.c_int),
     "mlb_adapt_destroy": ([_P], C.c_int),
     "mlb_system_diff": ([_P, _P, _D], C.c_int),
-    "mlb_system_encode": ([_P, _P, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
-    "mlb_system_decode": ([_P, C.c_size_t, C.c_int, C.POINTER(_P)], C.c_int),
+    "mlb_system_encode": ([_P, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t), _I], C.c_int),
+    "mlb_system_decode": ([_P, C.c_size_t, C.c_int, C.POINTER(_P), C.POINTER(C.c_size_t), _I], C.c_int),
     "mlb_dipole_write_wab": ([_P, C.c_char_p], C.c_int),
     "mlb_dipole_read_wab": ([_P, C.c_char_p], C.c_int),
     "mlb_rk_destroy": ([_P], C.c_int),
@@ -546,34 +546,42 @@ class SpinSystem:
         self.copyTo(c)
         return c
 
-    def encode(self):
+    def encode(self, first_index=0):
         """The bytes SpinSystem::encode writes (spinsystem.cpp:669-757) for
         this state, with the object header of an exported Lua value
-        (luamigrate.cpp:265-275): what a checkpoint of the reference holds."""
+        (luamigrate.cpp:265-275): what a checkpoint of the reference holds.
+        first_index: the system's object index in the enclosing stream."""
         n = C.c_size_t()
-        _ck(_lib.mlb_system_encode(self._h, None, 0, C.byref(n)))
+        _ck(_lib.mlb_system_encode(self._h, int(first_index), None, 0, C.byref(n), None))
         buf = C.create_string_buffer(n.value)
-        _ck(_lib.mlb_system_encode(self._h, buf, n.value, C.byref(n)))
+        nobj = C.c_int()
+        _ck(_lib.mlb_system_encode(self._h, int(first_index), buf, n.value, C.byref(n), C.byref(nobj)))
+        self._stream_objects = nobj.value
         return buf.raw[:n.value]
 
     @classmethod
-    def decode(cls, data, precision="f32"):
+    def decode(cls, data, precision="f32", partial=False):
         """A new system from a stream written by encode or by the reference's
-        SpinSystem::encode (decode, spinsystem.cpp:759-851)."""
+        SpinSystem::encode (decode, spinsystem.cpp:759-851).  partial=True:
+        the stream may continue after the system; returns (system, bytes
+        read, objects read)."""
         _ensure_init()
         rb = {"f32": 4, "f64": 8}.get(precision)
         if rb is None:
             raise MagLuaError(-1, "precision must be 'f32' or 'f64'")
         data = bytes(data)
         h = _P()
-        _ck(_lib.mlb_system_decode(data, len(data), rb, C.byref(h)))
+        used = C.c_size_t()
+        nobj = C.c_int()
+        _ck(_lib.mlb_system_decode(data, len(data), rb, C.byref(h), C.byref(used) if partial else None,
+                                   C.byref(nobj)))
         obj = cls.__new__(cls)
         obj._h = h
         d = (C.c_int * 3)()
         _ck(_lib.mlb_system_dims(h, d))
         obj._dims = (d[0], d[1], d[2])
         obj._precision = precision
-        return obj
+        return (obj, used.value, nobj.value) if partial else obj
 
 
 def _slotname(x):

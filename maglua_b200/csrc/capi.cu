@@ -2879,10 +2879,11 @@ std::vector<double> read_darray(StreamIn& in, int nx, int ny, int nz, std::map<i
 
 }  // namespace
 
-int mlb_system_encode(mlb_system* s, void* buf, size_t cap, size_t* len)
+int mlb_system_encode(mlb_system* s, int first_index, void* buf, size_t cap, size_t* len, int* objects)
 {
     return guard([&] {
         if (!s || !len) fail(MLB_EINVAL, "null argument");
+        if (first_index < 0) fail(MLB_EINVAL, "negative object index");
         if (s->capturing) fail(MLB_ESTATE, "encode during capture");
         std::vector<double> a[4];
         for (int c = 0; c < 3; c++) {
@@ -2891,11 +2892,11 @@ int mlb_system_encode(mlb_system* s, void* buf, size_t cap, size_t* len)
         }
         a[3] = s->ms_host;
         StreamOut o;
-        o.header("SpinSystem", 0);
+        o.header("SpinSystem", first_index);
         o.ch(0);
         o.i32(s->nx); o.i32(s->ny); o.i32(s->nz);
         o.f64(s->alpha); o.f64(s->dt); o.f64(s->gamma); o.f64(s->time);
-        int idx = 1;
+        int idx = first_index + 1;
         for (int c = 0; c < 4; c++) o.darray(idx++, s, a[c]);
         for (void* site : {s->sa, s->sg}) {
             o.i32(site ? 1 : 0);
@@ -2906,13 +2907,14 @@ int mlb_system_encode(mlb_system* s, void* buf, size_t cap, size_t* len)
         }
         o.i32(0);   // no site carries extra data
         *len = o.b.size();
+        if (objects) *objects = idx - first_index;
         if (!buf) return;
         if (cap < o.b.size()) fail(MLB_EINVAL, "buffer smaller than the stream");
         std::memcpy(buf, o.b.data(), o.b.size());
     });
 }
 
-int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** out)
+int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** out, size_t* used, int* objects)
 {
     return guard([&] {
         if (!buf || !out) fail(MLB_EINVAL, "null argument");
@@ -2943,7 +2945,7 @@ int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** 
         if (nextra < 0)
             for (long long i = 0; i < (long long)nx * ny * nz; i++)
                 if (in.i32() != kLuaNil) fail(MLB_EUNSUP, "sites carry extra data (Lua values)");
-        if (in.pos != in.len) fail(MLB_EINVAL, "malformed stream: trailing bytes");
+        if (!used && in.pos != in.len) fail(MLB_EINVAL, "malformed stream: trailing bytes");
         mlb_system* s = make_system(nx, ny, nz, real_bytes);
         try {
             s->alpha = alpha; s->dt = dt; s->gamma = gamma; s->time = time;
@@ -2962,6 +2964,8 @@ int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** 
             throw;
         }
         *out = s;
+        if (used) *used = in.pos;
+        if (objects) *objects = 1 + (int)seen.size();   // the system and the arrays new in the stream
     });
 }
 

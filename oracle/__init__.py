@@ -751,19 +751,20 @@ def _enc_darray(out, idx, a, dims):
 
 
 def encode_spinsystem(nx, ny, nz, alpha, dt, gamma, time, x, y, z, ms, site_alpha=None,
-                      site_gamma=None):
+                      site_gamma=None, first_index=0):
     """SpinSystem::encode (M/cpu/core/spinsystem.cpp:669-757) as exported as a
     Lua value (luamigrate.cpp:75-76, 265-275): the system's header, version 0,
     nx, ny, nz, alpha, dt, gamma, time, the arrays x, y, z, ms, the flag and
     array of per-site alpha, then of per-site gamma, and the count of sites
-    with extra data (0: none)."""
+    with extra data (0: none).  first_index: the system's index in the
+    stream's object list (its arrays take the next ones)."""
     import struct
     out = bytearray()
-    out += struct.pack("=iibib", LUA_TUSERDATA, type_hash32("SpinSystem"), ENC_NEW, 0, 0)
+    out += struct.pack("=iibib", LUA_TUSERDATA, type_hash32("SpinSystem"), ENC_NEW, first_index, 0)
     out += struct.pack("=iii", nx, ny, nz)
     out += struct.pack("=dddd", alpha, dt, gamma, time)
     dims = (nx, ny, nz)
-    idx = 1
+    idx = first_index + 1
     for a in (x, y, z, ms):
         _enc_darray(out, idx, a, dims)
         idx += 1

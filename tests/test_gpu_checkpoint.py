@@ -53,6 +53,7 @@ def test_encode_matches_the_oracle_bytes(M, precision, uniform_ms, site):
     ss, sa, sg = _state(M, (12, 10, 3), precision, 11, uniform_ms, site)
     got = ss.encode()
     assert got == _oracle_stream(ss, sa, sg)
+    assert ss._stream_objects == (7 if site else 5)
     d = O.decode_spinsystem(got)
     assert (d["nx"], d["ny"], d["nz"]) == (12, 10, 3)
     assert (d["alpha"], d["dt"], d["gamma"], d["time"]) == (0.125, 0.01, 1.75, 3.5)
@@ -142,3 +143,26 @@ def test_resume_from_a_checkpoint_follows_the_same_trajectory(M):
     M.run(resumed, ops(), llg, 15)
     assert ss.diff(resumed)[3] == 0.0
     assert resumed.time() == ss.time()
+
+
+def test_stream_inside_a_larger_checkpoint(M):
+    """The system as the fourth object of a stream (object indices 3..7) and
+    followed by more data: decode reads it and reports the bytes used."""
+    ss, _, _ = _state(M, (6, 5, 2), "f64", 71)
+    own = ss.encode()
+    inner = ss.encode(first_index=3)
+    assert len(inner) == len(own) and inner != own
+    assert inner == _oracle_stream_at(ss, 3)
+    tail = struct.pack("=id", 3, 42.0)
+    got, used, nobj = M.SpinSystem.decode(inner + tail, precision="f64", partial=True)
+    assert used == len(inner) and nobj == 5 and ss._stream_objects == 5
+    assert got.encode(first_index=3) == inner
+    with pytest.raises(M.MagLuaError, match="trailing"):
+        M.SpinSystem.decode(inner + tail, precision="f64")
+
+
+def _oracle_stream_at(ss, first):
+    x, y, z, ms = ss.spinArrays()
+    nx, ny, nz = ss._dims
+    return O.encode_spinsystem(nx, ny, nz, ss.alpha(), ss.timeStep(), ss.gamma(), ss.time(), x, y, z, ms,
+                               first_index=first)
