@@ -285,7 +285,8 @@ def run_lr2d(M, torch, calls=20):
 def run_ewald(M, edge=32):
     """The Ewald tensor of an edge^3 simple-cubic lattice (NSites 10: 9261
     real and reciprocal terms per element, 9 elements per site) computed on
-    the GPU (one FP64 thread per element), against the library's host path
+    the GPU (one warp per site, all nine components from shared
+    transcendentals), against the library's host path
     timed on a sample of elements (the reference evaluates elements one by
     one on the CPU)."""
     ew = M.DipoleEwald3D(edge, edge, edge)

@@ -13,7 +13,8 @@
 // on the host once per geometry.
 //
 // The per-element sum runs on the host for single elements and on the GPU,
-// one thread per element, for whole lattices (the loop of make_tensor.lua).
+// one warp per lattice site and all nine components at once, for whole
+// lattices (the loop of make_tensor.lua).
 #include "../../include/mlb200.h"
 
 #include <cuda_runtime.h>
@@ -121,19 +122,112 @@ double ew_next_shell(const EwaldGeo& g, int alpha, int beta, const double* r, do
     return tq + tr;
 }
 
-__global__ void k_ewald_tensor(EwaldGeo g, double a1x, double a1y, double a1z, double a2x, double a2y, double a2z,
-                               double a3x, double a3y, double a3z, double eta, int N, int nx, int ny, int nz,
-                               double* out)
+// The whole lattice: one warp per site r.  A term's exponentials, erfc and
+// cosine do not depend on the component, so each lane evaluates them once
+// per (n, m, k) for all nine components; the 32 lanes take every 32nd
+// triple and the real and reciprocal partial sums meet in a shuffle tree.
+// The result equals the per-element sum up to rounding (the order of the
+// additions and the component factors taken as products with reciprocals):
+// G_ab and G_ba come out equal here.
+constexpr int EW_SITES_PER_CTA = 8;
+
+__global__ void __launch_bounds__(32 * EW_SITES_PER_CTA)
+k_ewald_tensor(EwaldGeo g, double a1x, double a1y, double a1z, double a2x, double a2y, double a2z, double a3x,
+               double a3y, double a3z, double eta, int N, int nx, int ny, int nz, double* out)
 {
     const long long n = (long long)nx * ny * nz;
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n * 9) return;
-    // all nine components: G_ab and G_ba round differently, as in the reference
-    const int q = (int)(e / n);
-    const long long i = e % n;
+    const long long i = (long long)blockIdx.x * EW_SITES_PER_CTA + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;   // whole warps leave together
     const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long long)nx * ny));
     const double r[3] = {x * a1x + y * a2x + z * a3x, x * a1y + y * a2y + z * a3y, x * a1z + y * a2z + z * a3z};
-    out[(size_t)q * n + i] = ew_element(g, q / 3, q % 3, r, eta, N);
+    const bool r0 = ew_dot(r, r) == 0;
+    const double eta2 = eta * eta;
+    const double sqrtpi = 1.772453850905516027;
+    const double inv4eta2 = 1.0 / (4.0 * eta2);
+    // six independent components xx, xy, xz, yy, yz, zz
+    double tr[6] = {0, 0, 0, 0, 0, 0}, tq[6] = {0, 0, 0, 0, 0, 0};
+    const int S = 2 * N + 1;
+    const int terms = S * S * S;
+    for (int t = lane; t < terms; t += 32) {
+        const int nn = t / (S * S) - N, mm = (t / S) % S - N, kk = t % S - N;
+        double Q[3], R[3];
+        for (int c = 0; c < 3; c++) Q[c] = nn * g.b[0][c] + mm * g.b[1][c] + kk * g.b[2][c];
+        for (int c = 0; c < 3; c++) R[c] = nn * g.u[0][c] + mm * g.u[1][c] + kk * g.u[2][c] + (r0 ? 0.0 : r[c]);
+        const double Q2 = ew_dot(Q, Q);
+        if (Q2 > 0) {
+            const double ex = exp(-Q2 * inv4eta2);
+            if (r0) {
+                // -4 pi e (Q2 delta - 3 Qa Qb) / (3 vu Q2)
+                const double f = -4.0 * M_PI * ex / (3.0 * g.vu * Q2);
+                tq[0] += f * (Q2 - 3 * Q[0] * Q[0]);
+                tq[1] += f * (-3 * Q[0] * Q[1]);
+                tq[2] += f * (-3 * Q[0] * Q[2]);
+                tq[3] += f * (Q2 - 3 * Q[1] * Q[1]);
+                tq[4] += f * (-3 * Q[1] * Q[2]);
+                tq[5] += f * (Q2 - 3 * Q[2] * Q[2]);
+            } else {
+                // 4 pi Qa Qb cos(r.Q) e / (Q2 vu)
+                const double f = 4.0 * M_PI * cos(ew_dot(r, Q)) * ex / (Q2 * g.vu);
+                tq[0] += f * Q[0] * Q[0];
+                tq[1] += f * Q[0] * Q[1];
+                tq[2] += f * Q[0] * Q[2];
+                tq[3] += f * Q[1] * Q[1];
+                tq[4] += f * Q[1] * Q[2];
+                tq[5] += f * Q[2] * Q[2];
+            }
+        }
+        const double R2 = ew_dot(R, R);
+        if (R2 > 0) {
+            const double R1 = sqrt(R2);
+            const double R4 = R2 * R2;
+            const double R5 = R4 * R1;
+            const double ex = exp(-eta2 * R2);
+            const double ec = erfc(eta * R1) / R5;
+            if (r0) {
+                // (R2 delta - 3 Ra Rb) (2 eta e (3 + 2 R2 eta2) / (3 R4 sqrt(pi)) + erfc / R5)
+                const double f = 2.0 * eta * ex * (3.0 + 2.0 * R2 * eta2) / (3.0 * R4 * sqrtpi) + ec;
+                tr[0] += (R2 - 3.0 * R[0] * R[0]) * f;
+                tr[1] += (-3.0 * R[0] * R[1]) * f;
+                tr[2] += (-3.0 * R[0] * R[2]) * f;
+                tr[3] += (R2 - 3.0 * R[1] * R[1]) * f;
+                tr[4] += (-3.0 * R[1] * R[2]) * f;
+                tr[5] += (R2 - 3.0 * R[2] * R[2]) * f;
+            } else {
+                // 2 eta e (R2 delta - 3 Rab - 2 eta2 Rab R2) / (sqrt(pi) R4) + (R2 delta - 3 Rab) erfc / R5
+                const double A = 2.0 * eta * ex / (sqrtpi * R4);
+                const double w = 3.0 + 2.0 * eta2 * R2;
+                const double Rab[6] = {R[0] * R[0], R[0] * R[1], R[0] * R[2], R[1] * R[1], R[1] * R[2], R[2] * R[2]};
+                const double dl[6] = {R2, 0.0, 0.0, R2, 0.0, R2};
+#pragma unroll
+                for (int q = 0; q < 6; q++) tr[q] += A * (dl[q] - w * Rab[q]) + (dl[q] - 3.0 * Rab[q]) * ec;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        double a = tr[q], b = tq[q];
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        tr[q] = a;
+        tq[q] = b;
+    }
+    if (lane == 0) {
+        double G[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) G[q] = tq[q] + tr[q];
+        out[0 * n + i] = G[0];   // xx
+        out[1 * n + i] = G[1];   // xy
+        out[2 * n + i] = G[2];   // xz
+        out[3 * n + i] = G[1];   // yx
+        out[4 * n + i] = G[3];   // yy
+        out[5 * n + i] = G[4];   // yz
+        out[6 * n + i] = G[2];   // zx
+        out[7 * n + i] = G[4];   // zy
+        out[8 * n + i] = G[5];   // zz
+    }
 }
 
 } // namespace
@@ -389,9 +483,8 @@ int mlb_ewald3d_tensor(mlb_ewald3d* e, double* out9)
         double* dev = nullptr;
         cudaError_t rc = cudaMalloc(&dev, sizeof(double) * 9 * n);
         if (rc != cudaSuccess) throw EwErr{MLB_ENOMEM, std::string("Ewald tensor: ") + cudaGetErrorString(rc)};
-        const long long work = 9 * n;
-        const int nb = (int)((work + 127) / 128);
-        k_ewald_tensor<<<nb, 128>>>(e->g, e->a[0][0], e->a[0][1], e->a[0][2], e->a[1][0], e->a[1][1], e->a[1][2],
+        const long long nb = (n + EW_SITES_PER_CTA - 1) / EW_SITES_PER_CTA;
+        k_ewald_tensor<<<(unsigned)nb, 32 * EW_SITES_PER_CTA>>>(e->g, e->a[0][0], e->a[0][1], e->a[0][2], e->a[1][0], e->a[1][1], e->a[1][2],
                                     e->a[2][0], e->a[2][1], e->a[2][2], e->eta, e->nsites, e->d[0], e->d[1], e->d[2],
                                     dev);
         rc = cudaGetLastError();
