@@ -544,7 +544,18 @@ def main():
                     help="profiling driver: the Ewald tensor of an edge^3 simple-cubic lattice (NSites 10) and exit")
     ap.add_argument("--ncu-f64", type=int, default=0,
                     help="profiling driver: this many eager steps of the 256x256x8 film in FP64 and exit")
+    ap.add_argument("--ncu-rk4", type=int, default=0,
+                    help="profiling driver: this many RK4 steps (+ thermal kick) of the 256x256x8 film and exit")
     args = ap.parse_args()
+    if args.ncu_rk4:
+        import maglua_b200 as M
+        M.init(int(os.environ.get("LOCAL_RANK", "0")))
+        ss, ops, _ = build_system(M, 0)
+        th = [o for o in ops if isinstance(o, M.Thermal)][0]
+        rk = M.RungeKutta(ss, "RK4", [o for o in ops if o is not th], M.LLG.new("Quaternion"), temp=th)
+        rk.step(args.ncu_rk4)
+        ss.synchronize()
+        return
     if args.ncu_f64:
         import maglua_b200 as M
         M.init(int(os.environ.get("LOCAL_RANK", "0")))
