@@ -11,8 +11,9 @@
  * (M/common/luabaseobject/luabaseobject.h:643-700); a Lua 5.1 glue module
  * maps each method onto one call below.
  *
- * State lives on the GPU in FP32 (SoA x, y, z, ms; one stream per system);
- * host-facing values are FP64 like the reference.  Reductions are FP64.
+ * State lives on the GPU in FP32, or FP64 per system (SoA x, y, z, ms; one
+ * stream per system); host-facing values are FP64 like the reference.
+ * Reductions are FP64.
  */
 #ifndef MLB200_H
 #define MLB200_H
