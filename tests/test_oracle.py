@@ -541,3 +541,20 @@ def test_spinsystem_stream_round_trip_on_the_oracle():
     assert d["site_alpha"] is None and np.array_equal(d["site_gamma"], sg)
     # the uniform ms array is one value (flag 1)
     assert len(data) == 13 + 1 + 12 + 32 + 5 * 30 + 4 * 8 * n + 8 + 12
+
+
+def test_type_ids_against_the_built_reference_murmur():
+    """Where oracle/_ref holds the reference's MurmurHash3 built from its
+    source, the oracle's hash32 equals it on random names of every length."""
+    import ctypes
+    so = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "libmurmur.so")
+    if not os.path.exists(so):
+        pytest.skip("oracle/_ref/libmurmur.so not built (reference tree absent)")
+    fn = ctypes.CDLL(so)._Z18MurmurHash3_x86_32PKvijPv
+    r = np.random.default_rng(7)
+    for length in range(0, 40):
+        name = bytes(r.integers(32, 127, size=length).astype(np.uint8)).decode()
+        res = ctypes.c_int()
+        b = name.encode()
+        fn(b, len(b), 1000, ctypes.byref(res))
+        assert O.type_hash32(name) == res.value, name
