@@ -935,12 +935,16 @@ __global__ void __launch_bounds__(512) k_lr2d_ffty(ConvK c, FftLen Ly, const typ
 
 // The mixing on the split layout S2[kx][ky][comp][z] (FP32 power-of-two
 // ny, after k_sy_fast): a CTA's KB k-points are one contiguous block.
+// NZS > 0: the layer count known at compile time, so that the source loop
+// unrolls and each thread's tensor loads are all in flight together.
+template <int NZS>
 __global__ void __launch_bounds__(256) k_lr2d_mix_s2(ConvK c, float2* s2, const float2* Q, LR2DScale sc)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
+    const int nz = NZS > 0 ? NZS : c.nz;
     float2* Mk = reinterpret_cast<float2*>(smraw);   // [j][b][s]
-    float2* Hk = Mk + (size_t)3 * c.nz * LR2D_KB;      // [j][a][d]
-    const int kx = blockIdx.x, ky0 = blockIdx.y * LR2D_KB, ny = c.ny, nz = c.nz;
+    float2* Hk = Mk + (size_t)3 * nz * LR2D_KB;        // [j][a][d]
+    const int kx = blockIdx.x, ky0 = blockIdx.y * LR2D_KB, ny = c.ny;
     const int nk = min(LR2D_KB, ny - ky0);
     const int NL = 3 * nz;
     pdl_wait();
@@ -951,13 +955,14 @@ __global__ void __launch_bounds__(256) k_lr2d_mix_s2(ConvK c, float2* s2, const 
     for (int t = threadIdx.x; t < NL * nk; t += blockDim.x) {
         const int a = t % 3, rest = t / 3, d = rest % nz, j = rest / nz;
         float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
         for (int s = 0; s < nz; s++) {
             const float2* q = Qk + (((size_t)j * nz + s) * nz + d) * 9 + 3 * a;
             const float w = (float)sc.src[s];
 #pragma unroll
             for (int b = 0; b < 3; b++) {
                 const float2 m = Mk[(size_t)j * NL + b * nz + s];
-                const float2 qq = q[b];
+                const float2 qq = __ldcs(q + b);   // read once: evict first, S2 stays in L2
                 acc = cadd(acc, cmul(make_float2(w * qq.x, w * qq.y), m));
             }
         }
@@ -1312,7 +1317,8 @@ cudaError_t conv_configure()
     if ((e = max_smem(k_split_y<float>)) || (e = max_smem(k_split_y<double>)) || (e = max_smem(k_split_yi<float>)) ||
         (e = max_smem(k_split_yi<double>)) || (e = max_smem(k_split_z<float>)) || (e = max_smem(k_split_z<double>)))
         return e;
-    if ((e = max_smem(k_lr2d_mix_s2)) || (e = max_smem(k_lr2d_ffty<float>)) || (e = max_smem(k_lr2d_ffty<double>)) ||
+    if ((e = max_smem(k_lr2d_mix_s2<0>)) || (e = max_smem(k_lr2d_mix_s2<4>)) || (e = max_smem(k_lr2d_mix_s2<8>)) ||
+        (e = max_smem(k_lr2d_mix_s2<16>)) || (e = max_smem(k_lr2d_ffty<float>)) || (e = max_smem(k_lr2d_ffty<double>)) ||
         (e = max_smem(k_lr2d_mix<float>)) || (e = max_smem(k_lr2d_mix<double>)))
         return e;
     return max_smem(k_fft_lines<double2>);
@@ -1476,7 +1482,11 @@ static void lr2d_t(const ConvK& c, const FftLen L[3], const void* tw_, const voi
         {
             Prof pf("k_lr2d_mix", st);
             const size_t sm = (size_t)6 * c.nz * LR2D_KB * sizeof(float2);
-            launch_pdl(k_lr2d_mix_s2, dim3(c.Kx, (c.ny + LR2D_KB - 1) / LR2D_KB), dim3(256), sm, st, c,
+            auto kern = c.nz == 8 ? k_lr2d_mix_s2<8> : c.nz == 4 ? k_lr2d_mix_s2<4> :
+                        c.nz == 16 ? k_lr2d_mix_s2<16> : k_lr2d_mix_s2<0>;
+            // one thread per (k-point, component, layer) item, whole warps
+            const int nt = std::min(256, (3 * c.nz * LR2D_KB + 31) / 32 * 32);
+            launch_pdl(kern, dim3(c.Kx, (c.ny + LR2D_KB - 1) / LR2D_KB), dim3(nt), sm, st, c,
                        static_cast<float2*>(c.spec2), reinterpret_cast<const float2*>(Q), sc);
         }
         launch_split_y_fast(c, L, reinterpret_cast<const float2*>(tw), sp2, false, st);
