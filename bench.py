@@ -135,7 +135,6 @@ def run_surrogate(M, torch, steps, flush_l2=None):
     spin-steps/s of both on the same system, and the surrogate's relative
     dipolar-field error against the exact FFT field (the device FP32 field,
     itself within 1e-5 of the FP64 oracle) at each exact-evaluation period k."""
-    import oracle as O  # noqa: F401  (nn_paths only: set-up, not timed)
     dims = SUR_DIMS
     n = int(np.prod(dims))
     r = np.random.default_rng(1000)

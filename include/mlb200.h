@@ -9,7 +9,7 @@
  * to the MagLua project root; M/ = src/modules/).  In MagLua those are Lua
  * methods of C++ classes registered by luaT_register<T>
  * (M/common/luabaseobject/luabaseobject.h:643-700); a Lua 5.1 glue module
- * maps each method onto one call below (see INTEGRATION.md).
+ * maps each method onto one call below.
  *
  * State lives on the GPU in FP32, or FP64 per system (SoA x, y, z, ms; one
  * stream per system); host-facing values are FP64 like the reference.
@@ -491,9 +491,14 @@ int mlb_surrogate_gradients(mlb_surrogate* s, const float* const x[3], const flo
  * already exist (apply the operator once to an FP32 SpinSystem of its size;
  * that call allocates), else MLB_ESTATE.  The first call on each device looks
  * up the scratch's address with cudaGetSymbolAddress with that device
- * current; make it before any stream capture.  Every call shares the one
- * scratch: calls that overlap in time (two streams, two threads) race on it
- * and must be serialised by the caller. */
+ * current; make it before any stream capture.  That address is kept for the
+ * life of the process and does not survive a cudaDeviceReset.  The current
+ * device must be the one the operator's tensor spectrum was built on, else
+ * MLB_EINVAL before any launch.  Every call shares the one scratch: calls
+ * that overlap in time (two streams, two threads) race on it and must be
+ * serialised by the caller.  The scratch is part of this library's device
+ * code: every device on which the library's kernels are loaded holds its
+ * 16 MiB until the process exits, whether or not this call is used. */
 #define MLB_NOALLOC_SCRATCH_BYTES 16777216u
 int mlb_dipole_field_noalloc(mlb_op* op, const float* sx, const float* sy, const float* sz, float* hx, float* hy,
                              float* hz, void* stream);

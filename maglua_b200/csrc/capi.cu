@@ -35,6 +35,7 @@
 #include <vector>
 #include <thread>
 #include <atomic>
+#include <mutex>
 
 namespace {
 
@@ -164,6 +165,7 @@ struct ConvPlan {
     DBuf<char> ten9;     // TEN9[kx][kz][ky][9] (complex)
     DBuf<char> spec2;    // split passes: S2[kx][ky][c][z] (complex)
     double max_imag = 0; // largest |Im| of the FP64 tensor transform (6-component)
+    int device = -1;     // CUDA device the arrays above live on
     // SPEC holds the forward x transform of the spins of the system whose
     // spec_token equals this one (set by the fused x pass; 0 = none)
     unsigned long long spec_token = 0;
@@ -708,6 +710,7 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
     if (!op->plan_dirty && op->plan && op->plan->rb == rb) return;
     std::unique_ptr<ConvPlan> P(new ConvPlan());
     P->rb = rb;
+    CK(cudaGetDevice(&P->device));
     plan_sizes(op, *P);
     ConvK& k = P->k;
     const int Px = k.Px, Py = k.Py, Pz = k.Pz;
@@ -4984,15 +4987,17 @@ static __device__ __align__(256) unsigned char g_noalloc_spec[MLB_NOALLOC_SCRATC
 namespace {
 constexpr int kNoallocMaxDevices = 64;
 void* g_noalloc_addr[kNoallocMaxDevices] = {};   // device address of g_noalloc_spec per device
+std::mutex g_noalloc_mu;
 
-// Address of the scratch on the current device, looked up on the first call
-// made with that device current (the lookup may load this library's device
-// code, so that first call belongs before any stream capture).
-void* noalloc_scratch()
+// Address of the scratch on device dev (the current device), looked up on
+// the first call made with that device current (the lookup may load this
+// library's device code, so that first call belongs before any stream
+// capture).  The address is kept for the life of the process: it does not
+// survive a cudaDeviceReset.
+void* noalloc_scratch(int dev)
 {
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoallocMaxDevices) fail(MLB_EUNSUP, "device ordinal beyond the scratch table");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_addr[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_spec);
@@ -5028,7 +5033,12 @@ extern "C" int mlb_dipole_field_noalloc(mlb_op* op, const float* sx, const float
             fail(MLB_ESTATE, "tensor spectrum not built for FP32: apply the operator to an FP32 SpinSystem once "
                              "(that call allocates) before calling mlb_dipole_field_noalloc");
         if (!sx || !sy || !sz || !hx || !hy || !hz) fail(MLB_EINVAL, "null spin or field array");
-        void* scratch = noalloc_scratch();
+        int dev = -1;
+        CK(cudaGetDevice(&dev));
+        if (dev != op->plan->device)
+            fail(MLB_EINVAL, "current device " + std::to_string(dev) + " is not the device " +
+                                 std::to_string(op->plan->device) + " that holds the operator's tensor spectrum");
+        void* scratch = noalloc_scratch(dev);
         const ConvPlan& P = *op->plan;
         ConvK k = P.k;
         k.nrep = 1;

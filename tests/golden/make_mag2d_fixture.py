@@ -7,13 +7,14 @@ builder reproduces it with truncation 20 on every axis.  Its values carry
 the sign of a makeData that added +N; the current makeData
 (mag2d_luafuncs.lua:719-729) adds -N.
 
-Reads the reference tree at /root/reference, or at REFERENCE=<path>."""
+Reads the reference tree named by REFERENCE=<path> (default: a folder
+`reference` beside the repository)."""
 import json
 import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("REFERENCE", "/root/reference")
+REF = os.environ.get("REFERENCE", os.path.join(HERE, "..", "..", "..", "reference"))
 SRC = os.path.join(REF, "src", "modules", "cpu", "dipole2d", "save_test.lua")
 NAMES = ["XX", "XY", "XZ", "YX", "YY", "YZ", "ZX", "ZY", "ZZ"]
 

@@ -5,7 +5,8 @@ source by oracle/Makefile into oracle/_ref/libmurmur.so and called on the
 type names of the SpinSystem stream and on names of every tail length.
 Writes type_hashes.json.
 
-Reads the reference tree at /root/reference, or at REFERENCE=<path>."""
+Reads the reference tree named by REFERENCE=<path> (default: a folder
+`reference` beside the repository)."""
 import ctypes
 import json
 import os
@@ -19,8 +20,8 @@ NAMES = ["SpinSystem", "Array.Double", "Array.Float", "Array.Integer", "LLG.Quat
 
 
 def main():
-    env = dict(os.environ)
-    subprocess.check_call(["make", "-s", "-C", ORACLE, "_ref/libmurmur.so"], env=env)
+    ref = os.environ.get("REFERENCE", os.path.join(HERE, "..", "..", "..", "reference"))
+    subprocess.check_call(["make", "-s", "-C", ORACLE, "_ref/libmurmur.so", f"REFERENCE={os.path.abspath(ref)}"])
     lib = ctypes.CDLL(os.path.join(ORACLE, "_ref", "libmurmur.so"))
     fn = lib._Z18MurmurHash3_x86_32PKvijPv
     out = {}

@@ -70,6 +70,44 @@ def test_noalloc_matches_operator_apply_on_consecutive_calls(M, torch, dims, ope
         assert rel_err(got, ref) <= FIELD_TOL
 
 
+def _user_tensor_op(M, kind, dims, g):
+    """A LongRange with random elements at a few offsets, or a Dipole with
+    one element edited after its lattice sum: both take the general
+    (9-component complex) tensor multiply."""
+    nx, ny, nz = dims
+    r = np.random.default_rng(5)
+    if kind == "longrange":
+        op = M.LongRange(*dims)
+        for ab in ("XX", "XY", "XZ", "YY", "YZ", "ZZ"):
+            for off in ((0, 0, 0), (1, 0, 0), (0, -1, 0), (2, 1, 1 if nz > 1 else 0), (-1, 2, -1 if nz > 1 else 0)):
+                op.setMatrix(ab, off, float(r.normal()))
+    else:
+        op = M.Dipole(*dims)
+        op.getMatrix("XY", (1, 1, 0))        # builds the lattice sum
+        op.setMatrix("XY", (1, 1, 0), 0.37)
+    op.setStrength(g)
+    return op
+
+
+@pytest.mark.parametrize("kind", ["longrange", "edited_dipole"])
+@pytest.mark.parametrize("dims", [(16, 8, 3), (6, 5, 2)])
+def test_noalloc_matches_operator_apply_with_user_tensors(M, torch, kind, dims):
+    n = int(np.prod(dims))
+    s1 = random_spins(n, 81, lengths=True)
+    s2 = random_spins(n, 82)
+    op = _user_tensor_op(M, kind, dims, 0.2)
+    refs = []
+    for s in (s1, s2):
+        ss = M.SpinSystem(*dims)
+        ss.setSpinArrays(*s)
+        op.apply(ss)
+        refs.append(np.stack(ss.fieldArrays(op.slotName())))
+    got = [_noalloc(M, torch, op, s1), _noalloc(M, torch, op, s2)]
+    for g_, ref in zip(got, refs):
+        assert np.isfinite(g_).all()
+        assert rel_err(g_, ref) <= FIELD_TOL
+
+
 def test_noalloc_rejects_lattice_beyond_scratch(M):
     # 1024 x 256 x 8 periodic: (513 kx) x 3 x 8 x 256 complex FP32 = 25.2 MB > 16 MiB
     dip = M.Dipole(1024, 256, 8)
@@ -82,3 +120,23 @@ def test_noalloc_requires_built_tensor(M):
     dip = M.Dipole(8, 8, 2)
     rc = M._lib.mlb_dipole_field_noalloc(dip._h, None, None, None, None, None, None, None)
     assert rc == -4  # MLB_ESTATE
+
+
+def test_noalloc_rejects_another_current_device(M, torch):
+    # the tensor spectrum lives on device 0; with device 1 current the call
+    # must refuse before launching anything
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible devices")
+    dims = (8, 8, 2)
+    n = int(np.prod(dims))
+    dip = M.Dipole(*dims)
+    dip.setStrength(0.1)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*random_spins(n, 3))
+    dip.apply(ss)
+    ss.synchronize()
+    with torch.cuda.device(1):
+        t = [torch.zeros(n, device="cuda:1") for _ in range(6)]
+        rc = M._lib.mlb_dipole_field_noalloc(dip._h, *[x.data_ptr() for x in t], None)
+    assert rc == -1  # MLB_EINVAL
+    assert "holds the operator's tensor spectrum" in M._lib.mlb_last_error().decode()
