@@ -116,6 +116,7 @@ lib.orc_lr_apply.argtypes = [C.c_void_p, _PSS, C.c_char_p, C.c_double, C.c_doubl
 lib.orc_lr_free.argtypes = [C.c_void_p]
 lib.orc_longrange3d_apply.argtypes = [_PSS, _D * 9, C.c_double, C.c_double]
 lib.orc_dipole_direct.argtypes = [_PSS, _D, C.c_double, C.c_int, C.c_int, C.c_int, _D, _D, _D]
+lib.orc_dipole_open_tensor.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D]
 lib.orc_dipole_direct_sites.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, C.c_double,
                                         C.POINTER(C.c_longlong), C.c_int, _D]
 lib.orc_llg_default.argtypes = [C.POINTER(_LLG)]
@@ -374,6 +375,55 @@ def dipole_direct(ss, g, periodic=(0, 0, 0), ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
     hx, hy, hz = np.zeros(ss.n), np.zeros(ss.n), np.zeros(ss.n)
     lib.orc_dipole_direct(ss.p, _dp(abc), g, *[int(p) for p in periodic], _dp(hx), _dp(hy), _dp(hz))
     return np.stack([hx, hy, hz])
+
+
+def dipole_open_tensor(nx, ny, nz, ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
+    """Gamma(r) of every offset of an open lattice (orc_dipole_open_tensor):
+    six arrays XX..ZZ shaped (2nz-1, 2ny-1, 2nx-1), offset d at index d + n - 1."""
+    abc = _f64(ABC)
+    L = (2 * nx - 1) * (2 * ny - 1) * (2 * nz - 1)
+    out = np.zeros(6 * L)
+    lib.orc_dipole_open_tensor(nx, ny, nz, _dp(abc), _dp(out))
+    return out.reshape(6, 2 * nz - 1, 2 * ny - 1, 2 * nx - 1)
+
+
+class DipoleOpen:
+    """The physical open-boundary dipole field h_t = g sum_s Gamma(r_t - r_s) s_s
+    (the kernel of dipole_direct with no images) as a linear convolution by
+    FP64 FFT (numpy.fft) on a grid padded to 2n per axis: the same sum as
+    dipole_direct, in O(N log N), for trajectories of lattices too large for
+    the direct sum."""
+
+    def __init__(self, nx, ny, nz, ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
+        self.dims = (nx, ny, nz)
+        self.P = (2 * nz, 2 * ny, 2 * nx)
+        T = dipole_open_tensor(nx, ny, nz, ABC)
+        grid = np.zeros((6,) + self.P)
+        # offset d lands at index d mod P (negative offsets wrap): circular = linear on the padded grid
+        iz = np.arange(-(nz - 1), nz) % self.P[0]
+        iy = np.arange(-(ny - 1), ny) % self.P[1]
+        ix = np.arange(-(nx - 1), nx) % self.P[2]
+        grid[:, iz[:, None, None], iy[None, :, None], ix[None, None, :]] = T
+        self.TK = np.fft.rfftn(grid, axes=(1, 2, 3))
+
+    def field(self, spins, g):
+        nx, ny, nz = self.dims
+        S = np.zeros((3,) + self.P)
+        S[:, :nz, :ny, :nx] = np.asarray(spins, dtype=np.float64).reshape(3, nz, ny, nx)
+        SK = np.fft.rfftn(S, axes=(1, 2, 3))
+        t = self.TK
+        HK = np.stack([t[0] * SK[0] + t[1] * SK[1] + t[2] * SK[2],
+                       t[1] * SK[0] + t[3] * SK[1] + t[4] * SK[2],
+                       t[2] * SK[0] + t[4] * SK[1] + t[5] * SK[2]])
+        H = np.fft.irfftn(HK, s=self.P, axes=(1, 2, 3))[:, :nz, :ny, :nx]
+        return g * H.reshape(3, -1)
+
+    def apply(self, ss, g, slot="Dipole"):
+        h = self.field(ss.spins(), g)
+        v = ss.field_views(slot)
+        for c in range(3):
+            v[c][:] = h[c]
+        ss.set_slot_used(slot, True)
 
 
 # ---------------------------------------------------------------- LongRange2D / Dipole2D

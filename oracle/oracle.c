@@ -854,6 +854,27 @@ void orc_dipole_direct_sites(int nx, int ny, int nz, const double* x, const doub
     }
 }
 
+/* Gamma(r) for every offset d = t - s of an open nx x ny x nz lattice,
+ * r = d . ABC (the same kernel as orc_dipole_direct_sites), written as six
+ * arrays (XX, XY, XZ, YY, YZ, ZZ) of (2nx-1)(2ny-1)(2nz-1) values at
+ * (dx+nx-1) + (2nx-1)*((dy+ny-1) + (2ny-1)*(dz+nz-1)); Gamma(0) = 0.  The
+ * open-boundary field is this tensor's linear convolution with the spins. */
+void orc_dipole_open_tensor(int nx, int ny, int nz, const double ABC[9], double* out6)
+{
+    const long long Lx = 2 * nx - 1, Ly = 2 * ny - 1, Lz = 2 * nz - 1, L = Lx * Ly * Lz;
+    for (int dz = -(nz - 1); dz <= nz - 1; dz++)
+        for (int dy = -(ny - 1); dy <= ny - 1; dy++)
+            for (int dx = -(nx - 1); dx <= nx - 1; dx++) {
+                const double rx = dx * ABC[0] + dy * ABC[3] + dz * ABC[6];
+                const double ry = dx * ABC[1] + dy * ABC[4] + dz * ABC[7];
+                const double rz = dx * ABC[2] + dy * ABC[5] + dz * ABC[8];
+                double G[6];
+                gamma_dip(rx, ry, rz, G);
+                const long long o = (dx + nx - 1) + Lx * ((dy + ny - 1) + Ly * (long long)(dz + nz - 1));
+                for (int c = 0; c < 6; c++) out6[c * L + o] = G[c];
+            }
+}
+
 /* ------------------------------------------------------------------ */
 /* LLG                                                                  */
 /* ------------------------------------------------------------------ */

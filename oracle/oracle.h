@@ -102,6 +102,10 @@ void orc_longrange3d_apply(orc_ss* ss, double* const T9[9], double g, double gsc
 /* Physical open-boundary direct sum h_t = g * sum_s Gamma(r_t - r_s) s_s (no images). */
 void orc_dipole_direct_sites(int nx, int ny, int nz, const double* x, const double* y, const double* z,
                              const double ABC[9], double g, const long long* sites, int nsites, double* out);
+/* Gamma(r) of every offset of an open lattice (six arrays, XX..ZZ, of
+ * (2nx-1)(2ny-1)(2nz-1) values, offset (dx+nx-1) + (2nx-1)((dy+ny-1) +
+ * (2ny-1)(dz+nz-1))), the kernel of orc_dipole_direct_sites. */
+void orc_dipole_open_tensor(int nx, int ny, int nz, const double ABC[9], double* out6);
 void orc_dipole_direct(const orc_ss* ss, const double ABC[9], double g,
                        int px, int py, int pz, double* hx, double* hy, double* hz);
 

@@ -127,6 +127,19 @@ def test_longrange_matches_real_space_convolution():
     np.testing.assert_allclose(h, want.reshape(3, -1), atol=1e-12)
 
 
+@pytest.mark.parametrize("dims", [(5, 4, 3), (8, 6, 1), (7, 7, 2)])
+def test_open_dipole_fft_equals_direct_sum(dims):
+    # the FFT form of the open-boundary dipole field (O.DipoleOpen, used for
+    # ensemble trajectories) is the physical direct sum with no images
+    n = int(np.prod(dims))
+    s = random_spins(n, 6, lengths=True)
+    ss = O.SpinSystem(*dims)
+    ss.set_spins(*s)
+    want = O.dipole_direct(ss, 0.3)
+    got = O.DipoleOpen(*dims).field(s, 0.3)
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+
+
 def test_longrange_single_layer_equals_direct_periodic_sum():
     # nz = 1: the periodic lattice sum with a radius cut-off equals a direct
     # sum over all images inside the same cut-off.
