@@ -98,11 +98,14 @@ def ensemble_dims(nrep=512, seed=3):
     return [ENS_CLASSES[k] for k in r.integers(0, 4, nrep)]
 
 
-def run_batched(M, torch, steps, warmup):
-    dims = ensemble_dims()
-    e = M.Ensemble(dims)
+def _ensemble_configure(e, g):
     e.configure(alpha=0.1, dt=0.01, J=1.0, pbc=(0, 0, 0), K=0.2, axis=(0, 0, 1), T=0.2, seed=7,
-                B=(0, 0, 0), dB=(0, 0, -0.5 / 20000), g=0.02, open_xy=True, llg="Cartesian")
+                B=(0, 0, 0), dB=(0, 0, -0.5 / 20000), g=g, open_xy=True, llg="Cartesian")
+
+
+def _time_ensemble(M, torch, dims, g, steps, warmup):
+    e = M.Ensemble(dims)
+    _ensemble_configure(e, g)
     for r, d in enumerate(dims):
         n = int(np.prod(d))
         e.setSpins(r, np.zeros(n), np.zeros(n), np.ones(n))
@@ -114,11 +117,75 @@ def run_batched(M, torch, steps, warmup):
     e.run(steps)
     b.record(st)
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
+    return e, a.elapsed_time(b) / steps
+
+
+def _plain_replicas(M, torch, dims, steps):
+    """The plain path over the same replicas: one SpinSystem per replica
+    (each on its own stream) with the operator set shared per size class
+    (the reference's op:apply({ss...}) pattern), every replica's captured
+    step launched by a host loop; wall clock around whole steps of all
+    replicas, synchronised at both ends."""
+    ops_by = {}
+    systems = []
+    for d in dims:
+        n = int(np.prod(d))
+        ss = M.SpinSystem(*d)
+        ss.setSpinArrays(np.zeros(n), np.zeros(n), np.ones(n))
+        ss.setAlpha(0.1)
+        ss.setTimeStep(0.01)
+        if d not in ops_by:
+            ex = M.Exchange(*d)
+            ex.addPaths(*nn_paths(*d, pbc=(0, 0, 0)))
+            ani = M.Anisotropy(*d)
+            ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.2))
+            th = M.Thermal(*d)
+            th.setSeed(7)
+            th.setTemperature(0.2)
+            z = M.AppliedField(*d)
+            z.set(0, 0, 0)
+            z.setSweep(0, 0, -0.5 / 20000)
+            dip = M.Dipole(*d)
+            dip.setOpen(True, True, True)
+            dip.setStrength(0.02)
+            ops_by[d] = [ex, ani, th, z, dip]
+        llg = M.LLG.new("Cartesian")
+        systems.append((ss, M.Plan(ss, ops_by[d], llg)))
+    for ss, p in systems:
+        p.launch(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for ss, p in systems:
+            p.launch(1)
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) * 1e3 / steps
+
+
+def run_batched(M, torch, steps, warmup):
+    """Configuration 3: the packed ensemble (one captured graph per step,
+    classes on concurrent branches, tuned tile/grid/(y,z) variant), the same
+    replicas through the plain path one SpinSystem per replica, and the
+    ensemble without the dipole (the bound any dipole surrogate works under)."""
+    dims = ensemble_dims()
+    e, ms = _time_ensemble(M, torch, dims, 0.02, steps, warmup)
     info = e.info()
-    return {"value": info["sites"] * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
-            "sites": info["sites"], "replicas": len(dims), "fused_block_size": info["block_size"],
+    sites = info["sites"]
+    _, ms_nodip = _time_ensemble(M, torch, dims, 0.0, steps, warmup)
+    plain_ms = _plain_replicas(M, torch, dims, max(3, min(steps, 10)))
+    return {"value": sites * steps / (ms * steps * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "sites": sites, "replicas": len(dims), "fused_block_size": info["block_size"],
+            "config": e.configInfo(), "tune_log": e.tuneLog().strip().splitlines(),
             "workload": ENS_WORKLOAD,
+            "plain_one_system_per_replica": {"value": sites / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                                             "speedup_of_batched": plain_ms / ms,
+                                             "how": "512 SpinSystems, operators shared per size class, one captured "
+                                                    "plain step per replica launched by a host loop; wall clock over "
+                                                    "whole steps (synchronised at both ends)"},
+            "without_dipole": {"ms_per_step": ms_nodip, "value": sites / (ms_nodip * 1e-3),
+                               "amdahl_ceiling": ms / ms_nodip,
+                               "how": "the same ensemble with g = 0: every dipole pass removed, the bound on what "
+                                      "replacing the dipole evaluation by anything can gain"},
             "l2": "working set larger than L2 (no flush)"}
 
 
@@ -716,6 +783,19 @@ def main():
     ss.synchronize()
     ss_ms = e0.elapsed_time(e1)
 
+    # the same film without the dipole operator (the Amdahl bound of any
+    # dipole surrogate): the same plan shape, back to back, no flush
+    ss_nd, ops_nd, llg_nd = build_system(M, seed=rank)
+    plan_nd = M.Plan(ss_nd, ops_nd[:4], llg_nd)
+    plan_nd.launch(3)
+    st_nd = torch.cuda.ExternalStream(ss_nd.stream())
+    e0.record(st_nd)
+    plan_nd.launch(args.steps)
+    e1.record(st_nd)
+    ss_nd.synchronize()
+    nodip_ms = e0.elapsed_time(e1)
+    del plan_nd, ss_nd, ops_nd
+
     # end to end through the C ABI with host buffers
     hx, hy, hz = (torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(3))
     hm = torch.ones(n, dtype=torch.float32).pin_memory().numpy()
@@ -816,6 +896,9 @@ def main():
                           "frac": step_bytes_gbs / peak, "K_points": Kk},
         "steady_state_l2_resident": {"value": n * args.steps / (ss_ms * 1e-3), "ms_per_step": ss_ms / args.steps,
                                      "how": "the same captured step launched back to back, no flush"},
+        "film_without_dipole": {"ms_per_step": nodip_ms / args.steps, "amdahl_ceiling": ss_ms / nodip_ms,
+                                "how": "the film's captured step without the Dipole operator, back to back, no flush: "
+                                       "the bound on what replacing the dipole evaluation by anything can gain"},
         "cpu_baseline": cpu,
         "batched_ensemble": batched,
         "surrogate": surrogate,

@@ -340,13 +340,24 @@ int mlb_plan_destroy(mlb_plan* p);
 /* ---------------------------------------------------------------- ensembles
  * B200 extension for the reference's batched form op:apply({ss1, ss2, ...})
  * (SpinOperation::apply(SpinSystem**, n), spinoperation.cpp:288-300; the
- * CUDA build's *_N kernels need equal sizes): nrep independent replicas of
- * uneven sizes packed by size class, one launch per phase for all of them,
- * the step captured in CUDA graphs.  All replicas share the operator set of
- * mlb_ensemble_cfg: nearest-neighbour Exchange (normalised moments), uniform
- * Anisotropy, Thermal (Philox), AppliedField with a per-step sweep, Dipole
- * (open or periodic in-plane images), LLG.  Replica spins must share one
- * length.  dims holds nx, ny, nz per replica. */
+ * CUDA build's *_N kernels need equal sizes, e.g. cuda_llg_cart_apply_N,
+ * M/cuda/llg_cuda/llgcartesian.cu:133): nrep independent replicas of uneven
+ * sizes packed by size class.  One step is one captured CUDA graph: every
+ * class's dipole passes (all its replicas per launch; classes outside the
+ * power-of-two fast sizes run the generic passes replica by replica) on a
+ * branch of its own, the branches concurrent, then one fused step kernel
+ * whose CTAs walk a packed (replica, tile) table across all classes
+ * (persistent when the tuner finds it faster).  All replicas share the
+ * operator set of mlb_ensemble_cfg: nearest-neighbour Exchange (normalised
+ * moments), uniform Anisotropy, Thermal (Philox), AppliedField with a
+ * per-step sweep, Dipole (open or periodic in-plane images), LLG;
+ * temperature and applied field (start and sweep) may differ per replica
+ * (mlb_ensemble_set_replica_params).  Replica spins must share one length.
+ * dims holds nx, ny, nz per replica.  The first run tunes the (y,z) pass of
+ * every class and the fused kernel's tile size and grid by timing the
+ * candidates, and keeps the choices per process and in a cache file
+ * (MLB_TUNE_CACHE = its path or "off"; default
+ * $XDG_CACHE_HOME/maglua_b200/tune.txt or ~/.cache/maglua_b200/tune.txt). */
 typedef struct mlb_ensemble mlb_ensemble;
 typedef struct mlb_ensemble_cfg {
     double alpha, gamma, dt;
@@ -372,6 +383,19 @@ int mlb_ensemble_run(mlb_ensemble* e, int nsteps);
 int mlb_ensemble_netmoment(mlb_ensemble* e, double* out8);
 int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, double* time);
 int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
+/* Temperature, applied field at the next step and its per-step sweep of
+ * replica rep (mlb_ensemble_configure sets every replica to the cfg's
+ * values); the per-replica form of Thermal:set and AppliedField:set
+ * (spinoperationthermal.cpp:379-387, appliedfield_luafuncs.lua:46-60). */
+int mlb_ensemble_set_replica_params(mlb_ensemble* e, int rep, double T, const double B[3], const double dB[3]);
+/* The applied field replica rep takes at its next step. */
+int mlb_ensemble_get_replica_field(mlb_ensemble* e, int rep, double B[3]);
+/* The tuner's report of the last tuning (NUL-terminated text; *len = its
+ * size with the NUL; buf == NULL asks for the size alone). */
+int mlb_ensemble_tune_log(mlb_ensemble* e, char* buf, size_t cap, size_t* len);
+/* The fused kernel's grid (0: one CTA per tile), the number of size classes
+ * and how many of them run the generic (non power-of-two) passes. */
+int mlb_ensemble_config_info(mlb_ensemble* e, int* grid, int* nclasses, int* generic_classes);
 
 /* ---------------------------------------------------------------- fused run
  * B200 extension: nsteps repetitions of the canonical script step

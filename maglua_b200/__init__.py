@@ -192,6 +192,10 @@ _SIGS = {
     "mlb_ensemble_netmoment": ([_P, _D], C.c_int),
     "mlb_ensemble_info": ([_P, C.POINTER(C.c_longlong), _I, _D], C.c_int),
     "mlb_ensemble_get_stream": ([_P, C.POINTER(_P)], C.c_int),
+    "mlb_ensemble_set_replica_params": ([_P, C.c_int, C.c_double, _D, _D], C.c_int),
+    "mlb_ensemble_get_replica_field": ([_P, C.c_int, _D], C.c_int),
+    "mlb_ensemble_tune_log": ([_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+    "mlb_ensemble_config_info": ([_P, _I, _I, _I], C.c_int),
 }
 EXPORTED = tuple(_SIGS)
 
@@ -1525,6 +1529,27 @@ class Ensemble:
         out = _P()
         _ck(_lib.mlb_ensemble_get_stream(self._h, C.byref(out)))
         return out.value or 0
+
+    def setReplicaParams(self, rep, T, B=(0, 0, 0), dB=(0, 0, 0)):
+        """Temperature and applied field (start, per-step sweep) of one replica."""
+        _ck(_lib.mlb_ensemble_set_replica_params(self._h, int(rep), float(T), _dp(_f64(B, 3)), _dp(_f64(dB, 3))))
+
+    def replicaField(self, rep):
+        out = np.zeros(3)
+        _ck(_lib.mlb_ensemble_get_replica_field(self._h, int(rep), _dp(out)))
+        return tuple(out)
+
+    def tuneLog(self):
+        n = C.c_size_t()
+        _ck(_lib.mlb_ensemble_tune_log(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _ck(_lib.mlb_ensemble_tune_log(self._h, buf, n.value, C.byref(n)))
+        return buf.value.decode()
+
+    def configInfo(self):
+        g, nc, gc = C.c_int(), C.c_int(), C.c_int()
+        _ck(_lib.mlb_ensemble_config_info(self._h, C.byref(g), C.byref(nc), C.byref(gc)))
+        return {"grid": g.value, "classes": nc.value, "generic_classes": gc.value}
 
 
 def _f32(a):

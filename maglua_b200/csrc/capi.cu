@@ -36,6 +36,8 @@
 #include <thread>
 #include <atomic>
 #include <mutex>
+#include <cstdlib>
+#include <sys/stat.h>
 
 namespace {
 
@@ -2112,6 +2114,10 @@ struct EnsClass {
     int nx, ny, nz, nrep;
     long long base;             // first packed site of the class
     mlb_op* dip = nullptr;      // tensor spectrum holder for this size
+    bool fast = true;           // power-of-two fast passes (else the generic ones, replica by replica)
+    int yz_variant = 0;         // tuned (y,z) pass of the fast path (ConvK::yz_variant)
+    cudaStream_t st = nullptr;  // branch of the captured step
+    cudaEvent_t done = nullptr;
 };
 
 void ens_free_graphs(mlb_ensemble* e);
@@ -2133,21 +2139,37 @@ struct mlb_ensemble {
     bool configured = false;
     DevStep* dstep = nullptr;
     cudaStream_t st = nullptr, own = nullptr;
+    cudaEvent_t fork = nullptr;
     int4* rinfo = nullptr;
     int* brep = nullptr;
     int* bstart = nullptr;
     int nblk = 0;
-    int bs = 0;                       // fused-kernel block size (autotuned)
+    int bs = 0;                       // fused-kernel tile size (autotuned)
+    int grid = 0;                     // fused-kernel CTAs (autotuned; < nblk: persistent)
+    bool tuned = false;
+    std::string tune_log;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     double time = 0.0;
     uint64_t counter = 0;
-    double B[3] = {0, 0, 0};
+    // per packed replica: temperature, applied field at the next step and
+    // its per-step sweep (host values); device: field ping-pong by spin
+    // buffer, sweep, thermal deviation
+    std::vector<double> rT, rB, rdB;
+    double* d_rB[2] = {nullptr, nullptr};
+    double* d_rdB = nullptr;
+    float* d_rsig = nullptr;
+    bool rpar_dirty = true;
     double* mom = nullptr;
 };
 
 namespace {
 
-std::map<std::string, int> g_ens_tuned;   // class signature -> block size
+struct EnsTune {
+    int bs = 256, grid = 0;
+    std::vector<int> yz;   // per class
+};
+std::map<std::string, EnsTune> g_ens_tuned;   // tuning key -> choices (this process)
+std::mutex g_ens_tune_mu;
 
 void ens_free_graphs(mlb_ensemble* e)
 {
@@ -2176,6 +2198,40 @@ void ens_block_table(mlb_ensemble* e, int bs)
     e->bs = bs;
 }
 
+bool ens_thermal(const mlb_ensemble* e)
+{
+    if (!(e->cfg.gamma > 0)) return false;
+    for (double T : e->rT)
+        if (T != 0.0) return true;
+    return false;
+}
+
+// Device copies of the per-replica parameters (the field goes to the buffer
+// the next step reads: the one of the current spin buffer).
+void ens_upload_params(mlb_ensemble* e)
+{
+    if (!e->rpar_dirty) return;
+    const int n = e->nrep;
+    const mlb_ensemble_cfg& c = e->cfg;
+    std::vector<float> sig(n, 0.f);
+    for (int r = 0; r < n; r++)
+        if (e->rT[r] != 0.0 && c.gamma > 0)
+            sig[r] = (float)std::sqrt((2.0 * c.alpha * e->rT[r]) / (e->ms * c.dt * c.gamma));
+    CK(cudaStreamSynchronize(e->st));
+    CK(cudaMemcpy(e->d_rB[e->cur], e->rB.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_rdB, e->rdB.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(e->d_rsig, sig.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    e->rpar_dirty = false;
+}
+
+// The host's view of the per-replica fields after the steps run so far.
+void ens_download_fields(mlb_ensemble* e)
+{
+    if (e->rpar_dirty) return;
+    CK(cudaStreamSynchronize(e->st));
+    CK(cudaMemcpy(e->rB.data(), e->d_rB[e->cur], sizeof(double) * 3 * e->nrep, cudaMemcpyDeviceToHost));
+}
+
 FastK ens_fastk(mlb_ensemble* e)
 {
     const mlb_ensemble_cfg& c = e->cfg;
@@ -2191,14 +2247,13 @@ FastK ens_fastk(mlb_ensemble* e)
         for (int q = 0; q < 3; q++) F.axis[q] = (float)(c.axis[q] / al);
         F.ani_c = (float)(2.0 * c.K / (ms * ms));
     }
-    F.th = c.T != 0.0 && g > 0;
+    F.th = ens_thermal(e);
     if (F.th) {
-        F.sigma = (float)std::sqrt((2.0 * a * c.T) / (ms * dt * g));
         F.seed = c.seed;
         F.counter = 0;
         F.dctr = &e->dstep->th_counter;
     }
-    F.Bdev = e->dstep->B;
+    F.Bdev = nullptr;   // per replica (EnsLaunch::rB)
     F.addw = 1.f;
     F.llg_type = c.llg == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
     F.tof = 1;
@@ -2218,70 +2273,260 @@ FastK ens_fastk(mlb_ensemble* e)
     return F;
 }
 
+// The dipole field of every replica of class c from the spins s into H, on
+// stream st: the fast passes over all the class's replicas at once, or the
+// generic passes replica by replica (sizes outside the fast kernels).
+void ens_class_conv(mlb_ensemble* e, EnsClass& c, const float* const s[3], cudaStream_t st)
+{
+    ConvPlan& P = *c.dip->plan;
+    const long long n = (long long)c.nx * c.ny * c.nz;
+    if (c.fast) {
+        ConvK k = P.k;
+        k.yz_variant = c.yz_variant;
+        const float* cs[3] = {s[0] + c.base, s[1] + c.base, s[2] + c.base};
+        float* ch[3] = {e->H[0] + c.base, e->H[1] + c.base, e->H[2] + c.base};
+        CK(mlb::launch_conv_fast(k, P.L, reinterpret_cast<const float2*>(P.tw.p), cs,
+                                 reinterpret_cast<float2*>(P.spec.p), reinterpret_cast<const float*>(P.ten6.p), ch,
+                                 st));
+        return;
+    }
+    ConvK k = P.k;
+    k.nrep = 1;
+    for (int r = 0; r < c.nrep; r++) {
+        const long long o = c.base + r * n;
+        const void* cs[3] = {s[0] + o, s[1] + o, s[2] + o};
+        void* ch[3] = {e->H[0] + o, e->H[1] + o, e->H[2] + o};
+        CK(mlb::launch_conv(k, P.L[0], P.L[1], P.L[2], P.tw.p, cs, P.spec.p, P.ten6.p, P.ten9.p, ch, 4, st));
+    }
+}
+
+EnsLaunch ens_launch(mlb_ensemble* e, int q)
+{
+    EnsLaunch E{};
+    E.nblk = e->nblk; E.bs = e->bs; E.brep = e->brep; E.bstart = e->bstart; E.rinfo = e->rinfo;
+    E.grid = e->grid;
+    E.rB = e->d_rB[q]; E.rBn = e->d_rB[1 - q]; E.rdB = e->d_rdB; E.rsig = e->d_rsig;
+    return E;
+}
+
+// One step on spin buffer q: every class's dipole passes on a branch of its
+// own (the branches run concurrently in the captured graph), joined before
+// the fused step kernel over all replicas.
 void ens_enqueue_step(mlb_ensemble* e, int q)
 {
     const float* s[3] = {e->sp[q][0], e->sp[q][1], e->sp[q][2]};
     float* o[3] = {e->sp[1 - q][0], e->sp[1 - q][1], e->sp[1 - q][2]};
     const float* add[3] = {nullptr, nullptr, nullptr};
     if (e->cfg.g != 0.0) {
+        const bool branch = e->cls.size() > 1;
+        if (branch) CK(cudaEventRecord(e->fork, e->st));
         for (EnsClass& c : e->cls) {
-            ConvPlan& P = *c.dip->plan;
-            const float* cs[3] = {s[0] + c.base, s[1] + c.base, s[2] + c.base};
-            float* ch[3] = {e->H[0] + c.base, e->H[1] + c.base, e->H[2] + c.base};
-            CK(mlb::launch_conv_fast(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), cs,
-                                     reinterpret_cast<float2*>(P.spec.p), reinterpret_cast<const float*>(P.ten6.p), ch,
-                                     e->st));
+            if (branch) {
+                CK(cudaStreamWaitEvent(c.st, e->fork, 0));
+                ens_class_conv(e, c, s, c.st);
+                CK(cudaEventRecord(c.done, c.st));
+            } else {
+                ens_class_conv(e, c, s, e->st);
+            }
         }
+        if (branch)
+            for (EnsClass& c : e->cls) CK(cudaStreamWaitEvent(e->st, c.done, 0));
         for (int q3 = 0; q3 < 3; q3++) add[q3] = e->H[q3];
     }
-    EnsLaunch E{e->nblk, e->bs, e->brep, e->bstart, e->rinfo};
-    CK(mlb::launch_fused_ens(ens_fastk(e), E, s, add, o, e->st));
+    CK(mlb::launch_fused_ens(ens_fastk(e), ens_launch(e, q), s, add, o, e->st));
     CK(mlb::launch_advance_step(e->dstep, e->st));
 }
 
-// Block size of the fused ensemble kernel: time each candidate on the
-// current state (the kernel only writes the other spin buffer) and keep the
-// fastest; remembered per class signature for the process.
-void ens_autotune(mlb_ensemble* e)
+// ---------------------------------------------------------------- ensemble tuner
+// Choices per ensemble: the (y,z) pass variant of every fast class (the
+// register kernel where it applies, or the shared-memory Stockham kernel)
+// and the fused kernel's tile size and grid (one CTA per tile, or
+// persistent CTAs walking the tile table).  Each candidate is timed with
+// CUDA events on the ensemble's stream over repeated launches on the
+// current state (the passes write only H and the other spin buffer).  The
+// choices are kept per process and in a cache file keyed by the device and
+// the classes: MLB_TUNE_CACHE names the file ("off": none), else
+// $XDG_CACHE_HOME/maglua_b200/tune.txt or ~/.cache/maglua_b200/tune.txt.
+std::string tune_cache_path()
 {
-    std::string sig;
+    const char* p = std::getenv("MLB_TUNE_CACHE");
+    if (p) return strcasecmp(p, "off") == 0 ? std::string() : std::string(p);
+    const char* x = std::getenv("XDG_CACHE_HOME");
+    if (x && *x) return std::string(x) + "/maglua_b200/tune.txt";
+    const char* h = std::getenv("HOME");
+    if (h && *h) return std::string(h) + "/.cache/maglua_b200/tune.txt";
+    return std::string();
+}
+
+std::string ens_tune_key(mlb_ensemble* e)
+{
+    int dev = 0;
+    cudaDeviceProp pr;
+    CK(cudaGetDevice(&dev));
+    CK(cudaGetDeviceProperties(&pr, dev));
+    std::string k = std::string(pr.name) + "/" + std::to_string(pr.multiProcessorCount) + "/" +
+                    (e->cfg.llg == MLB_LLG_QUATERNION ? "Q" : "C") + (e->cfg.g != 0.0 ? "D" : "-") +
+                    (ens_thermal(e) ? "T" : "-") + "/";
+    for (char& ch : k)
+        if (ch == ' ') ch = '_';
     for (EnsClass& c : e->cls)
-        sig += std::to_string(c.nx) + "x" + std::to_string(c.ny) + "x" + std::to_string(c.nz) + ":" + std::to_string(c.nrep) + ";";
-    auto it = g_ens_tuned.find(sig);
-    if (it != g_ens_tuned.end()) { ens_block_table(e, it->second); return; }
-    const int cand[3] = {128, 256, 512};
-    float best = 1e30f;
-    int best_bs = 256;
+        k += std::to_string(c.nx) + "x" + std::to_string(c.ny) + "x" + std::to_string(c.nz) + "*" +
+             std::to_string(c.nrep) + ";";
+    return k;
+}
+
+bool tune_file_lookup(const std::string& key, EnsTune& t, size_t ncls)
+{
+    const std::string path = tune_cache_path();
+    if (path.empty()) return false;
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[4096];
+    bool found = false;
+    while (std::fgets(line, sizeof(line), f)) {
+        std::string l(line);
+        const size_t sp = l.find(' ');
+        if (sp == std::string::npos || l.substr(0, sp) != key) continue;
+        EnsTune u;
+        int pos = 0;
+        const char* v = l.c_str() + sp + 1;
+        if (std::sscanf(v, "%d %d%n", &u.bs, &u.grid, &pos) != 2) continue;
+        v += pos;
+        for (size_t i = 0; i < ncls; i++) {
+            int y = 0, m = 0;
+            if (std::sscanf(v, "%d%n", &y, &m) != 1) break;
+            u.yz.push_back(y);
+            v += m;
+        }
+        if (u.yz.size() == ncls && (u.bs == 128 || u.bs == 256 || u.bs == 512)) { t = u; found = true; }
+    }
+    std::fclose(f);
+    return found;
+}
+
+void tune_file_store(const std::string& key, const EnsTune& t)
+{
+    const std::string path = tune_cache_path();
+    if (path.empty()) return;
+    const size_t sl = path.rfind('/');
+    if (sl != std::string::npos) {
+        // create the cache directory (and its parent) when missing
+        const std::string dir = path.substr(0, sl);
+        const size_t sl2 = dir.rfind('/');
+        if (sl2 != std::string::npos && sl2 > 0) mkdir(dir.substr(0, sl2).c_str(), 0755);
+        mkdir(dir.c_str(), 0755);
+    }
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d %d", key.c_str(), t.bs, t.grid);
+    for (int y : t.yz) std::fprintf(f, " %d", y);
+    std::fprintf(f, "\n");
+    std::fclose(f);
+}
+
+template <class Fn>
+float ens_time(mlb_ensemble* e, Fn&& fn, int reps)
+{
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
-    const float* s[3] = {e->sp[e->cur][0], e->sp[e->cur][1], e->sp[e->cur][2]};
-    float* o[3] = {e->sp[1 - e->cur][0], e->sp[1 - e->cur][1], e->sp[1 - e->cur][2]};
-    const float* add[3] = {nullptr, nullptr, nullptr};
-    if (e->cfg.g != 0.0) for (int q = 0; q < 3; q++) add[q] = e->H[q];
-    for (int bs : cand) {
-        ens_block_table(e, bs);
-        EnsLaunch E{e->nblk, e->bs, e->brep, e->bstart, e->rinfo};
-        const FastK F = ens_fastk(e);
-        CK(mlb::launch_fused_ens(F, E, s, add, o, e->st));
-        CK(cudaEventRecord(a, e->st));
-        for (int k = 0; k < 10; k++) CK(mlb::launch_fused_ens(F, E, s, add, o, e->st));
-        CK(cudaEventRecord(b, e->st));
-        CK(cudaEventSynchronize(b));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, a, b));
-        if (ms < best) { best = ms; best_bs = bs; }
-    }
+    fn();
+    CK(cudaEventRecord(a, e->st));
+    for (int k = 0; k < reps; k++) fn();
+    CK(cudaEventRecord(b, e->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    g_ens_tuned[sig] = best_bs;
-    ens_block_table(e, best_bs);
+    return ms / reps;
+}
+
+void ens_autotune(mlb_ensemble* e)
+{
+    const std::string key = ens_tune_key(e);
+    EnsTune t;
+    bool have = false;
+    {
+        std::lock_guard<std::mutex> lk(g_ens_tune_mu);
+        auto it = g_ens_tuned.find(key);
+        if (it != g_ens_tuned.end()) { t = it->second; have = true; }
+    }
+    if (!have && tune_file_lookup(key, t, e->cls.size())) {
+        have = true;
+        e->tune_log = "tuner: cached choices for " + key + "\n";
+    }
+    const float* s[3] = {e->sp[e->cur][0], e->sp[e->cur][1], e->sp[e->cur][2]};
+    if (!have) {
+        char buf[256];
+        std::string log = "tuner: " + key + "\n";
+        // (y,z) pass variant per fast class
+        for (EnsClass& c : e->cls) {
+            int best_v = 0;
+            if (e->cfg.g != 0.0 && c.fast) {
+                float best = 1e30f;
+                for (int v : {0, 1}) {
+                    c.yz_variant = v;
+                    const float ms = ens_time(e, [&] { ens_class_conv(e, c, s, e->st); }, 10);
+                    std::snprintf(buf, sizeof(buf), "  class %dx%dx%d (%d replicas): (y,z) %s %.1f us per evaluation\n",
+                                  c.nx, c.ny, c.nz, c.nrep, v == 0 ? "register/automatic" : "Stockham", 1e3 * ms);
+                    log += buf;
+                    if (ms < best) { best = ms; best_v = v; }
+                }
+            }
+            c.yz_variant = best_v;
+            t.yz.push_back(best_v);
+        }
+        // fused step: tile size x grid
+        const float* add[3] = {nullptr, nullptr, nullptr};
+        if (e->cfg.g != 0.0) for (int q = 0; q < 3; q++) add[q] = e->H[q];
+        float* o[3] = {e->sp[1 - e->cur][0], e->sp[1 - e->cur][1], e->sp[1 - e->cur][2]};
+        int dev = 0, nsm = 148;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        float best = 1e30f;
+        // the tuner's launches write the field of the step after next into
+        // a scratch copy of the field buffer, not into the live one
+        double* scratchB = nullptr;
+        CK(cudaMalloc(&scratchB, sizeof(double) * 3 * e->nrep));
+        for (int bs : {128, 256, 512}) {
+            ens_block_table(e, bs);
+            for (int per_sm : {0, 2, 4, 8}) {
+                e->grid = per_sm ? per_sm * nsm : 0;
+                if (e->grid >= e->nblk) continue;
+                EnsLaunch E = ens_launch(e, e->cur);
+                E.rBn = scratchB;
+                const FastK F = ens_fastk(e);
+                const float ms = ens_time(e, [&] { CK(mlb::launch_fused_ens(F, E, s, add, o, e->st)); }, 10);
+                std::snprintf(buf, sizeof(buf), "  fused step: tile %d sites, %s: %.1f us\n", bs,
+                              per_sm ? (std::to_string(e->grid) + " persistent CTAs").c_str()
+                                     : (std::to_string(e->nblk) + " CTAs (one per tile)").c_str(),
+                              1e3 * ms);
+                log += buf;
+                if (ms < best) { best = ms; t.bs = bs; t.grid = e->grid; }
+            }
+        }
+        cudaFree(scratchB);
+        std::snprintf(buf, sizeof(buf), "  chosen: tile %d, grid %d (0 = one CTA per tile)\n", t.bs, t.grid);
+        log += buf;
+        e->tune_log = log;
+        tune_file_store(key, t);
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_ens_tune_mu);
+        g_ens_tuned[key] = t;
+    }
+    for (size_t i = 0; i < e->cls.size(); i++) e->cls[i].yz_variant = i < t.yz.size() ? t.yz[i] : 0;
+    ens_block_table(e, t.bs);
+    e->grid = t.grid;
+    e->tuned = true;
 }
 
 void ens_prepare(mlb_ensemble* e)
 {
     if (!e->configured) fail(MLB_ESTATE, "ensemble not configured");
     if (!e->have_ms) fail(MLB_ESTATE, "ensemble spins not set");
+    ens_upload_params(e);
     if (e->exec[0]) return;
     const mlb_ensemble_cfg& c = e->cfg;
     if (c.g != 0.0) {
@@ -2299,13 +2544,13 @@ void ens_prepare(mlb_ensemble* e)
             k.dip->plan_dirty = true;
             build_plan(k.dip, e->st, 4);
             ConvPlan& P = *k.dip->plan;
-            if (!mlb::conv_fast_ok(P.k)) fail(MLB_EUNSUP, "ensemble size class outside the fast FFT sizes");
-            P.k.nrep = k.nrep;
+            k.fast = mlb::conv_fast_ok(P.k) && !P.k.split;
             P.k.g = c.g / ((double)P.k.Px * P.k.Py * P.k.Pz);
-            P.spec.alloc((size_t)P.k.Kx * 3 * k.nz * k.ny * k.nrep * sizeof(float2));
+            P.k.nrep = k.fast ? k.nrep : 1;
+            P.spec.alloc((size_t)P.k.Kx * 3 * k.nz * k.ny * P.k.nrep * sizeof(float2));
         }
     }
-    ens_autotune(e);
+    if (!e->tuned) ens_autotune(e);
     CK(cudaStreamSynchronize(e->st));
     for (int q = 0; q < 2; q++) {
         cudaGraph_t graph = nullptr;
@@ -3789,6 +4034,20 @@ int mlb_ensemble_create(int nrep, const int* dims, mlb_ensemble** out)
         CK(cudaMalloc(&e->dstep, sizeof(DevStep)));
         CK(cudaMemset(e->dstep, 0, sizeof(DevStep)));
         CK(cudaMalloc(&e->mom, sizeof(double) * 6 * nrep));
+        for (int q = 0; q < 2; q++) {
+            CK(cudaMalloc(&e->d_rB[q], sizeof(double) * 3 * nrep));
+            CK(cudaMemset(e->d_rB[q], 0, sizeof(double) * 3 * nrep));
+        }
+        CK(cudaMalloc(&e->d_rdB, sizeof(double) * 3 * nrep));
+        CK(cudaMalloc(&e->d_rsig, sizeof(float) * nrep));
+        e->rT.assign(nrep, 0.0);
+        e->rB.assign(3 * (size_t)nrep, 0.0);
+        e->rdB.assign(3 * (size_t)nrep, 0.0);
+        CK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+        for (EnsClass& c : e->cls) {
+            CK(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+        }
         memset(&e->cfg, 0, sizeof(e->cfg));
         *out = e.release();
     });
@@ -3804,7 +4063,13 @@ int mlb_ensemble_destroy(mlb_ensemble* e)
             for (int c = 0; c < 3; c++) cudaFree(e->sp[b][c]);
         for (int c = 0; c < 3; c++) cudaFree(e->H[c]);
         cudaFree(e->rinfo); cudaFree(e->brep); cudaFree(e->bstart); cudaFree(e->dstep); cudaFree(e->mom);
-        for (EnsClass& c : e->cls) delete c.dip;
+        cudaFree(e->d_rB[0]); cudaFree(e->d_rB[1]); cudaFree(e->d_rdB); cudaFree(e->d_rsig);
+        for (EnsClass& c : e->cls) {
+            delete c.dip;
+            if (c.st) cudaStreamDestroy(c.st);
+            if (c.done) cudaEventDestroy(c.done);
+        }
+        if (e->fork) cudaEventDestroy(e->fork);
         if (e->own) cudaStreamDestroy(e->own);
         delete e;
     });
@@ -3814,10 +4079,16 @@ int mlb_ensemble_configure(mlb_ensemble* e, const mlb_ensemble_cfg* cfg)
 {
     return guard([&] {
         if (cfg->llg != MLB_LLG_CARTESIAN && cfg->llg != MLB_LLG_QUATERNION) fail(MLB_EINVAL, "unknown LLG type");
+        CK(cudaStreamSynchronize(e->st));
         e->cfg = *cfg;
         e->configured = true;
         e->counter = 0;
-        for (int a = 0; a < 3; a++) e->B[a] = cfg->B[a];
+        for (int r = 0; r < e->nrep; r++) {
+            e->rT[r] = cfg->T;
+            for (int a = 0; a < 3; a++) { e->rB[3 * r + a] = cfg->B[a]; e->rdB[3 * r + a] = cfg->dB[a]; }
+        }
+        e->rpar_dirty = true;
+        e->tuned = false;
         ens_free_graphs(e);
     });
 }
@@ -3838,6 +4109,8 @@ int mlb_ensemble_set_spins(mlb_ensemble* e, int rep, const double* x, const doub
         }
         if (e->have_ms && std::fabs(m0 - e->ms) > 1e-6f * std::max(1.f, m0))
             fail(MLB_EUNSUP, "ensemble spins must share one length");
+        if (!e->have_ms || e->ms != m0) e->rpar_dirty = true;
+        ens_download_fields(e);
         e->ms = m0;
         e->have_ms = true;
         CK(cudaStreamSynchronize(e->st));
@@ -3873,14 +4146,12 @@ int mlb_ensemble_run(mlb_ensemble* e, int nsteps)
         DevStep h;
         memset(&h, 0, sizeof(h));
         h.th_counter = e->counter;
-        for (int a = 0; a < 3; a++) { h.B[a] = e->B[a]; h.dB[a] = e->cfg.dB[a]; }
         CK(cudaMemcpyAsync(e->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, e->st));
         const bool cart = e->cfg.llg != MLB_LLG_QUATERNION;
         for (int k = 0; k < nsteps; k++) {
             CK(cudaGraphLaunch(e->exec[e->cur], e->st));
             e->cur = 1 - e->cur;
             if (!cart || e->cfg.dt != 0.0) e->time = e->time + e->cfg.dt;
-            for (int a = 0; a < 3; a++) e->B[a] += e->cfg.dB[a];
         }
         e->counter += (uint64_t)nsteps;
     });
@@ -3917,6 +4188,60 @@ int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, doubl
 int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
 {
     return guard([&] { *stream = (void*)e->st; });
+}
+
+int mlb_ensemble_set_replica_params(mlb_ensemble* e, int rep, double T, const double B[3], const double dB[3])
+{
+    return guard([&] {
+        if (!e || !B || !dB) fail(MLB_EINVAL, "null argument");
+        if (!e->configured) fail(MLB_ESTATE, "ensemble not configured");
+        if (rep < 0 || rep >= e->nrep) fail(MLB_ERANGE, "replica index");
+        if (!(T >= 0.0)) fail(MLB_EINVAL, "temperature must be non-negative");
+        ens_download_fields(e);
+        const int p = e->pos[rep];
+        const bool th_before = ens_thermal(e);
+        e->rT[p] = T;
+        for (int a = 0; a < 3; a++) { e->rB[3 * p + a] = B[a]; e->rdB[3 * p + a] = dB[a]; }
+        e->rpar_dirty = true;
+        if (ens_thermal(e) != th_before) { e->tuned = false; ens_free_graphs(e); }
+    });
+}
+
+int mlb_ensemble_get_replica_field(mlb_ensemble* e, int rep, double B[3])
+{
+    return guard([&] {
+        if (!e || !B) fail(MLB_EINVAL, "null argument");
+        if (rep < 0 || rep >= e->nrep) fail(MLB_ERANGE, "replica index");
+        ens_download_fields(e);
+        for (int a = 0; a < 3; a++) B[a] = e->rB[3 * e->pos[rep] + a];
+    });
+}
+
+int mlb_ensemble_tune_log(mlb_ensemble* e, char* buf, size_t cap, size_t* len)
+{
+    return guard([&] {
+        if (!e || !len) fail(MLB_EINVAL, "null argument");
+        *len = e->tune_log.size() + 1;
+        if (buf && cap) {
+            const size_t n = std::min(cap - 1, e->tune_log.size());
+            std::memcpy(buf, e->tune_log.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+int mlb_ensemble_config_info(mlb_ensemble* e, int* grid, int* nclasses, int* generic_classes)
+{
+    return guard([&] {
+        if (!e) fail(MLB_EINVAL, "null argument");
+        if (grid) *grid = e->grid;
+        if (nclasses) *nclasses = (int)e->cls.size();
+        if (generic_classes) {
+            int g = 0;
+            for (EnsClass& c : e->cls) g += c.fast ? 0 : 1;
+            *generic_classes = g;
+        }
+    });
 }
 
 } // extern "C"

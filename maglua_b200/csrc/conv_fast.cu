@@ -953,24 +953,35 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     }
 }
 
-// Packed ensemble: block b covers sites [bstart[b], bstart[b] + blockDim) of
-// replica brep[b]; rinfo[r] = {nx, ny, nz, first packed site}.
+// Packed ensemble: tile b covers sites [bstart[b], bstart[b] + blockDim) of
+// packed replica brep[b]; rinfo[r] = {nx, ny, nz, first packed site}.  CTAs
+// walk the tile table with stride gridDim.x (persistent when the grid is
+// smaller than the table).  Each replica takes its own applied field and
+// thermal deviation (E.rB, E.rsig); the CTA of a replica's first tile
+// writes the next step's field B + dB to E.rBn.
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
-__global__ void k_fused_ens(FastK F, const int* __restrict__ brep, const int* __restrict__ bstart,
-                            const int4* __restrict__ rinfo, const float* __restrict__ sx,
-                            const float* __restrict__ sy, const float* __restrict__ sz,
-                            const float* __restrict__ ax, const float* __restrict__ ay,
+__global__ void k_fused_ens(FastK F0, EnsLaunch E, const float* __restrict__ sx, const float* __restrict__ sy,
+                            const float* __restrict__ sz, const float* __restrict__ ax, const float* __restrict__ ay,
                             const float* __restrict__ az, float* __restrict__ ox, float* __restrict__ oy,
                             float* __restrict__ oz)
 {
-    const int4 r = __ldg(rinfo + __ldg(brep + blockIdx.x));
-    const int local = __ldg(bstart + blockIdx.x) + threadIdx.x;
-    const int n = r.x * r.y * r.z;
-    if (local >= n) return;
-    const int x = local % r.x;
-    const int y = (local / r.x) % r.y;
-    const int z = local / (r.x * r.y);
-    fused_site<LT, EXS, ANI, TH, ADD>(F, r.x, r.y, r.z, x, y, z, r.w + local, sx, sy, sz, ax, ay, az, ox, oy, oz);
+    FastK F = fastk_resolved(F0);
+    for (int b = blockIdx.x; b < E.nblk; b += gridDim.x) {
+        const int rep = __ldg(E.brep + b);
+        const int4 r = __ldg(E.rinfo + rep);
+        const int start = __ldg(E.bstart + b);
+        F.B[0] = (float)E.rB[3 * rep]; F.B[1] = (float)E.rB[3 * rep + 1]; F.B[2] = (float)E.rB[3 * rep + 2];
+        if (TH) F.sigma = __ldg(E.rsig + rep);
+        if (start == 0 && threadIdx.x < 3)
+            E.rBn[3 * rep + threadIdx.x] = E.rB[3 * rep + threadIdx.x] + E.rdB[3 * rep + threadIdx.x];
+        const int local = start + threadIdx.x;
+        const int n = r.x * r.y * r.z;
+        if (local >= n) continue;
+        const int x = local % r.x;
+        const int y = (local / r.x) % r.y;
+        const int z = local / (r.x * r.y);
+        fused_site<LT, EXS, ANI, TH, ADD>(F, r.x, r.y, r.z, x, y, z, r.w + local, sx, sy, sz, ax, ay, az, ox, oy, oz);
+    }
 }
 
 // FP64 per-replica sums (x, y, z, x^2, y^2, z^2): one block per replica.
@@ -1145,6 +1156,10 @@ template <int PY, int PZ>
 static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, const float* ten6, cudaStream_t st)
 {
     constexpr int RPZ = PZ <= 16 ? PZ : 16;
+    if (c.yz_variant == 1 && yz_fast_smem(PY, PZ, c.nz) <= 227 * 1024) {
+        const size_t smem = yz_fast_smem(PY, PZ, c.nz);
+        return launch_pdl(k_yz_fast<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZT<PY, PZ>::N), smem, st, c, twy, spec, ten6);
+    }
     if constexpr (PY >= 256) {
         if (yz_reg_ok(PY, PZ, c))
             return launch_pdl(k_yz_reg<PY, RPZ, 384>, dim3(c.Kx, c.nrep), dim3(384), YZR<PY, RPZ, 384>::smem(c.nz), st,
@@ -1429,8 +1444,9 @@ static void fused_ex(const FastKT<R>& F, const R* s[3], const R* a[3], R* o[3], 
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD>
 static void ens_t(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)
 {
-    k_fused_ens<LT, EXS, ANI, TH, ADD><<<E.nblk, E.bs, 0, st>>>(F, E.brep, E.bstart, E.rinfo, s[0], s[1], s[2], a[0], a[1],
-                                                               a[2], o[0], o[1], o[2]);
+    const int grid = E.grid > 0 && E.grid < E.nblk ? E.grid : E.nblk;
+    k_fused_ens<LT, EXS, ANI, TH, ADD><<<grid, E.bs, 0, st>>>(F, E, s[0], s[1], s[2], a[0], a[1], a[2], o[0], o[1],
+                                                             o[2]);
 }
 template <int LT, bool EXS, bool ANI, bool TH>
 static void ens_add(const FastK& F, const EnsLaunch& E, const float* s[3], const float* a[3], float* o[3], cudaStream_t st)

@@ -122,6 +122,7 @@ struct ConvK {
     int fx, fy, fz;          // FftLen indices
     int nrep;                // replicas of this size packed back to back (1 for a system)
     const int* run_if;       // when set, the passes run only while *run_if != 0
+    int yz_variant = 0;      // (y,z) pass of the fast path: 0 automatic, 1 shared-memory Stockham, 2 register
     // Planes too large for one CTA's shared memory: the (y,z) pass runs as
     // three passes (y, z with the tensor multiply, inverse y) through spec2,
     // S2[kx][ky][comp][z] (data layers only), and the tensor is stored
@@ -205,9 +206,20 @@ struct SurDev {
 };
 
 // Block table of the packed-ensemble fused kernel.
+// Packed ensemble step: the work table (replica, first site) of nblk
+// tiles of bs sites walked by `grid` CTAs (grid < nblk: persistent CTAs,
+// each taking every grid-th tile); per packed replica r the applied field
+// B[3r..3r+2] of this step (rB), its sweep (rdB) and thermal deviation
+// (rsig); the CTA holding tile 0 of a replica writes the next step's field
+// to rBn.
 struct EnsLaunch {
     int nblk, bs;
     const int* brep;
     const int* bstart;
     const int4* rinfo;
+    int grid;
+    const double* rB;
+    double* rBn;
+    const double* rdB;
+    const float* rsig;
 };
