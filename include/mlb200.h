@@ -74,6 +74,13 @@ int mlb_system_dims(const mlb_system* s, int out[3]);                  /* nx(), 
 int mlb_system_set_stream(mlb_system* s, void* cuda_stream);
 int mlb_system_get_stream(const mlb_system* s, void** cuda_stream);
 int mlb_system_synchronize(mlb_system* s);
+/* B200 extension (the reference only prints CUDA errors): the system's
+ * status word after the work queued so far -- bit 0 (MLB_STATUS_NONFINITE)
+ * is set once any LLG step of this system wrote a spin component that is not
+ * finite (NaN or infinity).  Synchronises the system's stream; clear != 0
+ * resets the word. */
+#define MLB_STATUS_NONFINITE 1u
+int mlb_system_status(mlb_system* s, int clear, unsigned* flags);
 /* setSpin(i,j,k, sx,sy,sz[, m]) for one site (l_setspin :1312-1361); idx is
  * the 0-based x + nx*(y + ny*z). */
 int mlb_system_set_spin(mlb_system* s, int idx, double sx, double sy, double sz);
@@ -181,6 +188,10 @@ int mlb_op_apply_many(mlb_op* op, mlb_system* const* s, int n);
 int mlb_exchange_add_path(mlb_op* op, int from, int to, double J);
 int mlb_exchange_add_paths(mlb_op* op, const int* from, const int* to, const double* J, int n);
 int mlb_exchange_set_normalize(mlb_op* op, int on);
+/* setPeriodicXYZ / periodicXYZ (spinoperationexchange.cpp:560-580): the
+ * flags the Lua add() wraps sites by, kept for getPeriodicXYZ and encode. */
+int mlb_exchange_set_pbc(mlb_op* op, int px, int py, int pz);
+int mlb_exchange_get_pbc(const mlb_op* op, int pbc[3]);
 int mlb_exchange_num_paths(const mlb_op* op, int* n);
 /* Anisotropy: ani:add(site, axis, K) (axis normalised, spinoperationanisotropy.cpp:367-410). */
 int mlb_anisotropy_add(mlb_op* op, int site, const double axis[3], double K);
@@ -214,7 +225,20 @@ int mlb_appliedfield_set_sweep(mlb_op* op, double dbx, double dby, double dbz);
  * truncation gmax {r, x, y, z}, unit cell, tensor elements. */
 int mlb_longrange_set_strength(mlb_op* op, double g);
 int mlb_longrange_get_strength(const mlb_op* op, double* g);
+/* setTruncation (spinoperationlongrange.cpp:505-568): gmax[0] < 0 is
+ * math.huge (every entry becomes -1).  A Dipole of truncation math.huge takes
+ * the reference's extrapolated lattice sum (dipoleLoad,
+ * M/cpu/dipole/dipolesupport.cpp:771-835), which in the reference always
+ * ends as the image sum over 1000 rings of 5 lattices (|X|, |Y| <= 4999):
+ * its C side reads a second return value from the Lua extrapolate() that
+ * the function never gives, so convergence is never reported.  FP64 on the
+ * GPU, one warp per tensor element. */
 int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4]);
+int mlb_longrange_get_truncation(const mlb_op* op, int gmax[4]);     /* getTruncation (-1 = math.huge) */
+/* B200 extension (no reference counterpart): the number of 5-lattice rings
+ * of the math.huge sum (the reference's fixed 1000), for checks on small
+ * ring counts. */
+int mlb_dipole_set_huge_rings(mlb_op* op, int rings);
 int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9]);
 /* B200 extension: open (zero-padded) boundaries per axis for Dipole; the
  * reference Dipole is periodic in x and y and open in z. */
@@ -314,6 +338,7 @@ int mlb_ewald3d_tensor(mlb_ewald3d* e, double* out9);
 #define MLB_LLG_QUATERNION 1
 int mlb_llg_create(int kind, mlb_llg** out);                            /* LLG.new("Cartesian") */
 int mlb_llg_destroy(mlb_llg* l);
+int mlb_llg_kind(const mlb_llg* l, int* kind);                          /* MLB_LLG_CARTESIAN or _QUATERNION */
 /* thermalOnlyFirstTerm (default 1), disableRenormalization (0),
  * unphysical precession / damping scales (1, 1). */
 int mlb_llg_set_flags(mlb_llg* l, int thermal_only_first_term, int disable_renormalization,
@@ -321,6 +346,30 @@ int mlb_llg_set_flags(mlb_llg* l, int thermal_only_first_term, int disable_renor
 /* llg:apply(from[, scale], dmdt, to[, advance]) */
 int mlb_llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb_system* to,
                   int advance);
+
+/* ---------------------------------------------------------------- operator and LLG streams
+ * encode / decode of operators and integrators: the bytes the reference's
+ * CPU build writes for them inside a checkpoint, as exported Lua values
+ * (LUA_TUSERDATA, type id, char 111 and the object index, then the class's
+ * encode): Exchange (M/cpu/exchange/spinoperationexchange.cpp:52-112),
+ * Anisotropy (M/cpu/anisotropy/spinoperationanisotropy.cpp:191-236),
+ * Anisotropy.Uniaxial (..._uniaxial.cpp:181-230), Anisotropy.Cubic
+ * (..._cubic.cpp:239-290), Thermal (M/cpu/thermal/spinoperationthermal.cpp:
+ * 51-77, its scale array an object of its own), AppliedField
+ * (M/cpu/appliedfield/spinoperationappliedfield.cpp:33-58), Dipole
+ * (M/cpu/dipole/spinoperationdipole.cpp:35-59 over LongRange's,
+ * M/cpu/longrange/spinoperationlongrange.cpp:55-95), LLG.Cartesian and
+ * LLG.Quaternion (M/cpu/llg/llg.cpp:50-88).  Arguments as for
+ * mlb_system_encode / mlb_system_decode; *objects = the objects the stream
+ * holds (2 for Thermal).  A plain LongRange gives MLB_EUNSUP: the
+ * reference's LongRange::encode writes no object header, so its stream
+ * cannot be read back.  Tensors, RNG state and injected noise are not part
+ * of the streams (as in the reference); a decoded Dipole builds its tensor
+ * on first use. */
+int mlb_op_encode(mlb_op* op, int first_index, void* buf, size_t cap, size_t* len, int* objects);
+int mlb_op_decode(const void* buf, size_t len, mlb_op** out, size_t* used, int* objects);
+int mlb_llg_encode(mlb_llg* l, int first_index, void* buf, size_t cap, size_t* len, int* objects);
+int mlb_llg_decode(const void* buf, size_t len, mlb_llg** out, size_t* used, int* objects);
 
 /* ---------------------------------------------------------------- plans
  * B200 extension (the reference steps from Lua, one operator call at a time):
@@ -383,6 +432,8 @@ int mlb_ensemble_run(mlb_ensemble* e, int nsteps);
 int mlb_ensemble_netmoment(mlb_ensemble* e, double* out8);
 int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, double* time);
 int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream);
+/* The ensemble's status word, as mlb_system_status (any replica). */
+int mlb_ensemble_status(mlb_ensemble* e, int clear, unsigned* flags);
 /* Temperature, applied field at the next step and its per-step sweep of
  * replica rep (mlb_ensemble_configure sets every replica to the cfg's
  * values); the per-replica form of Thermal:set and AppliedField:set
@@ -495,6 +546,14 @@ int mlb_surrogate_detach(mlb_system* ss);
 /* out: exact evaluations, surrogate evaluations, failed residual checks of
  * the last run; *last_bound: the last estimated relative field error. */
 int mlb_surrogate_stats(mlb_surrogate* s, long long out[3], double* last_bound);
+/* Polls of each tensor-core completion wait (mbarrier try_wait) before it
+ * gives up (default 2^24, about 0.1 s).  A wait that gives up sets the
+ * surrogate's error flag, then waits (bounded again) for the launch's own
+ * MMAs before its TMEM is read and freed, so the kernel always returns; the
+ * next host call that reads the flag (forward, gradients, train, validate,
+ * run) returns MLB_ECUDA and clears it.  0 makes every wait give up at once:
+ * a way to exercise that path. */
+int mlb_surrogate_set_wait_limit(mlb_surrogate* s, unsigned polls);
 /* Host-array forms for checks: x (3 arrays of nx*ny*nz, SpinSystem layout)
  * -> dh = net(x); and the gradients of L = |net(x) - t|^2 / |t|^2 with
  * respect to W and R (p: the prediction the gradients used; may be NULL). */

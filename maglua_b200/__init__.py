@@ -106,6 +106,15 @@ _SIGS = {
     "mlb_appliedfield_set_sweep": ([_P, C.c_double, C.c_double, C.c_double], C.c_int),
     "mlb_longrange_set_strength": ([_P, C.c_double], C.c_int),
     "mlb_longrange_get_strength": ([_P, _D], C.c_int),
+    "mlb_longrange_get_truncation": ([_P, _I], C.c_int),
+    "mlb_op_encode": ([_P, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), _I], C.c_int),
+    "mlb_op_decode": ([C.c_char_p, C.c_size_t, C.POINTER(_P), C.POINTER(C.c_size_t), _I], C.c_int),
+    "mlb_llg_encode": ([_P, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), _I], C.c_int),
+    "mlb_llg_decode": ([C.c_char_p, C.c_size_t, C.POINTER(_P), C.POINTER(C.c_size_t), _I], C.c_int),
+    "mlb_exchange_set_pbc": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
+    "mlb_llg_kind": ([_P, _I], C.c_int),
+    "mlb_exchange_get_pbc": ([_P, _I], C.c_int),
+    "mlb_dipole_set_huge_rings": ([_P, C.c_int], C.c_int),
     "mlb_longrange_set_truncation": ([_P, _I], C.c_int),
     "mlb_longrange_set_unit_cell": ([_P, _D], C.c_int),
     "mlb_longrange_set_open": ([_P, C.c_int, C.c_int, C.c_int], C.c_int),
@@ -192,6 +201,9 @@ _SIGS = {
     "mlb_ensemble_netmoment": ([_P, _D], C.c_int),
     "mlb_ensemble_info": ([_P, C.POINTER(C.c_longlong), _I, _D], C.c_int),
     "mlb_ensemble_get_stream": ([_P, C.POINTER(_P)], C.c_int),
+    "mlb_surrogate_set_wait_limit": ([_P, C.c_uint], C.c_int),
+    "mlb_ensemble_status": ([_P, C.c_int, C.POINTER(C.c_uint)], C.c_int),
+    "mlb_system_status": ([_P, C.c_int, C.POINTER(C.c_uint)], C.c_int),
     "mlb_ensemble_set_replica_params": ([_P, C.c_int, C.c_double, _D, _D], C.c_int),
     "mlb_ensemble_get_replica_field": ([_P, C.c_int, _D], C.c_int),
     "mlb_ensemble_tune_log": ([_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
@@ -349,6 +361,13 @@ class SpinSystem:
         _ck(_lib.mlb_system_synchronize(self._h))
 
     # spins
+    def status(self, clear=False):
+        """Status word of the steps queued so far (synchronises the system's
+        stream): bit 0 (1) when an LLG step wrote a non-finite spin."""
+        f = C.c_uint()
+        _ck(_lib.mlb_system_status(self._h, int(bool(clear)), C.byref(f)))
+        return f.value
+
     def setSpin(self, site, spin, m=None):
         """l_setspin (spinsystem.cpp:1312-1361): optional length m."""
         sx, sy, sz = (list(spin) + [0, 0, 0])[:3]
@@ -675,6 +694,11 @@ class SpinOperation:
         """Reproduce (True, default) or fix the reference's arithmetic quirks."""
         _ck(_lib.mlb_op_set_quirks(self._h, int(bool(on))))
 
+    def encode(self, first_index=0):
+        """The bytes the reference's encode writes for this operator inside a
+        checkpoint (mlb_op_encode)."""
+        return _encode_stream(_lib.mlb_op_encode, self._h, first_index, self)
+
 
 class Exchange(SpinOperation):
     """Exchange (M/cpu/exchange): pathways from -> to with strength J."""
@@ -688,6 +712,7 @@ class Exchange(SpinOperation):
 
     def setPeriodicXYZ(self, px=True, py=True, pz=True):
         self._pbc = [int(bool(px)), int(bool(py)), int(bool(pz))]
+        _ck(_lib.mlb_exchange_set_pbc(self._h, *self._pbc))
 
     def periodicXYZ(self):
         return tuple(bool(p) for p in self._pbc)
@@ -921,12 +946,18 @@ class LongRange(SpinOperation):
 
     def setTruncation(self, r, x=None, y=None, z=None):
         if x is None:
-            g = [int(r)] * 4
+            g = [-1] * 4 if r == float("inf") else [int(r)] * 4
         else:
             xs = [max(1, int(v)) for v in (x, y, z)]
             g = [max(xs)] + xs
         arr = (C.c_int * 4)(*g)
         _ck(_lib.mlb_longrange_set_truncation(self._h, arr))
+
+    def truncation(self):
+        """getTruncation: four values, math.huge (inf) for an infinite radius."""
+        g = (C.c_int * 4)()
+        _ck(_lib.mlb_longrange_get_truncation(self._h, g))
+        return tuple(float("inf") if v == -1 else v for v in g)
 
     def setUnitCell(self, A, B, C_):
         abc = _f64(list(A) + list(B) + list(C_), 9)
@@ -970,6 +1001,11 @@ LongRange = _wab_methods(LongRange)
 class Dipole(LongRange):
     """Dipole (M/cpu/dipole): periodic-in-plane lattice-sum tensor."""
     KIND = 7
+
+    def setHugeRings(self, rings):
+        """Rings of 5 lattices summed for truncation math.huge (default 1000,
+        the reference's count); a B200 extension for checks."""
+        _ck(_lib.mlb_dipole_set_huge_rings(self._h, int(rings)))
 
     def setOpen(self, ox=True, oy=True, oz=True):
         """Open (zero-padded) boundaries in x and y instead of periodic images."""
@@ -1380,6 +1416,79 @@ class _LLGBase:
         _ck(_lib.mlb_llg_apply(self._h, frm._h, scale, dmdt._h, to._h, int(advance)))
 
 
+def _encode_stream(fn, h, first_index, owner):
+    n = C.c_size_t()
+    _ck(fn(h, int(first_index), None, 0, C.byref(n), None))
+    buf = C.create_string_buffer(n.value)
+    nobj = C.c_int()
+    _ck(fn(h, int(first_index), buf, n.value, C.byref(n), C.byref(nobj)))
+    owner._stream_objects = nobj.value
+    return buf.raw[:n.value]
+
+
+def _encode_llg(self, first_index=0):
+    """The bytes LLG::encode writes inside a checkpoint (mlb_llg_encode)."""
+    return _encode_stream(_lib.mlb_llg_encode, self._h, first_index, self)
+
+
+_LLGBase.encode = _encode_llg
+
+
+def decode(data, partial=False):
+    """An operator or LLG object from a stream written by encode or by the
+    reference (Exchange, Anisotropy, Anisotropy.Uniaxial, Anisotropy.Cubic,
+    Thermal, AppliedField, Dipole, LLG.Cartesian, LLG.Quaternion).
+    partial=True: the stream may continue; returns (object, bytes read,
+    objects read)."""
+    _ensure_init()
+    data = bytes(data)
+    h = _P()
+    used = C.c_size_t()
+    nobj = C.c_int()
+    kinds = {1: Exchange, 2: Anisotropy, 3: AnisotropyUniaxial, 4: AnisotropyCubic, 5: Thermal, 6: AppliedField,
+             7: Dipole}
+    rc = _lib.mlb_op_decode(data, len(data), C.byref(h), C.byref(used) if partial else None, C.byref(nobj))
+    if rc == MLB_OK:
+        k = C.c_int()
+        _ck(_lib.mlb_op_kind(h, C.byref(k)))
+        cls = kinds[k.value]
+        obj = cls.__new__(cls)
+        obj._h = h
+        obj._dims = _op_dims_from_stream(data)
+        if cls is Exchange:
+            p = (C.c_int * 3)()
+            _ck(_lib.mlb_exchange_get_pbc(h, p))
+            obj._pbc = list(p)
+        if cls is Thermal:
+            obj._rng = None
+    else:
+        rc2 = _lib.mlb_llg_decode(data, len(data), C.byref(h), C.byref(used) if partial else None, C.byref(nobj))
+        if rc2 != MLB_OK:
+            _ck(rc)
+        k = C.c_int()
+        _ck(_lib.mlb_llg_kind(h, C.byref(k)))
+        cls = LLGQuaternion if k.value == 1 else LLGCartesian
+        obj = cls.__new__(cls)
+        obj._h = h
+        obj._flags = _llg_flags_from_stream(data)
+    return (obj, used.value, nobj.value) if partial else obj
+
+
+def _op_dims_from_stream(data):
+    # LUA_TUSERDATA, type, char 111, index, char version, nx, ny, nz
+    o = 4 + 4 + 1 + 4 + 1
+    return tuple(int.from_bytes(data[o + 4 * i:o + 4 * i + 4], "little", signed=True) for i in range(3))
+
+
+def _llg_flags_from_stream(data):
+    import struct
+    o = 4 + 4 + 1 + 4
+    v = data[o]
+    tof, dis = struct.unpack_from("<ii", data, o + 1)
+    pre, dmp = struct.unpack_from("<dd", data, o + 9) if v == 1 else (1.0, 1.0)
+    return [tof, dis, pre, dmp]
+
+
 class LLGCartesian(_LLGBase):
     KIND = 0
 
@@ -1530,6 +1639,12 @@ class Ensemble:
         _ck(_lib.mlb_ensemble_get_stream(self._h, C.byref(out)))
         return out.value or 0
 
+    def status(self, clear=False):
+        """Status word of the steps run so far (bit 0: a non-finite spin)."""
+        f = C.c_uint()
+        _ck(_lib.mlb_ensemble_status(self._h, int(bool(clear)), C.byref(f)))
+        return f.value
+
     def setReplicaParams(self, rep, T, B=(0, 0, 0), dB=(0, 0, 0)):
         """Temperature and applied field (start, per-step sweep) of one replica."""
         _ck(_lib.mlb_ensemble_set_replica_params(self._h, int(rep), float(T), _dp(_f64(B, 3)), _dp(_f64(dB, 3))))
@@ -1600,6 +1715,11 @@ class Surrogate:
 
     def setSchedule(self, k, tol=1e-3, eps=0.0):
         _ck(_lib.mlb_surrogate_set_schedule(self._h, int(k), float(tol), float(eps)))
+
+    def setWaitLimit(self, polls):
+        """Polls of each tensor-core completion wait before it gives up and
+        sets the error flag (default 2**24; 0 exercises the failure path)."""
+        _ck(_lib.mlb_surrogate_set_wait_limit(self._h, int(polls)))
 
     def forward(self, x):
         xs = [_f32(x[c]) for c in range(3)]

@@ -244,6 +244,7 @@ struct mlb_system {
     double* nm_host = nullptr;      // pinned, 5 x 6 doubles (the device writes them directly)
     double* nm_host_dev = nullptr;  // the device's address of nm_host
     unsigned* nm_counter = nullptr; // blocks done in the current netMoment launch
+    unsigned* status = nullptr;     // device status word (bit 0: a step wrote a non-finite spin)
     cudaEvent_t nm_ev[4] = {};
     bool nm_pending[4] = {};
     double* red = nullptr;
@@ -277,6 +278,7 @@ struct mlb_op {
     std::vector<int> ef, et;
     std::vector<double> eJ;
     bool normalize = true;
+    int ex_pbc[3] = {1, 1, 1};   // setPeriodicXYZ (Exchange::Exchange sets all three)
     bool ex_dirty = true;
     ExchangeK exk{};
     DBuf<int> eptr, ecol;
@@ -305,7 +307,8 @@ struct mlb_op {
     double dB[3] = {0, 0, 0};
     // longrange
     double g = 1.0;
-    int gmax[4] = {1000, 1000, 1000, 1000};
+    int gmax[4] = {1000, 1000, 1000, 1000};   // gmax[0] = -1: math.huge
+    int rings = 1000;                          // rings of 5 lattices of the math.huge sum
     double ABC[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     int open[3] = {0, 0, 1};
     std::vector<double> t6[6];
@@ -748,7 +751,11 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
             CK(mlb::launch_tensor_open(op->nx, op->ny, op->nz, op->ABC, Px, Py, Pz, W.p, st));
         } else {
             const int zsign = op->quirks ? -1 : 1;
-            CK(mlb::launch_tensor_lattice(op->nx, op->ny, op->nz, op->gmax, op->ABC, Px, Py, Pz, zsign, W.p, st));
+            if (op->gmax[0] < 0)   // truncation math.huge: the reference's ring sum
+                CK(mlb::launch_tensor_rings(op->nx, op->ny, op->nz, op->rings, 5, op->ABC, Px, Py, Pz, zsign, W.p, st));
+            else
+                CK(mlb::launch_tensor_lattice(op->nx, op->ny, op->nz, op->gmax, op->ABC, Px, Py, Pz, zsign, W.p,
+                                              st));
             // keep the reference-layout tensor on the host (getMatrix / tensor arrays)
             DBuf<double> raw;
             raw.alloc(ne * 6);
@@ -1503,9 +1510,10 @@ void op_apply(mlb_op* op, mlb_system* s)
 }
 
 // ------------------------------------------------------------------ llg
-LlgK llgk(const mlb_llg* l, double dt)
+LlgK llgk(const mlb_llg* l, double dt, unsigned* status)
 {
     LlgK k;
+    k.status = status;
     k.type = l->kind == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
     k.thermal_only_first_term = l->tof;
     k.renorm = l->disable_renorm ? 0 : 1;
@@ -1530,6 +1538,7 @@ bool fast_fused_t(mlb_system* s, const TermsK& T, const mlb_llg* l, double dt, d
     if (T.nadd > 1 || (T.nadd == 1 && T.add_is_thermal[0])) return false;
     const double ms = s->ms_u, a = s->alpha, g = s->gamma;
     memset(&F, 0, sizeof(F));
+    F.status = s->status;
     F.nx = s->nx; F.ny = s->ny; F.nz = s->nz;
     F.ex = T.ex.mode == EX_STENCIL;
     if (F.ex) {
@@ -1667,7 +1676,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         FusedK P;
         P.sys = sysk(s, s->cur);
         P.terms = T;
-        P.llg = llgk(l, dt);
+        P.llg = llgk(l, dt, s->status);
         P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
         CK(mlb::launch_fused(P, dt_sys, s->rb, s->st));
     }
@@ -1729,7 +1738,7 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
         if (th >= 0) for (int c = 0; c < 3; c++) Ht[c] = dmdt->slots[th].h[c];
         void* out[3] = {to->sp[to->cur][0], to->sp[to->cur][1], to->sp[to->cur][2]};
         CK(mlb::launch_llg(sysk(from, from->cur), m, H, Ht, dmdt->sa, dmdt->sg, dmdt->alpha, dmdt->gamma,
-                           llgk(l, dt), out, to->rb, to->st));
+                           llgk(l, dt, to->status), out, to->rb, to->st));
     }
     if (cart) {
         if (dt != 0.0 && advance) to->time = from->time + dt;
@@ -1795,6 +1804,8 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     s->ms_token = ++g_ms_token;
     CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
     CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
+    CK(cudaMalloc(&s->status, sizeof(unsigned)));
+    CK(cudaMemset(s->status, 0, sizeof(unsigned)));
     CK(cudaMallocHost(&s->nm_host, sizeof(double) * 30));
     // pinned memory is mapped for the device under unified addressing; the
     // call fails (host side) where it is not
@@ -1821,6 +1832,7 @@ void free_system(mlb_system* s)
     cudaFree(s->sa);
     cudaFree(s->sg);
     cudaFree(s->dstep);
+    cudaFree(s->status);
     for (int q = 0; q < 2; q++)
         for (int d = 0; d < 5; d++)
             if (s->nm_exec[q][d]) cudaGraphExecDestroy(s->nm_exec[q][d]);
@@ -2160,6 +2172,7 @@ struct mlb_ensemble {
     float* d_rsig = nullptr;
     bool rpar_dirty = true;
     double* mom = nullptr;
+    unsigned* status = nullptr;       // device status word (bit 0: a non-finite spin)
 };
 
 namespace {
@@ -2254,6 +2267,7 @@ FastK ens_fastk(mlb_ensemble* e)
         F.dctr = &e->dstep->th_counter;
     }
     F.Bdev = nullptr;   // per replica (EnsLaunch::rB)
+    F.status = e->status;
     F.addw = 1.f;
     F.llg_type = c.llg == MLB_LLG_QUATERNION ? LLG_QUAT : LLG_CART;
     F.tof = 1;
@@ -2465,11 +2479,15 @@ void ens_autotune(mlb_ensemble* e)
             int best_v = 0;
             if (e->cfg.g != 0.0 && c.fast) {
                 float best = 1e30f;
-                for (int v : {0, 1}) {
+                // 2 (the 384-thread register kernel) differs from 0 only for 256-wide planes
+                const int nv = c.dip->plan->k.Py == 256 ? 3 : 2;
+                for (int v = 0; v < nv; v++) {
                     c.yz_variant = v;
                     const float ms = ens_time(e, [&] { ens_class_conv(e, c, s, e->st); }, 10);
                     std::snprintf(buf, sizeof(buf), "  class %dx%dx%d (%d replicas): (y,z) %s %.1f us per evaluation\n",
-                                  c.nx, c.ny, c.nz, c.nrep, v == 0 ? "register/automatic" : "Stockham", 1e3 * ms);
+                                  c.nx, c.ny, c.nz, c.nrep,
+                                  v == 0 ? "automatic" : (v == 1 ? "Stockham" : "register, one thread per column"),
+                                  1e3 * ms);
                     log += buf;
                     if (ms < best) { best = ms; best_v = v; }
                 }
@@ -2643,6 +2661,16 @@ int mlb_system_dims(const mlb_system* s, int out[3])
 {
     return guard([&] {
         out[0] = s->nx; out[1] = s->ny; out[2] = s->nz;
+    });
+}
+
+int mlb_system_status(mlb_system* s, int clear, unsigned* flags)
+{
+    return guard([&] {
+        if (!s || !flags) fail(MLB_EINVAL, "null argument");
+        CK(cudaStreamSynchronize(s->st));
+        CK(cudaMemcpy(flags, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (clear) CK(cudaMemset(s->status, 0, sizeof(unsigned)));
     });
 }
 
@@ -3217,6 +3245,330 @@ int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** 
     });
 }
 
+// ---------------------------------------------------------------- operator and LLG streams
+// The bytes the reference's CPU build writes for its operators and
+// integrators inside a checkpoint, as an exported Lua value: LUA_TUSERDATA,
+// the type id, char 111 and the object's index, then the class's encode
+// (M/ = src/modules/):
+//   SpinOperation base  char 0, nx, ny, nz, global scale (M/cpu/core/spinoperation.cpp:67-75)
+//   Exchange            base, char 1, normalizeMoments, pbc[3], count, (from, to, J) per pathway
+//                       (M/cpu/exchange/spinoperationexchange.cpp:52-73)
+//   Anisotropy          base, char 0, count, (site, axis[3], K) (spinoperationanisotropy.cpp:191-207)
+//   Anisotropy.Uniaxial base, char 0, count, (site, axis[3], K1, K2) (..._uniaxial.cpp:181-199)
+//   Anisotropy.Cubic    base, char 0, count, (site, axis1[3], axis2[3], K[3]) (..._cubic.cpp:239-258)
+//   Thermal             base, char 0, temperature, the scale array by its own encode: char 111,
+//                       its index, char 0, nx, ny, nz, flag, one value or all
+//                       (M/cpu/thermal/spinoperationthermal.cpp:51-61, array_core_cpu.h:200-225)
+//   AppliedField        base, char 0, B[3] (spinoperationappliedfield.cpp:33-42)
+//   Dipole              LongRange's encode (base, char 0, gmax[4], g, ABC[9],
+//                       spinoperationlongrange.cpp:55-68), char 0 (spinoperationdipole.cpp:35-41)
+//   LLG.Cartesian / LLG.Quaternion  char 1, thermalOnlyFirstTerm, disableRenormalization,
+//                       precession and damping scales (M/cpu/llg/llg.cpp:50-60)
+// Pathway sites are 0-based, as stored.  A plain LongRange is not written:
+// LongRange::encode begins with no object header, so no reader (the
+// reference's decodeLuaBaseObject included) can take its stream back.
+// Reading: the reference's Thermal::decode hands the stream to
+// Array::decode, which does not read the array's header (char 111 and
+// index) that the array's encode wrote; this reader takes the header.
+namespace {
+
+const char* op_type_name(int kind)
+{
+    switch (kind) {
+    case MLB_OP_EXCHANGE: return "Exchange";
+    case MLB_OP_ANISOTROPY: return "Anisotropy";
+    case MLB_OP_UNIAXIAL: return "Anisotropy.Uniaxial";
+    case MLB_OP_CUBIC: return "Anisotropy.Cubic";
+    case MLB_OP_THERMAL: return "Thermal";
+    case MLB_OP_APPLIEDFIELD: return "AppliedField";
+    case MLB_OP_DIPOLE: return "Dipole";
+    }
+    return nullptr;
+}
+
+void put_stream(const StreamOut& o, void* buf, size_t cap, size_t* len)
+{
+    *len = o.b.size();
+    if (buf && cap >= o.b.size()) std::memcpy(buf, o.b.data(), o.b.size());
+    else if (buf) fail(MLB_ERANGE, "buffer smaller than the stream (" + std::to_string(o.b.size()) + " bytes)");
+}
+
+void ck_rc(int rc)
+{
+    if (rc != MLB_OK) fail(rc, g_err);
+}
+
+} // namespace
+
+int mlb_op_encode(mlb_op* op, int first_index, void* buf, size_t cap, size_t* len, int* objects)
+{
+    return guard([&] {
+        if (!op || !len) fail(MLB_EINVAL, "null argument");
+        if (first_index < 0) fail(MLB_EINVAL, "negative object index");
+        const char* name = op_type_name(op->kind);
+        if (!name)
+            fail(MLB_EUNSUP, op->kind == MLB_OP_LONGRANGE
+                                 ? "LongRange::encode writes no object header: its stream cannot be read back"
+                                 : "this operator has no encoded form in the reference");
+        StreamOut o;
+        o.header(name, first_index);
+        int nobj = 1;
+        o.ch(0);                       // SpinOperation::encode
+        o.i32(op->nx); o.i32(op->ny); o.i32(op->nz);
+        o.f64(op->gs);
+        switch (op->kind) {
+        case MLB_OP_EXCHANGE:
+            o.ch(1);
+            o.i32(op->normalize ? 1 : 0);
+            for (int a = 0; a < 3; a++) o.i32(op->ex_pbc[a]);
+            o.i32((int)op->ef.size());
+            for (size_t p = 0; p < op->ef.size(); p++) { o.i32(op->ef[p]); o.i32(op->et[p]); o.f64(op->eJ[p]); }
+            break;
+        case MLB_OP_ANISOTROPY:
+        case MLB_OP_UNIAXIAL:
+        case MLB_OP_CUBIC: {
+            o.ch(0);
+            o.i32((int)op->asite.size());
+            const int per = op->kind == MLB_OP_ANISOTROPY ? 4 : (op->kind == MLB_OP_UNIAXIAL ? 5 : 12);
+            for (size_t j = 0; j < op->asite.size(); j++) {
+                const double* v = &op->apar[j * per];
+                o.i32(op->asite[j]);
+                if (op->kind == MLB_OP_CUBIC) {
+                    for (int a = 0; a < 6; a++) o.f64(v[a]);     // two axes; the third is computed
+                    for (int a = 0; a < 3; a++) o.f64(v[9 + a]);
+                } else {
+                    for (int a = 0; a < per; a++) o.f64(v[a]);
+                }
+            }
+            break;
+        }
+        case MLB_OP_THERMAL: {
+            o.ch(0);
+            o.f64(op->T);
+            // the scale array, written by its own encode (object header without type)
+            o.ch(kEncNew);
+            o.i32(first_index + 1);
+            o.ch(0);
+            o.i32(op->nx); o.i32(op->ny); o.i32(op->nz);
+            const size_t n = (size_t)op->nx * op->ny * op->nz;
+            bool same = true;
+            for (size_t i = 1; i < op->tscale.size() && same; i++) same = op->tscale[i] == op->tscale[0];
+            if (op->tscale.empty() || same) {
+                o.i32(1);
+                o.f64(op->tscale.empty() ? 1.0 : op->tscale[0]);
+            } else {
+                o.i32(0);
+                o.put(op->tscale.data(), sizeof(double) * n);
+            }
+            nobj = 2;
+            break;
+        }
+        case MLB_OP_APPLIEDFIELD:
+            o.ch(0);
+            for (int a = 0; a < 3; a++) o.f64(op->B[a]);
+            break;
+        case MLB_OP_DIPOLE:
+            o.ch(0);
+            for (int a = 0; a < 4; a++) o.i32(op->gmax[a]);
+            o.f64(op->g);
+            for (int a = 0; a < 9; a++) o.f64(op->ABC[a]);
+            o.ch(0);
+            break;
+        }
+        put_stream(o, buf, cap, len);
+        if (objects) *objects = nobj;
+    });
+}
+
+int mlb_op_decode(const void* buf, size_t len, mlb_op** out, size_t* used, int* objects)
+{
+    return guard([&] {
+        if (!buf || !out) fail(MLB_EINVAL, "null argument");
+        *out = nullptr;
+        StreamIn in{static_cast<const char*>(buf), len};
+        if (in.i32() != kLuaUserdata) fail(MLB_EINVAL, "malformed stream: expected an object");
+        const int32_t tid = in.i32();
+        int kind = 0;
+        for (int k : {MLB_OP_EXCHANGE, MLB_OP_ANISOTROPY, MLB_OP_UNIAXIAL, MLB_OP_CUBIC, MLB_OP_THERMAL,
+                      MLB_OP_APPLIEDFIELD, MLB_OP_DIPOLE})
+            if (tid == type_id(op_type_name(k))) kind = k;
+        if (!kind) fail(MLB_EUNSUP, "stream does not hold an operator this library reads");
+        if (in.ch() != kEncNew) fail(MLB_EINVAL, "malformed stream: bad object flag");
+        const int idx = in.i32();
+        if (in.ch() != 0) fail(MLB_EUNSUP, "unknown SpinOperation version");
+        const int nx = in.i32(), ny = in.i32(), nz = in.i32();
+        if (nx <= 0 || ny <= 0 || nz <= 0) fail(MLB_EINVAL, "malformed stream: bad operator size");
+        if ((long long)nx * ny * nz > (1LL << 31) - 1) fail(MLB_EUNSUP, "more than 2^31-1 sites");
+        const double gs = in.f64();
+        mlb_op* op = nullptr;
+        ck_rc(mlb_op_create(kind, nx, ny, nz, &op));
+        std::unique_ptr<mlb_op> hold(op);
+        op->gs = gs;
+        int nobj = 1;
+        switch (kind) {
+        case MLB_OP_EXCHANGE: {
+            const int v = in.ch();
+            if (v < 0 || v > 1) fail(MLB_EUNSUP, "unknown Exchange version");
+            op->normalize = v >= 1 ? in.i32() != 0 : false;   // version 0: old-style, not normalised
+            for (int a = 0; a < 3; a++) op->ex_pbc[a] = in.i32();
+            const int np = in.i32();
+            if (np < 0) fail(MLB_EINVAL, "malformed stream: negative pathway count");
+            std::vector<int> f(np), t(np);
+            std::vector<double> J(np);
+            for (int p = 0; p < np; p++) { f[p] = in.i32(); t[p] = in.i32(); J[p] = in.f64(); }
+            ck_rc(mlb_exchange_add_paths(op, f.data(), t.data(), J.data(), np));
+            break;
+        }
+        case MLB_OP_ANISOTROPY:
+        case MLB_OP_UNIAXIAL:
+        case MLB_OP_CUBIC: {
+            if (in.ch() != 0) fail(MLB_EUNSUP, "unknown Anisotropy version");
+            const int nops = in.i32();
+            if (nops < 0) fail(MLB_EINVAL, "malformed stream: negative count");
+            for (int j = 0; j < nops; j++) {
+                const int site = in.i32();
+                if (kind == MLB_OP_ANISOTROPY) {
+                    // Anisotropy::decode stores the axis as written
+                    // (addAnisotropy, spinoperationanisotropy.cpp:172-187);
+                    // only the Lua add normalises it
+                    if (site < 0 || site >= nx * ny * nz) fail(MLB_EINVAL, "malformed stream: site outside");
+                    op->asite.push_back(site);
+                    for (int a = 0; a < 4; a++) op->apar.push_back(in.f64());
+                    op->a_dirty = true;
+                } else if (kind == MLB_OP_UNIAXIAL) {
+                    // through addAnisotropy, as Uniaxial's decode (it scales by 1/dot(a, a))
+                    double ax[3];
+                    for (double& v : ax) v = in.f64();
+                    const double k1 = in.f64(), k2 = in.f64();
+                    ck_rc(mlb_uniaxial_add(op, site, ax, k1, k2));
+                } else {
+                    double a1[3], a2[3], K[3];
+                    for (double& v : a1) v = in.f64();
+                    for (double& v : a2) v = in.f64();
+                    for (double& v : K) v = in.f64();
+                    ck_rc(mlb_cubic_add(op, site, a1, a2, K));
+                }
+            }
+            break;
+        }
+        case MLB_OP_THERMAL: {
+            if (in.ch() != 0) fail(MLB_EUNSUP, "unknown Thermal version");
+            op->T = in.f64();
+            if (in.ch() != kEncNew) fail(MLB_EUNSUP, "Thermal scale array: expected a new object");
+            in.i32();
+            if (in.ch() != 0) fail(MLB_EUNSUP, "unknown Array version");
+            if (in.i32() != nx || in.i32() != ny || in.i32() != nz) fail(MLB_EINVAL, "scale array size differs");
+            const size_t n = (size_t)nx * ny * nz;
+            const int flag = in.i32();
+            if (flag == 1) {
+                const double v = in.f64();
+                if (v != 1.0) op->tscale.assign(n, v);
+            } else if (flag == 0) {
+                op->tscale.resize(n);
+                in.take(op->tscale.data(), sizeof(double) * n);
+            } else {
+                fail(MLB_EINVAL, "malformed stream: bad array flag");
+            }
+            op->tscale_dirty = !op->tscale.empty();
+            nobj = 2;
+            break;
+        }
+        case MLB_OP_APPLIEDFIELD:
+            if (in.ch() != 0) fail(MLB_EUNSUP, "unknown AppliedField version");
+            for (int a = 0; a < 3; a++) op->B[a] = in.f64();
+            break;
+        case MLB_OP_DIPOLE: {
+            if (in.ch() != 0) fail(MLB_EUNSUP, "unknown LongRange version");
+            int gm[4];
+            for (int& v : gm) v = in.i32();
+            const double g = in.f64();
+            double abc[9];
+            for (double& v : abc) v = in.f64();
+            if (in.ch() != 0) fail(MLB_EUNSUP, "unknown Dipole version");
+            for (int a = 0; a < 4; a++) op->gmax[a] = gm[a];
+            op->g = g;
+            std::memcpy(op->ABC, abc, sizeof(abc));
+            break;
+        }
+        }
+        (void)idx;
+        if (used) *used = in.pos;
+        else if (in.pos != len) fail(MLB_EINVAL, "stream continues after the operator");
+        if (objects) *objects = nobj;
+        *out = hold.release();
+    });
+}
+
+int mlb_llg_encode(mlb_llg* l, int first_index, void* buf, size_t cap, size_t* len, int* objects)
+{
+    return guard([&] {
+        if (!l || !len) fail(MLB_EINVAL, "null argument");
+        if (first_index < 0) fail(MLB_EINVAL, "negative object index");
+        StreamOut o;
+        o.header(l->kind == MLB_LLG_QUATERNION ? "LLG.Quaternion" : "LLG.Cartesian", first_index);
+        o.ch(1);
+        o.i32(l->tof);
+        o.i32(l->disable_renorm);
+        o.f64(l->precess);
+        o.f64(l->damp);
+        put_stream(o, buf, cap, len);
+        if (objects) *objects = 1;
+    });
+}
+
+int mlb_llg_decode(const void* buf, size_t len, mlb_llg** out, size_t* used, int* objects)
+{
+    return guard([&] {
+        if (!buf || !out) fail(MLB_EINVAL, "null argument");
+        *out = nullptr;
+        StreamIn in{static_cast<const char*>(buf), len};
+        if (in.i32() != kLuaUserdata) fail(MLB_EINVAL, "malformed stream: expected an object");
+        const int32_t tid = in.i32();
+        int kind = -1;
+        if (tid == type_id("LLG.Cartesian")) kind = MLB_LLG_CARTESIAN;
+        if (tid == type_id("LLG.Quaternion")) kind = MLB_LLG_QUATERNION;
+        if (kind < 0) fail(MLB_EUNSUP, "stream does not hold an LLG.Cartesian or LLG.Quaternion");
+        if (in.ch() != kEncNew) fail(MLB_EINVAL, "malformed stream: bad object flag");
+        in.i32();
+        // LLG::decode (llg.cpp:62-88): versions 0 and 1, scales from version 1
+        const int v = in.ch();
+        if (v < 0 || v > 1) fail(MLB_EUNSUP, "unknown LLG version");
+        std::unique_ptr<mlb_llg> l(new mlb_llg());
+        l->kind = kind;
+        l->tof = in.i32();
+        l->disable_renorm = in.i32();
+        if (v == 1) { l->precess = in.f64(); l->damp = in.f64(); }
+        if (used) *used = in.pos;
+        else if (in.pos != len) fail(MLB_EINVAL, "stream continues after the LLG object");
+        if (objects) *objects = 1;
+        *out = l.release();
+    });
+}
+
+int mlb_llg_kind(const mlb_llg* l, int* kind)
+{
+    return guard([&] {
+        if (!l || !kind) fail(MLB_EINVAL, "null argument");
+        *kind = l->kind;
+    });
+}
+
+int mlb_exchange_set_pbc(mlb_op* op, int px, int py, int pz)
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_EXCHANGE) fail(MLB_EINVAL, "not an Exchange operator");
+        op->ex_pbc[0] = px ? 1 : 0; op->ex_pbc[1] = py ? 1 : 0; op->ex_pbc[2] = pz ? 1 : 0;
+    });
+}
+
+int mlb_exchange_get_pbc(const mlb_op* op, int pbc[3])
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_EXCHANGE) fail(MLB_EINVAL, "not an Exchange operator");
+        for (int a = 0; a < 3; a++) pbc[a] = op->ex_pbc[a];
+    });
+}
+
 int mlb_system_copy(mlb_system* dst, mlb_system* src, int with_fields)
 {
     return guard([&] {
@@ -3588,11 +3940,34 @@ int mlb_longrange_set_truncation(mlb_op* op, const int gmax[4])
 {
     return guard([&] {
         g_version++;
-        for (int i = 0; i < 4; i++) op->gmax[i] = gmax[i];
-        if (op->gmax[0] < 0) fail(MLB_EUNSUP, "infinite truncation (extrapolated lattice sum) is not built");
+        // l_settrunc (spinoperationlongrange.cpp:505-568): a negative radius
+        // is math.huge, stored as -1 in every entry
+        if (gmax[0] < 0)
+            for (int i = 0; i < 4; i++) op->gmax[i] = -1;
+        else
+            for (int i = 0; i < 4; i++) op->gmax[i] = gmax[i];
         op->t6_valid = false;
         op->t6_edited = false;
         op->plan_dirty = true;
+    });
+}
+
+int mlb_dipole_set_huge_rings(mlb_op* op, int rings)
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_DIPOLE) fail(MLB_EINVAL, "not a Dipole operator");
+        if (rings < 1) fail(MLB_EINVAL, "at least one ring");
+        g_version++;
+        op->rings = rings;
+        if (op->gmax[0] < 0) { op->t6_valid = false; op->t6_edited = false; op->plan_dirty = true; }
+    });
+}
+
+int mlb_longrange_get_truncation(const mlb_op* op, int gmax[4])
+{
+    return guard([&] {
+        if (!op || !gmax) fail(MLB_EINVAL, "null argument");
+        for (int i = 0; i < 4; i++) gmax[i] = op->gmax[i];
     });
 }
 
@@ -4034,6 +4409,8 @@ int mlb_ensemble_create(int nrep, const int* dims, mlb_ensemble** out)
         CK(cudaMalloc(&e->dstep, sizeof(DevStep)));
         CK(cudaMemset(e->dstep, 0, sizeof(DevStep)));
         CK(cudaMalloc(&e->mom, sizeof(double) * 6 * nrep));
+        CK(cudaMalloc(&e->status, sizeof(unsigned)));
+        CK(cudaMemset(e->status, 0, sizeof(unsigned)));
         for (int q = 0; q < 2; q++) {
             CK(cudaMalloc(&e->d_rB[q], sizeof(double) * 3 * nrep));
             CK(cudaMemset(e->d_rB[q], 0, sizeof(double) * 3 * nrep));
@@ -4064,6 +4441,7 @@ int mlb_ensemble_destroy(mlb_ensemble* e)
         for (int c = 0; c < 3; c++) cudaFree(e->H[c]);
         cudaFree(e->rinfo); cudaFree(e->brep); cudaFree(e->bstart); cudaFree(e->dstep); cudaFree(e->mom);
         cudaFree(e->d_rB[0]); cudaFree(e->d_rB[1]); cudaFree(e->d_rdB); cudaFree(e->d_rsig);
+        cudaFree(e->status);
         for (EnsClass& c : e->cls) {
             delete c.dip;
             if (c.st) cudaStreamDestroy(c.st);
@@ -4188,6 +4566,16 @@ int mlb_ensemble_info(mlb_ensemble* e, long long* nsites, int* block_size, doubl
 int mlb_ensemble_get_stream(mlb_ensemble* e, void** stream)
 {
     return guard([&] { *stream = (void*)e->st; });
+}
+
+int mlb_ensemble_status(mlb_ensemble* e, int clear, unsigned* flags)
+{
+    return guard([&] {
+        if (!e || !flags) fail(MLB_EINVAL, "null argument");
+        CK(cudaStreamSynchronize(e->st));
+        CK(cudaMemcpy(flags, e->status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (clear) CK(cudaMemset(e->status, 0, sizeof(unsigned)));
+    });
 }
 
 int mlb_ensemble_set_replica_params(mlb_ensemble* e, int rep, double T, const double B[3], const double dB[3])
@@ -4371,8 +4759,11 @@ int mlb_dipole_write_wab(mlb_op* op, const char* filename)
         FILE* f = fopen(filename, "w");
         if (!f) fail(MLB_EINVAL, std::string("cannot write ") + filename);
         fprintf(f, "-- This file contains dipole interaction matrices\n\n");
-        fprintf(f, "gmax = {%i, %i, %i, %i} -- radial max, maxX, maxY, maxZ\n", op->gmax[0], op->gmax[1], op->gmax[2],
-                op->gmax[3]);
+        if (op->gmax[0] < 0)   // dipole_write_matrix (dipolesupport.cpp:360-365)
+            fprintf(f, "gmax = {math.huge, math.huge, math.huge, math.huge}  -- radial max, maxX, maxY, maxZ\n");
+        else
+            fprintf(f, "gmax = {%i, %i, %i, %i} -- radial max, maxX, maxY, maxZ\n", op->gmax[0], op->gmax[1],
+                    op->gmax[2], op->gmax[3]);
         fprintf(f, "nx, ny, nz = %i, %i, %i\n", op->nx, op->ny, op->nz);
         const double* A = op->ABC;
         fprintf(f, "ABC = {{%g, %g, %g}, --unit cell\n       {%g, %g, %g},\n       {%g, %g, %g}}\n\n", A[0], A[1],
@@ -4409,11 +4800,15 @@ int mlb_dipole_read_wab(mlb_op* op, const char* filename)
             (int)v[1] != op->ny || (int)v[2] != op->nz)
             fail(MLB_EINVAL, "WAB file: nx, ny, nz differ from the operator's");
         if (!wab_numbers_after(t, "gmax", v, huge)) fail(MLB_EINVAL, "WAB file: no gmax");
-        if (huge) fail(MLB_EUNSUP, "WAB file with infinite gmax (extrapolated sums are not supported)");
-        if (v.size() == 1) v.assign(4, v[0]);   // old files: one radius
-        if (v.size() != 4) fail(MLB_EINVAL, "WAB file: malformed gmax");
-        for (int i = 0; i < 4; i++)
-            if ((int)v[i] != op->gmax[i]) fail(MLB_EINVAL, "WAB file: gmax differs from the operator's");
+        if (huge) {
+            // gmax = {math.huge, ...}: a file of the extrapolated (ring) sum
+            if (op->gmax[0] >= 0) fail(MLB_EINVAL, "WAB file: gmax differs from the operator's");
+        } else {
+            if (v.size() == 1) v.assign(4, v[0]);   // old files: one radius
+            if (v.size() != 4) fail(MLB_EINVAL, "WAB file: malformed gmax");
+            for (int i = 0; i < 4; i++)
+                if ((int)v[i] != op->gmax[i]) fail(MLB_EINVAL, "WAB file: gmax differs from the operator's");
+        }
         if (!wab_numbers_after(t, "ABC", v, huge) || v.size() != 9) fail(MLB_EINVAL, "WAB file: malformed ABC");
         for (int i = 0; i < 9; i++)
             if (!wab_near(v[i], op->ABC[i])) fail(MLB_EINVAL, "WAB file: unit cell differs from the operator's");
@@ -4930,6 +5325,15 @@ void sur_advance(mlb_system* s)
 
 extern "C" {
 
+int mlb_surrogate_set_wait_limit(mlb_surrogate* s, unsigned polls)
+{
+    return guard([&] {
+        if (!s) fail(MLB_EINVAL, "null surrogate");
+        g_version++;   // captured steps carry the limit: capture again
+        s->k.wait_polls = polls;
+    });
+}
+
 int mlb_surrogate_create(mlb_op* op, int mx, int my, int rad, mlb_surrogate** out)
 {
     return guard([&] {
@@ -4950,7 +5354,7 @@ int mlb_surrogate_create(mlb_op* op, int mx, int my, int rad, mlb_surrogate** ou
         S->nx = nx; S->ny = ny; S->nz = nz; S->n = nx * ny * nz;
         SurK& k = S->k;
         k.nx = nx; k.ny = ny; k.nz = nz; k.C = C; k.CP = CP; k.mx = mx; k.my = my; k.rad = rad;
-        k.nxc = nx / 64; k.skip_if = nullptr; k.ratio = 1.f;
+        k.nxc = nx / 64; k.skip_if = nullptr; k.ratio = 1.f; k.wait_polls = 1u << 24;
         const int dia = 2 * rad + 1;
         S->nw = dia * dia * C * C;
         S->nr = mx * my * C * C * 2;

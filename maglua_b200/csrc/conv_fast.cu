@@ -432,6 +432,145 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
     }
 }
 
+// ------------------------------------------------------------------ (y,z) pass, three threads per column
+// The register form for a film's 256-wide planes with 768 threads per kx:
+// the y transforms as in k_yz_reg (line l = (comp, z) stored at
+// Z[comp][z][ky]); the column work split three ways so that no thread holds
+// all three components: (a) one thread per (comp, ky) takes the z transform
+// of its column in registers and writes the Pz spectrum values back in
+// place (Z[comp][kz][ky]); (b) one thread per (kz, ky) applies the 3x3 real
+// tensor in place; (c) one thread per (comp, ky) takes the inverse z
+// transform and writes the data layers back.  The same operations as
+// k_yz_reg, element for element, at a third of its registers per thread,
+// so twice the warps per SM.
+template <int PY, int PZ>
+struct YZC {
+    static constexpr int NT = 768;
+    static constexpr int T = fr::Split<PY>::T;
+    static constexpr int E = fr::Split<PY>::E;
+    static constexpr int EX = E * (T + 1);              // exchange elements per line
+    static size_t smem(int nz) { return ((size_t)3 * PZ * PY + (size_t)3 * nz * EX + PY) * sizeof(float2); }
+};
+
+template <int PY, int PZ>
+__global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __restrict__ twy,
+                                                   float2* __restrict__ spec, const float* __restrict__ ten6)
+{
+    using Y = YZC<PY, PZ>;
+    constexpr int NT = Y::NT, T = Y::T, E = Y::E;
+    extern __shared__ float2 sm[];
+    const int kx = blockIdx.x;
+    const int nz = c.nz, ny = c.ny;
+    const int nlines = 3 * nz;
+    float2* Z = sm;                                  // [3][PZ][PY]
+    float2* ex = Z + (size_t)3 * PZ * PY;            // [3 nz][EX]
+    float2* twl = ex + (size_t)nlines * Y::EX;       // [PY]
+    const float* Tk = ten6 + (size_t)kx * PZ * PY * 6;
+    if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(PZ * PY * 6 * sizeof(float));
+        if ((((uintptr_t)Tk) & 15) == 0 && (bytes & 15) == 0)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tk), "r"(bytes) : "memory");
+    }
+    for (int k = threadIdx.x; k < PY; k += NT) twl[k] = twy[k];
+    pdl_trigger();
+    pdl_wait();
+    if (c.run_if && *c.run_if == 0) return;
+    float2* sp = spec + (size_t)blockIdx.y * c.Kx * nlines * ny + (size_t)kx * nlines * ny;
+    __syncthreads();
+    const int lr = threadIdx.x / T, t = threadIdx.x % T;
+    const unsigned mask = T >= 32 ? 0xffffffffu : (((1u << T) - 1u) << (((threadIdx.x & 31) / T) * T));
+    // forward y transforms: SPEC row (comp, z) -> Z[comp][z][*] (natural order)
+    {
+        const int l = lr;
+        if (l < nlines) {
+            const int comp = l / nz, z = l % nz;
+            float2* exl = ex + (size_t)l * Y::EX;
+            float2 v[E];
+#pragma unroll
+            for (int j = 0; j < E; j++) {
+                const int y = t + T * j;
+                v[j] = y < ny ? sp[(size_t)l * ny + y] : make_float2(0.f, 0.f);
+            }
+            fr::line_fft<PY, -1, float2>(v, exl, t, mask, twl);
+            float2* Zl = Z + ((size_t)comp * PZ + z) * PY;
+#pragma unroll
+            for (int r = 0; r < E; r++) Zl[fr::out_index<PY>(t, r)] = v[r];
+        }
+    }
+    __syncthreads();
+    // (a) z transform of one (comp, ky) column, in place
+    for (int item = threadIdx.x; item < 3 * PY; item += NT) {
+        const int comp = item / PY, ky = item % PY;
+        float2* col = Z + (size_t)comp * PZ * PY + ky;
+        float2 v[PZ];
+#pragma unroll
+        for (int z = 0; z < PZ; z++) v[z] = z < nz ? col[(size_t)z * PY] : make_float2(0.f, 0.f);
+        fr::RegFFT<PZ, -1, float2>::run(v);
+#pragma unroll
+        for (int z = 0; z < PZ; z++) col[(size_t)z * PY] = v[z];
+    }
+    __syncthreads();
+    // (b) 3x3 real tensor at each (kz, ky); a thread's tensor loads are all
+    // issued before its first multiply
+    const float gg = c.g;
+    constexpr int NI = (PZ * PY + NT - 1) / NT;
+    float tt[NI][6];
+#pragma unroll
+    for (int q = 0; q < NI; q++) {
+        const int item = threadIdx.x + q * NT;
+        if (item < PZ * PY) {
+            const float* Tp = Tk + (size_t)item * 6;
+#pragma unroll
+            for (int e = 0; e < 6; e++) tt[q][e] = __ldg(Tp + e);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NI; q++) {
+        const int item = threadIdx.x + q * NT;
+        if (item >= PZ * PY) break;
+        const int kz = item / PY, ky = item % PY;
+        const float t0 = tt[q][0] * gg, t1 = tt[q][1] * gg, t2 = tt[q][2] * gg;
+        const float t3 = tt[q][3] * gg, t4 = tt[q][4] * gg, t5 = tt[q][5] * gg;
+        float2* z0 = Z + (size_t)kz * PY + ky;
+        const float2 a = z0[0], b = z0[(size_t)PZ * PY], d = z0[(size_t)2 * PZ * PY];
+        z0[0] = make_float2(t0 * a.x + t1 * b.x + t2 * d.x, t0 * a.y + t1 * b.y + t2 * d.y);
+        z0[(size_t)PZ * PY] = make_float2(t1 * a.x + t3 * b.x + t4 * d.x, t1 * a.y + t3 * b.y + t4 * d.y);
+        z0[(size_t)2 * PZ * PY] = make_float2(t2 * a.x + t4 * b.x + t5 * d.x, t2 * a.y + t4 * b.y + t5 * d.y);
+    }
+    __syncthreads();
+    // (c) inverse z transform, data layers back
+    for (int item = threadIdx.x; item < 3 * PY; item += NT) {
+        const int comp = item / PY, ky = item % PY;
+        float2* col = Z + (size_t)comp * PZ * PY + ky;
+        float2 v[PZ];
+#pragma unroll
+        for (int z = 0; z < PZ; z++) v[z] = col[(size_t)z * PY];
+        fr::RegFFT<PZ, +1, float2>::run(v);
+#pragma unroll
+        for (int z = 0; z < PZ; z++)
+            if (z < nz) col[(size_t)z * PY] = v[z];
+    }
+    __syncthreads();
+    // inverse y transforms: Z[comp][z][*] -> SPEC data rows
+    {
+        const int l = lr;
+        if (l < nlines) {
+            const int comp = l / nz, z = l % nz;
+            float2* exl = ex + (size_t)l * Y::EX;
+            const float2* Zl = Z + ((size_t)comp * PZ + z) * PY;
+            float2 v[E];
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = Zl[t + T * j];
+            fr::line_fft<PY, +1, float2>(v, exl, t, mask, twl);
+#pragma unroll
+            for (int r = 0; r < E; r++) {
+                const int y = fr::out_index<PY>(t, r);
+                if (y < ny) sp[(size_t)l * ny + y] = v[r];
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ split (y,z) passes, FP32
 // Planes larger than shared memory (a 256^3 open cube pads to 512 x 512):
 // the (y,z) pass as three passes through S2[kx][ky][comp][z] (data layers
@@ -840,7 +979,10 @@ struct XSCfg {
     static constexpr int ROWS = 2 * L / 3;
     static constexpr int R2 = ROWS / 2;
     static constexpr int KX = PX / 2 + 1;
-    static constexpr int LINE = L * PX;
+    // line stride in shared memory: one complex past the line, so that the
+    // same k of consecutive lines falls in different banks
+    static constexpr int LS = PX + 1;
+    static constexpr int LINE = L * LS;
     static constexpr int SPEC = 3 * ROWS * KX;
     static constexpr int BUF = LINE > SPEC ? LINE : SPEC;
     static constexpr int SMEM = (PX + 2 * BUF) * 8;
@@ -856,10 +998,10 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
                                                   float* __restrict__ oy, float* __restrict__ oz)
 {
     using X = XSCfg<PX>;
-    constexpr int KX = X::KX, NT = X::NT, ROWS = X::ROWS, R2 = X::R2;
+    constexpr int KX = X::KX, NT = X::NT, ROWS = X::ROWS, R2 = X::R2, LS = X::LS;
     extern __shared__ float2 sm[];
     float2* twl = sm;               // [PX]
-    float2* A = twl + PX;           // [L][PX] lines
+    float2* A = twl + PX;           // [L][LS] lines
     float2* B = A + X::BUF;         // [3][ROWS][KX] spectra, then scratch
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     const int nr = nz * ny;                     // rows (z, y), flattened
@@ -869,6 +1011,19 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     pdl_trigger();
     pdl_wait();
     if (c.run_if && *c.run_if == 0) return;
+    // the rows' spins and their z-neighbour rows, into L2 while the inverse
+    // transform runs (the step reads them after it)
+    if (threadIdx.x < 9) {
+        const int comp = threadIdx.x % 3, which = threadIdx.x / 3;
+        const int r = which == 0 ? row0 : (which == 1 ? row0 - ny : row0 + ny);
+        const float* base = comp == 0 ? sx : (comp == 1 ? sy : sz);
+        if (r >= 0 && r + rows_here <= nr) {
+            const float* p = base + (size_t)r * nx;
+            const unsigned bytes = (unsigned)(rows_here * nx * sizeof(float));
+            if ((((uintptr_t)p) & 15) == 0 && (bytes & 15) == 0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+        }
+    }
     const FastK F = fastk_resolved(F0);
     // 1. spectrum rows SPEC[kx][comp][row0 + row] -> B[(comp ROWS + row) KX + kx]
     constexpr int IS = (X::SPEC + NT - 1) / NT;
@@ -892,11 +1047,12 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     }
     __syncthreads();
     // line l = comp R2 + p: Z[k] = S_row(2p)[k] + i S_row(2p+1)[k], Hermitian completion
-    constexpr int IL = (X::LINE + NT - 1) / NT;
+    constexpr int LD = X::L * PX;
+    constexpr int IL = (LD + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < IL; it++) {
         const int idx = threadIdx.x + it * NT;
-        if (idx >= X::LINE) continue;
+        if (idx >= LD) continue;
         const int l = idx / PX, k = idx % PX;
         const int comp = l / R2, p = l % R2;
         const float2* Sa = B + (comp * ROWS + 2 * p) * KX;
@@ -904,39 +1060,45 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
         float2 a, b;
         if (k < KX) { a = Sa[k]; b = Sb[k]; }
         else { a = cconj(Sa[PX - k]); b = cconj(Sb[PX - k]); }
-        A[idx] = make_float2(a.x - b.y, a.y + b.x);
+        A[l * LS + k] = make_float2(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
-    const float2* R = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
+    const float2* R = fr::sm_fft<PX, +1, X::TPL, float2, LS>(A, B, l, tl, twl, true);
     float2* W = (R == A) ? B : A;   // free buffer: the new spins' lines (FWD)
-    const float* Rf = reinterpret_cast<const float*>(R);
-    float* Wf = reinterpret_cast<float*>(W);
-    // 2. field of the rows to the slot, then the step of every site
-    constexpr int IO = (ROWS * PX + NT - 1) / NT;
+    // 2. field of the rows to the slot, then the step of every site: one
+    // (row pair, x) per item, the pair's two rows the real and imaginary
+    // parts of one line element
+    constexpr int IP = (R2 * PX + NT - 1) / NT;
 #pragma unroll 1
-    for (int it = 0; it < IO; it++) {
+    for (int it = 0; it < IP; it++) {
         const int idx = threadIdx.x + it * NT;
-        const int row = idx / PX, x = idx % PX;
-        const int fo = 2 * (((row >> 1)) * PX + x) + (row & 1);   // float offset of (row, x) in component 0's lines
-        const bool live = idx < ROWS * PX && row < rows_here && x < nx;
-        float rx = 0.f, ry = 0.f, rz = 0.f;
-        if (live) {
-            const float Ax = Rf[fo], Ay = Rf[fo + 2 * R2 * PX], Az = Rf[fo + 4 * R2 * PX];
-            const int r = row0 + row, zz = r / ny, y = r - zz * ny;
-            const size_t i = (size_t)r * nx + x;
-            hx[i] = Ax; hy[i] = Ay; hz[i] = Az;
-            fused_site_v<LT, EXS, ANI, TH, true>(F, nx, ny, nz, x, y, zz, (int)i, sx, sy, sz, Ax, Ay, Az, rx, ry, rz);
-            ox[i] = rx; oy[i] = ry; oz[i] = rz;
+        if (idx >= R2 * PX) break;
+        const int p = idx / PX, x = idx % PX;
+        const float2 Ax2 = R[(0 * R2 + p) * LS + x], Ay2 = R[(1 * R2 + p) * LS + x], Az2 = R[(2 * R2 + p) * LS + x];
+        float2 o0 = make_float2(0.f, 0.f), o1 = o0, o2 = o0;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int row = 2 * p + h;
+            if (row < rows_here && x < nx) {
+                const float Ax = h ? Ax2.y : Ax2.x, Ay = h ? Ay2.y : Ay2.x, Az = h ? Az2.y : Az2.x;
+                const int r = row0 + row, zz = r / ny, y = r - zz * ny;
+                const size_t i = (size_t)r * nx + x;
+                hx[i] = Ax; hy[i] = Ay; hz[i] = Az;
+                float rx, ry, rz;
+                fused_site_v<LT, EXS, ANI, TH, true>(F, nx, ny, nz, x, y, zz, (int)i, sx, sy, sz, Ax, Ay, Az, rx, ry,
+                                                     rz);
+                ox[i] = rx; oy[i] = ry; oz[i] = rz;
+                if (h) { o0.y = rx; o1.y = ry; o2.y = rz; }
+                else { o0.x = rx; o1.x = ry; o2.x = rz; }
+            }
         }
-        if (fwd && idx < ROWS * PX) {
-            Wf[fo] = rx; Wf[fo + 2 * R2 * PX] = ry; Wf[fo + 4 * R2 * PX] = rz;
-        }
+        if (fwd) { W[(0 * R2 + p) * LS + x] = o0; W[(1 * R2 + p) * LS + x] = o1; W[(2 * R2 + p) * LS + x] = o2; }
     }
     if (!fwd) return;
     __syncthreads();
     // 3. forward transform of the new spins' lines, split into the two rows
-    const float2* Q = fr::sm_fft<PX, -1, X::TPL>(W, const_cast<float2*>(R), l, tl, twl, true);
+    const float2* Q = fr::sm_fft<PX, -1, X::TPL, float2, LS>(W, const_cast<float2*>(R), l, tl, twl, true);
     constexpr int IQ = (X::SPEC + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < IQ; it++) {
@@ -944,7 +1106,7 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
         const int kx = idx / (3 * ROWS), rem = idx % (3 * ROWS);
         const int comp = rem / ROWS, row = rem % ROWS;
         if (idx >= X::SPEC || row >= rows_here) continue;
-        const float2* Z = Q + (comp * R2 + (row >> 1)) * PX;
+        const float2* Z = Q + (comp * R2 + (row >> 1)) * LS;
         const float2 zk = Z[kx], zn = Z[(PX - kx) & (PX - 1)];
         float2 o;
         if ((row & 1) == 0) o = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
@@ -1160,6 +1322,12 @@ static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, 
         const size_t smem = yz_fast_smem(PY, PZ, c.nz);
         return launch_pdl(k_yz_fast<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZT<PY, PZ>::N), smem, st, c, twy, spec, ten6);
     }
+    if constexpr (PY == 256 && PZ <= 16) {
+        if (c.yz_variant != 2 && 3 * c.nz <= YZC<PY, PZ>::NT / YZC<PY, PZ>::T &&
+            YZC<PY, PZ>::smem(c.nz) <= 227 * 1024)
+            return launch_pdl(k_yz_col3<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZC<PY, PZ>::NT), YZC<PY, PZ>::smem(c.nz),
+                              st, c, twy, spec, ten6);
+    }
     if constexpr (PY >= 256) {
         if (yz_reg_ok(PY, PZ, c))
             return launch_pdl(k_yz_reg<PY, RPZ, 384>, dim3(c.Kx, c.nrep), dim3(384), YZR<PY, RPZ, 384>::smem(c.nz), st,
@@ -1246,9 +1414,21 @@ static cudaError_t cfg_yzr()
     return cudaFuncSetAttribute(k_yz_reg<PY, 16, NTH>, a, 227 * 1024);
 }
 
+static cudaError_t cfg_yzc()
+{
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 1>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 2>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 4>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 8>, a, 227 * 1024)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_yz_col3<256, 16>, a, 227 * 1024);
+}
+
 cudaError_t conv_fast_configure()
 {
     cudaError_t e;
+    if ((e = cfg_yzc()) != cudaSuccess) return e;
     if ((e = cfg_x<16>()) || (e = cfg_x<32>()) || (e = cfg_x<64>()) || (e = cfg_x<128>()) || (e = cfg_x<256>()) ||
         (e = cfg_x<512>()))
         return e;

@@ -201,15 +201,16 @@ struct SmStages<N, SIGN, TPL, N, C> {
     __device__ __forceinline__ static C* run(C* a, C*, int, const C*, bool) { return a; }
 };
 
-// Transform line l (data at a + l*N, scratch at b + l*N) by its TPL threads
-// (tl = thread index within the line).  Every thread of the CTA must call
-// this (act = false for threads without a line): it synchronises the CTA
-// after each stage.  Returns the base (a or b) that holds the result.
-template <int N, int SIGN, int TPL, typename C>
+// Transform line l (data at a + l*LS, scratch at b + l*LS; LS = N or a
+// padded line stride) by its TPL threads (tl = thread index within the
+// line).  Every thread of the CTA must call this (act = false for threads
+// without a line): it synchronises the CTA after each stage.  Returns the
+// base (a or b) that holds the result.
+template <int N, int SIGN, int TPL, typename C, int LS = N>
 __device__ __forceinline__ C* sm_fft(C* a, C* b, int l, int tl, const C* tw, bool act)
 {
-    C* r = SmStages<N, SIGN, TPL, 1, C>::run(a + (size_t)l * N, b + (size_t)l * N, tl, tw, act);
-    return r == a + (size_t)l * N ? a : b;
+    C* r = SmStages<N, SIGN, TPL, 1, C>::run(a + (size_t)l * LS, b + (size_t)l * LS, tl, tw, act);
+    return r == a + (size_t)l * LS ? a : b;
 }
 
 } // namespace fr

@@ -175,5 +175,6 @@ __device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY,
         }
     }
     rx = nx_; ry = ny_; rz = nz_;
+    if (F.status && !(isfinite(nx_) && isfinite(ny_) && isfinite(nz_))) atomicOr(F.status, 1u);
 }
 

@@ -322,6 +322,7 @@ __global__ void __launch_bounds__(256) k_fused_step(FusedK P, double dt_sys)
         out = llg_site<R>(P.llg, S, S, F.H, F.Hth, ms, alpha_at<R>(P.sys, i), gamma_at<R>(P.sys, i));
     }
     if (P.llg.renorm) out = renorm<R>(out, ms);
+    if (P.llg.status && !(isfinite(out.x) && isfinite(out.y) && isfinite(out.z))) atomicOr(P.llg.status, 1u);
     static_cast<R*>(P.ox)[i] = out.x;
     static_cast<R*>(P.oy)[i] = out.y;
     static_cast<R*>(P.oz)[i] = out.z;
@@ -369,6 +370,7 @@ __global__ void __launch_bounds__(256) k_llg(SysK from, const void* mx, const vo
         out = llg_site<R>(L, S, M, H, Ht, ms, a, g);
     }
     if (L.renorm) out = renorm<R>(out, ms);
+    if (L.status && !(isfinite(out.x) && isfinite(out.y) && isfinite(out.z))) atomicOr(L.status, 1u);
     ox[i] = out.x; oy[i] = out.y; oz[i] = out.z;
 }
 
@@ -780,6 +782,73 @@ __global__ void k_tensor_lattice(int nx, int ny, int nz, int G, int lim0, int li
     const size_t plane = (size_t)Px * Py * Pz;
     const size_t off = ((size_t)zi * Py + j) * Px + i;
     for (int q = 0; q < 6; q++) W[q * plane + off] = make_double2(acc[q], 0.0);
+}
+
+// The Dipole tensor of truncation math.huge (M/cpu/dipole/dipolesupport.cpp:
+// 771-835): the images of each element summed ring by ring, rings of lstep
+// lattices (getWAB with smin = q lstep, smax = smin + lstep: for smin = 0 the
+// full square |X|, |Y| <= lstep - 1, else the square ring between), nrings
+// rings, each ring's sum added to the element's running total in ring
+// order.  (The reference's extrapolation never reports convergence -- its
+// C side reads a second return value its Lua function does not give -- so
+// its result is this sum over its maxiter = 1000 rings of 5 lattices.)  One
+// warp per element: the lanes split each ring's images, a shuffle tree
+// gives the ring's sum, lane 0 keeps the total.  FP64 throughout.
+__global__ void k_tensor_rings(int nx, int ny, int nz, int nrings, int lstep, double A0, double A1, double A2,
+                               double B0, double B1, double B2, double C0, double C1, double C2, int Px, int Py,
+                               int Pz, int zsign, double2* W)
+{
+    const long long ne = (long long)nx * ny * (2 * nz - 1);
+    const long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= ne) return;   // whole warps leave together
+    const int i = (int)(e % nx);
+    const int j = (int)((e / nx) % ny);
+    const int k = (int)(e / ((long long)nx * ny)) - (nz - 1);
+    double tot[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < nrings; q++) {
+        const int mn = q * lstep, mx = mn + lstep;
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        // the ring as 2 full-width bands (|Y| >= mn) and 2 side bands (|Y| < mn)
+        const int nrect = mn == 0 ? 1 : 4;
+        for (int r = 0; r < nrect; r++) {
+            int ax, bx, ay, by;
+            if (mn == 0) { ax = -(mx - 1); bx = mx - 1; ay = -(mx - 1); by = mx - 1; }
+            else if (r == 0) { ax = -(mx - 1); bx = mx - 1; ay = mn; by = mx - 1; }
+            else if (r == 1) { ax = -(mx - 1); bx = mx - 1; ay = -(mx - 1); by = -mn; }
+            else if (r == 2) { ax = -(mx - 1); bx = -mn; ay = -(mn - 1); by = mn - 1; }
+            else { ax = mn; bx = mx - 1; ay = -(mn - 1); by = mn - 1; }
+            // lanes stride along the band's long side, each walks the short side
+            const bool xlong = (bx - ax) >= (by - ay);
+            const int l0 = xlong ? ax : ay, l1 = xlong ? bx : by;
+            const int s0 = xlong ? ay : ax, s1 = xlong ? by : bx;
+            for (int u = l0 + lane; u <= l1; u += 32) {
+                for (int v = s0; v <= s1; v++) {
+                    const long long X = xlong ? u : v, Y = xlong ? v : u;
+                    const double fx = (double)(X * nx + i), fy = (double)(Y * ny + j), fz = (double)k;
+                    const double rx = __dadd_rn(__dadd_rn(__dmul_rn(fx, A0), __dmul_rn(fy, B0)), __dmul_rn(fz, C0));
+                    const double ry = __dadd_rn(__dadd_rn(__dmul_rn(fx, A1), __dmul_rn(fy, B1)), __dmul_rn(fz, C1));
+                    const double rz = __dadd_rn(__dadd_rn(__dmul_rn(fx, A2), __dmul_rn(fy, B2)), __dmul_rn(fz, C2));
+                    double g6[6];
+                    gamma_dip_d(rx, ry, rz, g6);
+#pragma unroll
+                    for (int c = 0; c < 6; c++) acc[c] += g6[c];
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            double v = acc[c];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            tot[c] += v;   // meaningful in lane 0
+        }
+    }
+    if (lane != 0) return;
+    int zi = (zsign * k) % Pz;
+    if (zi < 0) zi += Pz;
+    const size_t plane = (size_t)Px * Py * Pz;
+    const size_t off = ((size_t)zi * Py + j) * Px + i;
+    for (int c = 0; c < 6; c++) W[c * plane + off] = make_double2(tot[c], 0.0);
 }
 
 // Also stores the raw (unpadded) reference tensor for inspection:
@@ -1383,6 +1452,16 @@ cudaError_t launch_tensor_lattice(int nx, int ny, int nz, const int gmax[4], con
     k_tensor_lattice<<<blocks_for(ne, 128), 128, 0, st>>>(nx, ny, nz, gmax[0], lim0, limx, limy, ABC[0], ABC[1],
                                                           ABC[2], ABC[3], ABC[4], ABC[5], ABC[6], ABC[7], ABC[8],
                                                           Px, Py, Pz, zsign, W);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tensor_rings(int nx, int ny, int nz, int nrings, int lstep, const double ABC[9], int Px, int Py,
+                                int Pz, int zsign, double2* W, cudaStream_t st)
+{
+    const long long ne = (long long)nx * ny * (2 * nz - 1);
+    k_tensor_rings<<<blocks_for(ne * 32, 256), 256, 0, st>>>(nx, ny, nz, nrings, lstep, ABC[0], ABC[1], ABC[2], ABC[3],
+                                                              ABC[4], ABC[5], ABC[6], ABC[7], ABC[8], Px, Py, Pz,
+                                                              zsign, W);
     return cudaGetLastError();
 }
 

@@ -93,6 +93,7 @@ struct TermsK {
 };
 
 struct LlgK {
+    unsigned* status;         // bit 0 set when a new spin is not finite (null: not checked)
     int type;
     int thermal_only_first_term;
     int renorm;
@@ -170,6 +171,7 @@ struct FastKT {
     R addw;
     int llg_type, tof, renorm, dt_zero;
     R dt, precess, c_prec, c_damp, c_rot, ms;
+    unsigned* status;         // bit 0 set when a new spin is not finite (null: not checked)
 };
 // FP32 state (every fused kernel); FastKT<double> for FP64 state
 typedef FastKT<float> FastK;
@@ -189,6 +191,7 @@ struct SurK {
     int nxc;                  // 128-wide x chunks of the x-DFT (nx / 128)
     const int* skip_if;       // kernels return at once while *skip_if != 0
     float ratio;              // strength now / strength at training
+    unsigned wait_polls;      // polls of a tensor-core completion wait before it gives up
 };
 
 // Device state of a surrogate-driven run (one block per surrogate).

@@ -130,6 +130,8 @@ cudaError_t launch_conv(const ConvK& c, const FftLen& Lx, const FftLen& Ly, cons
                         int rb, cudaStream_t st);
 cudaError_t launch_tensor_lattice(int nx, int ny, int nz, const int gmax[4], const double ABC[9], int Px,
                                   int Py, int Pz, int zsign, double2* W, cudaStream_t st);
+cudaError_t launch_tensor_rings(int nx, int ny, int nz, int nrings, int lstep, const double ABC[9], int Px, int Py,
+                                int Pz, int zsign, double2* W, cudaStream_t st);
 cudaError_t launch_tensor_extract_ref(int nx, int ny, int nz, int Px, int Py, int Pz, int zsign,
                                       const double2* W, double* out, cudaStream_t st);
 cudaError_t launch_tensor_open(int nx, int ny, int nz, const double ABC[9], int Px, int Py, int Pz,

@@ -35,7 +35,10 @@
 
 namespace {
 
-constexpr uint32_t kWaitPolls = 1u << 24;   // bounded mbarrier wait (~0.1 s)
+// After a completion wait gives up (SurK::wait_polls polls; the error flag
+// is set) a second bounded wait lets the launch's own MMAs finish before the
+// accumulator is read and its TMEM freed.
+constexpr uint32_t kDrainPolls = 1u << 26;
 
 __device__ __forceinline__ uint32_t pack2(float a, float b)
 {
@@ -149,8 +152,11 @@ __global__ void __launch_bounds__(256) k_sur_xdft(SurK k, const float* a0, const
         }
     }
     if (warp == 0) {
-        const bool ok = umma::mbar_wait(&bar, 0, kWaitPolls);
-        if (!ok && lane == 0) atomicOr(err, 1);
+        const bool ok = umma::mbar_wait(&bar, 0, k.wait_polls);
+        if (!ok) {
+            if (lane == 0) atomicOr(err, 1);
+            umma::mbar_wait(&bar, 0, kDrainPolls);
+        }
         umma::fence_before_sync();
     }
     __syncthreads();
@@ -375,8 +381,11 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
             umma::mma_commit(&bar);
         }
         __syncwarp();
-        const bool ok = umma::mbar_wait(&bar, 0, kWaitPolls);
-        if (!ok && lane == 0) atomicOr(q.err, 1);
+        const bool ok = umma::mbar_wait(&bar, 0, k.wait_polls);
+        if (!ok) {
+            if (lane == 0) atomicOr(q.err, 1);
+            umma::mbar_wait(&bar, 0, kDrainPolls);
+        }
         umma::fence_before_sync();
     }
     __syncthreads();

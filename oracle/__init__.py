@@ -109,6 +109,7 @@ lib.orc_thermal_apply_noise.argtypes = [_PSS, C.c_double, _D, C.c_double, _D, _D
 lib.orc_thermal_draw.argtypes = [_PSS, C.c_double, C.POINTER(_MT), _D, _D, _D]
 lib.orc_zeeman_apply.argtypes = [_PSS, _D, C.c_double]
 lib.orc_dipole_tensor.argtypes = [C.c_int, C.c_int, C.c_int, _I, _D, _D, _D, _D, _D, _D, _D]
+lib.orc_dipole_tensor_rings.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D]
 lib.orc_longrange_apply.argtypes = [_PSS, C.c_char_p, _D * 6, C.c_double, C.c_double]
 lib.orc_lr_new.restype = C.c_void_p
 lib.orc_lr_new.argtypes = [C.c_int, C.c_int, C.c_int, _D * 6]
@@ -331,6 +332,16 @@ def dipole_tensor(nx, ny, nz, gmax=(1000, 1000, 1000, 1000), ABC=(1, 0, 0, 0, 1,
     n = nx * ny * (2 * nz - 1)
     arrs = [np.zeros(n) for _ in range(6)]
     lib.orc_dipole_tensor(nx, ny, nz, _ip(g), _dp(abc), *[_dp(a) for a in arrs])
+    return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
+
+
+def dipole_tensor_rings(nx, ny, nz, nrings=1000, lstep=5, ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1)):
+    """The Dipole tensor of truncation math.huge (orc_dipole_tensor_rings):
+    six arrays of shape (2nz-1, ny, nx)."""
+    abc = _f64(ABC)
+    n = nx * ny * (2 * nz - 1)
+    arrs = [np.zeros(n) for _ in range(6)]
+    lib.orc_dipole_tensor_rings(nx, ny, nz, _dp(abc), int(nrings), int(lstep), *[_dp(a) for a in arrs])
     return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
 
 
@@ -825,6 +836,126 @@ def encode_spinsystem(nx, ny, nz, alpha, dt, gamma, time, x, y, z, ms, site_alph
             idx += 1
     out += struct.pack("=i", 0)
     return bytes(out)
+
+
+def _enc_op_head(out, type_name, idx, nx, ny, nz, gs):
+    """encodeT header of an operator (type id, ENCODE_PREAMBLE) and
+    SpinOperation::encode (M/cpu/core/spinoperation.cpp:67-75): version 0,
+    nx, ny, nz, global scale."""
+    import struct
+    out += struct.pack("=iibib", LUA_TUSERDATA, type_hash32(type_name), ENC_NEW, idx, 0)
+    out += struct.pack("=iiid", nx, ny, nz, gs)
+
+
+def encode_exchange(nx, ny, nz, gs, normalize, pbc, frm, to, J, first_index=0):
+    """Exchange::encode (M/cpu/exchange/spinoperationexchange.cpp:52-73):
+    version 1, normalizeMoments, pbc[3], the pathway count and (from, to, J)
+    per pathway, sites 0-based as stored."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "Exchange", first_index, nx, ny, nz, gs)
+    out += struct.pack("=biiiii", 1, int(normalize), *[int(p) for p in pbc], len(frm))
+    for f, t, j in zip(frm, to, J):
+        out += struct.pack("=iid", int(f), int(t), float(j))
+    return bytes(out)
+
+
+def anisotropy_add_axis(a):
+    """The axis Anisotropy's Lua add stores (l_add,
+    spinoperationanisotropy.cpp:385-398): divided by its length."""
+    import math
+    a0, a1, a2 = (float(v) for v in a)
+    lena = math.sqrt(a0 * a0 + a1 * a1 + a2 * a2)
+    return (a0 / lena, a1 / lena, a2 / lena)
+
+
+def encode_anisotropy(nx, ny, nz, gs, sites, axes, K, first_index=0):
+    """Anisotropy::encode (M/cpu/anisotropy/spinoperationanisotropy.cpp:
+    191-207): version 0, the count, (site, axis[3], K) per entry."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "Anisotropy", first_index, nx, ny, nz, gs)
+    out += struct.pack("=bi", 0, len(sites))
+    for st, ax, k in zip(sites, axes, K):
+        out += struct.pack("=idddd", int(st), *[float(v) for v in ax], float(k))
+    return bytes(out)
+
+
+def encode_uniaxial(nx, ny, nz, gs, sites, axes, K1, K2, first_index=0):
+    """AnisotropyUniaxial::encode (..._uniaxial.cpp:181-199): version 0, the
+    count, (site, axis[3], K1, K2) per entry."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "Anisotropy.Uniaxial", first_index, nx, ny, nz, gs)
+    out += struct.pack("=bi", 0, len(sites))
+    for st, ax, k1, k2 in zip(sites, axes, K1, K2):
+        out += struct.pack("=iddddd", int(st), *[float(v) for v in ax], float(k1), float(k2))
+    return bytes(out)
+
+
+def encode_cubic(nx, ny, nz, gs, sites, axes9, K3, first_index=0):
+    """AnisotropyCubic::encode (..._cubic.cpp:239-258): version 0, the count,
+    (site, the first two axes, K[3]) per entry (the third axis is computed
+    on decode)."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "Anisotropy.Cubic", first_index, nx, ny, nz, gs)
+    out += struct.pack("=bi", 0, len(sites))
+    for st, ax, k in zip(sites, axes9, K3):
+        out += struct.pack("=i", int(st)) + struct.pack("=6d", *[float(v) for v in ax[:6]])
+        out += struct.pack("=3d", *[float(v) for v in k])
+    return bytes(out)
+
+
+def encode_thermal(nx, ny, nz, gs, T, scale=None, first_index=0):
+    """Thermal::encode (M/cpu/thermal/spinoperationthermal.cpp:51-61):
+    version 0, the temperature, then scale->encode: the array's own
+    ENCODE_PREAMBLE (char 111, the next object index) and Array::encode
+    without an encodeT type header (array_core_cpu.h:200-225)."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "Thermal", first_index, nx, ny, nz, gs)
+    out += struct.pack("=bd", 0, float(T))
+    out += struct.pack("=bibiii", ENC_NEW, first_index + 1, 0, nx, ny, nz)
+    a = np.ones(nx * ny * nz) if scale is None else np.ascontiguousarray(scale, dtype=np.float64).ravel()
+    if np.all(a == a[0]):
+        out += struct.pack("=id", 1, float(a[0]))
+    else:
+        out += struct.pack("=i", 0) + a.tobytes()
+    return bytes(out)
+
+
+def encode_appliedfield(nx, ny, nz, gs, B, first_index=0):
+    """AppliedField::encode (spinoperationappliedfield.cpp:33-42): version
+    0, B[3]."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "AppliedField", first_index, nx, ny, nz, gs)
+    out += struct.pack("=bddd", 0, *[float(v) for v in B])
+    return bytes(out)
+
+
+def encode_dipole(nx, ny, nz, gs, gmax, g, ABC, first_index=0):
+    """Dipole::encode (M/cpu/dipole/spinoperationdipole.cpp:35-41): the
+    preamble, LongRange::encode (spinoperationlongrange.cpp:55-68: the base,
+    version 0, gmax[4], g, ABC[9]), then the Dipole's version 0."""
+    import struct
+    out = bytearray()
+    _enc_op_head(out, "Dipole", first_index, nx, ny, nz, gs)
+    out += struct.pack("=biiii", 0, *[int(v) for v in gmax])
+    out += struct.pack("=d", float(g)) + struct.pack("=9d", *[float(v) for v in ABC])
+    out += struct.pack("=b", 0)
+    return bytes(out)
+
+
+def encode_llg(kind, thermal_only_first_term=1, disable_renormalization=0, precess=1.0, damp=1.0,
+               first_index=0):
+    """LLG::encode (M/cpu/llg/llg.cpp:50-60) of an LLG.Cartesian or
+    LLG.Quaternion: version 1, the two flags, the precession and damping
+    scales."""
+    import struct
+    return struct.pack("=iibibiidd", LUA_TUSERDATA, type_hash32("LLG." + kind), ENC_NEW, first_index, 1,
+                       int(thermal_only_first_term), int(disable_renormalization), float(precess), float(damp))
 
 
 def decode_spinsystem(buf):

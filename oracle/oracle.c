@@ -676,6 +676,66 @@ void orc_dipole_tensor(int nx, int ny, int nz, const int gmax[4], const double A
             }
 }
 
+/* getWAB_range over one rectangle of images [ax, bx] x [ay, by] (X outer,
+ * Y inner) with the truncation of the math.huge sum, truemax = {1e9, ...}:
+ * every box and radial test passes for lattices of fewer than 1e5 sites a
+ * side out to 5000 lattices (dipolesupport.cpp:71-128, the z test's
+ * truemax[4] taken large as in get_wab). */
+static void wab_rect(const double* ABC, int nA, int nB, int ix, int iy, int iz, int ax, int ay, int bx, int by,
+                     double* acc)
+{
+    for (long long X = ax; X <= bx; X++) {
+        const long long xx = X * nA + ix;
+        for (long long Y = ay; Y <= by; Y++) {
+            const long long yy = Y * nB + iy;
+            const long long zz = iz;
+            const double rx = ((double)xx) * ABC[0] + ((double)yy) * ABC[3] + ((double)zz) * ABC[6];
+            const double ry = ((double)xx) * ABC[1] + ((double)yy) * ABC[4] + ((double)zz) * ABC[7];
+            const double rz = ((double)xx) * ABC[2] + ((double)yy) * ABC[5] + ((double)zz) * ABC[8];
+            double g6[6];
+            gamma_dip(rx, ry, rz, g6);
+            for (int q = 0; q < 6; q++) acc[q] += g6[q];
+        }
+    }
+}
+
+/* The Dipole tensor of truncation math.huge (dipoleLoad, dipolesupport.cpp:
+ * 771-835): per element the images are summed ring by ring, rings of lstep
+ * lattices (getWAB with smin = q lstep, smax = smin + lstep: the full square
+ * for smin = 0, else its eight rectangles in getWAB's order, :150-232), each
+ * ring's sum added to the running total.  The reference asks its Lua
+ * extrapolate() for two results where the function returns one, so the
+ * convergence flag it reads is nil and the loop always runs its maxiter =
+ * 1000 rings of 5 lattices; the result is the last running total.  nrings
+ * and lstep are parameters here (1000 and 5 in the reference). */
+void orc_dipole_tensor_rings(int nx, int ny, int nz, const double ABC[9], int nrings, int lstep,
+                             double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ)
+{
+    int c = 0;
+    for (int k = -nz + 1; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                double s[6] = {0, 0, 0, 0, 0, 0};
+                for (int q = 0; q < nrings; q++) {
+                    const int mn = q * lstep, mx = mn + lstep;
+                    double t[6] = {0, 0, 0, 0, 0, 0};
+                    if (mn == 0) {
+                        wab_rect(ABC, nx, ny, i, j, k, -(mx - 1), -(mx - 1), mx - 1, mx - 1, t);
+                    } else {
+                        const int ax[8] = {-(mx - 1), -mn + 1, mn, -(mx - 1), mn, -(mx - 1), -mn + 1, mn};
+                        const int bx[8] = {-mn, mn - 1, mx - 1, -mn, mx - 1, -mn, mn - 1, mx - 1};
+                        const int ay[8] = {mn, mn, mn, -(mn - 1), -(mn - 1), -(mx - 1), -(mx - 1), -(mx - 1)};
+                        const int by[8] = {mx - 1, mx - 1, mx - 1, mn - 1, mn - 1, -mn, -mn, -mn};
+                        for (int r = 0; r < 8; r++) wab_rect(ABC, nx, ny, i, j, k, ax[r], ay[r], bx[r], by[r], t);
+                    }
+                    for (int a = 0; a < 6; a++) s[a] += t[a];
+                }
+                XX[c] = s[0]; XY[c] = s[1]; XZ[c] = s[2];
+                YY[c] = s[3]; YZ[c] = s[4]; ZZ[c] = s[5];
+                c++;
+            }
+}
+
 /* LongRange context: the tensor transforms of updateData, prescaled by
  * 1/(nx*ny), spinoperationlongrange.cpp:275-312, plus workspaces. */
 struct orc_lr {

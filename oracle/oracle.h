@@ -87,6 +87,10 @@ void orc_zeeman_apply(orc_ss* ss, const double B[3], double gscale);
 
 /* Dipole tensor: periodic-in-plane lattice sum, dipolesupport.cpp:34-240,717-851.
  * Output arrays have nx*ny*(2nz-1) entries, index i + nx*(j + ny*(k+nz-1)). */
+/* The math.huge Dipole tensor: images summed in rings of lstep lattices,
+ * nrings rings (the reference: 1000 rings of 5). */
+void orc_dipole_tensor_rings(int nx, int ny, int nz, const double ABC[9], int nrings, int lstep,
+                             double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ);
 void orc_dipole_tensor(int nx, int ny, int nz, const int gmax[4], const double ABC[9],
                        double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ);
 /* LongRange::apply, spinoperationlongrange.cpp:275-312,354-440.

@@ -166,3 +166,59 @@ def _oracle_stream_at(ss, first):
     nx, ny, nz = ss._dims
     return O.encode_spinsystem(nx, ny, nz, ss.alpha(), ss.timeStep(), ss.gamma(), ss.time(), x, y, z, ms,
                                first_index=first)
+
+
+def test_checkpoint_of_operators_and_llg_resumes_the_run(M):
+    """A whole script state -- the SpinSystem, Exchange, Anisotropy,
+    Anisotropy.Cubic, AppliedField, Dipole and the LLG -- encoded into one
+    stream (object indices running on), decoded into new objects, and the run
+    resumed from them: the same trajectory bit for bit as the run continued
+    in place (M/cpu/exchange/spinoperationexchange.cpp:52-112,
+    spinoperationanisotropy.cpp:191-236, ..._cubic.cpp:239-290,
+    spinoperationappliedfield.cpp:33-58, spinoperationdipole.cpp:35-59,
+    llg.cpp:50-88)."""
+    dims = (16, 8, 2)
+    n = int(np.prod(dims))
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*random_spins(n, 91))
+    ss.setAlpha(0.1)
+    ss.setTimeStep(0.01)
+    ex = M.Exchange(ss)
+    ex.setPeriodicXYZ(True, True, False)
+    ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 0)))
+    ani = M.Anisotropy(ss)
+    r = np.random.default_rng(4)
+    ani.addMany(np.arange(n), r.normal(size=(n, 3)), r.uniform(0.0, 0.2, n))
+    cub = M.AnisotropyCubic(ss)
+    cub.addMany(np.arange(n), np.tile([1.0, 0, 0], (n, 1)), np.tile([0, 1.0, 0], (n, 1)),
+                np.tile([0.05, 0.01, 0.0], (n, 1)))
+    z = M.AppliedField(ss)
+    z.set(0.02, 0.0, -0.05)
+    dip = M.Dipole(ss)
+    dip.setStrength(0.04)
+    llg = M.LLG.new("Quaternion")
+    ops = [ex, ani, cub, z, dip]
+    M.run(ss, ops, llg, 5)
+    stream = bytearray()
+    idx = 0
+    objs = [ss] + ops + [llg]
+    for o in objs:
+        b = o.encode(idx)
+        idx += o._stream_objects
+        stream += b
+    pos = 0
+    back = []
+    s2, used, k = M.SpinSystem.decode(bytes(stream), partial=True)
+    pos += used
+    for _ in range(len(ops) + 1):
+        o, used, k = M.decode(bytes(stream[pos:]), partial=True)
+        back.append(o)
+        pos += used
+    assert pos == len(stream)
+    assert [type(o).__name__ for o in back] == ["Exchange", "Anisotropy", "AnisotropyCubic", "AppliedField",
+                                                "Dipole", "LLGQuaternion"]
+    assert back[0].periodicXYZ() == (True, True, False)
+    M.run(ss, ops, llg, 20)
+    M.run(s2, back[:-1], back[-1], 20)
+    np.testing.assert_array_equal(np.stack(ss.spinArrays()[:3]), np.stack(s2.spinArrays()[:3]))
+    assert ss.time() == s2.time()

@@ -71,3 +71,53 @@ def test_step_without_operators(M):
     M.run(ss, [], M.LLG.new("Quaternion"), 3)
     np.testing.assert_allclose(np.stack(ss.spinArrays()[:3]), s, atol=1e-7)
     assert ss.time() == pytest.approx(0.03)
+
+
+@pytest.mark.parametrize("path", ["fused", "generic_f64", "eager_llg"])
+def test_nonfinite_spin_sets_the_status_word(M, path):
+    """A non-finite spin written by an LLG step sets bit 0 of the system's
+    status word (mlb_system_status), on the fused fast kernels, the generic
+    kernels and the stand-alone LLG; clearing resets it; a finite run leaves
+    it clear.  The bad input is made on the host (one site set to NaN)."""
+    dims = (16, 8, 2)
+    n = int(np.prod(dims))
+    prec = "f64" if path == "generic_f64" else "f32"
+
+    def build(s0):
+        ss = M.SpinSystem(*dims, precision=prec)
+        ss.setSpinArrays(*s0, np.ones(n))     # uniform moments: the fast kernels take the fused step
+        ss.setAlpha(0.1)
+        ss.setTimeStep(0.01)
+        if path == "generic_f64":
+            ss.setSiteAlphaArray(np.full(n, 0.1))      # per-site alpha: the generic kernels
+        ex = M.Exchange(ss)
+        ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 0)))
+        dip = M.Dipole(ss)
+        dip.setStrength(0.05)
+        return ss, [ex, dip]
+
+    def step(ss, ops, k):
+        llg = M.LLG.new("Quaternion")
+        if path == "eager_llg":
+            for _ in range(k):
+                ss.resetFields()
+                for op in ops:
+                    op.apply(ss)
+                ss.sumFields()
+                other = M.SpinSystem(*dims, precision=prec)
+                ss.copyTo(other)
+                llg.apply(other, 1.0, ss, ss)        # from != dmdt: the stand-alone LLG kernel
+        else:
+            M.run(ss, ops, llg, k)
+
+    s0 = tilted_spins(n, 96, deg=20.0)
+    ss, ops = build(s0)
+    step(ss, ops, 3)
+    assert ss.status() == 0
+    bad = s0.copy()
+    bad[0, 37] = np.nan
+    ss2, ops2 = build(bad)
+    step(ss2, ops2, 2)
+    assert ss2.status() & 1
+    assert ss2.status(clear=True) & 1
+    assert ss2.status() == 0

@@ -98,3 +98,54 @@ def test_wab_parameters_must_match(M, tmp_path):
     d.setTruncation(50)
     with pytest.raises(M.MagLuaError, match="gmax"):
         d.readWAB(f)
+
+
+# ---------------------------------------------------------------- truncation math.huge
+@pytest.mark.parametrize("dims,rings", [((6, 5, 3), 7), ((16, 4, 2), 3)])
+def test_huge_truncation_ring_sum_matches_oracle(M, dims, rings):
+    """Truncation math.huge (dipoleLoad, dipolesupport.cpp:771-835): the image
+    sum in rings of 5 lattices, here over a few rings (the ring count is a
+    parameter of the check; the reference's is 1000)."""
+    dip = M.Dipole(*dims)
+    dip.setTruncation(float("inf"))
+    assert dip.truncation() == (float("inf"),) * 4
+    dip.setHugeRings(rings)
+    got = dip.tensorArrays()
+    ref = O.dipole_tensor_rings(*dims, nrings=rings)
+    scale = max(np.abs(r).max() for r in ref)
+    for g, r in zip(got, ref):
+        assert np.abs(g - r).max() <= 1e-12 * scale
+
+
+def test_huge_truncation_full_ring_count_and_field(M, tmp_path):
+    """The reference's full count, 1000 rings (|X|, |Y| <= 4999), on a 2x2x1
+    lattice against the oracle; the field it gives; a WAB file written with
+    gmax = {math.huge, ...} read back by another operator of truncation
+    math.huge."""
+    dims = (2, 2, 1)
+    dip = M.Dipole(*dims)
+    dip.setTruncation(float("inf"))
+    got = dip.tensorArrays()
+    ref = O.dipole_tensor_rings(*dims, nrings=1000)
+    scale = max(np.abs(r).max() for r in ref)
+    for g, r in zip(got, ref):
+        assert np.abs(g - r).max() <= 1e-11 * scale
+    n = 4
+    s = random_spins(n, 81)
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    dip.setStrength(0.3)
+    dip.apply(ss)
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    O.LongRange(*dims, ref).apply(o, 0.3)
+    assert rel_err(np.stack(ss.fieldArrays("Dipole")), o.field("Dipole")) <= 1e-5
+    f = tmp_path / "WAB_2x2.1.lua"
+    dip.writeWAB(f)
+    assert "gmax = {math.huge, math.huge, math.huge, math.huge}" in f.read_text()
+    other = M.Dipole(*dims)
+    other.setTruncation(float("inf"))
+    other.setHugeRings(1)          # a read file replaces the sum
+    other.readWAB(f)
+    for g, r in zip(other.tensorArrays(), ref):
+        assert np.abs(g - r).max() <= 1e-11 * scale

@@ -210,3 +210,22 @@ def test_fused_surrogate_step_equals_individual_calls(M):
     np.testing.assert_array_equal(res[0][1], res[1][1])
     assert res[0][2]["exact"] == res[1][2]["exact"] == 3, res
     assert res[1][2]["surrogate"] == 5, res
+
+
+def test_completion_wait_limit_reports_and_recovers(M):
+    """A tensor-core completion wait that gives up sets the surrogate's error
+    flag and the host call returns MLB_ECUDA; the kernel still waits (bounded)
+    for its own MMAs before reading and freeing TMEM, so the context stays
+    usable: with the default limit the next forward equals a clean one."""
+    S, _ = _sur(M)
+    W, R = _random_params(12)
+    S.setParams(W, R)
+    x = random_spins(N, 13)
+    clean = S.forward(x)
+    S.setWaitLimit(0)            # every completion wait gives up at once
+    with pytest.raises(M.MagLuaError) as ei:
+        S.forward(x)
+    assert ei.value.code == -3 and "gave up" in str(ei.value)
+    S.setWaitLimit(1 << 24)
+    again = S.forward(x)
+    np.testing.assert_array_equal(again, clean)
