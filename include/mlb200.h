@@ -168,6 +168,7 @@ int mlb_system_decode(const void* buf, size_t len, int real_bytes, mlb_system** 
 #define MLB_OP_LONGRANGE2D 10   /* M/cpu/longrange2d (layer-pair tensors) */
 #define MLB_OP_DIPOLE2D 11      /* M/cpu/dipole2d (LongRange2D + tensor builder) */
 #define MLB_OP_MAGNETOSTATICS2D 12 /* M/cpu/magnetostatics2d (LongRange2D + prism tensors) */
+#define MLB_OP_MAGNETOSTATIC 13 /* M/cpu/magnetostatics (LongRange + volume-averaged prism tensors; deprecated there) */
 int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out);     /* X.new(nx,ny,nz) */
 int mlb_op_destroy(mlb_op* op);
 int mlb_op_kind(const mlb_op* op, int* kind);
@@ -240,6 +241,19 @@ int mlb_longrange_get_truncation(const mlb_op* op, int gmax[4]);     /* getTrunc
  * ring counts. */
 int mlb_dipole_set_huge_rings(mlb_op* op, int rings);
 int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9]);
+/* Magnetostatic (M/cpu/magnetostatics/spinoperationmagnetostatics.cpp:
+ * 99-160; slot "Magnetostatic"): a LongRange whose tensor is the
+ * demagnetising interaction of rectangular prisms of the cell dimensions
+ * (gamma_ab_v.cpp), switching per component to the point dipole (times the
+ * prism volume / 4 pi) from the first image, nearest first, where the two
+ * agree within the crossover tolerance (magnetostaticssupport.cpp:81-187;
+ * default 1e-5); built on host threads at first use.  A truncation of
+ * math.huge gives MLB_EUNSUP: the reference's ring sum for it keeps only the
+ * last of each ring's eight ranges. */
+int mlb_magnetostatic_set_cell_dimensions(mlb_op* op, const double d[3]);     /* setCellDimensions */
+int mlb_magnetostatic_get_cell_dimensions(const mlb_op* op, double d[3]);     /* cellDimensions */
+int mlb_magnetostatic_set_crossover_tolerance(mlb_op* op, double tol);        /* setCrossoverTolerance */
+int mlb_magnetostatic_get_crossover_tolerance(const mlb_op* op, double* tol);
 /* B200 extension: open (zero-padded) boundaries per axis for Dipole; the
  * reference Dipole is periodic in x and y and open in z. */
 int mlb_longrange_set_open(mlb_op* op, int open_x, int open_y, int open_z);

@@ -107,6 +107,10 @@ _SIGS = {
     "mlb_longrange_set_strength": ([_P, C.c_double], C.c_int),
     "mlb_longrange_get_strength": ([_P, _D], C.c_int),
     "mlb_longrange_get_truncation": ([_P, _I], C.c_int),
+    "mlb_magnetostatic_set_cell_dimensions": ([_P, _D], C.c_int),
+    "mlb_magnetostatic_get_cell_dimensions": ([_P, _D], C.c_int),
+    "mlb_magnetostatic_set_crossover_tolerance": ([_P, C.c_double], C.c_int),
+    "mlb_magnetostatic_get_crossover_tolerance": ([_P, _D], C.c_int),
     "mlb_op_encode": ([_P, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), _I], C.c_int),
     "mlb_op_decode": ([C.c_char_p, C.c_size_t, C.POINTER(_P), C.POINTER(C.c_size_t), _I], C.c_int),
     "mlb_llg_encode": ([_P, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), _I], C.c_int),
@@ -1010,6 +1014,30 @@ class Dipole(LongRange):
     def setOpen(self, ox=True, oy=True, oz=True):
         """Open (zero-padded) boundaries in x and y instead of periodic images."""
         _ck(_lib.mlb_longrange_set_open(self._h, int(bool(ox)), int(bool(oy)), int(bool(oz))))
+
+
+class Magnetostatic(LongRange):
+    """Magnetostatic (M/cpu/magnetostatics): LongRange with the volume-averaged
+    interaction of rectangular prisms (deprecated in the reference in favour
+    of Magnetostatics2D; kept for its scripts)."""
+    KIND = 13
+
+    def setCellDimensions(self, dx, dy=None, dz=None):
+        d = list(dx) if hasattr(dx, "__len__") else [dx, dy, dz]
+        _ck(_lib.mlb_magnetostatic_set_cell_dimensions(self._h, _dp(_f64(d, 3))))
+
+    def cellDimensions(self):
+        d = np.zeros(3)
+        _ck(_lib.mlb_magnetostatic_get_cell_dimensions(self._h, _dp(d)))
+        return tuple(d)
+
+    def setCrossoverTolerance(self, tol):
+        _ck(_lib.mlb_magnetostatic_set_crossover_tolerance(self._h, float(tol)))
+
+    def crossoverTolerance(self):
+        v = C.c_double()
+        _ck(_lib.mlb_magnetostatic_get_crossover_tolerance(self._h, C.byref(v)))
+        return v.value
 
 
 class LongRange3D(SpinOperation):

@@ -309,6 +309,8 @@ struct mlb_op {
     double g = 1.0;
     int gmax[4] = {1000, 1000, 1000, 1000};   // gmax[0] = -1: math.huge
     int rings = 1000;                          // rings of 5 lattices of the math.huge sum
+    double mag_prism[3] = {1, 1, 1};           // Magnetostatic: prism (cell) dimensions
+    double mag_tol = 0.00001;                  // Magnetostatic: crossover tolerance
     double ABC[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     int open[3] = {0, 0, 1};
     std::vector<double> t6[6];
@@ -632,7 +634,11 @@ void compile_thermal_scale(mlb_op* op)
 }
 
 // ------------------------------------------------------------------ convolution plans
-bool is_conv(int kind) { return kind == MLB_OP_DIPOLE || kind == MLB_OP_LONGRANGE || kind == MLB_OP_LONGRANGE3D; }
+bool is_conv(int kind)
+{
+    return kind == MLB_OP_DIPOLE || kind == MLB_OP_LONGRANGE || kind == MLB_OP_LONGRANGE3D ||
+           kind == MLB_OP_MAGNETOSTATIC;
+}
 
 void plan_sizes(mlb_op* op, ConvPlan& P)
 {
@@ -708,6 +714,191 @@ bool tensor_has_parities(const double2* W, const ConvK& k, cudaStream_t st)
     return d[0] > 0 && d[1] <= 1e-10 * d[0] && d[2] <= 1e-10 * d[0];
 }
 
+// ------------------------------------------------------------------ Magnetostatic tensor
+// The deprecated Magnetostatic operator (M/cpu/magnetostatics): LongRange
+// with the volume-averaged interaction of rectangular prisms.  Element
+// functions of M/cpu/magnetostatics/gamma_ab_v.cpp (after J. Geophys. Res.
+// 98 B6 9551, 1993): the demagnetising tensor N_ab of a prism (dx, dy, dz)
+// seen from another at offset (X, Y, Z), as second differences of f and g
+// with the reference's guards (a zero denominator in invtan, phi = asinh with
+// 1000 sign(n) for d = 0).  Host FP64, as the reference computes it.
+namespace mg {
+double invtan(double num, double den)
+{
+    if (den == 0) return num > 0 ? M_PI * 0.5 : -M_PI * 0.5;
+    return std::atan(num / den);
+}
+double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+double phi(double n, double d)
+{
+    if (n == 0) return 0;
+    if (d == 0) return 1000 * sgn(n);
+    const double p = n / d;
+    return std::log(p + std::sqrt(1.0 + p * p));
+}
+double gfun(double x, double y, double z)
+{
+    const double xx = x * x, yy = y * y, zz = z * z;
+    const double R = std::sqrt(xx + yy + zz);
+    return (x * y * z) * phi(z, std::sqrt(xx + yy)) + (y / 6.0) * (3.0 * zz - yy) * phi(x, std::sqrt(yy + zz)) +
+           (x / 6.0) * (3.0 * zz - xx) * phi(y, std::sqrt(xx + zz)) - (z * zz / 6.0) * invtan(x * y, (z * R)) -
+           (z * yy / 2.0) * invtan(x * z, (y * R)) - (z * xx / 2.0) * invtan(y * z, (x * R)) - (x * y * R / 3.0);
+}
+double G2(double x, double y, double z) { return gfun(x, y, z) - gfun(x, y, 0); }
+double G1(double X, double Y, double Z, double dx, double dz)
+{
+    return G2(X + dx, Y, Z + dz) - G2(X + dx, Y, Z) - G2(X, Y, Z + dz) + G2(X, Y, Z);
+}
+double G0(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    return G1(X, Y, Z, dx, dz) - G1(X, Y - dy, Z, dx, dz) - G1(X, Y, Z - dz, dx, dz) + G1(X, Y - dy, Z - dz, dx, dz);
+}
+double ffun(double x, double y, double z)
+{
+    const double xx = x * x, yy = y * y, zz = z * z;
+    const double R = std::sqrt(xx + yy + zz);
+    return y * 0.5 * (zz - xx) * phi(y, std::sqrt(xx + zz)) + z * 0.5 * (yy - xx) * phi(z, std::sqrt(xx + yy)) -
+           x * y * z * invtan(y * z, x * R) + (1.0 / 6.0) * (2.0 * xx - yy - zz) * R;
+}
+double F2(double X, double Y, double Z) { return ffun(X, Y, Z) - ffun(X, 0, Z) - ffun(X, Y, 0) + ffun(X, 0, 0); }
+double F1(double X, double Y, double Z, double dy, double dz)
+{
+    return F2(X, Y, Z) - F2(X, Y - dy, Z) - F2(X, Y, Z - dz) + F2(X, Y - dy, Z - dz);
+}
+double F0(double X, double Y, double Z, double dy, double dz)
+{
+    return F1(X, Y + dy, Z + dz, dy, dz) - F1(X, Y, Z + dz, dy, dz) - F1(X, Y + dy, Z, dy, dz) + F1(X, Y, Z, dy, dz);
+}
+double Nxx(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    const double tau = dx * dy * dz;
+    return -1.0 * (1.0 / (4.0 * M_PI * tau)) * (2.0 * F0(X, Y, Z, dy, dz) - F0(X + dx, Y, Z, dy, dz) - F0(X - dx, Y, Z, dy, dz));
+}
+double Nxy(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    const double tau = dx * dy * dz;
+    return -1.0 * (1.0 / (4.0 * M_PI * tau)) *
+           (G0(X, Y, Z, dx, dy, dz) - G0(X - dx, Y, Z, dx, dy, dz) - G0(X, Y + dy, Z, dx, dy, dz) +
+            G0(X - dx, Y + dy, Z, dx, dy, dz));
+}
+// XX, XY, XZ, YY, YZ, ZZ (gamma_ab_v.cpp:135-188)
+double gamma_v(int c, double x, double y, double z, const double* p)
+{
+    switch (c) {
+    case 0: return Nxx(x, y, z, p[0], p[1], p[2]);
+    case 1: return Nxy(x, y, z, p[0], p[1], p[2]);
+    case 2: return Nxy(x, z, y, p[0], p[2], p[1]);
+    case 3: return Nxx(y, x, z, p[1], p[0], p[2]);
+    case 4: return Nxy(y, z, x, p[1], p[2], p[0]);
+    default: return Nxx(z, y, x, p[2], p[1], p[0]);
+    }
+}
+// the point-dipole elements (dipolesupport.cpp:32-70)
+double gamma_dip(int c, double rx, double ry, double rz)
+{
+    const double r = std::sqrt(rx * rx + ry * ry + rz * rz);
+    if (r < 1E-40) return 0;
+    const double ir = 1.0 / r, ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
+    switch (c) {
+    case 0: return -1.0 * (ir3 - 3.0 * rx * rx * ir5);
+    case 1: return -1.0 * (-3.0 * rx * ry * ir5);
+    case 2: return -1.0 * (-3.0 * rx * rz * ir5);
+    case 3: return -1.0 * (ir3 - 3.0 * ry * ry * ir5);
+    case 4: return -1.0 * (-3.0 * ry * rz * ir5);
+    default: return -1.0 * (ir3 - 3.0 * rz * rz * ir5);
+    }
+}
+bool equal_tol(double a, double b, double tol)
+{
+    if (a == 0 && b == 0) return true;
+    if (b == 0 || a == 0) return false;
+    const double t1 = std::fabs((a - b) / a), t2 = std::fabs((a - b) / b);
+    return t1 < tol && t2 < tol;
+}
+struct Pt {
+    double x, y, z, r2;
+};
+} // namespace mg
+
+// magnetostaticsLoad for a finite truncation (magnetostaticssupport.cpp:
+// 799-866, getGAB with smin = 0 :191-318, getGAB_range :81-187): per element
+// (k from -nz+1, then j, i) the images inside the truncation (the tests of
+// the Dipole sum, truemax[4] taken large) in X-outer Y-inner order, sorted by
+// r^2 with std::sort as the reference sorts them; per component, from the
+// nearest out, the prism tensor until the first image where it and the point
+// dipole (1/(4 pi) x prism volume x gamma_dip) agree within the crossover
+// tolerance, the point dipole from there on; the crossover restarts at every
+// element.  Elements are independent: host threads take them in chunks.
+void build_magnetostatic_t6(mlb_op* op)
+{
+    if (op->gmax[0] < 0)
+        fail(MLB_EUNSUP, "Magnetostatic truncation math.huge: the reference's ring sum (getGAB with smin > 0) "
+                         "keeps only the last of each ring's eight ranges, so it is not a lattice sum");
+    const int nx = op->nx, ny = op->ny, nz = op->nz;
+    const size_t ne = (size_t)nx * ny * (2 * nz - 1);
+    ensure_t6_layout(op);
+    const int* gm = op->gmax;
+    const double* A = op->ABC;
+    const double* prism = op->mag_prism;
+    const double tol = op->mag_tol;
+    const double volume = prism[0] * prism[1] * prism[2];
+    const int G = gm[0];
+    std::atomic<size_t> next(0);
+    const size_t chunk = 16;
+    auto work = [&]() {
+        std::vector<mg::Pt> pts;
+        for (;;) {
+            const size_t e0 = next.fetch_add(chunk);
+            if (e0 >= ne) break;
+            for (size_t e = e0; e < std::min(ne, e0 + chunk); e++) {
+                const int i = (int)(e % nx), j = (int)((e / nx) % ny);
+                const int k = (int)(e / ((size_t)nx * ny)) - (nz - 1);
+                pts.clear();
+                if (std::abs(k) <= gm[0]) {
+                    for (int X = -(G - 1); X <= G - 1; X++) {
+                        const int xx = X * nx + i;
+                        if (!(std::abs(xx) <= gm[2] && std::abs(xx) <= gm[0])) continue;
+                        for (int Y = -(G - 1); Y <= G - 1; Y++) {
+                            const int yy = Y * ny + j;
+                            if (!(std::abs(yy) <= gm[3] && std::abs(yy) <= gm[0])) continue;
+                            if (((double)xx * xx + (double)yy * yy + (double)k * k) <= ((double)gm[0] * (double)gm[0])) {
+                                mg::Pt q;
+                                q.x = ((double)xx) * A[0] + ((double)yy) * A[3] + ((double)k) * A[6];
+                                q.y = ((double)xx) * A[1] + ((double)yy) * A[4] + ((double)k) * A[7];
+                                q.z = ((double)xx) * A[2] + ((double)yy) * A[5] + ((double)k) * A[8];
+                                q.r2 = q.x * q.x + q.y * q.y + q.z * q.z;
+                                pts.push_back(q);
+                            }
+                        }
+                    }
+                }
+                std::sort(pts.begin(), pts.end(), [](const mg::Pt& a, const mg::Pt& b) { return a.r2 < b.r2; });
+                for (int c = 0; c < 6; c++) {
+                    double cross_r2 = 1e10, g = 0;
+                    for (const mg::Pt& q : pts) {
+                        double dip = 0, mag;
+                        if (tol > 0) dip = (1.0 / (M_PI * 4.0)) * volume * mg::gamma_dip(c, q.x, q.y, q.z);
+                        if (q.r2 >= cross_r2) {
+                            mag = dip;
+                        } else {
+                            mag = mg::gamma_v(c, q.x, q.y, q.z, prism);
+                            if (tol > 0 && mg::equal_tol(mag, dip, tol) && q.r2 > 0 && q.r2 < cross_r2) cross_r2 = q.r2;
+                        }
+                        g += mag;
+                    }
+                    op->t6[c][e] = g;
+                }
+            }
+        }
+    };
+    const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; t++) th.emplace_back(work);
+    work();
+    for (std::thread& t : th) t.join();
+    op->t6_valid = true;
+}
+
 // Build or rebuild the tensor spectrum of op (FP64 on the GPU), stored at
 // rb bytes per real for the systems it is applied to.
 void build_plan(mlb_op* op, cudaStream_t st, int rb)
@@ -745,6 +936,7 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
     W.alloc(plane * ncomp);
     CK(cudaMemsetAsync(W.p, 0, sizeof(double2) * plane * ncomp, st));
     const size_t ne = (size_t)op->nx * op->ny * (2 * op->nz - 1);
+    if (op->kind == MLB_OP_MAGNETOSTATIC && !op->t6_valid) build_magnetostatic_t6(op);
     if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
         if (op->open[0] || op->open[1]) {
             if (!(op->open[0] && op->open[1])) fail(MLB_EUNSUP, "mixed periodic/open in-plane Dipole");
@@ -1463,7 +1655,8 @@ void op_apply(mlb_op* op, mlb_system* s)
     }
     case MLB_OP_DIPOLE:
     case MLB_OP_LONGRANGE:
-    case MLB_OP_LONGRANGE3D: {
+    case MLB_OP_LONGRANGE3D:
+    case MLB_OP_MAGNETOSTATIC: {
         if (s->capturing && (op->plan_dirty || !op->plan || op->plan->rb != s->rb))
             fail(MLB_ESTATE, "tensor changed during capture");
         build_plan(op, s->st, s->rb);
@@ -3627,6 +3820,7 @@ int mlb_op_create(int kind, int nx, int ny, int nz, mlb_op** out)
         case MLB_OP_APPLIEDFIELD: op->slot = "Zeeman"; break;
         case MLB_OP_DIPOLE: op->slot = "Dipole"; break;
         case MLB_OP_LONGRANGE: op->slot = "LongRange"; break;
+        case MLB_OP_MAGNETOSTATIC: op->slot = "Magnetostatic"; break;
         case MLB_OP_LONGRANGE3D: op->slot = "LongRange3D"; break;
         case MLB_OP_LONGRANGE2D: op->slot = "LongRange2D"; break;
         case MLB_OP_DIPOLE2D: op->slot = "Dipole2D"; break;
@@ -3982,6 +4176,46 @@ int mlb_longrange_set_unit_cell(mlb_op* op, const double ABC[9])
     });
 }
 
+int mlb_magnetostatic_set_cell_dimensions(mlb_op* op, const double d[3])
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_MAGNETOSTATIC) fail(MLB_EINVAL, "not a Magnetostatic operator");
+        g_version++;
+        for (int a = 0; a < 3; a++) op->mag_prism[a] = d[a];
+        op->t6_valid = false;
+        op->t6_edited = false;
+        op->plan_dirty = true;
+    });
+}
+
+int mlb_magnetostatic_get_cell_dimensions(const mlb_op* op, double d[3])
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_MAGNETOSTATIC) fail(MLB_EINVAL, "not a Magnetostatic operator");
+        for (int a = 0; a < 3; a++) d[a] = op->mag_prism[a];
+    });
+}
+
+int mlb_magnetostatic_set_crossover_tolerance(mlb_op* op, double tol)
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_MAGNETOSTATIC) fail(MLB_EINVAL, "not a Magnetostatic operator");
+        g_version++;
+        op->mag_tol = tol;
+        op->t6_valid = false;
+        op->t6_edited = false;
+        op->plan_dirty = true;
+    });
+}
+
+int mlb_magnetostatic_get_crossover_tolerance(const mlb_op* op, double* tol)
+{
+    return guard([&] {
+        if (!op || op->kind != MLB_OP_MAGNETOSTATIC) fail(MLB_EINVAL, "not a Magnetostatic operator");
+        *tol = op->mag_tol;
+    });
+}
+
 int mlb_longrange_set_open(mlb_op* op, int ox, int oy, int oz)
 {
     return guard([&] {
@@ -4010,9 +4244,11 @@ int mlb_longrange_set_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double 
 {
     return guard([&] {
         g_version++;
-        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE) fail(MLB_EINVAL, "not a LongRange operator");
+        if (op->kind != MLB_OP_DIPOLE && op->kind != MLB_OP_LONGRANGE && op->kind != MLB_OP_MAGNETOSTATIC)
+            fail(MLB_EINVAL, "not a LongRange operator");
         if (ab < 0 || ab > 5) fail(MLB_EINVAL, "1st argument must be matrix name: XX, XY, XZ, YY, YZ or ZZ");
         if (op->kind == MLB_OP_DIPOLE && (op->open[0] || op->open[1])) fail(MLB_EUNSUP, "open-boundary tensor");
+        if (op->kind == MLB_OP_MAGNETOSTATIC && !op->t6_valid) build_magnetostatic_t6(op);
         if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
             cudaStream_t st;
             CK(cudaStreamCreate(&st));
@@ -4035,6 +4271,7 @@ int mlb_longrange_get_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double*
 {
     return guard([&] {
         if (ab < 0 || ab > 5) fail(MLB_EINVAL, "1st argument must be matrix name: XX, XY, XZ, YY, YZ or ZZ");
+        if (op->kind == MLB_OP_MAGNETOSTATIC && !op->t6_valid) build_magnetostatic_t6(op);
         if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
             cudaStream_t st;
             CK(cudaStreamCreate(&st));
@@ -4051,6 +4288,7 @@ int mlb_longrange_get_matrix(mlb_op* op, int ab, int ox, int oy, int oz, double*
 int mlb_longrange_get_tensor(mlb_op* op, double* const t6[6])
 {
     return guard([&] {
+        if (op->kind == MLB_OP_MAGNETOSTATIC && !op->t6_valid) build_magnetostatic_t6(op);
         if (op->kind == MLB_OP_DIPOLE && !op->t6_valid) {
             if (op->open[0] || op->open[1]) fail(MLB_EUNSUP, "open-boundary tensor has no reference layout");
             cudaStream_t st;

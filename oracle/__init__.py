@@ -109,6 +109,7 @@ lib.orc_thermal_apply_noise.argtypes = [_PSS, C.c_double, _D, C.c_double, _D, _D
 lib.orc_thermal_draw.argtypes = [_PSS, C.c_double, C.POINTER(_MT), _D, _D, _D]
 lib.orc_zeeman_apply.argtypes = [_PSS, _D, C.c_double]
 lib.orc_dipole_tensor.argtypes = [C.c_int, C.c_int, C.c_int, _I, _D, _D, _D, _D, _D, _D, _D]
+lib.orc_magnetostatic_tensor.argtypes = [C.c_int, C.c_int, C.c_int, _I, _D, _D, C.c_double, _D, _D, _D, _D, _D, _D]
 lib.orc_dipole_tensor_rings.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D]
 lib.orc_longrange_apply.argtypes = [_PSS, C.c_char_p, _D * 6, C.c_double, C.c_double]
 lib.orc_lr_new.restype = C.c_void_p
@@ -332,6 +333,18 @@ def dipole_tensor(nx, ny, nz, gmax=(1000, 1000, 1000, 1000), ABC=(1, 0, 0, 0, 1,
     n = nx * ny * (2 * nz - 1)
     arrs = [np.zeros(n) for _ in range(6)]
     lib.orc_dipole_tensor(nx, ny, nz, _ip(g), _dp(abc), *[_dp(a) for a in arrs])
+    return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
+
+
+def magnetostatic_tensor(nx, ny, nz, gmax=(1000, 1000, 1000, 1000), ABC=(1, 0, 0, 0, 1, 0, 0, 0, 1),
+                         prism=(1.0, 1.0, 1.0), tol=1e-5):
+    """The Magnetostatic tensor (orc_magnetostatic_tensor): six arrays of
+    shape (2nz-1, ny, nx), XX, XY, XZ, YY, YZ, ZZ."""
+    g = _i32(gmax)
+    abc, pr = _f64(ABC), _f64(prism)
+    n = nx * ny * (2 * nz - 1)
+    arrs = [np.zeros(n) for _ in range(6)]
+    lib.orc_magnetostatic_tensor(nx, ny, nz, _ip(g), _dp(abc), _dp(pr), float(tol), *[_dp(a) for a in arrs])
     return [a.reshape(2 * nz - 1, ny, nx) for a in arrs]
 
 

@@ -736,6 +736,170 @@ void orc_dipole_tensor_rings(int nx, int ny, int nz, const double ABC[9], int nr
             }
 }
 
+/* ------------------------------------------------------------------ */
+/* Magnetostatic (deprecated LongRange subclass): prism tensors          */
+/* ------------------------------------------------------------------ */
+/* Restated from M/cpu/magnetostatics/gamma_ab_v.cpp (after J. Geophys. Res.
+ * 98 B6 9551, 1993): the demagnetising tensor N_ab of a rectangular prism
+ * (dx, dy, dz) seen from another at offset (X, Y, Z), with the reference's
+ * guards (invtan with a zero denominator, phi = asinh(n/d) with 1000 sign(n)
+ * for d = 0). */
+static double mg_invtan(double num, double den)
+{
+    if (den == 0) return num > 0 ? M_PI * 0.5 : -M_PI * 0.5;
+    return atan(num / den);
+}
+static double mg_sign(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+static double mg_phi(double n, double d)
+{
+    if (n == 0) return 0;
+    if (d == 0) return 1000 * mg_sign(n);
+    const double p = n / d;
+    return log(p + sqrt(1.0 + p * p));
+}
+static double mg_g(double x, double y, double z)
+{
+    const double xx = x * x, yy = y * y, zz = z * z;
+    const double R = sqrt(xx + yy + zz);
+    return (x * y * z) * mg_phi(z, sqrt(xx + yy)) + (y / 6.0) * (3.0 * zz - yy) * mg_phi(x, sqrt(yy + zz)) +
+           (x / 6.0) * (3.0 * zz - xx) * mg_phi(y, sqrt(xx + zz)) - (z * zz / 6.0) * mg_invtan(x * y, (z * R)) -
+           (z * yy / 2.0) * mg_invtan(x * z, (y * R)) - (z * xx / 2.0) * mg_invtan(y * z, (x * R)) - (x * y * R / 3.0);
+}
+static double mg_G2(double x, double y, double z) { return mg_g(x, y, z) - mg_g(x, y, 0); }
+static double mg_G1(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    (void)dy;
+    return mg_G2(X + dx, Y, Z + dz) - mg_G2(X + dx, Y, Z) - mg_G2(X, Y, Z + dz) + mg_G2(X, Y, Z);
+}
+static double mg_G0(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    return mg_G1(X, Y, Z, dx, dy, dz) - mg_G1(X, Y - dy, Z, dx, dy, dz) - mg_G1(X, Y, Z - dz, dx, dy, dz) +
+           mg_G1(X, Y - dy, Z - dz, dx, dy, dz);
+}
+static double mg_f(double x, double y, double z)
+{
+    const double xx = x * x, yy = y * y, zz = z * z;
+    const double R = sqrt(xx + yy + zz);
+    return y * 0.5 * (zz - xx) * mg_phi(y, sqrt(xx + zz)) + z * 0.5 * (yy - xx) * mg_phi(z, sqrt(xx + yy)) -
+           x * y * z * mg_invtan(y * z, x * R) + (1.0 / 6.0) * (2.0 * xx - yy - zz) * R;
+}
+static double mg_F2(double X, double Y, double Z) { return mg_f(X, Y, Z) - mg_f(X, 0, Z) - mg_f(X, Y, 0) + mg_f(X, 0, 0); }
+static double mg_F1(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    (void)dx;
+    return mg_F2(X, Y, Z) - mg_F2(X, Y - dy, Z) - mg_F2(X, Y, Z - dz) + mg_F2(X, Y - dy, Z - dz);
+}
+static double mg_F0(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    return mg_F1(X, Y + dy, Z + dz, dx, dy, dz) - mg_F1(X, Y, Z + dz, dx, dy, dz) - mg_F1(X, Y + dy, Z, dx, dy, dz) +
+           mg_F1(X, Y, Z, dx, dy, dz);
+}
+static double mg_Nxx(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    const double tau = dx * dy * dz;
+    return -1.0 * (1.0 / (4.0 * M_PI * tau)) *
+           (2.0 * mg_F0(X, Y, Z, dx, dy, dz) - mg_F0(X + dx, Y, Z, dx, dy, dz) - mg_F0(X - dx, Y, Z, dx, dy, dz));
+}
+static double mg_Nxy(double X, double Y, double Z, double dx, double dy, double dz)
+{
+    const double tau = dx * dy * dz;
+    return -1.0 * (1.0 / (4.0 * M_PI * tau)) *
+           (mg_G0(X, Y, Z, dx, dy, dz) - mg_G0(X - dx, Y, Z, dx, dy, dz) - mg_G0(X, Y + dy, Z, dx, dy, dz) +
+            mg_G0(X - dx, Y + dy, Z, dx, dy, dz));
+}
+/* the six components XX, XY, XZ, YY, YZ, ZZ (gamma_ab_v.cpp:135-188) */
+static double mg_gamma_v(int c, double x, double y, double z, const double* p)
+{
+    switch (c) {
+    case 0: return mg_Nxx(x, y, z, p[0], p[1], p[2]);
+    case 1: return mg_Nxy(x, y, z, p[0], p[1], p[2]);
+    case 2: return mg_Nxy(x, z, y, p[0], p[2], p[1]);
+    case 3: return mg_Nxx(y, x, z, p[1], p[0], p[2]);
+    case 4: return mg_Nxy(y, z, x, p[1], p[2], p[0]);
+    default: return mg_Nxx(z, y, x, p[2], p[1], p[0]);
+    }
+}
+static int mg_equal_tol(double a, double b, double tol)
+{
+    if (a == 0 && b == 0) return 1;
+    if (b == 0 || a == 0) return 0;
+    const double t1 = fabs((a - b) / a), t2 = fabs((a - b) / b);
+    return t1 < tol && t2 < tol;
+}
+typedef struct { double x, y, z, r2; } mg_pt;
+static int mg_cmp(const void* a, const void* b)
+{
+    const double u = ((const mg_pt*)a)->r2, v = ((const mg_pt*)b)->r2;
+    return u < v ? -1 : (u > v ? 1 : 0);
+}
+
+/* magnetostaticsLoad for a finite truncation (magnetostaticssupport.cpp:
+ * 799-866 with getGAB, :191-318, smin = 0, and getGAB_range, :81-187): per
+ * element the images inside the truncation (the tests of the Dipole sum,
+ * truemax[4] taken large) collected in X-outer Y-inner order, sorted by r^2,
+ * then per component summed from the nearest out: the prism tensor until the
+ * first image where it and the point dipole (DipMagConversion 1/(4 pi) times
+ * the prism volume times gamma_dip) agree within tol (relative, both ways),
+ * the point dipole from there on.  The crossover restarts for every
+ * element. */
+void orc_magnetostatic_tensor(int nx, int ny, int nz, const int gmax[4], const double ABC[9], const double prism[3],
+                              double tol, double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ)
+{
+    double* out[6] = {XX, XY, XZ, YY, YZ, ZZ};
+    const double volume = prism[0] * prism[1] * prism[2];
+    const int G = gmax[0];
+    const long long cap = (long long)(2 * G - 1) * (2 * G - 1);
+    mg_pt* pts = (mg_pt*)malloc(sizeof(mg_pt) * (size_t)(cap > 0 ? cap : 1));
+    int c = 0;
+    for (int k = -nz + 1; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                long long np = 0;
+                const int zz = k;
+                if (abs(zz) <= gmax[0]) {
+                    for (int X = -(G - 1); X <= G - 1; X++) {
+                        const int xx = X * nx + i;
+                        if (!(abs(xx) <= gmax[2] && abs(xx) <= gmax[0])) continue;
+                        for (int Y = -(G - 1); Y <= G - 1; Y++) {
+                            const int yy = Y * ny + j;
+                            if (!(abs(yy) <= gmax[3] && abs(yy) <= gmax[0])) continue;
+                            if (((double)xx * xx + (double)yy * yy + (double)zz * zz) <= ((double)gmax[0] * (double)gmax[0])) {
+                                mg_pt q;
+                                q.x = ((double)xx) * ABC[0] + ((double)yy) * ABC[3] + ((double)zz) * ABC[6];
+                                q.y = ((double)xx) * ABC[1] + ((double)yy) * ABC[4] + ((double)zz) * ABC[7];
+                                q.z = ((double)xx) * ABC[2] + ((double)yy) * ABC[5] + ((double)zz) * ABC[8];
+                                q.r2 = q.x * q.x + q.y * q.y + q.z * q.z;
+                                pts[np++] = q;
+                            }
+                        }
+                    }
+                }
+                qsort(pts, (size_t)np, sizeof(mg_pt), mg_cmp);
+                for (int a = 0; a < 6; a++) {
+                    double cross_r2 = 1e10, g = 0;
+                    for (long long p = 0; p < np; p++) {
+                        double dip = 0, mag;
+                        if (tol > 0) {
+                            double g6[6];
+                            gamma_dip(pts[p].x, pts[p].y, pts[p].z, g6);
+                            dip = (1.0 / (M_PI * 4.0)) * volume * g6[a];
+                        }
+                        if (pts[p].r2 >= cross_r2) {
+                            mag = dip;
+                        } else {
+                            mag = mg_gamma_v(a, pts[p].x, pts[p].y, pts[p].z, prism);
+                            if (tol > 0 && mg_equal_tol(mag, dip, tol) && pts[p].r2 > 0 && pts[p].r2 < cross_r2)
+                                cross_r2 = pts[p].r2;
+                        }
+                        g += mag;
+                    }
+                    out[a][c] = g;
+                }
+                c++;
+            }
+    free(pts);
+}
+
 /* LongRange context: the tensor transforms of updateData, prescaled by
  * 1/(nx*ny), spinoperationlongrange.cpp:275-312, plus workspaces. */
 struct orc_lr {

@@ -91,6 +91,11 @@ void orc_zeeman_apply(orc_ss* ss, const double B[3], double gscale);
  * nrings rings (the reference: 1000 rings of 5). */
 void orc_dipole_tensor_rings(int nx, int ny, int nz, const double ABC[9], int nrings, int lstep,
                              double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ);
+/* The Magnetostatic tensor of a finite truncation: prism-prism
+ * demagnetising elements (gamma_ab_v.cpp) with the crossover to the point
+ * dipole of getGAB_range. */
+void orc_magnetostatic_tensor(int nx, int ny, int nz, const int gmax[4], const double ABC[9], const double prism[3],
+                              double tol, double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ);
 void orc_dipole_tensor(int nx, int ny, int nz, const int gmax[4], const double ABC[9],
                        double* XX, double* XY, double* XZ, double* YY, double* YZ, double* ZZ);
 /* LongRange::apply, spinoperationlongrange.cpp:275-312,354-440.

@@ -632,3 +632,44 @@ def test_ensemble_thermal_replicas_independent(M):
     a, b = np.stack(e.spins(0)), np.stack(e.spins(1))
     assert np.abs(a - b).max() > 1e-3      # different noise per replica
     assert np.allclose(np.sqrt((a ** 2).sum(0)), 1.0, atol=1e-5)
+
+
+@pytest.mark.parametrize("dims,prism", [((16, 8, 2), (1.0, 1.0, 1.0)), ((6, 5, 3), (1.0, 1.0, 0.5))])
+def test_magnetostatic_field(M, dims, prism):
+    """Magnetostatic (M/cpu/magnetostatics): the field of the prism tensor
+    through the LongRange convolution (spinoperationlongrange.cpp:354-440)
+    against the oracle's tensor in the oracle's LongRange, slot
+    "Magnetostatic"; a step through the fused path."""
+    n = int(np.prod(dims))
+    s = random_spins(n, 99, lengths=True)
+    gm = 5
+    ss = M.SpinSystem(*dims)
+    ss.setSpinArrays(*s)
+    mag = M.Magnetostatic(ss)
+    mag.setTruncation(gm)
+    mag.setCellDimensions(*prism)
+    mag.setUnitCell((1, 0, 0), (0, 1, 0), (0, 0, prism[2]))
+    mag.setStrength(0.3)
+    mag.apply(ss)
+    o = O.SpinSystem(*dims)
+    o.set_spins(*s)
+    T6 = O.magnetostatic_tensor(*dims, gmax=(gm,) * 4, ABC=(1, 0, 0, 0, 1, 0, 0, 0, prism[2]), prism=prism)
+    O.LongRange(*dims, T6).apply(o, 0.3, slot="Magnetostatic")
+    assert rel_err(np.stack(ss.fieldArrays("Magnetostatic")), o.field("Magnetostatic")) <= FIELD_TOL
+    # fused steps with the exchange beside it
+    ex = M.Exchange(ss)
+    ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 0)))
+    ss.setAlpha(0.1)
+    ss.setTimeStep(0.01)
+    M.run(ss, [ex, mag], M.LLG.new("Quaternion"), 5)
+    o.alpha, o.dt = 0.1, 0.01
+    f, t, j = O.nn_paths(*dims, pbc=(1, 1, 0))
+    lr = O.LongRange(*dims, T6)
+    ol = O.LLG("Quaternion")
+    for _ in range(5):
+        o.reset_fields()
+        O.exchange_apply(o, f, t, j)
+        lr.apply(o, 0.3, slot="Magnetostatic")
+        o.sum_fields()
+        ol.apply(o)
+    assert float(np.abs(np.stack(ss.spinArrays()[:3]) - o.spins()).max()) < 1e-5

@@ -179,3 +179,37 @@ def test_truncated_and_foreign_streams_are_rejected(L):
     assert L.mlb_op_decode(want[:-3], len(want) - 3, C.byref(h), None, None) == -1
     ss = O.encode_spinsystem(1, 1, 1, 0.1, 0.01, 1.0, 0.0, [1.0], [0.0], [0.0], [1.0])
     assert L.mlb_op_decode(ss, len(ss), C.byref(h), None, None) == -7
+
+
+# ---------------------------------------------------------------- Magnetostatic tensor (host builder)
+@pytest.mark.parametrize("dims,gmax,prism,ABC", [
+    ((4, 4, 2), 6, (1.0, 1.0, 1.0), (1, 0, 0, 0, 1, 0, 0, 0, 1)),
+    ((5, 3, 3), 5, (1.0, 0.5, 2.0), (1, 0, 0, 0, 0.5, 0, 0, 0, 2.0)),
+])
+def test_magnetostatic_tensor_matches_oracle(L, dims, gmax, prism, ABC):
+    """The Magnetostatic tensor (M/cpu/magnetostatics/magnetostaticssupport.cpp:
+    81-187, 799-866 with gamma_ab_v.cpp) built on the host by the library,
+    against the oracle's restatement: equal up to the order of images at equal
+    distance (the reference sorts with std::sort, the oracle with qsort)."""
+    h = C.c_void_p()
+    assert L.mlb_op_create(13, *dims, C.byref(h)) == 0
+    assert L.mlb_longrange_set_truncation(h, (C.c_int * 4)(gmax, gmax, gmax, gmax)) == 0
+    assert L.mlb_longrange_set_unit_cell(h, _dp(ABC)) == 0
+    assert L.mlb_magnetostatic_set_cell_dimensions(h, _dp(prism)) == 0
+    n = dims[0] * dims[1] * (2 * dims[2] - 1)
+    arrs = [np.zeros(n) for _ in range(6)]
+    ptrs = (C.POINTER(C.c_double) * 6)(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs])
+    assert L.mlb_longrange_get_tensor(h, ptrs) == 0, L.mlb_last_error().decode()
+    ref = O.magnetostatic_tensor(*dims, gmax=(gmax,) * 4, ABC=ABC, prism=prism, tol=1e-5)
+    scale = max(np.abs(r).max() for r in ref)
+    for a, r in zip(arrs, ref):
+        assert np.abs(a.reshape(r.shape) - r).max() <= 1e-9 * scale
+    # the crossover is on: the far images use the point dipole, which differs
+    # from the prism tensor within the tolerance only
+    ref0 = O.magnetostatic_tensor(*dims, gmax=(gmax,) * 4, ABC=ABC, prism=prism, tol=0.0)
+    d = max(np.abs(r - r0).max() for r, r0 in zip(ref, ref0))
+    assert 0 < d < 1e-3 * scale
+    # math.huge is refused (the reference's ring sum for it is not a lattice sum)
+    assert L.mlb_longrange_set_truncation(h, (C.c_int * 4)(-1, 0, 0, 0)) == 0
+    assert L.mlb_longrange_get_tensor(h, ptrs) == -7
+    L.mlb_op_destroy(h)
