@@ -64,13 +64,20 @@ __device__ __forceinline__ double fs_rsqrt(double v) { return rsqrt(v); }
 __device__ __forceinline__ void fs_sincos(float a, float* s, float* c) { sincosf(a, s, c); }
 __device__ __forceinline__ void fs_sincos(double a, double* s, double* c) { sincos(a, s, c); }
 
-template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R = float>
-__device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
-                                             const R* __restrict__ sx, const R* __restrict__ sy,
-                                             const R* __restrict__ sz, R Ax, R Ay, R Az, R& rx, R& ry, R& rz)
+// The spins come through ld(c, j) (component c of site j): global loads, or
+// shared-memory copies of some rows (the fused x pass).
+template <typename R>
+struct GlobalSpins {
+    const R* __restrict__ s[3];
+    __device__ __forceinline__ R operator()(int c, int j) const { return __ldg(s[c] + j); }
+};
+
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R, class LD>
+__device__ __forceinline__ void fused_site_ld(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                              const LD& ld, R Ax, R Ay, R Az, R& rx, R& ry, R& rz)
 {
     const int nxy = NX * NY;
-    const R Sx = __ldg(sx + i), Sy = __ldg(sy + i), Sz = __ldg(sz + i);
+    const R Sx = ld(0, i), Sy = ld(1, i), Sz = ld(2, i);
     R Hx, Hy, Hz;
     if (F.Bdev) { Hx = (R)F.Bdev[0]; Hy = (R)F.Bdev[1]; Hz = (R)F.Bdev[2]; }
     else { Hx = F.B[0]; Hy = F.B[1]; Hz = F.B[2]; }
@@ -82,7 +89,7 @@ __device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY,
             if (cond) f = i + (off);                                                               \
             else if (wrapcond) f = i + (woff);                                                     \
             if (f >= 0) {                                                                          \
-                ex += (J) * __ldg(sx + f); ey += (J) * __ldg(sy + f); ez += (J) * __ldg(sz + f);   \
+                ex += (J) * ld(0, f); ey += (J) * ld(1, f); ez += (J) * ld(2, f);                \
             }                                                                                      \
         }
         MLB_NB(x + 1 < NX, F.pbc[0], 1, 1 - NX, F.J[0])
@@ -176,5 +183,14 @@ __device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY,
     }
     rx = nx_; ry = ny_; rz = nz_;
     if (F.status && !(isfinite(nx_) && isfinite(ny_) && isfinite(nz_))) atomicOr(F.status, 1u);
+}
+
+template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R = float>
+__device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
+                                             const R* __restrict__ sx, const R* __restrict__ sy,
+                                             const R* __restrict__ sz, R Ax, R Ay, R Az, R& rx, R& ry, R& rz)
+{
+    const GlobalSpins<R> g{{sx, sy, sz}};
+    fused_site_ld<LT, EXS, ANI, TH, ADD, R>(F, NX, NY, NZ, x, y, z, i, g, Ax, Ay, Az, rx, ry, rz);
 }
 
