@@ -194,34 +194,79 @@ SUR_DIMS = (512, 512, 4)
 SUR_WORKLOAD = ("film 512x512x4, periodic x/y, open z (z padded to 8), J=1, K=0.02 z, g=0.05, T=0.1, "
                 "alpha=0.02, dt=0.005, LLG.Quaternion; spins from a seeded random start relaxed 200 steps; "
                 "surrogate: linear spectral-conv net (BF16 tcgen05, 16x16 modes, radius-2 stencil) trained "
-                "online on the plain method")
+                "online on the plain method over 8 seeded random-start runs")
 
 
-def run_surrogate(M, torch, steps, flush_l2=None):
-    """Plain fused FFT path vs the learned surrogate on the 512x512x4 film:
-    spin-steps/s of both on the same system, and the surrogate's relative
-    dipolar-field error against the exact FFT field (the device FP32 field,
-    itself within 1e-5 of the FP64 oracle) at each exact-evaluation period k."""
-    dims = SUR_DIMS
+def _sur_system(M, dims, seed, relax, ops=None):
+    """A 512x512x4 film from a seeded random start with the surrogate
+    workload's operators (shared between systems of the size), relaxed by
+    `relax` plain steps."""
     n = int(np.prod(dims))
-    r = np.random.default_rng(1000)
+    r = np.random.default_rng(seed)
     v = r.normal(size=(3, n))
     v /= np.linalg.norm(v, axis=0)
     ss = M.SpinSystem(*dims)
     ss.setSpinArrays(*v)
     ss.setAlpha(0.02)
     ss.setTimeStep(0.005)
-    ex = M.Exchange(ss)
-    ex.addPaths(*nn_paths(*dims))
-    ani = M.Anisotropy(ss)
-    ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.02))
-    th = M.Thermal(ss, M.Random.Philox(1000))
-    th.setTemperature(0.1)
-    dip = M.Dipole(ss)
-    dip.setStrength(0.05)
-    ops = [ex, ani, th, dip]
+    if ops is None:
+        ex = M.Exchange(*dims)
+        ex.addPaths(*nn_paths(*dims))
+        ani = M.Anisotropy(*dims)
+        ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.02))
+        th = M.Thermal(*dims)
+        th.setSeed(1000)
+        th.setTemperature(0.1)
+        dip = M.Dipole(*dims)
+        dip.setStrength(0.05)
+        ops = [ex, ani, th, dip]
     llg = M.LLG.new("Quaternion")
-    M.run(ss, ops, llg, 200)
+    if relax:
+        M.run(ss, ops, llg, relax)
+    return ss, ops, llg
+
+
+def _sur_error_fp64(M, S, ss, ops, llg, k, windows):
+    """Relative dipolar-field error of the surrogate against the FP64 field:
+    per window, m0 and the exact FP32 field H0 at its start (what a surrogate
+    run holds), then for j = 1 .. k-1 plain steps H0 + net(m_j - m0) against
+    the field of m_j evaluated with FP64 state (FP64 FFT convolution of the
+    same Dipole tensor).  Returns mean and max of the error and the same for
+    holding H0 (the method without the network)."""
+    dims = ss._dims
+    d64 = M.SpinSystem(*dims, precision="f64")
+    dip64 = M.Dipole(*dims)
+    dip64.setStrength(ops[-1].strength())
+    dip = ops[-1]
+    errs, hold = [], []
+    for _ in range(windows):
+        m0 = np.stack(ss.spinArrays()[:3])
+        ss.resetFields()
+        dip.apply(ss)
+        h0 = np.stack(ss.fieldArrays("Dipole"))
+        for j in range(1, k):
+            M.run(ss, ops, llg, 1)
+            mj = np.stack(ss.spinArrays()[:3])
+            d64.setSpinArrays(*mj)
+            dip64.apply(d64)
+            h64 = np.stack(d64.fieldArrays("Dipole"))
+            pred = h0 + S.forward(mj - m0)
+            nrm = np.linalg.norm(h64)
+            errs.append(float(np.linalg.norm(pred - h64) / nrm))
+            hold.append(float(np.linalg.norm(h0 - h64) / nrm))
+        M.run(ss, ops, llg, 1)
+    return float(np.mean(errs)), float(np.max(errs)), float(np.mean(hold))
+
+
+def run_surrogate(M, torch, steps, train_runs=8, train_steps=250):
+    """Plain fused FFT path vs the learned surrogate on the 512x512x4 film:
+    spin-steps/s of both on the same system; the surrogate trained on the
+    plain method over `train_runs` seeded random-start runs; its relative
+    dipolar-field error against the FP64 field at each exact-evaluation
+    period k (and the run's own residual-check statistics)."""
+    dims = SUR_DIMS
+    n = int(np.prod(dims))
+    ss, ops, llg = _sur_system(M, dims, 1000, 200)
     st = torch.cuda.ExternalStream(ss.stream())
 
     def timed(fn, k):
@@ -236,21 +281,39 @@ def run_surrogate(M, torch, steps, flush_l2=None):
     plan = M.Plan(ss, ops, llg)
     plan.launch(3)
     plain_ms = timed(plan.launch, steps)
-    S = M.Surrogate(dip, (16, 16), 2)
+    plan_nd = M.Plan(ss, ops[:3], llg)
+    plan_nd.launch(3)
+    nodip_ms = timed(plan_nd.launch, steps)
+    del plan_nd
+    S = M.Surrogate(ops[-1], (16, 16), 2)
     t0 = time.perf_counter()
-    loss = S.train(ss, ops, llg, 1000, window=10, lr=2e-3)
+    losses = []
+    for r in range(train_runs):
+        tss, _, tl = _sur_system(M, dims, 2000 + r, 50, ops)
+        losses.append(S.train(tss, ops, tl, train_steps, window=10, lr=2e-3))
+        del tss
     train_s = time.perf_counter() - t0
     out = {"workload": SUR_WORKLOAD, "sites": n, "plain": {"value": n / (plain_ms * 1e-3), "ms_per_step": plain_ms},
-           "train": {"steps": 1000, "seconds": train_s, "final_rel_loss": loss}, "by_k": {}}
+           "without_dipole": {"ms_per_step": nodip_ms, "amdahl_ceiling": plain_ms / nodip_ms,
+                              "how": "the same film's captured step without the Dipole operator: the bound on what "
+                                     "replacing the dipole evaluation by anything can gain"},
+           "train": {"runs": train_runs, "steps_per_run": train_steps, "seconds": train_s,
+                     "final_rel_loss_per_run": losses,
+                     "how": "online training on the plain method, one seeded random-start run after another "
+                            "(seeds 2000..), each relaxed 50 steps first"},
+           "by_k": {}}
     for k in (5, 10, 20):
         val = S.validate(ss, ops, llg, 4 * k, window=k)
+        e64 = _sur_error_fp64(M, S, ss, ops, llg, k, 2)
         S.setSchedule(k, tol=1e-3)
         S.run(ss, ops, llg, k)
         ms = timed(lambda m: S.run(ss, ops, llg, m), max(steps, 10 * k))
         st_ = S.stats()
         out["by_k"][str(k)] = {"value": n / (ms * 1e-3), "ms_per_step": ms, "speedup_vs_plain": plain_ms / ms,
-                               "field_rel_err_mean": val["field_mean"], "field_rel_err_max": val["field_max"],
-                               "field_rel_err_without_net_mean": val["field_without_mean"],
+                               "field_rel_err_vs_fp64_mean": e64[0], "field_rel_err_vs_fp64_max": e64[1],
+                               "field_rel_err_vs_fp64_without_net_mean": e64[2],
+                               "field_rel_err_vs_fp32_mean": val["field_mean"],
+                               "field_rel_err_vs_fp32_max": val["field_max"],
                                "exact": st_["exact"], "surrogate": st_["surrogate"], "failed_checks": st_["failed"]}
     out["l2"] = "working set about 100 MB: L2-resident, no flush (both paths measured the same way)"
     return out
@@ -275,10 +338,18 @@ def run_rk(M, torch, steps=20):
     b.record(st)
     ss.synchronize()
     ms = a.elapsed_time(b) / steps
+    with M.profile() as prof:
+        rk.step(steps)
+        ss.synchronize()
+    kern_ms = sum(t for t, c in prof.kernels.values()) / steps
+    launches = sum(c for t, c in prof.kernels.values()) / steps
     n = NX * NY * NZ
     return {"workload": WORKLOAD.replace("LLG.Quaternion", "RK4 (LLG.Quaternion stages) + thermal kick"),
             "value": n / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-            "how": "mlb_rk_step: eager launches (no graph capture), L2 not flushed"}
+            "kernel_ms_per_step": kern_ms, "launches_per_step": launches,
+            "how": "mlb_rk_step: eager launches (no graph capture), L2 not flushed; kernel_ms_per_step sums the "
+                   "kernels' own event-timed durations, so ms_per_step - kernel_ms_per_step bounds what capturing "
+                   "the step in a graph could remove"}
 
 
 # ----------------------------------------------------------------- FP64 film
@@ -515,6 +586,13 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def wait_first(self, timeout_s=5.0):
+        """Until the sampler has produced its first line (nvidia-smi takes a
+        moment to start)."""
+        t_end = time.perf_counter() + timeout_s
+        while self.proc and not self.lines and time.perf_counter() < t_end:
+            time.sleep(0.01)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
@@ -740,9 +818,21 @@ def main():
     # timed region: one captured step per launch, per-step events, L2 flush
     # (write then read sweep) before every step, outside the events
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # clocks: nvidia-smi samples every 50 ms, longer than the timed region,
+    # so the sampling window runs from a quarter second of load (L2 flush
+    # sweeps) before the timed region to a quarter second after it
     clocks = ClockSampler(local)
-    barrier()
     clocks.start()
+    clocks.wait_first()
+
+    def load(seconds):
+        t_end = time.perf_counter() + seconds
+        while time.perf_counter() < t_end:
+            flush_l2()
+            ss.synchronize()
+
+    load(0.25)
+    barrier()
     for k in range(args.steps):
         flush_l2()
         evs[k][0].record(stream)
@@ -750,7 +840,9 @@ def main():
         evs[k][1].record(stream)
     ss.synchronize()
     barrier()
+    load(0.25)
     clk = clocks.stop()
+    clk["window"] = "0.25 s of load before the timed region to 0.25 s after it (samples every 50 ms)"
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
     if dist:
@@ -830,6 +922,31 @@ def main():
     # of three complete runs
     e2e_runs = sorted(e2e_run() for _ in range(3))
     e2e_s = e2e_runs[1]
+
+    # the same run split into its parts (each synchronised on its own): the
+    # one-off upload and download, and the per-step API loop
+    def e2e_parts():
+        barrier()
+        t0 = time.perf_counter()
+        ss.uploadF32(hx, hy, hz, hm)
+        ss.synchronize()
+        t1 = time.perf_counter()
+        depth = 2
+        for k in range(args.steps):
+            plan_nt.launch(1)
+            ss.netMomentAsync(k % 4)
+            if k >= depth:
+                ss.netMomentWait((k - depth) % 4)
+        for k in range(max(0, args.steps - depth), args.steps):
+            ss.netMomentWait(k % 4)
+        ss.synchronize()
+        t2 = time.perf_counter()
+        ss.downloadF32(hx, hy, hz)
+        ss.synchronize()
+        t3 = time.perf_counter()
+        return t1 - t0, t2 - t1, t3 - t2
+
+    parts = sorted((e2e_parts() for _ in range(3)), key=lambda p: p[1])[1]
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -885,10 +1002,16 @@ def main():
                    "llg": "Quaternion", "path": "plain fused FFT path"},
         "clocks": clk,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": (16 * n) / args.steps,
-                "d2h_bytes_per_step": 48 + (12 * n) / args.steps,
+                "d2h_bytes_per_step": 48 + (12 * n) / args.steps, "steps": args.steps,
                 "how": "C-ABI calls from host: pinned FP32 upload, per step mlb_plan_launch(1) + netMoment of that "
                        "step read into pinned memory and waited for once two more steps are queued, final download; median of "
-                       "three complete runs"},
+                       "three complete runs; the upload and download are once per run, so the figure depends on "
+                       "the step count",
+                "parts": {"upload_ms": parts[0] * 1e3, "loop_ms_per_step": parts[1] * 1e3 / args.steps,
+                          "download_ms": parts[2] * 1e3,
+                          "loop_value": n / (parts[1] / args.steps),
+                          "how": "the same run with a synchronisation after the upload and before the download: "
+                                 "upload, the per-step API loop (launch + netMoment read), download"}},
         "gpu_launches": launches,
         "roofline": roof,
         "kernels": kernels_out,
@@ -900,6 +1023,20 @@ def main():
                                 "how": "the film's captured step without the Dipole operator, back to back, no flush: "
                                        "the bound on what replacing the dipole evaluation by anything can gain"},
         "cpu_baseline": cpu,
+        "plain_vs_surrogate_batched": {
+            "batched_vs_plain_one_system_per_replica": batched["plain_one_system_per_replica"]["speedup_of_batched"],
+            "batched_value": batched["value"],
+            "plain_one_system_per_replica_value": batched["plain_one_system_per_replica"]["value"],
+            "ensemble_no_dipole_ceiling": batched["without_dipole"]["amdahl_ceiling"],
+            "film_no_dipole_ceiling": ss_ms / nodip_ms,
+            "surrogate_film_speedup_by_k": ({k: v["speedup_vs_plain"] for k, v in surrogate["by_k"].items()}
+                                            if surrogate else None),
+            "surrogate_film_field_err_vs_fp64_by_k": ({k: v["field_rel_err_vs_fp64_mean"]
+                                                       for k, v in surrogate["by_k"].items()} if surrogate else None),
+            "how": "configuration 3's replicas: the packed ensemble (exact FFT dipole, FP32) against the same "
+                   "replicas through the plain path one SpinSystem each; the learned surrogate on configuration "
+                   "4's film against that film's plain path, its field error against the FP64 field; the "
+                   "no-dipole ceilings bound what any dipole surrogate can gain on each workload"},
         "batched_ensemble": batched,
         "surrogate": surrogate,
         "cube_256": cube,
