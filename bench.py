@@ -162,6 +162,28 @@ def _plain_replicas(M, torch, dims, steps):
     return (time.perf_counter() - t0) * 1e3 / steps
 
 
+def _pow2_at_least(m):
+    p = 1
+    while p < m:
+        p *= 2
+    return p
+
+
+def ensemble_bytes(dims):
+    """Algorithmic bytes of one ensemble step by the per-site formula
+    B = 36 + 24 + (K/N)(24 + 48 * 2) per replica, K = (Px/2+1) Py Pz stored
+    k-points with every axis of an open replica padded to the power of two
+    at least 2n - 1 (z: 1 when nz = 1)."""
+    total = 0
+    for nx, ny, nz in dims:
+        n = nx * ny * nz
+        Px, Py = _pow2_at_least(2 * nx - 1), _pow2_at_least(2 * ny - 1)
+        Pz = 1 if nz == 1 else _pow2_at_least(2 * nz - 1)
+        K = (Px // 2 + 1) * Py * Pz
+        total += 60 * n + K * (24 + 48 * 2)
+    return total
+
+
 def run_batched(M, torch, steps, warmup):
     """Configuration 3: the packed ensemble (one captured graph per step,
     classes on concurrent branches, tuned tile/grid/(y,z) variant), the same
@@ -173,8 +195,14 @@ def run_batched(M, torch, steps, warmup):
     sites = info["sites"]
     _, ms_nodip = _time_ensemble(M, torch, dims, 0.0, steps, warmup)
     plain_ms = _plain_replicas(M, torch, dims, max(3, min(steps, 10)))
+    nbytes = ensemble_bytes(dims)
+    peak, peak_kind = measured_peak()
     return {"value": sites * steps / (ms * steps * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "sites": sites, "replicas": len(dims), "fused_block_size": info["block_size"],
+            "step_roofline": {"algorithmic_bytes_per_step": nbytes, "achieved_gbs": nbytes / (ms * 1e-3) / 1e9,
+                              "frac": nbytes / (ms * 1e-3) / 1e9 / peak, "peak": peak, "peak_kind": peak_kind,
+                              "how": "36 + 24 B per site + (24 + 96) B per stored k-point of each replica's padded "
+                                     "grid, over the event-timed step"},
             "config": e.configInfo(), "tune_log": e.tuneLog().strip().splitlines(),
             "workload": ENS_WORKLOAD,
             "plain_one_system_per_replica": {"value": sites / (plain_ms * 1e-3), "ms_per_step": plain_ms,
@@ -761,7 +789,7 @@ def main():
             ss.synchronize()
         if args.ncu_ensemble:
             import torch
-            run_batched(M, torch, args.ncu_ensemble, 3)
+            _time_ensemble(M, torch, ensemble_dims(), 0.02, args.ncu_ensemble, 3)
         return
     args.warmup = max(3, args.warmup)
 
