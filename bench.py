@@ -690,6 +690,17 @@ def cpu_baseline(procs=1, target_s=15.0):
                       f"FP64 C restatement (gcc -O2), Mersenne-Twister thermal noise, own FFT in place of FFTW"}
 
 
+# ----------------------------------------------------------------- ranks
+def reduce_max(v, dist):
+    """The maximum of v over the process group's ranks (every rank gets it):
+    the device time of a weak-scaling run is the slowest rank's."""
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ----------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -697,6 +708,8 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="reference arm: seconds of CPU work per process in its bounded sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate comparison")
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 open-cube precision study")
@@ -801,7 +814,7 @@ def main():
         if rank != 0:
             return
         procs = os.cpu_count() or 1
-        cb = cpu_baseline(procs=procs, target_s=20.0)
+        cb = cpu_baseline(procs=procs, target_s=args.cpu_seconds)
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -874,9 +887,7 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = reduce_max(total_ms, dist)
     value = world * n * args.steps / (total_ms * 1e-3)
 
     # per-kernel times: the same step captured with event nodes around each
@@ -976,9 +987,7 @@ def main():
 
     parts = sorted((e2e_parts() for _ in range(3)), key=lambda p: p[1])[1]
     if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = reduce_max(e2e_s, dist)
     e2e_val = world * n * args.steps / e2e_s
 
     batched = run_batched(M, torch, args.steps, args.warmup)
