@@ -2944,7 +2944,10 @@ int mlb_system_get_spins(mlb_system* s, double* x, double* y, double* z, double*
 int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const float* z, const float* ms)
 {
     return guard([&] {
-        g_version++;
+        // captured steps hold device pointers and the moment magnitudes'
+        // constants, not spin values: a write of the spins alone keeps them
+        // (the carried spectrum and lazy records are settled below)
+        if (ms) g_version++;
         spins_changing(s);
         const float* src[3] = {x, y, z};
         if (s->rb == 4) {

@@ -258,3 +258,24 @@ def test_uniform_cubic_on_the_fused_pass(M, quirk, llg):
         p.step_oracle(ol)
     err = float(np.abs(res[2] - p.o.spins()).max())
     assert err < 1e-5, err
+
+
+def test_plan_after_spin_upload_matches_a_fresh_run(M):
+    """mlb_system_upload_f32 of the spins alone (magnitudes kept) between plan
+    launches: the captured step is reused (no new capture) and the run from
+    the uploaded spins equals, bit for bit, a fresh system run from them."""
+    dims = (64, 32, 4)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 51, deg=25.0)
+    s1 = tilted_spins(n, 52, deg=35.0).astype(np.float32)
+    ssA, opsA, lA = build(M, dims, s0, llg="Quaternion", T=0.0)
+    ssA.setSpinArrays(*s0, np.ones(n))          # unit moments on both systems
+    plan = M.Plan(ssA, opsA, lA)
+    plan.launch(5)
+    ssA.uploadF32(*[np.ascontiguousarray(s1[c]) for c in range(3)])
+    plan.launch(7)
+    ssB, opsB, lB = build(M, dims, s1.astype(np.float64), llg="Quaternion", T=0.0)
+    ssB.setSpinArrays(*s1.astype(np.float64), np.ones(n))
+    M.run(ssB, opsB, lB, 7)
+    np.testing.assert_array_equal(np.stack(ssA.spinArrays()[:3]), np.stack(ssB.spinArrays()[:3]))
+    np.testing.assert_array_equal(np.stack(ssA.fieldArrays("Total")), np.stack(ssB.fieldArrays("Total")))
