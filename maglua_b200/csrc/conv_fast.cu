@@ -1025,42 +1025,45 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
         }
     }
     const FastK F = fastk_resolved(F0);
-    // 1. spectrum rows SPEC[kx][comp][row0 + row] -> B[(comp ROWS + row) KX + kx]
-    constexpr int IS = (X::SPEC + NT - 1) / NT;
+    // 1. line l = comp R2 + p: Z[k] = S_row(2p)[k] + i S_row(2p+1)[k] for
+    // k < KX, Hermitian completion Z[PX - k] from the conjugates; one item
+    // per (kx, comp, p), the row pair's two spectrum values (adjacent in
+    // SPEC[kx][comp][row]) loaded together when the pair is 16-byte aligned
+    constexpr int NPI = KX * 3 * R2;
+    constexpr int IS = (NPI + NT - 1) / NT;
     {
-        float2 v[IS];
+        float4 v[IS];
+        const bool pair_ld = (nr & 1) == 0;   // row0 is even: (kx 3 + comp) nr + row0 + 2p is even
 #pragma unroll
         for (int it = 0; it < IS; it++) {
             const int idx = threadIdx.x + it * NT;
-            const int kx = idx / (3 * ROWS), rem = idx % (3 * ROWS);
-            const int comp = rem / ROWS, row = rem % ROWS;
-            v[it] = make_float2(0.f, 0.f);
-            if (idx < X::SPEC && row < rows_here)
-                v[it] = spec[((size_t)kx * 3 + comp) * nr + row0 + row];
+            const int kx = idx / (3 * R2), rem = idx % (3 * R2);
+            const int comp = rem / R2, p = rem % R2;
+            v[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (idx < NPI && 2 * p < rows_here) {
+                const float2* src = spec + ((size_t)kx * 3 + comp) * nr + row0 + 2 * p;
+                if (pair_ld && 2 * p + 1 < rows_here) {
+                    v[it] = *reinterpret_cast<const float4*>(src);
+                } else {
+                    const float2 a = src[0];
+                    const float2 b = 2 * p + 1 < rows_here ? src[1] : make_float2(0.f, 0.f);
+                    v[it] = make_float4(a.x, a.y, b.x, b.y);
+                }
+            }
         }
 #pragma unroll
         for (int it = 0; it < IS; it++) {
             const int idx = threadIdx.x + it * NT;
-            const int kx = idx / (3 * ROWS), rem = idx % (3 * ROWS);
-            if (idx < X::SPEC) B[rem * KX + kx] = v[it];
+            if (idx >= NPI) continue;
+            const int kx = idx / (3 * R2), l = idx % (3 * R2);   // l = comp R2 + p
+            float2* Zl = A + l * LS;
+            float2 a = make_float2(v[it].x, v[it].y), b = make_float2(v[it].z, v[it].w);
+            Zl[kx] = make_float2(a.x - b.y, a.y + b.x);
+            if (kx > 0 && kx < PX - KX + 1) {
+                a = cconj(a); b = cconj(b);
+                Zl[PX - kx] = make_float2(a.x - b.y, a.y + b.x);
+            }
         }
-    }
-    __syncthreads();
-    // line l = comp R2 + p: Z[k] = S_row(2p)[k] + i S_row(2p+1)[k], Hermitian completion
-    constexpr int LD = X::L * PX;
-    constexpr int IL = (LD + NT - 1) / NT;
-#pragma unroll
-    for (int it = 0; it < IL; it++) {
-        const int idx = threadIdx.x + it * NT;
-        if (idx >= LD) continue;
-        const int l = idx / PX, k = idx % PX;
-        const int comp = l / R2, p = l % R2;
-        const float2* Sa = B + (comp * ROWS + 2 * p) * KX;
-        const float2* Sb = Sa + KX;
-        float2 a, b;
-        if (k < KX) { a = Sa[k]; b = Sb[k]; }
-        else { a = cconj(Sa[PX - k]); b = cconj(Sb[PX - k]); }
-        A[l * LS + k] = make_float2(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;

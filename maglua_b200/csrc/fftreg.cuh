@@ -179,18 +179,21 @@ __device__ __forceinline__ void sm_stage(const C* src, C* dst, int tl, const C* 
     }
 }
 
+// A line's TPL threads are consecutive and TPL divides 32, so every line
+// lies inside one warp: a stage only has to synchronise the warp.
 template <int N, int SIGN, int TPL, int NS, typename C>
 struct SmStages {
+    static_assert(TPL <= 32 && 32 % TPL == 0, "a line's threads must lie in one warp");
     // radix-4 while four more points fit, a final radix-2 when log2(N) is odd
     __device__ __forceinline__ static C* run(C* a, C* b, int tl, const C* tw, bool act)
     {
         if (NS * 4 <= N) {
             if (act) sm_stage<N, 4, NS, SIGN, TPL, C>(a, b, tl, tw);
-            __syncthreads();
+            __syncwarp();
             return SmStages<N, SIGN, TPL, (NS * 4 <= N ? NS * 4 : N), C>::run(b, a, tl, tw, act);
         } else if (NS * 2 <= N) {
             if (act) sm_stage<N, 2, NS, SIGN, TPL, C>(a, b, tl, tw);
-            __syncthreads();
+            __syncwarp();
             return b;
         }
         return a;
@@ -204,12 +207,14 @@ struct SmStages<N, SIGN, TPL, N, C> {
 // Transform line l (data at a + l*LS, scratch at b + l*LS; LS = N or a
 // padded line stride) by its TPL threads (tl = thread index within the
 // line).  Every thread of the CTA must call this (act = false for threads
-// without a line): it synchronises the CTA after each stage.  Returns the
-// base (a or b) that holds the result.
+// without a line): the stages synchronise the warp, and the CTA is
+// synchronised once after the last stage, so the caller may read any line.
+// Returns the base (a or b) that holds the result.
 template <int N, int SIGN, int TPL, typename C, int LS = N>
 __device__ __forceinline__ C* sm_fft(C* a, C* b, int l, int tl, const C* tw, bool act)
 {
     C* r = SmStages<N, SIGN, TPL, 1, C>::run(a + (size_t)l * LS, b + (size_t)l * LS, tl, tw, act);
+    __syncthreads();
     return r == a + (size_t)l * LS ? a : b;
 }
 

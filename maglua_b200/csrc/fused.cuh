@@ -82,23 +82,31 @@ __device__ __forceinline__ void fused_site_ld(const FastKT<R>& F, int NX, int NY
     if (F.Bdev) { Hx = (R)F.Bdev[0]; Hy = (R)F.Bdev[1]; Hz = (R)F.Bdev[2]; }
     else { Hx = F.B[0]; Hy = F.B[1]; Hz = F.B[2]; }
     if (EXS) {
-        R ex = 0, ey = 0, ez = 0;
-#define MLB_NB(cond, wrapcond, off, woff, J)                                                       \
-        if ((J) != (R)0) {                                                                         \
-            int f = -1;                                                                            \
-            if (cond) f = i + (off);                                                               \
-            else if (wrapcond) f = i + (woff);                                                     \
-            if (f >= 0) {                                                                          \
-                ex += (J) * ld(0, f); ey += (J) * ld(1, f); ez += (J) * ld(2, f);                \
-            }                                                                                      \
+        // the six neighbours (+x, -x, +y, -y, +z, -z; wrapped where periodic,
+        // absent (-1) at an open edge); all eighteen loads are issued before
+        // the first sum (an absent neighbour loads the site itself and is not
+        // added), then the terms are added in the fixed neighbour order
+        int f[6];
+        f[0] = x + 1 < NX ? i + 1 : (F.pbc[0] ? i + 1 - NX : -1);
+        f[1] = x > 0 ? i - 1 : (F.pbc[0] ? i + NX - 1 : -1);
+        f[2] = y + 1 < NY ? i + NX : (F.pbc[1] ? i + NX - nxy : -1);
+        f[3] = y > 0 ? i - NX : (F.pbc[1] ? i + nxy - NX : -1);
+        f[4] = z + 1 < NZ ? i + nxy : (F.pbc[2] ? i + nxy - nxy * NZ : -1);
+        f[5] = z > 0 ? i - nxy : (F.pbc[2] ? i + nxy * NZ - nxy : -1);
+        R nb[6][3];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const int j = f[k] >= 0 ? f[k] : i;
+            nb[k][0] = ld(0, j); nb[k][1] = ld(1, j); nb[k][2] = ld(2, j);
         }
-        MLB_NB(x + 1 < NX, F.pbc[0], 1, 1 - NX, F.J[0])
-        MLB_NB(x > 0, F.pbc[0], -1, NX - 1, F.J[1])
-        MLB_NB(y + 1 < NY, F.pbc[1], NX, NX - nxy, F.J[2])
-        MLB_NB(y > 0, F.pbc[1], -NX, nxy - NX, F.J[3])
-        MLB_NB(z + 1 < NZ, F.pbc[2], nxy, nxy - nxy * NZ, F.J[4])
-        MLB_NB(z > 0, F.pbc[2], -nxy, nxy * NZ - nxy, F.J[5])
-#undef MLB_NB
+        R ex = 0, ey = 0, ez = 0;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const R J = F.J[k];
+            if (J != (R)0 && f[k] >= 0) {
+                ex += J * nb[k][0]; ey += J * nb[k][1]; ez += J * nb[k][2];
+            }
+        }
         Hx += ex; Hy += ey; Hz += ez;
     }
     if (ANI) {
