@@ -60,9 +60,42 @@ struct XCfg {
     static constexpr int LINE = L * PX;                        // line buffer
     static constexpr int SPEC = ROWS * KX;                     // [ROWS][KX] staging
     static constexpr int BUF = LINE > SPEC ? LINE : SPEC;      // each of A, B
-    static constexpr int SMEM = (PX + 2 * BUF) * 8;            // bytes (FP32)
+    // FP32 256-point lines use the register four-step transform, with
+    // one exchange buffer per line after the two line buffers
+    static constexpr int EX = PX == 256 ? L * 16 * 17 : 0;
+    static constexpr int SMEM = (PX + 2 * BUF + EX) * 8;       // bytes (FP32)
     static constexpr int SMEM_D = (PX + 2 * BUF) * 16;         // bytes (FP64)
 };
+
+// 256-point FP32 lines: the four-step register FFT of fr::line_fft (16
+// lanes x 16 points, one warp-synchronous exchange through ex, 16 x 17
+// elements per line), in place on a natural-order line: the lanes have
+// read the whole line before any of them writes it back.
+constexpr int X256_EX = 16 * 17;
+template <int SIGN>
+__device__ __forceinline__ void x256_line(float2* line, float2* ex, int t, unsigned mask, const float2* tw)
+{
+    float2 v[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = line[t + 16 * j];
+    fr::line_fft<256, SIGN, float2>(v, ex, t, mask, tw);
+#pragma unroll
+    for (int r = 0; r < 16; r++) line[fr::out_index<256>(t, r)] = v[r];
+}
+
+// The CTA's nl lines (line l at base + l ls) in place, line l by threads
+// 16 l .. 16 l + 15.  Every thread of the CTA calls this; the CTA is
+// synchronised after the transforms.
+template <int SIGN>
+__device__ __forceinline__ void x256_lines(float2* base, int ls, int nl, float2* ex, const float2* tw)
+{
+    const int l = threadIdx.x >> 4, t = threadIdx.x & 15;
+    if (l < nl) {
+        const unsigned mask = 0xffffu << (threadIdx.x & 16);
+        x256_line<SIGN>(base + (size_t)l * ls, ex + (size_t)l * X256_EX, t, mask, tw);
+    }
+    __syncthreads();
+}
 
 // R = float or double (state precision), C the matching complex type.
 template <int PX, typename R = float>
@@ -107,8 +140,14 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const typename CT<R>::
         if (idx < X::LINE) A[idx] = v[it];
     }
     __syncthreads();
-    const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
-    const C* Rl = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
+    const C* Rl;
+    if constexpr (PX == 256 && sizeof(R) == 4) {
+        x256_lines<-1>(A, PX, X::L, B + X::BUF, twl);
+        Rl = A;
+    } else {
+        const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
+        Rl = fr::sm_fft<PX, -1, X::TPL>(A, B, l, tl, twl, true);
+    }
     // split the two real rows and store SPEC[kx][comp][row] (row = z ny + y)
     const int rows_here = min(X::ROWS, nr - row0);
     constexpr int IS = (X::SPEC + NT - 1) / NT;
@@ -183,8 +222,14 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const typename CT<R>::
         A[idx] = cmk<C>(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
-    const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
-    const C* Rl = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
+    const C* Rl;
+    if constexpr (PX == 256 && sizeof(R) == 4) {
+        x256_lines<+1>(A, PX, X::L, B + X::BUF, twl);
+        Rl = A;
+    } else {
+        const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
+        Rl = fr::sm_fft<PX, +1, X::TPL>(A, B, l, tl, twl, true);
+    }
     constexpr int IO = (X::ROWS * PX + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < IO; it++) {
@@ -971,7 +1016,7 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastKT<R> F0, const R* __res
 // The spectrum rows a CTA reads in 1 and writes in 3 are its own.  Every
 // arithmetic step repeats k_ix_fast, fused_site and k_fx_fast operation for
 // operation, so the result is bitwise that of the three separate kernels.
-template <int PX>
+template <int PX, bool TH = false>
 struct XSCfg {
     static constexpr int NT = 384;
     static constexpr int TPL = fr::Tpl<PX>::V;
@@ -985,7 +1030,13 @@ struct XSCfg {
     static constexpr int LINE = L * LS;
     static constexpr int SPEC = 3 * ROWS * KX;
     static constexpr int BUF = LINE > SPEC ? LINE : SPEC;
-    static constexpr int SMEM = (PX + 2 * BUF) * 8;
+    // thermal: the rows' normals, drawn while the spectrum loads are in
+    // flight, [3][ROWS][PX] floats (where two CTAs per SM still fit)
+    static constexpr bool PRE = TH && PX <= 256;
+    static constexpr int NOISE = PRE ? 3 * ROWS * PX : 0;
+    // 256-point lines: register four-step transforms, one exchange buffer per line
+    static constexpr int EX = PX == 256 ? L * X256_EX : 0;
+    static constexpr int SMEM = (PX + 2 * BUF + EX) * 8 + NOISE * 4;
     static_assert(L % 3 == 0 && ROWS % 2 == 0, "line layout");
 };
 
@@ -997,12 +1048,14 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
                                                   float* __restrict__ hz, float* __restrict__ ox,
                                                   float* __restrict__ oy, float* __restrict__ oz)
 {
-    using X = XSCfg<PX>;
+    using X = XSCfg<PX, TH>;
     constexpr int KX = X::KX, NT = X::NT, ROWS = X::ROWS, R2 = X::R2, LS = X::LS;
     extern __shared__ float2 sm[];
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][LS] lines
-    float2* B = A + X::BUF;         // [3][ROWS][KX] spectra, then scratch
+    float2* B = A + X::BUF;         // [L][LS] scratch
+    float2* EXB = B + X::BUF;       // [L][16 * 17] exchange buffers (PX = 256)
+    float* noise = reinterpret_cast<float*>(EXB + X::EX);   // [3][ROWS][PX] (X::PRE)
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     const int nr = nz * ny;                     // rows (z, y), flattened
     const int row0 = blockIdx.x * ROWS;
@@ -1051,6 +1104,26 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
                 }
             }
         }
+        // the normals of this thread's sites in the step below, while the
+        // loads are in flight
+        constexpr int IP = (R2 * PX + NT - 1) / NT;
+        if (X::PRE) {
+#pragma unroll 1
+            for (int it = 0; it < IP; it++) {
+                const int idx = threadIdx.x + it * NT;
+                if (idx >= R2 * PX) break;
+                const int p = idx / PX, x = idx % PX;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int row = 2 * p + h;
+                    if (row < rows_here && x < nx) {
+                        const float3 g = thermal_normal3(F, (row0 + row) * nx + x);
+                        float* q = noise + row * PX + x;
+                        q[0] = g.x; q[ROWS * PX] = g.y; q[2 * ROWS * PX] = g.z;
+                    }
+                }
+            }
+        }
 #pragma unroll
         for (int it = 0; it < IS; it++) {
             const int idx = threadIdx.x + it * NT;
@@ -1067,7 +1140,13 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     }
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
-    const float2* R = fr::sm_fft<PX, +1, X::TPL, float2, LS>(A, B, l, tl, twl, true);
+    const float2* R;
+    if constexpr (PX == 256) {
+        x256_lines<+1>(A, LS, X::L, EXB, twl);
+        R = A;
+    } else {
+        R = fr::sm_fft<PX, +1, X::TPL, float2, LS>(A, B, l, tl, twl, true);
+    }
     float2* W = (R == A) ? B : A;   // free buffer: the new spins' lines (FWD)
     // 2. field of the rows to the slot, then the step of every site: one
     // (row pair, x) per item, the pair's two rows the real and imaginary
@@ -1089,8 +1168,13 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
                 const size_t i = (size_t)r * nx + x;
                 hx[i] = Ax; hy[i] = Ay; hz[i] = Az;
                 float rx, ry, rz;
+                float3 g;
+                if (X::PRE) {
+                    const float* q = noise + row * PX + x;
+                    g = make_float3(q[0], q[ROWS * PX], q[2 * ROWS * PX]);
+                }
                 fused_site_v<LT, EXS, ANI, TH, true>(F, nx, ny, nz, x, y, zz, (int)i, sx, sy, sz, Ax, Ay, Az, rx, ry,
-                                                     rz);
+                                                     rz, X::PRE ? &g : nullptr);
                 ox[i] = rx; oy[i] = ry; oz[i] = rz;
                 if (h) { o0.y = rx; o1.y = ry; o2.y = rz; }
                 else { o0.x = rx; o1.x = ry; o2.x = rz; }
@@ -1101,7 +1185,13 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     if (!fwd) return;
     __syncthreads();
     // 3. forward transform of the new spins' lines, split into the two rows
-    const float2* Q = fr::sm_fft<PX, -1, X::TPL, float2, LS>(W, const_cast<float2*>(R), l, tl, twl, true);
+    const float2* Q;
+    if constexpr (PX == 256) {
+        x256_lines<-1>(W, LS, X::L, EXB, twl);
+        Q = W;
+    } else {
+        Q = fr::sm_fft<PX, -1, X::TPL, float2, LS>(W, const_cast<float2*>(R), l, tl, twl, true);
+    }
     constexpr int IQ = (X::SPEC + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < IQ; it++) {
@@ -1530,7 +1620,7 @@ template <int PX, int LT, bool ANI, bool TH>
 static cudaError_t xstep_t(const ConvK& c, const FastK& F, int fwd, const float2* tw, float2* spec,
                            const float* s[3], float* h[3], float* o[3], cudaStream_t st)
 {
-    using X = XSCfg<PX>;
+    using X = XSCfg<PX, TH>;
     dim3 grid((c.nz * c.ny + X::ROWS - 1) / X::ROWS, 1, 1);
     return launch_pdl(k_xstep<PX, LT, true, ANI, TH>, grid, dim3(X::NT), (size_t)X::SMEM, st, c, F, fwd, tw, spec,
                       s[0], s[1], s[2], h[0], h[1], h[2], o[0], o[1], o[2]);
@@ -1573,7 +1663,7 @@ template <int PX, int LT, bool ANI, bool TH>
 static cudaError_t cfg_xs1()
 {
     cudaError_t e = cudaFuncSetAttribute(k_xstep<PX, LT, true, ANI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         XSCfg<PX>::SMEM);
+                                         XSCfg<PX, TH>::SMEM);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_xstep<PX, LT, true, ANI, TH>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared);

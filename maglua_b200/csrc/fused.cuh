@@ -72,9 +72,19 @@ struct GlobalSpins {
     __device__ __forceinline__ R operator()(int c, int j) const { return __ldg(s[c] + j); }
 };
 
+// The thermal site's three standard normals are those of thermal_normal3();
+// a caller that drew them earlier passes them in pre (else nullptr).
+template <typename R>
+__device__ __forceinline__ float3 thermal_normal3(const FastKT<R>& F, int i)
+{
+    const uint64_t ctr = F.counter + (F.dctr ? *F.dctr : 0ull);
+    return philox_normal3(F.seed, ctr, (uint32_t)i, 0x6d6c6232u);
+}
+
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R, class LD>
 __device__ __forceinline__ void fused_site_ld(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
-                                              const LD& ld, R Ax, R Ay, R Az, R& rx, R& ry, R& rz)
+                                              const LD& ld, R Ax, R Ay, R Az, R& rx, R& ry, R& rz,
+                                              const float3* pre = nullptr)
 {
     const int nxy = NX * NY;
     const R Sx = ld(0, i), Sy = ld(1, i), Sz = ld(2, i);
@@ -123,8 +133,7 @@ __device__ __forceinline__ void fused_site_ld(const FastKT<R>& F, int NX, int NY
     }
     R Tx = 0, Ty = 0, Tz = 0;
     if (TH) {
-        const uint64_t ctr = F.counter + (F.dctr ? *F.dctr : 0ull);
-        const float3 nrm = philox_normal3(F.seed, ctr, (uint32_t)i, 0x6d6c6232u);
+        const float3 nrm = pre ? *pre : thermal_normal3(F, i);
         Tx = F.sigma * nrm.x; Ty = F.sigma * nrm.y; Tz = F.sigma * nrm.z;
         Hx += Tx; Hy += Ty; Hz += Tz;
     }
@@ -196,9 +205,10 @@ __device__ __forceinline__ void fused_site_ld(const FastKT<R>& F, int NX, int NY
 template <int LT, bool EXS, bool ANI, bool TH, bool ADD, typename R = float>
 __device__ __forceinline__ void fused_site_v(const FastKT<R>& F, int NX, int NY, int NZ, int x, int y, int z, int i,
                                              const R* __restrict__ sx, const R* __restrict__ sy,
-                                             const R* __restrict__ sz, R Ax, R Ay, R Az, R& rx, R& ry, R& rz)
+                                             const R* __restrict__ sz, R Ax, R Ay, R Az, R& rx, R& ry, R& rz,
+                                             const float3* pre = nullptr)
 {
     const GlobalSpins<R> g{{sx, sy, sz}};
-    fused_site_ld<LT, EXS, ANI, TH, ADD, R>(F, NX, NY, NZ, x, y, z, i, g, Ax, Ay, Az, rx, ry, rz);
+    fused_site_ld<LT, EXS, ANI, TH, ADD, R>(F, NX, NY, NZ, x, y, z, i, g, Ax, Ay, Az, rx, ry, rz, pre);
 }
 
