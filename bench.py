@@ -905,6 +905,21 @@ def main():
             kern_n[nm] = kern_n.get(nm, 0) + 1
     ss.synchronize()
 
+    # device timeline of the same flushed steps with the step's dependent
+    # launches kept (no event nodes): each pass from its first CTA released
+    # from the dependency wait to its last CTA's end (%globaltimer)
+    plan_dt = M.Plan(ss, ops, llg, timing=2)
+    plan_dt.launch(2)
+    plan_dt.deviceTimes()
+    dev_us = {}
+    for k in range(ksteps):
+        flush_l2()
+        plan_dt.launch(1)
+        for nm, us in plan_dt.deviceTimes().items():
+            dev_us.setdefault(nm, []).append(us)
+    ss.synchronize()
+    del plan_dt
+
     # steady state without flushes (L2-resident state), same plan
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
@@ -1021,7 +1036,20 @@ def main():
         tr = traffic.get(dom)
         roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_kind": peak_kind + " (burst copy)",
-                "traffic": tr, "algorithmic_bytes_per_launch": per_launch[dom]}
+                "traffic": tr, "algorithmic_bytes_per_launch": per_launch[dom],
+                "timing": "CUDA event nodes around the kernel in a timing copy of the captured step (the "
+                          "kernel's own launch latency included)"}
+        if dev_us.get(dom):
+            dus = float(np.median(dev_us[dom]))
+            dach = per_launch[dom] / (dus * 1e-6) / 1e9
+            roof["device_timeline"] = {
+                "us": dus, "achieved": dach, "frac": dach / peak,
+                "how": "median over the flushed timed steps of the captured step with its dependent launches "
+                       "(no event nodes): %globaltimer from the first CTA released from the dependency wait to "
+                       "the last CTA's end"}
+    for k, v in dev_us.items():
+        if k in kernels_out:
+            kernels_out[k]["device_us"] = float(np.median(v))
     step_bytes_gbs = bytes_step / (total_ms / args.steps * 1e-3) / 1e9
     cpu = None
     if not args.no_cpu and world == 1:

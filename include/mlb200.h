@@ -391,13 +391,20 @@ int mlb_llg_decode(const void* buf, size_t len, mlb_llg** out, size_t* used, int
  * apply; sumFields; llg:apply) as CUDA graphs so that one host call
  * enqueues a whole step.  The Thermal counter and the applied field (with
  * its sweep) advance on the device; any other parameter change makes the
- * next launch capture again.  With timing set, every kernel of the step is
+ * next launch capture again.  With timing = 1, every kernel of the step is
  * bracketed by graph event nodes and mlb_plan_kernel_times returns the
- * milliseconds of the last launched step per kernel (48-byte name slots). */
+ * milliseconds of the last launched step per kernel (48-byte name slots).
+ * With timing = 2 the step keeps its dependent launches and the fused (y,z)
+ * and x passes of an FP32 dipole convolution record a device timeline
+ * (%globaltimer): mlb_plan_device_times returns, in microseconds, each
+ * pass's span over the steps launched since the previous call (one step:
+ * that step's span) from its first CTA released from the dependency wait to
+ * its last CTA's end (-1 where a pass did not run), and resets the stamps. */
 typedef struct mlb_plan mlb_plan;
 int mlb_plan_create(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int timing, mlb_plan** out);
 int mlb_plan_launch(mlb_plan* p, int nsteps);
 int mlb_plan_kernel_times(mlb_plan* p, int cap, char* names, double* ms, int* count);
+int mlb_plan_device_times(mlb_plan* p, double* yz_us, double* xstep_us);
 int mlb_plan_destroy(mlb_plan* p);
 
 /* ---------------------------------------------------------------- ensembles

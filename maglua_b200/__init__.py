@@ -195,6 +195,7 @@ _SIGS = {
     "mlb_plan_create": ([_P, C.POINTER(_P), C.c_int, _P, C.c_int, C.POINTER(_P)], C.c_int),
     "mlb_plan_launch": ([_P, C.c_int], C.c_int),
     "mlb_plan_kernel_times": ([_P, C.c_int, C.c_char_p, _D, _I], C.c_int),
+    "mlb_plan_device_times": ([_P, _D, _D], C.c_int),
     "mlb_plan_destroy": ([_P], C.c_int),
     "mlb_ensemble_create": ([C.c_int, _I, C.POINTER(_P)], C.c_int),
     "mlb_ensemble_destroy": ([_P], C.c_int),
@@ -1563,14 +1564,17 @@ class profile:
 class Plan:
     """The canonical step of ss (resetFields; op.apply for op in ops;
     sumFields; llg.apply) captured as CUDA graphs; launch(n) runs n steps with
-    one graph launch each.  timing=True adds event nodes around every kernel
-    (kernelTimes() -> {name: ms} of the last launched step)."""
+    one graph launch each.  timing=True (or 1) adds event nodes around every
+    kernel (kernelTimes() -> {name: ms} of the last launched step); timing=2
+    keeps the step's dependent launches and records a device timeline of the
+    fused (y,z) and x passes (deviceTimes())."""
 
     def __init__(self, ss, ops, llg, timing=False):
         self._keep = (ss, list(ops), llg)
         arr = (_P * len(ops))(*[o._h for o in ops])
         h = _P()
-        _ck(_lib.mlb_plan_create(ss._h, arr, len(ops), llg._h, int(bool(timing)), C.byref(h)))
+        mode = 2 if timing == 2 else int(bool(timing))
+        _ck(_lib.mlb_plan_create(ss._h, arr, len(ops), llg._h, mode, C.byref(h)))
         self._h = h
 
     def launch(self, nsteps=1):
@@ -1587,6 +1591,20 @@ class Plan:
         for k in range(cnt.value):
             nm = raw[48 * k:48 * (k + 1)].split(b"\0", 1)[0].decode()
             out[nm] = out.get(nm, 0.0) + float(ms[k])
+        return out
+
+    def deviceTimes(self):
+        """{"k_conv_yz": us, "k_xstep": us} over the steps launched since the
+        last call (timing=2 plans): each pass from its first CTA released from
+        the dependency wait to its last CTA's end; passes that did not run are
+        left out."""
+        a, b = C.c_double(), C.c_double()
+        _ck(_lib.mlb_plan_device_times(self._h, C.byref(a), C.byref(b)))
+        out = {}
+        if a.value >= 0:
+            out["k_conv_yz"] = a.value
+        if b.value >= 0:
+            out["k_xstep"] = b.value
         return out
 
     def __del__(self):

@@ -265,6 +265,7 @@ struct mlb_system {
     int pend_si = -1;               // and its slot
     bool cap_carry = false;         // capture: assume SPEC holds the current spins' x transform
     mlb_op* cap_xstep = nullptr;    // capture: the convolution whose x pass the captured step fused
+    unsigned long long* cap_tl = nullptr;   // capture: device timeline stamps of a timing plan
     unsigned long long spec_token = 0;   // matches ConvPlan::spec_token while that holds
 };
 
@@ -348,7 +349,9 @@ struct mlb_plan {
     mlb_system* s = nullptr;
     std::vector<mlb_op*> ops;
     mlb_llg* l = nullptr;
-    bool timing = false;
+    bool timing = false;            // event nodes around every kernel
+    bool timeline = false;          // device timeline of the fused (y,z) and x passes
+    DBuf<unsigned long long> tl;    // its four stamps (ConvK::tl)
     cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<mlb::ProfCaptured> ev[4];
     mlb_op* carry_op = nullptr;   // the convolution whose SPEC a step leaves carried (null: none)
@@ -1677,7 +1680,9 @@ void op_apply(mlb_op* op, mlb_system* s)
                 // forward x pass only when SPEC does not already hold it
                 const bool carry = s->capturing ? s->cap_carry
                                                 : (s->spec_token != 0 && s->spec_token == P.spec_token);
-                CK(mlb::launch_conv_fast_fyz(P.k, P.L, reinterpret_cast<const float2*>(P.tw.p), sp,
+                ConvK kk = P.k;
+                kk.tl = s->capturing ? s->cap_tl : nullptr;
+                CK(mlb::launch_conv_fast_fyz(kk, P.L, reinterpret_cast<const float2*>(P.tw.p), sp,
                                              reinterpret_cast<float2*>(P.spec.p),
                                              reinterpret_cast<const float*>(P.ten6.p), !carry, s->st));
                 if (!s->capturing) P.spec_token = 0;
@@ -1839,7 +1844,9 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
                            static_cast<float*>(s->slots[s->pend_si].h[2])};
             s->pend_op = nullptr;
             s->pend_si = -1;
-            CK(mlb::launch_xstep(CP->k, CP->L, reinterpret_cast<const float2*>(CP->tw.p),
+            ConvK kx = CP->k;
+            kx.tl = s->capturing ? s->cap_tl : nullptr;
+            CK(mlb::launch_xstep(kx, CP->L, reinterpret_cast<const float2*>(CP->tw.p),
                                  reinterpret_cast<float2*>(CP->spec.p), F, true, sp, h, out, s->st));
             carried = true;
             if (s->capturing) {
@@ -2165,6 +2172,13 @@ void load_state(mlb_system* s, const std::vector<mlb_op*>& ops, const HostState&
     }
 }
 
+// the device timeline's stamps back to (earliest = all ones, latest = 0)
+void plan_timeline_reset(mlb_plan* p)
+{
+    const unsigned long long init[4] = {~0ull, 0ull, ~0ull, 0ull};
+    CK(cudaMemcpy(p->tl.p, init, sizeof(init), cudaMemcpyHostToDevice));
+}
+
 void plan_release(mlb_plan* p)
 {
     for (int q = 0; q < 4; q++) {
@@ -2208,6 +2222,7 @@ void plan_capture(mlb_plan* p)
             CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
             s->capturing = true;
             s->cap_xstep = nullptr;
+            s->cap_tl = p->timeline ? p->tl.p : nullptr;
             if (p->timing) mlb::prof_set_capture_sink(&p->ev[q]);
             bool ok = true;
             std::string why;
@@ -2220,6 +2235,7 @@ void plan_capture(mlb_plan* p)
             mlb::prof_set_capture_sink(nullptr);
             s->capturing = false;
             s->cap_carry = false;
+            s->cap_tl = nullptr;
             if (q < 2) {
                 // the carried variants exist only when both parities end in the fused x pass
                 if (q == 0) p->carry_op = s->cap_xstep;
@@ -2240,6 +2256,7 @@ void plan_capture(mlb_plan* p)
         s->dry = false;
         s->capturing = false;
         s->cap_carry = false;
+        s->cap_tl = nullptr;
         mlb::prof_set_capture_sink(nullptr);
         load_state(s, p->ops, h0);
         throw;
@@ -4522,9 +4539,30 @@ int mlb_plan_create(mlb_system* s, mlb_op* const* ops, int nops, mlb_llg* l, int
         p->s = s;
         p->ops.assign(ops, ops + nops);
         p->l = l;
-        p->timing = timing != 0;
+        p->timing = timing == 1;
+        p->timeline = timing == 2;
+        if (p->timeline) {
+            p->tl.alloc(4);
+            plan_timeline_reset(p.get());
+        }
         plan_capture(p.get());
         *out = p.release();
+    });
+}
+
+int mlb_plan_device_times(mlb_plan* p, double* yz_us, double* xstep_us)
+{
+    return guard([&] {
+        if (!p->timeline) fail(MLB_ESTATE, "not a device-timeline plan (timing = 2)");
+        CK(cudaStreamSynchronize(p->s->st));
+        unsigned long long t[4];
+        CK(cudaMemcpy(t, p->tl.p, sizeof(t), cudaMemcpyDeviceToHost));
+        auto span = [](unsigned long long a, unsigned long long b) {
+            return (a != ~0ull && b != 0ull && b >= a) ? (double)(b - a) * 1e-3 : -1.0;
+        };
+        *yz_us = span(t[0], t[1]);
+        *xstep_us = span(t[2], t[3]);
+        plan_timeline_reset(p);
     });
 }
 

@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, YZT<PY, PZ>::MINB) k_yz_fast(C
     for (int k = threadIdx.x; k < PY; k += blockDim.x) twl[k] = twy[k];
     pdl_trigger();
     pdl_wait();
+    tl_start(c.tl);
     if (c.run_if && *c.run_if == 0) return;
     float2* sp = spec + (size_t)kx * nlines * ny;
     {
@@ -353,6 +354,7 @@ __global__ void __launch_bounds__(YZT<PY, PZ>::N, YZT<PY, PZ>::MINB) k_yz_fast(C
             if (l < nlines && y < ny) sp[(size_t)l * ny + y] = Y[idx];
         }
     }
+    tl_end(c.tl);
 }
 
 // ------------------------------------------------------------------ (y,z) pass, register form
@@ -399,6 +401,7 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
     for (int k = threadIdx.x; k < PY; k += NT) twl[k] = twy[k];
     pdl_trigger();
     pdl_wait();
+    tl_start(c.tl);
     if (c.run_if && *c.run_if == 0) return;
     // replica blockIdx.y of a packed size class (one for a single film)
     float2* sp = spec + (size_t)blockIdx.y * c.Kx * nlines * ny + (size_t)kx * nlines * ny;
@@ -475,6 +478,7 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
             }
         }
     }
+    tl_end(c.tl);
 }
 
 // ------------------------------------------------------------------ (y,z) pass, three threads per column
@@ -519,6 +523,7 @@ __global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __res
     for (int k = threadIdx.x; k < PY; k += NT) twl[k] = twy[k];
     pdl_trigger();
     pdl_wait();
+    tl_start(c.tl);
     if (c.run_if && *c.run_if == 0) return;
     float2* sp = spec + (size_t)blockIdx.y * c.Kx * nlines * ny + (size_t)kx * nlines * ny;
     __syncthreads();
@@ -614,6 +619,7 @@ __global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __res
             }
         }
     }
+    tl_end(c.tl);
 }
 
 // ------------------------------------------------------------------ split (y,z) passes, FP32
@@ -1063,6 +1069,8 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     for (int k = threadIdx.x; k < PX; k += NT) twl[k] = tw[k];
     pdl_trigger();
     pdl_wait();
+    unsigned long long* tls = c.tl ? c.tl + 2 : nullptr;
+    tl_start(tls);
     if (c.run_if && *c.run_if == 0) return;
     // the rows' spins and their z-neighbour rows, into L2 while the inverse
     // transform runs (the step reads them after it)
@@ -1182,7 +1190,10 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
         }
         if (fwd) { W[(0 * R2 + p) * LS + x] = o0; W[(1 * R2 + p) * LS + x] = o1; W[(2 * R2 + p) * LS + x] = o2; }
     }
-    if (!fwd) return;
+    if (!fwd) {
+        tl_end(tls);
+        return;
+    }
     __syncthreads();
     // 3. forward transform of the new spins' lines, split into the two rows
     const float2* Q;
@@ -1206,6 +1217,7 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
         else o = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
         spec[((size_t)kx * 3 + comp) * nr + row0 + row] = o;
     }
+    tl_end(tls);
 }
 
 // Packed ensemble: tile b covers sites [bstart[b], bstart[b] + blockDim) of

@@ -18,6 +18,27 @@
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Device timeline stamps (%globaltimer, ns): slot t[0] takes the earliest
+// start over the CTAs that call tl_start, t[1] the latest end over those
+// that call tl_end (after the CTA's last store).  No-ops for a null t.
+__device__ __forceinline__ unsigned long long gtimer_ns()
+{
+    unsigned long long v;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+    return v;
+}
+__device__ __forceinline__ void tl_start(unsigned long long* t)
+{
+    if (t && threadIdx.x == 0) atomicMin(t, gtimer_ns());
+}
+__device__ __forceinline__ void tl_end(unsigned long long* t)
+{
+    if (t) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(t + 1, gtimer_ns());
+    }
+}
+
 #ifndef MLB_HD
 #define MLB_HD __host__ __device__ __forceinline__
 #endif

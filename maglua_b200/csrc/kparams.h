@@ -136,6 +136,11 @@ struct ConvK {
     // for ky <= Py/2 and kz <= Pz/2 only, TEN[kx][ky][kz][q], and each z-pass
     // CTA takes mirrored ky columns together.
     int quarter = 0;
+    // Device timeline of a timing plan (null otherwise): the single-CTA-plane
+    // (y,z) kernels write tl[0] = first CTA released from the dependency
+    // wait, tl[1] = last CTA finished; the fused x pass tl[2], tl[3]
+    // (%globaltimer, ns)
+    unsigned long long* tl = nullptr;
 };
 
 // LongRange2D layer scales (spinoperationlongrange2d.cpp:430-530): the

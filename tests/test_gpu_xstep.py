@@ -279,3 +279,30 @@ def test_plan_after_spin_upload_matches_a_fresh_run(M):
     M.run(ssB, opsB, lB, 7)
     np.testing.assert_array_equal(np.stack(ssA.spinArrays()[:3]), np.stack(ssB.spinArrays()[:3]))
     np.testing.assert_array_equal(np.stack(ssA.fieldArrays("Total")), np.stack(ssB.fieldArrays("Total")))
+
+
+def test_device_timeline_plan(M):
+    """A timing=2 plan (device timeline of the fused (y,z) and x passes) steps
+    exactly as a plain plan and reports both passes' spans per step; a plan
+    without the timeline refuses deviceTimes."""
+    dims = (256, 32, 4)
+    n = int(np.prod(dims))
+    s0 = random_spins(n, 61)
+    out = []
+    for timing in (False, 2):
+        ss, ops, l = build(M, dims, s0, llg="Quaternion", T=0.5)
+        p = M.Plan(ss, ops, l, timing=timing)
+        spans = []
+        for _ in range(4):
+            p.launch(1)
+            if timing == 2:
+                spans.append(p.deviceTimes())
+        out.append(state(ss))
+        if timing == 2:
+            for d in spans[1:]:
+                assert set(d) == {"k_conv_yz", "k_xstep"}, d
+                assert all(0.0 < v < 5e4 for v in d.values()), d
+        else:
+            with pytest.raises(M.MagLuaError):
+                p.deviceTimes()
+    assert_same(out[0], out[1])
