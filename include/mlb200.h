@@ -494,11 +494,18 @@ int mlb_dipole_read_wab(mlb_op* op, const char* filename);
  * message).  ops make the deterministic field (resetFields, apply each,
  * sumFields); temp (may be NULL) is a Thermal operator applied after the
  * stages with llg:apply(ss, false).  The stage systems are copies of ss made
- * here (fields included), on ss's stream.  mlb_rk_step runs nsteps steps. */
+ * here (fields included), on ss's stream.  mlb_rk_step runs nsteps steps;
+ * a step whose parameters did not change since the previous step runs as
+ * a CUDA graph (the same kernels and arguments as the eager step, recorded
+ * with their dependent-launch edges, the step graph updated in place), so
+ * its results are those of eager steps bit for bit.  mlb_rk_set_graph(r, 0)
+ * keeps every step eager; mlb_rk_graph_steps counts the graph steps run. */
 typedef struct mlb_rk mlb_rk;
 int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops, mlb_llg* l, mlb_op* temp,
                   mlb_rk** out);
 int mlb_rk_step(mlb_rk* r, int nsteps);
+int mlb_rk_set_graph(mlb_rk* r, int on);
+int mlb_rk_graph_steps(mlb_rk* r, long long* steps);
 /* The step function called on another system of the same size, as the
  * script's step(ss_input, skip_temperature) (RungeKutta.lua:194-213). */
 int mlb_rk_step_on(mlb_rk* r, mlb_system* ss, int skip_temperature);

@@ -182,6 +182,8 @@ _SIGS = {
     "mlb_surrogate_gradients": ([_P, C.POINTER(_F), C.POINTER(_F), _F, _F, C.POINTER(_F), _D], C.c_int),
     "mlb_rk_create": ([_P, C.c_char_p, C.POINTER(_P), C.c_int, _P, _P, C.POINTER(_P)], C.c_int),
     "mlb_rk_step": ([_P, C.c_int], C.c_int),
+    "mlb_rk_set_graph": ([_P, C.c_int], C.c_int),
+    "mlb_rk_graph_steps": ([_P, C.POINTER(C.c_longlong)], C.c_int),
     "mlb_rk_step_on": ([_P, _P, C.c_int], C.c_int),
     "mlb_adapt_create": ([_P, _P, C.c_double, _P, _P, C.POINTER(_P)], C.c_int),
     "mlb_adapt_step": ([_P, _I], C.c_int),
@@ -1825,7 +1827,8 @@ class RungeKutta:
     RungeKutta.lua, run natively: step(n) advances ss by n steps of the
     Butcher scheme `kind` (RK1, RK2, K3, RK4, RK3, RK4_38, RK6, BS3) with the
     field of ops and the optional Thermal operator temp applied after the
-    stages."""
+    stages.  Steps whose parameters did not change since the previous step
+    run as CUDA graphs of the same kernels (setGraph(False): all eager)."""
 
     def __init__(self, ss, kind, ops, llg, temp=None):
         arr = (_P * len(ops))(*[o._h for o in ops])
@@ -1837,6 +1840,14 @@ class RungeKutta:
 
     def step(self, n=1):
         _ck(_lib.mlb_rk_step(self._h, int(n)))
+
+    def setGraph(self, on=True):
+        _ck(_lib.mlb_rk_set_graph(self._h, int(bool(on))))
+
+    def graphSteps(self):
+        n = C.c_longlong()
+        _ck(_lib.mlb_rk_graph_steps(self._h, C.byref(n)))
+        return n.value
 
     def __call__(self, ss=None, skip_temperature=False):
         """The script's step(ss_input, skip_temperature)."""

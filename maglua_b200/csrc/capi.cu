@@ -5171,6 +5171,15 @@ struct mlb_rk {
     mlb_llg* l = nullptr;
     mlb_op* temp = nullptr;              // optional Thermal operator
     std::vector<std::vector<double>> bt; // Butcher rows (the c column is not used)
+    // Graph steps: a step whose parameters did not change since the previous
+    // step is captured (its host logic runs as in an eager step, its kernels
+    // are recorded with their dependent-launch edges), the step graph is
+    // updated in place and launched.
+    bool graph = true;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long version = 0;      // g_version at the previous step
+    int fail_streak = 0;                 // consecutive captures that failed (3: graph steps off)
+    long long graph_steps = 0;           // steps run as graphs
 };
 
 namespace {
@@ -5234,6 +5243,72 @@ void rk_step(mlb_rk* r, mlb_system* ss, bool skip_temperature)
     }
 }
 
+// One step of r on its own system as a graph (see mlb_rk): false when it
+// must run eagerly (parameters changed since the previous step, injected
+// noise pending, a surrogate attached, graph steps off or failing).
+bool rk_graph_ok(mlb_rk* r)
+{
+    if (!r->graph || r->fail_streak >= 3 || r->version != g_version || r->ss->sur) return false;
+    for (mlb_system* c : r->k)
+        if (c->st != r->ss->st) return false;
+    for (mlb_op* o : r->ops)
+        if (o->inject_pending) return false;
+    if (r->temp && r->temp->inject_pending) return false;
+    return true;
+}
+
+void rk_step_graph(mlb_rk* r)
+{
+    mlb_system* ss = r->ss;
+    std::vector<mlb_op*> all = r->ops;
+    if (r->temp) all.push_back(r->temp);
+    std::vector<mlb_system*> sys = {ss};
+    for (mlb_system* c : r->k) sys.push_back(c);
+    std::vector<HostState> saved;
+    for (mlb_system* x : sys) saved.push_back(save_state(x, all));
+    cudaStream_t st = ss->st;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    bool ok = true;
+    try {
+        rk_step(r, ss, false);
+        for (mlb_system* x : sys) flush_pending(x);
+    } catch (Err&) {
+        ok = false;
+    }
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (!ok || e != cudaSuccess || !g) {
+        // nothing was launched: put the bookkeeping back and run the step eagerly
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        for (size_t i = 0; i < sys.size(); i++) {
+            load_state(sys[i], all, saved[i]);
+            sys[i]->spec_token = 0;
+        }
+        r->fail_streak++;
+        rk_step(r, ss, false);
+        return;
+    }
+    if (r->exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(r->exec, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(r->exec);
+            r->exec = nullptr;
+        }
+    }
+    cudaError_t ie = cudaSuccess;
+    if (!r->exec) ie = cudaGraphInstantiate(&r->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        r->exec = nullptr;
+        fail(MLB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    CK(cudaGraphLaunch(r->exec, st));
+    r->fail_streak = 0;
+    r->graph_steps++;
+}
+
 } // namespace
 
 extern "C" {
@@ -5279,7 +5354,28 @@ int mlb_rk_create(mlb_system* ss, const char* type, mlb_op* const* ops, int nops
 int mlb_rk_step(mlb_rk* r, int nsteps)
 {
     return guard([&] {
-        for (int k = 0; k < nsteps; k++) rk_step(r, r->ss, false);
+        for (int k = 0; k < nsteps; k++) {
+            if (rk_graph_ok(r)) rk_step_graph(r);
+            else rk_step(r, r->ss, false);
+            r->version = g_version;
+        }
+    });
+}
+
+int mlb_rk_set_graph(mlb_rk* r, int on)
+{
+    return guard([&] {
+        if (!r) fail(MLB_EINVAL, "null scheme");
+        r->graph = on != 0;
+        r->fail_streak = 0;
+    });
+}
+
+int mlb_rk_graph_steps(mlb_rk* r, long long* steps)
+{
+    return guard([&] {
+        if (!r || !steps) fail(MLB_EINVAL, "null argument");
+        *steps = r->graph_steps;
     });
 }
 
@@ -5296,6 +5392,7 @@ int mlb_rk_destroy(mlb_rk* r)
 {
     return guard([&] {
         if (!r) return;
+        if (r->exec) cudaGraphExecDestroy(r->exec);
         for (mlb_system* c : r->k) free_system(c);
         delete r;
     });

@@ -230,3 +230,39 @@ def test_adaptive_time_step_matches_oracle(M, kind, tol):
         assert g[2] == pytest.approx(r[2], rel=1e-4, abs=1e-9)
     err = float(np.abs(np.stack(p.g.spinArrays()[:3]) - o.spins()).max())
     assert err < 2e-5, err
+
+
+@pytest.mark.parametrize("kind,llg", [("RK4", "Quaternion"), ("RK2", "Cartesian"), ("RK6", "Quaternion")])
+def test_rk_graph_steps_equal_eager_steps(M, kind, llg):
+    """Steps run as graphs (the same kernels and arguments recorded with their
+    dependent-launch edges) leave the spins, the stage systems' effect and the
+    time exactly as eager steps do, through a parameter change in between
+    (which runs that step eagerly)."""
+    dims = (64, 32, 4)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 72, deg=20.0)
+    res = []
+    for graph in (False, True):
+        ss = M.SpinSystem(*dims)
+        ss.setSpinArrays(*s0)
+        ss.setAlpha(0.05)
+        ss.setTimeStep(0.005)
+        ex = M.Exchange(ss)
+        ex.addPaths(*O.nn_paths(*dims, pbc=(1, 1, 0)))
+        ani = M.Anisotropy(ss)
+        ani.addMany(np.arange(n), np.tile([0, 0, 1.0], (n, 1)), np.full(n, 0.05))
+        z = M.AppliedField(ss)
+        z.set(0.1, 0.0, 0.02)
+        dip = M.Dipole(ss)
+        dip.setStrength(0.03)
+        th = M.Thermal(ss, M.Random.Philox(5))
+        th.setTemperature(0.3)
+        rk = M.RungeKutta(ss, kind, [ex, ani, z, dip], M.LLG.new(llg), temp=th)
+        rk.setGraph(graph)
+        rk.step(5)
+        th.setTemperature(0.2)
+        rk.step(5)
+        res.append((np.stack(ss.spinArrays()[:3]), ss.time(), rk.graphSteps()))
+    np.testing.assert_array_equal(res[0][0], res[1][0])
+    assert res[0][1] == res[1][1]
+    assert res[0][2] == 0 and res[1][2] >= 6, (res[0][2], res[1][2])
