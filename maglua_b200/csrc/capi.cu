@@ -231,9 +231,13 @@ struct mlb_system {
     std::vector<Slot> slots;
     cudaStream_t own = nullptr;
     cudaStream_t st = nullptr;
-    DevStep* dstep = nullptr;       // device step block (captured steps)
-    DevStep dstep_mirror{};         // what the device block holds, when dstep_known
+    // device step blocks of captured steps, one per spin-buffer parity: a
+    // step with parity q reads dstep[q] and writes the next step's values
+    // into dstep[1 - q]
+    DevStep* dstep = nullptr;
+    DevStep dstep_mirror{};         // what dstep[dstep_cur] holds, when dstep_known
     bool dstep_known = false;
+    int dstep_cur = 0;
     // netMoment: reduction + copy to pinned memory captured once per spin
     // buffer (and per length argument m)
     // netMoment: the reduction and its copy to pinned memory captured once per
@@ -1349,13 +1353,13 @@ bool terms_add(TermsK& T, const Term& t, bool th_sub, mlb_system* s, bool captur
         T.th.seed = op->seed;
         // captured steps read the counter from the device step block
         T.th.counter = capture ? 0 : t.counter;
-        T.th.dctr = capture ? &s->dstep->th_counter : nullptr;
+        T.th.dctr = capture ? &s->dstep[s->cur].th_counter : nullptr;
         return true;
     case MLB_OP_APPLIEDFIELD:
         if (T.zee.on) return false;
         T.zee.on = 1;
         for (int a = 0; a < 3; a++) T.zee.B[a] = t.B[a];
-        T.zee.Bdev = capture ? s->dstep->B : nullptr;
+        T.zee.Bdev = capture ? s->dstep[s->cur].B : nullptr;
         return true;
     }
     return false;
@@ -1825,6 +1829,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
     FastK F;
     FastKT<double> Fd;
     bool carried = false;   // SPEC ends holding the new spins' x transform
+    bool advanced = false;  // a kernel of the step wrote the next step's block
     if (s->dry) {
         // bookkeeping only: the kernels of this step ran in a captured graph
     } else if (fast_fused(s, T, l, dt, dt_sys, F)) {
@@ -1846,6 +1851,11 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
             s->pend_si = -1;
             ConvK kx = CP->k;
             kx.tl = s->capturing ? s->cap_tl : nullptr;
+            if (s->capturing) {
+                F.adv_cur = s->dstep + s->cur;
+                F.adv_next = s->dstep + (1 - s->cur);
+                advanced = true;
+            }
             CK(mlb::launch_xstep(kx, CP->L, reinterpret_cast<const float2*>(CP->tw.p),
                                  reinterpret_cast<float2*>(CP->spec.p), F, true, sp, h, out, s->st));
             carried = true;
@@ -1880,7 +1890,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         P.ox = s->sp[nb][0]; P.oy = s->sp[nb][1]; P.oz = s->sp[nb][2];
         CK(mlb::launch_fused(P, dt_sys, s->rb, s->st));
     }
-    if (s->capturing) CK(mlb::launch_advance_step(s->dstep, s->st));
+    if (s->capturing && !advanced) CK(mlb::launch_advance_step(s->dstep + s->cur, s->dstep + (1 - s->cur), s->st));
     if (!carried && !s->capturing && !s->dry) s->spec_token = 0;
     s->cur = nb;
     s->gen++;
@@ -2002,8 +2012,8 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     s->ms_host.assign(n, 0.0);
     s->ms_dirty = true;
     s->ms_token = ++g_ms_token;
-    CK(cudaMalloc(&s->dstep, sizeof(DevStep)));
-    CK(cudaMemset(s->dstep, 0, sizeof(DevStep)));
+    CK(cudaMalloc(&s->dstep, 2 * sizeof(DevStep)));
+    CK(cudaMemset(s->dstep, 0, 2 * sizeof(DevStep)));
     CK(cudaMalloc(&s->status, sizeof(unsigned)));
     CK(cudaMemset(s->status, 0, sizeof(unsigned)));
     CK(cudaMallocHost(&s->nm_host, sizeof(double) * 30));
@@ -2292,12 +2302,13 @@ void plan_launch(mlb_plan* p, int nsteps)
     }
     // upload only what the device block does not already hold (consecutive
     // launches: the steps advanced it exactly as the host mirror below)
-    if (!s->dstep_known || memcmp(&h, &s->dstep_mirror, sizeof(h)) != 0) {
+    if (!s->dstep_known || s->dstep_cur != s->cur || memcmp(&h, &s->dstep_mirror, sizeof(h)) != 0) {
         // (a pageable source is staged before cudaMemcpyAsync returns)
-        CK(cudaMemcpyAsync(s->dstep, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->dstep + s->cur, &h, sizeof(h), cudaMemcpyHostToDevice, s->st));
         s->dstep_mirror = h;
     }
-    // the device advances the block once per step (k_advance_step)
+    // each step writes the next step's block (the fused x pass, or
+    // k_advance_step)
     for (int k = 0; k < nsteps; k++) {
         s->dstep_mirror.th_counter += 1ull;
         for (int a = 0; a < 3; a++) s->dstep_mirror.B[a] += s->dstep_mirror.dB[a];
@@ -2329,6 +2340,7 @@ void plan_launch(mlb_plan* p, int nsteps)
     }
     s->dry = false;
     advance_sweep(p->ops.data(), (int)p->ops.size());
+    s->dstep_cur = s->cur;   // the block the next step reads
 }
 
 // ------------------------------------------------------------------ packed ensembles
@@ -2558,7 +2570,7 @@ void ens_enqueue_step(mlb_ensemble* e, int q)
         for (int q3 = 0; q3 < 3; q3++) add[q3] = e->H[q3];
     }
     CK(mlb::launch_fused_ens(ens_fastk(e), ens_launch(e, q), s, add, o, e->st));
-    CK(mlb::launch_advance_step(e->dstep, e->st));
+    CK(mlb::launch_advance_step(e->dstep, e->dstep, e->st));
 }
 
 // ---------------------------------------------------------------- ensemble tuner

@@ -1071,6 +1071,17 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     pdl_wait();
     unsigned long long* tls = c.tl ? c.tl + 2 : nullptr;
     tl_start(tls);
+    // captured steps: the next step's block (the other of the pair; no
+    // kernel of this step reads it)
+    if (F0.adv_next && blockIdx.x == 0 && threadIdx.x == 0) {
+        const DevStep* cu = F0.adv_cur;
+        DevStep* nx_ = F0.adv_next;
+        nx_->th_counter = cu->th_counter + 1ull;
+        for (int a = 0; a < 3; a++) {
+            nx_->B[a] = cu->B[a] + cu->dB[a];
+            nx_->dB[a] = cu->dB[a];
+        }
+    }
     if (c.run_if && *c.run_if == 0) return;
     // the rows' spins and their z-neighbour rows, into L2 while the inverse
     // transform runs (the step reads them after it)

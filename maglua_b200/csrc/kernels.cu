@@ -375,11 +375,15 @@ __global__ void __launch_bounds__(256) k_llg(SysK from, const void* mx, const vo
 }
 
 // One step of the device step block: next Thermal counter, swept field.
-__global__ void k_advance_step(DevStep* d)
+__global__ void k_advance_step(const DevStep* cur, DevStep* next)
 {
-    pdl_wait();   // the step's kernels read d until they complete
-    d->th_counter += 1ull;
-    for (int a = 0; a < 3; a++) d->B[a] += d->dB[a];
+    pdl_wait();   // the step's kernels read cur until they complete
+    const DevStep c = *cur;
+    next->th_counter = c.th_counter + 1ull;
+    for (int a = 0; a < 3; a++) {
+        next->B[a] = c.B[a] + c.dB[a];
+        next->dB[a] = c.dB[a];
+    }
 }
 
 // FP64 partial sums for netMoment: per block (sum v*m, sum (v*m)^2) x 3.
@@ -1327,9 +1331,9 @@ cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* con
     return cudaGetLastError();
 }
 
-cudaError_t launch_advance_step(DevStep* d, cudaStream_t st)
+cudaError_t launch_advance_step(const DevStep* cur, DevStep* next, cudaStream_t st)
 {
-    return launch_pdl(k_advance_step, dim3(1), dim3(1), 0, st, d);
+    return launch_pdl(k_advance_step, dim3(1), dim3(1), 0, st, cur, next);
 }
 
 cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st)

@@ -177,6 +177,11 @@ struct FastKT {
     int llg_type, tof, renorm, dt_zero;
     R dt, precess, c_prec, c_damp, c_rot, ms;
     unsigned* status;         // bit 0 set when a new spin is not finite (null: not checked)
+    // captured steps of the fused x pass: the step reads adv_cur (through
+    // dctr and Bdev) and the pass writes the next step's block into adv_next
+    // (null: the step block is advanced by a kernel of its own)
+    DevStep* adv_cur;
+    DevStep* adv_next;
 };
 // FP32 state (every fused kernel); FastKT<double> for FP64 state
 typedef FastKT<float> FastK;

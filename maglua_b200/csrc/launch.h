@@ -110,7 +110,7 @@ cudaError_t launch_eval(const SysK& s, const TermsK& T, double dt_sys, void* con
 cudaError_t launch_llg(const SysK& from, const void* const m[3], const void* const H[3], const void* const Ht[3],
                        const void* dsa, const void* dsg, double da, double dg, const LlgK& L,
                        void* const out[3], int rb, cudaStream_t st);
-cudaError_t launch_advance_step(DevStep* d, cudaStream_t st);
+cudaError_t launch_advance_step(const DevStep* cur, DevStep* next, cudaStream_t st);
 cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st);
 // netMoment as one launch (partials, then the last block's fixed-order
 // final sums into pinned host memory and out_dev); counter starts at 0.
