@@ -997,11 +997,15 @@ void build_plan(mlb_op* op, cudaStream_t st, int rb)
     if (k.general) {
         P->ten9.alloc((size_t)k.Kx * Py * Pz * 9 * 2 * rb);
         CK(mlb::launch_tensor_pack9(W.p, Px, Py, Pz, k.Kx, P->ten9.p, rb, k.split, st));
-    } else if (quarter_ok(k, rb) && tensor_has_parities(W.p, k, st)) {
-        // the split FP32 passes read a quarter of the tensor (ky <= Py/2, kz <= Pz/2)
+    } else if ((quarter_ok(k, rb) || (rb == 4 && mlb::yz_col3_ok(k))) && tensor_has_parities(W.p, k, st)) {
+        // the split FP32 passes and the single-CTA-plane (y,z) kernel read a
+        // quarter of the tensor (ky <= Py/2, kz <= Pz/2)
         k.quarter = 1;
-        P->ten6.alloc((size_t)k.Kx * (Py / 2 + 1) * (Pz / 2 + 1) * 6 * rb);
-        CK(mlb::launch_tensor_pack6q(W.p, Px, Py, Pz, k.Kx, reinterpret_cast<float*>(P->ten6.p), st));
+        const size_t q6 = (size_t)(Py / 2 + 1) * (Pz / 2 + 1) * 6;
+        const size_t per_kx = k.split ? q6 : ((q6 + 3) & ~(size_t)3);
+        P->ten6.alloc((size_t)k.Kx * per_kx * rb);
+        CK(cudaMemsetAsync(P->ten6.p, 0, (size_t)k.Kx * per_kx * rb, st));
+        CK(mlb::launch_tensor_pack6q(W.p, Px, Py, Pz, k.Kx, reinterpret_cast<float*>(P->ten6.p), k.split ? 0 : 1, st));
     } else {
         P->ten6.alloc((size_t)k.Kx * Py * Pz * 6 * rb);
         DBuf<double> mi;

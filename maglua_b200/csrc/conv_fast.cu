@@ -501,12 +501,18 @@ struct YZC {
     static size_t smem(int nz) { return ((size_t)3 * PZ * PY + (size_t)3 * nz * EX + PY) * sizeof(float2); }
 };
 
-template <int PY, int PZ>
+// QT: the tensor is stored for ky <= PY/2 and kz <= PZ/2 only (a tensor
+// with the per-axis parities of a point-dipole tensor on an orthogonal
+// lattice: XY and YZ odd in ky, XZ and YZ odd in kz), TEN[kx][kz][ky][6]
+// with a per-kx stride padded to 16 bytes, mirrored with those signs.
+template <int PY, int PZ, bool QT>
 __global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __restrict__ twy,
                                                    float2* __restrict__ spec, const float* __restrict__ ten6)
 {
     using Y = YZC<PY, PZ>;
     constexpr int NT = Y::NT, T = Y::T, E = Y::E;
+    constexpr int QY = PY / 2 + 1, QZ = PZ / 2 + 1;
+    constexpr int KS = QT ? ((QZ * QY * 6 + 3) & ~3) : PZ * PY * 6;   // tensor floats per kx
     extern __shared__ float2 sm[];
     const int kx = blockIdx.x;
     const int nz = c.nz, ny = c.ny;
@@ -514,9 +520,9 @@ __global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __res
     float2* Z = sm;                                  // [3][PZ][PY]
     float2* ex = Z + (size_t)3 * PZ * PY;            // [3 nz][EX]
     float2* twl = ex + (size_t)nlines * Y::EX;       // [PY]
-    const float* Tk = ten6 + (size_t)kx * PZ * PY * 6;
+    const float* Tk = ten6 + (size_t)kx * KS;
     if (threadIdx.x == 0) {
-        const unsigned bytes = (unsigned)(PZ * PY * 6 * sizeof(float));
+        const unsigned bytes = (unsigned)(KS * sizeof(float));
         if ((((uintptr_t)Tk) & 15) == 0 && (bytes & 15) == 0)
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Tk), "r"(bytes) : "memory");
     }
@@ -569,9 +575,21 @@ __global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __res
     for (int q = 0; q < NI; q++) {
         const int item = threadIdx.x + q * NT;
         if (item < PZ * PY) {
-            const float* Tp = Tk + (size_t)item * 6;
+            if (QT) {
+                const int kz = item / PY, ky = item % PY;
+                const int kyq = ky <= PY / 2 ? ky : PY - ky, kzq = kz <= PZ / 2 ? kz : PZ - kz;
+                const float* Tp = Tk + ((size_t)kzq * QY + kyq) * 6;
 #pragma unroll
-            for (int e = 0; e < 6; e++) tt[q][e] = __ldg(Tp + e);
+                for (int e = 0; e < 6; e++) tt[q][e] = __ldg(Tp + e);
+                const float sy = ky > PY / 2 ? -1.f : 1.f, sz = kz > PZ / 2 ? -1.f : 1.f;
+                tt[q][1] *= sy;
+                tt[q][2] *= sz;
+                tt[q][4] *= sy * sz;
+            } else {
+                const float* Tp = Tk + (size_t)item * 6;
+#pragma unroll
+                for (int e = 0; e < 6; e++) tt[q][e] = __ldg(Tp + e);
+            }
         }
     }
 #pragma unroll
@@ -1342,6 +1360,26 @@ cudaError_t launch_split_fast_f64(const ConvK& c, const FftLen L[3], const doubl
     return launch_split_fast<double2>(c, tw + L[1].tw_off, tw + L[2].tw_off, spec, ten6, st);
 }
 
+// The 256-wide single-CTA-plane (y,z) kernel runs this pass (so the pass may
+// read a quarter tensor): FP32 fast path, one system, automatic variant.
+template <int PZ>
+static bool col3_fits(const ConvK& c)
+{
+    return 3 * c.nz <= YZC<256, PZ>::NT / YZC<256, PZ>::T && YZC<256, PZ>::smem(c.nz) <= 227 * 1024;
+}
+bool yz_col3_ok(const ConvK& c)
+{
+    if (c.split || c.general || c.nrep != 1 || c.yz_variant != 0 || c.Py != 256 || !conv_fast_ok(c)) return false;
+    switch (c.Pz) {
+    case 1: return col3_fits<1>(c);
+    case 2: return col3_fits<2>(c);
+    case 4: return col3_fits<4>(c);
+    case 8: return col3_fits<8>(c);
+    case 16: return col3_fits<16>(c);
+    }
+    return false;
+}
+
 bool split_y_fast_ok(const ConvK& c)
 {
     return c.nrep == 1 && c.Py >= 32 && c.Py <= 512 && (c.Py & (c.Py - 1)) == 0;
@@ -1440,10 +1478,16 @@ static cudaError_t launch_yz_t(const ConvK& c, const float2* twy, float2* spec, 
     }
     if constexpr (PY == 256 && PZ <= 16) {
         if (c.yz_variant != 2 && 3 * c.nz <= YZC<PY, PZ>::NT / YZC<PY, PZ>::T &&
-            YZC<PY, PZ>::smem(c.nz) <= 227 * 1024)
-            return launch_pdl(k_yz_col3<PY, PZ>, dim3(c.Kx, c.nrep), dim3(YZC<PY, PZ>::NT), YZC<PY, PZ>::smem(c.nz),
-                              st, c, twy, spec, ten6);
+            YZC<PY, PZ>::smem(c.nz) <= 227 * 1024) {
+            if (c.quarter)
+                return launch_pdl(k_yz_col3<PY, PZ, true>, dim3(c.Kx, c.nrep), dim3(YZC<PY, PZ>::NT),
+                                  YZC<PY, PZ>::smem(c.nz), st, c, twy, spec, ten6);
+            return launch_pdl(k_yz_col3<PY, PZ, false>, dim3(c.Kx, c.nrep), dim3(YZC<PY, PZ>::NT),
+                              YZC<PY, PZ>::smem(c.nz), st, c, twy, spec, ten6);
+        }
     }
+    // a quarter tensor is read by the kernel above only
+    if (c.quarter) return cudaErrorInvalidValue;
     if constexpr (PY >= 256) {
         if (yz_reg_ok(PY, PZ, c))
             return launch_pdl(k_yz_reg<PY, RPZ, 384>, dim3(c.Kx, c.nrep), dim3(384), YZR<PY, RPZ, 384>::smem(c.nz), st,
@@ -1534,11 +1578,16 @@ static cudaError_t cfg_yzc()
 {
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 1>, a, 227 * 1024)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 2>, a, 227 * 1024)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 4>, a, 227 * 1024)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 8>, a, 227 * 1024)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_yz_col3<256, 16>, a, 227 * 1024);
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 1, false>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 2, false>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 4, false>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 8, false>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 16, false>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 1, true>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 2, true>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 4, true>, a, 227 * 1024)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_yz_col3<256, 8, true>, a, 227 * 1024)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_yz_col3<256, 16, true>, a, 227 * 1024);
 }
 
 cudaError_t conv_fast_configure()

@@ -1642,18 +1642,34 @@ __global__ void k_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int 
 }
 
 // Quarter tensor TEN6Q[kx][ky <= Py/2][kz <= Pz/2][q] = Re W_q in FP32.
-__global__ void k_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten)
+// Quarter tensor (ky <= Py/2, kz <= Pz/2): ky-major TEN[kx][ky][kz][6] for the
+// split passes, or (zmaj) TEN[kx][kz][ky][6] with the per-kx stride padded to
+// a multiple of four floats for the single-CTA-plane (y,z) kernel.
+__global__ void k_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, int zmaj)
 {
     const int Qy = Py / 2 + 1, Qz = Pz / 2 + 1;
     const long long total = (long long)Kx * Qy * Qz;
     const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= total) return;
-    const int kz = (int)(e % Qz);
-    const long long r = e / Qz;
-    const int ky = (int)(r % Qy), kx = (int)(r / Qy);
+    int kx, ky, kz;
+    size_t o;
+    if (zmaj) {
+        ky = (int)(e % Qy);
+        const long long r = e / Qy;
+        kz = (int)(r % Qz);
+        kx = (int)(r / Qz);
+        const size_t ks = ((size_t)Qz * Qy * 6 + 3) & ~(size_t)3;
+        o = (size_t)kx * ks + ((size_t)kz * Qy + ky) * 6;
+    } else {
+        kz = (int)(e % Qz);
+        const long long r = e / Qz;
+        ky = (int)(r % Qy);
+        kx = (int)(r / Qy);
+        o = (size_t)e * 6;
+    }
     const size_t plane = (size_t)Px * Py * Pz;
     const size_t off = ((size_t)kz * Py + ky) * Px + kx;
-    for (int q = 0; q < 6; q++) ten[e * 6 + q] = (float)W[q * plane + off].x;
+    for (int q = 0; q < 6; q++) ten[o + q] = (float)W[q * plane + off].x;
 }
 
 cudaError_t launch_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int Kx, unsigned long long* out3,
@@ -1665,10 +1681,11 @@ cudaError_t launch_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, cudaStream_t st)
+cudaError_t launch_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, int zmaj,
+                                cudaStream_t st)
 {
     const long long total = (long long)Kx * (Py / 2 + 1) * (Pz / 2 + 1);
-    k_tensor_pack6q<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten);
+    k_tensor_pack6q<<<blocks_for(total, 256), 256, 0, st>>>(W, Px, Py, Pz, Kx, ten, zmaj);
     return cudaGetLastError();
 }
 

@@ -63,6 +63,8 @@ struct Prof {
 cudaError_t fftreg_init();
 cudaError_t conv_fast_configure();
 bool conv_fast_ok(const ConvK& c);
+// the 256-wide single-CTA-plane (y,z) kernel runs this pass (it can read a quarter tensor)
+bool yz_col3_ok(const ConvK& c);
 // FP32 x passes alone (power-of-two periodic x, 16..512): the forward
 // transform of the spins to SPEC (fwd) or the inverse to the field h.
 bool x_fast_ok(const ConvK& c);
@@ -152,7 +154,8 @@ cudaError_t launch_fft3d_d(double2* W, int ncomp, int Px, int Py, int Pz, const 
 // and the FP32 quarter tensor of the split passes (ConvK::quarter).
 cudaError_t launch_tensor_symcheck(const double2* W, int Px, int Py, int Pz, int Kx, unsigned long long* out3,
                                    cudaStream_t st);
-cudaError_t launch_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, cudaStream_t st);
+cudaError_t launch_tensor_pack6q(const double2* W, int Px, int Py, int Pz, int Kx, float* ten, int zmaj,
+                                cudaStream_t st);
 cudaError_t launch_tensor_pack6(const double2* W, int Px, int Py, int Pz, int Kx, void* ten6, double* maxim,
                                 int rb, int kmaj, cudaStream_t st);
 cudaError_t launch_tensor_pack9(const double2* W, int Px, int Py, int Pz, int Kx, void* ten9, int rb, int kmaj,
