@@ -60,39 +60,46 @@ struct XCfg {
     static constexpr int LINE = L * PX;                        // line buffer
     static constexpr int SPEC = ROWS * KX;                     // [ROWS][KX] staging
     static constexpr int BUF = LINE > SPEC ? LINE : SPEC;      // each of A, B
-    // FP32 256-point lines use the register four-step transform, with
-    // one exchange buffer per line after the two line buffers
-    static constexpr int EX = PX == 256 ? L * 16 * 17 : 0;
+    // FP32 lines of 32 to 256 points use the register four-step
+    // transform, with one exchange buffer per line after the two line buffers
+    static constexpr int EX = (PX >= 32 && PX <= 256) ? L * fr::Split<PX>::E * (fr::Split<PX>::T + 1) : 0;
     static constexpr int SMEM = (PX + 2 * BUF + EX) * 8;       // bytes (FP32)
     static constexpr int SMEM_D = (PX + 2 * BUF) * 16;         // bytes (FP64)
 };
 
-// 256-point FP32 lines: the four-step register FFT of fr::line_fft (16
-// lanes x 16 points, one warp-synchronous exchange through ex, 16 x 17
-// elements per line), in place on a natural-order line: the lanes have
-// read the whole line before any of them writes it back.
-constexpr int X256_EX = 16 * 17;
-template <int SIGN>
-__device__ __forceinline__ void x256_line(float2* line, float2* ex, int t, unsigned mask, const float2* tw)
+// FP32 x lines of 32 to 256 points: the four-step register FFT of
+// fr::line_fft (Split<N>::T lanes x Split<N>::E points, one warp-synchronous
+// exchange through ex, E (T + 1) elements per line), in place on a
+// natural-order line: the lanes have read the whole line before any of them
+// writes it back.
+template <int N>
+struct XReg {
+    static constexpr bool OK = N >= 32 && N <= 256;
+    static constexpr int T = fr::Split<N>::T, E = fr::Split<N>::E, EX = E * (T + 1);
+};
+template <int N, int SIGN>
+__device__ __forceinline__ void xreg_line(float2* line, float2* ex, int t, unsigned mask, const float2* tw)
 {
-    float2 v[16];
+    constexpr int T = XReg<N>::T, E = XReg<N>::E;
+    float2 v[E];
 #pragma unroll
-    for (int j = 0; j < 16; j++) v[j] = line[t + 16 * j];
-    fr::line_fft<256, SIGN, float2>(v, ex, t, mask, tw);
+    for (int j = 0; j < E; j++) v[j] = line[t + T * j];
+    fr::line_fft<N, SIGN, float2>(v, ex, t, mask, tw);
 #pragma unroll
-    for (int r = 0; r < 16; r++) line[fr::out_index<256>(t, r)] = v[r];
+    for (int r = 0; r < E; r++) line[fr::out_index<N>(t, r)] = v[r];
 }
 
 // The CTA's nl lines (line l at base + l ls) in place, line l by threads
-// 16 l .. 16 l + 15.  Every thread of the CTA calls this; the CTA is
+// T l .. T l + T - 1.  Every thread of the CTA calls this; the CTA is
 // synchronised after the transforms.
-template <int SIGN>
-__device__ __forceinline__ void x256_lines(float2* base, int ls, int nl, float2* ex, const float2* tw)
+template <int N, int SIGN>
+__device__ __forceinline__ void xreg_lines(float2* base, int ls, int nl, float2* ex, const float2* tw)
 {
-    const int l = threadIdx.x >> 4, t = threadIdx.x & 15;
+    constexpr int T = XReg<N>::T;
+    const int l = threadIdx.x / T, t = threadIdx.x % T;
     if (l < nl) {
-        const unsigned mask = 0xffffu << (threadIdx.x & 16);
-        x256_line<SIGN>(base + (size_t)l * ls, ex + (size_t)l * X256_EX, t, mask, tw);
+        const unsigned mask = ((1u << T) - 1u) << ((threadIdx.x & 31) & ~(T - 1));
+        xreg_line<N, SIGN>(base + (size_t)l * ls, ex + (size_t)l * XReg<N>::EX, t, mask, tw);
     }
     __syncthreads();
 }
@@ -141,8 +148,8 @@ __global__ void __launch_bounds__(256) k_fx_fast(ConvK c, const typename CT<R>::
     }
     __syncthreads();
     const C* Rl;
-    if constexpr (PX == 256 && sizeof(R) == 4) {
-        x256_lines<-1>(A, PX, X::L, B + X::BUF, twl);
+    if constexpr (XReg<PX>::OK && sizeof(R) == 4) {
+        xreg_lines<PX, -1>(A, PX, X::L, B + X::BUF, twl);
         Rl = A;
     } else {
         const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
@@ -223,8 +230,8 @@ __global__ void __launch_bounds__(256) k_ix_fast(ConvK c, const typename CT<R>::
     }
     __syncthreads();
     const C* Rl;
-    if constexpr (PX == 256 && sizeof(R) == 4) {
-        x256_lines<+1>(A, PX, X::L, B + X::BUF, twl);
+    if constexpr (XReg<PX>::OK && sizeof(R) == 4) {
+        xreg_lines<PX, +1>(A, PX, X::L, B + X::BUF, twl);
         Rl = A;
     } else {
         const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
@@ -1058,8 +1065,8 @@ struct XSCfg {
     // flight, [3][ROWS][PX] floats (where two CTAs per SM still fit)
     static constexpr bool PRE = TH && PX <= 256;
     static constexpr int NOISE = PRE ? 3 * ROWS * PX : 0;
-    // 256-point lines: register four-step transforms, one exchange buffer per line
-    static constexpr int EX = PX == 256 ? L * X256_EX : 0;
+    // 32- to 256-point lines: register four-step transforms, one exchange buffer per line
+    static constexpr int EX = XReg<PX>::OK ? L * XReg<PX>::EX : 0;
     static constexpr int SMEM = (PX + 2 * BUF + EX) * 8 + NOISE * 4;
     static_assert(L % 3 == 0 && ROWS % 2 == 0, "line layout");
 };
@@ -1078,7 +1085,7 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     float2* twl = sm;               // [PX]
     float2* A = twl + PX;           // [L][LS] lines
     float2* B = A + X::BUF;         // [L][LS] scratch
-    float2* EXB = B + X::BUF;       // [L][16 * 17] exchange buffers (PX = 256)
+    float2* EXB = B + X::BUF;       // [L][XReg<PX>::EX] exchange buffers (XReg<PX>::OK)
     float* noise = reinterpret_cast<float*>(EXB + X::EX);   // [3][ROWS][PX] (X::PRE)
     const int nx = c.nx, ny = c.ny, nz = c.nz;
     const int nr = nz * ny;                     // rows (z, y), flattened
@@ -1178,8 +1185,8 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     __syncthreads();
     const int l = threadIdx.x / X::TPL, tl = threadIdx.x % X::TPL;
     const float2* R;
-    if constexpr (PX == 256) {
-        x256_lines<+1>(A, LS, X::L, EXB, twl);
+    if constexpr (XReg<PX>::OK) {
+        xreg_lines<PX, +1>(A, LS, X::L, EXB, twl);
         R = A;
     } else {
         R = fr::sm_fft<PX, +1, X::TPL, float2, LS>(A, B, l, tl, twl, true);
@@ -1226,8 +1233,8 @@ __global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, co
     __syncthreads();
     // 3. forward transform of the new spins' lines, split into the two rows
     const float2* Q;
-    if constexpr (PX == 256) {
-        x256_lines<-1>(W, LS, X::L, EXB, twl);
+    if constexpr (XReg<PX>::OK) {
+        xreg_lines<PX, -1>(W, LS, X::L, EXB, twl);
         Q = W;
     } else {
         Q = fr::sm_fft<PX, -1, X::TPL, float2, LS>(W, const_cast<float2*>(R), l, tl, twl, true);
