@@ -1995,6 +1995,26 @@ void spins_changing(mlb_system* s)
     s->spec_token = 0;
 }
 
+// A write of the current spin buffer alone (moment magnitudes and site
+// arrays kept): only the records that read that buffer (the current
+// generation) are settled; those of the previous generation read the other
+// buffer, which the write leaves as it is.
+void current_spins_changing(mlb_system* s)
+{
+    flush_pending(s);
+    auto reads_current = [&](const Slot& x) { return x.state == ST_LAZY && x.gen == s->gen; };
+    for (size_t j = 0; j < s->slots.size(); j++) {
+        if (s->slots[j].state != ST_SUM) continue;
+        bool cur = false;
+        for (int m : s->slots[j].sum_list)
+            if (reads_current(s->slots[m])) cur = true;
+        if (cur) materialize(s, (int)j);
+    }
+    for (size_t j = 0; j < s->slots.size(); j++)
+        if (reads_current(s->slots[j])) materialize(s, (int)j);
+    s->spec_token = 0;
+}
+
 mlb_system* make_system(int nx, int ny, int nz, int rb)
 {
     if (rb != 4 && rb != 8) fail(MLB_EINVAL, "bytes per real must be 4 or 8");
@@ -2980,8 +3000,12 @@ int mlb_system_upload_f32(mlb_system* s, const float* x, const float* y, const f
         // captured steps hold device pointers and the moment magnitudes'
         // constants, not spin values: a write of the spins alone keeps them
         // (the carried spectrum and lazy records are settled below)
-        if (ms) g_version++;
-        spins_changing(s);
+        if (ms) {
+            g_version++;
+            spins_changing(s);
+        } else {
+            current_spins_changing(s);
+        }
         const float* src[3] = {x, y, z};
         if (s->rb == 4) {
             for (int c = 0; c < 3; c++)

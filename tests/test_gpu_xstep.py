@@ -306,3 +306,27 @@ def test_device_timeline_plan(M):
             with pytest.raises(M.MagLuaError):
                 p.deviceTimes()
     assert_same(out[0], out[1])
+
+
+def test_fields_after_spin_upload_are_the_steps_fields(M):
+    """The fields of the last step (lazy records of the previous spin
+    generation) read after a spins-only FP32 upload are, bit for bit, those
+    read before it: the upload overwrites the current spin buffer only."""
+    dims = (64, 32, 4)
+    n = int(np.prod(dims))
+    s0 = tilted_spins(n, 53, deg=25.0)
+    s1 = tilted_spins(n, 54, deg=35.0).astype(np.float32)
+    names = ("Total", "Exchange", "Anisotropy", "Thermal", "Dipole")
+    out = []
+    for upload in (False, True):
+        ss, ops, l = build(M, dims, s0, llg="Quaternion", T=0.4)
+        ss.setSpinArrays(*s0, np.ones(n))
+        p = M.Plan(ss, ops, l)
+        p.launch(3)
+        if upload:
+            ss.uploadF32(*[np.ascontiguousarray(s1[c]) for c in range(3)])
+        out.append([np.stack(ss.fieldArrays(nm)) for nm in names])
+        if upload:
+            np.testing.assert_array_equal(np.stack(ss.spinArrays()[:3]), s1.astype(np.float64))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
