@@ -254,6 +254,18 @@ struct mlb_system {
     double* red = nullptr;
     double* redout = nullptr;
     int red_nb = 1;
+    // mlb_system_netmoment_async runs on a stream of its own (its own
+    // partial sums and counter), concurrently with the next steps; slot k
+    // reads spin buffer nm_buf[k] until nm_ev[k], and nm_reading[k] stays set
+    // until the system's stream has been made to wait for it before a write
+    // of that buffer
+    cudaStream_t nm_st = nullptr;
+    cudaEvent_t nm_go[4] = {};
+    int nm_buf[4] = {};
+    bool nm_reading[4] = {};
+    double* red_a = nullptr;
+    double* redout_a = nullptr;
+    unsigned* nm_counter_a = nullptr;
     bool capturing = false;
     bool dry = false;               // replay host bookkeeping without launching
     // a system the library owns and never shows to the caller (Runge-Kutta
@@ -364,6 +376,8 @@ struct mlb_plan {
 };
 
 namespace {
+
+void nm_guard(mlb_system* s, int q);
 
 std::set<mlb_system*> g_systems;
 unsigned long long g_ms_token = 0;
@@ -1830,6 +1844,7 @@ bool llg_fused(mlb_llg* l, mlb_system* s, double dt)
         }
     }
     const int nb = 1 - s->cur;
+    if (!s->dry) nm_guard(s, nb);
     FastK F;
     FastKT<double> Fd;
     bool carried = false;   // SPEC ends holding the new spins' x transform
@@ -1951,6 +1966,7 @@ void llg_apply(mlb_llg* l, mlb_system* from, double scale, mlb_system* dmdt, mlb
         const void* Ht[3] = {nullptr, nullptr, nullptr};
         if (th >= 0) for (int c = 0; c < 3; c++) Ht[c] = dmdt->slots[th].h[c];
         void* out[3] = {to->sp[to->cur][0], to->sp[to->cur][1], to->sp[to->cur][2]};
+        nm_guard(to, to->cur);
         CK(mlb::launch_llg(sysk(from, from->cur), m, H, Ht, dmdt->sa, dmdt->sg, dmdt->alpha, dmdt->gamma,
                            llgk(l, dt, to->status), out, to->rb, to->st));
     }
@@ -1987,9 +2003,22 @@ void reset_fields(mlb_system* s)
     }
 }
 
+// Before the system's stream writes spin buffer q (q < 0: either buffer):
+// the stream waits for the side-stream netMoment reads of that buffer.
+void nm_guard(mlb_system* s, int q)
+{
+    if (s->capturing) return;   // a captured step is guarded where its graph is launched
+    for (int k = 0; k < 4; k++)
+        if (s->nm_reading[k] && (q < 0 || s->nm_buf[k] == q)) {
+            CK(cudaStreamWaitEvent(s->st, s->nm_ev[k], 0));
+            s->nm_reading[k] = false;
+        }
+}
+
 void spins_changing(mlb_system* s)
 {
     // lazy records read the current buffer, which is about to change
+    nm_guard(s, -1);
     flush_pending(s);
     materialize_all(s);
     s->spec_token = 0;
@@ -2001,6 +2030,7 @@ void spins_changing(mlb_system* s)
 // buffer, which the write leaves as it is.
 void current_spins_changing(mlb_system* s)
 {
+    nm_guard(s, s->cur);
     flush_pending(s);
     auto reads_current = [&](const Slot& x) { return x.state == ST_LAZY && x.gen == s->gen; };
     for (size_t j = 0; j < s->slots.size(); j++) {
@@ -2049,6 +2079,10 @@ mlb_system* make_system(int nx, int ny, int nz, int rb)
     s->red_nb = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
     CK(cudaMalloc(&s->red, sizeof(double) * 6 * s->red_nb));
     CK(cudaMalloc(&s->redout, sizeof(double) * 8));
+    CK(cudaMalloc(&s->red_a, sizeof(double) * 6 * s->red_nb));
+    CK(cudaMalloc(&s->redout_a, sizeof(double) * 8));
+    CK(cudaMalloc(&s->nm_counter_a, sizeof(unsigned)));
+    CK(cudaMemset(s->nm_counter_a, 0, sizeof(unsigned)));
     slot_register(s.get(), "Total");
     mlb_system* r = s.release();
     g_systems.insert(r);
@@ -2070,12 +2104,19 @@ void free_system(mlb_system* s)
     for (int q = 0; q < 2; q++)
         for (int d = 0; d < 5; d++)
             if (s->nm_exec[q][d]) cudaGraphExecDestroy(s->nm_exec[q][d]);
-    for (int k = 0; k < 4; k++)
+    if (s->nm_st) cudaStreamSynchronize(s->nm_st);
+    for (int k = 0; k < 4; k++) {
         if (s->nm_ev[k]) cudaEventDestroy(s->nm_ev[k]);
+        if (s->nm_go[k]) cudaEventDestroy(s->nm_go[k]);
+    }
+    if (s->nm_st) cudaStreamDestroy(s->nm_st);
     cudaFreeHost(s->nm_host);
     cudaFree(s->nm_counter);
     cudaFree(s->red);
     cudaFree(s->redout);
+    cudaFree(s->nm_counter_a);
+    cudaFree(s->red_a);
+    cudaFree(s->redout_a);
     for (Slot& x : s->slots)
         for (int c = 0; c < 3; c++) cudaFree(x.h[c]);
     if (s->own) cudaStreamDestroy(s->own);
@@ -2239,6 +2280,7 @@ void plan_capture(mlb_plan* p)
     for (mlb_op* o : p->ops) { nth += o->kind == MLB_OP_THERMAL; nz += o->kind == MLB_OP_APPLIEDFIELD; }
     if (nth > 1 || nz > 1) fail(MLB_ESTATE, "a captured step holds at most one Thermal and one AppliedField");
     plan_release(p);
+    nm_guard(s, -1);
     const HostState h0 = save_state(s, p->ops);
     try {
         s->dry = true;
@@ -2342,6 +2384,7 @@ void plan_launch(mlb_plan* p, int nsteps)
     for (int k = 0; k < nsteps; k++) {
         const bool carry = CP && s->spec_token != 0 && s->spec_token == CP->spec_token;
         const int gi = s->cur + (carry ? 2 : 0);
+        nm_guard(s, 1 - s->cur);   // the step writes the other spin buffer
         CK(cudaGraphLaunch(p->exec[gi], s->st));
         p->last = &p->ev[gi];
         if (CP) {
@@ -3201,17 +3244,23 @@ int mlb_system_ensure_slot(mlb_system* s, const char* slot)
 // The netMoment reduction of the current spins with its copy to pinned
 // destination d (6 doubles at nm_host + 6 d), enqueued on the system's stream
 // as one captured graph per spin buffer and destination.
-static void netmoment_enqueue(mlb_system* s, double m, int d)
+static void netmoment_enqueue(mlb_system* s, double m, int d, cudaStream_t st)
 {
     const int q = s->cur;
+    // the synchronous read (d = 0) and the slots (on their own stream) use
+    // separate partial sums and counters
+    double* red = d ? s->red_a : s->red;
+    double* redout = d ? s->redout_a : s->redout;
+    unsigned* counter = d ? s->nm_counter_a : s->nm_counter;
     if (!s->nm_exec[q][d] || s->nm_m[q][d] != m) {
         if (s->nm_exec[q][d]) { cudaGraphExecDestroy(s->nm_exec[q][d]); s->nm_exec[q][d] = nullptr; }
         CK(cudaStreamSynchronize(s->st));
+        if (s->nm_st) CK(cudaStreamSynchronize(s->nm_st));
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
         // one kernel: the last block writes the sums into the pinned slot
-        cudaError_t e = mlb::launch_netmoment_one(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, s->red,
-                                                  std::min(s->red_nb, 2 * 148), s->nm_counter, s->nm_host_dev + 6 * d, s->redout, s->rb,
+        cudaError_t e = mlb::launch_netmoment_one(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, red,
+                                                  std::min(s->red_nb, 2 * 148), counter, s->nm_host_dev + 6 * d, redout, s->rb,
                                                   s->st);
         cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
         if (e == cudaSuccess) e = e2;
@@ -3223,7 +3272,7 @@ static void netmoment_enqueue(mlb_system* s, double m, int d)
         }
         s->nm_m[q][d] = m;
     }
-    CK(cudaGraphLaunch(s->nm_exec[q][d], s->st));
+    CK(cudaGraphLaunch(s->nm_exec[q][d], st));
 }
 
 static void netmoment_out(const double* r, double out8[8])
@@ -3237,7 +3286,7 @@ static void netmoment_out(const double* r, double out8[8])
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8])
 {
     return guard([&] {
-        netmoment_enqueue(s, m, 0);
+        netmoment_enqueue(s, m, 0, s->st);
         CK(cudaStreamSynchronize(s->st));
         double r[6];
         for (int k = 0; k < 6; k++) r[k] = s->nm_host[k];
@@ -3249,9 +3298,23 @@ int mlb_system_netmoment_async(mlb_system* s, double m, int slot)
 {
     return guard([&] {
         if (slot < 0 || slot > 3) fail(MLB_EINVAL, "netMoment slot must be 0..3");
+        if (!s->nm_st) CK(cudaStreamCreateWithFlags(&s->nm_st, cudaStreamNonBlocking));
         if (!s->nm_ev[slot]) CK(cudaEventCreateWithFlags(&s->nm_ev[slot], cudaEventDisableTiming));
-        netmoment_enqueue(s, m, 1 + slot);
-        CK(cudaEventRecord(s->nm_ev[slot], s->st));
+        if (!s->nm_go[slot]) CK(cudaEventCreateWithFlags(&s->nm_go[slot], cudaEventDisableTiming));
+        // a slot still reading a buffer: the system's stream waits for it
+        // before anything later, as before this call reused it
+        if (s->nm_reading[slot]) {
+            CK(cudaStreamWaitEvent(s->st, s->nm_ev[slot], 0));
+            s->nm_reading[slot] = false;
+        }
+        // the reduction of the current spins runs on the side stream once
+        // the system's stream has produced them, next to the following steps
+        CK(cudaEventRecord(s->nm_go[slot], s->st));
+        CK(cudaStreamWaitEvent(s->nm_st, s->nm_go[slot], 0));
+        netmoment_enqueue(s, m, 1 + slot, s->nm_st);
+        CK(cudaEventRecord(s->nm_ev[slot], s->nm_st));
+        s->nm_buf[slot] = s->cur;
+        s->nm_reading[slot] = true;
         s->nm_pending[slot] = true;
     });
 }
@@ -5306,6 +5369,7 @@ void rk_step_graph(mlb_rk* r)
     for (mlb_system* c : r->k) sys.push_back(c);
     std::vector<HostState> saved;
     for (mlb_system* x : sys) saved.push_back(save_state(x, all));
+    for (mlb_system* x : sys) nm_guard(x, -1);   // no waits on outside events inside the capture
     cudaStream_t st = ss->st;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
