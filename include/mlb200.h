@@ -122,9 +122,12 @@ int mlb_system_ensure_slot(mlb_system* s, const char* slot);          /* _ensure
 int mlb_system_netmoment(mlb_system* s, double m, double out8[8]);
 /* B200 extension (no reference counterpart): netMoment without waiting.
  * _async enqueues the reduction of the current spins and its copy into
- * pinned slot 0..3 on the system's stream and returns; _wait blocks until
- * that slot's copy has landed and fills out8 as mlb_system_netmoment does.
- * A caller can launch the next step before reading this step's result. */
+ * pinned slot 0..3 and returns: the reduction waits for the work already on
+ * the system's stream and runs on a stream of its own, next to the steps
+ * enqueued after it (the system's stream waits for it before it next writes
+ * the spin buffer it reads); _wait blocks until that slot's copy has landed
+ * and fills out8 as mlb_system_netmoment does.  A caller can launch the
+ * next steps before reading this step's result. */
 int mlb_system_netmoment_async(mlb_system* s, double m, int slot);
 int mlb_system_netmoment_wait(mlb_system* s, int slot, double out8[8]);
 /* sum_i s_i . h_slot,i in FP64 (the fieldArray:dot(spinArray) energy pattern). */
