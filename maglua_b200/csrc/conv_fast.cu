@@ -1047,11 +1047,16 @@ __global__ void __launch_bounds__(256) k_fused_fast(FastKT<R> F0, const R* __res
 // The spectrum rows a CTA reads in 1 and writes in 3 are its own.  Every
 // arithmetic step repeats k_ix_fast, fused_site and k_fx_fast operation for
 // operation, so the result is bitwise that of the three separate kernels.
+// 32- to 256-point lines (register transforms, a line per T-lane group)
+// take 512 threads: the transforms occupy the same L T lanes, and the site
+// step has two items per thread (384 threads left a third of them idle in
+// the last of three rounds); two CTAs per SM at 64 registers.  512-point
+// lines (shared-memory Stockham, TPL threads per line) take 384.
 template <int PX, bool TH = false>
 struct XSCfg {
-    static constexpr int NT = 384;
+    static constexpr int NT = XReg<PX>::OK ? 512 : 384;
     static constexpr int TPL = fr::Tpl<PX>::V;
-    static constexpr int L = NT / TPL;                 // complex lines = 3 ROWS / 2
+    static constexpr int L = 384 / TPL;                 // complex lines = 3 ROWS / 2
     static constexpr int ROWS = 2 * L / 3;
     static constexpr int R2 = ROWS / 2;
     static constexpr int KX = PX / 2 + 1;
@@ -1069,10 +1074,11 @@ struct XSCfg {
     static constexpr int EX = XReg<PX>::OK ? L * XReg<PX>::EX : 0;
     static constexpr int SMEM = (PX + 2 * BUF + EX) * 8 + NOISE * 4;
     static_assert(L % 3 == 0 && ROWS % 2 == 0, "line layout");
+    static_assert(XReg<PX>::OK ? L * XReg<PX>::T <= NT : L * TPL == NT, "lines per CTA");
 };
 
 template <int PX, int LT, bool EXS, bool ANI, bool TH>
-__global__ void __launch_bounds__(384, 2) k_xstep(ConvK c, FastK F0, int fwd, const float2* __restrict__ tw,
+__global__ void __launch_bounds__(XSCfg<PX, TH>::NT, 2) k_xstep(ConvK c, FastK F0, int fwd, const float2* __restrict__ tw,
                                                   float2* __restrict__ spec, const float* __restrict__ sx,
                                                   const float* __restrict__ sy, const float* __restrict__ sz,
                                                   float* __restrict__ hx, float* __restrict__ hy,
