@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
 }
 
 // ------------------------------------------------------------------ (y,z) pass, three threads per column
-// The register form for a film's 256-wide planes with 768 threads per kx:
+// The register form for a film's 256-wide planes with 1024 threads per kx:
 // the y transforms as in k_yz_reg (line l = (comp, z) stored at
 // Z[comp][z][ky]); the column work split three ways so that no thread holds
 // all three components: (a) one thread per (comp, ky) takes the z transform
@@ -497,11 +497,11 @@ __global__ void __launch_bounds__(NTH, NTH >= 384 ? 1 : 4) k_yz_reg(ConvK c, con
 // place (Z[comp][kz][ky]); (b) one thread per (kz, ky) applies the 3x3 real
 // tensor in place; (c) one thread per (comp, ky) takes the inverse z
 // transform and writes the data layers back.  The same operations as
-// k_yz_reg, element for element, at a third of its registers per thread,
-// so twice the warps per SM.
+// k_yz_reg, element for element, at 64 registers per thread, so more than
+// twice the warps per SM.
 template <int PY, int PZ>
 struct YZC {
-    static constexpr int NT = 768;
+    static constexpr int NT = 1024;   // four tensor items per thread (768 left a third of the sixth round busy)
     static constexpr int T = fr::Split<PY>::T;
     static constexpr int E = fr::Split<PY>::E;
     static constexpr int EX = E * (T + 1);              // exchange elements per line
@@ -513,7 +513,7 @@ struct YZC {
 // lattice: XY and YZ odd in ky, XZ and YZ odd in kz), TEN[kx][kz][ky][6]
 // with a per-kx stride padded to 16 bytes, mirrored with those signs.
 template <int PY, int PZ, bool QT>
-__global__ void __launch_bounds__(768, 1) k_yz_col3(ConvK c, const float2* __restrict__ twy,
+__global__ void __launch_bounds__(YZC<PY, PZ>::NT, 1) k_yz_col3(ConvK c, const float2* __restrict__ twy,
                                                    float2* __restrict__ spec, const float* __restrict__ ten6)
 {
     using Y = YZC<PY, PZ>;
