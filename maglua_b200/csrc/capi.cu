@@ -3259,9 +3259,10 @@ static void netmoment_enqueue(mlb_system* s, double m, int d, cudaStream_t st)
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
         // one kernel: the last block writes the sums into the pinned slot
-        cudaError_t e = mlb::launch_netmoment_one(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, red,
-                                                  std::min(s->red_nb, 2 * 148), counter, s->nm_host_dev + 6 * d, redout, s->rb,
-                                                  s->st);
+        // the slots' reads (d > 0) run on a few SMs next to the following steps
+        const int nb = std::min(s->red_nb, mlb::netmoment_blocks(s->n, d > 0));
+        cudaError_t e = mlb::launch_netmoment_one(s->sp[q][0], s->sp[q][1], s->sp[q][2], s->n, m, red, nb, counter,
+                                                  s->nm_host_dev + 6 * d, redout, s->rb, s->st);
         cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess) e = cudaGraphInstantiate(&s->nm_exec[q][d], g, 0);

@@ -420,9 +420,11 @@ __global__ void __launch_bounds__(256) k_netmoment_partial(const void* x_, const
 // k_netmoment_partial does; the last block to finish (a device counter,
 // reset for the next launch) reduces them, one warp per quantity in a fixed
 // order, and writes the six results to out (pinned host memory the device
-// reaches directly) and out_dev.
+// reaches directly) and out_dev.  NMT = 1024 threads per block, so that a
+// few blocks keep enough loads in flight (launch_netmoment_one).
+constexpr int NMT = 1024;
 template <typename R>
-__global__ void __launch_bounds__(256) k_netmoment_one(const void* x_, const void* y_, const void* z_, int n,
+__global__ void __launch_bounds__(NMT) k_netmoment_one(const void* x_, const void* y_, const void* z_, int n,
                                                        double m, double* part, unsigned* counter, double* out,
                                                        double* out_dev)
 {
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(256) k_netmoment_one(const void* x_, const voi
             acc[3] += a * a; acc[4] += b * b; acc[5] += c * c;
         }
     }
-    __shared__ double sh[6][8];
+    __shared__ double sh[6][NMT / 32];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -489,13 +491,23 @@ __global__ void __launch_bounds__(256) k_netmoment_one(const void* x_, const voi
 }
 
 namespace mlb {
+// side = false (a synchronous read): enough blocks of NMT threads for one
+// round of 8 sites each (at most 2 x 148); side = true (a read on its own
+// stream next to the following steps, whose kernels take whole SMs): at most
+// 16 blocks, so that most SMs stay free for the steps.  part holds nb x 6.
+int netmoment_blocks(int n, bool side)
+{
+    const int full = std::max(1, std::min(2 * 148, (n + 8 * NMT - 1) / (8 * NMT)));
+    return side ? std::max(1, std::min(16, (n + NMT - 1) / NMT)) : full;
+}
+
 cudaError_t launch_netmoment_one(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
                                  unsigned* counter, double* out_host, double* out_dev, int rb, cudaStream_t st)
 {
     if (rb == 8)
-        k_netmoment_one<double><<<nb, 256, 0, st>>>(x, y, z, n, m, part, counter, out_host, out_dev);
+        k_netmoment_one<double><<<nb, NMT, 0, st>>>(x, y, z, n, m, part, counter, out_host, out_dev);
     else
-        k_netmoment_one<float><<<nb, 256, 0, st>>>(x, y, z, n, m, part, counter, out_host, out_dev);
+        k_netmoment_one<float><<<nb, NMT, 0, st>>>(x, y, z, n, m, part, counter, out_host, out_dev);
     return cudaGetLastError();
 }
 } // namespace mlb

@@ -116,6 +116,8 @@ cudaError_t launch_advance_step(const DevStep* cur, DevStep* next, cudaStream_t 
 cudaError_t launch_partial_final(const double* part, int nb, int nq, double* out, cudaStream_t st);
 // netMoment as one launch (partials, then the last block's fixed-order
 // final sums into pinned host memory and out_dev); counter starts at 0.
+// blocks of a netMoment read of n sites: a synchronous read, or one on a side stream
+int netmoment_blocks(int n, bool side);
 cudaError_t launch_netmoment_one(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,
                                  unsigned* counter, double* out_host, double* out_dev, int rb, cudaStream_t st);
 cudaError_t launch_netmoment(const void* x, const void* y, const void* z, int n, double m, double* part, int nb,

@@ -336,7 +336,8 @@ def test_async_net_moment_overlapping_steps(M):
     """netMomentAsync runs on a stream of its own next to the following steps
     (the next step writes the other spin buffer; the one after waits for the
     read): every step's moment equals the synchronous netMoment of the same
-    step, bit for bit, and the trajectory is unchanged."""
+    step (up to the order of the FP64 additions: the side read runs on fewer
+    blocks), and the trajectory is unchanged bit for bit."""
     dims = (128, 64, 4)
     n = int(np.prod(dims))
     s0 = tilted_spins(n, 55, deg=30.0)
@@ -359,5 +360,5 @@ def test_async_net_moment_overlapping_steps(M):
                 got.append(ss.netMomentWait(k % 4))
         moments.append(np.array(got))
         spins.append(np.stack(ss.spinArrays()[:3]))
-    np.testing.assert_array_equal(moments[0], moments[1])
+    np.testing.assert_allclose(moments[0], moments[1], rtol=1e-13, atol=1e-12)
     np.testing.assert_array_equal(spins[0], spins[1])
