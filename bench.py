@@ -347,6 +347,145 @@ def run_surrogate(M, torch, steps, train_runs=8, train_steps=250):
     return out
 
 
+def run_fno_study(M, torch, runs=64, snaps=24, window=8, steps_per_eval=20):
+    """The network the learned-surrogate configuration names -- a 4-layer
+    spectral-convolution network (FNO: lift 1x1 to 32 channels, four layers
+    of a spectral convolution over 16 x 16 retained modes plus a 1x1
+    convolution, GELU between layers, projection to the 12 channels), BF16
+    1x1 convolutions, FP32 FFTs -- trained on (dm, dH_dip) pairs of the
+    plain method from `runs` seeded random-start runs of the 512x512x4 film,
+    against the library's linear stencil + spectral network trained on the
+    same runs.  Reports both networks' relative dipolar-field error against
+    the FP64 field at k = 5, 10, 20 and their cost per evaluation.  A
+    comparison study in PyTorch (torch.fft, cuBLAS 1x1 convolutions): the
+    product's surrogate is the library's own network and kernels."""
+    import torch.nn.functional as Fn
+    dims = SUR_DIMS
+    nx, ny, nz = dims
+    n = int(np.prod(dims))
+    C, W, MD, L = 3 * nz, 32, 16, 4
+    dev = "cuda"
+    g = torch.Generator(device="cpu").manual_seed(5)
+
+    def prm(*shape, scale):
+        return torch.nn.Parameter((torch.randn(*shape, generator=g) * scale).to(dev))
+
+    P = {"lift_w": prm(W, C, scale=1 / np.sqrt(C)), "lift_b": prm(W, scale=0.0),
+         "proj_w": prm(C, W, scale=1 / np.sqrt(W)), "proj_b": prm(C, scale=0.0)}
+    for l in range(L):
+        P[f"spec{l}"] = prm(W, W, MD, MD, 2, scale=1 / W)
+        P[f"pw{l}"] = prm(W, W, scale=1 / np.sqrt(W))
+        P[f"pb{l}"] = prm(W, scale=0.0)
+
+    def fno(x):   # x [B, C, ny, nx] (normalised dm) -> [B, C, ny, nx]
+        with torch.autocast("cuda", dtype=torch.bfloat16):
+            h = torch.einsum("oc,bcyx->boyx", P["lift_w"], x) + P["lift_b"][None, :, None, None]
+        h = h.float()
+        for l in range(L):
+            X = torch.fft.rfft2(h)
+            Wc = torch.view_as_complex(P[f"spec{l}"])       # [W, W, ky 16, kx 16]
+            Y = torch.zeros_like(X)
+            Y[:, :, :MD // 2, :MD] = torch.einsum("biyx,ioyx->boyx", X[:, :, :MD // 2, :MD], Wc[:, :, :MD // 2])
+            Y[:, :, -MD // 2:, :MD] = torch.einsum("biyx,ioyx->boyx", X[:, :, -MD // 2:, :MD], Wc[:, :, MD // 2:])
+            sp = torch.fft.irfft2(Y, s=h.shape[-2:])
+            with torch.autocast("cuda", dtype=torch.bfloat16):
+                pw = torch.einsum("oc,bcyx->boyx", P[f"pw{l}"], h) + P[f"pb{l}"][None, :, None, None]
+            h = sp + pw.float()
+            if l < L - 1:
+                h = Fn.gelu(h)
+        with torch.autocast("cuda", dtype=torch.bfloat16):
+            out = torch.einsum("oc,bcyx->boyx", P["proj_w"], h) + P["proj_b"][None, :, None, None]
+        return out.float()
+
+    def chan(v):   # (3, n) numpy -> [1, C, ny, nx] on the GPU
+        return torch.as_tensor(np.asarray(v, np.float32).reshape(3 * nz, ny, nx), device=dev)[None]
+
+    ops = None
+    S = None
+    opt = torch.optim.Adam(list(P.values()), lr=1e-3)
+    sx = sy = None
+    losses = []
+    t0 = time.perf_counter()
+    for r in range(runs):
+        tss, ops, tl = _sur_system(M, dims, 3000 + r, 50, ops)
+        if S is None:
+            S = M.Surrogate(ops[-1], (16, 16), 2)
+        # the library's network on this run (its own online training)
+        S.train(tss, ops, tl, snaps, window=window, lr=2e-3)
+        dip = ops[-1]
+        for w in range(max(1, snaps // window)):
+            tss.resetFields(); dip.apply(tss)
+            m0 = np.stack(tss.spinArrays()[:3]); h0 = np.stack(tss.fieldArrays("Dipole"))
+            for j in range(1, window + 1):
+                M.run(tss, ops, tl, 1)
+                tss.resetFields(); dip.apply(tss)
+                x = chan(np.stack(tss.spinArrays()[:3]) - m0)
+                t = chan(np.stack(tss.fieldArrays("Dipole")) - h0)
+                if sx is None:   # normalisation from the first pair
+                    sx = float(x.std()) + 1e-12
+                    sy = float(t.std()) + 1e-12
+                pred = fno(x / sx)
+                loss = ((pred - t / sy) ** 2).sum() / ((t / sy) ** 2).sum()
+                opt.zero_grad()
+                loss.backward()
+                opt.step()
+                losses.append(loss.item())
+        del tss
+    train_s = time.perf_counter() - t0
+
+    # errors against the FP64 field on the held-out film (seed 1000), as the
+    # surrogate leg measures them
+    ss, _, llg = _sur_system(M, dims, 1000, 200, ops)
+    with torch.no_grad():
+        fno_np = lambda d: (fno(chan(d) / sx) * sy).cpu().numpy()[0].reshape(3, n).astype(np.float64)
+        q = max(1, len(losses) // 8)
+        out = {"workload": SUR_WORKLOAD, "runs": runs, "pairs_per_run": max(1, snaps // window) * window,
+               "train_seconds": train_s, "fno_final_rel_loss": float(np.mean(losses[-window:])),
+               "fno_rel_loss_by_eighth": [float(np.mean(losses[i * q:(i + 1) * q])) for i in range(8)], "by_k": {}}
+        for k in (5, 10, 20):
+            e_lin = _sur_error_fp64(M, S, ss, ops, llg, k, 2)
+            F = type("FNOFwd", (), {"forward": staticmethod(fno_np)})
+            e_fno = _sur_error_fp64(M, F, ss, ops, llg, k, 2)
+            out["by_k"][str(k)] = {"linear_err_mean": e_lin[0], "linear_err_max": e_lin[1],
+                                   "fno_err_mean": e_fno[0], "fno_err_max": e_fno[1], "hold_err_mean": e_lin[2]}
+        # cost per evaluation: the FNO's forward (batch 1) and the library
+        # network's forward, CUDA events; the exact FP32 dipole evaluation
+        x = torch.randn(1, C, ny, nx, device=dev)
+        for _ in range(3):
+            fno(x)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(); a.record()
+        for _ in range(steps_per_eval):
+            fno(x)
+        b.record(); torch.cuda.synchronize()
+        out["fno_us_per_eval"] = a.elapsed_time(b) * 1e3 / steps_per_eval
+    st = torch.cuda.ExternalStream(ss.stream())
+    plan = M.Plan(ss, ops, llg)
+    plan.launch(3)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ss.synchronize(); a.record(st); plan.launch(steps_per_eval); b.record(st); ss.synchronize()
+    out["plain_step_us"] = a.elapsed_time(b) * 1e3 / steps_per_eval
+    plan_nd = M.Plan(ss, ops[:3], llg)
+    plan_nd.launch(3)
+    ss.synchronize(); a.record(st); plan_nd.launch(steps_per_eval); b.record(st); ss.synchronize()
+    out["step_without_dipole_us"] = a.elapsed_time(b) * 1e3 / steps_per_eval
+    out["fno_step_lower_bound_us"] = out["step_without_dipole_us"] + out["fno_us_per_eval"]
+    # HBM bound of any implementation of the network: BF16 activations, each
+    # layer fused into one read and one write of its W channels (truncated
+    # DFTs as GEMMs, spectral inverse + 1x1 + GELU in one pass), lift and
+    # projection one pass each over their inputs and outputs
+    act = 2.0 * n / nz   # bytes per channel plane (BF16)
+    fno_bytes = L * 2 * W * act + (C + W) * act * 2
+    out["fno_hbm_bound_us"] = fno_bytes / (measured_peak()[0] * 1e9) * 1e6
+    out["fno_hbm_bound_step_us"] = out["step_without_dipole_us"] + out["fno_hbm_bound_us"]
+    out["fno_speedup_bound"] = out["plain_step_us"] / out["fno_step_lower_bound_us"]
+    out["how"] = ("both networks trained on the plain method over the same seeded random-start runs (seeds 3000..); "
+                  "errors: |H0 + net(m_j - m0) - H64(m_j)| / |H64(m_j)| over two windows of each k on the held-out "
+                  "film; fno_step_lower_bound_us: the step without the dipole plus one FNO evaluation (no exact "
+                  "evaluations, no residual check)")
+    return out
+
+
 # ----------------------------------------------------------------- Runge-Kutta
 def run_rk(M, torch, steps=20):
     """The 256x256x8 film stepped by the native RK4 scheme (RungeKutta.lua's
@@ -724,6 +863,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate comparison")
     ap.add_argument("--no-cube", action="store_true", help="skip the 256^3 open-cube precision study")
+    ap.add_argument("--fno-study", action="store_true",
+                    help="only the study of the 4-layer spectral-convolution network (PyTorch) against the library's "
+                         "surrogate network; prints its JSON line")
     ap.add_argument("--ncu-steps", type=int, default=0,
                     help="profiling driver: run this many eager steps of the workload and exit (for ncu)")
     ap.add_argument("--ncu-surrogate", type=int, default=0,
@@ -751,6 +893,12 @@ def main():
         rk = M.RungeKutta(ss, "RK4", [o for o in ops if o is not th], M.LLG.new("Quaternion"), temp=th)
         rk.step(args.ncu_rk4)
         ss.synchronize()
+        return
+    if args.fno_study:
+        import torch
+        import maglua_b200 as M
+        M.init(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"fno_study": run_fno_study(M, torch)}), flush=True)
         return
     if args.ncu_f64:
         import maglua_b200 as M
