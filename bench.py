@@ -1124,9 +1124,11 @@ def main():
             ss.netMomentAsync(k % 4)
             if k >= depth:
                 ss.netMomentWait((k - depth) % 4)
+        # the final spins' download is queued behind the last step before the
+        # host waits for the last two steps' moments
+        ss.downloadF32(hx, hy, hz)
         for k in range(max(0, args.steps - depth), args.steps):
             ss.netMomentWait(k % 4)
-        ss.downloadF32(hx, hy, hz)
         ss.synchronize()
         return time.perf_counter() - t0
 

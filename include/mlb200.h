@@ -126,8 +126,10 @@ int mlb_system_netmoment(mlb_system* s, double m, double out8[8]);
  * the system's stream and runs on a stream of its own, next to the steps
  * enqueued after it (the system's stream waits for it before it next writes
  * the spin buffer it reads); _wait blocks until that slot's copy has landed
- * and fills out8 as mlb_system_netmoment does.  A caller can launch the
- * next steps before reading this step's result. */
+ * and fills out8 as mlb_system_netmoment does (the same sums up to the
+ * order of the FP64 additions: the side-stream read runs on at most 16
+ * blocks, so that most SMs stay free for the following steps).  A caller
+ * can launch the next steps before reading this step's result. */
 int mlb_system_netmoment_async(mlb_system* s, double m, int slot);
 int mlb_system_netmoment_wait(mlb_system* s, int slot, double out8[8]);
 /* sum_i s_i . h_slot,i in FP64 (the fieldArray:dot(spinArray) energy pattern). */
