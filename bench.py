@@ -221,7 +221,7 @@ def run_batched(M, torch, steps, warmup):
 SUR_DIMS = (512, 512, 4)
 SUR_WORKLOAD = ("film 512x512x4, periodic x/y, open z (z padded to 8), J=1, K=0.02 z, g=0.05, T=0.1, "
                 "alpha=0.02, dt=0.005, LLG.Quaternion; spins from a seeded random start relaxed 200 steps; "
-                "surrogate: linear spectral-conv net (BF16 tcgen05, 16x16 modes, radius-2 stencil) trained "
+                "surrogate: linear spectral-conv net (BF16 tcgen05, 16x16 modes, radius-3 stencil) trained "
                 "online on the plain method over 8 seeded random-start runs")
 
 
@@ -286,7 +286,7 @@ def _sur_error_fp64(M, S, ss, ops, llg, k, windows):
     return float(np.mean(errs)), float(np.max(errs)), float(np.mean(hold))
 
 
-def run_surrogate(M, torch, steps, train_runs=8, train_steps=250):
+def run_surrogate(M, torch, steps, train_runs=8, train_steps=250, radius=3):
     """Plain fused FFT path vs the learned surrogate on the 512x512x4 film:
     spin-steps/s of both on the same system; the surrogate trained on the
     plain method over `train_runs` seeded random-start runs; its relative
@@ -313,7 +313,7 @@ def run_surrogate(M, torch, steps, train_runs=8, train_steps=250):
     plan_nd.launch(3)
     nodip_ms = timed(plan_nd.launch, steps)
     del plan_nd
-    S = M.Surrogate(ops[-1], (16, 16), 2)
+    S = M.Surrogate(ops[-1], (16, 16), radius)
     t0 = time.perf_counter()
     losses = []
     for r in range(train_runs):
@@ -321,7 +321,8 @@ def run_surrogate(M, torch, steps, train_runs=8, train_steps=250):
         losses.append(S.train(tss, ops, tl, train_steps, window=10, lr=2e-3))
         del tss
     train_s = time.perf_counter() - t0
-    out = {"workload": SUR_WORKLOAD, "sites": n, "plain": {"value": n / (plain_ms * 1e-3), "ms_per_step": plain_ms},
+    out = {"workload": SUR_WORKLOAD, "sites": n, "radius": radius, "modes": [16, 16],
+           "plain": {"value": n / (plain_ms * 1e-3), "ms_per_step": plain_ms},
            "without_dipole": {"ms_per_step": nodip_ms, "amdahl_ceiling": plain_ms / nodip_ms,
                               "how": "the same film's captured step without the Dipole operator: the bound on what "
                                      "replacing the dipole evaluation by anything can gain"},
@@ -347,15 +348,15 @@ def run_surrogate(M, torch, steps, train_runs=8, train_steps=250):
     return out
 
 
-def run_fno_study(M, torch, runs=64, snaps=24, window=8, steps_per_eval=20):
+def run_fno_study(M, torch, runs=64, snaps=24, window=8, steps_per_eval=20, lin_radius=2):
     """The network the learned-surrogate configuration names -- a 4-layer
     spectral-convolution network (FNO: lift 1x1 to 32 channels, four layers
     of a spectral convolution over 16 x 16 retained modes plus a 1x1
     convolution, GELU between layers, projection to the 12 channels), BF16
     1x1 convolutions, FP32 FFTs -- trained on (dm, dH_dip) pairs of the
     plain method from `runs` seeded random-start runs of the 512x512x4 film,
-    against the library's linear stencil + spectral network trained on the
-    same runs.  Reports both networks' relative dipolar-field error against
+    against the library's linear stencil + spectral network (stencil radius
+    lin_radius) trained on the same runs.  Reports both networks' relative dipolar-field error against
     the FP64 field at k = 5, 10, 20 and their cost per evaluation.  A
     comparison study in PyTorch (torch.fft, cuBLAS 1x1 convolutions): the
     product's surrogate is the library's own network and kernels."""
@@ -409,7 +410,7 @@ def run_fno_study(M, torch, runs=64, snaps=24, window=8, steps_per_eval=20):
     for r in range(runs):
         tss, ops, tl = _sur_system(M, dims, 3000 + r, 50, ops)
         if S is None:
-            S = M.Surrogate(ops[-1], (16, 16), 2)
+            S = M.Surrogate(ops[-1], (16, 16), lin_radius)
         # the library's network on this run (its own online training)
         S.train(tss, ops, tl, snaps, window=window, lr=2e-3)
         dip = ops[-1]
@@ -439,7 +440,8 @@ def run_fno_study(M, torch, runs=64, snaps=24, window=8, steps_per_eval=20):
     with torch.no_grad():
         fno_np = lambda d: (fno(chan(d) / sx) * sy).cpu().numpy()[0].reshape(3, n).astype(np.float64)
         q = max(1, len(losses) // 8)
-        out = {"workload": SUR_WORKLOAD, "runs": runs, "pairs_per_run": max(1, snaps // window) * window,
+        out = {"workload": SUR_WORKLOAD, "linear_radius": lin_radius, "runs": runs,
+               "pairs_per_run": max(1, snaps // window) * window,
                "train_seconds": train_s, "fno_final_rel_loss": float(np.mean(losses[-window:])),
                "fno_rel_loss_by_eighth": [float(np.mean(losses[i * q:(i + 1) * q])) for i in range(8)], "by_k": {}}
         for k in (5, 10, 20):
