@@ -950,9 +950,9 @@ def main():
             dip = M.Dipole(ss)
             dip.setStrength(0.05)
             ops, llg = [ex, dip], M.LLG.new("Quaternion")
-            S = M.Surrogate(dip, (16, 16), 2)
+            S = M.Surrogate(dip, (16, 16), 3)   # the surrogate leg's network
             r = np.random.default_rng(9)
-            W = r.normal(size=(25, S.C, S.C)) * 1e-3
+            W = r.normal(size=(49, S.C, S.C)) * 1e-3
             R = (r.normal(size=(16, 16, S.C, S.C)) + 1j * r.normal(size=(16, 16, S.C, S.C))) * 1e-3
             S.setParams(W, R)
             S.setSchedule(1 << 30, tol=1e30, eps=1e-6)
