@@ -299,11 +299,20 @@ struct OutArgs {
     int mode;               // 0: out = h0 + ratio * dH; 1: out = dH
 };
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+// One bulk copy global -> shared of `bytes` (a multiple of 16, both
+// addresses 16-byte aligned), completing on the mbarrier bar.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(umma::smem_u32(smem)), "l"(gmem) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     umma::smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(umma::smem_u32(bar))
+                 : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(umma::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
 
 // grid (nx / 128, ny), 128 threads (thread t owns output site x0 + t, TMEM
 // lane t).
@@ -322,26 +331,56 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
     uint8_t* Fs = Ws + DIA * DIA * WT;                         // 128 x 32 BF16
     uint8_t* Zs = Fs + 8192;                                   // CP x 32 BF16
     __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t lbar;   // the staged operands' bulk copies
     __shared__ uint32_t slot;
     __shared__ double red[2][4];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int y = blockIdx.y, x0 = blockIdx.x * 128;
-    if (tid == 0) umma::mbar_init(&bar, 1);
+    if (tid == 0) {
+        umma::mbar_init(&bar, 1);
+        umma::mbar_init(&lbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
     if (warp == 0) {
         umma::tmem_alloc(&slot, 32);
         umma::tmem_relinquish();
     }
-    // halo records (p, r, s) = 8 channels at (x0 + s - RAD, y + r - RAD), periodic
-    for (int u = tid; u < NPL * DIA * HW; u += 128) {
-        const int s = u % HW, r = (u / HW) % DIA, p = u / (HW * DIA);
-        int yy = y + r - RAD, xx = x0 + s - RAD;
-        yy = yy < 0 ? yy + k.ny : (yy >= k.ny ? yy - k.ny : yy);
-        xx = xx < 0 ? xx + k.nx : (xx >= k.nx ? xx - k.nx : xx);
-        cp_async16(Hs + p * PL + (r * HW + s) * 16, q.Xb + ((size_t)p * k.ny + yy) * k.nx + xx);
+    __syncthreads();   // the barriers' initialisation
+    // operands by bulk copies issued by warp 0, on lbar: the halo records
+    // (p, r, s) = 8 channels at (x0 + s - RAD, y + r - RAD), periodic, as
+    // three runs per halo row (the RAD records left of x0 and right of
+    // x0 + 127, wrapped at the lattice's x edges, and the 128 between), the
+    // stencil weights, the CTA's inverse x-DFT rows and the row's spectrum tile
+    constexpr uint32_t HALO = NPL * DIA * HW * 16;
+    constexpr uint32_t TX = HALO + DIA * DIA * WT + 8192 + CP * 64;
+    if (warp == 0) {
+        if (lane == 0) mbar_expect_tx(&lbar, TX);
+        __syncwarp();
+        for (int it = lane; it < NPL * DIA * 3 + 3; it += 32) {
+            if (it < NPL * DIA * 3) {
+                const int piece = it % 3, r = (it / 3) % DIA, p = it / (3 * DIA);
+                int yy = y + r - RAD;
+                yy = yy < 0 ? yy + k.ny : (yy >= k.ny ? yy - k.ny : yy);
+                const uint4* row = q.Xb + ((size_t)p * k.ny + yy) * k.nx;
+                uint8_t* dst = Hs + p * PL + r * HW * 16;
+                if (piece == 0 && RAD > 0) {
+                    const int xx = x0 - RAD < 0 ? x0 - RAD + k.nx : x0 - RAD;
+                    bulk_g2s(dst, row + xx, RAD * 16, &lbar);
+                } else if (piece == 1) {
+                    bulk_g2s(dst + RAD * 16, row + x0, 128 * 16, &lbar);
+                } else if (piece == 2 && RAD > 0) {
+                    const int xx = x0 + 128 >= k.nx ? x0 + 128 - k.nx : x0 + 128;
+                    bulk_g2s(dst + (RAD + 128) * 16, row + xx, RAD * 16, &lbar);
+                }
+            } else if (it == NPL * DIA * 3) {
+                bulk_g2s(Ws, q.Wc, DIA * DIA * WT, &lbar);
+            } else if (it == NPL * DIA * 3 + 1) {
+                bulk_g2s(Fs, q.Fc + (size_t)x0 * 64, 8192, &lbar);
+            } else {
+                bulk_g2s(Zs, q.Zb + (size_t)y * CP * 64, CP * 64, &lbar);
+            }
+        }
     }
-    for (int u = tid; u < (int)(DIA * DIA * WT / 16); u += 128) cp_async16(Ws + 16 * u, q.Wc + 16 * (size_t)u);
-    for (int u = tid; u < 512; u += 128) cp_async16(Fs + 16 * u, q.Fc + (size_t)x0 * 64 + 16 * (size_t)u);
-    for (int u = tid; u < CP * 4; u += 128) cp_async16(Zs + 16 * u, q.Zb + (size_t)y * CP * 64 + 16 * (size_t)u);
     // this thread's H0 while the copies land
     const int x = x0 + tid;
     float h0v[CP];
@@ -354,7 +393,12 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
             h0v[co] = __ldg(hp + ((size_t)(co % k.nz) * k.ny + y) * k.nx + x);
         }
     }
-    cp_async_wait_all();
+    // the operands landed (a wait that gives up flags the error and waits,
+    // bounded again, for the copies before their buffers are read)
+    if (!umma::mbar_wait(&lbar, 0, k.wait_polls)) {
+        if (lane == 0) atomicOr(q.err, 1);
+        umma::mbar_wait(&lbar, 0, kDrainPolls);
+    }
     umma::fence_async_smem();
     umma::fence_before_sync();
     __syncthreads();
