@@ -1202,6 +1202,9 @@ __global__ void __launch_bounds__(XSCfg<PX, TH>::NT, 2) k_xstep(ConvK c, FastK F
     // (row pair, x) per item, the pair's two rows the real and imaginary
     // parts of one line element
     constexpr int IP = (R2 * PX + NT - 1) / NT;
+    // (z, y) of the CTA's first row; a later row's by counting forward (no
+    // division per site)
+    const int zr0 = row0 / ny, yr0 = row0 - zr0 * ny;
 #pragma unroll 1
     for (int it = 0; it < IP; it++) {
         const int idx = threadIdx.x + it * NT;
@@ -1214,7 +1217,9 @@ __global__ void __launch_bounds__(XSCfg<PX, TH>::NT, 2) k_xstep(ConvK c, FastK F
             const int row = 2 * p + h;
             if (row < rows_here && x < nx) {
                 const float Ax = h ? Ax2.y : Ax2.x, Ay = h ? Ay2.y : Ay2.x, Az = h ? Az2.y : Az2.x;
-                const int r = row0 + row, zz = r / ny, y = r - zz * ny;
+                const int r = row0 + row;
+                int zz = zr0, y = yr0 + row;
+                while (y >= ny) { y -= ny; zz++; }
                 const size_t i = (size_t)r * nx + x;
                 hx[i] = Ax; hy[i] = Ay; hz[i] = Az;
                 float rx, ry, rz;
