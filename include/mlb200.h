@@ -605,7 +605,12 @@ int mlb_surrogate_gradients(mlb_surrogate* s, const float* const x[3], const flo
  * Kx*3*nz*ny complex FP32 values with Kx = Px/2+1 (256x256x8 needs 6.3 MB).
  * Larger lattices return MLB_ERANGE.  The operator's tensor spectrum must
  * already exist (apply the operator once to an FP32 SpinSystem of its size;
- * that call allocates), else MLB_ESTATE.  The first call on each device looks
+ * that call allocates), else MLB_ESTATE.  It is for callers that cannot
+ * allocate in the middle of a run: a host whose caching allocator already
+ * holds the GPU's memory (a PyTorch job sized to the whole device), where a
+ * cudaMalloc fails for want of memory or a cudaFree stalls the device, and
+ * loops over trial configurations that must not pay an allocation per
+ * evaluation.  The first call on each device looks
  * up the scratch's address with cudaGetSymbolAddress with that device
  * current; make it before any stream capture.  That address is kept for the
  * life of the process and does not survive a cudaDeviceReset.  The current
