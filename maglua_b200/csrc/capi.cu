@@ -5895,7 +5895,7 @@ int mlb_surrogate_create(mlb_op* op, int mx, int my, int rad, mlb_surrogate** ou
         S->err.alloc(1);
         CK(cudaMemset(S->err.p, 0, sizeof(int)));
         S->dev.alloc(1);
-        S->rnp = (nx / 128) * ny;
+        S->rnp = mlb::sur_out_ctas(nx, ny);
         S->rpart.alloc((size_t)2 * S->rnp);
 
         SurDev h{};

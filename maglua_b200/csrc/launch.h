@@ -168,6 +168,8 @@ cudaError_t launch_conv_split_yz(const ConvK& c, const FftLen& Ly, const FftLen&
                                  const void* ten6, const void* ten9, int rb, cudaStream_t st);
 // Learned surrogate (surrogate.cu).
 size_t sur_out_smem(int CP, int rad);
+// CTAs of the surrogate output kernel (one per 128 x-sites of a block of rows): its residual partials
+int sur_out_ctas(int nx, int ny);
 size_t sur_gw_smem(int C, int rad);
 size_t sur_ydft_smem(const SurK& k);
 cudaError_t sur_configure();

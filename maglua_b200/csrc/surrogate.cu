@@ -314,75 +314,90 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
                  : "memory");
 }
 
-// grid (nx / 128, ny), 128 threads (thread t owns output site x0 + t, TMEM
-// lane t).
+// Output rows per CTA: the rows' MMAs are issued together into one TMEM
+// accumulator per row and complete on one barrier, and the weights and
+// inverse x-DFT rows are staged once for all of them; warp w takes row w / 4
+// in the epilogue (TMEM lanes 32 (w % 4) ..).  Per launch of the 512x512x4
+// film's radius-3 network: 1, 2, 4 rows per CTA gave surrogate steps of
+// 115.8, 107.1, 104.8 us (k = 5), the same outputs bit for bit.
+constexpr int SUR_ROWS = 4;
+
+// grid (nx / 128, ny / SUR_ROWS), 128 SUR_ROWS threads (thread t owns output
+// site x0 + t % 128 of row y0 + t / 128, TMEM lane t % 128).  Halo planes
+// [p][DIA + SUR_ROWS - 1 rows][HW sites] of 16-byte records: the stencil
+// operand of row j and offset (oy, ox) is the view starting at record ox of
+// halo row j + oy.
 template <int CP, int RAD>
-__global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
+__global__ void __launch_bounds__(128 * SUR_ROWS) k_sur_out(SurK k, OutArgs q)
 {
     pdl_trigger();
     pdl_wait();
     if (k.skip_if && *k.skip_if) return;
-    constexpr int NPL = CP / 8, DIA = 2 * RAD + 1, HW = 128 + 2 * RAD;
-    constexpr uint32_t PL = (DIA * HW * 16 + 127) & ~127u;   // bytes per halo plane
-    constexpr uint32_t WT = CP * CP * 2;                       // bytes per offset tile
+    constexpr int NR = SUR_ROWS;
+    constexpr int NPL = CP / 8, DIA = 2 * RAD + 1, HW = 128 + 2 * RAD, HR = DIA + NR - 1;
+    constexpr uint32_t PL = (HR * HW * 16 + 127) & ~127u;      // bytes per halo plane
+    constexpr uint32_t WT = CP * CP * 2;                        // bytes per offset tile
+    constexpr uint32_t ZT = CP * 64;                            // bytes per row's spectrum tile
+    constexpr uint32_t NCOL = NR * CP < 32 ? 32 : NR * CP;      // TMEM columns: one accumulator per row
     extern __shared__ uint8_t smraw[];
     uint8_t* Hs = align1k(smraw);
     uint8_t* Ws = Hs + NPL * PL;
-    uint8_t* Fs = Ws + DIA * DIA * WT;                         // 128 x 32 BF16
-    uint8_t* Zs = Fs + 8192;                                   // CP x 32 BF16
+    uint8_t* Fs = Ws + DIA * DIA * WT;                          // 128 x 32 BF16
+    uint8_t* Zs = Fs + 8192;                                    // [NR] CP x 32 BF16
     __shared__ __align__(8) uint64_t bar;
     __shared__ __align__(8) uint64_t lbar;   // the staged operands' bulk copies
     __shared__ uint32_t slot;
-    __shared__ double red[2][4];
+    __shared__ double red[2][4 * NR];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int y = blockIdx.y, x0 = blockIdx.x * 128;
+    const int y0 = blockIdx.y * NR, x0 = blockIdx.x * 128;
+    const int row = tid >> 7, y = y0 + row;
     if (tid == 0) {
         umma::mbar_init(&bar, 1);
         umma::mbar_init(&lbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 0) {
-        umma::tmem_alloc(&slot, 32);
+        umma::tmem_alloc(&slot, NCOL);
         umma::tmem_relinquish();
     }
     __syncthreads();   // the barriers' initialisation
     // operands by bulk copies issued by warp 0, on lbar: the halo records
-    // (p, r, s) = 8 channels at (x0 + s - RAD, y + r - RAD), periodic, as
+    // (p, r, s) = 8 channels at (x0 + s - RAD, y0 + r - RAD), periodic, as
     // three runs per halo row (the RAD records left of x0 and right of
     // x0 + 127, wrapped at the lattice's x edges, and the 128 between), the
-    // stencil weights, the CTA's inverse x-DFT rows and the row's spectrum tile
-    constexpr uint32_t HALO = NPL * DIA * HW * 16;
-    constexpr uint32_t TX = HALO + DIA * DIA * WT + 8192 + CP * 64;
+    // stencil weights, the CTA's inverse x-DFT rows and the rows' spectrum tiles
+    constexpr uint32_t HALO = NPL * HR * HW * 16;
+    constexpr uint32_t TX = HALO + DIA * DIA * WT + 8192 + NR * ZT;
     if (warp == 0) {
         if (lane == 0) mbar_expect_tx(&lbar, TX);
         __syncwarp();
-        for (int it = lane; it < NPL * DIA * 3 + 3; it += 32) {
-            if (it < NPL * DIA * 3) {
-                const int piece = it % 3, r = (it / 3) % DIA, p = it / (3 * DIA);
-                int yy = y + r - RAD;
-                yy = yy < 0 ? yy + k.ny : (yy >= k.ny ? yy - k.ny : yy);
-                const uint4* row = q.Xb + ((size_t)p * k.ny + yy) * k.nx;
+        for (int it = lane; it < NPL * HR * 3 + 3; it += 32) {
+            if (it < NPL * HR * 3) {
+                const int piece = it % 3, r = (it / 3) % HR, p = it / (3 * HR);
+                int yy = (y0 + r - RAD) % k.ny;
+                yy = yy < 0 ? yy + k.ny : yy;
+                const uint4* src = q.Xb + ((size_t)p * k.ny + yy) * k.nx;
                 uint8_t* dst = Hs + p * PL + r * HW * 16;
                 if (piece == 0 && RAD > 0) {
                     const int xx = x0 - RAD < 0 ? x0 - RAD + k.nx : x0 - RAD;
-                    bulk_g2s(dst, row + xx, RAD * 16, &lbar);
+                    bulk_g2s(dst, src + xx, RAD * 16, &lbar);
                 } else if (piece == 1) {
-                    bulk_g2s(dst + RAD * 16, row + x0, 128 * 16, &lbar);
+                    bulk_g2s(dst + RAD * 16, src + x0, 128 * 16, &lbar);
                 } else if (piece == 2 && RAD > 0) {
                     const int xx = x0 + 128 >= k.nx ? x0 + 128 - k.nx : x0 + 128;
-                    bulk_g2s(dst + (RAD + 128) * 16, row + xx, RAD * 16, &lbar);
+                    bulk_g2s(dst + (RAD + 128) * 16, src + xx, RAD * 16, &lbar);
                 }
-            } else if (it == NPL * DIA * 3) {
+            } else if (it == NPL * HR * 3) {
                 bulk_g2s(Ws, q.Wc, DIA * DIA * WT, &lbar);
-            } else if (it == NPL * DIA * 3 + 1) {
+            } else if (it == NPL * HR * 3 + 1) {
                 bulk_g2s(Fs, q.Fc + (size_t)x0 * 64, 8192, &lbar);
             } else {
-                bulk_g2s(Zs, q.Zb + (size_t)y * CP * 64, CP * 64, &lbar);
+                bulk_g2s(Zs, q.Zb + (size_t)y0 * ZT, NR * ZT, &lbar);
             }
         }
     }
     // this thread's H0 while the copies land
-    const int x = x0 + tid;
+    const int x = x0 + (tid & 127);
     float h0v[CP];
 #pragma unroll
     for (int co = 0; co < CP; co++) {
@@ -409,19 +424,29 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
             const uint32_t id = umma::idesc_bf16_f32(128, CP);
             const uint32_t hs = umma::smem_u32(Hs), ws = umma::smem_u32(Ws), fs = umma::smem_u32(Fs),
                            zs = umma::smem_u32(Zs);
+            // each row's accumulator takes its MMAs in the order of a
+            // one-row tile (offsets, then the spectral pair); the rows
+            // alternate per offset so that each weight tile's descriptor
+            // serves every row at once
 #pragma unroll
             for (int o = 0; o < DIA * DIA; o++) {
-                const uint32_t site = (uint32_t)((o / DIA) * HW + o % DIA) * 16;
 #pragma unroll
-                for (int kk = 0; kk < CP / 16; kk++)
-                    umma::mma_bf16(taddr, umma::desc_nosw(hs + 2 * kk * PL + site, PL, 128),
-                                   umma::desc_nosw(ws + o * WT + kk * 256, 128, (CP / 8) * 128), id,
-                                   (o | kk) ? 1u : 0u);
+                for (int kk = 0; kk < CP / 16; kk++) {
+                    const uint64_t bd = umma::desc_nosw(ws + o * WT + kk * 256, 128, (CP / 8) * 128);
+#pragma unroll
+                    for (int j = 0; j < NR; j++) {
+                        const uint32_t site = (uint32_t)((j + o / DIA) * HW + o % DIA) * 16;
+                        umma::mma_bf16(taddr + (uint32_t)(j * CP), umma::desc_nosw(hs + 2 * kk * PL + site, PL, 128),
+                                       bd, id, (o | kk) ? 1u : 0u);
+                    }
+                }
             }
 #pragma unroll
             for (int ks = 0; ks < 2; ks++)
-                umma::mma_bf16(taddr, umma::desc_nosw(fs + ks * 256, 128, 512), umma::desc_nosw(zs + ks * 256, 128, 512),
-                               id, 1u);
+#pragma unroll
+                for (int j = 0; j < NR; j++)
+                    umma::mma_bf16(taddr + (uint32_t)(j * CP), umma::desc_nosw(fs + ks * 256, 128, 512),
+                                   umma::desc_nosw(zs + j * ZT + ks * 256, 128, 512), id, 1u);
             umma::mma_commit(&bar);
         }
         __syncwarp();
@@ -438,7 +463,7 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
 #pragma unroll
     for (int cb = 0; cb < CP / 16; cb++) {
         float v[16];
-        umma::tmem_ld16(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)(16 * cb), v);
+        umma::tmem_ld16(taddr + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(row * CP + 16 * cb), v);
 #pragma unroll
         for (int j = 0; j < 16; j++) {
             const int co = 16 * cb + j;
@@ -459,7 +484,7 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
     }
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(taddr, 32);
+    if (warp == 0) umma::tmem_dealloc(taddr, NCOL);
     if (q.mode == 1 || !q.part) return;
     // residual statistics: this CTA's sums (k_sur_advance reduces them)
     for (int s = 16; s > 0; s >>= 1) {
@@ -470,7 +495,7 @@ __global__ void __launch_bounds__(128) k_sur_out(SurK k, OutArgs q)
     __syncthreads();
     if (tid == 0) {
         double a = 0, b = 0;
-        for (int w = 0; w < 4; w++) { a += red[0][w]; b += red[1][w]; }
+        for (int w = 0; w < 4 * NR; w++) { a += red[0][w]; b += red[1][w]; }
         const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
         q.part[2 * cta] = a;
         q.part[2 * cta + 1] = b;
@@ -696,9 +721,11 @@ namespace mlb {
 size_t sur_out_smem(int CP, int rad)
 {
     const int dia = 2 * rad + 1, hw = 128 + 2 * rad;
-    const size_t pl = (size_t)((dia * hw * 16 + 127) & ~127);
-    return 1024 + (CP / 8) * pl + (size_t)dia * dia * CP * CP * 2 + 8192 + (size_t)CP * 64;
+    const size_t pl = (size_t)(((dia + SUR_ROWS - 1) * hw * 16 + 127) & ~127);
+    return 1024 + (CP / 8) * pl + (size_t)dia * dia * CP * CP * 2 + 8192 + (size_t)SUR_ROWS * CP * 64;
 }
+
+int sur_out_ctas(int nx, int ny) { return (nx / 128) * (ny / SUR_ROWS); }
 
 template <int CP, int RAD>
 static cudaError_t out_attr()
@@ -770,10 +797,10 @@ cudaError_t launch_sur_out(const SurK& k, const uint4* Xb, const float* const h0
         q.out[c] = out[c];
     }
     q.Wc = Wc; q.Fc = Fc; q.Zb = Zb; q.dev = dev; q.part = part; q.err = err; q.mode = mode;
-    dim3 g(k.nx / 128, k.ny);
+    dim3 g(k.nx / 128, k.ny / SUR_ROWS);
     const size_t sm = sur_out_smem(k.CP, k.rad);
     cudaError_t e = cudaSuccess;
-#define MLB_SUR_OUT(CPV, RV) launch_pdl(k_sur_out<CPV, RV>, g, dim3(128), sm, st, k, q)
+#define MLB_SUR_OUT(CPV, RV) launch_pdl(k_sur_out<CPV, RV>, g, dim3(128 * SUR_ROWS), sm, st, k, q)
     if (k.CP == 16) {
         switch (k.rad) {
         case 0: e = MLB_SUR_OUT(16, 0); break;
