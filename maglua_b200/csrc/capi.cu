@@ -361,6 +361,10 @@ struct mlb_llg {
 // (index q + 2 c); c = 1 when the convolution's SPEC already holds the
 // forward x transform of the current spins (left there by the previous
 // step's fused x pass), so the step starts at the (y,z) pass.
+// Carried steps captured in one graph by a plan (an even count: a graph
+// starts and ends on the same spin buffer).
+constexpr int kMultiSteps = 4;
+
 struct mlb_plan {
     mlb_system* s = nullptr;
     std::vector<mlb_op*> ops;
@@ -369,6 +373,10 @@ struct mlb_plan {
     bool timeline = false;          // device timeline of the fused (y,z) and x passes
     DBuf<unsigned long long> tl;    // its four stamps (ConvK::tl)
     cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    // carried steady state: kMultiSteps consecutive steps in one graph per
+    // starting parity (null: none; plans with event nodes or a device
+    // timeline keep one step per graph)
+    cudaGraphExec_t multi[2] = {nullptr, nullptr};
     std::vector<mlb::ProfCaptured> ev[4];
     mlb_op* carry_op = nullptr;   // the convolution whose SPEC a step leaves carried (null: none)
     std::vector<mlb::ProfCaptured>* last = nullptr;
@@ -2256,6 +2264,10 @@ void plan_timeline_reset(mlb_plan* p)
 
 void plan_release(mlb_plan* p)
 {
+    for (int q = 0; q < 2; q++) {
+        if (p->multi[q]) cudaGraphExecDestroy(p->multi[q]);
+        p->multi[q] = nullptr;
+    }
     for (int q = 0; q < 4; q++) {
         if (p->exec[q]) cudaGraphExecDestroy(p->exec[q]);
         p->exec[q] = nullptr;
@@ -2328,6 +2340,48 @@ void plan_capture(mlb_plan* p)
             if (e != cudaSuccess) fail(MLB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
             load_state(s, p->ops, h0);
         }
+        // kMultiSteps carried steps in one graph: the host logic of the steps
+        // runs one after the other while the stream is captured, so the
+        // graph holds the single-step graphs' kernels in sequence with the
+        // dependent-launch edges kept across the step boundaries (the next
+        // step's first pass is scheduled while the last one drains).  A step
+        // that does not end in the fused x pass leaves the plan without it.
+        if (p->carry_op && !p->timing && !p->timeline) {
+            for (int q = 0; q < 2; q++) {
+                s->cur = q;
+                cudaGraph_t graph = nullptr;
+                CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+                s->capturing = true;
+                bool ok = true;
+                try {
+                    for (int j = 0; j < kMultiSteps && ok; j++) {
+                        s->cap_carry = true;
+                        s->cap_xstep = nullptr;
+                        do_step(s, p->ops.data(), nops, p->l);
+                        ok = s->cap_xstep == p->carry_op;
+                        advance_sweep(p->ops.data(), nops);
+                    }
+                } catch (Err&) {
+                    ok = false;
+                }
+                s->capturing = false;
+                s->cap_carry = false;
+                cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+                if (ok && e == cudaSuccess) e = cudaGraphInstantiate(&p->multi[q], graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                if (!ok || e != cudaSuccess) {
+                    cudaGetLastError();
+                    p->multi[q] = nullptr;
+                }
+                load_state(s, p->ops, h0);
+            }
+            if (!p->multi[0] || !p->multi[1]) {
+                for (int q = 0; q < 2; q++) {
+                    if (p->multi[q]) cudaGraphExecDestroy(p->multi[q]);
+                    p->multi[q] = nullptr;
+                }
+            }
+        }
     } catch (...) {
         s->dry = false;
         s->capturing = false;
@@ -2383,6 +2437,23 @@ void plan_launch(mlb_plan* p, int nsteps)
     ConvPlan* CP = p->carry_op ? p->carry_op->plan.get() : nullptr;
     for (int k = 0; k < nsteps; k++) {
         const bool carry = CP && s->spec_token != 0 && s->spec_token == CP->spec_token;
+        if (carry && p->multi[s->cur] && nsteps - k >= kMultiSteps) {
+            // kMultiSteps carried steps in one launch; they write both spin
+            // buffers
+            nm_guard(s, -1);
+            CK(cudaGraphLaunch(p->multi[s->cur], s->st));
+            p->last = nullptr;
+            for (int j = 0; j < kMultiSteps; j++, k++) {
+                CP->spec_token = ++g_spec_token;
+                s->spec_token = CP->spec_token;
+                if (k < nsteps - 1) {
+                    advance_host(p);
+                    advance_sweep(p->ops.data(), (int)p->ops.size());
+                }
+            }
+            k--;   // the loop's increment
+            continue;
+        }
         const int gi = s->cur + (carry ? 2 : 0);
         nm_guard(s, 1 - s->cur);   // the step writes the other spin buffer
         CK(cudaGraphLaunch(p->exec[gi], s->st));
