@@ -394,9 +394,11 @@ int mlb_llg_decode(const void* buf, size_t len, mlb_llg** out, size_t* used, int
  * B200 extension (the reference steps from Lua, one operator call at a time):
  * a plan captures the canonical step of a system (resetFields; each op's
  * apply; sumFields; llg:apply) as CUDA graphs so that one host call
- * enqueues a whole step.  The Thermal counter and the applied field (with
- * its sweep) advance on the device; any other parameter change makes the
- * next launch capture again.  With timing = 1, every kernel of the step is
+ * enqueues a whole step.  Once a step leaves the convolution's x spectrum
+ * carried, runs of four or more steps go four to a graph (dependent launches
+ * across the step boundaries).  The Thermal counter and the applied field
+ * (with its sweep) advance on the device; any other parameter change makes
+ * the next launch capture again.  With timing = 1, every kernel of the step is
  * bracketed by graph event nodes and mlb_plan_kernel_times returns the
  * milliseconds of the last launched step per kernel (48-byte name slots).
  * With timing = 2 the step keeps its dependent launches and the fused (y,z)
