@@ -1246,7 +1246,7 @@ def main():
         "step_roofline": {"bytes_per_spin_step": bytes_step / n, "achieved_gbs": step_bytes_gbs,
                           "frac": step_bytes_gbs / peak, "K_points": Kk},
         "steady_state_l2_resident": {"value": n * args.steps / (ss_ms * 1e-3), "ms_per_step": ss_ms / args.steps,
-                                     "how": "the same captured step launched back to back, no flush"},
+                                     "how": "the same plan launched for all the steps back to back (carried steps four to a graph), no flush"},
         "film_without_dipole": {"ms_per_step": nodip_ms / args.steps, "amdahl_ceiling": ss_ms / nodip_ms,
                                 "how": "the film's captured step without the Dipole operator, back to back, no flush: "
                                        "the bound on what replacing the dipole evaluation by anything can gain"},
